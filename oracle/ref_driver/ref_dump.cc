@@ -1,0 +1,459 @@
+// Oracle driver over the compiled reference (strict FP64 build).  Test infrastructure only.
+//
+//   snapi_ref_dump pack   <job.cfg> <out.tsk>
+//       Parse a reference job config (run in a directory holding the reference's atom/molecule
+//       configs and atmosphere file) and write a task blob: the packed 1-column atmosphere,
+//       the packed node model and the observation's wavelength grid.
+//   snapi_ref_dump dump   <task.tsk> <nodes.f64> <npix> <flags> <out.sbin>
+//       For each pixel's node vector: build_from_nodes, then dump the column record the GPU
+//       path consumes, the reference Stokes (obs_stokes) and, by flag, the reference node
+//       responses (obs_stokes_responses_to_nodes), the record tangents d(record)/d(node)
+//       (central differences of build_from_nodes / interpolate_from_nodes with the
+//       reference's own steps) and the reference's normalised opacity at a few wavelengths.
+//   snapi_ref_dump lmfit  <task.tsk> <nodes0.f64> <target.f64> <mask.f64> <npix> <iters> <out.sbin>
+//       Run stokes_lm_fit per pixel from the initial nodes against target Stokes.
+//
+// flags: 1 = responses, 2 = tangents, 4 = opacity probe (pixel 0 only)
+//
+// Output ".sbin": a sequence of arrays [int32 name_len][name][int32 ndim][int64 dims...]
+// [float64 data], read by tests/golden/sbin.py.
+#include "ref_common.h"
+
+struct SbinWriter {
+  FILE *f;
+  explicit SbinWriter(const char *fn) { f = fopen(fn, "wb"); if (!f) { perror(fn); exit(2); } }
+  ~SbinWriter() { fclose(f); }
+  void put(const std::string &name, const std::vector<int64_t> &dims, const double *d) {
+    int32_t nl = name.size(); fwrite(&nl, 4, 1, f); fwrite(name.data(), 1, nl, f);
+    int32_t nd = dims.size(); fwrite(&nd, 4, 1, f);
+    int64_t n = 1;
+    for (auto x : dims) { fwrite(&x, 8, 1, f); n *= x; }
+    fwrite(d, 8, n, f);
+  }
+};
+
+// ----------------------------------------------------------------------------------------------
+// pack: jsub-side job set-up
+static int do_pack(const char *cfgname, const char *outname) {
+  const char *argv[] = {"snapi_ref_dump", "-cfg", cfgname, "-q", "-q", "-q", 0};
+  const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
+  int ac = 6; cmdln cmd(ac, (char **)argv, options, maps);
+  io_class io(cmd);
+  struct gcfg cfg(cmd, io);
+  char wd[4096];
+  if (!getcwd(wd, sizeof wd)) return 2;
+  // reference flow: construct from cfg, pack, unpack, init, extract one column
+  atmosphere *a0 = atmos_new(cfg.atm[0], io);
+  int32_t sz = a0->size(io);
+  uint8_t *buf = new uint8_t[sz];
+  a0->pack(buf, 0, io);
+  int32_t offs = 0;
+  atmosphere *a1 = atmos_new(buf, offs, 0, io);
+  a1->init(wd, &io);
+  atmosphere *col = a1->extract(1, 1, io);
+  std::vector<uint8_t> abuf(col->size(io));
+  col->pack(abuf.data(), 0, io);
+  model *m = model_new(cfg.mod[0], io);
+  std::vector<uint8_t> mbuf(m->size(io));
+  m->pack(mbuf.data(), 0, io);
+
+  FILE *f = fopen(outname, "wb");
+  fwrite("SNAPITSK", 1, 8, f);
+  int32_t nl = cfg.obs[0]->nlambda;
+  double el = cfg.obs[0]->el, az = cfg.obs[0]->az;
+  fwrite(&nl, 4, 1, f); fwrite(&el, 8, 1, f); fwrite(&az, 8, 1, f);
+  fwrite(cfg.obs[0]->lambda, 8, nl, f);
+  int32_t n = abuf.size(); fwrite(&n, 4, 1, f); fwrite(abuf.data(), 1, n, f);
+  n = mbuf.size(); fwrite(&n, 4, 1, f); fwrite(mbuf.data(), 1, n, f);
+  fclose(f);
+  fprintf(stderr, "packed task: nd=%d nlambda=%d el=%g az=%g nodes=%d\n",
+          col->x3h - col->x3l + 1, nl, el, az, m->get_N_nodes_total());
+  return 0;
+}
+
+// ----------------------------------------------------------------------------------------------
+// Column record: the per-depth state that obs_stokes uses before its wavelength loop.
+struct LineInfo {
+  int species, z, lo, up, split;
+  double lam0, sf, ar, mass, A;
+  int n[3];
+  std::vector<double> S[3], D[3];
+};
+
+struct Record {
+  int nd = 0, nlines = 0;
+  std::vector<double> tau500;           // [nd]  tau500 (positive), top -> bottom
+  std::vector<double> T, vt, ne, vlos, B, inc, azi, kap, hmbf, hmff, bfop, bfem;  // [nd]
+  std::vector<double> lop, lem, lgc;    // [nlines][nd]
+  std::vector<double> dld, adamp;       // [nlines][nd] reference's own Doppler width / damping
+  std::vector<LineInfo> lines;
+  bool bf_edge_in_window = false;
+};
+
+static const int NFIELD = 12;  // per-depth scalar fields before the per-line fields
+
+// Opens the atmosphere state exactly as atmosphere::obs_stokes does (atmos/atmos_obs.cc:22-57),
+// then reads every per-depth quantity that feeds atmosphere::op_em_vector.
+static void extract_record(atmosphere *a, const Task &t, Record &r, std::vector<double> *opprobe,
+                           const std::vector<int> &probe_l) {
+  const int x3l = a->x3l, x3h = a->x3h, nd = x3h - x3l + 1;
+  const fp_t theta = t.el, phi = t.az;
+  a->set_grid(a->tau_grid);
+  a->boundary_condition_for_rt = -1;
+  a->popsetup();
+  a->compute_op_referent();
+  if (!a->tau_grid) a->compute_tau_referent();
+  a->nltepops();
+  a->atm_pop_setup();
+  a->atm_pop_fill();
+  fp_t ***Vr = a->project(a->Vx, a->Vy, a->Vz, theta, phi, 1, 1, 1, 1, x3l, x3h);
+  fp_t ****Bt = a->transform(a->Bx, a->By, a->Bz, theta, phi, 1, 1, 1, 1, x3l, x3h);
+  for (int i = 0; i < a->natm; ++i) { a->atml[i]->rtsetup(1, 1, 1, 1, x3l, x3h); a->atml[i]->zeeman_setup(); }
+  fp_t *lv = airtovac((fp_t *)t.lambda.data(), t.nlambda) - 1;
+  const int nl = t.nlambda;
+
+  r.nd = nd;
+  auto rs = [&](std::vector<double> &v) { v.assign(nd, 0.0); };
+  rs(r.tau500); rs(r.T); rs(r.vt); rs(r.ne); rs(r.vlos); rs(r.B); rs(r.inc); rs(r.azi);
+  rs(r.kap); rs(r.hmbf); rs(r.hmff); rs(r.bfop); rs(r.bfem);
+  h_minus_mol *hm = 0;
+  for (int i = 0; i < a->natm; ++i) if (!hm) hm = dynamic_cast<h_minus_mol *>(a->atml[i]);
+  for (int kk = 0; kk < nd; ++kk) {
+    int x = x3l + kk;
+    fp_t T = a->T[1][1][x], Ne = a->Ne[1][1][x];
+    r.tau500[kk] = -a->rt_grid[x];
+    r.T[kk] = T; r.vt[kk] = a->Vt[1][1][x]; r.ne[kk] = Ne; r.vlos[kk] = Vr[1][1][x];
+    r.B[kk] = Bt[1][1][1][x]; r.inc[kk] = Bt[2][1][1][x]; r.azi[kk] = Bt[3][1][1][x];
+    r.kap[kk] = a->op_referent[1][1][x];
+    if (hm) {
+      fp_t nH0 = hm->fetch_population(1, 1, x, 0, 0);
+      fp_t tp = 5040.0 / T;
+      r.hmbf[kk] = 4.158E-28 * Ne * k * T * pow(tp, 2.5) * pow(10.0, 0.754 * tp) * nH0;
+      r.hmff[kk] = 1E-26 * Ne * k * T * nH0;
+    }
+  }
+  // bound-free totals (atom::boundfree_op_em_vector), flat within the window below the edge
+  fp_t ******op = ft6dim(1, nl, 1, 1, 1, 1, x3l, x3h, 1, 4, 1, 4);
+  fp_t *****em = ft5dim(1, nl, 1, 1, 1, 1, x3l, x3h, 1, 4);
+  memset(op[1][1][1][x3l][1] + 1, 0, nl * nd * 16 * sizeof(fp_t));
+  memset(em[1][1][1][x3l] + 1, 0, nl * nd * 4 * sizeof(fp_t));
+  for (int i = 0; i < a->natm; ++i)
+    if (atom *at = dynamic_cast<atom *>(a->atml[i]))
+      at->boundfree_op_em_vector(a->T, a->Ne, Vr, theta, phi, lv, nl, op, em);
+  for (int kk = 0; kk < nd; ++kk) {
+    r.bfop[kk] = op[1][1][1][x3l + kk][1][1];
+    r.bfem[kk] = em[1][1][1][x3l + kk][1];
+    if (op[nl][1][1][x3l + kk][1][1] != r.bfop[kk]) r.bf_edge_in_window = true;
+  }
+  // bound-bound transitions (atom::boundbound_op_em_vector, A > 1)
+  r.lines.clear();
+  std::vector<std::vector<double>> lop, lem, lgc, ldld, la;
+  for (int i = 0; i < a->natm; ++i) {
+    atom *at = dynamic_cast<atom *>(a->atml[i]);
+    if (!at) continue;
+    for (int z = 0; z <= at->Z; ++z)
+      for (int up = 1; up < at->nl[z]; ++up)
+        for (int lo = 0; lo < up; ++lo) {
+          if (!(at->A[z][up][lo] > 1E0)) continue;
+          LineInfo L;
+          L.species = i; L.z = z; L.lo = lo; L.up = up;
+          L.lam0 = h * c / (at->ee[z][up] - at->ee[z][lo]);
+          L.ar = at->damp_rad(at->A[z], lo, up);
+          L.sf = L.lam0 * L.lam0 / (4.0 * pi * c);
+          L.mass = at->mass;
+          L.A = at->A[z][up][lo];
+          int tr = at->tmap[z][up][lo];
+          L.split = at->split[tr];
+          for (int gi = 0; gi < 3; ++gi) L.n[gi] = 0;
+          if (L.split) {
+            fp_t *Sx[3] = {at->S_p[tr], at->S_b[tr], at->S_r[tr]};
+            fp_t *Dx[3] = {at->delta_lambda_p[tr], at->delta_lambda_b[tr], at->delta_lambda_r[tr]};
+            for (int gi = 0; gi < 3; ++gi) {
+              L.n[gi] = at->nm[tr][gi];
+              L.S[gi].assign(Sx[gi], Sx[gi] + L.n[gi]);
+              L.D[gi].assign(Dx[gi], Dx[gi] + L.n[gi]);
+            }
+          }
+          std::vector<double> o(nd), em_(nd), gcv(nd), dd(nd), aa(nd);
+          fp_t Blu = at->B[z][lo][up], Bul = at->B[z][up][lo];
+          for (int kk = 0; kk < nd; ++kk) {
+            int x = x3l + kk;
+            fp_t T = a->T[1][1][x], Ne = a->Ne[1][1][x];
+            o[kk] = (at->pop[1][1][x].n[z][lo] * Blu - at->pop[1][1][x].n[z][up] * Bul) * h * c / L.lam0 / 4.0 / pi;
+            em_[kk] = at->pop[1][1][x].n[z][up] * L.A * h * c / L.lam0 / 4.0 / pi;
+            gcv[kk] = at->damp_col(1, 1, x, z, up, lo, T, Ne, L.lam0);
+            dd[kk] = at->broad_dop(L.lam0, T, a->Vt[1][1][x]);
+            aa[kk] = L.sf * (L.ar + gcv[kk] * turn_on_damping) / dd[kk];
+          }
+          r.lines.push_back(L);
+          lop.push_back(o); lem.push_back(em_); lgc.push_back(gcv); ldld.push_back(dd); la.push_back(aa);
+        }
+  }
+  r.nlines = r.lines.size();
+  r.lop.clear(); r.lem.clear(); r.lgc.clear(); r.dld.clear(); r.adamp.clear();
+  for (int j = 0; j < r.nlines; ++j) {
+    r.lop.insert(r.lop.end(), lop[j].begin(), lop[j].end());
+    r.lem.insert(r.lem.end(), lem[j].begin(), lem[j].end());
+    r.lgc.insert(r.lgc.end(), lgc[j].begin(), lgc[j].end());
+    r.dld.insert(r.dld.end(), ldld[j].begin(), ldld[j].end());
+    r.adamp.insert(r.adamp.end(), la[j].begin(), la[j].end());
+  }
+  // optional: the reference's full normalised opacity at a few wavelengths
+  if (opprobe) {
+    a->op_em_vector(Vr, Bt, theta, phi, lv, nl, op, em);
+    opprobe->clear();
+    for (int li : probe_l) {
+      if (a->tau_grid) a->normalize_to_referent_opacity(op[li + 1], em[li + 1]);
+      for (int kk = 0; kk < nd; ++kk) {
+        for (int s = 1; s <= 4; ++s)
+          for (int sp = 1; sp <= 4; ++sp) opprobe->push_back(op[li + 1][1][1][x3l + kk][s][sp]);
+        for (int s = 1; s <= 4; ++s) opprobe->push_back(em[li + 1][1][1][x3l + kk][s]);
+      }
+    }
+  }
+  del_ft6dim(op, 1, nl, 1, 1, 1, 1, x3l, x3h, 1, 4, 1, 4);
+  del_ft5dim(em, 1, nl, 1, 1, 1, 1, x3l, x3h, 1, 4);
+  delete[] (lv + 1);
+  del_ft4dim(Bt, 1, 3, 1, 1, 1, 1, x3l, x3h);
+  del_ft3dim(Vr, 1, 1, 1, 1, x3l, x3h);
+  for (int i = 0; i < a->natm; ++i) { a->atml[i]->rtclean(0, 0, 1, 1, 1, 1, x3l, x3h); a->atml[i]->zeeman_clear(); }
+  a->popclean();
+}
+
+// record -> flat vector [nd][NFIELD + 3*nlines] (depth-major), the layout of the tangents
+static std::vector<double> record_flat(const Record &r) {
+  int nf = NFIELD + 3 * r.nlines;
+  std::vector<double> v(r.nd * nf);
+  for (int kk = 0; kk < r.nd; ++kk) {
+    double *p = &v[kk * nf];
+    p[0] = r.T[kk]; p[1] = r.vt[kk]; p[2] = r.ne[kk]; p[3] = r.vlos[kk]; p[4] = r.B[kk];
+    p[5] = r.inc[kk]; p[6] = r.azi[kk]; p[7] = r.kap[kk]; p[8] = r.hmbf[kk]; p[9] = r.hmff[kk];
+    p[10] = r.bfop[kk]; p[11] = r.bfem[kk];
+    for (int j = 0; j < r.nlines; ++j) {
+      p[NFIELD + 3 * j + 0] = r.lop[j * r.nd + kk];
+      p[NFIELD + 3 * j + 1] = r.lem[j * r.nd + kk];
+      p[NFIELD + 3 * j + 2] = r.lgc[j * r.nd + kk];
+    }
+  }
+  return v;
+}
+
+static void set_nodes(model *m, const double *nodes) {
+  int np = m->get_N_nodes_total();
+  fp_t *p = new fp_t[np] - 1;
+  for (int i = 0; i < np; ++i) p[i + 1] = nodes[i];
+  m->set_parameters(p);
+  delete[] (p + 1);
+}
+
+static double node_step(model *m, int p /*1-based*/) {
+  switch (m->which_parameter(p)) {
+    case 1: return delta_T;
+    case 2: return delta_vt;
+    case 3: return delta_vr;
+    case 4: return delta_B;
+    default: return delta_angle;
+  }
+}
+
+static int do_dump(const char *tskname, const char *nodesname, int npix, int flags, const char *outname) {
+  const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
+  const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
+  int ac = 4; cmdln cmd(ac, (char **)argv, options, maps);
+  io_class io(cmd);
+  Task t = load_task(tskname);
+  std::vector<uint8_t> nb = read_file_bytes(nodesname);
+  const double *nodes = (const double *)nb.data();
+  model *m = task_model(t, io);
+  const int np = m->get_N_nodes_total(), nl = t.nlambda;
+  if ((int)(nb.size() / 8) < npix * np) { fprintf(stderr, "nodes file too short\n"); return 2; }
+  fp_t *lam1 = lambda_1based(t);
+
+  std::vector<double> allrec, allstokes, allresp, alltan, allrf_ok, alldld, alla, tau;
+  std::vector<double> opprobe;
+  std::vector<int> probe_l = {0, 40, 80, 100, 120, 160, 200};
+  Record r0;
+  int nd = 0, nf = 0;
+  double t_build = 0, t_synth = 0, t_resp = 0;
+  for (int ip = 0; ip < npix; ++ip) {
+    atmosphere *a = task_atmos(t, io);
+    set_nodes(m, nodes + ip * np);
+    double t0 = wall_s();
+    a->build_from_nodes(m);
+    t_build += wall_s() - t0;
+    Record r;
+    extract_record(a, t, r, (ip == 0 && (flags & 4)) ? &opprobe : 0, probe_l);
+    if (ip == 0) { r0 = r; nd = r.nd; nf = NFIELD + 3 * r.nlines; tau = r.tau500; }
+    std::vector<double> fl = record_flat(r);
+    allrec.insert(allrec.end(), fl.begin(), fl.end());
+    alldld.insert(alldld.end(), r.dld.begin(), r.dld.end());
+    alla.insert(alla.end(), r.adamp.begin(), r.adamp.end());
+    for (int kk = 0; kk < nd; ++kk)
+      if (fabs(r.tau500[kk] - tau[kk]) > 1e-12 * tau[kk]) { fprintf(stderr, "tau grid differs between pixels\n"); return 3; }
+    // reference synthesis
+    t0 = wall_s();
+    observable *o = a->obs_stokes(t.el, t.az, lam1, nl);
+    t_synth += wall_s() - t0;
+    fp_t **S = o->get_S(1, 1);
+    for (int l = 1; l <= nl; ++l) for (int s = 1; s <= 4; ++s) allstokes.push_back(S[s][l]);
+    del_ft2dim(S, 1, 4, 1, nl);
+    delete o;
+    // reference node responses (semi-analytic)
+    if (flags & 1) {
+      fp_t ***resp = ft3dim(1, np, 1, nl, 1, 4);
+      t0 = wall_s();
+      observable *o2 = a->obs_stokes_responses_to_nodes(m, t.el, t.az, lam1, nl, resp, 0);
+      t_resp += wall_s() - t0;
+      for (int p = 1; p <= np; ++p) for (int l = 1; l <= nl; ++l) for (int s = 1; s <= 4; ++s) allresp.push_back(resp[p][l][s]);
+      del_ft3dim(resp, 1, np, 1, nl, 1, 4);
+      delete o2;
+    }
+    // record tangents by central differences of the node -> atmosphere map
+    if (flags & 2) {
+      for (int p = 1; p <= np; ++p) {
+        double st = node_step(m, p);
+        bool thermal = (m->which_parameter(p) == 1);
+        std::vector<double> plus, minus;
+        for (int side = 0; side < 2; ++side) {
+          atmosphere *b = task_atmos(t, io);
+          m->perturb_node_value(p, side == 0 ? 0.5 * st : -0.5 * st);
+          b->build_from_nodes(m);   // T nodes: full build (HE + chemistry), as atmos_fit.cc:1227-1249
+          if (!thermal) {           // other nodes: base build, then interpolation only (:1253-1307)
+            m->perturb_node_value(p, side == 0 ? -0.5 * st : 0.5 * st);
+            b->build_from_nodes(m);
+            m->perturb_node_value(p, side == 0 ? 0.5 * st : -0.5 * st);
+            b->interpolate_from_nodes(m);
+          }
+          m->perturb_node_value(p, side == 0 ? -0.5 * st : 0.5 * st);
+          Record rr;
+          extract_record(b, t, rr, 0, probe_l);
+          (side == 0 ? plus : minus) = record_flat(rr);
+          delete b;
+        }
+        for (size_t i = 0; i < plus.size(); ++i) alltan.push_back((plus[i] - minus[i]) / st);
+      }
+    }
+    delete a;
+  }
+  fprintf(stderr, "ref timings per pixel: build %.4f s, obs_stokes %.4f s, responses %.4f s\n",
+          t_build / npix, t_synth / npix, (flags & 1) ? t_resp / npix : 0.0);
+
+  SbinWriter w(outname);
+  double meta[8] = {(double)nd, (double)nl, (double)np, (double)r0.nlines, (double)NFIELD, t.el, t.az,
+                    r0.bf_edge_in_window ? 1.0 : 0.0};
+  w.put("meta", {8}, meta);
+  w.put("lambda_air", {nl}, t.lambda.data());
+  w.put("tau500", {nd}, tau.data());
+  w.put("nodes", {npix, np}, nodes);
+  std::vector<double> which(np);
+  for (int p = 1; p <= np; ++p) which[p - 1] = m->which_parameter(p);
+  w.put("node_kind", {np}, which.data());
+  // line constants: [nlines][8] = lam0, sf, ar, mass, A, split, species, z ; patterns [nlines][3][2][16]
+  std::vector<double> lc, pat(r0.nlines * 3 * 2 * 16, 0.0), pn(r0.nlines * 3, 0.0);
+  for (int j = 0; j < r0.nlines; ++j) {
+    const LineInfo &L = r0.lines[j];
+    double v[8] = {L.lam0, L.sf, L.ar, L.mass, L.A, (double)L.split, (double)L.species, (double)L.z};
+    lc.insert(lc.end(), v, v + 8);
+    for (int gi = 0; gi < 3; ++gi) {
+      pn[j * 3 + gi] = L.n[gi];
+      for (int i = 0; i < L.n[gi] && i < 16; ++i) {
+        pat[((j * 3 + gi) * 2 + 0) * 16 + i] = L.S[gi][i];
+        pat[((j * 3 + gi) * 2 + 1) * 16 + i] = L.D[gi][i];
+      }
+    }
+  }
+  w.put("line_const", {r0.nlines, 8}, lc.data());
+  w.put("line_ncomp", {r0.nlines, 3}, pn.data());
+  w.put("line_pattern", {r0.nlines, 3, 2, 16}, pat.data());
+  w.put("record", {npix, nd, nf}, allrec.data());
+  w.put("ref_dld", {npix, r0.nlines, nd}, alldld.data());
+  w.put("ref_adamp", {npix, r0.nlines, nd}, alla.data());
+  w.put("stokes", {npix, nl, 4}, allstokes.data());
+  if (flags & 1) w.put("responses", {npix, np, nl, 4}, allresp.data());
+  if (flags & 2) w.put("tangent", {npix, np, nd, nf}, alltan.data());
+  if (flags & 4) {
+    std::vector<double> pl(probe_l.begin(), probe_l.end());
+    w.put("probe_l", {(int64_t)pl.size()}, pl.data());
+    w.put("opacity_probe", {(int64_t)probe_l.size(), nd, 20}, opprobe.data());
+  }
+  double tm[3] = {t_build / npix, t_synth / npix, (flags & 1) ? t_resp / npix : 0.0};
+  w.put("ref_seconds_per_pixel", {3}, tm);
+  delete m;
+  delete[] (lam1 + 1);
+  return 0;
+}
+
+// ----------------------------------------------------------------------------------------------
+// lmfit: reference LM inversion per pixel (atmos_fit.cc:18-227)
+static int do_lmfit(const char *tskname, const char *n0name, const char *tgtname, const char *maskname,
+                    int npix, int iters, const char *outname) {
+  const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
+  const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
+  int ac = 4; cmdln cmd(ac, (char **)argv, options, maps);
+  io_class io(cmd);
+  Task t = load_task(tskname);
+  std::vector<uint8_t> nb = read_file_bytes(n0name), tb = read_file_bytes(tgtname), mb = read_file_bytes(maskname);
+  const double *n0 = (const double *)nb.data(), *tgt = (const double *)tb.data(), *msk = (const double *)mb.data();
+  model *m = task_model(t, io);
+  const int np = m->get_N_nodes_total(), nl = t.nlambda;
+  fp_t *lam1 = lambda_1based(t);
+  std::vector<double> out_nodes, out_stokes, out_chi;
+  double t_fit = 0;
+  for (int ip = 0; ip < npix; ++ip) {
+    atmosphere *a = task_atmos(t, io);
+    model *mm = task_model(t, io);
+    set_nodes(mm, n0 + ip * np);
+    observable *o = new observable(1, 1, 4, nl);
+    o->set_lambda(lam1);
+    fp_t ****S = ft4dim(1, 1, 1, 1, 1, 4, 1, nl);
+    for (int l = 0; l < nl; ++l) for (int s = 0; s < 4; ++s) S[1][1][s + 1][l + 1] = tgt[(ip * nl + l) * 4 + s];
+    o->set(S);
+    del_ft4dim(S, 1, 1, 1, 1, 1, 4, 1, nl);
+    fp_t *mask = new fp_t[nl] - 1;
+    for (int l = 0; l < nl; ++l) mask[l + 1] = msk[ip * nl + l];
+    o->set_mask(mask);
+    delete[] (mask + 1);
+    o->set_viewing_angle(t.el, t.az);
+    o->set_to_invert(1);
+    o->set_no_iterations(iters);
+    o->set_start_lambda(1E3);
+    o->set_stopping_chisq(1E-30);
+    fp_t ws[4] = {1.0, 1.0, 1.0, 1.0};
+    o->set_w_stokes(ws);
+    o->set_inv_parameters(0.0, 0.0, 1.0, 1.0);
+    double t0 = wall_s();
+    observable *fit = a->stokes_lm_fit(o, t.el, t.az, mm);
+    t_fit += wall_s() - t0;
+    for (int p = 1; p <= np; ++p) out_nodes.push_back(mm->get_parameter(p));
+    fp_t **F = fit->get_S(1, 1);
+    double chi = 0;
+    for (int l = 1; l <= nl; ++l)
+      for (int s = 1; s <= 4; ++s) {
+        out_stokes.push_back(F[s][l]);
+        double d = (tgt[(ip * nl + l - 1) * 4 + s - 1] - F[s][l]) * msk[ip * nl + l - 1];
+        chi += d * d;
+      }
+    out_chi.push_back(chi);
+    del_ft2dim(F, 1, 4, 1, nl);
+    delete fit; delete o; delete mm; delete a;
+  }
+  SbinWriter w(outname);
+  w.put("fit_nodes", {npix, np}, out_nodes.data());
+  w.put("fit_stokes", {npix, nl, 4}, out_stokes.data());
+  w.put("fit_chi2", {npix}, out_chi.data());
+  double tf = t_fit / npix;
+  w.put("ref_seconds_per_pixel", {1}, &tf);
+  delete m;
+  delete[] (lam1 + 1);
+  return 0;
+}
+
+int main(int argc, char **argv) {
+  if (argc >= 4 && !strcmp(argv[1], "pack")) return do_pack(argv[2], argv[3]);
+  if (argc >= 7 && !strcmp(argv[1], "dump"))
+    return do_dump(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]), argv[6]);
+  if (argc >= 9 && !strcmp(argv[1], "lmfit"))
+    return do_lmfit(argv[2], argv[3], argv[4], argv[5], atoi(argv[6]), atoi(argv[7]), argv[8]);
+  fprintf(stderr, "usage: snapi_ref_dump pack|dump|lmfit ...\n");
+  return 1;
+}
