@@ -1,0 +1,136 @@
+/*
+ * libsnapi_cuda -- B200 (sm_100a) drop-in for SNAPI's per-pixel Stokes hot path.
+ *
+ * Plain C ABI: plain pointers and sizes, no C++ or torch types.  One context per host thread;
+ * calls on one context are serialised on the context's CUDA stream and return when done.
+ *
+ * Interfaces replaced (paths within the reference project):
+ *   atmosphere::obs_stokes                     atmos/atmos.h:275, atmos/atmos_obs.cc:16-87
+ *       -> snapi_synth
+ *   atmosphere::obs_stokes_responses_to_nodes  atmos/atmos.h:269, atmos/atmos_fit.cc:1205-1352,
+ *   (+ obs_stokes_responses, formal_pert_numerical)  atmos/atmos_rad_synthesis.cc:166-399,
+ *                                              atmos/plpar/atmos_ppbez_rts.cc:1780-1857
+ *       -> snapi_responses (forward mode), snapi_adjoint (reverse mode, chi2 gradient)
+ *   atmosphere::stokes_lm_fit (one damped step)  atmos/atmos.h:300, atmos/atmos_fit.cc:93-205
+ *       -> snapi_lm_step
+ *   atom::zeeman_setup                         atmos/atmol/atom/atom.cc:1620-1773
+ *       -> snapi_zeeman_pattern
+ *
+ * Data model.  The caller (the reference's islave, after build_from_nodes / chemistry) marshals
+ * each pixel's column into a "record": depth-major float32 [nd][nfield] with
+ * nfield = SNAPI_NFIELD0 + 3 * nlines:
+ *   0 T [K]   1 v_turb [cm/s]   2 n_e [cm^-3]   3 v_los projected on the ray [cm/s]
+ *   4 |B| [G] 5 inclination [deg, ray frame]   6 azimuth [deg, ray frame]   7 kappa_500 [cm^-1]
+ *   8 H- bound-free factor 4.158e-28 n_e k T theta^2.5 10^(0.754 theta) n_H0
+ *   9 H- free-free factor 1e-26 n_e k T n_H0            (theta = 5040/T)
+ *   10 bound-free opacity of all atoms   11 bound-free emissivity of all atoms
+ *   12+3j  line j opacity factor  (n_l B_lu - n_u B_ul) h c / (4 pi lambda0)
+ *   13+3j  line j emissivity factor n_u A_ul h c / (4 pi lambda0)
+ *   14+3j  line j collisional damping rate (atom::damp_col)
+ * Records of npix pixels are contiguous.  Depth index 0 is the top of the atmosphere.
+ *
+ * Node tangents for the gradient / responses: float32 [npix][npar][nd][nfield], the derivative
+ * of each record field with respect to each node (the reference builds the same map with
+ * central differences of build_from_nodes / interpolate_from_nodes, atmos_fit.cc:1225-1307).
+ *
+ * Memory: every array argument lives either in host memory (mem = SNAPI_MEM_HOST; the call
+ * copies in and out, pinned memory from snapi_host_alloc is fastest) or in device memory of the
+ * context's GPU (mem = SNAPI_MEM_DEVICE; no copies).
+ */
+#ifndef SNAPI_CUDA_H
+#define SNAPI_CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SNAPI_OK 0
+#define SNAPI_EINVAL (-1)
+#define SNAPI_ECUDA (-2)
+#define SNAPI_ETIMEOUT (-3)
+#define SNAPI_ENONCONV (-4)
+#define SNAPI_ENOMEM (-5)
+
+#define SNAPI_MEM_HOST 0
+#define SNAPI_MEM_DEVICE 1
+
+#define SNAPI_NFIELD0 12
+#define SNAPI_MAX_LINES 8
+#define SNAPI_MAX_COMP 16
+#define SNAPI_MAX_LAMBDA 1024
+
+typedef struct snapi_ctx snapi_ctx;
+
+/* One spectral line (bound-bound transition with A > 1, atom_rad_synthesis.cc:403). */
+typedef struct {
+  double lam0;           /* vacuum line centre [cm] = h c / (E_u - E_l) */
+  double sf;             /* lam0^2 / (4 pi c) */
+  double ar;             /* radiative damping rate, atom::damp_rad [s^-1] */
+  double mass;           /* atomic mass [g] */
+  int split;             /* 1: Zeeman split (pattern below), 0: single Voigt profile */
+  int ncomp[3];          /* number of pi, sigma_b, sigma_r components */
+  double S[3][SNAPI_MAX_COMP];  /* component strengths, normalised per group */
+  double D[3][SNAPI_MAX_COMP];  /* component shifts in units of lambda_B = 4.67e-5 lam0^2 B */
+} snapi_line;
+
+typedef struct {
+  int nd;                    /* depth points (>= 3) */
+  int nlambda;               /* wavelengths (1..SNAPI_MAX_LAMBDA) */
+  int nlines;                /* lines (0..SNAPI_MAX_LINES) */
+  const double *lambda_air;  /* [nlambda] air wavelengths [cm]; converted with airtovac */
+  const double *tau500;      /* [nd] tau_500 of the depth grid, increasing top -> bottom */
+  double mu;                 /* cosine of the ray to the outward normal (reference: -cos(EL)), (0,1] */
+  const snapi_line *lines;   /* [nlines] */
+  double stokes_scale;       /* chi2 is computed internally in units of stokes_scale^2 (> 0) */
+  int max_batch;             /* pixels per device batch (sizes the work buffers); 0 = 4096 */
+} snapi_problem;
+
+/* Create a context on CUDA device `device`.  Returns NULL on error (status set). */
+snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status);
+void snapi_destroy(snapi_ctx *ctx);
+/* Last error message of the context (never NULL). */
+const char *snapi_last_error(const snapi_ctx *ctx);
+
+/* Stokes synthesis: stokes [npix][nlambda][4] (I, Q, U, V), from records [npix][nd][nfield]. */
+int snapi_synth(snapi_ctx *ctx, int npix, const float *records, float *stokes, int mem);
+
+/* Synthesis + chi2 + its gradient w.r.t. npar nodes in one forward and one reverse (adjoint)
+ * sweep.  obs [npix][nlambda][4]; w_stokes [4]; mask [npix][nlambda] (NULL = all ones);
+ * tangents [npix][npar][nd][nfield] (NULL when npar == 0).
+ * chi2 = sum_{l,s} ((obs - S) w_s mask_l)^2 (atmos_fit.cc:239-248).
+ * Outputs: stokes (may be NULL), chi2 [npix], grad [npix][npar] (d chi2 / d node),
+ * rec_grad [npix][nd][nfield] (d chi2 / d record field; may be NULL). */
+int snapi_adjoint(snapi_ctx *ctx, int npix, const float *records, const float *obs, const double *w_stokes,
+                  const float *mask, int npar, const float *tangents, float *stokes, double *chi2,
+                  double *grad, double *rec_grad, int mem);
+
+/* Node responses (forward mode): dstokes [npix][npar][nlambda][4] = d Stokes / d node, the
+ * quantity obs_stokes_responses_to_nodes returns; stokes may be NULL. */
+int snapi_responses(snapi_ctx *ctx, int npix, const float *records, int npar, const float *tangents,
+                    float *stokes, float *dstokes, int mem);
+
+/* Plain finite-difference gradient (the baseline the adjoint replaces): for each node p the
+ * records are perturbed by +-step[p] * tangent_p and synthesised again (2 npar + 1 solves).
+ * step [npar] in node units. */
+int snapi_fd_grad(snapi_ctx *ctx, int npix, const float *records, const float *obs, const double *w_stokes,
+                  const float *mask, int npar, const float *tangents, const double *step, double *chi2,
+                  double *grad, int mem);
+
+/* Zeeman pattern of a transition, 2J values ju2 / jl2 and Lande factors (atom::zeeman_setup). */
+int snapi_zeeman_pattern(int ju2, int jl2, double g_upper, double g_lower, snapi_line *line);
+
+/* Pinned host memory for SNAPI_MEM_HOST arguments. */
+void *snapi_host_alloc(size_t bytes);
+void snapi_host_free(void *p);
+
+/* The context's CUDA stream (a cudaStream_t) and the device time of the kernels of the last
+ * call, measured with CUDA events on that stream [ms]. */
+void *snapi_stream(snapi_ctx *ctx);
+double snapi_last_kernel_ms(const snapi_ctx *ctx);
+/* Number of kernel launches of the last call. */
+int snapi_last_launches(const snapi_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,278 @@
+"""Python host mirror of the C ABI of libsnapi_cuda (include/snapi_cuda.h).
+
+The calls mirror the reference's per-pixel entry points (atmos/atmos.h):
+  Context.synth       ~ atmosphere::obs_stokes(theta, phi, lambda, nlambda)
+  Context.adjoint     ~ chi2 and d chi2 / d nodes of atmosphere::stokes_lm_fit's inner loop,
+                        evaluated by reverse mode instead of obs_stokes_responses_to_nodes
+  Context.responses   ~ atmosphere::obs_stokes_responses_to_nodes
+  Context.fd_grad     ~ the plain finite-difference gradient the adjoint replaces
+but batched over pixels.  Arrays are numpy (host) or raw device pointers (int) with mem=DEVICE.
+Errors raise SnapiError with the library's message; there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libsnapi_cuda.so")
+
+OK, EINVAL, ECUDA, ETIMEOUT, ENONCONV, ENOMEM = 0, -1, -2, -3, -4, -5
+MEM_HOST, MEM_DEVICE = 0, 1
+NFIELD0 = 12
+MAX_LINES = 8
+MAX_COMP = 16
+
+# record field indices (include/snapi_cuda.h)
+F_T, F_VT, F_NE, F_VLOS, F_B, F_INC, F_AZI, F_KAP, F_HMBF, F_HMFF, F_BFOP, F_BFEM = range(12)
+FIELD_NAMES = ["T", "vt", "ne", "vlos", "B", "inc", "azi", "kap500", "hm_bf", "hm_ff", "bf_op", "bf_em"]
+
+
+class SnapiError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("snapi error %d: %s" % (code, msg))
+        self.code = code
+
+
+class SnapiLine(ctypes.Structure):
+    """Mirror of snapi_line."""
+    _fields_ = [
+        ("lam0", ctypes.c_double),
+        ("sf", ctypes.c_double),
+        ("ar", ctypes.c_double),
+        ("mass", ctypes.c_double),
+        ("split", ctypes.c_int),
+        ("ncomp", ctypes.c_int * 3),
+        ("S", (ctypes.c_double * MAX_COMP) * 3),
+        ("D", (ctypes.c_double * MAX_COMP) * 3),
+    ]
+
+
+class SnapiProblem(ctypes.Structure):
+    _fields_ = [
+        ("nd", ctypes.c_int),
+        ("nlambda", ctypes.c_int),
+        ("nlines", ctypes.c_int),
+        ("lambda_air", ctypes.POINTER(ctypes.c_double)),
+        ("tau500", ctypes.POINTER(ctypes.c_double)),
+        ("mu", ctypes.c_double),
+        ("lines", ctypes.POINTER(SnapiLine)),
+        ("stokes_scale", ctypes.c_double),
+        ("max_batch", ctypes.c_int),
+    ]
+
+
+_LIB = None
+
+
+def lib():
+    """Load libsnapi_cuda.so (raises if it was not built: there is no fallback)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libsnapi_cuda.so is missing: run `python -m snapi_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, dp, fp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_int
+        L.snapi_create.restype = vp
+        L.snapi_create.argtypes = [ctypes.POINTER(SnapiProblem), ip, ctypes.POINTER(ctypes.c_int)]
+        L.snapi_destroy.argtypes = [vp]
+        L.snapi_last_error.restype = ctypes.c_char_p
+        L.snapi_last_error.argtypes = [vp]
+        L.snapi_synth.argtypes = [vp, ip, fp, fp, ip]
+        L.snapi_adjoint.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, fp, ip]
+        L.snapi_responses.argtypes = [vp, ip, fp, ip, fp, fp, fp, ip]
+        L.snapi_fd_grad.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, ip]
+        L.snapi_zeeman_pattern.argtypes = [ip, ip, ctypes.c_double, ctypes.c_double, ctypes.POINTER(SnapiLine)]
+        L.snapi_host_alloc.restype = vp
+        L.snapi_host_alloc.argtypes = [ctypes.c_size_t]
+        L.snapi_host_free.argtypes = [vp]
+        L.snapi_stream.restype = vp
+        L.snapi_stream.argtypes = [vp]
+        L.snapi_last_kernel_ms.restype = ctypes.c_double
+        L.snapi_last_kernel_ms.argtypes = [vp]
+        L.snapi_last_launches.restype = ip
+        L.snapi_last_launches.argtypes = [vp]
+        if hasattr(L, "snapi_lm_step"):
+            L.snapi_lm_step.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, fp, fp, fp, ip]
+        _LIB = L
+    return _LIB
+
+
+def zeeman_pattern(ju2, jl2, g_upper, g_lower):
+    line = SnapiLine()
+    rc = lib().snapi_zeeman_pattern(int(ju2), int(jl2), float(g_upper), float(g_lower), ctypes.byref(line))
+    if rc != OK:
+        raise SnapiError(rc, "zeeman_pattern")
+    return line
+
+
+def lines_from_arrays(line_const, line_ncomp, line_pattern):
+    """snapi_line array from arrays: line_const [n, >=6] = (lam0, sf, ar, mass, A, split),
+    line_ncomp [n, 3], line_pattern [n, 3, 2, 16] (strengths, shifts)."""
+    n = int(line_const.shape[0])
+    arr = (SnapiLine * max(n, 1))()
+    for j in range(n):
+        L = arr[j]
+        L.lam0, L.sf, L.ar, L.mass = (float(v) for v in line_const[j, :4])
+        L.split = int(line_const[j, 5])
+        for g in range(3):
+            L.ncomp[g] = int(line_ncomp[j, g])
+            for i in range(MAX_COMP):
+                L.S[g][i] = float(line_pattern[j, g, 0, i])
+                L.D[g][i] = float(line_pattern[j, g, 1, i])
+    return arr, n
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return ctypes.c_void_p(a)
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Context:
+    """A libsnapi_cuda context for one problem geometry (depth grid, wavelengths, line list)."""
+
+    def __init__(self, lambda_air, tau500, lines, nlines, mu=1.0, stokes_scale=1.0, max_batch=4096, device=0):
+        self._lam = np.ascontiguousarray(lambda_air, dtype=np.float64)
+        self._tau = np.ascontiguousarray(tau500, dtype=np.float64)
+        self._lines = lines
+        self.nd = int(self._tau.shape[0])
+        self.nl = int(self._lam.shape[0])
+        self.nlines = int(nlines)
+        self.nfield = NFIELD0 + 3 * self.nlines
+        prob = SnapiProblem()
+        prob.nd, prob.nlambda, prob.nlines = self.nd, self.nl, self.nlines
+        prob.lambda_air = self._lam.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        prob.tau500 = self._tau.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        prob.mu = float(mu)
+        prob.lines = ctypes.cast(lines, ctypes.POINTER(SnapiLine))
+        prob.stokes_scale = float(stokes_scale)
+        prob.max_batch = int(max_batch)
+        st = ctypes.c_int(0)
+        self._ctx = lib().snapi_create(ctypes.byref(prob), int(device), ctypes.byref(st))
+        if not self._ctx:
+            raise SnapiError(st.value, "snapi_create failed")
+
+    @classmethod
+    def from_fixture(cls, fx, **kw):
+        """Context from a fixture / problem dict (lambda_air, tau500, line_const, line_ncomp, line_pattern)."""
+        lines, n = lines_from_arrays(fx["line_const"], fx["line_ncomp"], fx["line_pattern"])
+        return cls(fx["lambda_air"], fx["tau500"], lines, n, **kw)
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            lib().snapi_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != OK:
+            raise SnapiError(rc, lib().snapi_last_error(self._ctx).decode())
+
+    @property
+    def stream(self):
+        return lib().snapi_stream(self._ctx)
+
+    @property
+    def last_kernel_ms(self):
+        return lib().snapi_last_kernel_ms(self._ctx)
+
+    @property
+    def last_launches(self):
+        return lib().snapi_last_launches(self._ctx)
+
+    def _npix(self, records):
+        r = np.asarray(records)
+        if r.ndim != 3 or r.shape[1] != self.nd or r.shape[2] != self.nfield:
+            raise ValueError("records must be [npix, %d, %d]" % (self.nd, self.nfield))
+        return r.shape[0]
+
+    # --- host-memory API ------------------------------------------------------------------
+    def synth(self, records):
+        """Stokes [npix, nlambda, 4] from records [npix, nd, nfield] (obs_stokes, batched)."""
+        rec = _f32(records)
+        npix = self._npix(rec)
+        out = np.zeros((npix, self.nl, 4), np.float32)
+        self._check(lib().snapi_synth(self._ctx, npix, _ptr(rec), _ptr(out), MEM_HOST))
+        return out
+
+    def adjoint(self, records, obs, tangents=None, w_stokes=(1.0, 1.0, 1.0, 1.0), mask=None, want_stokes=True,
+                want_rec_grad=False):
+        """chi2 [npix], d chi2/d node [npix, npar] (and Stokes, d chi2 / d record) by one forward and
+        one reverse sweep."""
+        rec = _f32(records)
+        npix = self._npix(rec)
+        ob = _f32(obs)
+        tn = _f32(tangents)
+        npar = 0 if tn is None else tn.shape[1]
+        mk = _f32(mask)
+        ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
+        st = np.zeros((npix, self.nl, 4), np.float32) if want_stokes else None
+        chi2 = np.zeros(npix)
+        grad = np.zeros((npix, max(npar, 1)))
+        rg = np.zeros((npix, self.nd, self.nfield)) if want_rec_grad else None
+        self._check(lib().snapi_adjoint(self._ctx, npix, _ptr(rec), _ptr(ob), _ptr(ws), _ptr(mk), npar, _ptr(tn),
+                                        _ptr(st), _ptr(chi2), _ptr(grad), _ptr(rg), MEM_HOST))
+        out = {"chi2": chi2, "grad": grad[:, :npar]}
+        if want_stokes:
+            out["stokes"] = st
+        if want_rec_grad:
+            out["rec_grad"] = rg
+        return out
+
+    def fd_grad(self, records, obs, tangents, step, w_stokes=(1.0, 1.0, 1.0, 1.0), mask=None):
+        rec = _f32(records)
+        npix = self._npix(rec)
+        ob = _f32(obs)
+        tn = _f32(tangents)
+        npar = tn.shape[1]
+        mk = _f32(mask)
+        ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
+        stp = np.ascontiguousarray(np.broadcast_to(step, (npar,)), dtype=np.float64)
+        chi2 = np.zeros(npix)
+        grad = np.zeros((npix, npar))
+        self._check(lib().snapi_fd_grad(self._ctx, npix, _ptr(rec), _ptr(ob), _ptr(ws), _ptr(mk), npar, _ptr(tn),
+                                        _ptr(stp), _ptr(chi2), _ptr(grad), MEM_HOST))
+        return {"chi2": chi2, "grad": grad}
+
+    def responses(self, records, tangents, want_stokes=True):
+        """d Stokes / d node [npix, npar, nlambda, 4] (obs_stokes_responses_to_nodes, batched)."""
+        rec = _f32(records)
+        npix = self._npix(rec)
+        tn = _f32(tangents)
+        npar = tn.shape[1]
+        st = np.zeros((npix, self.nl, 4), np.float32) if want_stokes else None
+        ds = np.zeros((npix, npar, self.nl, 4), np.float32)
+        self._check(lib().snapi_responses(self._ctx, npix, _ptr(rec), npar, _ptr(tn), _ptr(st), _ptr(ds), MEM_HOST))
+        return (st, ds) if want_stokes else ds
+
+    # --- device-memory API (raw pointers, e.g. torch tensor .data_ptr()) --------------------
+    def synth_device(self, npix, rec_ptr, stokes_ptr):
+        self._check(lib().snapi_synth(self._ctx, int(npix), _ptr(int(rec_ptr)), _ptr(int(stokes_ptr)), MEM_DEVICE))
+
+    def adjoint_device(self, npix, rec_ptr, obs_ptr, npar, tan_ptr, chi2_ptr, grad_ptr, stokes_ptr=None,
+                       mask_ptr=None, w_stokes=(1.0, 1.0, 1.0, 1.0)):
+        ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
+        self._check(lib().snapi_adjoint(self._ctx, int(npix), _ptr(int(rec_ptr)), _ptr(int(obs_ptr)), _ptr(ws),
+                                        _ptr(int(mask_ptr)) if mask_ptr else None, int(npar), _ptr(int(tan_ptr)),
+                                        _ptr(int(stokes_ptr)) if stokes_ptr else None, _ptr(int(chi2_ptr)),
+                                        _ptr(int(grad_ptr)), None, MEM_DEVICE))
+
+    def fd_grad_device(self, npix, rec_ptr, obs_ptr, npar, tan_ptr, step, chi2_ptr, grad_ptr,
+                       w_stokes=(1.0, 1.0, 1.0, 1.0)):
+        ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
+        stp = np.ascontiguousarray(np.broadcast_to(step, (npar,)), dtype=np.float64)
+        self._check(lib().snapi_fd_grad(self._ctx, int(npix), _ptr(int(rec_ptr)), _ptr(int(obs_ptr)), _ptr(ws),
+                                        None, int(npar), _ptr(int(tan_ptr)), _ptr(stp), _ptr(int(chi2_ptr)),
+                                        _ptr(int(grad_ptr)), MEM_DEVICE))

@@ -1,0 +1,65 @@
+"""Build libsnapi_cuda.so in-tree for sm_100a (nvcc), plus the test-side helpers.
+
+The library is plain CUDA C++ with a C ABI (include/snapi_cuda.h); no PyTorch is linked.
+"""
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB = os.path.join(PKG, "libsnapi_cuda.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+SOURCES = ["snapi_cuda.cu", "snapi_resp.cu", "snapi_lm.cu"]
+HEADERS = ["snapi_core.cuh", "snapi_sweep.cuh", "snapi_internal.cuh"]
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
+
+
+def build_cuda(force=False, verbose=False):
+    srcs = [os.path.join(CSRC, s) for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "snapi_cuda.h")]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+                           "-Xptxas", "-v" if verbose else "-O3", "-o", LIB] + srcs
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed for libsnapi_cuda.so")
+    if verbose:
+        sys.stderr.write(r.stderr)
+    return LIB
+
+
+def build_oracle():
+    """Compile the oracle's C restatement (test infrastructure) and, when the reference sources are
+    present, the compiled-reference drivers."""
+    odir = os.path.join(ROOT, "oracle")
+    subprocess.run(["make", "-s", "-C", odir, "oracle"], check=True)
+    if os.path.isdir("/root/reference"):
+        subprocess.run(["make", "-s", "-j8", "-C", odir, "ref"], check=True)
+
+
+def build_emulator():
+    """CPU emulator of the kernels (test infrastructure)."""
+    src = os.path.join(ROOT, "tests", "emu", "snapi_emu.cc")
+    out = os.path.join(ROOT, "tests", "emu", "libsnapi_emu.so")
+    deps = [src, os.path.join(CSRC, "snapi_core.cuh"), os.path.join(CSRC, "snapi_sweep.cuh")]
+    if _stale(out, deps):
+        subprocess.run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-o", out, src], check=True)
+    return out
+
+
+if __name__ == "__main__":
+    build_cuda(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    build_oracle()
+    build_emulator()
+    print(LIB)

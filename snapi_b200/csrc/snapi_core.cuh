@@ -1,0 +1,794 @@
+// snapi_core.cuh -- per-cell math of the B200 Stokes synthesis / adjoint path.
+//
+// Everything here is __host__ __device__ so that the CUDA kernels (snapi_cuda.cu) and the
+// CPU emulator used by the tests run the same FP32 arithmetic.
+//
+// Physics follows the reference:
+//   W4 Voigt-Faraday                  cmlib/profiles.cc:7-37
+//   Zeeman pi / sigma assembly        atmos/atmol/atom/atom_rad_synthesis.cc:416-499
+//   Thomson, bound-free, H-           atmos/atmos_rad_synthesis.cc:31-50,
+//                                     atmos/atmol/atom/atom_rad_synthesis.cc:226-262,
+//                                     atmos/atmol/mol/mol.cc:379-412, :516-632
+//   normalisation by kappa_500        atmos/atmos_rad.cc:175-185
+//   polarized linear-DELO step        atmos/plpar/atmos_ppbez_rts.cc:1055-1197 (w2 = 0 branch:
+//                                     bezier_delimiter = 1e10 is never exceeded, :13, :1073)
+//   Bezier optical depth              atmos/plpar/atmos_ppbez_rts.cc:962-988
+// The adjoint functions are hand-written reverse-mode derivatives of exactly these forms
+// (including the W4 region formulas, not the Faddeeva identity), so the gradient is the
+// gradient of the forward model that is actually evaluated.
+#pragma once
+
+#include <math.h>
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define SNAPI_HD __host__ __device__ __forceinline__
+#else
+#define SNAPI_HD inline
+#endif
+
+namespace snapi {
+
+// ---------------------------------------------------------------------------------------------
+// Column record layout (per pixel, depth-major [nd][nfield], nfield = 12 + 3*nlines)
+enum RecField : int {
+  F_T = 0, F_VT = 1, F_NE = 2, F_VLOS = 3, F_B = 4, F_INC = 5, F_AZI = 6, F_KAP = 7,
+  F_HMBF = 8, F_HMFF = 9, F_BFOP = 10, F_BFEM = 11, F_LINE0 = 12
+};
+constexpr int kMaxLines = 8;
+constexpr int kMaxComp = 16;      // per Zeeman group
+constexpr int kNumRed = 10;       // depth-level adjoint sums that are not per line
+constexpr int kRedPerLine = 6;    // per-line depth-level adjoint sums
+
+// reduced adjoint vector per depth: [kNumRed + kRedPerLine*nlines]
+enum RedIdx : int {
+  R_COP = 0, R_CEM = 1, R_HB = 2, R_HF = 3, R_INVT = 4, R_LT = 5,
+  R_ST2 = 6, R_CTB = 7, R_C2 = 8, R_S2 = 9
+};
+enum RedLine : int { RL_OPN = 0, RL_EMN = 1, RL_XL = 2, RL_XD = 3, RL_B = 4, RL_A = 5 };
+
+// physical constants as the reference defines them (cmlib/const.h)
+constexpr double kC = 2.99792458E10;
+constexpr double kH = 6.6260687652E-27;
+constexpr double kK = 1.3806503E-16;
+constexpr double kPi = 3.141592653589793238462643383279502884197169399375105;
+constexpr float kSqrtPiInv = 1.0f / 1.77245386399759f;
+constexpr float kSigmaT = 6.65E-25f;
+constexpr float kLn10 = 2.302585092994046f;
+
+// per-line constants (identical for every pixel)
+struct LineConst {
+  double lam0;         // vacuum line centre [cm]
+  float sf;            // lam0^2 / (4 pi c)
+  float ar;            // radiative damping
+  float two_k_over_m;  // 2 k / mass
+  float lam0_over_c;
+  float zee;           // 4.67e-5 * lam0^2 (Zeeman splitting per Gauss)
+  int split;
+  int ncomp[3];
+  int comp_off;        // offset of this line's components in the component table
+};
+
+// per-wavelength constants of one thread
+struct LamConst {
+  float lam;           // vacuum wavelength [cm]
+  float afud;          // H- bound-free alpha(lambda) * fudge
+  float F0, f1, f2;    // H- free-free exponent coefficients (F0 includes log10(fudge))
+  float xs;            // h c / (lambda k)  (stimulated emission)
+  float xp;            // 1.4387769 / lambda (Planck)
+  float pp;            // 2 h c^2 / lambda^5 (Planck prefactor, reference's constants)
+};
+
+// per-depth, per-pixel constants (wavelength independent), built from the record
+struct DepthConst {
+  float cop, cem;      // normalised flat continuum opacity / emissivity
+  float beta;          // v_los / c
+  float st2, ctb, opc2, c2, s2;  // sin^2 theta_B, cos theta_B, 1+cos^2, cos 2phi, sin 2phi
+  float hb, hf;        // H- bound-free / free-free depth factors (normalised)
+  float invT, lt;      // 1/T, log10(5040/T)
+};
+struct LineDepth {
+  float inv_dld, a, bsh, opn, emn;
+};
+
+// ---------------------------------------------------------------------------------------------
+// small complex helpers (the reference's own formulation of * and /, cmlib/types.h:28-55)
+struct cf { float re, im; };
+SNAPI_HD cf cmk(float r, float i) { cf z; z.re = r; z.im = i; return z; }
+SNAPI_HD cf cadd(cf a, cf b) { return cmk(a.re + b.re, a.im + b.im); }
+SNAPI_HD cf csub(cf a, cf b) { return cmk(a.re - b.re, a.im - b.im); }
+SNAPI_HD cf cmul(cf a, cf b) { return cmk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+SNAPI_HD cf cdiv(cf a, cf b) {
+  float f = b.re * b.re + b.im * b.im;
+  return cmk((a.re * b.re + a.im * b.im) / f, (a.im * b.re - a.re * b.im) / f);
+}
+SNAPI_HD cf caddr(float a, cf b) { return cmk(b.re + a, b.im); }
+SNAPI_HD cf csubr(float a, cf b) { return cmk(a - b.re, -b.im); }
+SNAPI_HD cf cscl(cf a, float s) { return cmk(a.re * s, a.im * s); }
+struct cd { double re, im; };
+SNAPI_HD cd dmk(double r, double i) { cd z; z.re = r; z.im = i; return z; }
+SNAPI_HD cd dadd(cd a, cd b) { return dmk(a.re + b.re, a.im + b.im); }
+SNAPI_HD cd dsub(cd a, cd b) { return dmk(a.re - b.re, a.im - b.im); }
+SNAPI_HD cd dmul(cd a, cd b) { return dmk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+SNAPI_HD cd ddiv(cd a, cd b) {
+  double f = b.re * b.re + b.im * b.im;
+  return dmk((a.re * b.re + a.im * b.im) / f, (a.im * b.re - a.re * b.im) / f);
+}
+SNAPI_HD cd daddr(double a, cd b) { return dmk(b.re + a, b.im); }
+SNAPI_HD cd dsubr(double a, cd b) { return dmk(a - b.re, -b.im); }
+SNAPI_HD cd dscl(cd a, double s) { return dmk(a.re * s, a.im * s); }
+
+#ifdef __CUDA_ARCH__
+SNAPI_HD float fexp(float x) { return expf(x); }
+SNAPI_HD void fsincos(float x, float *s, float *c) { sincosf(x, s, c); }
+#else
+SNAPI_HD float fexp(float x) { return expf(x); }
+SNAPI_HD void fsincos(float x, float *s, float *c) { *s = sinf(x); *c = cosf(x); }
+#endif
+
+// Humlicek W4 (published region split and coefficients); H, F divided by sqrt(pi).
+SNAPI_HD void voigt(float x, float a, float &H, float &F) {
+  const float v = x;
+  const float s = fabsf(v) + a;
+  const cf t = cmk(a, -v);
+  const cf u = cmk(a * a - v * v, -2.0f * a * v);
+  cf w4;
+  if (s >= 15.0f) {
+    w4 = cdiv(cscl(t, 0.5641896f), caddr(0.5f, u));
+  } else if (s > 5.5f) {
+    w4 = cdiv(cmul(t, caddr(1.410474f, cscl(u, 0.5641896f))), caddr(0.75f, cmul(u, caddr(3.0f, u))));
+  } else if (a > (0.195f * fabsf(v) - 0.176f)) {
+    cf n = caddr(3.778987f, cscl(t, 0.5642236f));
+    n = caddr(11.96482f, cmul(t, n));
+    n = caddr(20.20933f, cmul(t, n));
+    n = caddr(16.4955f, cmul(t, n));
+    cf d = caddr(6.699398f, t);
+    d = caddr(21.69274f, cmul(t, d));
+    d = caddr(39.27121f, cmul(t, d));
+    d = caddr(38.82363f, cmul(t, d));
+    d = caddr(16.4955f, cmul(t, d));
+    w4 = cdiv(n, d);
+  } else {
+    cf p = csubr(1.320522f, cscl(u, 0.56419f));
+    p = csubr(35.76683f, cmul(u, p));
+    p = csubr(219.0313f, cmul(u, p));
+    p = csubr(1540.787f, cmul(u, p));
+    p = csubr(3321.9905f, cmul(u, p));
+    p = csubr(36183.31f, cmul(u, p));
+    cf q = csubr(1.841439f, u);
+    q = csubr(61.57037f, cmul(u, q));
+    q = csubr(364.2191f, cmul(u, q));
+    q = csubr(2186.181f, cmul(u, q));
+    q = csubr(9022.228f, cmul(u, q));
+    q = csubr(24322.84f, cmul(u, q));
+    q = csubr(32066.6f, cmul(u, q));
+    float su, cu;
+    fsincos(u.im, &su, &cu);
+    const float eu = fexp(u.re);
+    w4 = csub(cmk(eu * sqrtf(1.0f - su * su), eu * su), cdiv(cmul(t, p), q));
+  }
+  H = w4.re * kSqrtPiInv;
+  F = w4.im * kSqrtPiInv;
+}
+
+// W4 with its exact partial derivatives with respect to x (= v) and a.
+SNAPI_HD void voigt_grad(float x, float a, float &H, float &F, float &Hx, float &Fx, float &Ha, float &Fa) {
+  const float v = x;
+  const float s = fabsf(v) + a;
+  const cf t = cmk(a, -v);
+  const cf u = cmk(a * a - v * v, -2.0f * a * v);
+  cf w4, dwa, dwv;  // dw/da, dw/dv
+  if (s >= 15.0f || s > 5.5f || a > (0.195f * fabsf(v) - 0.176f)) {
+    cf n, np, d, dp;  // numerator / denominator as functions of t, and d/dt
+    if (s >= 15.0f) {
+      n = cscl(t, 0.5641896f);
+      np = cmk(0.5641896f, 0.0f);
+      d = caddr(0.5f, u);
+      dp = cscl(t, 2.0f);
+    } else if (s > 5.5f) {
+      n = cmul(t, caddr(1.410474f, cscl(u, 0.5641896f)));
+      np = caddr(1.410474f, cscl(u, 3.0f * 0.5641896f));
+      d = caddr(0.75f, cmul(u, caddr(3.0f, u)));
+      dp = cmul(t, caddr(6.0f, cscl(u, 4.0f)));
+    } else {
+      n = caddr(3.778987f, cscl(t, 0.5642236f));
+      n = caddr(11.96482f, cmul(t, n));
+      n = caddr(20.20933f, cmul(t, n));
+      n = caddr(16.4955f, cmul(t, n));
+      np = caddr(3.0f * 3.778987f, cscl(t, 4.0f * 0.5642236f));
+      np = caddr(2.0f * 11.96482f, cmul(t, np));
+      np = caddr(20.20933f, cmul(t, np));
+      d = caddr(6.699398f, t);
+      d = caddr(21.69274f, cmul(t, d));
+      d = caddr(39.27121f, cmul(t, d));
+      d = caddr(38.82363f, cmul(t, d));
+      d = caddr(16.4955f, cmul(t, d));
+      dp = caddr(4.0f * 6.699398f, cscl(t, 5.0f));
+      dp = caddr(3.0f * 21.69274f, cmul(t, dp));
+      dp = caddr(2.0f * 39.27121f, cmul(t, dp));
+      dp = caddr(38.82363f, cmul(t, dp));
+    }
+    w4 = cdiv(n, d);
+    // w' = (n' d - n d') / d^2 = (n' - w d') / d
+    cf wp = cdiv(csub(np, cmul(w4, dp)), d);
+    dwa = wp;                        // dt/da = 1
+    dwv = cmk(wp.im, -wp.re);        // dt/dv = -i
+  } else {
+    // Region 4 in FP64: near |v| ~ 5 the real part of dw/dv is ~1e-3 of |dw/dv| and the
+    // quotient-rule terms cancel far below FP32 resolution.
+    const double ad = a, vd = v;
+    const cd td = dmk(ad, -vd);
+    const cd ud = dmk(ad * ad - vd * vd, -2.0 * ad * vd);
+    cd p = dsubr(1.320522, dscl(ud, 0.56419));
+    p = dsubr(35.76683, dmul(ud, p));
+    p = dsubr(219.0313, dmul(ud, p));
+    p = dsubr(1540.787, dmul(ud, p));
+    p = dsubr(3321.9905, dmul(ud, p));
+    p = dsubr(36183.31, dmul(ud, p));
+    // p(u) = c0 - c1 u + c2 u^2 - c3 u^3 + c4 u^4 - c5 u^5 + c6 u^6
+    // p'(u) = -c1 + 2 c2 u - 3 c3 u^2 + 4 c4 u^3 - 5 c5 u^4 + 6 c6 u^5
+    cd pp = dmk(6.0 * 0.56419, 0.0);
+    pp = daddr(-5.0 * 1.320522, dmul(ud, pp));
+    pp = daddr(4.0 * 35.76683, dmul(ud, pp));
+    pp = daddr(-3.0 * 219.0313, dmul(ud, pp));
+    pp = daddr(2.0 * 1540.787, dmul(ud, pp));
+    pp = daddr(-3321.9905, dmul(ud, pp));
+    cd q = dsubr(1.841439, ud);
+    q = dsubr(61.57037, dmul(ud, q));
+    q = dsubr(364.2191, dmul(ud, q));
+    q = dsubr(2186.181, dmul(ud, q));
+    q = dsubr(9022.228, dmul(ud, q));
+    q = dsubr(24322.84, dmul(ud, q));
+    q = dsubr(32066.6, dmul(ud, q));
+    // q(u) = d0 - d1 u + d2 u^2 - d3 u^3 + d4 u^4 - d5 u^5 + d6 u^6 - u^7
+    cd qp = dmk(-7.0, 0.0);
+    qp = daddr(6.0 * 1.841439, dmul(ud, qp));
+    qp = daddr(-5.0 * 61.57037, dmul(ud, qp));
+    qp = daddr(4.0 * 364.2191, dmul(ud, qp));
+    qp = daddr(-3.0 * 2186.181, dmul(ud, qp));
+    qp = daddr(2.0 * 9022.228, dmul(ud, qp));
+    qp = daddr(-24322.84, dmul(ud, qp));
+    const double su = sin(ud.im), cu = cos(ud.im);
+    const double eu = exp(ud.re);
+    const double ca = sqrt(1.0 - su * su);
+    const cd R = ddiv(dmul(td, p), q);
+    const cd E = dmk(eu * ca, eu * su);
+    const cd wd = dsub(E, R);
+    // dR/dt = p/q + 2 t^2 (p' q - p q') / q^2
+    const cd Rp = dadd(ddiv(p, q), dmul(dscl(ud, 2.0), ddiv(dsub(dmul(pp, q), dmul(p, qp)), dmul(q, q))));
+    // E = e^{ur} (|cos ui|, sin ui): dE/dur = E, dE/dui = e^{ur} (-sgn(cos ui) sin ui, cos ui)
+    const double sg = (cu > 0.0) ? 1.0 : ((cu < 0.0) ? -1.0 : 0.0);
+    const cd Eui = dmk(-eu * sg * su, eu * cu);
+    // ur = a^2 - v^2, ui = -2 a v, dt/da = 1, dt/dv = -i
+    const cd dwad = dsub(dadd(dscl(E, 2.0 * ad), dscl(Eui, -2.0 * vd)), Rp);
+    const cd Rv = dmk(Rp.im, -Rp.re);
+    const cd dwvd = dsub(dadd(dscl(E, -2.0 * vd), dscl(Eui, -2.0 * ad)), Rv);
+    w4 = cmk((float)wd.re, (float)wd.im);
+    dwa = cmk((float)dwad.re, (float)dwad.im);
+    dwv = cmk((float)dwvd.re, (float)dwvd.im);
+  }
+  H = w4.re * kSqrtPiInv;
+  F = w4.im * kSqrtPiInv;
+  Hx = dwv.re * kSqrtPiInv;
+  Fx = dwv.im * kSqrtPiInv;
+  Ha = dwa.re * kSqrtPiInv;
+  Fa = dwa.im * kSqrtPiInv;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Planck function with the reference's constants (cmlib/mathtools.cc:1150-1152), lambda in cm
+SNAPI_HD double planck_d(double lam, double T) {
+  return 2.0 * 6.62606957 * 8.9875517E-7 / lam / lam / lam / lam / lam / (exp(1.4387769 / lam / T) - 1.0);
+}
+
+// per-depth precompute from the record row rec[nfield]; lam_mid: mid vacuum wavelength
+SNAPI_HD void depth_precompute(const float *rec, int nlines, const LineConst *lc, float lam_mid,
+                               DepthConst &d, LineDepth *ld) {
+  const float T = rec[F_T], vt = rec[F_VT], ne = rec[F_NE], B = rec[F_B];
+  const float invk = 1.0f / rec[F_KAP];
+  const float xpm = 1.4387769f / lam_mid;
+  const float Em = fexp(xpm / T);
+  const float plm = (float)(2.0 * 6.62606957 * 8.9875517E-7) / (lam_mid * lam_mid * lam_mid * lam_mid * lam_mid) / (Em - 1.0f);
+  const float ope = ne * kSigmaT;
+  d.cop = (ope + rec[F_BFOP]) * invk;
+  d.cem = (ope * plm + rec[F_BFEM]) * invk;
+  d.beta = rec[F_VLOS] * (float)(1.0 / kC);
+  float th = rec[F_INC] * (float)(kPi / 180.0), ph = rec[F_AZI] * (float)(kPi / 180.0);
+  if (B < 0.001f) th = ph = 0.0f;
+  float sth, cth, s2p, c2p;
+  fsincos(th, &sth, &cth);
+  fsincos(2.0f * ph, &s2p, &c2p);
+  d.st2 = sth * sth;
+  d.ctb = cth;
+  d.opc2 = 1.0f + cth * cth;
+  d.c2 = c2p;
+  d.s2 = s2p;
+  d.hb = rec[F_HMBF] * invk;
+  d.hf = rec[F_HMFF] * invk;
+  d.invT = 1.0f / T;
+  d.lt = log10f(5040.0f / T);
+  for (int j = 0; j < nlines; ++j) {
+    const LineConst &L = lc[j];
+    const float *rl = rec + F_LINE0 + 3 * j;
+    const float W = L.two_k_over_m * T + vt * vt;
+    const float dld = sqrtf(W) * L.lam0_over_c;
+    const float idl = 1.0f / dld;
+    ld[j].inv_dld = idl;
+    ld[j].a = L.sf * (L.ar + rl[2]) * idl;
+    ld[j].bsh = L.zee * B * idl;
+    ld[j].opn = rl[0] * invk * idl;
+    ld[j].emn = rl[1] * invk * idl;
+  }
+}
+
+// per-wavelength constants; lam_vac in cm (double)
+SNAPI_HD void lambda_precompute(double lam, LamConst &c) {
+  static const double ca[7] = {1.99654, -1.18267E-5, 2.64243E-6, -4.40524E-10, 3.23992E-14,
+                               -1.39568E-18, 2.78701E-23};
+  double lA = lam * 1E8, alpha = 0.0, pw = 1.0;
+  for (int i = 0; i < 7; ++i) { alpha += ca[i] * pw; pw *= lA; }
+  double lb = 2.1177 * exp(-(lA - 2087.7) * (lA - 2087.7) / 2.421E6) + 0.68738;
+  if (lA > 4500.0) lb = 0.0;
+  double fud = 1.0 + 0.666667 * lb;
+  double l = log10(lA);
+  double f0 = -2.2763 - 1.6850 * l + 0.76661 * l * l - 0.053346 * l * l * l;
+  double f1 = 15.2827 - 9.2846 * l + 1.99381 * l * l - 0.142631 * l * l * l;
+  double f2 = -197.789 + 190.266 * l - 67.9775 * l * l + 10.6913 * l * l * l - 0.625151 * l * l * l * l;
+  c.lam = (float)lam;
+  c.afud = (float)(alpha * fud);
+  c.F0 = (float)(f0 + log10(fud));
+  c.f1 = (float)f1;
+  c.f2 = (float)f2;
+  c.xs = (float)(kH * kC / lam / kK);
+  c.xp = (float)(1.4387769 / lam);
+  c.pp = (float)(2.0 * 6.62606957 * 8.9875517E-7 / lam / lam / lam / lam / lam);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Opacity (eta_I, eta_Q, eta_U, eta_V, rho_Q, rho_U, rho_V) and emissivity (j_I..j_V), both
+// normalised by kappa_500, at one (lambda, depth).  delta[j] = lam0_j - lambda (FP64 -> FP32).
+SNAPI_HD void cell_opacity(const DepthConst &d, const LineDepth *ld, const LineConst *lc, int nlines,
+                           const float *compS, const float *compD, const LamConst &lc_l,
+                           const float *delta, float *eta, float *jj) {
+  eta[0] = d.cop;
+  eta[1] = eta[2] = eta[3] = eta[4] = eta[5] = eta[6] = 0.0f;
+  jj[0] = d.cem;
+  jj[1] = jj[2] = jj[3] = 0.0f;
+  for (int j = 0; j < nlines; ++j) {
+    const LineConst &L = lc[j];
+    const LineDepth &q = ld[j];
+    const float x0 = (delta[j] - lc_l.lam * d.beta) * q.inv_dld;
+    if (!L.split) {
+      float H, F;
+      voigt(x0, q.a, H, F);
+      eta[0] += q.opn * H;
+      jj[0] += q.emn * H;
+    } else {
+      float Hs[3] = {0.f, 0.f, 0.f}, Fs[3] = {0.f, 0.f, 0.f};
+      int off = L.comp_off;
+      for (int g = 0; g < 3; ++g) {
+        for (int i = 0; i < L.ncomp[g]; ++i, ++off) {
+          float H, F;
+          voigt(x0 + compD[off] * q.bsh, q.a, H, F);
+          Hs[g] += H * compS[off];
+          Fs[g] += F * compS[off];
+        }
+      }
+      const float hpm = Hs[0] - 0.5f * (Hs[2] + Hs[1]);
+      const float fpm = Fs[0] - 0.5f * (Fs[2] + Fs[1]);
+      const float eI = 0.5f * (Hs[0] * d.st2 + 0.5f * (Hs[2] + Hs[1]) * d.opc2);
+      const float eQ = 0.5f * hpm * d.st2 * d.c2;
+      const float eU = 0.5f * hpm * d.st2 * d.s2;
+      const float eV = 0.5f * (Hs[2] - Hs[1]) * d.ctb;
+      const float rQ = 0.5f * fpm * d.st2 * d.c2;
+      const float rU = 0.5f * fpm * d.st2 * d.s2;
+      const float rV = 0.5f * (Fs[2] - Fs[1]) * d.ctb;
+      eta[0] += eI * q.opn; eta[1] += eQ * q.opn; eta[2] += eU * q.opn; eta[3] += eV * q.opn;
+      eta[4] += rQ * q.opn; eta[5] += rU * q.opn; eta[6] += rV * q.opn;
+      jj[0] += eI * q.emn; jj[1] += eQ * q.emn; jj[2] += eU * q.emn; jj[3] += eV * q.emn;
+    }
+  }
+  // H- bound-free + free-free, LTE emissivity
+  const float e1 = fexp(-lc_l.xs * d.invT);
+  const float opbf = lc_l.afud * d.hb * (1.0f - e1);
+  const float E10 = fexp(kLn10 * (lc_l.F0 + lc_l.f1 * d.lt + lc_l.f2 * d.lt * d.lt));
+  const float opff = d.hf * E10;
+  const float oph = opbf + opff;
+  const float Ep = fexp(lc_l.xp * d.invT);
+  const float pl = lc_l.pp / (Ep - 1.0f);
+  eta[0] += oph;
+  jj[0] += oph * pl;
+}
+
+// Reverse of cell_opacity: given eta_bar[7], j_bar[4] accumulate the depth-level adjoint sums
+// red[kNumRed + kRedPerLine*nlines] (wavelength-summed later).
+SNAPI_HD void cell_opacity_adjoint(const DepthConst &d, const LineDepth *ld, const LineConst *lc, int nlines,
+                                   const float *compS, const float *compD, const LamConst &lc_l,
+                                   const float *delta, const float *etab, const float *jb, float *red) {
+  red[R_COP] += etab[0];
+  red[R_CEM] += jb[0];
+  float st2b = 0.f, ctbb = 0.f, c2b = 0.f, s2b = 0.f;
+  for (int j = 0; j < nlines; ++j) {
+    const LineConst &L = lc[j];
+    const LineDepth &q = ld[j];
+    float *rl = red + kNumRed + kRedPerLine * j;
+    const float xd = delta[j] - lc_l.lam * d.beta;
+    const float x0 = xd * q.inv_dld;
+    float x0b = 0.f, bb = 0.f, ab = 0.f;
+    if (!L.split) {
+      float H, F, Hx, Fx, Ha, Fa;
+      voigt_grad(x0, q.a, H, F, Hx, Fx, Ha, Fa);
+      rl[RL_OPN] += etab[0] * H;
+      rl[RL_EMN] += jb[0] * H;
+      const float Hb_ = q.opn * etab[0] + q.emn * jb[0];
+      x0b += Hb_ * Hx;
+      ab += Hb_ * Ha;
+    } else {
+      float Hs[3] = {0.f, 0.f, 0.f}, Fs[3] = {0.f, 0.f, 0.f};
+      int off = L.comp_off;
+      for (int g = 0; g < 3; ++g)
+        for (int i = 0; i < L.ncomp[g]; ++i, ++off) {
+          float H, F;
+          voigt(x0 + compD[off] * q.bsh, q.a, H, F);
+          Hs[g] += H * compS[off];
+          Fs[g] += F * compS[off];
+        }
+      const float hpm = Hs[0] - 0.5f * (Hs[2] + Hs[1]);
+      const float fpm = Fs[0] - 0.5f * (Fs[2] + Fs[1]);
+      const float P[7] = {0.5f * (Hs[0] * d.st2 + 0.5f * (Hs[2] + Hs[1]) * d.opc2),
+                          0.5f * hpm * d.st2 * d.c2,
+                          0.5f * hpm * d.st2 * d.s2,
+                          0.5f * (Hs[2] - Hs[1]) * d.ctb,
+                          0.5f * fpm * d.st2 * d.c2,
+                          0.5f * fpm * d.st2 * d.s2,
+                          0.5f * (Fs[2] - Fs[1]) * d.ctb};
+      float gop = 0.f, gem = 0.f;
+      for (int k = 0; k < 7; ++k) gop += etab[k] * P[k];
+      for (int k = 0; k < 4; ++k) gem += jb[k] * P[k];
+      rl[RL_OPN] += gop;
+      rl[RL_EMN] += gem;
+      float Pb[7];
+      for (int k = 0; k < 7; ++k) Pb[k] = q.opn * etab[k] + (k < 4 ? q.emn * jb[k] : 0.0f);
+      // P -> Hs, Fs, angle factors
+      const float hsum = Hs[2] + Hs[1];
+      float Hsb[3], Fsb[3];
+      // P0 = 0.5*Hs0*st2 + 0.25*hsum*opc2
+      Hsb[0] = 0.5f * d.st2 * Pb[0];
+      Hsb[1] = 0.25f * d.opc2 * Pb[0];
+      Hsb[2] = 0.25f * d.opc2 * Pb[0];
+      st2b += 0.5f * Hs[0] * Pb[0];
+      float opc2b = 0.25f * hsum * Pb[0];
+      // P1 = 0.5 hpm st2 c2, P2 = 0.5 hpm st2 s2
+      float hpmb = 0.5f * d.st2 * (d.c2 * Pb[1] + d.s2 * Pb[2]);
+      st2b += 0.5f * hpm * (d.c2 * Pb[1] + d.s2 * Pb[2]);
+      c2b += 0.5f * hpm * d.st2 * Pb[1];
+      s2b += 0.5f * hpm * d.st2 * Pb[2];
+      Hsb[0] += hpmb; Hsb[1] -= 0.5f * hpmb; Hsb[2] -= 0.5f * hpmb;
+      // P3 = 0.5 (Hs2 - Hs1) ctb
+      Hsb[2] += 0.5f * d.ctb * Pb[3]; Hsb[1] -= 0.5f * d.ctb * Pb[3];
+      ctbb += 0.5f * (Hs[2] - Hs[1]) * Pb[3];
+      // P4, P5 (rho_Q, rho_U)
+      float fpmb = 0.5f * d.st2 * (d.c2 * Pb[4] + d.s2 * Pb[5]);
+      st2b += 0.5f * fpm * (d.c2 * Pb[4] + d.s2 * Pb[5]);
+      c2b += 0.5f * fpm * d.st2 * Pb[4];
+      s2b += 0.5f * fpm * d.st2 * Pb[5];
+      Fsb[0] = fpmb; Fsb[1] = -0.5f * fpmb; Fsb[2] = -0.5f * fpmb;
+      // P6 = 0.5 (Fs2 - Fs1) ctb
+      Fsb[2] += 0.5f * d.ctb * Pb[6]; Fsb[1] -= 0.5f * d.ctb * Pb[6];
+      ctbb += 0.5f * (Fs[2] - Fs[1]) * Pb[6];
+      ctbb += 2.0f * d.ctb * opc2b;
+      // components
+      off = L.comp_off;
+      for (int g = 0; g < 3; ++g)
+        for (int i = 0; i < L.ncomp[g]; ++i, ++off) {
+          float H, F, Hx, Fx, Ha, Fa;
+          voigt_grad(x0 + compD[off] * q.bsh, q.a, H, F, Hx, Fx, Ha, Fa);
+          const float hb_ = Hsb[g] * compS[off], fb_ = Fsb[g] * compS[off];
+          const float xb = hb_ * Hx + fb_ * Fx;
+          x0b += xb;
+          bb += xb * compD[off];
+          ab += hb_ * Ha + fb_ * Fa;
+        }
+    }
+    rl[RL_XL] += x0b * lc_l.lam;
+    rl[RL_XD] += x0b * xd;
+    rl[RL_B] += bb;
+    rl[RL_A] += ab;
+  }
+  red[R_ST2] += st2b;
+  red[R_CTB] += ctbb;
+  red[R_C2] += c2b;
+  red[R_S2] += s2b;
+  // H-
+  const float e1 = fexp(-lc_l.xs * d.invT);
+  const float E10 = fexp(kLn10 * (lc_l.F0 + lc_l.f1 * d.lt + lc_l.f2 * d.lt * d.lt));
+  const float oph = lc_l.afud * d.hb * (1.0f - e1) + d.hf * E10;
+  const float Ep = fexp(lc_l.xp * d.invT);
+  const float pl = lc_l.pp / (Ep - 1.0f);
+  const float ophb = etab[0] + jb[0] * pl;
+  const float plb = jb[0] * oph;
+  red[R_HB] += ophb * lc_l.afud * (1.0f - e1);
+  red[R_HF] += ophb * E10;
+  red[R_INVT] += ophb * lc_l.afud * d.hb * lc_l.xs * e1 - plb * pl * lc_l.xp * Ep / (Ep - 1.0f);
+  red[R_LT] += ophb * d.hf * E10 * kLn10 * (lc_l.f1 + 2.0f * lc_l.f2 * d.lt);
+}
+
+// Chain the wavelength-summed depth adjoint sums red[] to the record fields (adds into rb[nfield]).
+SNAPI_HD void depth_chain_adjoint(const float *rec, int nlines, const LineConst *lc, float lam_mid,
+                                  const DepthConst &d, const LineDepth *ld, const float *red, float *rb) {
+  const float T = rec[F_T], vt = rec[F_VT], ne = rec[F_NE], B = rec[F_B];
+  const float invk = 1.0f / rec[F_KAP];
+  const float xpm = 1.4387769f / lam_mid;
+  const float Em = fexp(xpm / T);
+  const float plm = (float)(2.0 * 6.62606957 * 8.9875517E-7) / (lam_mid * lam_mid * lam_mid * lam_mid * lam_mid) / (Em - 1.0f);
+  const float dplm_dT = plm * xpm * Em / (Em - 1.0f) / (T * T);
+  float Tb = 0.f, vtb = 0.f, kapb = 0.f, Bb = 0.f, betab = 0.f;
+  // continuum
+  rb[F_NE] += red[R_COP] * kSigmaT * invk + red[R_CEM] * kSigmaT * plm * invk;
+  rb[F_BFOP] += red[R_COP] * invk;
+  rb[F_BFEM] += red[R_CEM] * invk;
+  kapb -= (red[R_COP] * d.cop + red[R_CEM] * d.cem) * invk;
+  Tb += red[R_CEM] * ne * kSigmaT * dplm_dT * invk;
+  // H-
+  rb[F_HMBF] += red[R_HB] * invk;
+  rb[F_HMFF] += red[R_HF] * invk;
+  kapb -= (red[R_HB] * d.hb + red[R_HF] * d.hf) * invk;
+  Tb += -red[R_INVT] * d.invT * d.invT - red[R_LT] / (T * kLn10);
+  // angles
+  if (!(B < 0.001f)) {
+    const float th = rec[F_INC] * (float)(kPi / 180.0), ph = rec[F_AZI] * (float)(kPi / 180.0);
+    float sth, cth, s2p, c2p;
+    fsincos(th, &sth, &cth);
+    fsincos(2.0f * ph, &s2p, &c2p);
+    const float dr = (float)(kPi / 180.0);
+    rb[F_INC] += (red[R_ST2] * 2.0f * sth * cth - red[R_CTB] * sth) * dr;
+    rb[F_AZI] += (-red[R_C2] * 2.0f * s2p + red[R_S2] * 2.0f * c2p) * dr;
+  }
+  // lines
+  for (int j = 0; j < nlines; ++j) {
+    const LineConst &L = lc[j];
+    const LineDepth &q = ld[j];
+    const float *rl = red + kNumRed + kRedPerLine * j;
+    const float *rec_l = rec + F_LINE0 + 3 * j;
+    const float opnb = rl[RL_OPN], emnb = rl[RL_EMN], ab = rl[RL_A], bshb = rl[RL_B];
+    betab += -q.inv_dld * rl[RL_XL];
+    float idlb = rl[RL_XD];
+    idlb += ab * L.sf * (L.ar + rec_l[2]);
+    idlb += bshb * L.zee * B;
+    idlb += opnb * rec_l[0] * invk + emnb * rec_l[1] * invk;
+    const float W = L.two_k_over_m * T + vt * vt;
+    // inv_dld = 1/(sqrt(W) lam0/c): d/dW = -0.5 inv_dld / W
+    const float dW = -0.5f * q.inv_dld / W * idlb;
+    Tb += dW * L.two_k_over_m;
+    vtb += dW * 2.0f * vt;
+    Bb += bshb * L.zee * q.inv_dld;
+    float *rbl = rb + F_LINE0 + 3 * j;
+    rbl[0] += opnb * invk * q.inv_dld;
+    rbl[1] += emnb * invk * q.inv_dld;
+    rbl[2] += ab * L.sf * q.inv_dld;
+    kapb -= (opnb * q.opn + emnb * q.emn) * invk;
+  }
+  rb[F_T] += Tb;
+  rb[F_VT] += vtb;
+  rb[F_KAP] += kapb;
+  rb[F_B] += Bb;
+  rb[F_VLOS] += betab * (float)(1.0 / kC);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Reduced absorption matrix K' = K/eta_I - 1 from the 7 opacities: kp = (q,u,v,rq,ru,rv)
+//   K' = [[0, q, u, v], [q, 0, rv, -ru], [u, -rv, 0, rq], [v, ru, -rq, 0]]
+SNAPI_HD void kprime_full(const float *kp, float *M) {
+  M[0] = 0.f;   M[1] = kp[0];  M[2] = kp[1];  M[3] = kp[2];
+  M[4] = kp[0]; M[5] = 0.f;    M[6] = kp[5];  M[7] = -kp[4];
+  M[8] = kp[1]; M[9] = -kp[5]; M[10] = 0.f;  M[11] = kp[3];
+  M[12] = kp[2]; M[13] = kp[4]; M[14] = -kp[3]; M[15] = 0.f;
+}
+// adjoint of kprime_full: accumulate d<Mb, K'>/dkp
+SNAPI_HD void kprime_proj(const float *Mb, float *kpb) {
+  kpb[0] += Mb[1] + Mb[4];
+  kpb[1] += Mb[2] + Mb[8];
+  kpb[2] += Mb[3] + Mb[12];
+  kpb[3] += Mb[11] - Mb[14];
+  kpb[4] += Mb[13] - Mb[7];
+  kpb[5] += Mb[6] - Mb[9];
+}
+
+// Crout LU without pivoting, unit upper diagonal (cmlib/mathtools.cc:487-514)
+SNAPI_HD void crout4(const float *S, float *D) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+#pragma unroll
+    for (int i = k; i < 4; ++i) {
+      float sum = 0.f;
+#pragma unroll
+      for (int p = 0; p < k; ++p) sum += D[i * 4 + p] * D[p * 4 + k];
+      D[i * 4 + k] = S[i * 4 + k] - sum;
+    }
+#pragma unroll
+    for (int j = k + 1; j < 4; ++j) {
+      float sum = 0.f;
+#pragma unroll
+      for (int p = 0; p < k; ++p) sum += D[k * 4 + p] * D[p * 4 + j];
+      D[k * 4 + j] = (S[k * 4 + j] - sum) / D[k * 4 + k];
+    }
+  }
+}
+SNAPI_HD void solve_crout4(const float *LU, const float *b, float *x) {
+  float y[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    float sum = 0.f;
+#pragma unroll
+    for (int k = 0; k < i; ++k) sum += LU[i * 4 + k] * y[k];
+    y[i] = (b[i] - sum) / LU[i * 4 + i];
+  }
+#pragma unroll
+  for (int i = 3; i >= 0; --i) {
+    float sum = 0.f;
+#pragma unroll
+    for (int k = i + 1; k < 4; ++k) sum += LU[i * 4 + k] * x[k];
+    x[i] = (y[i] - sum);
+  }
+}
+
+// linear DELO weights (atmos_ppbez_rts.cc:1070, :1085-1096).  Evaluated in FP64: above the
+// Taylor switch at 1e-2 the closed forms 1/tb - e^-tb (1 + 1/tb) and 1 - 1/tb + e^-tb/tb cancel
+// to ~tb/2 from terms of size 1/tb, which FP32 cannot resolve.
+SNAPI_HD void delo_weights(double tb, float &w0, float &w1, float &etb) {
+  if (tb < 1E-2) {
+    etb = (float)(1.0 - tb + tb * tb * 0.5 - tb * tb * tb / 6.0);
+    w0 = (float)(tb * (0.5 - tb * (1.0 / 3.0 - tb / 8.0)));
+    w1 = (float)(0.5 * tb * (1.0 - tb / 3.0 * (1.0 - tb / 4.0)));
+  } else {
+    const double e = exp(-tb);
+    etb = (float)e;
+    w0 = (float)(1.0 / tb - e * (1.0 + 1.0 / tb));
+    w1 = (float)(1.0 - 1.0 / tb + e / tb);
+  }
+}
+SNAPI_HD void delo_weights_grad(double tb, float &dw0, float &dw1, float &detb) {
+  if (tb < 1E-2) {
+    detb = (float)(-1.0 + tb - 0.5 * tb * tb);
+    dw0 = (float)(0.5 - tb * (2.0 / 3.0 - 3.0 * tb / 8.0));
+    // w1 = 0.5 tb - tb^2/6 + tb^3/24
+    dw1 = (float)(0.5 - tb / 3.0 + tb * tb / 8.0);
+  } else {
+    const double e = exp(-tb);
+    detb = (float)(-e);
+    // w0 = 1/tb - e (1 + 1/tb)
+    dw0 = (float)(-1.0 / (tb * tb) + e * (1.0 + 1.0 / tb) + e / (tb * tb));
+    // w1 = 1 - 1/tb + e/tb
+    dw1 = (float)(1.0 / (tb * tb) - e / tb - e / (tb * tb));
+  }
+}
+
+// One linear-DELO step: I_c = (1 + w1 K'_c)^-1 [ -w0 K'_p I_p + w0 S_p + w1 S_c + etb I_p ]
+SNAPI_HD void delo_step(const float *Ip, const float *kpp, const float *Sp, const float *kpc, const float *Sc,
+                        double tb, float *Ic) {
+  float w0, w1, etb;
+  delo_weights(tb, w0, w1, etb);
+  float Kp[16], Kc[16], A[16], LU[16], B[4], tv[4];
+  kprime_full(kpp, Kp);
+  kprime_full(kpc, Kc);
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    tv[s] = Kp[s * 4 + 0] * Ip[0] + Kp[s * 4 + 1] * Ip[1] + Kp[s * 4 + 2] * Ip[2] + Kp[s * 4 + 3] * Ip[3];
+  }
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+#pragma unroll
+    for (int sp = 0; sp < 4; ++sp) A[s * 4 + sp] = w1 * Kc[s * 4 + sp];
+    A[s * 4 + s] += 1.0f;
+  }
+#pragma unroll
+  for (int s = 0; s < 4; ++s) B[s] = -w0 * tv[s] + w0 * Sp[s] + w1 * Sc[s] + Ip[s] * etb;
+  crout4(A, LU);
+  solve_crout4(LU, B, Ic);
+}
+
+// Reverse of delo_step.  Inputs: forward values and Icb (adjoint of I_c).  Accumulates into
+// Ipb, kppb, Spb, kpcb, Scb and returns the adjoint of tb.
+SNAPI_HD float delo_step_adjoint(const float *Ip, const float *kpp, const float *Sp, const float *kpc,
+                                 const float *Sc, double tb, const float *Ic, const float *Icb, float *Ipb,
+                                 float *kppb, float *Spb, float *kpcb, float *Scb) {
+  float w0, w1, etb, dw0, dw1, detb;
+  delo_weights(tb, w0, w1, etb);
+  delo_weights_grad(tb, dw0, dw1, detb);
+  float Kp[16], Kc[16], AT[16], LU[16], Bb[4], tv[4];
+  kprime_full(kpp, Kp);
+  kprime_full(kpc, Kc);
+  // A^T = 1 + w1 K_c^T ; solve A^T Bb = Icb
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+#pragma unroll
+    for (int sp = 0; sp < 4; ++sp) AT[s * 4 + sp] = w1 * Kc[sp * 4 + s];
+    AT[s * 4 + s] += 1.0f;
+  }
+  crout4(AT, LU);
+  solve_crout4(LU, Icb, Bb);
+  // A-bar = -Bb Ic^T ; A = 1 + w1 Kc
+  float Ab[16];
+  float w1b = 0.f;
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int sp = 0; sp < 4; ++sp) {
+      Ab[s * 4 + sp] = -Bb[s] * Ic[sp];
+      w1b += Ab[s * 4 + sp] * Kc[s * 4 + sp];
+    }
+  float KcbM[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) KcbM[i] = w1 * Ab[i];
+  kprime_proj(KcbM, kpcb);
+  // B = -w0 Kp Ip + w0 Sp + w1 Sc + etb Ip
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+    tv[s] = Kp[s * 4 + 0] * Ip[0] + Kp[s * 4 + 1] * Ip[1] + Kp[s * 4 + 2] * Ip[2] + Kp[s * 4 + 3] * Ip[3];
+  float w0b = 0.f, etbb = 0.f;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    w0b += Bb[s] * (Sp[s] - tv[s]);
+    w1b += Bb[s] * Sc[s];
+    etbb += Bb[s] * Ip[s];
+    Spb[s] += w0 * Bb[s];
+    Scb[s] += w1 * Bb[s];
+  }
+  // Ip-bar = etb Bb - w0 Kp^T Bb ; Kp-bar = -w0 Bb Ip^T
+#pragma unroll
+  for (int sp = 0; sp < 4; ++sp) {
+    float acc = 0.f;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) acc += Kp[s * 4 + sp] * Bb[s];
+    Ipb[sp] += etb * Bb[sp] - w0 * acc;
+  }
+  float KpbM[16];
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int sp = 0; sp < 4; ++sp) KpbM[s * 4 + sp] = -w0 * Bb[s] * Ip[sp];
+  kprime_proj(KpbM, kppb);
+  return w0b * dw0 + w1b * dw1 + etbb * detb;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Optical depth (FP64): monotone derivative of eta_I at an interior point and the Bezier
+// increment over one interval (atmos_ppbez_rts.cc:966-988), written on the path-length
+// intervals D[i] = (tau500[i+1] - tau500[i]) / mu between depths i (above) and i+1 (below).
+//
+// interior point z (1..nd-2):  h1 = D[z] (upwind side, below), h2 = D[z-1] (downwind, above)
+SNAPI_HD double opd_interior(double e_up, double e_c, double e_dn, double h1, double h2) {
+  // e_up = eta[z+1] (below), e_c = eta[z], e_dn = eta[z-1] (above)
+  const double d1 = (e_c - e_up) / h1;
+  const double d2 = (e_dn - e_c) / h2;
+  if (d1 * d2 > 0) {
+    const double alpha = (1.0 + h1 / (h1 + h2)) / 3.0;
+    return d1 * d2 / (alpha * d1 + (1.0 - alpha) * d2);
+  }
+  return 0.0;
+}
+// gradient of opd_interior w.r.t. (e_up, e_c, e_dn)
+SNAPI_HD void opd_interior_grad(double e_up, double e_c, double e_dn, double h1, double h2, double g,
+                                double &gup, double &gc, double &gdn) {
+  const double d1 = (e_c - e_up) / h1;
+  const double d2 = (e_dn - e_c) / h2;
+  if (d1 * d2 > 0) {
+    const double alpha = (1.0 + h1 / (h1 + h2)) / 3.0;
+    const double den = alpha * d1 + (1.0 - alpha) * d2;
+    const double dd1 = (1.0 - alpha) * d2 * d2 / (den * den);
+    const double dd2 = alpha * d1 * d1 / (den * den);
+    gup += -g * dd1 / h1;
+    gc += g * dd1 / h1 - g * dd2 / h2;
+    gdn += g * dd2 / h2;
+  }
+}
+// Bezier optical depth over the interval between depth z (above) and z+1 (below):
+//   dl = D[z];  C0 = e_z - dl/2 opd_z ;  C1 = e_{z+1} + dl/2 opd_{z+1} ;  dtau = dl/3 (e_{z+1} + e_z + (C0+C1)/2)
+SNAPI_HD double bezier_dtau(double e_below, double e_above, double opd_below, double opd_above, double dl) {
+  const double C0 = e_above - dl / 2.0 * opd_above;
+  const double C1 = e_below + dl / 2.0 * opd_below;
+  const double C = 0.5 * (C0 + C1);
+  return dl / 3.0 * (e_below + e_above + C);
+}
+
+}  // namespace snapi

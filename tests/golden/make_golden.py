@@ -1,0 +1,217 @@
+"""Generate the golden fixtures of the tests from the compiled reference (test infrastructure).
+
+Runs in the development container only (it reads the reference's atom / molecule configs and
+its 80-depth atmosphere file from REF and runs oracle/_ref/snapi_ref_dump).  Writes:
+
+  tests/golden/c1.tsk, c3.tsk     task blobs (packed atmosphere column + node model + lambda
+                                  grid), the payload the reference's master sends a slave
+  tests/golden/config1.npz        one column, 80 depths, 201 lambda: record, reference Stokes,
+                                  reference opacity at 7 wavelengths, line constants
+  tests/golden/config2.npz        16 pixels of the seeded 256x256 synthesis cube (seed 2)
+  tests/golden/config3.npz        8 pixels of the seeded 64x64 node-model cube (seed 3): records,
+                                  node tangents, reference Stokes, reference node responses,
+                                  noisy target Stokes
+
+Synthetic inputs stand in for observations: seeded numpy generators with the shapes and value
+distributions of the benchmark configurations (no dataset is read).
+
+usage:  python tests/golden/make_golden.py [--ref /root/reference]
+"""
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+from sbin import read_sbin  # noqa: E402
+
+DUMP = os.path.join(ROOT, "oracle", "_ref", "snapi_ref_dump")
+CFG_FILES = ["atoms_6300.cfg", "mol.cfg", "hydrogen_3lvl.cfg", "helium.cfg", "carbon.cfg", "nitrogen.cfg",
+             "oxygen.cfg", "calcium.cfg", "silicon.cfg", "aluminium.cfg", "iron_6300.cfg", "falc_80z.dat"]
+
+ND = 80
+LOGTAU = np.linspace(-6.0, 1.0, ND)
+
+
+def config1_temperature(x):
+    """Config 1 temperature profile: 4400 K at the minimum, tanh rises to 9000 K at log tau = -6
+    and 9500 K at log tau = +1 (closed form defined here)."""
+    st = lambda z: 0.5 * (1.0 + np.tanh(z))  # noqa: E731
+    return (4400.0 + 4600.0 * st((-4.8 - x) / 0.4) / st((-4.8 + 6.0) / 0.4)
+            + 5100.0 * st((x - 0.3) / 0.6) / st((1.0 - 0.3) / 0.6))
+
+
+def write_cfg(path, t_taus, t_vals, vs_taus, vs_vals, vt=1e5, B=1000.0, theta_deg=45.0, phi_deg=30.0):
+    fmt = lambda a: ",".join("%.6f" % v for v in a)  # noqa: E731
+    cfg = f"""atmos{{
+  ID=col
+  TYPE=SPINOR
+  FILE=falc_80z.dat
+  GEOMETRY=PLANEPARALLEL
+  RTSOLVER=Bezier
+  ATOM=atoms_6300.cfg
+  MOL=mol.cfg
+  TAU_GRID=1
+}}
+obs{{
+  ID=obs1
+  EL=3.14159265359
+  AZ=0.0
+  NAME=none
+  LAMBDA=6301.0-6303.4
+  DLAMBDA=0.012
+}}
+model{{
+  ID=m1
+  TAUGRID=-6.0,1.0
+  parameter{{
+    ID=TEMP
+    TAU={fmt(t_taus)}
+    VALUE={fmt(t_vals)}
+  }}
+  parameter{{
+    ID=VT
+    TAU=0
+    VALUE={vt:.6f}
+  }}
+  parameter{{
+    ID=VS
+    TAU={fmt(vs_taus)}
+    VALUE={fmt(vs_vals)}
+  }}
+  parameter{{
+    ID=B
+    TAU=0
+    VALUE={B:.6f}
+  }}
+  parameter{{
+    ID=THETA
+    TAU=0
+    VALUE={theta_deg:.6f}
+  }}
+  parameter{{
+    ID=PHI
+    TAU=0
+    VALUE={phi_deg:.6f}
+  }}
+}}
+"""
+    with open(path, "w") as f:
+        f.write(cfg)
+
+
+def run(args, cwd):
+    r = subprocess.run(args, cwd=cwd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("%s failed:\n%s\n%s" % (args, r.stdout, r.stderr))
+    return r.stderr
+
+
+def dump(tmp, task, nodes, flags, name):
+    nf = os.path.join(tmp, name + "_nodes.f64")
+    np.ascontiguousarray(nodes, dtype="<f8").tofile(nf)
+    out = os.path.join(tmp, name + ".sbin")
+    log = run([DUMP, "dump", task, nf, str(nodes.shape[0]), str(flags), out], tmp)
+    sys.stderr.write(log)
+    return read_sbin(out)
+
+
+def line_arrays(d):
+    return {"line_const": d["line_const"], "line_ncomp": d["line_ncomp"], "line_pattern": d["line_pattern"]}
+
+
+def config2_nodes(npix, seed=2):
+    """Seeded config-2 pixels: T = config-1 profile + Gaussian-smoothed N(0, 300 K) (sigma = 5 depth
+    points), B log-uniform 10..3000 G, cos(inclination) U(-1,1), azimuth U(0, pi), v_los N(0, 2 km/s),
+    v_turb U(0.5, 2) km/s.  Node vector: 80 T nodes (one per depth), v_turb, v_los, B, theta, phi."""
+    rng = np.random.default_rng(seed)
+    base = config1_temperature(LOGTAU)
+    k = np.arange(-15, 16)
+    ker = np.exp(-0.5 * (k / 5.0) ** 2)
+    ker /= np.sqrt(np.sum(ker ** 2))
+    nodes = np.zeros((npix, ND + 5))
+    for i in range(npix):
+        pert = np.convolve(rng.standard_normal(ND + 30), ker, mode="valid")[:ND] * 300.0
+        nodes[i, :ND] = np.clip(base + pert, 3500.0, 11500.0)
+        nodes[i, ND] = rng.uniform(0.5e5, 2.0e5)
+        nodes[i, ND + 1] = rng.normal(0.0, 2.0e5)
+        nodes[i, ND + 2] = 10.0 ** rng.uniform(1.0, np.log10(3000.0))
+        nodes[i, ND + 3] = np.arccos(rng.uniform(-1.0, 1.0))
+        nodes[i, ND + 4] = rng.uniform(0.0, np.pi)
+    return nodes
+
+
+C3_TTAU = np.array([-4.0, -2.5, -1.0, 0.5])
+C3_VSTAU = np.array([-2.0, 0.0])
+C3_TRUTH = np.array([4600.0, 4900.0, 5500.0, 7400.0, 1.0e5, 0.0, 0.0, 800.0, np.deg2rad(60.0), np.deg2rad(40.0)])
+
+
+def config3_nodes(npix, seed=3):
+    """Seeded config-3 truth nodes (node order of the reference's model: T x4, v_turb, v_los x2,
+    B, theta, phi; velocities in cm/s, angles in rad)."""
+    rng = np.random.default_rng(seed)
+    nodes = np.tile(C3_TRUTH, (npix, 1))
+    nodes[:, 0:4] += rng.normal(0.0, 150.0, (npix, 4))
+    nodes[:, 4] = rng.uniform(0.5e5, 2.0e5, npix)
+    nodes[:, 5:7] = rng.normal(0.0, 1.0e5, (npix, 2))
+    nodes[:, 7] = 10.0 ** rng.uniform(2.0, np.log10(2500.0), npix)
+    nodes[:, 8] = rng.uniform(np.deg2rad(20.0), np.deg2rad(160.0), npix)
+    nodes[:, 9] = rng.uniform(np.deg2rad(10.0), np.deg2rad(170.0), npix)
+    return nodes
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--c2pix", type=int, default=16)
+    ap.add_argument("--c3pix", type=int, default=8)
+    a = ap.parse_args()
+    if not os.path.exists(DUMP):
+        raise SystemExit("build the oracle first: make -C oracle")
+    tmp = tempfile.mkdtemp(prefix="snapi_golden_")
+    try:
+        for f in CFG_FILES:
+            shutil.copy(os.path.join(a.ref, "cfg", f), tmp)
+        # config 1: dense temperature nodes (one per depth) reproduce the closed-form profile
+        T1 = config1_temperature(LOGTAU)
+        write_cfg(os.path.join(tmp, "c1.cfg"), LOGTAU, T1, [0.0], [0.0])
+        run([DUMP, "pack", "c1.cfg", "c1.tsk"], tmp)
+        shutil.copy(os.path.join(tmp, "c1.tsk"), os.path.join(HERE, "c1.tsk"))
+        n1 = np.concatenate([T1, [1e5, 0.0, 1000.0, np.deg2rad(45.0), np.deg2rad(30.0)]])[None, :]
+        d1 = dump(tmp, os.path.join(tmp, "c1.tsk"), n1, 4, "c1")
+        np.savez_compressed(os.path.join(HERE, "config1.npz"), lambda_air=d1["lambda_air"], tau500=d1["tau500"],
+                            record=d1["record"], stokes=d1["stokes"], nodes=d1["nodes"], probe_l=d1["probe_l"],
+                            opacity_probe=d1["opacity_probe"], ref_dld=d1["ref_dld"], ref_adamp=d1["ref_adamp"],
+                            meta=d1["meta"], **line_arrays(d1))
+        # config 2 subset
+        n2 = config2_nodes(a.c2pix)
+        d2 = dump(tmp, os.path.join(tmp, "c1.tsk"), n2, 0, "c2")
+        np.savez_compressed(os.path.join(HERE, "config2.npz"), lambda_air=d2["lambda_air"], tau500=d2["tau500"],
+                            record=d2["record"], stokes=d2["stokes"], nodes=d2["nodes"], meta=d2["meta"],
+                            **line_arrays(d2))
+        # config 3: ten-node model
+        write_cfg(os.path.join(tmp, "c3.cfg"), C3_TTAU, C3_TRUTH[:4], C3_VSTAU, C3_TRUTH[5:7])
+        run([DUMP, "pack", "c3.cfg", "c3.tsk"], tmp)
+        shutil.copy(os.path.join(tmp, "c3.tsk"), os.path.join(HERE, "c3.tsk"))
+        n3 = config3_nodes(a.c3pix)
+        d3 = dump(tmp, os.path.join(tmp, "c3.tsk"), n3, 3, "c3")
+        rng = np.random.default_rng(33)
+        Ic = d3["stokes"][:, :, 0].max(axis=1)
+        target = d3["stokes"] + rng.normal(0.0, 1e-3, d3["stokes"].shape) * Ic[:, None, None]
+        np.savez_compressed(os.path.join(HERE, "config3.npz"), lambda_air=d3["lambda_air"], tau500=d3["tau500"],
+                            record=d3["record"], stokes=d3["stokes"], nodes=d3["nodes"], node_kind=d3["node_kind"],
+                            tangent=d3["tangent"].astype(np.float32), responses=d3["responses"], target=target,
+                            ref_seconds_per_pixel=d3["ref_seconds_per_pixel"], meta=d3["meta"], **line_arrays(d3))
+        print("fixtures written to", HERE)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,226 @@
+"""GPU parity: libsnapi_cuda (through its C ABI) against the FP64 oracle and the emulator."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from helpers import P, emu_lines, node_scales, oracle_grad, scaled_rel_err
+
+pytestmark = pytest.mark.gpu
+
+IC_TOL = 1e-5  # Stokes tolerance, in units of the continuum intensity
+
+
+@pytest.fixture(scope="module")
+def sb():
+    import snapi_b200
+    from snapi_b200 import build as b
+    b.build_cuda()
+    return snapi_b200
+
+
+def _ic(fx):
+    return float(fx["stokes"][:, :, 0].max())
+
+
+def _ctx(sb, fx, **kw):
+    kw.setdefault("stokes_scale", _ic(fx))
+    return sb.Context.from_fixture(fx, **kw)
+
+
+@pytest.mark.parametrize("cfg", ["config1", "config2", "config3"])
+def test_synth_matches_oracle(sb, oracle_lib, cfg, request):
+    fx = request.getfixturevalue(cfg)
+    ctx = _ctx(sb, fx)
+    st = ctx.synth(fx["record"])
+    assert ctx.last_launches >= 1 and ctx.last_kernel_ms > 0.0
+    ctx.close()
+    ic = fx["stokes"][:, :, 0].max(axis=1)[:, None, None]
+    err = np.abs(st - fx["stokes"]) / ic
+    assert np.all(np.isfinite(st))
+    assert err.max() < IC_TOL, err.max()
+
+
+def test_synth_matches_emulator(sb, emu, oracle_lib, config2):
+    fx = config2
+    ctx = _ctx(sb, fx)
+    st = ctx.synth(fx["record"])
+    ctx.close()
+    lines = emu_lines(oracle_lib, fx)
+    rec = np.ascontiguousarray(fx["record"], np.float32)
+    npix, nd, _ = rec.shape
+    nl = fx["lambda_air"].shape[0]
+    out = np.zeros((npix, nl, 4), np.float32)
+    emu.emu_synth(nd, nl, len(lines), P(fx["lambda_air"]), P(fx["tau500"]), 1.0, ctypes.addressof(lines), npix, P(rec),
+                  P(out))
+    assert np.abs(st - out).max() / _ic(fx) < 2e-6
+
+
+def test_adjoint_gradient(sb, oracle_lib, config3):
+    fx = config3
+    n = 4
+    ctx = _ctx(sb, fx)
+    out = ctx.adjoint(fx["record"][:n], fx["target"][:n], fx["tangent"][:n], want_rec_grad=True)
+    ctx.close()
+    assert np.all(np.isfinite(out["grad"])) and np.all(np.isfinite(out["rec_grad"]))
+    lines = emu_lines(oracle_lib, fx)
+    s64 = oracle_lib.synth(fx["lambda_air"], fx["tau500"], fx["record"][:n], lines)
+    ic = _ic(fx)
+    assert np.abs(out["stokes"] - s64).max() / ic < IC_TOL
+    for p in range(n):
+        c_ref, g_ref = oracle_grad(oracle_lib, fx, p, fx["target"][p])
+        assert abs(out["chi2"][p] - c_ref) < 1e-4 * c_ref
+        assert scaled_rel_err(out["grad"][p], g_ref, fx["node_kind"]) < 1e-2
+        _, g_same = oracle_grad(oracle_lib, fx, p, fx["target"][p] + (s64[p] - out["stokes"][p]))
+        assert scaled_rel_err(out["grad"][p], g_same, fx["node_kind"]) < 1e-3
+
+
+def test_adjoint_coherent_residual(sb, oracle_lib, config3):
+    fx = config3
+    obs = fx["stokes"][:2] * 0.97
+    ctx = _ctx(sb, fx)
+    out = ctx.adjoint(fx["record"][:2], obs, fx["tangent"][:2])
+    ctx.close()
+    for p in range(2):
+        _, g_ref = oracle_grad(oracle_lib, fx, p, obs[p])
+        assert scaled_rel_err(out["grad"][p], g_ref, fx["node_kind"]) < 1e-4
+
+
+def test_fd_gradient_agrees_with_adjoint(sb, config3):
+    """The plain FD baseline (2 npar + 1 FP32 solves) agrees with the adjoint to its own accuracy."""
+    fx = config3
+    obs = fx["stokes"][:4] * 0.97
+    steps = np.array([5.0, 5.0, 5.0, 5.0, 2e3, 2e3, 2e3, 5.0, 5e-3, 5e-3])
+    ctx = _ctx(sb, fx)
+    a = ctx.adjoint(fx["record"][:4], obs, fx["tangent"][:4])
+    f = ctx.fd_grad(fx["record"][:4], obs, fx["tangent"][:4], steps)
+    ctx.close()
+    np.testing.assert_allclose(f["chi2"], a["chi2"], rtol=1e-5)
+    for p in range(4):
+        assert scaled_rel_err(f["grad"][p], a["grad"][p], fx["node_kind"]) < 2e-2
+
+
+def test_mask_and_stokes_weights(sb, oracle_lib, config3):
+    fx = config3
+    nl = fx["lambda_air"].shape[0]
+    rng = np.random.default_rng(7)
+    mask = (rng.uniform(size=(1, nl)) > 0.3).astype(np.float32)
+    mask[0, :40] = 0.0
+    ws = (1.0, 0.5, 0.5, 2.0)
+    ctx = _ctx(sb, fx)
+    out = ctx.adjoint(fx["record"][:1], fx["target"][:1], fx["tangent"][:1], w_stokes=ws, mask=mask)
+    ctx.close()
+    r = (fx["target"][0] - out["stokes"][0]) * np.array(ws)[None, :] * mask[0][:, None]
+    assert abs(out["chi2"][0] - np.sum(r.astype(np.float64) ** 2)) < 1e-6 * out["chi2"][0]
+
+
+def test_batches_larger_than_device_batch(sb, config2):
+    fx = config2
+    ctx1 = _ctx(sb, fx, max_batch=5)
+    ctx2 = _ctx(sb, fx)
+    a = ctx1.synth(fx["record"])
+    b = ctx2.synth(fx["record"])
+    ctx1.close()
+    ctx2.close()
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("nl", [1, 37, 64, 201])
+def test_ragged_wavelength_counts(sb, oracle_lib, config1, nl):
+    """Wavelength counts that are not multiples of the warp size (inactive lanes) and one
+    wavelength only."""
+    fx = dict(config1)
+    idx = np.linspace(0, 200, nl).astype(int) if nl > 1 else np.array([116])
+    fx["lambda_air"] = np.ascontiguousarray(fx["lambda_air"][idx])
+    ctx = _ctx(sb, fx)
+    st = ctx.synth(fx["record"])
+    ctx.close()
+    lines = emu_lines(oracle_lib, fx)
+    ref = oracle_lib.synth(fx["lambda_air"], fx["tau500"], fx["record"], lines)
+    assert np.abs(st - ref).max() / _ic(config1) < IC_TOL
+
+
+def test_weak_field_branch(sb, oracle_lib, config3):
+    """|B| < 0.001 G: the reference zeroes both field angles (atom_rad_synthesis.cc:419-420)."""
+    fx = config3
+    rec = fx["record"][:1].copy()
+    rec[0, :, 4] = 0.0
+    ctx = _ctx(sb, fx)
+    st = ctx.synth(rec)
+    out = ctx.adjoint(rec, fx["target"][:1], fx["tangent"][:1])
+    ctx.close()
+    lines = emu_lines(oracle_lib, fx)
+    ref = oracle_lib.synth(fx["lambda_air"], fx["tau500"], rec, lines)
+    assert np.abs(st - ref).max() / _ic(fx) < IC_TOL
+    assert np.all(np.isfinite(out["grad"]))
+    assert np.abs(st[0, :, 1:]).max() < 1e-6 * _ic(fx)
+
+
+def test_empty_batch_and_invalid_arguments(sb, config3):
+    fx = config3
+    ctx = _ctx(sb, fx)
+    st = ctx.synth(np.zeros((0, fx["record"].shape[1], fx["record"].shape[2]), np.float32))
+    assert st.shape[0] == 0
+    with pytest.raises(ValueError):
+        ctx.synth(fx["record"][:, :10])
+    lib = sb.lib()
+    rc = lib.snapi_synth(ctypes.c_void_p(ctx._ctx), -1, None, None, 0)
+    assert rc == -1
+    rc = lib.snapi_adjoint(ctypes.c_void_p(ctx._ctx), 1, None, None, None, None, 0, None, None, None, None, None, 0)
+    assert rc == -1
+    ctx.close()
+    bad = dict(fx)
+    bad["tau500"] = fx["tau500"][::-1].copy()
+    with pytest.raises(sb.SnapiError):
+        sb.Context.from_fixture(bad, stokes_scale=1.0)
+    with pytest.raises(sb.SnapiError):
+        sb.Context.from_fixture(fx, stokes_scale=1.0, mu=0.0)
+
+
+def test_device_pointer_api(sb, config3):
+    import torch
+    fx = config3
+    n = 3
+    ctx = _ctx(sb, fx)
+    ref = ctx.adjoint(fx["record"][:n], fx["target"][:n], fx["tangent"][:n])
+    dev = torch.device("cuda:0")
+    rec = torch.tensor(fx["record"][:n], dtype=torch.float32, device=dev)
+    obs = torch.tensor(fx["target"][:n], dtype=torch.float32, device=dev)
+    tan = torch.tensor(fx["tangent"][:n], dtype=torch.float32, device=dev)
+    chi2 = torch.zeros(n, dtype=torch.float64, device=dev)
+    grad = torch.zeros(n, 10, dtype=torch.float64, device=dev)
+    st = torch.zeros(n, fx["lambda_air"].shape[0], 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    ctx.adjoint_device(n, rec.data_ptr(), obs.data_ptr(), 10, tan.data_ptr(), chi2.data_ptr(), grad.data_ptr(),
+                       stokes_ptr=st.data_ptr())
+    ctx.close()
+    np.testing.assert_allclose(chi2.cpu().numpy(), ref["chi2"], rtol=1e-12)
+    # equal up to the order of the shared-memory float atomics of the reduction
+    np.testing.assert_allclose(grad.cpu().numpy(), ref["grad"], rtol=1e-5, atol=1e-6 * np.abs(ref["grad"]).max())
+    assert np.array_equal(st.cpu().numpy(), ref["stokes"])
+
+
+def test_size_independent_properties_at_scale(sb, config3):
+    """Full-size batch (64x64 pixels built from the fixture columns): finite outputs, identical
+    results for identical pixels, and linearity of the gradient in the tangents."""
+    fx = config3
+    npix = 4096
+    idx = np.arange(npix) % fx["record"].shape[0]
+    rec = fx["record"][idx]
+    obs = fx["target"][idx]
+    tan = fx["tangent"][idx]
+    ctx = _ctx(sb, fx)
+    out = ctx.adjoint(rec, obs, tan)
+    out2 = ctx.adjoint(rec[:8], obs[:8], 2.0 * tan[:8])
+    ctx.close()
+    assert np.all(np.isfinite(out["grad"])) and np.all(np.isfinite(out["stokes"]))
+    k = fx["record"].shape[0]
+    gmax = np.abs(out["grad"]).max(axis=0)
+    for p in range(k):
+        # identical pixels: equal up to the order of the shared-memory float atomics
+        same = out["grad"][idx == p]
+        assert np.all(np.abs(same - same[0]) <= 1e-5 * gmax)
+        st = out["stokes"][idx == p]
+        assert np.all(st == st[0])
+    np.testing.assert_allclose(out2["grad"], 2.0 * out["grad"][:8], rtol=1e-6,
+                               atol=1e-6 * np.abs(out["grad"][:8]).max())
