@@ -1,0 +1,389 @@
+"""Benchmark: pixels/s of Stokes synthesis + chi2 gradient w.r.t. 10 nodes on one B200.
+
+Workload (configs[2] of the metric): 64 x 64 pixels, 80 depths (log tau500 -6..1), 201 wavelengths
+(Fe I 6301.5 / 6302.5, 12 mA), mu = 1, ten-node model (T x4, v_turb, v_los x2, B, inclination,
+azimuth).  One step = one call over all pixels: forward synthesis, chi2 against a noisy target
+and the adjoint (reverse) sweep giving d chi2 / d node for every pixel.
+
+Inputs: the thermal structure of each pixel is one of 32 columns built by the reference's own
+hydrostatic-equilibrium + chemistry code (tests/golden/bench_pool.npz, seed 303, with the node
+tangents of the reference's build_from_nodes); v_turb, v_los, B, inclination and azimuth are
+drawn per pixel (seed 3) -- they enter the columns linearly through the node interpolation.
+Target = synthesised truth + N(0, 1e-3 Ic); the evaluated model = truth with fixed node offsets.
+Inputs (~400 MB) exceed the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl snapi|reference]
+
+Prints one JSON line (rank 0).  --impl reference times the reference's own CPU implementation
+(oracle/_ref/snapi_ref_bench, the reference sources compiled with their -O3 -ffast-math flags)
+on the host cores for the same metric.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+POOL = os.path.join(ROOT, "tests", "golden", "bench_pool.npz")
+TASK = os.path.join(ROOT, "tests", "golden", "c3.tsk")
+REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "snapi_ref_bench")
+METRIC = "pixels/s Stokes synth+grad on 1 B200, adjoint vs plain FD, at 1e-5 Ic"
+NPIX = 64 * 64
+FD_STEPS = np.array([5.0, 5.0, 5.0, 5.0, 2e3, 2e3, 2e3, 5.0, 5e-3, 5e-3])
+
+
+def make_workload(pool, npix=NPIX, seed=3):
+    """Per-pixel records / tangents / truth for the benchmark (see the module docstring)."""
+    rng = np.random.default_rng(seed)
+    ncol = pool["record"].shape[0]
+    col = rng.integers(0, ncol, npix)
+    rec = pool["record"][col].astype(np.float32)
+    tan = pool["tangent"][col].astype(np.float32)
+    w1 = pool["tangent"][0, 5, :, 3].astype(np.float64)  # d v_los(depth) / d v_los node 1
+    w2 = pool["tangent"][0, 6, :, 3].astype(np.float64)
+    truth = {
+        "vt": rng.uniform(0.5e5, 2.0e5, npix),
+        "v1": rng.normal(0.0, 1.0e5, npix),
+        "v2": rng.normal(0.0, 1.0e5, npix),
+        "B": 10.0 ** rng.uniform(2.0, np.log10(2500.0), npix),
+        "th": rng.uniform(np.deg2rad(20.0), np.deg2rad(160.0), npix),
+        "ph": rng.uniform(np.deg2rad(10.0), np.deg2rad(170.0), npix),
+    }
+
+    def apply(r, p):
+        r = r.copy()
+        r[:, :, 1] = p["vt"][:, None]
+        r[:, :, 3] = p["v1"][:, None] * w1[None, :] + p["v2"][:, None] * w2[None, :]
+        r[:, :, 4] = p["B"][:, None]
+        r[:, :, 5] = np.rad2deg(p["th"])[:, None]
+        az = np.rad2deg(p["ph"])
+        r[:, :, 6] = np.where(az > 90.0, az - 180.0, az)[:, None]  # atan quirk, atmos_rad.cc:45
+        return r
+
+    model = dict(truth)
+    model["vt"] = truth["vt"] + 0.3e5
+    model["v1"] = truth["v1"] + 0.3e5
+    model["v2"] = truth["v2"] - 0.3e5
+    model["B"] = truth["B"] + 200.0
+    model["th"] = truth["th"] + 0.1
+    model["ph"] = truth["ph"] + 0.1
+    return apply(rec, truth), apply(rec, model), tan
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks and throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(prefix="clocks_", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.out.close()
+        rows = [ln.split(",") for ln in open(self.out.name).read().strip().splitlines() if ln.strip()]
+        os.unlink(self.out.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() in ("active", "1"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def reduce_max(x, world, device):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_snapi(args):
+    import torch
+
+    sys.path.insert(0, ROOT)
+    import snapi_b200 as sb
+    from snapi_b200 import build as b
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    b.build_cuda()
+    pool = dict(np.load(POOL))
+    truth, model, tan = make_workload(pool, NPIX, seed=3 + 1000 * rank)
+    ic = float(pool["stokes"][:, :, 0].max())
+    npar = tan.shape[1]
+    nl = pool["lambda_air"].shape[0]
+    ctx = sb.Context.from_fixture(pool, stokes_scale=ic, max_batch=NPIX, device=local)
+    # target: synthesised truth + noise (set-up, not timed)
+    obs = ctx.synth(truth)
+    obs += np.random.default_rng(77 + rank).normal(0.0, 1e-3 * ic, obs.shape).astype(np.float32)
+    # device-resident inputs
+    d_rec = torch.from_numpy(model).to(dev)
+    d_obs = torch.from_numpy(obs).to(dev)
+    d_tan = torch.from_numpy(tan).to(dev)
+    d_chi2 = torch.zeros(NPIX, dtype=torch.float64, device=dev)
+    d_grad = torch.zeros(NPIX, npar, dtype=torch.float64, device=dev)
+    d_st = torch.zeros(NPIX, nl, 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    torch.cuda.synchronize()
+
+    def step():
+        ctx.adjoint_device(NPIX, d_rec.data_ptr(), d_obs.data_ptr(), npar, d_tan.data_ptr(), d_chi2.data_ptr(),
+                           d_grad.data_ptr(), stokes_ptr=d_st.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    kern_ms = 0.0
+    launches = 0
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        kern_ms += ctx.last_kernel_ms
+        launches += ctx.last_launches
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    total_ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    barrier(world)
+    total_ms = reduce_max(total_ms, world, dev)
+    ms_step = total_ms / args.steps
+    value = NPIX * world / (ms_step / 1e3)
+
+    # plain FD gradient (2 npar + 1 forward solves) on the same inputs, for the adjoint-vs-FD ratio
+    def fd_step():
+        ctx.fd_grad_device(NPIX, d_rec.data_ptr(), d_obs.data_ptr(), npar, d_tan.data_ptr(), FD_STEPS,
+                           d_chi2.data_ptr(), d_grad.data_ptr())
+
+    fd_step()
+    torch.cuda.synchronize()
+    nfd = max(1, args.steps // 5)
+    ev0.record(stream)
+    for _ in range(nfd):
+        fd_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    fd_ms = reduce_max(ev0.elapsed_time(ev1) / nfd, world, dev)
+
+    # end to end through the host API: pinned host inputs, H2D + kernel + D2H every step
+    h_rec = np.frombuffer((ctypes_buffer(ctx, model.nbytes)), dtype=np.float32).reshape(model.shape)
+    h_rec[...] = model
+    h_obs = np.frombuffer((ctypes_buffer(ctx, obs.nbytes)), dtype=np.float32).reshape(obs.shape)
+    h_obs[...] = obs
+    h_tan = np.frombuffer((ctypes_buffer(ctx, tan.nbytes)), dtype=np.float32).reshape(tan.shape)
+    h_tan[...] = tan
+    ctx.adjoint(h_rec, h_obs, h_tan)
+    torch.cuda.synchronize()
+    barrier(world)
+    ne = max(1, args.steps // 2)
+    ev0.record(stream)
+    for _ in range(ne):
+        out = ctx.adjoint(h_rec, h_obs, h_tan)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = reduce_max(ev0.elapsed_time(ev1) / ne, world, dev)
+    h2d = model.nbytes + obs.nbytes + tan.nbytes
+    d2h = out["stokes"].nbytes + out["chi2"].nbytes + out["grad"].nbytes
+
+    line = None
+    if rank == 0:
+        kern_per_launch_ms = kern_ms / max(launches, 1)
+        # algorithmic bytes per pixel: record + tangents + target in, Stokes + grad + chi2 out
+        nd = model.shape[1]
+        nf = model.shape[2]
+        bytes_pix = 4 * (nd * nf + npar * nd * nf + nl * 4) + 4 * nl * 4 + 8 * (npar + 1)
+        achieved = bytes_pix * NPIX / (kern_per_launch_ms / 1e3) / 1e9
+        peaks = load_peaks()
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "pixels/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 (profiles, formal solver); f64 (optical depth, DELO weights, W4 core derivative)",
+            "data": "synthetic: reference-built columns (HE + chemistry) x seeded per-pixel field/velocity nodes",
+            "config": {"workload": "64x64 pixels x 80 depths x 201 wavelengths, Fe I 6301.5/6302.5, mu=1, "
+                                   "10 nodes (T x4, vturb, vlos x2, B, incl, azi): synthesis + chi2 + adjoint "
+                                   "d chi2/d nodes", "pixels_per_gpu": NPIX, "nd": int(nd), "nlambda": int(nl),
+                       "npar": int(npar), "l2_flush": "inputs ~0.4 GB per step exceed the 126 MB L2",
+                       "parallelism": "replicas (pixels independent)"},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "e2e": {"value": NPIX * world / (e2e_ms / 1e3), "unit": "pixels/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "fd_baseline": {"value": NPIX * world / (fd_ms / 1e3), "unit": "pixels/s", "ms_per_step": fd_ms,
+                            "solves_per_gradient": 2 * npar + 1, "adjoint_speedup": fd_ms / ms_step},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                         "peak_source": peaks["source"], "kernel": "k_adjoint",
+                         "note": "compute (FP32/SFU issue) bound, not HBM bound; see DESIGN.md"},
+        }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = reference_cpu_rate(samples_per_core=1, mode=1)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def ctypes_buffer(ctx, nbytes):
+    import ctypes
+
+    import snapi_b200 as sb
+    p = sb.lib().snapi_host_alloc(nbytes)
+    if not p:
+        raise MemoryError("snapi_host_alloc")
+    return (ctypes.c_char * nbytes).from_address(p)
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def reference_cpu_rate(samples_per_core=1, mode=1, cores=None):
+    """Run the reference's own CPU code (oracle/_ref/snapi_ref_bench) as one process per host
+    core, the reference's islave model, on seeded config-3 pixels."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import config3_nodes
+    ncores = cores or os.cpu_count() or 1
+    npix = ncores * samples_per_core
+    nodes = config3_nodes(npix, seed=3)
+    nf = tempfile.NamedTemporaryFile(suffix=".f64", delete=False)
+    nodes.astype("<f8").tofile(nf.name)
+    t0 = time.perf_counter()
+    procs = [subprocess.Popen([REF_BENCH, TASK, nf.name, str(i * samples_per_core), str(samples_per_core), str(mode)],
+                              stdout=subprocess.PIPE, stderr=subprocess.DEVNULL) for i in range(ncores)]
+    outs = [p.communicate()[0].decode() for p in procs]
+    wall = time.perf_counter() - t0
+    os.unlink(nf.name)
+    ok = all(p.returncode == 0 for p in procs) and all(o.startswith("pixels") for o in outs)
+    what = {0: "obs_stokes", 1: "obs_stokes_responses_to_nodes", 2: "obs_stokes_num_responses_to_nodes"}[mode]
+    return {"value": npix / wall if ok else None, "unit": "pixels/s", "cores": ncores, "kind": "reference",
+            "sample": "%d seeded config-3 pixels (%d per core), build_from_nodes + %s, reference sources "
+                      "compiled -O3 -ffast-math, one process per core" % (npix, samples_per_core, what),
+            "wall_s": wall}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    ncores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        reference_cpu_rate(samples_per_core=1, mode=1, cores=ncores)
+    t0 = time.perf_counter()
+    tot = 0
+    last = None
+    for _ in range(args.steps):
+        last = reference_cpu_rate(samples_per_core=1, mode=1, cores=ncores)
+        tot += ncores
+    wall = time.perf_counter() - t0
+    value = tot / wall
+    cpu = dict(last)
+    cpu["value"] = value
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "pixels/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": wall / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: seeded config-3 node models (seed 3), the reference builds the columns itself",
+        "config": {"workload": "config-3 pixels (80 depths x 201 wavelengths, 10 nodes): build_from_nodes + "
+                               "obs_stokes_responses_to_nodes (synthesis + node responses)",
+                   "pixels_per_step": ncores, "parallelism": "one process per host core"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": "pixels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="snapi", choices=["snapi", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    line = run_reference(args) if args.impl == "reference" else run_snapi(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -57,7 +57,7 @@ extern "C" {
 #define SNAPI_NFIELD0 12
 #define SNAPI_MAX_LINES 8
 #define SNAPI_MAX_COMP 16
-#define SNAPI_MAX_LAMBDA 1024
+#define SNAPI_MAX_LAMBDA 8192
 
 typedef struct snapi_ctx snapi_ctx;
 

@@ -15,7 +15,7 @@ import os
 import numpy as np
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "libsnapi_cuda.so")
+LIB_PATH = os.environ.get("SNAPI_LIB", os.path.join(_PKG, "libsnapi_cuda.so"))
 
 OK, EINVAL, ECUDA, ETIMEOUT, ENONCONV, ENOMEM = 0, -1, -2, -3, -4, -5
 MEM_HOST, MEM_DEVICE = 0, 1

@@ -26,6 +26,18 @@
 #else
 #define SNAPI_HD inline
 #endif
+// The Voigt evaluations are the largest code blocks; out of line they keep the kernels'
+// instruction footprint small (one copy instead of one per call site).
+#ifndef SNAPI_VOIGT_NOINLINE
+#define SNAPI_VOIGT_NOINLINE 1
+#endif
+#if defined(__CUDACC__) && SNAPI_VOIGT_NOINLINE
+#define SNAPI_VOIGT_FN __host__ __device__ __noinline__
+#elif defined(__CUDACC__)
+#define SNAPI_VOIGT_FN __host__ __device__ __forceinline__
+#else
+#define SNAPI_VOIGT_FN inline
+#endif
 
 namespace snapi {
 
@@ -98,9 +110,10 @@ SNAPI_HD cf cmk(float r, float i) { cf z; z.re = r; z.im = i; return z; }
 SNAPI_HD cf cadd(cf a, cf b) { return cmk(a.re + b.re, a.im + b.im); }
 SNAPI_HD cf csub(cf a, cf b) { return cmk(a.re - b.re, a.im - b.im); }
 SNAPI_HD cf cmul(cf a, cf b) { return cmk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+SNAPI_HD float frcp(float x);
 SNAPI_HD cf cdiv(cf a, cf b) {
-  float f = b.re * b.re + b.im * b.im;
-  return cmk((a.re * b.re + a.im * b.im) / f, (a.im * b.re - a.re * b.im) / f);
+  const float r = frcp(b.re * b.re + b.im * b.im);
+  return cmk((a.re * b.re + a.im * b.im) * r, (a.im * b.re - a.re * b.im) * r);
 }
 SNAPI_HD cf caddr(float a, cf b) { return cmk(b.re + a, b.im); }
 SNAPI_HD cf csubr(float a, cf b) { return cmk(a - b.re, -b.im); }
@@ -118,16 +131,22 @@ SNAPI_HD cd daddr(double a, cd b) { return dmk(b.re + a, b.im); }
 SNAPI_HD cd dsubr(double a, cd b) { return dmk(a - b.re, -b.im); }
 SNAPI_HD cd dscl(cd a, double s) { return dmk(a.re * s, a.im * s); }
 
+// Transcendentals of the per-cell math.  On the device the SFU forms are used: their error
+// (about 2 ulp for exp; for sin / cos an absolute error ~1e-6 |x| / pi, with |x| < 10 in W4 region 4
+// where the factor e^{a^2 - v^2} multiplying them is < 2e-4 whenever |x| > 2) stays far below
+// the FP32 rounding of the sums they feed.  frcp is the correctly rounded reciprocal.
 #ifdef __CUDA_ARCH__
-SNAPI_HD float fexp(float x) { return expf(x); }
-SNAPI_HD void fsincos(float x, float *s, float *c) { sincosf(x, s, c); }
+SNAPI_HD float fexp(float x) { return __expf(x); }
+SNAPI_HD void fsincos(float x, float *s, float *c) { __sincosf(x, s, c); }
+SNAPI_HD float frcp(float x) { return __frcp_rn(x); }
 #else
 SNAPI_HD float fexp(float x) { return expf(x); }
 SNAPI_HD void fsincos(float x, float *s, float *c) { *s = sinf(x); *c = cosf(x); }
+SNAPI_HD float frcp(float x) { return 1.0f / x; }
 #endif
 
 // Humlicek W4 (published region split and coefficients); H, F divided by sqrt(pi).
-SNAPI_HD void voigt(float x, float a, float &H, float &F) {
+SNAPI_VOIGT_FN void voigt(float x, float a, float &H, float &F) {
   const float v = x;
   const float s = fabsf(v) + a;
   const cf t = cmk(a, -v);
@@ -171,8 +190,62 @@ SNAPI_HD void voigt(float x, float a, float &H, float &F) {
   F = w4.im * kSqrtPiInv;
 }
 
+// Region 4 of W4 with its exact derivatives.  With R = t p(u)/q(u) the derivative is written as
+// r = p/q, r' = (p' - r q')/q, dR/dt = r + 2u r', which keeps every intermediate within FP32
+// range (|q| < 3e10 in this region; forming q^2 and dividing by it would overflow).
+SNAPI_VOIGT_FN void voigt_grad_core(float a, float v, cf &w4, cf &dwa, cf &dwv) {
+  const cf t = cmk(a, -v);
+  const cf u = cmk(a * a - v * v, -2.0f * a * v);
+  cf p = csubr(1.320522f, cscl(u, 0.56419f));
+  p = csubr(35.76683f, cmul(u, p));
+  p = csubr(219.0313f, cmul(u, p));
+  p = csubr(1540.787f, cmul(u, p));
+  p = csubr(3321.9905f, cmul(u, p));
+  p = csubr(36183.31f, cmul(u, p));
+  // p(u) = c0 - c1 u + c2 u^2 - c3 u^3 + c4 u^4 - c5 u^5 + c6 u^6
+  // p'(u) = -c1 + 2 c2 u - 3 c3 u^2 + 4 c4 u^3 - 5 c5 u^4 + 6 c6 u^5
+  cf pp = cmk(6.0f * 0.56419f, 0.0f);
+  pp = caddr(-5.0f * 1.320522f, cmul(u, pp));
+  pp = caddr(4.0f * 35.76683f, cmul(u, pp));
+  pp = caddr(-3.0f * 219.0313f, cmul(u, pp));
+  pp = caddr(2.0f * 1540.787f, cmul(u, pp));
+  pp = caddr(-3321.9905f, cmul(u, pp));
+  cf q = csubr(1.841439f, u);
+  q = csubr(61.57037f, cmul(u, q));
+  q = csubr(364.2191f, cmul(u, q));
+  q = csubr(2186.181f, cmul(u, q));
+  q = csubr(9022.228f, cmul(u, q));
+  q = csubr(24322.84f, cmul(u, q));
+  q = csubr(32066.6f, cmul(u, q));
+  // q(u) = d0 - d1 u + d2 u^2 - d3 u^3 + d4 u^4 - d5 u^5 + d6 u^6 - u^7
+  cf qp = cmk(-7.0f, 0.0f);
+  qp = caddr(6.0f * 1.841439f, cmul(u, qp));
+  qp = caddr(-5.0f * 61.57037f, cmul(u, qp));
+  qp = caddr(4.0f * 364.2191f, cmul(u, qp));
+  qp = caddr(-3.0f * 2186.181f, cmul(u, qp));
+  qp = caddr(2.0f * 9022.228f, cmul(u, qp));
+  qp = caddr(-24322.84f, cmul(u, qp));
+  float su, cu;
+  fsincos(u.im, &su, &cu);
+  const float eu = fexp(u.re);
+  const float ca = sqrtf(1.0f - su * su);
+  const cf r = cdiv(p, q);
+  const cf rp = cdiv(csub(pp, cmul(r, qp)), q);
+  const cf R = cmul(t, r);
+  const cf E = cmk(eu * ca, eu * su);
+  w4 = csub(E, R);
+  const cf Rp = cadd(r, cmul(cscl(u, 2.0f), rp));
+  // E = e^{ur} (|cos ui|, sin ui): dE/dur = E, dE/dui = e^{ur} (-sgn(cos ui) sin ui, cos ui)
+  const float sg = (cu > 0.0f) ? 1.0f : ((cu < 0.0f) ? -1.0f : 0.0f);
+  const cf Eui = cmk(-eu * sg * su, eu * cu);
+  // ur = a^2 - v^2, ui = -2 a v, dt/da = 1, dt/dv = -i
+  dwa = csub(cadd(cscl(E, 2.0f * a), cscl(Eui, -2.0f * v)), Rp);
+  const cf Rv = cmk(Rp.im, -Rp.re);
+  dwv = csub(cadd(cscl(E, -2.0f * v), cscl(Eui, -2.0f * a)), Rv);
+}
+
 // W4 with its exact partial derivatives with respect to x (= v) and a.
-SNAPI_HD void voigt_grad(float x, float a, float &H, float &F, float &Hx, float &Fx, float &Ha, float &Fa) {
+SNAPI_VOIGT_FN void voigt_grad(float x, float a, float &H, float &F, float &Hx, float &Fx, float &Ha, float &Fa) {
   const float v = x;
   const float s = fabsf(v) + a;
   const cf t = cmk(a, -v);
@@ -214,58 +287,7 @@ SNAPI_HD void voigt_grad(float x, float a, float &H, float &F, float &Hx, float 
     dwa = wp;                        // dt/da = 1
     dwv = cmk(wp.im, -wp.re);        // dt/dv = -i
   } else {
-    // Region 4 in FP64: near |v| ~ 5 the real part of dw/dv is ~1e-3 of |dw/dv| and the
-    // quotient-rule terms cancel far below FP32 resolution.
-    const double ad = a, vd = v;
-    const cd td = dmk(ad, -vd);
-    const cd ud = dmk(ad * ad - vd * vd, -2.0 * ad * vd);
-    cd p = dsubr(1.320522, dscl(ud, 0.56419));
-    p = dsubr(35.76683, dmul(ud, p));
-    p = dsubr(219.0313, dmul(ud, p));
-    p = dsubr(1540.787, dmul(ud, p));
-    p = dsubr(3321.9905, dmul(ud, p));
-    p = dsubr(36183.31, dmul(ud, p));
-    // p(u) = c0 - c1 u + c2 u^2 - c3 u^3 + c4 u^4 - c5 u^5 + c6 u^6
-    // p'(u) = -c1 + 2 c2 u - 3 c3 u^2 + 4 c4 u^3 - 5 c5 u^4 + 6 c6 u^5
-    cd pp = dmk(6.0 * 0.56419, 0.0);
-    pp = daddr(-5.0 * 1.320522, dmul(ud, pp));
-    pp = daddr(4.0 * 35.76683, dmul(ud, pp));
-    pp = daddr(-3.0 * 219.0313, dmul(ud, pp));
-    pp = daddr(2.0 * 1540.787, dmul(ud, pp));
-    pp = daddr(-3321.9905, dmul(ud, pp));
-    cd q = dsubr(1.841439, ud);
-    q = dsubr(61.57037, dmul(ud, q));
-    q = dsubr(364.2191, dmul(ud, q));
-    q = dsubr(2186.181, dmul(ud, q));
-    q = dsubr(9022.228, dmul(ud, q));
-    q = dsubr(24322.84, dmul(ud, q));
-    q = dsubr(32066.6, dmul(ud, q));
-    // q(u) = d0 - d1 u + d2 u^2 - d3 u^3 + d4 u^4 - d5 u^5 + d6 u^6 - u^7
-    cd qp = dmk(-7.0, 0.0);
-    qp = daddr(6.0 * 1.841439, dmul(ud, qp));
-    qp = daddr(-5.0 * 61.57037, dmul(ud, qp));
-    qp = daddr(4.0 * 364.2191, dmul(ud, qp));
-    qp = daddr(-3.0 * 2186.181, dmul(ud, qp));
-    qp = daddr(2.0 * 9022.228, dmul(ud, qp));
-    qp = daddr(-24322.84, dmul(ud, qp));
-    const double su = sin(ud.im), cu = cos(ud.im);
-    const double eu = exp(ud.re);
-    const double ca = sqrt(1.0 - su * su);
-    const cd R = ddiv(dmul(td, p), q);
-    const cd E = dmk(eu * ca, eu * su);
-    const cd wd = dsub(E, R);
-    // dR/dt = p/q + 2 t^2 (p' q - p q') / q^2
-    const cd Rp = dadd(ddiv(p, q), dmul(dscl(ud, 2.0), ddiv(dsub(dmul(pp, q), dmul(p, qp)), dmul(q, q))));
-    // E = e^{ur} (|cos ui|, sin ui): dE/dur = E, dE/dui = e^{ur} (-sgn(cos ui) sin ui, cos ui)
-    const double sg = (cu > 0.0) ? 1.0 : ((cu < 0.0) ? -1.0 : 0.0);
-    const cd Eui = dmk(-eu * sg * su, eu * cu);
-    // ur = a^2 - v^2, ui = -2 a v, dt/da = 1, dt/dv = -i
-    const cd dwad = dsub(dadd(dscl(E, 2.0 * ad), dscl(Eui, -2.0 * vd)), Rp);
-    const cd Rv = dmk(Rp.im, -Rp.re);
-    const cd dwvd = dsub(dadd(dscl(E, -2.0 * vd), dscl(Eui, -2.0 * ad)), Rv);
-    w4 = cmk((float)wd.re, (float)wd.im);
-    dwa = cmk((float)dwad.re, (float)dwad.im);
-    dwv = cmk((float)dwvd.re, (float)dwvd.im);
+    voigt_grad_core(a, v, w4, dwa, dwv);
   }
   H = w4.re * kSqrtPiInv;
   F = w4.im * kSqrtPiInv;
@@ -424,14 +446,35 @@ SNAPI_HD void cell_opacity_adjoint(const DepthConst &d, const LineDepth *ld, con
       x0b += Hb_ * Hx;
       ab += Hb_ * Ha;
     } else {
+      // adjoints of the component sums depend only on (eta-bar, j-bar) and the angles, so one
+      // pass of voigt_grad per component gives both the sums and the x / a adjoints
+      float Pb[7];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) Pb[k] = q.opn * etab[k] + (k < 4 ? q.emn * jb[k] : 0.0f);
+      const float hpmb = 0.5f * d.st2 * (d.c2 * Pb[1] + d.s2 * Pb[2]);
+      const float fpmb = 0.5f * d.st2 * (d.c2 * Pb[4] + d.s2 * Pb[5]);
+      float Hsb[3], Fsb[3];
+      Hsb[0] = 0.5f * d.st2 * Pb[0] + hpmb;
+      Hsb[1] = 0.25f * d.opc2 * Pb[0] - 0.5f * hpmb - 0.5f * d.ctb * Pb[3];
+      Hsb[2] = 0.25f * d.opc2 * Pb[0] - 0.5f * hpmb + 0.5f * d.ctb * Pb[3];
+      Fsb[0] = fpmb;
+      Fsb[1] = -0.5f * fpmb - 0.5f * d.ctb * Pb[6];
+      Fsb[2] = -0.5f * fpmb + 0.5f * d.ctb * Pb[6];
       float Hs[3] = {0.f, 0.f, 0.f}, Fs[3] = {0.f, 0.f, 0.f};
       int off = L.comp_off;
+#pragma unroll
       for (int g = 0; g < 3; ++g)
         for (int i = 0; i < L.ncomp[g]; ++i, ++off) {
-          float H, F;
-          voigt(x0 + compD[off] * q.bsh, q.a, H, F);
-          Hs[g] += H * compS[off];
-          Fs[g] += F * compS[off];
+          float H, F, Hx, Fx, Ha, Fa;
+          voigt_grad(x0 + compD[off] * q.bsh, q.a, H, F, Hx, Fx, Ha, Fa);
+          const float S = compS[off];
+          Hs[g] += H * S;
+          Fs[g] += F * S;
+          const float hb_ = Hsb[g] * S, fb_ = Fsb[g] * S;
+          const float xb = hb_ * Hx + fb_ * Fx;
+          x0b += xb;
+          bb += xb * compD[off];
+          ab += hb_ * Ha + fb_ * Fa;
         }
       const float hpm = Hs[0] - 0.5f * (Hs[2] + Hs[1]);
       const float fpm = Fs[0] - 0.5f * (Fs[2] + Fs[1]);
@@ -443,52 +486,18 @@ SNAPI_HD void cell_opacity_adjoint(const DepthConst &d, const LineDepth *ld, con
                           0.5f * fpm * d.st2 * d.s2,
                           0.5f * (Fs[2] - Fs[1]) * d.ctb};
       float gop = 0.f, gem = 0.f;
+#pragma unroll
       for (int k = 0; k < 7; ++k) gop += etab[k] * P[k];
+#pragma unroll
       for (int k = 0; k < 4; ++k) gem += jb[k] * P[k];
       rl[RL_OPN] += gop;
       rl[RL_EMN] += gem;
-      float Pb[7];
-      for (int k = 0; k < 7; ++k) Pb[k] = q.opn * etab[k] + (k < 4 ? q.emn * jb[k] : 0.0f);
-      // P -> Hs, Fs, angle factors
-      const float hsum = Hs[2] + Hs[1];
-      float Hsb[3], Fsb[3];
-      // P0 = 0.5*Hs0*st2 + 0.25*hsum*opc2
-      Hsb[0] = 0.5f * d.st2 * Pb[0];
-      Hsb[1] = 0.25f * d.opc2 * Pb[0];
-      Hsb[2] = 0.25f * d.opc2 * Pb[0];
-      st2b += 0.5f * Hs[0] * Pb[0];
-      float opc2b = 0.25f * hsum * Pb[0];
-      // P1 = 0.5 hpm st2 c2, P2 = 0.5 hpm st2 s2
-      float hpmb = 0.5f * d.st2 * (d.c2 * Pb[1] + d.s2 * Pb[2]);
-      st2b += 0.5f * hpm * (d.c2 * Pb[1] + d.s2 * Pb[2]);
-      c2b += 0.5f * hpm * d.st2 * Pb[1];
-      s2b += 0.5f * hpm * d.st2 * Pb[2];
-      Hsb[0] += hpmb; Hsb[1] -= 0.5f * hpmb; Hsb[2] -= 0.5f * hpmb;
-      // P3 = 0.5 (Hs2 - Hs1) ctb
-      Hsb[2] += 0.5f * d.ctb * Pb[3]; Hsb[1] -= 0.5f * d.ctb * Pb[3];
-      ctbb += 0.5f * (Hs[2] - Hs[1]) * Pb[3];
-      // P4, P5 (rho_Q, rho_U)
-      float fpmb = 0.5f * d.st2 * (d.c2 * Pb[4] + d.s2 * Pb[5]);
-      st2b += 0.5f * fpm * (d.c2 * Pb[4] + d.s2 * Pb[5]);
-      c2b += 0.5f * fpm * d.st2 * Pb[4];
-      s2b += 0.5f * fpm * d.st2 * Pb[5];
-      Fsb[0] = fpmb; Fsb[1] = -0.5f * fpmb; Fsb[2] = -0.5f * fpmb;
-      // P6 = 0.5 (Fs2 - Fs1) ctb
-      Fsb[2] += 0.5f * d.ctb * Pb[6]; Fsb[1] -= 0.5f * d.ctb * Pb[6];
-      ctbb += 0.5f * (Fs[2] - Fs[1]) * Pb[6];
-      ctbb += 2.0f * d.ctb * opc2b;
-      // components
-      off = L.comp_off;
-      for (int g = 0; g < 3; ++g)
-        for (int i = 0; i < L.ncomp[g]; ++i, ++off) {
-          float H, F, Hx, Fx, Ha, Fa;
-          voigt_grad(x0 + compD[off] * q.bsh, q.a, H, F, Hx, Fx, Ha, Fa);
-          const float hb_ = Hsb[g] * compS[off], fb_ = Fsb[g] * compS[off];
-          const float xb = hb_ * Hx + fb_ * Fx;
-          x0b += xb;
-          bb += xb * compD[off];
-          ab += hb_ * Ha + fb_ * Fa;
-        }
+      st2b += 0.5f * Hs[0] * Pb[0] + 0.5f * hpm * (d.c2 * Pb[1] + d.s2 * Pb[2]) +
+              0.5f * fpm * (d.c2 * Pb[4] + d.s2 * Pb[5]);
+      ctbb += 2.0f * d.ctb * (0.25f * (Hs[2] + Hs[1]) * Pb[0]) + 0.5f * (Hs[2] - Hs[1]) * Pb[3] +
+              0.5f * (Fs[2] - Fs[1]) * Pb[6];
+      c2b += 0.5f * d.st2 * (hpm * Pb[1] + fpm * Pb[4]);
+      s2b += 0.5f * d.st2 * (hpm * Pb[2] + fpm * Pb[5]);
     }
     rl[RL_XL] += x0b * lc_l.lam;
     rl[RL_XD] += x0b * xd;
@@ -610,7 +619,7 @@ SNAPI_HD void crout4(const float *S, float *D) {
       float sum = 0.f;
 #pragma unroll
       for (int p = 0; p < k; ++p) sum += D[k * 4 + p] * D[p * 4 + j];
-      D[k * 4 + j] = (S[k * 4 + j] - sum) / D[k * 4 + k];
+      D[k * 4 + j] = (S[k * 4 + j] - sum) * frcp(D[k * 4 + k]);
     }
   }
 }
@@ -621,7 +630,7 @@ SNAPI_HD void solve_crout4(const float *LU, const float *b, float *x) {
     float sum = 0.f;
 #pragma unroll
     for (int k = 0; k < i; ++k) sum += LU[i * 4 + k] * y[k];
-    y[i] = (b[i] - sum) / LU[i * 4 + i];
+    y[i] = (b[i] - sum) * frcp(LU[i * 4 + i]);
   }
 #pragma unroll
   for (int i = 3; i >= 0; --i) {
@@ -632,55 +641,107 @@ SNAPI_HD void solve_crout4(const float *LU, const float *b, float *x) {
   }
 }
 
-// linear DELO weights (atmos_ppbez_rts.cc:1070, :1085-1096).  Evaluated in FP64: above the
-// Taylor switch at 1e-2 the closed forms 1/tb - e^-tb (1 + 1/tb) and 1 - 1/tb + e^-tb/tb cancel
-// to ~tb/2 from terms of size 1/tb, which FP32 cannot resolve.
-SNAPI_HD void delo_weights(double tb, float &w0, float &w1, float &etb) {
-  if (tb < 1E-2) {
-    etb = (float)(1.0 - tb + tb * tb * 0.5 - tb * tb * tb / 6.0);
-    w0 = (float)(tb * (0.5 - tb * (1.0 / 3.0 - tb / 8.0)));
-    w1 = (float)(0.5 * tb * (1.0 - tb / 3.0 * (1.0 - tb / 4.0)));
+// linear DELO weights (atmos_ppbez_rts.cc:1070, :1085-1096).  Below tb = 1e-2 the reference's own
+// three-term expansion.  Above it the closed forms 1/tb - e^-tb (1 + 1/tb) and 1 - 1/tb + e^-tb/tb
+// cancel to ~tb/2 from terms of size 1/tb, so up to tb = 0.5 they are evaluated by their exact
+// power series (w0 = sum_k (-1)^(k+1) k/(k+1)! tb^k, w1 = sum_k (-1)^(k+1) tb^k/(k+1)!, truncated
+// after the tb^11 term: < 1e-11 relative), above that by the closed forms (cancellation <= 16x).
+SNAPI_HD void delo_weights(float tb, float &w0, float &w1, float &etb) {
+  if (tb < 1E-2f) {
+    etb = 1.0f - tb + tb * tb * 0.5f - tb * tb * tb / 6.0f;
+    w0 = tb * (0.5f - tb * (1.0f / 3.0f - tb / 8.0f));
+    w1 = 0.5f * tb * (1.0f - tb / 3.0f * (1.0f - tb / 4.0f));
+  } else if (tb < 0.5f) {
+    etb = fexp(-tb);
+    // coefficients of tb^k, k = 11 .. 1
+    float a = -11.0f / 479001600.0f, b = -1.0f / 479001600.0f;
+    a = a * tb + 10.0f / 39916800.0f;  b = b * tb + 1.0f / 39916800.0f;
+    a = a * tb - 9.0f / 3628800.0f;    b = b * tb - 1.0f / 3628800.0f;
+    a = a * tb + 8.0f / 362880.0f;     b = b * tb + 1.0f / 362880.0f;
+    a = a * tb - 7.0f / 40320.0f;      b = b * tb - 1.0f / 40320.0f;
+    a = a * tb + 6.0f / 5040.0f;       b = b * tb + 1.0f / 5040.0f;
+    a = a * tb - 5.0f / 720.0f;        b = b * tb - 1.0f / 720.0f;
+    a = a * tb + 4.0f / 120.0f;        b = b * tb + 1.0f / 120.0f;
+    a = a * tb - 3.0f / 24.0f;         b = b * tb - 1.0f / 24.0f;
+    a = a * tb + 2.0f / 6.0f;          b = b * tb + 1.0f / 6.0f;
+    a = a * tb - 0.5f;                 b = b * tb - 0.5f;
+    w0 = -a * tb;
+    w1 = -b * tb;
   } else {
-    const double e = exp(-tb);
-    etb = (float)e;
-    w0 = (float)(1.0 / tb - e * (1.0 + 1.0 / tb));
-    w1 = (float)(1.0 - 1.0 / tb + e / tb);
+    etb = fexp(-tb);
+    const float it = frcp(tb);
+    w0 = it - etb * (1.0f + it);
+    w1 = 1.0f - it + etb * it;
   }
 }
-SNAPI_HD void delo_weights_grad(double tb, float &dw0, float &dw1, float &detb) {
-  if (tb < 1E-2) {
-    detb = (float)(-1.0 + tb - 0.5 * tb * tb);
-    dw0 = (float)(0.5 - tb * (2.0 / 3.0 - 3.0 * tb / 8.0));
-    // w1 = 0.5 tb - tb^2/6 + tb^3/24
-    dw1 = (float)(0.5 - tb / 3.0 + tb * tb / 8.0);
+SNAPI_HD void delo_weights_grad(float tb, float &dw0, float &dw1, float &detb) {
+  if (tb < 1E-2f) {
+    detb = -1.0f + tb - 0.5f * tb * tb;
+    dw0 = 0.5f - tb * (2.0f / 3.0f - 3.0f * tb / 8.0f);
+    dw1 = 0.5f - tb / 3.0f + tb * tb / 8.0f;
+  } else if (tb < 0.5f) {
+    detb = -fexp(-tb);
+    // d/dtb of the series above: sum_k (-1)^(k+1) k^2/(k+1)! tb^(k-1), sum_k (-1)^(k+1) k/(k+1)! tb^(k-1)
+    float a = -121.0f / 479001600.0f, b = -11.0f / 479001600.0f;
+    a = a * tb + 100.0f / 39916800.0f; b = b * tb + 10.0f / 39916800.0f;
+    a = a * tb - 81.0f / 3628800.0f;   b = b * tb - 9.0f / 3628800.0f;
+    a = a * tb + 64.0f / 362880.0f;    b = b * tb + 8.0f / 362880.0f;
+    a = a * tb - 49.0f / 40320.0f;     b = b * tb - 7.0f / 40320.0f;
+    a = a * tb + 36.0f / 5040.0f;      b = b * tb + 6.0f / 5040.0f;
+    a = a * tb - 25.0f / 720.0f;       b = b * tb - 5.0f / 720.0f;
+    a = a * tb + 16.0f / 120.0f;       b = b * tb + 4.0f / 120.0f;
+    a = a * tb - 9.0f / 24.0f;         b = b * tb - 3.0f / 24.0f;
+    a = a * tb + 4.0f / 6.0f;          b = b * tb + 2.0f / 6.0f;
+    dw0 = -(a * tb - 0.5f);
+    dw1 = -(b * tb - 0.5f);
   } else {
-    const double e = exp(-tb);
-    detb = (float)(-e);
-    // w0 = 1/tb - e (1 + 1/tb)
-    dw0 = (float)(-1.0 / (tb * tb) + e * (1.0 + 1.0 / tb) + e / (tb * tb));
-    // w1 = 1 - 1/tb + e/tb
-    dw1 = (float)(1.0 / (tb * tb) - e / tb - e / (tb * tb));
+    const float e = fexp(-tb);
+    const float it = frcp(tb);
+    detb = -e;
+    dw0 = -it * it + e * (1.0f + it) + e * it * it;
+    dw1 = it * it - e * it - e * it * it;
   }
+}
+
+// y = K' x and y = K'^T x for K' given by kp = (q,u,v,rq,ru,rv)
+SNAPI_HD void kp_mul(const float *kp, const float *x, float *y) {
+  y[0] = kp[0] * x[1] + kp[1] * x[2] + kp[2] * x[3];
+  y[1] = kp[0] * x[0] + kp[5] * x[2] - kp[4] * x[3];
+  y[2] = kp[1] * x[0] - kp[5] * x[1] + kp[3] * x[3];
+  y[3] = kp[2] * x[0] + kp[4] * x[1] - kp[3] * x[2];
+}
+SNAPI_HD void kp_mul_t(const float *kp, const float *x, float *y) {
+  y[0] = kp[0] * x[1] + kp[1] * x[2] + kp[2] * x[3];
+  y[1] = kp[0] * x[0] - kp[5] * x[2] + kp[4] * x[3];
+  y[2] = kp[1] * x[0] + kp[5] * x[1] - kp[3] * x[3];
+  y[3] = kp[2] * x[0] - kp[4] * x[1] + kp[3] * x[2];
+}
+// adjoint of y = K'(kp) x w.r.t. kp for the outer product yb x^T: d<yb, K'x>/dkp
+SNAPI_HD void kp_outer_proj(const float *yb, const float *x, float scale, float *kpb) {
+  kpb[0] += scale * (yb[0] * x[1] + yb[1] * x[0]);
+  kpb[1] += scale * (yb[0] * x[2] + yb[2] * x[0]);
+  kpb[2] += scale * (yb[0] * x[3] + yb[3] * x[0]);
+  kpb[3] += scale * (yb[2] * x[3] - yb[3] * x[2]);
+  kpb[4] += scale * (yb[3] * x[1] - yb[1] * x[3]);
+  kpb[5] += scale * (yb[1] * x[2] - yb[2] * x[1]);
+}
+// A = 1 + w1 K' (transpose: flip the sign of the rho terms)
+SNAPI_HD void build_A(const float *kp, float w1, bool transpose, float *A) {
+  const float r = transpose ? -w1 : w1;
+  A[0] = 1.0f;        A[1] = w1 * kp[0]; A[2] = w1 * kp[1]; A[3] = w1 * kp[2];
+  A[4] = w1 * kp[0];  A[5] = 1.0f;       A[6] = r * kp[5];  A[7] = -r * kp[4];
+  A[8] = w1 * kp[1];  A[9] = -r * kp[5]; A[10] = 1.0f;      A[11] = r * kp[3];
+  A[12] = w1 * kp[2]; A[13] = r * kp[4]; A[14] = -r * kp[3]; A[15] = 1.0f;
 }
 
 // One linear-DELO step: I_c = (1 + w1 K'_c)^-1 [ -w0 K'_p I_p + w0 S_p + w1 S_c + etb I_p ]
 SNAPI_HD void delo_step(const float *Ip, const float *kpp, const float *Sp, const float *kpc, const float *Sc,
-                        double tb, float *Ic) {
+                        float tb, float *Ic) {
   float w0, w1, etb;
   delo_weights(tb, w0, w1, etb);
-  float Kp[16], Kc[16], A[16], LU[16], B[4], tv[4];
-  kprime_full(kpp, Kp);
-  kprime_full(kpc, Kc);
-#pragma unroll
-  for (int s = 0; s < 4; ++s) {
-    tv[s] = Kp[s * 4 + 0] * Ip[0] + Kp[s * 4 + 1] * Ip[1] + Kp[s * 4 + 2] * Ip[2] + Kp[s * 4 + 3] * Ip[3];
-  }
-#pragma unroll
-  for (int s = 0; s < 4; ++s) {
-#pragma unroll
-    for (int sp = 0; sp < 4; ++sp) A[s * 4 + sp] = w1 * Kc[s * 4 + sp];
-    A[s * 4 + s] += 1.0f;
-  }
+  float A[16], LU[16], B[4], tv[4];
+  kp_mul(kpp, Ip, tv);
+  build_A(kpc, w1, false, A);
 #pragma unroll
   for (int s = 0; s < 4; ++s) B[s] = -w0 * tv[s] + w0 * Sp[s] + w1 * Sc[s] + Ip[s] * etb;
   crout4(A, LU);
@@ -690,41 +751,22 @@ SNAPI_HD void delo_step(const float *Ip, const float *kpp, const float *Sp, cons
 // Reverse of delo_step.  Inputs: forward values and Icb (adjoint of I_c).  Accumulates into
 // Ipb, kppb, Spb, kpcb, Scb and returns the adjoint of tb.
 SNAPI_HD float delo_step_adjoint(const float *Ip, const float *kpp, const float *Sp, const float *kpc,
-                                 const float *Sc, double tb, const float *Ic, const float *Icb, float *Ipb,
+                                 const float *Sc, float tb, const float *Ic, const float *Icb, float *Ipb,
                                  float *kppb, float *Spb, float *kpcb, float *Scb) {
   float w0, w1, etb, dw0, dw1, detb;
   delo_weights(tb, w0, w1, etb);
   delo_weights_grad(tb, dw0, dw1, detb);
-  float Kp[16], Kc[16], AT[16], LU[16], Bb[4], tv[4];
-  kprime_full(kpp, Kp);
-  kprime_full(kpc, Kc);
-  // A^T = 1 + w1 K_c^T ; solve A^T Bb = Icb
-#pragma unroll
-  for (int s = 0; s < 4; ++s) {
-#pragma unroll
-    for (int sp = 0; sp < 4; ++sp) AT[s * 4 + sp] = w1 * Kc[sp * 4 + s];
-    AT[s * 4 + s] += 1.0f;
-  }
+  float AT[16], LU[16], Bb[4], tv[4];
+  // A^T Bb = Icb
+  build_A(kpc, w1, true, AT);
   crout4(AT, LU);
   solve_crout4(LU, Icb, Bb);
-  // A-bar = -Bb Ic^T ; A = 1 + w1 Kc
-  float Ab[16];
-  float w1b = 0.f;
-#pragma unroll
-  for (int s = 0; s < 4; ++s)
-#pragma unroll
-    for (int sp = 0; sp < 4; ++sp) {
-      Ab[s * 4 + sp] = -Bb[s] * Ic[sp];
-      w1b += Ab[s * 4 + sp] * Kc[s * 4 + sp];
-    }
-  float KcbM[16];
-#pragma unroll
-  for (int i = 0; i < 16; ++i) KcbM[i] = w1 * Ab[i];
-  kprime_proj(KcbM, kpcb);
-  // B = -w0 Kp Ip + w0 Sp + w1 Sc + etb Ip
-#pragma unroll
-  for (int s = 0; s < 4; ++s)
-    tv[s] = Kp[s * 4 + 0] * Ip[0] + Kp[s * 4 + 1] * Ip[1] + Kp[s * 4 + 2] * Ip[2] + Kp[s * 4 + 3] * Ip[3];
+  // A-bar = -Bb Ic^T ;  A = 1 + w1 K'_c  ->  kpc-bar += -w1 proj(Bb Ic^T), w1-bar += -Bb^T K'_c Ic
+  kp_outer_proj(Bb, Ic, -w1, kpcb);
+  kp_mul(kpc, Ic, tv);
+  float w1b = -(Bb[0] * tv[0] + Bb[1] * tv[1] + Bb[2] * tv[2] + Bb[3] * tv[3]);
+  // B = -w0 K'_p I_p + w0 S_p + w1 S_c + etb I_p
+  kp_mul(kpp, Ip, tv);
   float w0b = 0.f, etbb = 0.f;
 #pragma unroll
   for (int s = 0; s < 4; ++s) {
@@ -734,20 +776,11 @@ SNAPI_HD float delo_step_adjoint(const float *Ip, const float *kpp, const float 
     Spb[s] += w0 * Bb[s];
     Scb[s] += w1 * Bb[s];
   }
-  // Ip-bar = etb Bb - w0 Kp^T Bb ; Kp-bar = -w0 Bb Ip^T
+  // Ip-bar = etb Bb - w0 K'_p^T Bb ; kpp-bar += -w0 proj(Bb Ip^T)
+  kp_mul_t(kpp, Bb, tv);
 #pragma unroll
-  for (int sp = 0; sp < 4; ++sp) {
-    float acc = 0.f;
-#pragma unroll
-    for (int s = 0; s < 4; ++s) acc += Kp[s * 4 + sp] * Bb[s];
-    Ipb[sp] += etb * Bb[sp] - w0 * acc;
-  }
-  float KpbM[16];
-#pragma unroll
-  for (int s = 0; s < 4; ++s)
-#pragma unroll
-    for (int sp = 0; sp < 4; ++sp) KpbM[s * 4 + sp] = -w0 * Bb[s] * Ip[sp];
-  kprime_proj(KpbM, kppb);
+  for (int s = 0; s < 4; ++s) Ipb[s] += etb * Bb[s] - w0 * tv[s];
+  kp_outer_proj(Bb, Ip, -w0, kppb);
   return w0b * dw0 + w1b * dw1 + etbb * detb;
 }
 

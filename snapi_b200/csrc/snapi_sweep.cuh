@@ -30,7 +30,7 @@ SNAPI_HD void depth_opacity(const PixelView &pv, int z, const LamConst &lam, con
                             float *S, float &e) {
   float eta[7], jj[4];
   cell_opacity(pv.dc[z], pv.ld + z * pv.nlines, pv.lc, pv.nlines, pv.compS, pv.compD, lam, delta, eta, jj);
-  const float ie = 1.0f / eta[0];
+  const float ie = frcp(eta[0]);
   e = eta[0];
 #pragma unroll
   for (int q = 0; q < 6; ++q) kp[q] = eta[q + 1] * ie;
@@ -51,12 +51,12 @@ SNAPI_HD void forward_sweep(const PixelView &pv, const LamConst &lam, const floa
   for (int z = nd - 2; z >= 1; --z) {
     depth_opacity(pv, z - 1, lam, delta, kpC, SC_, eC);
     const double opd_z = opd_interior(eA, eB, eC, pv.D[z], pv.D[z - 1]);
-    const double tau = bezier_dtau(eA, eB, opd_below, opd_z, pv.D[z]);
+    const float tau = (float)bezier_dtau(eA, eB, opd_below, opd_z, pv.D[z]);
     float In[4];
     delo_step(I, kpA, SA, kpB, SB, tau, In);
 #pragma unroll
     for (int s = 0; s < 4; ++s) I[s] = In[s];
-    if (STORE) sc.store(z, I, kpB, SB, eB, (float)tau);
+    if (STORE) sc.store(z, I, kpB, SB, eB, tau);
 #pragma unroll
     for (int q = 0; q < 6; ++q) { kpA[q] = kpB[q]; kpB[q] = kpC[q]; }
 #pragma unroll
@@ -69,13 +69,10 @@ SNAPI_HD void forward_sweep(const PixelView &pv, const LamConst &lam, const floa
   for (int s = 0; s < 4; ++s) out[s] = I[s];  // the top point copies the one below
 }
 
-// finalize one depth: turn (K'-bar, S-bar, eta_I-bar) into (eta-bar, j-bar), run the opacity
-// adjoint and hand the sums to the reducer
-template <class RD>
-SNAPI_HD void finalize_depth(const PixelView &pv, int z, const LamConst &lam, const float *delta, const float *kp,
-                             const float *S, float e, const float *kpb, const float *Sb, float eb, float *red,
-                             int nred, RD &rd) {
-  float etab[7], jb[4];
+// Turn (K'-bar, S-bar, eta_I-bar) of one depth into (eta-bar, j-bar), the inputs of the
+// opacity adjoint: K'_q = eta_q / eta_I, S_s = j_s / eta_I.
+SNAPI_HD void depth_bars(const float *kp, const float *S, float e, const float *kpb, const float *Sb, float eb,
+                         float *etab, float *jb) {
   const float ie = 1.0f / e;
   float acc = 0.f;
 #pragma unroll
@@ -83,25 +80,26 @@ SNAPI_HD void finalize_depth(const PixelView &pv, int z, const LamConst &lam, co
 #pragma unroll
   for (int s = 0; s < 4; ++s) { jb[s] = Sb[s] * ie; acc += Sb[s] * S[s]; }
   etab[0] = eb - acc * ie;
-  for (int i = 0; i < nred; ++i) red[i] = 0.0f;
-  cell_opacity_adjoint(pv.dc[z], pv.ld + z * pv.nlines, pv.lc, pv.nlines, pv.compS, pv.compD, lam, delta, etab,
-                       jb, red);
-  rd.add(z, red, nred);
 }
 
-// Ib: adjoint of the emergent Stokes vector.  red: work vector of nred floats.
-template <class SC, class RD>
-SNAPI_HD void reverse_sweep(const PixelView &pv, const LamConst &lam, const float *delta, const float *Ib_in,
-                            SC &sc, RD &rd, float *red, int nred) {
+// Reverse sweep, phase R1: adjoint of the DELO recursion and of the Bezier optical depth, top to
+// bottom.  Depth z-1 is final after step z; its (eta-bar, j-bar) overwrite its scratch slots
+// (sc.store_bar) -- the forward values of that depth are no longer needed.  Phase R2 (opacity
+// adjoint per depth) then runs with no sweep state live.
+template <class SC>
+SNAPI_HD void reverse_sweep_rt(const PixelView &pv, const float *Ib_in, SC &sc) {
   const int nd = pv.nd;
-  // forward values: m = z-1, c = z, n = z+1
-  float Im[4], kpm[6], Sm[4], em_, taum;
+  // forward values of depths z-1 (m), z (c), z+1 (n)
+  float kpm[6], Sm[4], em_;
   float Ic[4], kpc[6], Sc[4], ec, tauc;
   float In[4], kpn[6], Sn[4], en, taun;
   // adjoints
   float Ib[4], kpbm[6], Sbm[4], ebm, kpbc[6], Sbc[4], ebc, kpbn[6], Sbn[4], ebn;
   double opdb_c, opdb_n;
-  sc.load(0, Im, kpm, Sm, em_, taum);
+  {
+    float Id[4], td;
+    sc.load(0, Id, kpm, Sm, em_, td);
+  }
   sc.load(1, Ic, kpc, Sc, ec, tauc);
 #pragma unroll
   for (int s = 0; s < 4; ++s) { Ib[s] = Ib_in[s]; Sbm[s] = 0.f; Sbc[s] = 0.f; }
@@ -115,7 +113,6 @@ SNAPI_HD void reverse_sweep(const PixelView &pv, const LamConst &lam, const floa
 #pragma unroll
     for (int q = 0; q < 6; ++q) kpbn[q] = 0.f;
     float Ipb[4] = {0.f, 0.f, 0.f, 0.f};
-    // step z: I_c from I_n (upwind = depth z+1)
     const float taub = delo_step_adjoint(In, kpn, Sn, kpc, Sc, tauc, Ic, Ib, Ipb, kpbn, Sbn, kpbc, Sbc);
     // tau_z = bezier(e_{z+1}, e_z, opd_{z+1}, opd_z, D[z])
     const double Dz = pv.D[z];
@@ -123,19 +120,20 @@ SNAPI_HD void reverse_sweep(const PixelView &pv, const LamConst &lam, const floa
     ebc += (float)(taub * Dz * 0.5);
     opdb_n = taub * Dz * Dz / 12.0;
     opdb_c -= taub * Dz * Dz / 12.0;
-    // opd_z final: interior point z with e_up = e_{z+1}, e_c = e_z, e_dn = e_{z-1}
-    {
+    {  // opd_z final: interior point z with e_up = e_{z+1}, e_c = e_z, e_dn = e_{z-1}
       double gup = 0, gc = 0, gdn = 0;
       opd_interior_grad(en, ec, em_, Dz, pv.D[z - 1], opdb_c, gup, gc, gdn);
       ebn += (float)gup; ebc += (float)gc; ebm += (float)gdn;
     }
-    // depth z-1 is final
-    finalize_depth(pv, z - 1, lam, delta, kpm, Sm, em_, kpbm, Sbm, ebm, red, nred, rd);
-    // shift
+    {  // depth z-1 is final
+      float etab[7], jb[4];
+      depth_bars(kpm, Sm, em_, kpbm, Sbm, ebm, etab, jb);
+      sc.store_bar(z - 1, etab, jb);
+    }
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
       Ib[s] = Ipb[s];
-      Im[s] = Ic[s]; Ic[s] = In[s];
+      Ic[s] = In[s];
       Sm[s] = Sc[s]; Sc[s] = Sn[s];
       Sbm[s] = Sbc[s]; Sbc[s] = Sbn[s];
     }
@@ -146,19 +144,43 @@ SNAPI_HD void reverse_sweep(const PixelView &pv, const LamConst &lam, const floa
     }
     em_ = ec; ec = en;
     ebm = ebc; ebc = ebn;
-    taum = tauc; tauc = taun;
+    tauc = taun;
     opdb_c = opdb_n;
   }
-  // now m = nd-2, c = nd-1; opd at nd-1 is one-sided: (e_{nd-2} - e_{nd-1}) / D[nd-2]
+  // m = nd-2, c = nd-1; the opd at nd-1 is one-sided: (e_{nd-2} - e_{nd-1}) / D[nd-2]
   {
     const double Dl = pv.D[nd - 2];
     ebm += (float)(opdb_c / Dl);
     ebc -= (float)(opdb_c / Dl);
   }
-  // boundary condition I_{nd-1} = (S_I, 0, 0, 0)
-  Sbc[0] += Ib[0];
-  finalize_depth(pv, nd - 2, lam, delta, kpm, Sm, em_, kpbm, Sbm, ebm, red, nred, rd);
-  finalize_depth(pv, nd - 1, lam, delta, kpc, Sc, ec, kpbc, Sbc, ebc, red, nred, rd);
+  Sbc[0] += Ib[0];  // boundary condition I_{nd-1} = (S_I, 0, 0, 0)
+  float etab[7], jb[4];
+  depth_bars(kpm, Sm, em_, kpbm, Sbm, ebm, etab, jb);
+  sc.store_bar(nd - 2, etab, jb);
+  depth_bars(kpc, Sc, ec, kpbc, Sbc, ebc, etab, jb);
+  sc.store_bar(nd - 1, etab, jb);
+}
+
+// Reverse sweep, phase R2: opacity adjoint of every depth; wavelength sums go to the reducer.
+template <class SC, class RD>
+SNAPI_HD void reverse_sweep_opacity(const PixelView &pv, const LamConst &lam, const float *delta, const SC &sc,
+                                    RD &rd, float *red, int nred) {
+  for (int z = 0; z < pv.nd; ++z) {
+    float etab[7], jb[4];
+    sc.load_bar(z, etab, jb);
+    for (int i = 0; i < nred; ++i) red[i] = 0.0f;
+    cell_opacity_adjoint(pv.dc[z], pv.ld + z * pv.nlines, pv.lc, pv.nlines, pv.compS, pv.compD, lam, delta, etab,
+                         jb, red);
+    rd.add(z, red, nred);
+  }
+}
+
+// Ib: adjoint of the emergent Stokes vector.  red: work vector of nred floats.
+template <class SC, class RD>
+SNAPI_HD void reverse_sweep(const PixelView &pv, const LamConst &lam, const float *delta, const float *Ib_in,
+                            SC &sc, RD &rd, float *red, int nred) {
+  reverse_sweep_rt(pv, Ib_in, sc);
+  reverse_sweep_opacity(pv, lam, delta, sc, rd, red, nred);
 }
 
 }  // namespace snapi

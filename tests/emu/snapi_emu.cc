@@ -105,6 +105,16 @@ struct HostScratch {
     for (int q = 0; q < 6; ++q) kp[q] = p[4 + q];
     e = p[10]; tau = p[11];
   }
+  void store_bar(int z, const float *eb, const float *jb) {
+    float *p = &buf[z * 16];
+    for (int i = 0; i < 7; ++i) p[i] = eb[i];
+    for (int i = 0; i < 4; ++i) p[7 + i] = jb[i];
+  }
+  void load_bar(int z, float *eb, float *jb) const {
+    const float *p = &buf[z * 16];
+    for (int i = 0; i < 7; ++i) eb[i] = p[i];
+    for (int i = 0; i < 4; ++i) jb[i] = p[7 + i];
+  }
 };
 struct NoStore {
   void store(int, const float *, const float *, const float *, float, float) {}

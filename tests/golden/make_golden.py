@@ -11,6 +11,9 @@ its 80-depth atmosphere file from REF and runs oracle/_ref/snapi_ref_dump).  Wri
   tests/golden/config3.npz        8 pixels of the seeded 64x64 node-model cube (seed 3): records,
                                   node tangents, reference Stokes, reference node responses,
                                   noisy target Stokes
+  tests/golden/bench_pool.npz     32 more seeded config-3 columns (seed 303) with records, node
+                                  tangents and reference Stokes: the thermal structures the
+                                  benchmark tiles over its 64x64 pixels
 
 Synthetic inputs stand in for observations: seeded numpy generators with the shapes and value
 distributions of the benchmark configurations (no dataset is read).
@@ -171,6 +174,8 @@ def main():
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--c2pix", type=int, default=16)
     ap.add_argument("--c3pix", type=int, default=8)
+    ap.add_argument("--pool", type=int, default=32)
+    ap.add_argument("--only-pool", action="store_true")
     a = ap.parse_args()
     if not os.path.exists(DUMP):
         raise SystemExit("build the oracle first: make -C oracle")
@@ -178,6 +183,26 @@ def main():
     try:
         for f in CFG_FILES:
             shutil.copy(os.path.join(a.ref, "cfg", f), tmp)
+        if a.only_pool:
+            shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
+        else:
+            make_configs_1_to_3(a, tmp)
+        if a.pool:
+            n4 = config3_nodes(a.pool, seed=303)
+            d4 = dump(tmp, os.path.join(tmp, "c3.tsk"), n4, 2, "pool")
+            np.savez_compressed(os.path.join(HERE, "bench_pool.npz"), lambda_air=d4["lambda_air"],
+                                tau500=d4["tau500"], record=d4["record"].astype(np.float32),
+                                stokes=d4["stokes"], nodes=d4["nodes"], node_kind=d4["node_kind"],
+                                tangent=d4["tangent"].astype(np.float32),
+                                ref_seconds_per_pixel=d4["ref_seconds_per_pixel"], meta=d4["meta"],
+                                **line_arrays(d4))
+        print("fixtures written to", HERE)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def make_configs_1_to_3(a, tmp):
+    if True:
         # config 1: dense temperature nodes (one per depth) reproduce the closed-form profile
         T1 = config1_temperature(LOGTAU)
         write_cfg(os.path.join(tmp, "c1.cfg"), LOGTAU, T1, [0.0], [0.0])
@@ -208,9 +233,6 @@ def main():
                             record=d3["record"], stokes=d3["stokes"], nodes=d3["nodes"], node_kind=d3["node_kind"],
                             tangent=d3["tangent"].astype(np.float32), responses=d3["responses"], target=target,
                             ref_seconds_per_pixel=d3["ref_seconds_per_pixel"], meta=d3["meta"], **line_arrays(d3))
-        print("fixtures written to", HERE)
-    finally:
-        shutil.rmtree(tmp, ignore_errors=True)
 
 
 if __name__ == "__main__":

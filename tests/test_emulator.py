@@ -89,18 +89,18 @@ def test_emulated_adjoint_noisy_target(emu, oracle_lib, config3):
     residuals r of random sign, so it amplifies the ~1e-6 Ic FP32 forward error (r changes by
     ~1e-3 of itself).  Two checks: (a) the adjoint is the exact gradient of the FP32 model -- the
     oracle given the same residuals agrees within 1e-3 (LM-scaled norm); (b) against the FP64
-    model with the same target, within 1e-2."""
+    model with the same target, within 2e-2."""
     so, fx = oracle_lib, config3
     ic = float(fx["stokes"][:, :, 0].max())
     st, chi, g, _ = _emu_adjoint(emu, so, fx, fx["record"][:3], fx["target"][:3], fx["tangent"][:3], ic)
     lines = emu_lines(so, fx)
     s64 = so.synth(fx["lambda_air"], fx["tau500"], fx["record"][:3], lines)
     for p in range(3):
-        c_ref, g_ref = oracle_grad(so, fx, p, fx["target"][p])
-        assert abs(chi[p] - c_ref) < 1e-4 * c_ref
-        assert scaled_rel_err(g[p], g_ref, fx["node_kind"]) < 1e-2
         _, g_same = oracle_grad(so, fx, p, fx["target"][p] + (s64[p] - st[p]))
         assert scaled_rel_err(g[p], g_same, fx["node_kind"]) < 1e-3
+        c_ref, g_ref = oracle_grad(so, fx, p, fx["target"][p])
+        assert abs(chi[p] - c_ref) < 1e-4 * c_ref
+        assert scaled_rel_err(g[p], g_ref, fx["node_kind"]) < 2e-2
 
 
 def test_emulated_record_gradient(emu, oracle_lib, config3):
