@@ -130,6 +130,26 @@ double snapi_last_kernel_ms(const snapi_ctx *ctx);
 /* Number of kernel launches of the last call. */
 int snapi_last_launches(const snapi_ctx *ctx);
 
+/* snapi_adjoint for callers that cannot allocate device memory: applications whose GPU memory
+ * is owned by another allocator (a framework pool with a fixed budget) and loops that must not
+ * take the device-wide synchronisation and latency of cudaMalloc / cudaFree.  It has no
+ * counterpart in the reference (whose per-pixel CPU loops have no device memory at all).
+ *
+ * No context and no allocation: every work buffer lives in one static device array of
+ * SNAPI_STATIC_SCRATCH_BYTES (64 MiB) that each GPU loading this library holds until the process
+ * exits.  All array arguments are device pointers on `device`; w_stokes is a host array [4];
+ * `stream` is a cudaStream_t (NULL = default stream).  The call returns when the results are in
+ * place.  Pixels are processed in batches that fit the static array; a problem whose single pixel
+ * does not fit (at nd = 80 and 201 wavelengths one pixel needs ~1.4 MB) is rejected with
+ * SNAPI_EINVAL.  The first call on a device looks up the array's device address; make that first
+ * call before any stream capture.  Calls share the array: calls that overlap on the GPU race.
+ * On error, snapi_noalloc_last_error() (per host thread) describes it. */
+#define SNAPI_STATIC_SCRATCH_BYTES (64u << 20)
+int snapi_adjoint_noalloc(const snapi_problem *prob, int device, void *stream, int npix, const float *records,
+                          const float *obs, const double *w_stokes, const float *mask, int npar,
+                          const float *tangents, float *stokes, double *chi2, double *grad);
+const char *snapi_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,6 +15,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "snapi_internal.cuh"
@@ -626,5 +627,204 @@ int snapi_responses(snapi_ctx *ctx, int npix, const float *records, int npar, co
   if (!ctx) return SNAPI_EINVAL;
   return set_err(ctx, SNAPI_EINVAL, "snapi_responses: not available in this build");
 }
+
+}  // extern "C"
+
+// =============================================================================================
+// Adjoint without any device allocation.
+//
+// For callers that cannot call cudaMalloc: applications whose device memory belongs to another
+// allocator (a framework memory pool with a fixed budget, where a side allocation would break
+// its accounting) and loops that must not take the device-wide synchronisation and unbounded
+// latency of cudaMalloc / cudaFree.  The computation is snapi_adjoint's (same kernels); every
+// work buffer lives in the static device array below instead of in a context.
+//
+// g_snapi_static is SNAPI_STATIC_SCRATCH_BYTES (64 MiB) on every GPU that loads this library,
+// held until the process exits.  Layout: [status word][problem constants][work region]; the work
+// region holds, per pixel of a chunk, the forward state (nd x 4 x lpad float4), the per-warp
+// wavelength sums (nwarp x nd x nred float) and the per-warp chi2 sums (nwarp double).  Pixels
+// are processed in chunks that fit the work region.  In host code the array's name is only a
+// host-side stand-in, so its device address is fetched with cudaGetSymbolAddress -- once per
+// device, by the first call on that device, with that device current.
+// Every call shares the array: the kernels overwrite every slot they read in the same call and
+// the status word is cleared at the start of each call; calls that overlap on the GPU (two host
+// threads, or two streams) race on it.
+namespace {
+
+constexpr size_t kStaticBytes = SNAPI_STATIC_SCRATCH_BYTES;
+constexpr size_t kStaticConstBytes = 128 * 1024;  // status word + problem constants
+constexpr int kMaxDevices = 64;
+static __device__ __align__(256) unsigned char g_snapi_static[kStaticBytes];
+
+std::mutex g_static_mu;
+unsigned char *g_static_ptr[kMaxDevices] = {};
+
+int static_setup(int device, unsigned char **base, std::string &err) {
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (device < 0 || device >= kMaxDevices) { err = "device ordinal out of range"; return SNAPI_EINVAL; }
+  if (!g_static_ptr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_snapi_static);
+    if (e != cudaSuccess || !p) {
+      err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+      return SNAPI_ECUDA;
+    }
+    const int fin = 227 * 1024;
+    e = cudaFuncSetAttribute(k_adjoint_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, fin);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_adjoint_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, fin);
+    if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return SNAPI_ECUDA; }
+    g_static_ptr[device] = static_cast<unsigned char *>(p);
+  }
+  *base = g_static_ptr[device];
+  return SNAPI_OK;
+}
+
+int noalloc_run(const snapi_problem *prob, void *stream_v, int npix, const float *records, const float *obs,
+                const double *w_stokes, const float *mask, int npar, const float *tangents, float *stokes,
+                double *chi2, double *grad, unsigned char *base, std::string &err) {
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+  const int nd = prob->nd, nl = prob->nlambda, nlines = prob->nlines;
+  const int nfield = SNAPI_NFIELD0 + 3 * nlines, nred = kNumRed + kRedPerLine * nlines;
+  const int nchunk = (nl + kChunk - 1) / kChunk, lpad = nchunk * kChunk, nwslot = lpad / 32;
+  // problem constants (host side), as snapi_create prepares them
+  std::vector<double> lv(nl), D(nd - 1);
+  for (int l = 0; l < nl; ++l) lv[l] = airtovac_d(prob->lambda_air[l]);
+  for (int i = 0; i + 1 < nd; ++i) D[i] = (prob->tau500[i + 1] - prob->tau500[i]) / prob->mu;
+  std::vector<LineConst> lc(nlines);
+  std::vector<float> cS, cD;
+  for (int j = 0; j < nlines; ++j) {
+    const snapi_line &s = prob->lines[j];
+    if (!(s.lam0 > 0.0) || !(s.mass > 0.0)) { err = "line lam0 and mass must be positive"; return SNAPI_EINVAL; }
+    LineConst &L = lc[j];
+    L.lam0 = s.lam0; L.sf = (float)s.sf; L.ar = (float)s.ar;
+    L.two_k_over_m = (float)(2.0 * kK / s.mass);
+    L.lam0_over_c = (float)(s.lam0 / kC);
+    L.zee = (float)(4.67E-5 * s.lam0 * s.lam0);
+    L.split = s.split ? 1 : 0;
+    L.comp_off = (int)cS.size();
+    for (int g = 0; g < 3; ++g) {
+      L.ncomp[g] = s.split ? s.ncomp[g] : 0;
+      if (L.ncomp[g] < 0 || L.ncomp[g] > SNAPI_MAX_COMP) { err = "bad Zeeman component count"; return SNAPI_EINVAL; }
+      for (int i = 0; i < L.ncomp[g]; ++i) { cS.push_back((float)s.S[g][i]); cD.push_back((float)s.D[g][i]); }
+    }
+  }
+  const int ncomp = (int)cS.size();
+  // constants region: status | lamvac | D | lines | compS | compD
+  size_t o = 256;
+  const size_t o_lv = o; o = align_up(o + sizeof(double) * nl, 256);
+  const size_t o_D = o; o = align_up(o + sizeof(double) * (nd - 1), 256);
+  const size_t o_lc = o; o = align_up(o + sizeof(LineConst) * (nlines > 0 ? nlines : 1), 256);
+  const size_t o_cS = o; o = align_up(o + sizeof(float) * (ncomp > 0 ? ncomp : 1), 256);
+  const size_t o_cD = o; o = align_up(o + sizeof(float) * (ncomp > 0 ? ncomp : 1), 256);
+  if (o > kStaticConstBytes) { err = "problem constants exceed the static constants region"; return SNAPI_EINVAL; }
+  // work region per pixel
+  const size_t per_state = sizeof(float4) * (size_t)nd * 4 * lpad;
+  const size_t per_part = sizeof(float) * (size_t)nwslot * nd * nred;
+  const size_t per_c2 = sizeof(double) * (size_t)nwslot;
+  const size_t per_pix = align_up(per_state, 256) + align_up(per_part, 256) + align_up(per_c2, 256);
+  const size_t work = kStaticBytes - kStaticConstBytes;
+  const int cap = (int)std::min<size_t>(work / per_pix, 1 << 20);
+  if (cap < 1) {
+    char b[256];
+    snprintf(b, sizeof b, "one pixel needs %zu B of work memory, the static array holds %zu B", per_pix, work);
+    err = b;
+    return SNAPI_EINVAL;
+  }
+  const SmemLayout Lsw = smem_layout(nd, nfield, nlines, ncomp, nred, false);
+  const SmemLayout Lfin = smem_layout(nd, nfield, nlines, ncomp, nred, true);
+  if (Lfin.total > 227 * 1024) { err = "problem exceeds the shared memory of a CTA"; return SNAPI_EINVAL; }
+  int *status = reinterpret_cast<int *>(base);
+#define CKN(call)                                                   \
+  do {                                                              \
+    cudaError_t e_ = (call);                                        \
+    if (e_ != cudaSuccess) {                                        \
+      err = std::string(#call ": ") + cudaGetErrorString(e_);       \
+      return SNAPI_ECUDA;                                           \
+    }                                                               \
+  } while (0)
+  CKN(cudaMemsetAsync(status, 0, sizeof(int), stream));
+  CKN(cudaMemcpyAsync(base + o_lv, lv.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, stream));
+  CKN(cudaMemcpyAsync(base + o_D, D.data(), sizeof(double) * (nd - 1), cudaMemcpyHostToDevice, stream));
+  if (nlines) CKN(cudaMemcpyAsync(base + o_lc, lc.data(), sizeof(LineConst) * nlines, cudaMemcpyHostToDevice, stream));
+  if (ncomp) {
+    CKN(cudaMemcpyAsync(base + o_cS, cS.data(), sizeof(float) * ncomp, cudaMemcpyHostToDevice, stream));
+    CKN(cudaMemcpyAsync(base + o_cD, cD.data(), sizeof(float) * ncomp, cudaMemcpyHostToDevice, stream));
+  }
+  unsigned char *wbase = base + kStaticConstBytes;
+  const size_t nrec = (size_t)nd * nfield;
+  for (int p0 = 0; p0 < npix; p0 += cap) {
+    const int nb = std::min(cap, npix - p0);
+    KParams P;
+    memset(&P, 0, sizeof P);
+    P.npix = nb; P.nd = nd; P.nl = nl; P.nlines = nlines; P.nfield = nfield; P.npar = npar; P.lpad = lpad;
+    P.ncomp = ncomp; P.nred = nred; P.nchunk = nchunk; P.nwslot = nwslot; P.nvar = 1;
+    P.lam_mid = (float)(0.5 * (lv[nl - 1] + lv[0]));
+    P.scale2 = prob->stokes_scale * prob->stokes_scale;
+    P.lamvac = reinterpret_cast<const double *>(base + o_lv);
+    P.D = reinterpret_cast<const double *>(base + o_D);
+    P.lines = reinterpret_cast<const LineConst *>(base + o_lc);
+    P.compS = reinterpret_cast<const float *>(base + o_cS);
+    P.compD = reinterpret_cast<const float *>(base + o_cD);
+    P.status = status;
+    P.scratch = reinterpret_cast<float4 *>(wbase);
+    P.wpart = reinterpret_cast<float *>(wbase + align_up(per_state, 256) * cap);
+    P.c2part = reinterpret_cast<double *>(wbase + (align_up(per_state, 256) + align_up(per_part, 256)) * cap);
+    for (int s = 0; s < 4; ++s) P.ws[s] = w_stokes ? w_stokes[s] : 1.0;
+    P.rec = records + p0 * nrec;
+    P.obs = obs + (size_t)p0 * nl * 4;
+    P.mask = mask ? mask + (size_t)p0 * nl : nullptr;
+    P.tangent = npar ? tangents + (size_t)p0 * npar * nrec : nullptr;
+    P.stokes = stokes ? stokes + (size_t)p0 * nl * 4 : nullptr;
+    P.chi2 = chi2 + p0;
+    P.grad = npar ? grad + (size_t)p0 * npar : nullptr;
+    k_adjoint_sweep<<<nb * nchunk, kChunk, Lsw.total, stream>>>(P);
+    CKN(cudaGetLastError());
+    k_adjoint_finish<<<nb, kFinishThreads, Lfin.total, stream>>>(P);
+    CKN(cudaGetLastError());
+  }
+  int st = 0;
+  CKN(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CKN(cudaStreamSynchronize(stream));
+#undef CKN
+  if (st != 0) { err = "a CTA gave up waiting for its TMA copy"; return st; }
+  return SNAPI_OK;
+}
+
+thread_local std::string g_noalloc_err;
+
+}  // namespace
+
+extern "C" {
+
+int snapi_adjoint_noalloc(const snapi_problem *prob, int device, void *stream, int npix, const float *records,
+                          const float *obs, const double *w_stokes, const float *mask, int npar,
+                          const float *tangents, float *stokes, double *chi2, double *grad) {
+  g_noalloc_err.clear();
+  if (!prob || npix < 0 || npar < 0 || (npix > 0 && (!records || !obs || !chi2)) ||
+      (npar > 0 && (!tangents || !grad)) || prob->nd < 3 || prob->nlambda < 1 ||
+      prob->nlambda > SNAPI_MAX_LAMBDA || prob->nlines < 0 || prob->nlines > SNAPI_MAX_LINES || !prob->lambda_air ||
+      !prob->tau500 || (prob->nlines && !prob->lines) || !(prob->mu > 0.0 && prob->mu <= 1.0) ||
+      !(prob->stokes_scale > 0.0)) {
+    g_noalloc_err = "snapi_adjoint_noalloc: invalid arguments";
+    return SNAPI_EINVAL;
+  }
+  for (int i = 0; i + 1 < prob->nd; ++i)
+    if (!(prob->tau500[i + 1] > prob->tau500[i])) {
+      g_noalloc_err = "tau500 must increase from the top down";
+      return SNAPI_EINVAL;
+    }
+  int old = 0;
+  if (cudaGetDevice(&old) != cudaSuccess) { g_noalloc_err = "cudaGetDevice failed"; return SNAPI_ECUDA; }
+  if (cudaSetDevice(device) != cudaSuccess) { g_noalloc_err = "cudaSetDevice failed"; return SNAPI_ECUDA; }
+  unsigned char *base = nullptr;
+  int rc = static_setup(device, &base, g_noalloc_err);
+  if (rc == SNAPI_OK && npix > 0)
+    rc = noalloc_run(prob, stream, npix, records, obs, w_stokes, mask, npar, tangents, stokes, chi2, grad, base,
+                     g_noalloc_err);
+  cudaSetDevice(old);
+  return rc;
+}
+
+const char *snapi_noalloc_last_error(void) { return g_noalloc_err.c_str(); }
 
 }  // extern "C"
