@@ -158,6 +158,7 @@ def run_snapi(args):
     dev = torch.device("cuda", local)
     b.build_cuda()
     pool = dict(np.load(POOL))
+    NPIX = args.pixels
     truth, model, tan = make_workload(pool, NPIX, seed=3 + 1000 * rank)
     ic = float(pool["stokes"][:, :, 0].max())
     npar = tan.shape[1]
@@ -242,7 +243,8 @@ def run_snapi(args):
 
     line = None
     if rank == 0:
-        kern_per_launch_ms = kern_ms / max(launches, 1)
+        # one call = k_adjoint_sweep (>99 % of the device time) + k_adjoint_finish, timed together
+        kern_per_launch_ms = kern_ms / args.steps
         # algorithmic bytes per pixel: record + tangents + target in, Stokes + grad + chi2 out
         nd = model.shape[1]
         nf = model.shape[2]
@@ -262,7 +264,8 @@ def run_snapi(args):
             "vs_baseline": None,
             "dtype": "f32 (profiles, formal solver); f64 (optical depth, DELO weights, W4 core derivative)",
             "data": "synthetic: reference-built columns (HE + chemistry) x seeded per-pixel field/velocity nodes",
-            "config": {"workload": "64x64 pixels x 80 depths x 201 wavelengths, Fe I 6301.5/6302.5, mu=1, "
+            "config": {"workload": ("64x64" if NPIX == 64 * 64 else str(NPIX)) +
+                                   " pixels x 80 depths x 201 wavelengths, Fe I 6301.5/6302.5, mu=1, "
                                    "10 nodes (T x4, vturb, vlos x2, B, incl, azi): synthesis + chi2 + adjoint "
                                    "d chi2/d nodes", "pixels_per_gpu": NPIX, "nd": int(nd), "nlambda": int(nl),
                        "npar": int(npar), "l2_flush": "inputs ~0.4 GB per step exceed the 126 MB L2",
@@ -377,6 +380,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="snapi", choices=["snapi", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pixels", type=int, default=NPIX, help="pixels per GPU (smaller cases for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

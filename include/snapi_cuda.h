@@ -104,10 +104,13 @@ int snapi_adjoint(snapi_ctx *ctx, int npix, const float *records, const float *o
                   const float *mask, int npar, const float *tangents, float *stokes, double *chi2,
                   double *grad, double *rec_grad, int mem);
 
-/* Node responses (forward mode): dstokes [npix][npar][nlambda][4] = d Stokes / d node, the
- * quantity obs_stokes_responses_to_nodes returns; stokes may be NULL. */
+/* Node responses dstokes [npix][npar][nlambda][4] = d Stokes / d node, the quantity
+ * obs_stokes_responses_to_nodes returns (atmos_fit.cc:1205-1352), by central differences of the
+ * record along each node tangent: (S(rec + h_p t_p) - S(rec - h_p t_p)) / 2 h_p, step [npar] in
+ * node units (2 npar forward solves; FP32, ~1e-3 relative with steps ~1e-3 of the node scale).
+ * stokes (the unperturbed synthesis) may be NULL. */
 int snapi_responses(snapi_ctx *ctx, int npix, const float *records, int npar, const float *tangents,
-                    float *stokes, float *dstokes, int mem);
+                    const double *step, float *stokes, float *dstokes, int mem);
 
 /* Plain finite-difference gradient (the baseline the adjoint replaces): for each node p the
  * records are perturbed by +-step[p] * tangent_p and synthesised again (2 npar + 1 solves).

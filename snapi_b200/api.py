@@ -80,7 +80,7 @@ def lib():
         L.snapi_last_error.argtypes = [vp]
         L.snapi_synth.argtypes = [vp, ip, fp, fp, ip]
         L.snapi_adjoint.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, fp, ip]
-        L.snapi_responses.argtypes = [vp, ip, fp, ip, fp, fp, fp, ip]
+        L.snapi_responses.argtypes = [vp, ip, fp, ip, fp, fp, fp, fp, ip]
         L.snapi_fd_grad.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, ip]
         L.snapi_zeeman_pattern.argtypes = [ip, ip, ctypes.c_double, ctypes.c_double, ctypes.POINTER(SnapiLine)]
         L.snapi_host_alloc.restype = vp
@@ -246,15 +246,18 @@ class Context:
                                         _ptr(stp), _ptr(chi2), _ptr(grad), MEM_HOST))
         return {"chi2": chi2, "grad": grad}
 
-    def responses(self, records, tangents, want_stokes=True):
-        """d Stokes / d node [npix, npar, nlambda, 4] (obs_stokes_responses_to_nodes, batched)."""
+    def responses(self, records, tangents, step, want_stokes=True):
+        """d Stokes / d node [npix, npar, nlambda, 4] (obs_stokes_responses_to_nodes, batched) by
+        central differences of the records along the node tangents with steps `step` [npar]."""
         rec = _f32(records)
         npix = self._npix(rec)
         tn = _f32(tangents)
         npar = tn.shape[1]
+        stp = np.ascontiguousarray(np.broadcast_to(step, (npar,)), dtype=np.float64)
         st = np.zeros((npix, self.nl, 4), np.float32) if want_stokes else None
         ds = np.zeros((npix, npar, self.nl, 4), np.float32)
-        self._check(lib().snapi_responses(self._ctx, npix, _ptr(rec), npar, _ptr(tn), _ptr(st), _ptr(ds), MEM_HOST))
+        self._check(lib().snapi_responses(self._ctx, npix, _ptr(rec), npar, _ptr(tn), _ptr(stp), _ptr(st), _ptr(ds),
+                                          MEM_HOST))
         return (st, ds) if want_stokes else ds
 
     # --- device-memory API (raw pointers, e.g. torch tensor .data_ptr()) --------------------

@@ -185,6 +185,34 @@ __global__ void k_fd_finish(KParams P) {
     P.grad[(size_t)pix * P.npar + p] = (c2(2 * p + 1) - c2(2 * p + 2)) / (2.0 * P.fd_step[p]);
 }
 
+// Node responses dS/dnode_p by central differences of the record along the node tangent:
+// CTA (pixel, node, chunk) synthesises the +h and -h records in turn and writes the difference.
+__global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_resp_sweep(KParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const SmemLayout L = smem_layout(P.nd, P.nfield, P.nlines, P.ncomp, P.nred, false);
+  const CtaPos c = cta_pos(P);  // var = node index
+  float plus[4], out[4];
+  for (int side = 0; side < 2; ++side) {
+    PixelView pv;
+    if (!stage_pixel(P, c.pix, smem, L, pv, c.var, side == 0 ? 1.f : -1.f)) return;
+    if (c.warp0 < P.nl) {
+      const int le = c.l < P.nl ? c.l : P.nl - 1;
+      LamConst lam;
+      float delta[kMaxLines];
+      thread_lambda(P, pv, le, lam, delta);
+      NoScratch ns;
+      forward_sweep<false>(pv, lam, delta, side == 0 ? plus : out, ns);
+    }
+    __syncthreads();  // the shared record is restaged for the other side
+  }
+  if (c.l < P.nl) {
+    const float ih = (float)(0.5 / P.fd_step[c.var]);
+    float4 *o = reinterpret_cast<float4 *>(P.dstokes + (((size_t)c.pix * P.npar + c.var) * P.nl + c.l) * 4);
+    *o = make_float4((plus[0] - out[0]) * ih, (plus[1] - out[1]) * ih, (plus[2] - out[2]) * ih,
+                     (plus[3] - out[3]) * ih);
+  }
+}
+
 double airtovac_d(double lambda_air) {  // cmlib/mathtools.cc:1325-1330
   double s = 1E4 / (lambda_air * 1E8);
   double n = 1.0 + 0.00008336624212083 + 0.02408926869968 / (130.1065924522 - s * s) +
@@ -465,6 +493,7 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
   CKC(cudaMalloc(&ctx->d_wpart, sizeof(float) * B * ctx->nwslot * ctx->nd * ctx->nred));
   CKC(cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
   CKC(cudaFuncSetAttribute(k_fd_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
+  CKC(cudaFuncSetAttribute(k_resp_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
   CKC(cudaFuncSetAttribute(k_adjoint_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
   CKC(cudaFuncSetAttribute(k_adjoint_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lfin.total));
 #undef CKC
@@ -622,10 +651,61 @@ int snapi_fd_grad(snapi_ctx *ctx, int npix, const float *records, const float *o
   return check_status(ctx);
 }
 
-int snapi_responses(snapi_ctx *ctx, int npix, const float *records, int npar, const float *tangents, float *stokes,
-                    float *dstokes, int mem) {
+int snapi_responses(snapi_ctx *ctx, int npix, const float *records, int npar, const float *tangents,
+                    const double *step, float *stokes, float *dstokes, int mem) {
   if (!ctx) return SNAPI_EINVAL;
-  return set_err(ctx, SNAPI_EINVAL, "snapi_responses: not available in this build");
+  if (npix < 0 || npar < 1 || (npix > 0 && (!records || !tangents || !dstokes)) || !step ||
+      (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
+    return set_err(ctx, SNAPI_EINVAL, "snapi_responses: invalid arguments");
+  for (int p = 0; p < npar; ++p)
+    if (!(step[p] > 0.0)) return set_err(ctx, SNAPI_EINVAL, "snapi_responses: steps must be positive");
+  SNAPI_CK(cudaSetDevice(ctx->device));
+  int st = ensure_npar(ctx, npar);
+  if (st) return st;
+  const size_t nrec = (size_t)ctx->nd * ctx->nfield;
+  const SmemLayout L = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false);
+  SNAPI_CK(cudaMemcpyAsync(ctx->d_step, step, sizeof(double) * npar, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->last_ms = 0.0;
+  ctx->last_launches = 0;
+  for (int p0 = 0; p0 < npix; p0 += ctx->max_batch) {
+    const int nb = std::min(ctx->max_batch, npix - p0);
+    KParams P = base_params(ctx);
+    P.npix = nb;
+    P.npar = npar;
+    P.nvar = npar;
+    const float *rec, *tn;
+    if ((st = stage_in(ctx, records + p0 * nrec, ctx->d_rec, nb * nrec, mem, &rec))) return st;
+    if ((st = stage_in(ctx, tangents + (size_t)p0 * npar * nrec, ctx->d_tan, (size_t)nb * npar * nrec, mem, &tn)))
+      return st;
+    P.rec = rec; P.tangent = tn; P.fd_step = ctx->d_step;
+    const bool dev = mem == SNAPI_MEM_DEVICE;
+    P.dstokes = dev ? dstokes + (size_t)p0 * npar * ctx->nl * 4 : ctx->d_dstokes;
+    P.stokes = stokes ? (dev ? stokes + (size_t)p0 * ctx->nl * 4 : ctx->d_stokes) : nullptr;
+    SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (P.stokes) {
+      KParams Q = P;
+      Q.nvar = 1;
+      k_synth<<<sweep_ctas(ctx, nb), kChunk, L.total, ctx->stream>>>(Q);
+      SNAPI_CK(cudaGetLastError());
+      ctx->last_launches += 1;
+    }
+    k_resp_sweep<<<sweep_ctas(ctx, nb, npar), kChunk, L.total, ctx->stream>>>(P);
+    SNAPI_CK(cudaGetLastError());
+    SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    ctx->last_launches += 1;
+    if (!dev) {
+      if (stokes)
+        SNAPI_CK(cudaMemcpyAsync(stokes + (size_t)p0 * ctx->nl * 4, ctx->d_stokes, sizeof(float) * nb * ctx->nl * 4,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+      SNAPI_CK(cudaMemcpyAsync(dstokes + (size_t)p0 * npar * ctx->nl * 4, ctx->d_dstokes,
+                               sizeof(float) * nb * npar * ctx->nl * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    SNAPI_CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    SNAPI_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->last_ms += ms;
+  }
+  return check_status(ctx);
 }
 
 }  // extern "C"

@@ -85,6 +85,8 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 
 __device__ inline bool tma_bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *mbar) {
   const uint32_t mb = smem_u32(mbar);
+  // the destination may hold this CTA's earlier generic-proxy writes (a record staged again)
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");

@@ -229,3 +229,30 @@ def test_size_independent_properties_at_scale(sb, config3):
         assert np.all(st == st[0])
     np.testing.assert_allclose(out2["grad"], 2.0 * out["grad"][:8], rtol=1e-6,
                                atol=1e-6 * np.abs(out["grad"][:8]).max())
+
+
+def test_responses_match_oracle_and_reference(sb, oracle_lib, config3):
+    """dStokes/dnode: the device central differences against the FP64 oracle's central differences
+    with the same steps, and against the reference's own responses_to_nodes output."""
+    fx = config3
+    n = 3
+    kinds = fx["node_kind"]
+    steps = 1e-2 * node_scales(kinds)
+    ctx = _ctx(sb, fx)
+    st, ds = ctx.responses(fx["record"][:n], fx["tangent"][:n], steps)
+    ctx.close()
+    lines = emu_lines(oracle_lib, fx)
+    ic = _ic(fx)
+    assert np.abs(st - fx["stokes"][:n]).max() / ic < IC_TOL
+    for p in range(n):
+        tan = fx["tangent"][p].astype(np.float64) * steps[:, None, None]
+        ref = oracle_lib.stokes_jvp_fd(fx["lambda_air"], fx["tau500"], fx["record"][p], lines, tan, 1.0)
+        ref /= steps[:, None, None]
+        for q in range(ref.shape[0]):
+            scale = np.abs(ref[q]).max()
+            # FP32 solves differenced over a 1e-2 node step: a few ulp of I / (2 h |dS/dnode|)
+            assert np.abs(ds[p, q] - ref[q]).max() < 5e-3 * scale, (p, q)
+            # the reference's semi-analytic responses differ from central differences by up to ~5 %
+            # (inclination nodes; 0.1-1 % elsewhere)
+            rr = fx["responses"][p, q]
+            assert np.abs(ds[p, q] - rr).max() < 8e-2 * np.abs(rr).max(), (p, q)
