@@ -424,102 +424,110 @@ SNAPI_HD void cell_opacity(const DepthConst &d, const LineDepth *ld, const LineC
 
 // Reverse of cell_opacity: given eta_bar[7], j_bar[4] accumulate the depth-level adjoint sums
 // red[kNumRed + kRedPerLine*nlines] (wavelength-summed later).
-SNAPI_HD void cell_opacity_adjoint(const DepthConst &d, const LineDepth *ld, const LineConst *lc, int nlines,
-                                   const float *compS, const float *compD, const LamConst &lc_l,
-                                   const float *delta, const float *etab, const float *jb, float *red) {
-  red[R_COP] += etab[0];
-  red[R_CEM] += jb[0];
-  float st2b = 0.f, ctbb = 0.f, c2b = 0.f, s2b = 0.f;
-  for (int j = 0; j < nlines; ++j) {
-    const LineConst &L = lc[j];
-    const LineDepth &q = ld[j];
-    float *rl = red + kNumRed + kRedPerLine * j;
-    const float xd = delta[j] - lc_l.lam * d.beta;
-    const float x0 = xd * q.inv_dld;
-    float x0b = 0.f, bb = 0.f, ab = 0.f;
-    if (!L.split) {
-      float H, F, Hx, Fx, Ha, Fa;
-      voigt_grad(x0, q.a, H, F, Hx, Fx, Ha, Fa);
-      rl[RL_OPN] += etab[0] * H;
-      rl[RL_EMN] += jb[0] * H;
-      const float Hb_ = q.opn * etab[0] + q.emn * jb[0];
-      x0b += Hb_ * Hx;
-      ab += Hb_ * Ha;
-    } else {
-      // adjoints of the component sums depend only on (eta-bar, j-bar) and the angles, so one
-      // pass of voigt_grad per component gives both the sums and the x / a adjoints
-      float Pb[7];
+// Opacity adjoint of transition j at one (lambda, depth): adds the six per-line sums rl[RL_*] and
+// the four angle sums ang[] (st2, ctb, c2, s2).  lam = (float) vacuum wavelength, delta_j =
+// lam0_j - lambda (FP64 -> FP32).
+SNAPI_HD void line_opacity_adjoint(const DepthConst &d, const LineDepth &q, const LineConst &L, const float *compS,
+                                   const float *compD, float lam, float delta_j, const float *etab, const float *jb,
+                                   float *rl, float *ang) {
+  const float xd = delta_j - lam * d.beta;
+  const float x0 = xd * q.inv_dld;
+  float x0b = 0.f, bb = 0.f, ab = 0.f;
+  if (!L.split) {
+    float H, F, Hx, Fx, Ha, Fa;
+    voigt_grad(x0, q.a, H, F, Hx, Fx, Ha, Fa);
+    rl[RL_OPN] += etab[0] * H;
+    rl[RL_EMN] += jb[0] * H;
+    const float Hb_ = q.opn * etab[0] + q.emn * jb[0];
+    x0b += Hb_ * Hx;
+    ab += Hb_ * Ha;
+  } else {
+    // adjoints of the component sums depend only on (eta-bar, j-bar) and the angles, so one
+    // pass of voigt_grad per component gives both the sums and the x / a adjoints
+    float Pb[7];
 #pragma unroll
-      for (int k = 0; k < 7; ++k) Pb[k] = q.opn * etab[k] + (k < 4 ? q.emn * jb[k] : 0.0f);
-      const float hpmb = 0.5f * d.st2 * (d.c2 * Pb[1] + d.s2 * Pb[2]);
-      const float fpmb = 0.5f * d.st2 * (d.c2 * Pb[4] + d.s2 * Pb[5]);
-      float Hsb[3], Fsb[3];
-      Hsb[0] = 0.5f * d.st2 * Pb[0] + hpmb;
-      Hsb[1] = 0.25f * d.opc2 * Pb[0] - 0.5f * hpmb - 0.5f * d.ctb * Pb[3];
-      Hsb[2] = 0.25f * d.opc2 * Pb[0] - 0.5f * hpmb + 0.5f * d.ctb * Pb[3];
-      Fsb[0] = fpmb;
-      Fsb[1] = -0.5f * fpmb - 0.5f * d.ctb * Pb[6];
-      Fsb[2] = -0.5f * fpmb + 0.5f * d.ctb * Pb[6];
-      float Hs[3] = {0.f, 0.f, 0.f}, Fs[3] = {0.f, 0.f, 0.f};
-      int off = L.comp_off;
+    for (int k = 0; k < 7; ++k) Pb[k] = q.opn * etab[k] + (k < 4 ? q.emn * jb[k] : 0.0f);
+    const float hpmb = 0.5f * d.st2 * (d.c2 * Pb[1] + d.s2 * Pb[2]);
+    const float fpmb = 0.5f * d.st2 * (d.c2 * Pb[4] + d.s2 * Pb[5]);
+    float Hsb[3], Fsb[3];
+    Hsb[0] = 0.5f * d.st2 * Pb[0] + hpmb;
+    Hsb[1] = 0.25f * d.opc2 * Pb[0] - 0.5f * hpmb - 0.5f * d.ctb * Pb[3];
+    Hsb[2] = 0.25f * d.opc2 * Pb[0] - 0.5f * hpmb + 0.5f * d.ctb * Pb[3];
+    Fsb[0] = fpmb;
+    Fsb[1] = -0.5f * fpmb - 0.5f * d.ctb * Pb[6];
+    Fsb[2] = -0.5f * fpmb + 0.5f * d.ctb * Pb[6];
+    float Hs[3] = {0.f, 0.f, 0.f}, Fs[3] = {0.f, 0.f, 0.f};
+    int off = L.comp_off;
 #pragma unroll
-      for (int g = 0; g < 3; ++g)
-        for (int i = 0; i < L.ncomp[g]; ++i, ++off) {
-          float H, F, Hx, Fx, Ha, Fa;
-          voigt_grad(x0 + compD[off] * q.bsh, q.a, H, F, Hx, Fx, Ha, Fa);
-          const float S = compS[off];
-          Hs[g] += H * S;
-          Fs[g] += F * S;
-          const float hb_ = Hsb[g] * S, fb_ = Fsb[g] * S;
-          const float xb = hb_ * Hx + fb_ * Fx;
-          x0b += xb;
-          bb += xb * compD[off];
-          ab += hb_ * Ha + fb_ * Fa;
-        }
-      const float hpm = Hs[0] - 0.5f * (Hs[2] + Hs[1]);
-      const float fpm = Fs[0] - 0.5f * (Fs[2] + Fs[1]);
-      const float P[7] = {0.5f * (Hs[0] * d.st2 + 0.5f * (Hs[2] + Hs[1]) * d.opc2),
-                          0.5f * hpm * d.st2 * d.c2,
-                          0.5f * hpm * d.st2 * d.s2,
-                          0.5f * (Hs[2] - Hs[1]) * d.ctb,
-                          0.5f * fpm * d.st2 * d.c2,
-                          0.5f * fpm * d.st2 * d.s2,
-                          0.5f * (Fs[2] - Fs[1]) * d.ctb};
-      float gop = 0.f, gem = 0.f;
+    for (int g = 0; g < 3; ++g)
+      for (int i = 0; i < L.ncomp[g]; ++i, ++off) {
+        float H, F, Hx, Fx, Ha, Fa;
+        voigt_grad(x0 + compD[off] * q.bsh, q.a, H, F, Hx, Fx, Ha, Fa);
+        const float S = compS[off];
+        Hs[g] += H * S;
+        Fs[g] += F * S;
+        const float hb_ = Hsb[g] * S, fb_ = Fsb[g] * S;
+        const float xb = hb_ * Hx + fb_ * Fx;
+        x0b += xb;
+        bb += xb * compD[off];
+        ab += hb_ * Ha + fb_ * Fa;
+      }
+    const float hpm = Hs[0] - 0.5f * (Hs[2] + Hs[1]);
+    const float fpm = Fs[0] - 0.5f * (Fs[2] + Fs[1]);
+    const float P[7] = {0.5f * (Hs[0] * d.st2 + 0.5f * (Hs[2] + Hs[1]) * d.opc2),
+                        0.5f * hpm * d.st2 * d.c2,
+                        0.5f * hpm * d.st2 * d.s2,
+                        0.5f * (Hs[2] - Hs[1]) * d.ctb,
+                        0.5f * fpm * d.st2 * d.c2,
+                        0.5f * fpm * d.st2 * d.s2,
+                        0.5f * (Fs[2] - Fs[1]) * d.ctb};
+    float gop = 0.f, gem = 0.f;
 #pragma unroll
-      for (int k = 0; k < 7; ++k) gop += etab[k] * P[k];
+    for (int k = 0; k < 7; ++k) gop += etab[k] * P[k];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) gem += jb[k] * P[k];
-      rl[RL_OPN] += gop;
-      rl[RL_EMN] += gem;
-      st2b += 0.5f * Hs[0] * Pb[0] + 0.5f * hpm * (d.c2 * Pb[1] + d.s2 * Pb[2]) +
+    for (int k = 0; k < 4; ++k) gem += jb[k] * P[k];
+    rl[RL_OPN] += gop;
+    rl[RL_EMN] += gem;
+    ang[0] += 0.5f * Hs[0] * Pb[0] + 0.5f * hpm * (d.c2 * Pb[1] + d.s2 * Pb[2]) +
               0.5f * fpm * (d.c2 * Pb[4] + d.s2 * Pb[5]);
-      ctbb += 2.0f * d.ctb * (0.25f * (Hs[2] + Hs[1]) * Pb[0]) + 0.5f * (Hs[2] - Hs[1]) * Pb[3] +
+    ang[1] += 2.0f * d.ctb * (0.25f * (Hs[2] + Hs[1]) * Pb[0]) + 0.5f * (Hs[2] - Hs[1]) * Pb[3] +
               0.5f * (Fs[2] - Fs[1]) * Pb[6];
-      c2b += 0.5f * d.st2 * (hpm * Pb[1] + fpm * Pb[4]);
-      s2b += 0.5f * d.st2 * (hpm * Pb[2] + fpm * Pb[5]);
-    }
-    rl[RL_XL] += x0b * lc_l.lam;
-    rl[RL_XD] += x0b * xd;
-    rl[RL_B] += bb;
-    rl[RL_A] += ab;
+    ang[2] += 0.5f * d.st2 * (hpm * Pb[1] + fpm * Pb[4]);
+    ang[3] += 0.5f * d.st2 * (hpm * Pb[2] + fpm * Pb[5]);
   }
-  red[R_ST2] += st2b;
-  red[R_CTB] += ctbb;
-  red[R_C2] += c2b;
-  red[R_S2] += s2b;
-  // H-
+  rl[RL_XL] += x0b * lam;
+  rl[RL_XD] += x0b * xd;
+  rl[RL_B] += bb;
+  rl[RL_A] += ab;
+}
+
+// Continuum part of the opacity adjoint (Thomson + bound-free totals, H-): adds red[R_COP..R_LT].
+SNAPI_HD void continuum_opacity_adjoint(const DepthConst &d, const LamConst &lc_l, float etab0, float jb0,
+                                        float *red) {
+  red[R_COP] += etab0;
+  red[R_CEM] += jb0;
   const float e1 = fexp(-lc_l.xs * d.invT);
   const float E10 = fexp(kLn10 * (lc_l.F0 + lc_l.f1 * d.lt + lc_l.f2 * d.lt * d.lt));
   const float oph = lc_l.afud * d.hb * (1.0f - e1) + d.hf * E10;
   const float Ep = fexp(lc_l.xp * d.invT);
   const float pl = lc_l.pp / (Ep - 1.0f);
-  const float ophb = etab[0] + jb[0] * pl;
-  const float plb = jb[0] * oph;
+  const float ophb = etab0 + jb0 * pl;
+  const float plb = jb0 * oph;
   red[R_HB] += ophb * lc_l.afud * (1.0f - e1);
   red[R_HF] += ophb * E10;
   red[R_INVT] += ophb * lc_l.afud * d.hb * lc_l.xs * e1 - plb * pl * lc_l.xp * Ep / (Ep - 1.0f);
   red[R_LT] += ophb * d.hf * E10 * kLn10 * (lc_l.f1 + 2.0f * lc_l.f2 * d.lt);
+}
+
+// Adjoint of cell_opacity at one (lambda, depth): adds every depth sum of red[] (continuum, angle
+// and per-line terms).
+SNAPI_HD void cell_opacity_adjoint(const DepthConst &d, const LineDepth *ld, const LineConst *lc, int nlines,
+                                   const float *compS, const float *compD, const LamConst &lc_l,
+                                   const float *delta, const float *etab, const float *jb, float *red) {
+  for (int j = 0; j < nlines; ++j)
+    line_opacity_adjoint(d, ld[j], lc[j], compS, compD, lc_l.lam, delta[j], etab, jb, red + kNumRed + kRedPerLine * j,
+                         red + R_ST2);
+  continuum_opacity_adjoint(d, lc_l, etab[0], jb[0], red);
 }
 
 // Chain the wavelength-summed depth adjoint sums red[] to the record fields (adds into rb[nfield]).

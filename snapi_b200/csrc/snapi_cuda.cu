@@ -6,10 +6,14 @@
 // once per CTA in shared memory, and every thread runs the depth recursion of its wavelength in
 // registers (snapi_sweep.cuh).
 //   k_synth          forward sweep -> Stokes
-//   k_adjoint_sweep  forward sweep (state to scratch) -> chi2 seed -> reverse sweep; per-warp
-//                    wavelength sums of the depth-level adjoint terms -> partial buffer
-//   k_adjoint_finish one CTA per pixel: fixed-order sum of the partials, chain rule to the record
+//   k_adj_forward    forward sweep (state to scratch) -> Stokes, chi2 partials, adjoint seed
+//   k_adj_rt         reverse DELO + optical-depth sweep per wavelength -> (eta-bar, j-bar) per depth
+//   k_adj_opacity    one thread per (pixel, depth, transition or continuum): opacity adjoint summed
+//                    over wavelengths in registers -> partial buffer
+//   k_adjoint_finish one CTA per pixel: fixed-order gather of the partials, chain rule to the record
 //                    fields, contraction with the node tangents -> d chi2 / d node
+// The adjoint runs as three kernels rather than one so that every SM holds only one phase's
+// instructions at a time and each phase gets its own register budget.
 //   k_fd_sweep / k_fd_finish: the plain finite-difference gradient (2 npar + 1 forward solves)
 #include <algorithm>
 #include <cstdarg>
@@ -29,9 +33,7 @@ namespace {
 #ifndef SNAPI_SYN_MINB
 #define SNAPI_SYN_MINB (640 / SNAPI_CHUNK)
 #endif
-#ifndef SNAPI_ADJ_MINB
-#define SNAPI_ADJ_MINB (512 / SNAPI_CHUNK)
-#endif
+constexpr int kOpThreads = 256;  // k_adj_opacity: threads per CTA (depths; larger nd loops)
 
 struct CtaPos {
   int pix, var, chunk, l, warp0, wslot;
@@ -71,7 +73,9 @@ __global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_synth(KParams P) {
   }
 }
 
-__global__ void __launch_bounds__(kChunk, SNAPI_ADJ_MINB) k_adjoint_sweep(KParams P) {
+// Adjoint, phase F: forward sweep storing the per-depth state, the emergent Stokes vector, the
+// chi2 partials and the adjoint seed of every wavelength.
+__global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_adj_forward(KParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const SmemLayout L = smem_layout(P.nd, P.nfield, P.nlines, P.ncomp, P.nred, false);
   const CtaPos c = cta_pos(P);
@@ -98,14 +102,76 @@ __global__ void __launch_bounds__(kChunk, SNAPI_ADJ_MINB) k_adjoint_sweep(KParam
     }
     c2 = residual_seed(P, c.pix, c.l, out, seed);
   }
+  P.seed[(size_t)c.pix * P.lpad + c.l] = make_float4(seed[0], seed[1], seed[2], seed[3]);
   c2 = warp_sum(c2);
   if ((threadIdx.x & 31) == 0) P.c2part[(size_t)c.pix * P.nwslot + c.wslot] = c2;
+}
+
+// Adjoint, phase R1: reverse DELO sweep and optical-depth adjoint per wavelength (no opacity
+// work, no shared memory); writes (eta-bar, j-bar) of every depth.
+__global__ void __launch_bounds__(kChunk) k_adj_rt(KParams P) {
+  const CtaPos c = cta_pos(P);
+  if (c.warp0 >= P.nl) return;
+  PixelView pv;
+  pv.nd = P.nd;
+  pv.D = P.D;
+  RtScratch sc;
+  sc.state = P.scratch + (size_t)c.pix * P.nd * 4 * P.lpad;
+  sc.bars = P.bars + (size_t)c.pix * P.nl * 3 * P.nd;
+  sc.lpad = P.lpad;
+  sc.l = c.l;
+  sc.nd = P.nd;
+  sc.write = c.l < P.nl;
+  const float4 s4 = P.seed[(size_t)c.pix * P.lpad + c.l];
+  const float seed[4] = {s4.x, s4.y, s4.z, s4.w};
   reverse_sweep_rt(pv, seed, sc);
-  WarpPartReducer rd;
-  rd.part = P.wpart + ((size_t)c.pix * P.nwslot + c.wslot) * P.nd * P.nred;
-  rd.nred = P.nred;
-  float red[kRedMax];
-  reverse_sweep_opacity(pv, lam, delta, sc, rd, red, P.nred);
+}
+
+// Adjoint, phase R2: opacity adjoint.  CTA = (pixel, group): group 0 the continuum, group 1 + j
+// transition j; one thread per depth walks every wavelength and keeps its sums in registers, so
+// the wavelength sums need no shuffles.  Wavelengths whose bars are all zero (masked) are skipped.
+__global__ void __launch_bounds__(kOpThreads) k_adj_opacity(KParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const SmemLayout L = smem_layout(P.nd, P.nfield, P.nlines, P.ncomp, P.nred, false);
+  const int ng = 1 + P.nlines;
+  const int pix = blockIdx.x / ng, g = blockIdx.x % ng;
+  PixelView pv;
+  if (!stage_pixel(P, pix, smem, L, pv, -1, 0.f)) return;
+  const float4 *bars = P.bars + (size_t)pix * P.nl * 3 * P.nd;
+  for (int z = threadIdx.x; z < P.nd; z += blockDim.x) {
+    float acc[kOpSlots];
+#pragma unroll
+    for (int i = 0; i < kOpSlots; ++i) acc[i] = 0.f;
+    const DepthConst d = pv.dc[z];
+    if (g == 0) {
+      for (int l = 0; l < P.nl; ++l) {
+        const float eb0 = bars[(size_t)l * 3 * P.nd + z].x;
+        const float jb0 = bars[((size_t)l * 3 + 1) * P.nd + z].w;
+        if (eb0 == 0.f && jb0 == 0.f) continue;
+        LamConst lam;
+        lambda_precompute(P.lamvac[l], lam);
+        continuum_opacity_adjoint(d, lam, eb0, jb0, acc);
+      }
+    } else {
+      const LineConst Lc = pv.lc[g - 1];
+      const LineDepth q = pv.ld[z * P.nlines + g - 1];
+      for (int l = 0; l < P.nl; ++l) {
+        const float4 *b = bars + (size_t)l * 3 * P.nd + z;
+        const float4 a = b[0], e = b[P.nd], f = b[2 * P.nd];
+        const float etab[7] = {a.x, a.y, a.z, a.w, e.x, e.y, e.z};
+        const float jb[4] = {e.w, f.x, f.y, f.z};
+        if (a.x == 0.f && a.y == 0.f && a.z == 0.f && a.w == 0.f && e.x == 0.f && e.y == 0.f && e.z == 0.f &&
+            e.w == 0.f && f.x == 0.f && f.y == 0.f && f.z == 0.f)
+          continue;
+        const double lv = P.lamvac[l];
+        line_opacity_adjoint(d, q, Lc, pv.compS, pv.compD, (float)lv, (float)(Lc.lam0 - lv), etab, jb, acc,
+                             acc + kRedPerLine);
+      }
+    }
+    float *o = P.opart + (((size_t)pix * ng + g) * P.nd + z) * kOpSlots;
+#pragma unroll
+    for (int i = 0; i < kOpSlots; ++i) o[i] = acc[i];
+  }
 }
 
 __global__ void __launch_bounds__(kFinishThreads) k_adjoint_finish(KParams P) {
@@ -118,11 +184,19 @@ __global__ void __launch_bounds__(kFinishThreads) k_adjoint_finish(KParams P) {
   PixelView pv;
   if (!stage_pixel(P, pix, smem, L, pv, -1, 0.f)) return;
   const int nw = (P.nl + 31) / 32;  // warps that held wavelengths
-  const int nacc = P.nd * P.nred, nrec = P.nd * P.nfield;
-  const float *part = P.wpart + (size_t)pix * P.nwslot * nacc;
+  const int nacc = P.nd * P.nred, nrec = P.nd * P.nfield, ng = 1 + P.nlines;
+  const float *part = P.opart + (size_t)pix * ng * P.nd * kOpSlots;
   for (int e = threadIdx.x; e < nacc; e += blockDim.x) {
+    const int z = e / P.nred, t = e % P.nred;
     float s = 0.f;
-    for (int w = 0; w < nw; ++w) s += part[(size_t)w * nacc + e];
+    if (t < R_ST2) {
+      s = part[(size_t)z * kOpSlots + t];  // continuum group
+    } else if (t < kNumRed) {
+      for (int j = 0; j < P.nlines; ++j) s += part[((size_t)(1 + j) * P.nd + z) * kOpSlots + kRedPerLine + t - R_ST2];
+    } else {
+      const int j = (t - kNumRed) / kRedPerLine, k = (t - kNumRed) % kRedPerLine;
+      s = part[((size_t)(1 + j) * P.nd + z) * kOpSlots + k];
+    }
     acc[e] = s;
   }
   for (int i = threadIdx.x; i < nrec; i += blockDim.x) rb[i] = 0.f;
@@ -232,6 +306,16 @@ int stage_in(snapi_ctx *ctx, const T *src, T *dbuf, size_t n, int mem, const T *
 
 int sweep_ctas(const snapi_ctx *ctx, int nb, int nvar = 1) { return nb * nvar * ctx->nchunk; }
 
+// the adjoint's kernel sequence for nb pixels (P.npix = nb)
+constexpr int kAdjointLaunches = 4;
+void launch_adjoint(const KParams &P, int nb, int nchunk, size_t smem_sweep, size_t smem_fin, cudaStream_t st) {
+  k_adj_forward<<<nb * nchunk, kChunk, smem_sweep, st>>>(P);
+  k_adj_rt<<<nb * nchunk, kChunk, 0, st>>>(P);
+  const int nthr = std::min(kOpThreads, (P.nd + 31) / 32 * 32);
+  k_adj_opacity<<<nb * (1 + P.nlines), nthr, smem_sweep, st>>>(P);
+  k_adjoint_finish<<<nb, kFinishThreads, smem_fin, st>>>(P);
+}
+
 }  // namespace
 
 namespace snapi {
@@ -271,7 +355,8 @@ KParams base_params(const snapi_ctx *ctx) {
   P.lam_mid = ctx->lam_mid; P.scale2 = ctx->scale2;
   P.lamvac = ctx->d_lamvac; P.lines = ctx->d_lines; P.compS = ctx->d_compS; P.compD = ctx->d_compD;
   P.D = ctx->d_D; P.status = ctx->d_status;
-  P.scratch = ctx->d_scratch; P.wpart = ctx->d_wpart; P.c2part = ctx->d_c2part;
+  P.scratch = ctx->d_scratch; P.seed = ctx->d_seed; P.bars = ctx->d_bars; P.opart = ctx->d_opart;
+  P.c2part = ctx->d_c2part;
   return P;
 }
 
@@ -368,7 +453,7 @@ void snapi_destroy(snapi_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   void *bufs[] = {ctx->d_lamvac, ctx->d_D, ctx->d_lines, ctx->d_compS, ctx->d_compD, ctx->d_status,
                   ctx->d_rec, ctx->d_stokes, ctx->d_obs, ctx->d_mask, ctx->d_tan, ctx->d_recgrad,
-                  ctx->d_dstokes, ctx->d_wpart, ctx->d_grad, ctx->d_chi2, ctx->d_c2part, ctx->d_step,
+                  ctx->d_dstokes, ctx->d_opart, ctx->d_seed, ctx->d_bars, ctx->d_grad, ctx->d_chi2, ctx->d_c2part, ctx->d_step,
                   ctx->d_scratch};
   for (void *b : bufs)
     if (b) cudaFree(b);
@@ -490,11 +575,14 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
   CKC(cudaMalloc(&ctx->d_recgrad, sizeof(double) * B * nrec));
   CKC(cudaMalloc(&ctx->d_chi2, sizeof(double) * B));
   CKC(cudaMalloc(&ctx->d_scratch, sizeof(float4) * B * ctx->nd * 4 * ctx->lpad));
-  CKC(cudaMalloc(&ctx->d_wpart, sizeof(float) * B * ctx->nwslot * ctx->nd * ctx->nred));
+  CKC(cudaMalloc(&ctx->d_seed, sizeof(float4) * B * ctx->lpad));
+  CKC(cudaMalloc(&ctx->d_bars, sizeof(float4) * B * ctx->nl * 3 * ctx->nd));
+  CKC(cudaMalloc(&ctx->d_opart, sizeof(float) * B * (1 + ctx->nlines) * ctx->nd * kOpSlots));
   CKC(cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
   CKC(cudaFuncSetAttribute(k_fd_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
   CKC(cudaFuncSetAttribute(k_resp_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
-  CKC(cudaFuncSetAttribute(k_adjoint_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
+  CKC(cudaFuncSetAttribute(k_adj_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
+  CKC(cudaFuncSetAttribute(k_adj_opacity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
   CKC(cudaFuncSetAttribute(k_adjoint_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lfin.total));
 #undef CKC
   if (ensure_npar(ctx, 1) != SNAPI_OK) return fail(ctx, SNAPI_ENOMEM);
@@ -572,12 +660,10 @@ int snapi_adjoint(snapi_ctx *ctx, int npix, const float *records, const float *o
     P.grad = npar ? (dev ? grad + (size_t)p0 * npar : ctx->d_grad) : ctx->d_grad;
     P.rec_grad = rec_grad ? (dev ? rec_grad + (size_t)p0 * nrec : ctx->d_recgrad) : nullptr;
     SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    k_adjoint_sweep<<<sweep_ctas(ctx, nb), kChunk, Lsw.total, ctx->stream>>>(P);
-    SNAPI_CK(cudaGetLastError());
-    k_adjoint_finish<<<nb, kFinishThreads, Lfin.total, ctx->stream>>>(P);
+    launch_adjoint(P, nb, ctx->nchunk, Lsw.total, Lfin.total, ctx->stream);
     SNAPI_CK(cudaGetLastError());
     SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    ctx->last_launches += 2;
+    ctx->last_launches += kAdjointLaunches;
     if (!dev) {
       if (stokes)
         SNAPI_CK(cudaMemcpyAsync(stokes + (size_t)p0 * ctx->nl * 4, ctx->d_stokes, sizeof(float) * nb * ctx->nl * 4,
@@ -721,9 +807,10 @@ int snapi_responses(snapi_ctx *ctx, int npix, const float *records, int npar, co
 //
 // g_snapi_static is SNAPI_STATIC_SCRATCH_BYTES (64 MiB) on every GPU that loads this library,
 // held until the process exits.  Layout: [status word][problem constants][work region]; the work
-// region holds, per pixel of a chunk, the forward state (nd x 4 x lpad float4), the per-warp
-// wavelength sums (nwarp x nd x nred float) and the per-warp chi2 sums (nwarp double).  Pixels
-// are processed in chunks that fit the work region.  In host code the array's name is only a
+// region holds, per pixel of a chunk, the forward state (nd x 4 x lpad float4), the adjoint
+// seed (lpad float4), the adjoint bars (nl x 3 x nd float4), the opacity-adjoint sums
+// ((1 + nlines) x nd x kOpSlots float) and the per-warp chi2 sums (nwarp double).  Pixels
+// are processed in chunks that fit the work region.
 // host-side stand-in, so its device address is fetched with cudaGetSymbolAddress -- once per
 // device, by the first call on that device, with that device current.
 // Every call shares the array: the kernels overwrite every slot they read in the same call and
@@ -750,7 +837,8 @@ int static_setup(int device, unsigned char **base, std::string &err) {
       return SNAPI_ECUDA;
     }
     const int fin = 227 * 1024;
-    e = cudaFuncSetAttribute(k_adjoint_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, fin);
+    e = cudaFuncSetAttribute(k_adj_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, fin);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_adj_opacity, cudaFuncAttributeMaxDynamicSharedMemorySize, fin);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_adjoint_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, fin);
     if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return SNAPI_ECUDA; }
     g_static_ptr[device] = static_cast<unsigned char *>(p);
@@ -799,9 +887,13 @@ int noalloc_run(const snapi_problem *prob, void *stream_v, int npix, const float
   if (o > kStaticConstBytes) { err = "problem constants exceed the static constants region"; return SNAPI_EINVAL; }
   // work region per pixel
   const size_t per_state = sizeof(float4) * (size_t)nd * 4 * lpad;
-  const size_t per_part = sizeof(float) * (size_t)nwslot * nd * nred;
+  const size_t per_seed = sizeof(float4) * (size_t)lpad;
+  const size_t per_bars = sizeof(float4) * (size_t)nl * 3 * nd;
+  const size_t per_part = sizeof(float) * (size_t)(1 + nlines) * nd * kOpSlots;
   const size_t per_c2 = sizeof(double) * (size_t)nwslot;
-  const size_t per_pix = align_up(per_state, 256) + align_up(per_part, 256) + align_up(per_c2, 256);
+  const size_t a_state = align_up(per_state, 256), a_seed = align_up(per_seed, 256), a_bars = align_up(per_bars, 256),
+               a_part = align_up(per_part, 256), a_c2 = align_up(per_c2, 256);
+  const size_t per_pix = a_state + a_seed + a_bars + a_part + a_c2;
   const size_t work = kStaticBytes - kStaticConstBytes;
   const int cap = (int)std::min<size_t>(work / per_pix, 1 << 20);
   if (cap < 1) {
@@ -847,8 +939,10 @@ int noalloc_run(const snapi_problem *prob, void *stream_v, int npix, const float
     P.compD = reinterpret_cast<const float *>(base + o_cD);
     P.status = status;
     P.scratch = reinterpret_cast<float4 *>(wbase);
-    P.wpart = reinterpret_cast<float *>(wbase + align_up(per_state, 256) * cap);
-    P.c2part = reinterpret_cast<double *>(wbase + (align_up(per_state, 256) + align_up(per_part, 256)) * cap);
+    P.seed = reinterpret_cast<float4 *>(wbase + a_state * cap);
+    P.bars = reinterpret_cast<float4 *>(wbase + (a_state + a_seed) * cap);
+    P.opart = reinterpret_cast<float *>(wbase + (a_state + a_seed + a_bars) * cap);
+    P.c2part = reinterpret_cast<double *>(wbase + (a_state + a_seed + a_bars + a_part) * cap);
     for (int s = 0; s < 4; ++s) P.ws[s] = w_stokes ? w_stokes[s] : 1.0;
     P.rec = records + p0 * nrec;
     P.obs = obs + (size_t)p0 * nl * 4;
@@ -857,9 +951,7 @@ int noalloc_run(const snapi_problem *prob, void *stream_v, int npix, const float
     P.stokes = stokes ? stokes + (size_t)p0 * nl * 4 : nullptr;
     P.chi2 = chi2 + p0;
     P.grad = npar ? grad + (size_t)p0 * npar : nullptr;
-    k_adjoint_sweep<<<nb * nchunk, kChunk, Lsw.total, stream>>>(P);
-    CKN(cudaGetLastError());
-    k_adjoint_finish<<<nb, kFinishThreads, Lfin.total, stream>>>(P);
+    launch_adjoint(P, nb, nchunk, Lsw.total, Lfin.total, stream);
     CKN(cudaGetLastError());
   }
   int st = 0;

@@ -25,6 +25,9 @@ constexpr int kChunk = SNAPI_CHUNK;           // wavelengths (threads) per sweep
 constexpr int kFinishThreads = 128;           // threads of the per-pixel finish kernels
 constexpr long long kWaitLimit = 1LL << 26;   // mbarrier polls before a CTA gives up
 constexpr int kRedMax = kNumRed + kRedPerLine * kMaxLines;  // <= 64
+// Opacity-adjoint sums per (pixel, group, depth): group 0 (continuum) fills R_COP..R_LT, group
+// 1 + j (transition j) fills RL_OPN..RL_A then its share of R_ST2..R_S2.
+constexpr int kOpSlots = kRedPerLine + 4;
 
 struct KParams {
   int npix, nd, nl, nlines, nfield, npar, lpad, ncomp, nred, nchunk, nwslot, nvar;
@@ -40,8 +43,10 @@ struct KParams {
   double ws[4];
   const float *mask;            // [npix][nl] or null
   const float *tangent;         // [npix][npar][nd][nfield] or null
-  float4 *scratch;              // [npix][nd][4][lpad]
-  float *wpart;                 // [npix][nwslot][nd][nred]  per-warp wavelength sums
+  float4 *scratch;              // [npix][nd][4][lpad]     forward state of the adjoint
+  float4 *seed;                 // [npix][lpad]            adjoint of the emergent Stokes vector
+  float4 *bars;                 // [npix][nl][3][nd]       (eta-bar, j-bar) per wavelength, depth
+  float *opart;                 // [npix][1+nlines][nd][kOpSlots] wavelength sums of the opacity adjoint
   double *c2part;               // [npix][nvar][nwslot]      per-warp chi2 sums
   double *rec_grad;             // [npix][nd][nfield] or null
   double *grad;                 // [npix][npar]
@@ -131,19 +136,29 @@ struct DevScratch {
     kp[4] = c.x; kp[5] = c.y; e = c.z; tau = c.w;
     S[0] = d.x; S[1] = d.y; S[2] = d.z; S[3] = d.w;
   }
-  // (eta-bar[7], j-bar[4]) of a finished depth, in the same slots
-  __device__ void store_bar(int z, const float *eb, const float *jb) {
-    float4 *p = base + (size_t)z * 4 * lpad + l;
-    p[0] = make_float4(eb[0], eb[1], eb[2], eb[3]);
-    p[lpad] = make_float4(eb[4], eb[5], eb[6], jb[0]);
-    p[2 * lpad] = make_float4(jb[1], jb[2], jb[3], 0.f);
+};
+
+// Reverse DELO sweep (phase R1): reads the forward state of wavelength l, writes the adjoint bars
+// of each finished depth depth-contiguous ([l][plane][z]) for the per-depth opacity adjoint.
+struct RtScratch {
+  const float4 *state;
+  float4 *bars;
+  int lpad, l, nd;
+  bool write;  // false for the padding lanes of the last wavelength chunk
+  __device__ void load(int z, float *I, float *kp, float *S, float &e, float &tau) const {
+    const float4 *p = state + (size_t)z * 4 * lpad + l;
+    float4 a = p[0], b = p[lpad], c = p[2 * lpad], d = p[3 * lpad];
+    I[0] = a.x; I[1] = a.y; I[2] = a.z; I[3] = a.w;
+    kp[0] = b.x; kp[1] = b.y; kp[2] = b.z; kp[3] = b.w;
+    kp[4] = c.x; kp[5] = c.y; e = c.z; tau = c.w;
+    S[0] = d.x; S[1] = d.y; S[2] = d.z; S[3] = d.w;
   }
-  __device__ void load_bar(int z, float *eb, float *jb) const {
-    const float4 *p = base + (size_t)z * 4 * lpad + l;
-    float4 a = p[0], b = p[lpad], c = p[2 * lpad];
-    eb[0] = a.x; eb[1] = a.y; eb[2] = a.z; eb[3] = a.w;
-    eb[4] = b.x; eb[5] = b.y; eb[6] = b.z; jb[0] = b.w;
-    jb[1] = c.x; jb[2] = c.y; jb[3] = c.z;
+  __device__ void store_bar(int z, const float *eb, const float *jb) {
+    if (!write) return;
+    float4 *p = bars + (size_t)l * 3 * nd + z;
+    p[0] = make_float4(eb[0], eb[1], eb[2], eb[3]);
+    p[nd] = make_float4(eb[4], eb[5], eb[6], jb[0]);
+    p[2 * nd] = make_float4(jb[1], jb[2], jb[3], 0.f);
   }
 };
 struct NoScratch {
@@ -162,25 +177,6 @@ __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
-
-// Reducer of the reverse sweep: per depth, the warp's wavelength sums of the nred adjoint terms
-// go to part[z][0..nred) of this warp's slot; lane i keeps term i and i+32 (coalesced stores).
-struct WarpPartReducer {
-  float *part;  // this warp's slot: [nd][nred]
-  int nred;
-  __device__ void add(int z, const float *red, int n) {
-    const int lane = threadIdx.x & 31;
-    float k0 = 0.f, k1 = 0.f;
-    for (int i = 0; i < n; ++i) {
-      const float v = warp_sum(red[i]);
-      if (i == lane) k0 = v;
-      if (i == lane + 32) k1 = v;
-    }
-    float *dst = part + (size_t)z * nred;
-    if (lane < n) dst[lane] = k0;
-    if (lane + 32 < n) dst[lane + 32] = k1;
-  }
-};
 
 // sum over the CTA (valid in thread 0)
 __device__ inline double block_sum(double v, double *wred) {
@@ -276,7 +272,8 @@ struct snapi_ctx {
   int *d_status = nullptr;
   // work buffers (max_batch pixels)
   float *d_rec = nullptr, *d_stokes = nullptr, *d_obs = nullptr, *d_mask = nullptr, *d_tan = nullptr;
-  float *d_dstokes = nullptr, *d_wpart = nullptr;
+  float *d_dstokes = nullptr, *d_opart = nullptr;
+  float4 *d_seed = nullptr, *d_bars = nullptr;
   double *d_recgrad = nullptr, *d_grad = nullptr, *d_chi2 = nullptr, *d_c2part = nullptr, *d_step = nullptr;
   float4 *d_scratch = nullptr;
   int cap_npar = 0;
