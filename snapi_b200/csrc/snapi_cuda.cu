@@ -34,6 +34,13 @@ namespace {
 #define SNAPI_SYN_MINB (640 / SNAPI_CHUNK)
 #endif
 constexpr int kOpThreads = 256;  // k_adj_opacity: threads per CTA (depths; larger nd loops)
+// k_adj_opacity at <= 85 registers (3 x 256 threads per SM): 8 of its 96-thread CTAs per SM
+#ifndef SNAPI_OP_MINB
+#define SNAPI_OP_MINB 3
+#endif
+#ifndef SNAPI_RT_MINB
+#define SNAPI_RT_MINB 1
+#endif
 
 struct CtaPos {
   int pix, var, chunk, l, warp0, wslot;
@@ -109,7 +116,7 @@ __global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_adj_forward(KParams 
 
 // Adjoint, phase R1: reverse DELO sweep and optical-depth adjoint per wavelength (no opacity
 // work, no shared memory); writes (eta-bar, j-bar) of every depth.
-__global__ void __launch_bounds__(kChunk) k_adj_rt(KParams P) {
+__global__ void __launch_bounds__(kChunk, SNAPI_RT_MINB) k_adj_rt(KParams P) {
   const CtaPos c = cta_pos(P);
   if (c.warp0 >= P.nl) return;
   PixelView pv;
@@ -130,7 +137,7 @@ __global__ void __launch_bounds__(kChunk) k_adj_rt(KParams P) {
 // Adjoint, phase R2: opacity adjoint.  CTA = (pixel, group): group 0 the continuum, group 1 + j
 // transition j; one thread per depth walks every wavelength and keeps its sums in registers, so
 // the wavelength sums need no shuffles.  Wavelengths whose bars are all zero (masked) are skipped.
-__global__ void __launch_bounds__(kOpThreads) k_adj_opacity(KParams P) {
+__global__ void __launch_bounds__(kOpThreads, SNAPI_OP_MINB) k_adj_opacity(KParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const SmemLayout L = smem_layout(P.nd, P.nfield, P.nlines, P.ncomp, P.nred, false);
   const int ng = 1 + P.nlines;
