@@ -11,8 +11,8 @@
  *   (+ obs_stokes_responses, formal_pert_numerical)  atmos/atmos_rad_synthesis.cc:166-399,
  *                                              atmos/plpar/atmos_ppbez_rts.cc:1780-1857
  *       -> snapi_responses (forward mode), snapi_adjoint (reverse mode, chi2 gradient)
- *   atmosphere::stokes_lm_fit (one damped step)  atmos/atmos.h:300, atmos/atmos_fit.cc:93-205
- *       -> snapi_lm_step
+ *   atmosphere::stokes_lm_fit                  atmos/atmos.h:300, atmos/atmos_fit.cc:18-227
+ *       -> snapi_lm_begin / snapi_lm_step (one reference iteration) / snapi_lm_result
  *   atom::zeeman_setup                         atmos/atmol/atom/atom.cc:1620-1773
  *       -> snapi_zeeman_pattern
  *
@@ -120,6 +120,49 @@ int snapi_fd_grad(snapi_ctx *ctx, int npix, const float *records, const float *o
                   double *grad, int mem);
 
 /* Zeeman pattern of a transition, 2J values ju2 / jl2 and Lande factors (atom::zeeman_setup). */
+/* ---------------------------------------------------------------------------------------------
+ * Batched Levenberg-Marquardt node fit: stokes_lm_fit (atmos/atmos_fit.cc:18-227) for many pixels
+ * at once, each with its own damping, iteration count, mask and stop decision.  The node ->
+ * record map (build_from_nodes: interpolation, hydrostatic equilibrium, chemistry) stays with
+ * the caller; every step hands back the node vectors whose records and tangents the next step
+ * needs, so one step per reference iteration:
+ *   snapi_lm_begin(ctx, npix, &opts, nodes0, obs, w_stokes, mask, request, mem);
+ *   do { build records + tangents at request[p] for pixels with active[p];
+ *        snapi_lm_step(ctx, records, tangents, request, active, &n_active, mem); } while (n_active);
+ *   snapi_lm_result(ctx, nodes, chi2, iters, stokes, mem);
+ * Per pixel and step (atmos_fit.cc:93-205): synthesis at the trial nodes; chi2; accept (damping
+ * / sqrt(10), floor 1e-5, chi2 tracked, stop when the relative change of the last two tracked
+ * values is below delta) or reject (damping * sqrt(10)); on acceptance the Jacobian at the new
+ * nodes (snapi_responses on the given tangents); J scaled by T 5000 K, velocities 1e5 cm/s,
+ * B 1000 G, angles 1 (atmos_fit.cc:250-260), J^T J and J^T r in FP64, diagonal * (1 + damping),
+ * solution by the symmetric eigen-decomposition with singular values below max / 1e6 dropped
+ * (solve_svd, cmlib/mathtools.cc:344-390), correction added and bracketed to the node bounds
+ * (T 3400..12000 K, v_turb 1e2..1.5e6, v_los -1.5e6..1.5e6 cm/s, B 1..1e4 G,
+ * atmos_model.cc:12-19,957-977).  Angles are polished (acos cos, atan tan) in snapi_lm_result.
+ * chi2 here is sum(((obs - S) w_s mask)^2) / stokes_scale^2. */
+#define SNAPI_LM_MAX_PAR 32
+typedef struct {
+  int npar;                 /* nodes per pixel (<= SNAPI_LM_MAX_PAR) */
+  const int *node_kind;     /* [npar]: 1 T, 2 v_turb, 3 v_los, 4 B, 5 inclination, 6 azimuth */
+  double lm_start;          /* initial damping (observable start_lambda) */
+  int max_iter;             /* iterations (observable no_iterations) */
+  double delta;             /* relative chi2 change that ends the fit (atmos_fit.cc:16, 1e-3) */
+  double stopping_chisq;    /* chi2 below which the fit ends after one more step */
+  const double *resp_step;  /* [npar] central-difference steps of the Jacobian, node units */
+} snapi_lm_opts;
+
+/* nodes0, request: double [npix][npar]; obs float [npix][nlambda][4]; mask float [npix][nlambda]
+ * or NULL; w_stokes double [4] or NULL.  request receives the bracketed initial nodes. */
+int snapi_lm_begin(snapi_ctx *ctx, int npix, const snapi_lm_opts *opts, const double *nodes0, const float *obs,
+                   const double *w_stokes, const float *mask, double *request, int mem);
+/* records / tangents of the node vectors in request (rows of inactive pixels are ignored);
+ * request, active [npix] and *n_active are updated. */
+int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, double *request, int *active,
+                  int *n_active, int mem);
+/* fitted nodes [npix][npar], chi2 [npix], iterations [npix] and Stokes [npix][nlambda][4]
+ * (any may be NULL). */
+int snapi_lm_result(snapi_ctx *ctx, double *nodes, double *chi2, int *iters, float *stokes, int mem);
+
 int snapi_zeeman_pattern(int ju2, int jl2, double g_upper, double g_lower, snapi_line *line);
 
 /* Pinned host memory for SNAPI_MEM_HOST arguments. */

@@ -62,6 +62,18 @@ class SnapiProblem(ctypes.Structure):
     ]
 
 
+class SnapiLmOpts(ctypes.Structure):
+    _fields_ = [
+        ("npar", ctypes.c_int),
+        ("node_kind", ctypes.POINTER(ctypes.c_int)),
+        ("lm_start", ctypes.c_double),
+        ("max_iter", ctypes.c_int),
+        ("delta", ctypes.c_double),
+        ("stopping_chisq", ctypes.c_double),
+        ("resp_step", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
 _LIB = None
 
 
@@ -92,8 +104,9 @@ def lib():
         L.snapi_last_kernel_ms.argtypes = [vp]
         L.snapi_last_launches.restype = ip
         L.snapi_last_launches.argtypes = [vp]
-        if hasattr(L, "snapi_lm_step"):
-            L.snapi_lm_step.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, fp, fp, fp, ip]
+        L.snapi_lm_begin.argtypes = [vp, ip, ctypes.POINTER(SnapiLmOpts), fp, fp, fp, fp, fp, ip]
+        L.snapi_lm_step.argtypes = [vp, fp, fp, fp, fp, ctypes.POINTER(ctypes.c_int), ip]
+        L.snapi_lm_result.argtypes = [vp, fp, fp, fp, fp, ip]
         _LIB = L
     return _LIB
 
@@ -245,6 +258,63 @@ class Context:
         self._check(lib().snapi_fd_grad(self._ctx, npix, _ptr(rec), _ptr(ob), _ptr(ws), _ptr(mk), npar, _ptr(tn),
                                         _ptr(stp), _ptr(chi2), _ptr(grad), MEM_HOST))
         return {"chi2": chi2, "grad": grad}
+
+    # ---- batched Levenberg-Marquardt (stokes_lm_fit) ----------------------------------------
+    def lm_begin(self, nodes0, obs, node_kind, resp_step, mask=None, w_stokes=(1.0, 1.0, 1.0, 1.0), lm_start=1e3,
+                 max_iter=30, delta=1e-3, stopping_chisq=1e-30):
+        """Start a fit of every pixel; returns the (bracketed) node vectors to build first."""
+        n0 = np.ascontiguousarray(nodes0, dtype=np.float64)
+        npix, npar = n0.shape
+        ob = _f32(obs)
+        mk = None if mask is None else _f32(mask)
+        self._lm_kind = np.ascontiguousarray(node_kind, dtype=np.int32)
+        self._lm_step = np.ascontiguousarray(np.broadcast_to(resp_step, (npar,)), dtype=np.float64)
+        opts = SnapiLmOpts(npar, self._lm_kind.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), float(lm_start),
+                           int(max_iter), float(delta), float(stopping_chisq),
+                           self._lm_step.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
+        req = np.zeros_like(n0)
+        self._check(lib().snapi_lm_begin(self._ctx, npix, ctypes.byref(opts), _ptr(n0), _ptr(ob), _ptr(ws), _ptr(mk),
+                                         _ptr(req), MEM_HOST))
+        self._lm_shape = (npix, npar)
+        return req
+
+    def lm_step(self, records, tangents):
+        """One LM iteration for every active pixel, from the records / tangents of the node vectors
+        the previous call requested.  Returns (request, active, n_active)."""
+        rec = _f32(records)
+        tn = _f32(tangents)
+        req = np.zeros(self._lm_shape)
+        act = np.zeros(self._lm_shape[0], np.int32)
+        na = ctypes.c_int(0)
+        self._check(lib().snapi_lm_step(self._ctx, _ptr(rec), _ptr(tn), _ptr(req), _ptr(act), ctypes.byref(na),
+                                        MEM_HOST))
+        return req, act.astype(bool), na.value
+
+    def lm_result(self):
+        npix, npar = self._lm_shape
+        nodes = np.zeros((npix, npar))
+        chi2 = np.zeros(npix)
+        iters = np.zeros(npix, np.int32)
+        st = np.zeros((npix, self.nl, 4), np.float32)
+        self._check(lib().snapi_lm_result(self._ctx, _ptr(nodes), _ptr(chi2), _ptr(iters), _ptr(st), MEM_HOST))
+        return {"nodes": nodes, "chi2": chi2, "iters": iters, "stokes": st}
+
+    def lm_fit(self, nodes0, obs, builder, node_kind, resp_step, **kw):
+        """Run the fit to the end.  builder(nodes [n, npar], active [n] bool) returns (records,
+        tangents) for all n rows (rows of inactive pixels may hold anything)."""
+        req = self.lm_begin(nodes0, obs, node_kind, resp_step, **kw)
+        active = np.ones(req.shape[0], bool)
+        steps = 0
+        while True:
+            rec, tan = builder(req, active)
+            req, active, n = self.lm_step(rec, tan)
+            steps += 1
+            if n == 0:
+                break
+        out = self.lm_result()
+        out["steps"] = steps
+        return out
 
     def responses(self, records, tangents, step, want_stokes=True):
         """d Stokes / d node [npix, npar, nlambda, 4] (obs_stokes_responses_to_nodes, batched) by

@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_synth(KParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const SmemLayout L = smem_layout(P.nd, P.nfield, P.nlines, P.ncomp, P.nred, false);
   const CtaPos c = cta_pos(P);
+  if (P.skip && P.skip[c.pix]) return;  // CTA-uniform
   PixelView pv;
   if (!stage_pixel(P, c.pix, smem, L, pv, -1, 0.f)) return;
   if (c.warp0 >= P.nl) return;  // warp-uniform: no wavelength left for this warp
@@ -272,6 +273,7 @@ __global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_resp_sweep(KParams P
   extern __shared__ __align__(16) unsigned char smem[];
   const SmemLayout L = smem_layout(P.nd, P.nfield, P.nlines, P.ncomp, P.nred, false);
   const CtaPos c = cta_pos(P);  // var = node index
+  if (P.skip && P.skip[c.pix]) return;  // CTA-uniform
   float plus[4], out[4];
   for (int side = 0; side < 2; ++side) {
     PixelView pv;
@@ -312,6 +314,21 @@ int stage_in(snapi_ctx *ctx, const T *src, T *dbuf, size_t n, int mem, const T *
 }
 
 int sweep_ctas(const snapi_ctx *ctx, int nb, int nvar = 1) { return nb * nvar * ctx->nchunk; }
+
+}  // namespace
+
+cudaError_t snapi::launch_synth(const snapi_ctx *ctx, const KParams &P) {
+  const SmemLayout L = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false);
+  k_synth<<<P.npix * ctx->nchunk, kChunk, L.total, ctx->stream>>>(P);
+  return cudaGetLastError();
+}
+cudaError_t snapi::launch_responses(const snapi_ctx *ctx, const KParams &P) {
+  const SmemLayout L = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false);
+  k_resp_sweep<<<P.npix * P.nvar * ctx->nchunk, kChunk, L.total, ctx->stream>>>(P);
+  return cudaGetLastError();
+}
+
+namespace {
 
 // the adjoint's kernel sequence for nb pixels (P.npix = nb)
 constexpr int kAdjointLaunches = 4;
@@ -458,6 +475,7 @@ void snapi_destroy(snapi_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  lm_free(ctx);
   void *bufs[] = {ctx->d_lamvac, ctx->d_D, ctx->d_lines, ctx->d_compS, ctx->d_compD, ctx->d_status,
                   ctx->d_rec, ctx->d_stokes, ctx->d_obs, ctx->d_mask, ctx->d_tan, ctx->d_recgrad,
                   ctx->d_dstokes, ctx->d_opart, ctx->d_seed, ctx->d_bars, ctx->d_grad, ctx->d_chi2, ctx->d_c2part, ctx->d_step,

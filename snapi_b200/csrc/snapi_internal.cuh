@@ -53,6 +53,7 @@ struct KParams {
   double *chi2;                 // [npix]
   float *dstokes;               // [npix][npar][nl][4] (responses)
   const double *fd_step;        // [npar]
+  const int *skip;              // [npix] or null: pixels whose CTAs return at once (LM)
   int *status;                  // device error word
 };
 
@@ -289,6 +290,10 @@ int set_err(snapi_ctx *c, int code, const char *fmt, ...);
 int ensure_npar(snapi_ctx *ctx, int npar);
 KParams base_params(const snapi_ctx *ctx);
 int check_status(snapi_ctx *ctx);
+// sweep launches for other translation units (P.npix pixels; P.nvar nodes for the responses)
+cudaError_t launch_synth(const snapi_ctx *ctx, const KParams &P);
+cudaError_t launch_responses(const snapi_ctx *ctx, const KParams &P);
+void lm_free(snapi_ctx *ctx);  // LM work buffers (snapi_lm.cu)
 }  // namespace snapi
 
 #define SNAPI_CK(call)                                                                                  \

@@ -36,6 +36,11 @@ def config3():
 
 
 @pytest.fixture(scope="session")
+def config4():
+    return load_fixture("config4")
+
+
+@pytest.fixture(scope="session")
 def oracle_lib():
     from snapi_b200 import build as b
     b.build_oracle() if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libsnapi_oracle.so")) else None

@@ -39,6 +39,7 @@ CFG_FILES = ["atoms_6300.cfg", "mol.cfg", "hydrogen_3lvl.cfg", "helium.cfg", "ca
              "oxygen.cfg", "calcium.cfg", "silicon.cfg", "aluminium.cfg", "iron_6300.cfg", "falc_80z.dat"]
 
 ND = 80
+NLAMBDA = 201
 LOGTAU = np.linspace(-6.0, 1.0, ND)
 
 
@@ -169,6 +170,58 @@ def config3_nodes(npix, seed=3):
     return nodes
 
 
+C4_OFFSET = np.array([200.0, 200.0, 200.0, 200.0, 3.0e4, 3.0e4, 3.0e4, 200.0, 0.1, 0.1])
+
+
+def config4_inputs(npix, seed=4):
+    """Config-4 LM problem: truth nodes (config-3 model, seed 4), initial guess = truth + fixed
+    offsets (T +200 K, velocities +0.3 km/s, B +200 G, angles +0.1 rad) and per-pixel masks keeping
+    120..201 of the 201 wavelengths (a random contiguous window, then random single drops)."""
+    truth = config3_nodes(npix, seed=seed)
+    rng = np.random.default_rng(seed + 40)
+    mask = np.zeros((npix, NLAMBDA))
+    for i in range(npix):
+        keep = int(rng.integers(120, 202))
+        width = min(NLAMBDA, keep + int(rng.integers(0, 20)))
+        start = int(rng.integers(0, NLAMBDA - width + 1))
+        m = np.zeros(NLAMBDA)
+        m[start:start + width] = 1.0
+        on = np.flatnonzero(m)
+        drop = rng.choice(on, size=max(0, on.size - keep), replace=False)
+        m[drop] = 0.0
+        mask[i] = m
+    return truth, truth + C4_OFFSET, mask
+
+
+def make_config4(tmp, npix, iters=30):
+    """Reference LM (stokes_lm_fit, DELTA 1e-3 as compiled, start lambda 1e3) on config-4 pixels,
+    one process per pixel."""
+    task = os.path.join(tmp, "c3.tsk")
+    truth, nodes0, mask = config4_inputs(npix)
+    d = dump(tmp, task, truth, 0, "c4truth")
+    rng = np.random.default_rng(44)
+    ic = d["stokes"][:, :, 0].max(axis=1)
+    target = d["stokes"] + rng.normal(0.0, 1e-3, d["stokes"].shape) * ic[:, None, None]
+    procs = []
+    for i in range(npix):
+        for nm, arr in (("n0", nodes0[i:i + 1]), ("tg", target[i:i + 1]), ("mk", mask[i:i + 1])):
+            np.ascontiguousarray(arr, dtype="<f8").tofile(os.path.join(tmp, "c4_%s_%d.f64" % (nm, i)))
+        args = [DUMP, "lmfit", task] + [os.path.join(tmp, "c4_%s_%d.f64" % (nm, i)) for nm in ("n0", "tg", "mk")] + \
+               ["1", str(iters), os.path.join(tmp, "c4_fit_%d.sbin" % i)]
+        procs.append(subprocess.Popen(args, cwd=tmp, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+    for p in procs:
+        if p.wait() != 0:
+            raise RuntimeError("lmfit failed")
+    fits = [read_sbin(os.path.join(tmp, "c4_fit_%d.sbin" % i)) for i in range(npix)]
+    np.savez_compressed(os.path.join(HERE, "config4.npz"), lambda_air=d["lambda_air"], tau500=d["tau500"],
+                        node_kind=d["node_kind"], truth=truth, nodes0=nodes0, mask=mask, target=target,
+                        fit_nodes=np.concatenate([f["fit_nodes"] for f in fits]),
+                        fit_stokes=np.concatenate([f["fit_stokes"] for f in fits]),
+                        fit_chi2=np.concatenate([f["fit_chi2"] for f in fits]),
+                        ref_seconds_per_pixel=np.array([np.mean([f["ref_seconds_per_pixel"][0] for f in fits])]),
+                        iters=np.array([iters]), **line_arrays(d))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -176,6 +229,8 @@ def main():
     ap.add_argument("--c3pix", type=int, default=8)
     ap.add_argument("--pool", type=int, default=32)
     ap.add_argument("--only-pool", action="store_true")
+    ap.add_argument("--only-c4", action="store_true")
+    ap.add_argument("--c4pix", type=int, default=8)
     a = ap.parse_args()
     if not os.path.exists(DUMP):
         raise SystemExit("build the oracle first: make -C oracle")
@@ -183,11 +238,13 @@ def main():
     try:
         for f in CFG_FILES:
             shutil.copy(os.path.join(a.ref, "cfg", f), tmp)
-        if a.only_pool:
+        if a.only_pool or a.only_c4:
             shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
         else:
             make_configs_1_to_3(a, tmp)
-        if a.pool:
+        if a.c4pix:
+            make_config4(tmp, a.c4pix)
+        if a.pool and not a.only_c4:
             n4 = config3_nodes(a.pool, seed=303)
             d4 = dump(tmp, os.path.join(tmp, "c3.tsk"), n4, 2, "pool")
             np.savez_compressed(os.path.join(HERE, "bench_pool.npz"), lambda_air=d4["lambda_air"],

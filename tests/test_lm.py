@@ -1,0 +1,76 @@
+"""Batched Levenberg-Marquardt fit (snapi_lm_begin / snapi_lm_step / snapi_lm_result) against the
+reference's stokes_lm_fit (config-4 pixels: uneven wavelength masks, 10 nodes, noisy targets)."""
+import numpy as np
+import pytest
+
+from helpers import emu_lines, node_scales
+from ref_builder import LinearBuilder, RefBuilder, ref_builder_available
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sb():
+    import snapi_b200
+    from snapi_b200 import build as b
+    b.build_cuda()
+    return snapi_b200
+
+
+def _ic(fx):
+    return float(np.abs(fx["target"][:, :, 0]).max())
+
+
+def test_lm_linear_nodes_recovers_truth(sb, oracle_lib, config3):
+    """Fit v_turb, v_los x2, B, inclination, azimuth (records exactly linear in them) from offset
+    starting values; the fit reaches the noise level and the FP64 oracle agrees on its chi2."""
+    fx = config3
+    sel = np.arange(4, 10)
+    truth = fx["nodes"][:, sel]
+    kinds = fx["node_kind"][sel]
+    offs = np.array([3e4, 3e4, 3e4, 200.0, 0.1, 0.1])
+    n0 = truth + offs
+    tan = fx["tangent"][:, sel]
+    build = LinearBuilder(fx["record"], tan, truth)
+    ic = _ic(fx)
+    ctx = sb.Context.from_fixture(fx, stokes_scale=ic)
+    out = ctx.lm_fit(n0, fx["target"], build, kinds, 1e-2 * node_scales(kinds), lm_start=1e3, max_iter=30,
+                     delta=1e-3)
+    ctx.close()
+    npix, nl = fx["target"].shape[:2]
+    noise = (1e-3 * fx["stokes"][:, :, 0].max(axis=1) / ic) ** 2 * 4 * nl
+    assert np.all(out["chi2"] < 1.5 * noise), out["chi2"] / noise
+    assert np.all(np.abs(out["nodes"][:, 3] - truth[:, 3]) < 20.0)  # B [G]
+    # the FP64 oracle at the fitted nodes gives the same chi2
+    lines = emu_lines(oracle_lib, fx)
+    rec, _ = build(out["nodes"], np.ones(npix, bool))
+    s64 = oracle_lib.synth(fx["lambda_air"], fx["tau500"], rec.astype(np.float64), lines)
+    c64 = (((fx["target"] - s64) / ic) ** 2).sum(axis=(1, 2))
+    np.testing.assert_allclose(out["chi2"], c64, rtol=2e-3)
+
+
+@pytest.mark.skipif(not ref_builder_available(), reason="reference builder (oracle/_ref) not built")
+def test_lm_matches_reference_fit(sb, config4):
+    """Same starting nodes, targets and masks as the reference's stokes_lm_fit run (DELTA 1e-3,
+    start damping 1e3, 30 iterations).  The device fit reaches a chi2 at least as low as the
+    reference's (measured 3-13 % lower: the reference stops on DELTA while its semi-analytic
+    responses, 0.1-5 % off the exact derivative, still slow its steps) and the same nodes within a
+    fraction of their noise-limited spread."""
+    fx = config4
+    ic = _ic(fx)
+    kinds = fx["node_kind"]
+    ctx = sb.Context.from_fixture(fx, stokes_scale=ic)
+    out = ctx.lm_fit(fx["nodes0"], fx["target"], RefBuilder(), kinds, 1e-2 * node_scales(kinds),
+                     mask=fx["mask"], lm_start=1e3, max_iter=int(fx["iters"][0]), delta=1e-3)
+    ctx.close()
+    ours = out["chi2"] * ic * ic
+    ref = fx["fit_chi2"]
+    print("chi2 ours / reference:", ours / ref, "iterations", out["iters"], "steps", out["steps"])
+    print("node differences:", np.round(out["nodes"] - fx["fit_nodes"], 3))
+    assert np.all(ours / ref < 1.01) and np.all(ours / ref > 0.8)
+    d = out["nodes"] - fx["fit_nodes"]
+    d[:, 9] = (d[:, 9] + np.pi / 2) % np.pi - np.pi / 2  # azimuth is defined modulo pi
+    assert np.all(np.abs(d[:, :4]) < 80.0)           # T nodes [K]
+    assert np.all(np.abs(d[:, 4:7]) < 5e3)           # velocities [cm/s]
+    assert np.all(np.abs(d[:, 7]) < 10.0)            # B [G]
+    assert np.all(np.abs(d[:, 8:10]) < 0.02)         # angles [rad]
