@@ -221,9 +221,10 @@ class Context:
         return out
 
     def adjoint(self, records, obs, tangents=None, w_stokes=(1.0, 1.0, 1.0, 1.0), mask=None, want_stokes=True,
-                want_rec_grad=False):
+                want_rec_grad=False, out=None):
         """chi2 [npix], d chi2/d node [npix, npar] (and Stokes, d chi2 / d record) by one forward and
-        one reverse sweep."""
+        one reverse sweep.  out: optional dict of preallocated "stokes" / "chi2" / "grad" arrays
+        (e.g. page-locked from snapi_host_alloc) that receive the results."""
         rec = _f32(records)
         npix = self._npix(rec)
         ob = _f32(obs)
@@ -231,18 +232,22 @@ class Context:
         npar = 0 if tn is None else tn.shape[1]
         mk = _f32(mask)
         ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
-        st = np.zeros((npix, self.nl, 4), np.float32) if want_stokes else None
-        chi2 = np.zeros(npix)
-        grad = np.zeros((npix, max(npar, 1)))
+        out = out or {}
+        st = out.get("stokes", np.zeros((npix, self.nl, 4), np.float32)) if want_stokes else None
+        chi2 = out.get("chi2", np.zeros(npix))
+        grad = out.get("grad", np.zeros((npix, max(npar, 1))))
+        assert st is None or (st.dtype == np.float32 and st.flags.c_contiguous and st.size == npix * self.nl * 4)
+        assert chi2.dtype == np.float64 and chi2.size == npix and grad.dtype == np.float64
+        assert grad.flags.c_contiguous and grad.size >= npix * max(npar, 1)
         rg = np.zeros((npix, self.nd, self.nfield)) if want_rec_grad else None
         self._check(lib().snapi_adjoint(self._ctx, npix, _ptr(rec), _ptr(ob), _ptr(ws), _ptr(mk), npar, _ptr(tn),
                                         _ptr(st), _ptr(chi2), _ptr(grad), _ptr(rg), MEM_HOST))
-        out = {"chi2": chi2, "grad": grad[:, :npar]}
+        res = {"chi2": chi2, "grad": grad.reshape(npix, -1)[:, :npar]}
         if want_stokes:
-            out["stokes"] = st
+            res["stokes"] = st
         if want_rec_grad:
-            out["rec_grad"] = rg
-        return out
+            res["rec_grad"] = rg
+        return res
 
     def fd_grad(self, records, obs, tangents, step, w_stokes=(1.0, 1.0, 1.0, 1.0), mask=None):
         rec = _f32(records)

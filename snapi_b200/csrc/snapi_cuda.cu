@@ -475,6 +475,7 @@ void snapi_destroy(snapi_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   lm_free(ctx);
   void *bufs[] = {ctx->d_lamvac, ctx->d_D, ctx->d_lines, ctx->d_compS, ctx->d_compD, ctx->d_status,
                   ctx->d_rec, ctx->d_stokes, ctx->d_obs, ctx->d_mask, ctx->d_tan, ctx->d_recgrad,
@@ -485,6 +486,11 @@ void snapi_destroy(snapi_ctx *ctx) {
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  for (int h = 0; h < 2; ++h) {
+    if (ctx->ev_copy[h]) cudaEventDestroy(ctx->ev_copy[h]);
+    if (ctx->ev_free[h]) cudaEventDestroy(ctx->ev_free[h]);
+  }
   delete ctx;
 }
 
@@ -576,6 +582,11 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
     }                                                                                    \
   } while (0)
   CKC(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  CKC(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  for (int h = 0; h < 2; ++h) {
+    CKC(cudaEventCreateWithFlags(&ctx->ev_copy[h], cudaEventDisableTiming));
+    CKC(cudaEventCreateWithFlags(&ctx->ev_free[h], cudaEventDisableTiming));
+  }
   CKC(cudaEventCreate(&ctx->ev0));
   CKC(cudaEventCreate(&ctx->ev1));
   CKC(cudaMalloc(&ctx->d_lamvac, sizeof(double) * ctx->nl));
@@ -659,52 +670,81 @@ int snapi_adjoint(snapi_ctx *ctx, int npix, const float *records, const float *o
   SNAPI_CK(cudaSetDevice(ctx->device));
   int st = ensure_npar(ctx, npar > 0 ? npar : 1);
   if (st) return st;
-  const size_t nrec = (size_t)ctx->nd * ctx->nfield;
+  const size_t nrec = (size_t)ctx->nd * ctx->nfield, nl4 = (size_t)ctx->nl * 4;
   const SmemLayout Lsw = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false);
   const SmemLayout Lfin = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, true);
   ctx->last_ms = 0.0;
   ctx->last_launches = 0;
-  for (int p0 = 0; p0 < npix; p0 += ctx->max_batch) {
-    const int nb = std::min(ctx->max_batch, npix - p0);
-    KParams P = base_params(ctx);
-    P.npix = nb;
-    P.npar = npar;
-    for (int s = 0; s < 4; ++s) P.ws[s] = w_stokes ? w_stokes[s] : 1.0;
-    const float *rec, *ob, *mk, *tn;
-    if ((st = stage_in(ctx, records + p0 * nrec, ctx->d_rec, nb * nrec, mem, &rec))) return st;
-    if ((st = stage_in(ctx, obs + (size_t)p0 * ctx->nl * 4, ctx->d_obs, (size_t)nb * ctx->nl * 4, mem, &ob))) return st;
-    if ((st = stage_in(ctx, mask ? mask + (size_t)p0 * ctx->nl : nullptr, ctx->d_mask, (size_t)nb * ctx->nl, mem, &mk)))
-      return st;
-    if ((st = stage_in(ctx, npar ? tangents + (size_t)p0 * npar * nrec : nullptr, ctx->d_tan, (size_t)nb * npar * nrec,
-                       mem, &tn)))
-      return st;
-    P.rec = rec; P.obs = ob; P.mask = mk; P.tangent = tn;
-    const bool dev = mem == SNAPI_MEM_DEVICE;
-    P.stokes = stokes ? (dev ? stokes + (size_t)p0 * ctx->nl * 4 : ctx->d_stokes) : nullptr;
-    P.chi2 = dev ? chi2 + p0 : ctx->d_chi2;
-    P.grad = npar ? (dev ? grad + (size_t)p0 * npar : ctx->d_grad) : ctx->d_grad;
-    P.rec_grad = rec_grad ? (dev ? rec_grad + (size_t)p0 * nrec : ctx->d_recgrad) : nullptr;
-    SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    launch_adjoint(P, nb, ctx->nchunk, Lsw.total, Lfin.total, ctx->stream);
-    SNAPI_CK(cudaGetLastError());
-    SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    ctx->last_launches += kAdjointLaunches;
+  const bool dev = mem == SNAPI_MEM_DEVICE;
+  // Host inputs: each round of up to max_batch pixels goes in chunks that alternate between the
+  // two halves of the staging buffers; chunk k+1 is copied on the copy stream while chunk k
+  // computes, so the host->device traffic (the tangents dominate it) hides under the kernels.
+  // Outputs of a round come back after its last chunk.  (Overlap needs page-locked host inputs,
+  // e.g. from snapi_host_alloc; pageable copies serialise with the host thread.)
+  const int half = std::max(1, ctx->max_batch / 2);
+  const int chunk = dev ? ctx->max_batch : std::min(half, std::max(1, (std::min(npix, ctx->max_batch) + 3) / 4));
+  int k = 0;
+  for (int r0 = 0; r0 < npix; r0 += ctx->max_batch) {
+    const int nr = std::min(ctx->max_batch, npix - r0);
+    for (int p0 = r0; p0 < r0 + nr; p0 += chunk, ++k) {
+      const int nb = std::min(chunk, r0 + nr - p0), lo = p0 - r0;  // lo: offset within the round
+      KParams P = base_params(ctx);
+      P.npix = nb;
+      P.npar = npar;
+      for (int s = 0; s < 4; ++s) P.ws[s] = w_stokes ? w_stokes[s] : 1.0;
+      const int h = ctx->max_batch >= 2 ? (k & 1) : 0;  // one pixel of staging: no second half
+      if (dev) {
+        P.rec = records + p0 * nrec;
+        P.obs = obs + (size_t)p0 * nl4;
+        P.mask = mask ? mask + (size_t)p0 * ctx->nl : nullptr;
+        P.tangent = npar ? tangents + (size_t)p0 * npar * nrec : nullptr;
+      } else {
+        const size_t off = (size_t)h * half;
+        float *drec = ctx->d_rec + off * nrec, *dobs = ctx->d_obs + off * nl4, *dmask = ctx->d_mask + off * ctx->nl;
+        float *dtan = ctx->d_tan + off * (size_t)(npar ? npar : 1) * nrec;
+        cudaStream_t cs = ctx->copy_stream;
+        SNAPI_CK(cudaStreamWaitEvent(cs, ctx->ev_free[h], 0));  // chunk k-2 is done with this half
+        SNAPI_CK(cudaMemcpyAsync(drec, records + p0 * nrec, sizeof(float) * nb * nrec, cudaMemcpyHostToDevice, cs));
+        SNAPI_CK(cudaMemcpyAsync(dobs, obs + (size_t)p0 * nl4, sizeof(float) * nb * nl4, cudaMemcpyHostToDevice, cs));
+        if (mask)
+          SNAPI_CK(cudaMemcpyAsync(dmask, mask + (size_t)p0 * ctx->nl, sizeof(float) * nb * ctx->nl,
+                                   cudaMemcpyHostToDevice, cs));
+        if (npar)
+          SNAPI_CK(cudaMemcpyAsync(dtan, tangents + (size_t)p0 * npar * nrec, sizeof(float) * nb * npar * nrec,
+                                   cudaMemcpyHostToDevice, cs));
+        SNAPI_CK(cudaEventRecord(ctx->ev_copy[h], cs));
+        SNAPI_CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_copy[h], 0));
+        P.rec = drec; P.obs = dobs; P.mask = mask ? dmask : nullptr; P.tangent = npar ? dtan : nullptr;
+      }
+      P.stokes = stokes ? (dev ? stokes + (size_t)p0 * nl4 : ctx->d_stokes + (size_t)lo * nl4) : nullptr;
+      P.chi2 = dev ? chi2 + p0 : ctx->d_chi2 + lo;
+      P.grad = npar ? (dev ? grad + (size_t)p0 * npar : ctx->d_grad + (size_t)lo * npar) : ctx->d_grad;
+      P.rec_grad = rec_grad ? (dev ? rec_grad + (size_t)p0 * nrec : ctx->d_recgrad + (size_t)lo * nrec) : nullptr;
+      if (k == 0) SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+      launch_adjoint(P, nb, ctx->nchunk, Lsw.total, Lfin.total, ctx->stream);
+      SNAPI_CK(cudaGetLastError());
+      ctx->last_launches += kAdjointLaunches;
+      if (!dev) SNAPI_CK(cudaEventRecord(ctx->ev_free[h], ctx->stream));
+    }
     if (!dev) {
       if (stokes)
-        SNAPI_CK(cudaMemcpyAsync(stokes + (size_t)p0 * ctx->nl * 4, ctx->d_stokes, sizeof(float) * nb * ctx->nl * 4,
+        SNAPI_CK(cudaMemcpyAsync(stokes + (size_t)r0 * nl4, ctx->d_stokes, sizeof(float) * nr * nl4,
                                  cudaMemcpyDeviceToHost, ctx->stream));
-      SNAPI_CK(cudaMemcpyAsync(chi2 + p0, ctx->d_chi2, sizeof(double) * nb, cudaMemcpyDeviceToHost, ctx->stream));
+      SNAPI_CK(cudaMemcpyAsync(chi2 + r0, ctx->d_chi2, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
       if (npar)
-        SNAPI_CK(cudaMemcpyAsync(grad + (size_t)p0 * npar, ctx->d_grad, sizeof(double) * nb * npar,
+        SNAPI_CK(cudaMemcpyAsync(grad + (size_t)r0 * npar, ctx->d_grad, sizeof(double) * nr * npar,
                                  cudaMemcpyDeviceToHost, ctx->stream));
       if (rec_grad)
-        SNAPI_CK(cudaMemcpyAsync(rec_grad + (size_t)p0 * nrec, ctx->d_recgrad, sizeof(double) * nb * nrec,
+        SNAPI_CK(cudaMemcpyAsync(rec_grad + (size_t)r0 * nrec, ctx->d_recgrad, sizeof(double) * nr * nrec,
                                  cudaMemcpyDeviceToHost, ctx->stream));
     }
+  }
+  if (npix > 0) {
+    SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
     SNAPI_CK(cudaStreamSynchronize(ctx->stream));
     float ms = 0.f;
     SNAPI_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-    ctx->last_ms += ms;
+    ctx->last_ms = ms;  // first kernel start to the end of the last chunk (host copies included)
   }
   return check_status(ctx);
 }
