@@ -13,6 +13,8 @@
  *       -> snapi_responses (forward mode), snapi_adjoint (reverse mode, chi2 gradient)
  *   atmosphere::stokes_lm_fit                  atmos/atmos.h:300, atmos/atmos_fit.cc:18-227
  *       -> snapi_lm_begin / snapi_lm_step (one reference iteration) / snapi_lm_result
+ *   atmosphere::nltepops                       atmos/atmos.h, atmos/atmos_pop.cc:67-240
+ *       -> snapi_ali_create / snapi_ali_iter
  *   atom::zeeman_setup                         atmos/atmol/atom/atom.cc:1620-1773
  *       -> snapi_zeeman_pattern
  *
@@ -162,6 +164,61 @@ int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, d
 /* fitted nodes [npix][npar], chi2 [npix], iterations [npix] and Stokes [npix][nlambda][4]
  * (any may be NULL). */
 int snapi_lm_result(snapi_ctx *ctx, double *nodes, double *chi2, int *iters, float *stokes, int mem);
+
+/* ---------------------------------------------------------------------------------------------
+ * NLTE level populations: the accelerated lambda iteration of atmosphere::nltepops
+ * (atmos/atmos_pop.cc:67-240) for one NLTE atom in many 1-D columns.  Per iteration and column:
+ * for every ray and wavelength of the NLTE grid the scalar formal solution with its diagonal
+ * operator (atmos_ppbez::formal, atmos/plpar/atmos_ppbez_rts.cc:21-219: Bezier optical depth with
+ * monotone derivatives, linear short characteristics, Taylor branch below 1e-2) of background +
+ * active opacity; the profile-weighted mean intensities and operators of every transition
+ * (atom::add, atmos/atmol/atom/atom.cc:1865-1927); per depth the rate equations with the local
+ * operator (atom::newpops, atom_pop.cc:27-145; R_ij_local_ALO, R_i_cont, R_cont_i, atom_rad.cc:
+ * 1732-1901), the most populated level replaced by particle conservation, an LU solve in FP64;
+ * the maximum relative change; negative populations -> the same step without the operator, and
+ * the column stops with status -1 if they stay negative (atmos_pop.cc:185-210).
+ * Everything that does not depend on the NLTE populations comes from the caller (the reference's
+ * own set-up in islave): the wavelength grid (atom::getlambda) and weights, the rays
+ * (anglesetup), the LTE background opacity / emissivity per ray and wavelength, the collisional
+ * rates per depth, Doppler widths and damping per line, the bound-free cross sections. */
+typedef struct {
+  int nd, nlambda, nray, nlevel, ntrans;
+  const double *grid;       /* [nd] coordinate of the formal solution (-tau500, top first) */
+  const double *lambda;     /* [nlambda] NLTE wavelength grid [cm] */
+  const double *lambda_w;   /* [nlambda] wavelength integration weights */
+  const double *fudge;      /* [nlambda] bound-free opacity fudge factor */
+  const double *ray_theta;  /* [nray] ray angles [rad] (theta > pi/2: outgoing) */
+  const double *ray_w;      /* [nray] angular weights */
+  const int *trans;         /* [ntrans][2]: lower, upper level; a transition whose upper level is
+                               a continuum (cont_of[lower] == upper) is bound-free */
+  const double *line_c;     /* [ntrans][4] for lines: lambda0 [cm], A_ul, B_lu, B_ul */
+  const double *line_e;     /* [ntrans] E_upper - E_lower [erg] (lines) */
+  const double *A, *B;      /* [nlevel][nlevel] Einstein coefficients from -> to (same stage) */
+  const int *stage;         /* [nlevel] ionisation stage of each level */
+  const int *cont_of;       /* [nlevel] level index of the continuum of each level, -1 if none */
+  const double *sigma;      /* [ntrans][nlambda] bound-free cross sections (rows of bf transitions) */
+} snapi_ali_problem;
+
+typedef struct {            /* per column; lines / bf transitions in transition order */
+  const double *T, *ne, *na, *kappa;  /* [ncol][nd]: temperature, electrons, atom total, kappa_500 */
+  const double *vray;                 /* [ncol][nray][nd] velocity projected on each ray [cm/s] */
+  const double *dld, *adamp;          /* [ncol][nline][nd] Doppler width [cm], damping parameter */
+  const double *bfratio;              /* [ncol][nbf][nd] n_e saha T^-1.5 g_i/g_c exp((ip-E_i)/kT) */
+  const double *coll;                 /* [ncol][nd][nlevel][nlevel] collisional rate from -> to */
+  const double *bg_op, *bg_em;        /* [ncol][nray][nlambda][nd] LTE background */
+} snapi_ali_columns;
+
+typedef struct snapi_ali_ctx snapi_ali_ctx;
+snapi_ali_ctx *snapi_ali_create(const snapi_ali_problem *prob, int device, int *status);
+void snapi_ali_destroy(snapi_ali_ctx *ctx);
+const char *snapi_ali_last_error(const snapi_ali_ctx *ctx);
+/* Iterates every column (pops [ncol][nd][nlevel] in: starting populations, out: result) until
+ * its maximum relative change falls below tol or max_iter iterations; rel_change [ncol], iters
+ * [ncol], status [ncol] (0 converged or stopped at max_iter, -1 negative populations) may be
+ * NULL.  Host arrays (SNAPI_MEM_HOST) or device arrays (SNAPI_MEM_DEVICE). */
+int snapi_ali_iter(snapi_ali_ctx *ctx, int ncol, const snapi_ali_columns *cols, double *pops, int max_iter,
+                   double tol, double *rel_change, int *iters, int *status, int mem);
+double snapi_ali_last_kernel_ms(const snapi_ali_ctx *ctx);
 
 int snapi_zeeman_pattern(int ju2, int jl2, double g_upper, double g_lower, snapi_line *line);
 

@@ -12,6 +12,9 @@
 //       reference's own steps) and the reference's normalised opacity at a few wavelengths.
 //   snapi_ref_dump lmfit  <task.tsk> <nodes0.f64> <target.f64> <mask.f64> <npix> <iters> <out.sbin>
 //       Run stokes_lm_fit per pixel from the initial nodes against target Stokes.
+//   snapi_ref_dump ali    <task.tsk> <nodes.f64> <ncol> <niter> <out.sbin>
+//       NLTE level-population iteration inputs, niter iterations of the reference's loop, and the
+//       populations nltepops converges to (see do_ali).
 //
 // flags: 1 = responses, 2 = tangents, 4 = opacity probe (pixel 0 only)
 //
@@ -448,10 +451,245 @@ static int do_lmfit(const char *tskname, const char *n0name, const char *tgtname
   return 0;
 }
 
+// ----------------------------------------------------------------------------------------------
+// ali: inputs and per-iteration populations of the NLTE level-population iteration
+// (atmosphere::nltepops, atmos/atmos_pop.cc:67-240) for each column built from the nodes.
+// The iteration body is the reference's own: opacity_active_only + formal (scalar, with the
+// diagonal operator) + atom::add + atmosphere::newpops, run niter times; then a fresh copy of
+// the column runs nltepops() itself to convergence.
+static int do_ali(const char *tskname, const char *nodesname, int ncol, int niter, const char *outname) {
+  const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
+  const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
+  int ac = 4; cmdln cmd(ac, (char **)argv, options, maps);
+  io_class io(cmd);
+  Task t = load_task(tskname);
+  std::vector<uint8_t> nb = read_file_bytes(nodesname);
+  const double *nodes = (const double *)nb.data();
+  model *m = task_model(t, io);
+  const int np = m->get_N_nodes_total();
+  std::vector<double> oT, oNe, oNa, oKap, oGrid, oLam, oLw, oFudge, oTh, oBin, oVr, oDld, oAd, oSig, oBfr, oColl,
+      oBgop, oBgem, oPop0, oPopIt, oRel, oPopConv, oTr, oTrc, oA, oB, oWall;
+  int nd = 0, nlam = 0, ntp = 0, nmap = 0, nline = 0, nbf = 0;
+  for (int ic = 0; ic < ncol; ++ic) {
+    atmosphere *a = task_atmos(t, io);
+    set_nodes(m, nodes + ic * np);
+    a->build_from_nodes(m);
+    const int x3l = a->x3l, x3h = a->x3h;
+    nd = x3h - x3l + 1;
+    a->set_grid(a->tau_grid);
+    a->boundary_condition_for_rt = -1;
+    a->popsetup();
+    a->compute_op_referent();
+    // nltepops prologue (atmos_pop.cc:70-130)
+    a->ltepops();
+    fp_t *lambda = 0;
+    int32_t nlambda = 0;
+    for (int i = 0; i < a->natm; ++i) a->atml[i]->rtsetup(a->x1l, a->x1h, a->x2l, a->x2h, x3l, x3h);
+    for (int i = 0; i < a->natm; ++i)
+      lambda = a->atml[i]->getlambda(lambda, nlambda, a->T[1][1][x3h], a->Nt[1][1][x3h], a->Ne[1][1][x3h]);
+    fp_t *th, *ph;
+    fp_t *bin = a->anglesetup(th, ph, ntp);
+    std::vector<double> lw(nlambda);
+    if (nlambda >= 2) {
+      lw[0] = (lambda[1] - lambda[0]) * 0.5;
+      lw[nlambda - 1] = (lambda[nlambda - 1] - lambda[nlambda - 2]) * 0.5;
+      for (int l = 1; l < nlambda - 1; ++l) lw[l] = (lambda[l + 1] - lambda[l - 1]) * 0.5;
+    } else if (nlambda) {
+      lw[0] = 1.0;
+    }
+    if (a->tau_grid) a->compute_op_referent();
+    for (int i = 0; i < a->natm; ++i) a->atml[i]->compute_active_population(a->T, a->Ne);
+    atom *at = 0;
+    for (int i = 0; i < a->natm; ++i)
+      if (a->atml[i]->check_if_nlte()) at = dynamic_cast<atom *>(a->atml[i]);
+    if (!at || !nlambda) { fprintf(stderr, "no NLTE atom / wavelengths\n"); return 4; }
+    nlam = nlambda;
+    nmap = at->nmap;
+    // transitions (1-based tr): type 0 line, 1 bound-free; lower / upper mapped levels
+    std::vector<int> trl, tru, trz, trt;
+    for (int tr = 1; tr <= at->ntr; ++tr) {
+      int z = at->inverse_tmap[tr][2], lo = at->inverse_tmap[tr][3], up = at->inverse_tmap[tr][4];
+      trz.push_back(z);
+      if (up < at->nl[z]) { trt.push_back(0); trl.push_back(at->rmap[z][lo]); tru.push_back(at->rmap[z][up]); }
+      else { trt.push_back(1); trl.push_back(at->rmap[z][lo]); tru.push_back(at->rmap[z + 1][0]); }
+    }
+    if (ic == 0) {
+      for (int l = 0; l < nlambda; ++l) { oLam.push_back(lambda[l]); oLw.push_back(lw[l]); oFudge.push_back(a->get_opacity_fudge(lambda[l])); }
+      for (int tp = 1; tp <= ntp; ++tp) { oTh.push_back(th[tp]); oBin.push_back(bin[tp]); }
+      nline = nbf = 0;
+      for (size_t q = 0; q < trt.size(); ++q) {
+        const int z = trz[q], lo = at->lmap[trl[q]];
+        oTr.push_back(trt[q]); oTr.push_back(trl[q]); oTr.push_back(tru[q]); oTr.push_back(z);
+        if (trt[q] == 0) {
+          const int up = at->lmap[tru[q]];
+          const double lam0 = h * c / (at->ee[z][up] - at->ee[z][lo]);
+          oTrc.push_back(lam0); oTrc.push_back(at->A[z][up][lo]); oTrc.push_back(at->B[z][lo][up]);
+          oTrc.push_back(at->B[z][up][lo]); oTrc.push_back(at->ee[z][up] - at->ee[z][lo]);
+          oTrc.push_back(lam0 * lam0 / (4.0 * pi * c)); oTrc.push_back(at->damp_rad(at->A[z], lo, up));
+          oTrc.push_back(0.0);
+          ++nline;
+        } else {
+          for (int q8 = 0; q8 < 8; ++q8) oTrc.push_back(0.0);
+          for (int l = 0; l < nlambda; ++l) oSig.push_back(at->bf[z][lo] ? at->bf[z][lo]->U(lambda[l]) : 0.0);
+          ++nbf;
+        }
+      }
+      for (int i = 0; i < nmap; ++i)
+        for (int j = 0; j < nmap; ++j) {
+          const int zi = at->zmap[i], li = at->lmap[i], zj = at->zmap[j], lj = at->lmap[j];
+          oA.push_back(zi == zj ? at->A[zi][li][lj] : 0.0);
+          oB.push_back(zi == zj ? at->B[zi][li][lj] : 0.0);
+        }
+    }
+    fp_t ***T = a->T, ***Ne = a->Ne;
+    for (int kk = 0; kk < nd; ++kk) {
+      const int x = x3l + kk;
+      oT.push_back(T[1][1][x]); oNe.push_back(Ne[1][1][x]); oNa.push_back(at->pop[1][1][x].Na);
+      oKap.push_back(a->op_referent[1][1][x]); if (ic == 0) oGrid.push_back(a->rt_grid[x]);
+      for (int i = 0; i < nmap; ++i) oPop0.push_back(at->get_mapped_pop(1, 1, x, i));
+    }
+    for (int tp = 1; tp <= ntp; ++tp) {
+      fp_t ***Vr = a->project(a->Vx, a->Vy, a->Vz, th[tp], ph[tp], 1, 1, 1, 1, x3l, x3h);
+      for (int kk = 0; kk < nd; ++kk) oVr.push_back(Vr[1][1][x3l + kk]);
+      fp_t ****Bt = a->transform(a->Bx, a->By, a->Bz, th[tp], ph[tp], 1, 1, 1, 1, x3l, x3h);
+      for (int l = 0; l < nlambda; ++l) {
+        fp_t ***op = a->opacity_lte(T, Ne, Vr, a->Vt, Bt, th[tp], ph[tp], lambda[l]);
+        fp_t ***em = a->emissivity_lte(T, Ne, Vr, a->Vt, Bt, th[tp], ph[tp], lambda[l]);
+        fp_t ***ff = at->freefree_op(T, Ne, Vr, lambda[l]);
+        fp_t ***ry = at->rayleigh_op(lambda[l]);
+        for (int kk = 0; kk < nd; ++kk) {
+          const int x = x3l + kk;
+          const double pas = ff[1][1][x] + ry[1][1][x];
+          oBgop.push_back(op[1][1][x] + pas);
+          oBgem.push_back(em[1][1][x] + pas * Planck_f(lambda[l], T[1][1][x]));
+        }
+        del_ft3dim(op, 1, 1, 1, 1, x3l, x3h); del_ft3dim(em, 1, 1, 1, 1, x3l, x3h);
+        del_ft3dim(ff, 1, 1, 1, 1, x3l, x3h); del_ft3dim(ry, 1, 1, 1, 1, x3l, x3h);
+      }
+      del_ft4dim(Bt, 1, 3, 1, 1, 1, 1, x3l, x3h);
+      del_ft3dim(Vr, 1, 1, 1, 1, x3l, x3h);
+    }
+    // per line transition and depth: Doppler width and damping (atom_rad.cc boundbound_op)
+    for (size_t q = 0; q < trt.size(); ++q) {
+      if (trt[q] != 0) continue;
+      const int z = trz[q], lo = at->lmap[trl[q]], up = at->lmap[tru[q]];
+      const double lam0 = h * c / (at->ee[z][up] - at->ee[z][lo]);
+      const double ar = at->damp_rad(at->A[z], lo, up), sf = lam0 * lam0 / (4.0 * pi * c);
+      for (int kk = 0; kk < nd; ++kk) {
+        const int x = x3l + kk;
+        const double dld = at->broad_dop(lam0, T[1][1][x], a->Vt[1][1][x]);
+        const double gc = at->damp_col(1, 1, x, z, up, lo, T[1][1][x], Ne[1][1][x], lam0);
+        oDld.push_back(dld);
+        oAd.push_back(sf * (ar + gc * turn_on_damping) / dld);
+      }
+    }
+    // per bound-free transition and depth: n_cont * ratio = LTE-like population factor
+    // (atom_rad.cc boundfree_op: ne saha T^-1.5 g_i/g_c exp((ip - E_i)/kT))
+    for (size_t q = 0; q < trt.size(); ++q) {
+      if (trt[q] != 1) continue;
+      const int z = trz[q], lo = at->lmap[trl[q]];
+      for (int kk = 0; kk < nd; ++kk) {
+        const int x = x3l + kk;
+        const double TT = T[1][1][x];
+        oBfr.push_back(Ne[1][1][x] * saha_const * pow(TT, -1.5) * double(at->g[z][lo]) / double(at->g[z + 1][0]) *
+                       exp((at->ip[z] - at->ee[z][lo]) / k / TT));
+      }
+    }
+    // collisional rates from mapped level i to j (atom_pop.cc:27-145 rate matrix)
+    for (int kk = 0; kk < nd; ++kk) {
+      const int x = x3l + kk;
+      const double TT = T[1][1][x], ne = Ne[1][1][x];
+      std::vector<double> C(nmap * nmap, 0.0);
+      for (int i = 0; i < nmap - 1; ++i) {
+        const int z = at->zmap[i], l = at->lmap[i];
+        for (int ll = 0; ll < at->nl[z]; ++ll) {
+          const int j = i + (ll - l);
+          C[i * nmap + j] = at->C_ij(z, l, ll, TT, ne);
+        }
+        if (int dl = at->nl[z] - l) {
+          C[i * nmap + i + dl] = at->C_i_cont(z, l, TT, ne);
+          C[(i + dl) * nmap + i] = at->C_cont_i(z, l, TT, ne);
+        }
+      }
+      oColl.insert(oColl.end(), C.begin(), C.end());
+    }
+    // the reference's own iteration, niter times (atmos_pop.cc:133-214), populations after each
+    fp_t ***S = ft3dim(a->x1l, a->x1h, a->x2l, a->x2h, x3l, x3h);
+    fp_t ***L = ft3dim(a->x1l, a->x1h, a->x2l, a->x2h, x3l, x3h);
+    for (int it = 0; it < niter; ++it) {
+      for (int i = 0; i < a->natm; ++i) a->atml[i]->rtinit();
+      for (int tp = 1; tp <= ntp; ++tp) {
+        fp_t ***Vr = a->project(a->Vx, a->Vy, a->Vz, th[tp], ph[tp], 1, 1, 1, 1, x3l, x3h);
+        fp_t ****Bt = a->transform(a->Bx, a->By, a->Bz, th[tp], ph[tp], 1, 1, 1, 1, x3l, x3h);
+        for (int l = 0; l < nlambda; ++l) {
+          for (int i = 0; i < a->natm; ++i) a->atml[i]->prof_init();
+          fp_t ***op = a->opacity_lte(T, Ne, Vr, a->Vt, Bt, th[tp], ph[tp], lambda[l]);
+          fp_t ***em = a->emissivity_lte(T, Ne, Vr, a->Vt, Bt, th[tp], ph[tp], lambda[l]);
+          op = a->add(a->opacity_active_only(T, Ne, Vr, a->Vt, Bt, th[tp], ph[tp], lambda[l]), op, 1, 1, 1, 1, x3l, x3h);
+          em = a->add(a->emissivity_active_only(T, Ne, Vr, a->Vt, Bt, th[tp], ph[tp], lambda[l]), em, 1, 1, 1, 1, x3l, x3h);
+          if (a->tau_grid) a->normalize_to_referent_opacity(op, em);
+          a->formal(a->rt_grid, S, L, op, em, th[tp], ph[tp], a->boundary_condition_for_rt);
+          if (a->tau_grid) a->de_normalize(op, em);
+          for (int i = 0; i < a->natm; ++i) a->atml[i]->add(S, L, op, lambda[l], lw[l], bin[tp]);
+          del_ft3dim(em, 1, 1, 1, 1, x3l, x3h);
+          del_ft3dim(op, 1, 1, 1, 1, x3l, x3h);
+        }
+        del_ft4dim(Bt, 1, 3, 1, 1, 1, 1, x3l, x3h);
+        del_ft3dim(Vr, 1, 1, 1, 1, x3l, x3h);
+      }
+      double rc = a->newpops(T, a->Nt, Ne, lambda, nlambda, 1);
+      if (rc < 0.0) rc = -1.0 - fabs(a->newpops(T, a->Nt, Ne, lambda, nlambda, 0));
+      oRel.push_back(rc);
+      for (int kk = 0; kk < nd; ++kk)
+        for (int i = 0; i < nmap; ++i) oPopIt.push_back(at->get_mapped_pop(1, 1, x3l + kk, i));
+    }
+    del_ft3dim(S, a->x1l, a->x1h, a->x2l, a->x2h, x3l, x3h);
+    del_ft3dim(L, a->x1l, a->x1h, a->x2l, a->x2h, x3l, x3h);
+    // the reference's nltepops on a fresh copy of the column
+    {
+      atmosphere *b = task_atmos(t, io);
+      b->build_from_nodes(m);
+      b->set_grid(b->tau_grid);
+      b->boundary_condition_for_rt = -1;
+      b->popsetup();
+      b->compute_op_referent();
+      double t0 = wall_s();
+      b->nltepops();
+      oWall.push_back(wall_s() - t0);
+      atom *bt = 0;
+      for (int i = 0; i < b->natm; ++i)
+        if (b->atml[i]->check_if_nlte()) bt = dynamic_cast<atom *>(b->atml[i]);
+      for (int kk = 0; kk < nd; ++kk)
+        for (int i = 0; i < nmap; ++i) oPopConv.push_back(bt->get_mapped_pop(1, 1, x3l + kk, i));
+      delete b;
+    }
+    delete a;
+  }
+  SbinWriter w(outname);
+  const int64_t nC = ncol, nD = nd, nLm = nlam, nR = ntp, nM = nmap, nT = oTr.size() / 4;
+  w.put("ali_T", {nC, nD}, oT.data()); w.put("ali_ne", {nC, nD}, oNe.data()); w.put("ali_na", {nC, nD}, oNa.data());
+  w.put("ali_kap", {nC, nD}, oKap.data()); w.put("ali_grid", {nD}, oGrid.data());
+  w.put("ali_lambda", {nLm}, oLam.data()); w.put("ali_lw", {nLm}, oLw.data()); w.put("ali_fudge", {nLm}, oFudge.data());
+  w.put("ali_th", {nR}, oTh.data()); w.put("ali_bin", {nR}, oBin.data()); w.put("ali_vray", {nC, nR, nD}, oVr.data());
+  w.put("ali_tr", {nT, 4}, oTr.data()); w.put("ali_trc", {nT, 8}, oTrc.data());
+  w.put("ali_A", {nM, nM}, oA.data()); w.put("ali_B", {nM, nM}, oB.data());
+  w.put("ali_dld", {nC, (int64_t)nline, nD}, oDld.data()); w.put("ali_adamp", {nC, (int64_t)nline, nD}, oAd.data());
+  w.put("ali_sigma", {(int64_t)nbf, nLm}, oSig.data()); w.put("ali_bfratio", {nC, (int64_t)nbf, nD}, oBfr.data());
+  w.put("ali_coll", {nC, nD, nM, nM}, oColl.data());
+  w.put("ali_bgop", {nC, nR, nLm, nD}, oBgop.data()); w.put("ali_bgem", {nC, nR, nLm, nD}, oBgem.data());
+  w.put("ali_pop0", {nC, nD, nM}, oPop0.data());
+  w.put("ali_pops_iter", {nC, (int64_t)niter, nD, nM}, oPopIt.data()); w.put("ali_relchange", {nC, (int64_t)niter}, oRel.data());
+  w.put("ali_pop_conv", {nC, nD, nM}, oPopConv.data()); w.put("ali_ref_seconds", {nC}, oWall.data());
+  delete m;
+  return 0;
+}
+
 int main(int argc, char **argv) {
   if (argc >= 4 && !strcmp(argv[1], "pack")) return do_pack(argv[2], argv[3]);
   if (argc >= 7 && !strcmp(argv[1], "dump"))
     return do_dump(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]), argv[6]);
+  if (argc >= 7 && !strcmp(argv[1], "ali"))
+    return do_ali(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]), argv[6]);
   if (argc >= 9 && !strcmp(argv[1], "lmfit"))
     return do_lmfit(argv[2], argv[3], argv[4], argv[5], atoi(argv[6]), atoi(argv[7]), argv[8]);
   fprintf(stderr, "usage: snapi_ref_dump pack|dump|lmfit ...\n");

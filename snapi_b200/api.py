@@ -354,3 +354,106 @@ class Context:
         self._check(lib().snapi_fd_grad(self._ctx, int(npix), _ptr(int(rec_ptr)), _ptr(int(obs_ptr)), _ptr(ws),
                                         None, int(npar), _ptr(int(tan_ptr)), _ptr(stp), _ptr(int(chi2_ptr)),
                                         _ptr(int(grad_ptr)), MEM_DEVICE))
+
+
+# ---- NLTE level populations (snapi_ali_*) ---------------------------------------------------
+class SnapiAliProblem(ctypes.Structure):
+    _fields_ = [("nd", ctypes.c_int), ("nlambda", ctypes.c_int), ("nray", ctypes.c_int), ("nlevel", ctypes.c_int),
+                ("ntrans", ctypes.c_int)] + [(n, ctypes.c_void_p) for n in (
+                    "grid", "lambda_", "lambda_w", "fudge", "ray_theta", "ray_w", "trans", "line_c", "line_e", "A",
+                    "B", "stage", "cont_of", "sigma")]
+
+
+class SnapiAliColumns(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("T", "ne", "na", "kappa", "vray", "dld", "adamp", "bfratio", "coll",
+                                               "bg_op", "bg_em")]
+
+
+def _ali_lib():
+    L = lib()
+    if not getattr(L, "_ali_set", False):
+        vp, ip = ctypes.c_void_p, ctypes.c_int
+        L.snapi_ali_create.restype = vp
+        L.snapi_ali_create.argtypes = [ctypes.POINTER(SnapiAliProblem), ip, ctypes.POINTER(ctypes.c_int)]
+        L.snapi_ali_destroy.argtypes = [vp]
+        L.snapi_ali_last_error.restype = ctypes.c_char_p
+        L.snapi_ali_last_error.argtypes = [vp]
+        L.snapi_ali_iter.argtypes = [vp, ip, ctypes.POINTER(SnapiAliColumns), vp, ip, ctypes.c_double, vp, vp, vp, ip]
+        L.snapi_ali_last_kernel_ms.restype = ctypes.c_double
+        L.snapi_ali_last_kernel_ms.argtypes = [vp]
+        L._ali_set = True
+    return L
+
+
+class AliContext:
+    """NLTE populations of one atom in many columns (atmosphere::nltepops, batched).
+
+    transitions: [ntrans, 2] (lower, upper) level pairs; a pair whose upper level is the lower
+    level's continuum (cont_of) is bound-free.  line_c [ntrans, 4]: lambda0, A_ul, B_lu, B_ul;
+    line_e [ntrans]: E_u - E_l; sigma [ntrans, nlambda]: bound-free cross sections."""
+
+    def __init__(self, grid, lam, lam_w, fudge, ray_theta, ray_w, transitions, line_c, line_e, A, B, stage, cont_of,
+                 sigma, device=0):
+        d = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)  # noqa: E731
+        self._keep = [d(grid), d(lam), d(lam_w), d(fudge), d(ray_theta), d(ray_w), i32(transitions), d(line_c),
+                      d(line_e), d(A), d(B), i32(stage), i32(cont_of), d(sigma)]
+        k = self._keep
+        self.nd, self.nl, self.nray, self.nlev = len(k[0]), len(k[1]), len(k[4]), k[9].shape[0]
+        self.ntr = k[6].shape[0]
+        p = SnapiAliProblem(self.nd, self.nl, self.nray, self.nlev, self.ntr, *[a.ctypes.data for a in k])
+        st = ctypes.c_int(0)
+        self._ctx = _ali_lib().snapi_ali_create(ctypes.byref(p), device, ctypes.byref(st))
+        if not self._ctx:
+            raise RuntimeError("snapi_ali_create failed (%d)" % st.value)
+
+    @classmethod
+    def from_fixture(cls, fx, **kw):
+        tr = np.asarray(fx["ali_tr"]).astype(int)  # type, lower, upper, stage of the lower level
+        nlev = fx["ali_A"].shape[0]
+        stage = np.zeros(nlev, int)
+        cont = -np.ones(nlev, int)
+        for t, lo, up, z in tr:
+            stage[lo] = z
+            stage[up] = z + 1 if t == 1 else z
+            if t == 1:
+                cont[lo] = up
+        sig = np.zeros((tr.shape[0], fx["ali_lambda"].shape[0]))
+        sig[tr[:, 0] == 1] = fx["ali_sigma"]
+        trc = np.asarray(fx["ali_trc"])
+        return cls(fx["ali_grid"], fx["ali_lambda"], fx["ali_lw"], fx["ali_fudge"], fx["ali_th"], fx["ali_bin"],
+                   tr[:, 1:3], trc[:, :4], trc[:, 4], fx["ali_A"], fx["ali_B"], stage, cont, sig, **kw)
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            _ali_lib().snapi_ali_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        self.close()
+
+    @staticmethod
+    def columns_from_fixture(fx):
+        return {k: fx["ali_" + k] for k in ("T", "ne", "na", "kap", "vray", "dld", "adamp", "bfratio", "coll",
+                                             "bgop", "bgem")}
+
+    def iterate(self, cols, pops, max_iter=100, tol=1e-2):
+        """Iterate all columns; returns (pops, rel_change, iters, status)."""
+        d = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        arrs = [d(cols["T"]), d(cols["ne"]), d(cols["na"]), d(cols["kap"]), d(cols["vray"]), d(cols["dld"]),
+                d(cols["adamp"]), d(cols["bfratio"]), d(cols["coll"]), d(cols["bgop"]), d(cols["bgem"])]
+        c = SnapiAliColumns(*[a.ctypes.data for a in arrs])
+        p = d(pops).copy()
+        ncol = p.shape[0]
+        rel = np.zeros(ncol)
+        it = np.zeros(ncol, np.int32)
+        st = np.zeros(ncol, np.int32)
+        rc = _ali_lib().snapi_ali_iter(self._ctx, ncol, ctypes.byref(c), p.ctypes.data, int(max_iter), float(tol),
+                                       rel.ctypes.data, it.ctypes.data, st.ctypes.data, MEM_HOST)
+        if rc != 0:
+            raise RuntimeError("snapi_ali_iter: %s" % _ali_lib().snapi_ali_last_error(self._ctx).decode())
+        return p, rel, it, st
+
+    @property
+    def last_kernel_ms(self):
+        return _ali_lib().snapi_ali_last_kernel_ms(self._ctx)

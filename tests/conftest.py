@@ -41,6 +41,11 @@ def config4():
 
 
 @pytest.fixture(scope="session")
+def config5():
+    return load_fixture("config5")
+
+
+@pytest.fixture(scope="session")
 def oracle_lib():
     from snapi_b200 import build as b
     b.build_oracle() if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libsnapi_oracle.so")) else None

@@ -36,7 +36,12 @@ from sbin import read_sbin  # noqa: E402
 
 DUMP = os.path.join(ROOT, "oracle", "_ref", "snapi_ref_dump")
 CFG_FILES = ["atoms_6300.cfg", "mol.cfg", "hydrogen_3lvl.cfg", "helium.cfg", "carbon.cfg", "nitrogen.cfg",
-             "oxygen.cfg", "calcium.cfg", "silicon.cfg", "aluminium.cfg", "iron_6300.cfg", "falc_80z.dat"]
+             "oxygen.cfg", "calcium.cfg", "silicon.cfg", "aluminium.cfg", "iron_6300.cfg", "falc_80z.dat",
+             "calcium_ir_rh.cfg"]
+# config 5: the Fe I 6300 background atoms with Ca II (5 levels + continuum, NLTE = 1) instead of
+# the LTE calcium model
+C5_ATOMS = ["hydrogen_3lvl.cfg", "helium.cfg", "carbon.cfg", "nitrogen.cfg", "oxygen.cfg", "calcium_ir_rh.cfg",
+            "silicon.cfg", "aluminium.cfg", "iron_6300.cfg"]
 
 ND = 80
 NLAMBDA = 201
@@ -51,7 +56,8 @@ def config1_temperature(x):
             + 5100.0 * st((x - 0.3) / 0.6) / st((1.0 - 0.3) / 0.6))
 
 
-def write_cfg(path, t_taus, t_vals, vs_taus, vs_vals, vt=1e5, B=1000.0, theta_deg=45.0, phi_deg=30.0):
+def write_cfg(path, t_taus, t_vals, vs_taus, vs_vals, vt=1e5, B=1000.0, theta_deg=45.0, phi_deg=30.0,
+              atoms="atoms_6300.cfg", lam="6301.0-6303.4", dlam=0.012):
     fmt = lambda a: ",".join("%.6f" % v for v in a)  # noqa: E731
     cfg = f"""atmos{{
   ID=col
@@ -59,7 +65,7 @@ def write_cfg(path, t_taus, t_vals, vs_taus, vs_vals, vt=1e5, B=1000.0, theta_de
   FILE=falc_80z.dat
   GEOMETRY=PLANEPARALLEL
   RTSOLVER=Bezier
-  ATOM=atoms_6300.cfg
+  ATOM={atoms}
   MOL=mol.cfg
   TAU_GRID=1
 }}
@@ -68,8 +74,8 @@ obs{{
   EL=3.14159265359
   AZ=0.0
   NAME=none
-  LAMBDA=6301.0-6303.4
-  DLAMBDA=0.012
+  LAMBDA={lam}
+  DLAMBDA={dlam}
 }}
 model{{
   ID=m1
@@ -222,6 +228,25 @@ def make_config4(tmp, npix, iters=30):
                         iters=np.array([iters]), **line_arrays(d))
 
 
+def make_config5(tmp, ncol, niter=3):
+    """NLTE Ca II (config 5): the inputs of the level-population iteration per column, the
+    populations after each of the reference's first niter iterations, and the populations its
+    nltepops converges to.  Columns: the ten-node model with seeded T / v_los / B (seed 5)."""
+    with open(os.path.join(tmp, "atoms_c5.cfg"), "w") as f:
+        f.write("".join("ATOM=%s\n" % a for a in C5_ATOMS))
+    write_cfg(os.path.join(tmp, "c5.cfg"), C3_TTAU, C3_TRUTH[:4], C3_VSTAU, C3_TRUTH[5:7], atoms="atoms_c5.cfg",
+              lam="8538.5-8545.985", dlam=0.025)
+    run([DUMP, "pack", "c5.cfg", "c5.tsk"], tmp)
+    shutil.copy(os.path.join(tmp, "c5.tsk"), os.path.join(HERE, "c5.tsk"))
+    nodes = config3_nodes(ncol, seed=5)
+    nf = os.path.join(tmp, "c5_nodes.f64")
+    np.ascontiguousarray(nodes, dtype="<f8").tofile(nf)
+    out = os.path.join(tmp, "c5.sbin")
+    sys.stderr.write(run([DUMP, "ali", "c5.tsk", nf, str(ncol), str(niter), out], tmp))
+    d = read_sbin(out)
+    np.savez_compressed(os.path.join(HERE, "config5.npz"), nodes=nodes, **{k: v for k, v in d.items()})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -231,6 +256,8 @@ def main():
     ap.add_argument("--only-pool", action="store_true")
     ap.add_argument("--only-c4", action="store_true")
     ap.add_argument("--c4pix", type=int, default=8)
+    ap.add_argument("--only-c5", action="store_true")
+    ap.add_argument("--c5col", type=int, default=3)
     a = ap.parse_args()
     if not os.path.exists(DUMP):
         raise SystemExit("build the oracle first: make -C oracle")
@@ -238,13 +265,15 @@ def main():
     try:
         for f in CFG_FILES:
             shutil.copy(os.path.join(a.ref, "cfg", f), tmp)
-        if a.only_pool or a.only_c4:
+        if a.only_pool or a.only_c4 or a.only_c5:
             shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
         else:
             make_configs_1_to_3(a, tmp)
-        if a.c4pix:
+        if a.c4pix and not a.only_c5:
             make_config4(tmp, a.c4pix)
-        if a.pool and not a.only_c4:
+        if a.c5col and not a.only_c4:
+            make_config5(tmp, a.c5col)
+        if a.pool and not (a.only_c4 or a.only_c5):
             n4 = config3_nodes(a.pool, seed=303)
             d4 = dump(tmp, os.path.join(tmp, "c3.tsk"), n4, 2, "pool")
             np.savez_compressed(os.path.join(HERE, "bench_pool.npz"), lambda_air=d4["lambda_air"],

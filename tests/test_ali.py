@@ -1,0 +1,50 @@
+"""NLTE level populations (snapi_ali_iter) against the reference's own iteration
+(atmosphere::nltepops on Ca II 8542 columns, tests/golden/config5.npz): the populations after each
+of the first iterations, and the populations the reference converges to."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sb():
+    import snapi_b200
+    from snapi_b200 import build as b
+    b.build_cuda()
+    return snapi_b200
+
+
+def _rel(a, b):
+    return np.abs(a / b - 1.0)
+
+
+def test_ali_iterations_follow_reference(sb, config5):
+    fx = config5
+    ctx = sb.api.AliContext.from_fixture(fx)
+    cols = ctx.columns_from_fixture(fx)
+    ref_it = fx["ali_pops_iter"]  # [ncol, niter, nd, nlevel]
+    for n in range(1, ref_it.shape[1] + 1):
+        pops, rel, iters, st = ctx.iterate(cols, fx["ali_pop0"], max_iter=n, tol=1e-30)
+        assert np.all(iters == n) and np.all(st == 0)
+        err = _rel(pops, ref_it[:, n - 1])
+        print("iteration", n, "max relative population difference", err.max(), "relative change", rel,
+              "reference", fx["ali_relchange"][:, n - 1])
+        # FP32 W4 profiles (SFU exp / sin, ~1e-6 relative), FP64 everywhere else: measured 2e-5
+        # after the first step, which moves the populations by factors up to 3.7
+        assert err.max() < 1e-4, (n, err.max())
+        np.testing.assert_allclose(rel, fx["ali_relchange"][:, n - 1], rtol=1e-4)
+    ctx.close()
+
+
+def test_ali_converges_to_reference_populations(sb, config5):
+    fx = config5
+    ctx = sb.api.AliContext.from_fixture(fx)
+    pops, rel, iters, st = ctx.iterate(ctx.columns_from_fixture(fx), fx["ali_pop0"], max_iter=100, tol=1e-2)
+    assert np.all(st == 0) and np.all(rel < 1e-2)
+    err = _rel(pops, fx["ali_pop_conv"])
+    print("iterations", iters, "max relative difference to the reference's converged populations", err.max())
+    # both stop once the largest relative change of an iteration is below 1e-2, after the same
+    # number of iterations (10, 16, 14 for these columns)
+    assert err.max() < 1e-3
+    ctx.close()

@@ -99,3 +99,17 @@ def test_chi2_fd_gradient_linear_in_step(oracle_lib, config3):
     _, g2 = so.chi2_grad_fd(fx["lambda_air"], fx["tau500"], fx["record"][0], lines, obs, np.ones(4), np.ones(nl),
                             tan, 0.25)
     assert abs(g1[0] - g2[0]) <= 1e-5 * abs(g1[0])
+
+
+def test_ali_restatement_matches_reference_iterations(config5):
+    """The numpy restatement of the NLTE iteration (oracle/ali_oracle.py) reproduces the
+    reference's own first two iterations on a Ca II column."""
+    import ali_oracle as ao  # oracle/ is on sys.path (conftest)
+    fx = config5
+    P = ao.Problem(fx)
+    p = fx["ali_pop0"][0].copy()
+    for it in range(2):
+        p, r, neg = ao.iterate(P, fx, 0, p)
+        assert not neg
+        assert np.abs(p / fx["ali_pops_iter"][0, it] - 1.0).max() < 1e-9
+        assert abs(r / fx["ali_relchange"][0, it] - 1.0) < 1e-9
