@@ -38,8 +38,9 @@ NPIX = 64 * 64
 FD_STEPS = np.array([5.0, 5.0, 5.0, 5.0, 2e3, 2e3, 2e3, 5.0, 5e-3, 5e-3])
 
 
-def make_workload(pool, npix=NPIX, seed=3):
-    """Per-pixel records / tangents / truth for the benchmark (see the module docstring)."""
+def make_workload(pool, npix=NPIX, seed=3, return_nodes=False):
+    """Per-pixel records / tangents / truth for the benchmark (see the module docstring); with
+    return_nodes also the truth node vectors (T x4, v_turb, v_los x2, B, inclination, azimuth)."""
     rng = np.random.default_rng(seed)
     ncol = pool["record"].shape[0]
     col = rng.integers(0, ncol, npix)
@@ -73,6 +74,10 @@ def make_workload(pool, npix=NPIX, seed=3):
     model["B"] = truth["B"] + 200.0
     model["th"] = truth["th"] + 0.1
     model["ph"] = truth["ph"] + 0.1
+    if return_nodes:
+        nodes = np.concatenate([pool["nodes"][col, :4], np.stack([truth[k] for k in ("vt", "v1", "v2", "B", "th", "ph")],
+                                                                 axis=1)], axis=1)
+        return apply(rec, truth), apply(rec, model), tan, nodes
     return apply(rec, truth), apply(rec, model), tan
 
 
@@ -287,12 +292,106 @@ def run_snapi(args):
         }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = reference_cpu_rate(samples_per_core=1, mode=1)
+    if rank == 0 and not args.no_extras:
+        line["lm"] = bench_lm(sb, pool, ic, local)
+        line["ali"] = bench_ali(sb, local, cpu=not args.no_cpu_baseline)
     ctx.close()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
     return line
+
+
+def bench_lm(sb, pool, ic, device, npix=4096, iters=10):
+    """Device time of the batched LM (snapi_lm_step): 10-node fits of npix pixels from offset
+    starting nodes.  The node -> record map between steps is the caller's; here it is the
+    records' linearisation along the node tangents (numpy, not timed on the device)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ref_builder import LinearBuilder
+    truth, _, tan, nodes_t = make_workload(pool, npix, seed=11, return_nodes=True)
+    build = LinearBuilder(truth, tan, nodes_t)
+    ctx = sb.Context.from_fixture(pool, stokes_scale=ic, max_batch=npix, device=device)
+    obs = ctx.synth(truth)
+    obs += np.random.default_rng(12).normal(0.0, 1e-3 * ic, obs.shape).astype(np.float32)
+    kinds = pool["node_kind"].astype(int)
+    scale = np.array([{1: 5000.0, 2: 1e5, 3: 1e5, 4: 1000.0}.get(k, 1.0) for k in kinds])
+    n0 = nodes_t + np.array([200.0, 200.0, 200.0, 200.0, 3e4, 3e4, 3e4, 200.0, 0.1, 0.1])
+    req = ctx.lm_begin(n0, obs, kinds, 1e-2 * scale, lm_start=1e3, max_iter=iters, delta=1e-4)
+    dev_ms, steps, active = 0.0, 0, np.ones(npix, bool)
+    t0 = time.perf_counter()
+    while True:
+        rec, tn = build(req, active)
+        req, active, n = ctx.lm_step(rec, tn)
+        dev_ms += ctx.last_kernel_ms
+        steps += 1
+        if n == 0:
+            break
+    wall = time.perf_counter() - t0
+    res = ctx.lm_result()
+    ctx.close()
+    return {"pixels": npix, "npar": int(tan.shape[1]), "steps": steps, "device_ms_per_step": dev_ms / steps,
+            "device_pixel_steps_per_s": npix * steps / (dev_ms / 1e3), "wall_s_with_host_linear_builder": wall,
+            "median_iterations": float(np.median(res["iters"])),
+            "note": "device work per step: synthesis at the trial nodes, Jacobian (2 npar solves) at accepted "
+                    "nodes, FP64 J^T J and damped eigen-solve; node -> record map on the host"}
+
+
+def bench_ali(sb, device, ncol=1024, cpu=True):
+    """NLTE Ca II populations (snapi_ali_iter) for ncol columns to the reference's convergence
+    criterion (max relative change < 1e-2): the three reference-built columns of
+    tests/golden/config5.npz tiled to ncol (80 depths, 444 NLTE wavelengths, 2 rays)."""
+    fx = dict(np.load(os.path.join(ROOT, "tests", "golden", "config5.npz")))
+    ctx = sb.api.AliContext.from_fixture(fx, device=device)
+    cols = ctx.columns_from_fixture(fx)
+    idx = np.arange(ncol) % fx["ali_T"].shape[0]
+    cols = {k: np.ascontiguousarray(v[idx]) for k, v in cols.items()}
+    pops0 = np.ascontiguousarray(fx["ali_pop0"][idx])
+    ctx.iterate({k: v[:8] for k, v in cols.items()}, pops0[:8], max_iter=2, tol=1e-2)  # warm-up
+    t0 = time.perf_counter()
+    pops, rel, iters, st = ctx.iterate(cols, pops0, max_iter=100, tol=1e-2)
+    wall = time.perf_counter() - t0
+    dev_ms = ctx.last_kernel_ms
+    ctx.close()
+    out = {"columns": ncol, "nd": int(fx["ali_T"].shape[1]), "nlambda": int(fx["ali_lambda"].shape[0]),
+           "rays": int(fx["ali_th"].shape[0]), "levels": int(fx["ali_A"].shape[0]),
+           "iterations_max": int(iters.max()), "device_ms": dev_ms, "columns_per_s_device": ncol / (dev_ms / 1e3),
+           "columns_per_s_e2e": ncol / wall, "max_rel_to_reference_converged":
+               float(np.abs(pops[:3] / fx["ali_pop_conv"] - 1.0).max()), "negative_columns": int((st < 0).sum())}
+    if cpu:
+        out["reference_cpu"] = reference_ali_rate()
+    return out
+
+
+def reference_ali_rate(cores=None):
+    """The reference's nltepops on config-5 columns, one process per host core (one column each)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import config3_nodes
+    from sbin import read_sbin
+    dump = os.path.join(ROOT, "oracle", "_ref", "snapi_ref_dump")
+    task = os.path.join(ROOT, "tests", "golden", "c5.tsk")
+    if not os.path.exists(dump):
+        return None
+    ncores = cores or os.cpu_count() or 1
+    nodes = config3_nodes(ncores, seed=5)
+    tmp = tempfile.mkdtemp(prefix="snapi_ali_ref_")
+    procs = []
+    for i in range(ncores):
+        nf = os.path.join(tmp, "n%d.f64" % i)
+        nodes[i:i + 1].astype("<f8").tofile(nf)
+        procs.append(subprocess.Popen([dump, "ali", task, nf, "1", "0", os.path.join(tmp, "o%d.sbin" % i)],
+                                      stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+    ok = all(p.wait() == 0 for p in procs)
+    secs = [float(read_sbin(os.path.join(tmp, "o%d.sbin" % i))["ali_ref_seconds"][0]) for i in range(ncores)] if ok \
+        else []
+    for f in os.listdir(tmp):
+        os.unlink(os.path.join(tmp, f))
+    os.rmdir(tmp)
+    if not ok:
+        return None
+    return {"columns_per_s": ncores / max(secs), "cores": ncores, "seconds_per_column_mean": float(np.mean(secs)),
+            "kind": "reference", "sample": "%d seeded config-5 columns, atmosphere::nltepops (strict FP64 build), "
+                                          "one process per core" % ncores}
 
 
 def ctypes_buffer(ctx, nbytes):
@@ -385,6 +484,7 @@ def main():
     ap.add_argument("--impl", default="snapi", choices=["snapi", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--pixels", type=int, default=NPIX, help="pixels per GPU (smaller cases for profiling)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the LM and NLTE measurements")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

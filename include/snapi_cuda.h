@@ -57,7 +57,7 @@ extern "C" {
 #define SNAPI_MEM_DEVICE 1
 
 #define SNAPI_NFIELD0 12
-#define SNAPI_MAX_LINES 8
+#define SNAPI_MAX_LINES 16
 #define SNAPI_MAX_COMP 16
 #define SNAPI_MAX_LAMBDA 8192
 

@@ -49,7 +49,7 @@ enum RecField : int {
   F_T = 0, F_VT = 1, F_NE = 2, F_VLOS = 3, F_B = 4, F_INC = 5, F_AZI = 6, F_KAP = 7,
   F_HMBF = 8, F_HMFF = 9, F_BFOP = 10, F_BFEM = 11, F_LINE0 = 12
 };
-constexpr int kMaxLines = 8;
+constexpr int kMaxLines = 16;
 constexpr int kMaxComp = 16;      // per Zeeman group
 constexpr int kNumRed = 10;       // depth-level adjoint sums that are not per line
 constexpr int kRedPerLine = 6;    // per-line depth-level adjoint sums

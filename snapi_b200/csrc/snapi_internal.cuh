@@ -24,7 +24,6 @@ namespace snapi {
 constexpr int kChunk = SNAPI_CHUNK;           // wavelengths (threads) per sweep CTA
 constexpr int kFinishThreads = 128;           // threads of the per-pixel finish kernels
 constexpr long long kWaitLimit = 1LL << 26;   // mbarrier polls before a CTA gives up
-constexpr int kRedMax = kNumRed + kRedPerLine * kMaxLines;  // <= 64
 // Opacity-adjoint sums per (pixel, group, depth): group 0 (continuum) fills R_COP..R_LT, group
 // 1 + j (transition j) fills RL_OPN..RL_A then its share of R_ST2..R_S2.
 constexpr int kOpSlots = kRedPerLine + 4;

@@ -244,7 +244,12 @@ def make_config5(tmp, ncol, niter=3):
     out = os.path.join(tmp, "c5.sbin")
     sys.stderr.write(run([DUMP, "ali", "c5.tsk", nf, str(ncol), str(niter), out], tmp))
     d = read_sbin(out)
-    np.savez_compressed(os.path.join(HERE, "config5.npz"), nodes=nodes, **{k: v for k, v in d.items()})
+    # the reference's synthesis of the 8542 window with those NLTE populations (obs_stokes runs
+    # nltepops itself) and the column records the device synthesis takes
+    s = dump(tmp, os.path.join(tmp, "c5.tsk"), nodes, 0, "c5syn")
+    np.savez_compressed(os.path.join(HERE, "config5.npz"), nodes=nodes, **{k: v for k, v in d.items()},
+                        lambda_air=s["lambda_air"], tau500=s["tau500"], record=s["record"], stokes=s["stokes"],
+                        ref_synth_seconds=s["ref_seconds_per_pixel"], **line_arrays(s))
 
 
 def main():

@@ -28,7 +28,7 @@ def _ctx(sb, fx, **kw):
     return sb.Context.from_fixture(fx, **kw)
 
 
-@pytest.mark.parametrize("cfg", ["config1", "config2", "config3"])
+@pytest.mark.parametrize("cfg", ["config1", "config2", "config3", "config5"])
 def test_synth_matches_oracle(sb, oracle_lib, cfg, request):
     fx = request.getfixturevalue(cfg)
     ctx = _ctx(sb, fx)

@@ -47,6 +47,12 @@ def test_stokes_config3(oracle_lib, config3):
     assert _stokes_err(oracle_lib, config3) < 1e-12
 
 
+def test_stokes_config5_nlte_ca(oracle_lib, config5):
+    """Ca II 8542 window with the reference's NLTE populations in the record (10 transitions:
+    Ca II H, K and the infrared triplet, the hydrogen far wings, Fe I 6301/6302)."""
+    assert _stokes_err(oracle_lib, config5) < 1e-12
+
+
 def test_zeeman_pattern_matches_reference(oracle_lib, config1):
     so, fx = oracle_lib, config1
     # Fe I 6301.5 (2J 4 -> 4, g 1.5 / 1.83) and 6302.5 (2J 0 -> 2, g 0 / 2.5): iron_6300.cfg
