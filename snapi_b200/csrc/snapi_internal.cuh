@@ -27,9 +27,23 @@ constexpr long long kWaitLimit = 1LL << 26;   // mbarrier polls before a CTA giv
 // Opacity-adjoint sums per (pixel, group, depth): group 0 (continuum) fills R_COP..R_LT, group
 // 1 + j (transition j) fills RL_OPN..RL_A then its share of R_ST2..R_S2.
 constexpr int kOpSlots = kRedPerLine + 4;
+constexpr int kOpThreads = 256;  // k_adj_opacity: threads per CTA at most
+// Wavelength slices of the opacity adjoint: enough that nd x slices fills whole warps (80 depths
+// -> 2 slices, 160 threads), at most kOpThreads threads.
+__host__ __device__ inline int op_slices(int nd) {
+#ifdef SNAPI_OP_NOSLICE
+  return 1;
+#endif
+  int g = 32, a = nd;
+  while (a % g) g >>= 1;  // gcd(nd, 32)
+  int s = 32 / g;
+  while (s > 1 && nd * s > kOpThreads) s >>= 1;
+  return s;
+}
 
 struct KParams {
   int npix, nd, nl, nlines, nfield, npar, lpad, ncomp, nred, nchunk, nwslot, nvar;
+  int nslice;                   // wavelength slices of the opacity adjoint (threads = nd x nslice)
   float lam_mid;
   double scale2;                // stokes_scale^2
   const float *rec;             // [npix][nd][nfield]
@@ -45,7 +59,7 @@ struct KParams {
   float4 *scratch;              // [npix][nd][4][lpad]     forward state of the adjoint
   float4 *seed;                 // [npix][lpad]            adjoint of the emergent Stokes vector
   float4 *bars;                 // [npix][nl][3][nd]       (eta-bar, j-bar) per wavelength, depth
-  float *opart;                 // [npix][1+nlines][nd][kOpSlots] wavelength sums of the opacity adjoint
+  float *opart;                 // [npix][1+nlines][nslice][nd][kOpSlots] wavelength sums of the opacity adjoint
   double *c2part;               // [npix][nvar][nwslot]      per-warp chi2 sums
   double *rec_grad;             // [npix][nd][nfield] or null
   double *grad;                 // [npix][npar]
