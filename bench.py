@@ -10,7 +10,9 @@ hydrostatic-equilibrium + chemistry code (tests/golden/bench_pool.npz, seed 303,
 tangents of the reference's build_from_nodes); v_turb, v_los, B, inclination and azimuth are
 drawn per pixel (seed 3) -- they enter the columns linearly through the node interpolation.
 Target = synthesised truth + N(0, 1e-3 Ic); the evaluated model = truth with fixed node offsets.
-Inputs (~400 MB) exceed the 126 MB L2, so no flush is needed between steps.
+The adjoint takes the node tangents packed (per node only the record fields it moves: 100 of 270
+columns).  Inputs (0.18 GB) and the adjoint's state (8 GB) per step exceed the 126 MB L2, so no
+flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl snapi|reference]
 
@@ -175,7 +177,11 @@ def run_snapi(args):
     # device-resident inputs
     d_rec = torch.from_numpy(model).to(dev)
     d_obs = torch.from_numpy(obs).to(dev)
-    d_tan = torch.from_numpy(tan).to(dev)
+    d_tan = torch.from_numpy(tan).to(dev)  # dense: the FD baseline perturbs records along it
+    # the adjoint takes the node tangents packed: per node only the record fields it moves
+    fmask = sb.tangent_field_mask(tan)
+    ptan = sb.pack_tangents(tan, fmask)
+    d_ptan = torch.from_numpy(ptan).to(dev)
     d_chi2 = torch.zeros(NPIX, dtype=torch.float64, device=dev)
     d_grad = torch.zeros(NPIX, npar, dtype=torch.float64, device=dev)
     d_st = torch.zeros(NPIX, nl, 4, dtype=torch.float32, device=dev)
@@ -183,7 +189,7 @@ def run_snapi(args):
     torch.cuda.synchronize()
 
     def step():
-        ctx.adjoint_device(NPIX, d_rec.data_ptr(), d_obs.data_ptr(), npar, d_tan.data_ptr(), d_chi2.data_ptr(),
+        ctx.adjoint_packed_device(NPIX, d_rec.data_ptr(), d_obs.data_ptr(), fmask, d_ptan.data_ptr(), d_chi2.data_ptr(),
                            d_grad.data_ptr(), stokes_ptr=d_st.data_ptr())
 
     for _ in range(args.warmup):
@@ -231,23 +237,23 @@ def run_snapi(args):
     h_rec[...] = model
     h_obs = np.frombuffer((ctypes_buffer(ctx, obs.nbytes)), dtype=np.float32).reshape(obs.shape)
     h_obs[...] = obs
-    h_tan = np.frombuffer((ctypes_buffer(ctx, tan.nbytes)), dtype=np.float32).reshape(tan.shape)
-    h_tan[...] = tan
+    h_tan = np.frombuffer((ctypes_buffer(ctx, ptan.nbytes)), dtype=np.float32).reshape(ptan.shape)
+    h_tan[...] = ptan
     # results land in page-locked buffers too (the C ABI writes into caller-owned memory)
     h_out = {"stokes": np.frombuffer(ctypes_buffer(ctx, 4 * NPIX * nl * 4), dtype=np.float32).reshape(NPIX, nl, 4),
              "chi2": np.frombuffer(ctypes_buffer(ctx, 8 * NPIX), dtype=np.float64),
              "grad": np.frombuffer(ctypes_buffer(ctx, 8 * NPIX * npar), dtype=np.float64).reshape(NPIX, npar)}
-    ctx.adjoint(h_rec, h_obs, h_tan, out=h_out)
+    ctx.adjoint_packed(h_rec, h_obs, fmask, h_tan, out=h_out)
     torch.cuda.synchronize()
     barrier(world)
     ne = max(1, args.steps // 2)
     ev0.record(stream)
     for _ in range(ne):
-        out = ctx.adjoint(h_rec, h_obs, h_tan, out=h_out)
+        out = ctx.adjoint_packed(h_rec, h_obs, fmask, h_tan, out=h_out)
     ev1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = reduce_max(ev0.elapsed_time(ev1) / ne, world, dev)
-    h2d = model.nbytes + obs.nbytes + tan.nbytes
+    h2d = model.nbytes + obs.nbytes + ptan.nbytes
     d2h = out["stokes"].nbytes + out["chi2"].nbytes + out["grad"].nbytes
 
     line = None
@@ -257,7 +263,8 @@ def run_snapi(args):
         # algorithmic bytes per pixel: record + tangents + target in, Stokes + grad + chi2 out
         nd = model.shape[1]
         nf = model.shape[2]
-        bytes_pix = 4 * (nd * nf + npar * nd * nf + nl * 4) + 4 * nl * 4 + 8 * (npar + 1)
+        ntcol = ptan.shape[1]
+        bytes_pix = 4 * (nd * nf + ntcol * nd + nl * 4) + 4 * nl * 4 + 8 * (npar + 1)
         achieved = bytes_pix * NPIX / (kern_per_launch_ms / 1e3) / 1e9
         peaks = load_peaks()
         line = {
@@ -277,7 +284,9 @@ def run_snapi(args):
                                    " pixels x 80 depths x 201 wavelengths, Fe I 6301.5/6302.5, mu=1, "
                                    "10 nodes (T x4, vturb, vlos x2, B, incl, azi): synthesis + chi2 + adjoint "
                                    "d chi2/d nodes", "pixels_per_gpu": NPIX, "nd": int(nd), "nlambda": int(nl),
-                       "npar": int(npar), "l2_flush": "inputs ~0.4 GB per step exceed the 126 MB L2",
+                       "npar": int(npar), "node_tangents": "packed: %d of %d record-field columns per pixel"
+                                                            % (ntcol, npar * nf),
+                       "l2_flush": "inputs (0.18 GB) and adjoint state (8 GB) per step exceed the 126 MB L2",
                        "parallelism": "replicas (pixels independent)"},
             "gpu_launches": launches,
             "clocks": clk,

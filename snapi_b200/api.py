@@ -94,6 +94,7 @@ def lib():
         L.snapi_adjoint.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, fp, ip]
         L.snapi_responses.argtypes = [vp, ip, fp, ip, fp, fp, fp, fp, ip]
         L.snapi_fd_grad.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, ip]
+        L.snapi_adjoint_packed.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, fp, ip]
         L.snapi_zeeman_pattern.argtypes = [ip, ip, ctypes.c_double, ctypes.c_double, ctypes.POINTER(SnapiLine)]
         L.snapi_host_alloc.restype = vp
         L.snapi_host_alloc.argtypes = [ctypes.c_size_t]
@@ -146,6 +147,25 @@ def _ptr(a):
 
 def _f32(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+def tangent_field_mask(tangents):
+    """Per node, the bit mask of record fields its tangent touches anywhere in the batch:
+    tangents [npix, npar, nd, nfield] -> uint64 [npar]."""
+    nz = (np.asarray(tangents) != 0).any(axis=(0, 2))
+    return np.array([sum(1 << int(f) for f in np.flatnonzero(nz[p])) for p in range(nz.shape[0])], dtype=np.uint64)
+
+
+def pack_tangents(tangents, field_mask):
+    """Dense tangents [npix, npar, nd, nfield] -> packed [npix, ntcol, nd] (node by node, fields in
+    increasing order), the layout of snapi_adjoint_packed."""
+    t = np.asarray(tangents)
+    cols = []
+    for p, m in enumerate(np.asarray(field_mask, dtype=np.uint64)):
+        for f in range(t.shape[3]):
+            if (int(m) >> f) & 1:
+                cols.append(t[:, p, :, f])
+    return np.ascontiguousarray(np.stack(cols, axis=1), dtype=np.float32)
 
 
 class Context:
@@ -346,6 +366,34 @@ class Context:
                                         _ptr(int(mask_ptr)) if mask_ptr else None, int(npar), _ptr(int(tan_ptr)),
                                         _ptr(int(stokes_ptr)) if stokes_ptr else None, _ptr(int(chi2_ptr)),
                                         _ptr(int(grad_ptr)), None, MEM_DEVICE))
+
+    def adjoint_packed_device(self, npix, rec_ptr, obs_ptr, field_mask, ptan_ptr, chi2_ptr, grad_ptr,
+                              stokes_ptr=None, mask_ptr=None, w_stokes=(1.0, 1.0, 1.0, 1.0)):
+        fm = np.ascontiguousarray(field_mask, dtype=np.uint64)
+        ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
+        self._check(lib().snapi_adjoint_packed(self._ctx, int(npix), _ptr(int(rec_ptr)), _ptr(int(obs_ptr)), _ptr(ws),
+                                               _ptr(int(mask_ptr)) if mask_ptr else None, len(fm), _ptr(fm),
+                                               _ptr(int(ptan_ptr)), _ptr(int(stokes_ptr)) if stokes_ptr else None,
+                                               _ptr(int(chi2_ptr)), _ptr(int(grad_ptr)), MEM_DEVICE))
+
+    def adjoint_packed(self, records, obs, field_mask, packed_tangents, w_stokes=(1.0, 1.0, 1.0, 1.0), mask=None,
+                       out=None):
+        """snapi_adjoint with packed node tangents (see pack_tangents); host arrays."""
+        rec = _f32(records)
+        npix = self._npix(rec)
+        ob = _f32(obs)
+        pt = _f32(packed_tangents)
+        mk = _f32(mask)
+        fm = np.ascontiguousarray(field_mask, dtype=np.uint64)
+        npar = len(fm)
+        ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
+        out = out or {}
+        st = out.get("stokes", np.zeros((npix, self.nl, 4), np.float32))
+        chi2 = out.get("chi2", np.zeros(npix))
+        grad = out.get("grad", np.zeros((npix, npar)))
+        self._check(lib().snapi_adjoint_packed(self._ctx, npix, _ptr(rec), _ptr(ob), _ptr(ws), _ptr(mk), npar, _ptr(fm),
+                                               _ptr(pt), _ptr(st), _ptr(chi2), _ptr(grad), MEM_HOST))
+        return {"stokes": st, "chi2": chi2, "grad": grad.reshape(npix, npar)}
 
     def fd_grad_device(self, npix, rec_ptr, obs_ptr, npar, tan_ptr, step, chi2_ptr, grad_ptr,
                        w_stokes=(1.0, 1.0, 1.0, 1.0)):

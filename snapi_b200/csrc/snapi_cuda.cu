@@ -234,9 +234,18 @@ __global__ void __launch_bounds__(kFinishThreads) k_adjoint_finish(KParams P) {
     for (int i = threadIdx.x; i < nrec; i += blockDim.x)
       P.rec_grad[(size_t)pix * nrec + i] = (double)rb[i] * P.scale2;
   for (int p = 0; p < P.npar; ++p) {
-    const float *tp = P.tangent + ((size_t)pix * P.npar + p) * nrec;
     double g = 0.0;
-    for (int i = threadIdx.x; i < nrec; i += blockDim.x) g += (double)rb[i] * (double)tp[i];
+    if (P.ntcol) {  // packed: node p's columns, each a depth profile of one record field
+      const int c0 = P.tcol_off[p], n = (P.tcol_off[p + 1] - c0) * P.nd;
+      const float *tp = P.tangent + ((size_t)pix * P.ntcol + c0) * P.nd;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int c = i / P.nd, z = i % P.nd;
+        g += (double)rb[z * P.nfield + P.tcol_field[c0 + c]] * (double)tp[i];
+      }
+    } else {
+      const float *tp = P.tangent + ((size_t)pix * P.npar + p) * nrec;
+      for (int i = threadIdx.x; i < nrec; i += blockDim.x) g += (double)rb[i] * (double)tp[i];
+    }
     const double gt = block_sum(g, wred);
     if (threadIdx.x == 0) P.grad[(size_t)pix * P.npar + p] = gt * P.scale2;
   }
@@ -499,7 +508,7 @@ void snapi_destroy(snapi_ctx *ctx) {
   void *bufs[] = {ctx->d_lamvac, ctx->d_D, ctx->d_lines, ctx->d_compS, ctx->d_compD, ctx->d_status,
                   ctx->d_rec, ctx->d_stokes, ctx->d_obs, ctx->d_mask, ctx->d_tan, ctx->d_recgrad,
                   ctx->d_dstokes, ctx->d_opart, ctx->d_seed, ctx->d_bars, ctx->d_grad, ctx->d_chi2, ctx->d_c2part, ctx->d_step,
-                  ctx->d_scratch};
+                  ctx->d_scratch, ctx->d_tcol};
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -679,17 +688,18 @@ int snapi_synth(snapi_ctx *ctx, int npix, const float *records, float *stokes, i
   return check_status(ctx);
 }
 
-int snapi_adjoint(snapi_ctx *ctx, int npix, const float *records, const float *obs, const double *w_stokes,
-                  const float *mask, int npar, const float *tangents, float *stokes, double *chi2, double *grad,
-                  double *rec_grad, int mem) {
-  if (!ctx) return SNAPI_EINVAL;
-  if (npix < 0 || npar < 0 || (npix > 0 && (!records || !obs || !chi2)) || (npar > 0 && (!tangents || !grad)) ||
-      (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
-    return set_err(ctx, SNAPI_EINVAL, "snapi_adjoint: invalid arguments");
-  SNAPI_CK(cudaSetDevice(ctx->device));
+}  // extern "C"
+
+namespace {
+// the adjoint for dense (ntcol = 0) or packed (ntcol columns per pixel) node tangents
+int adjoint_impl(snapi_ctx *ctx, int npix, const float *records, const float *obs, const double *w_stokes,
+                 const float *mask, int npar, int ntcol, const float *tangents, float *stokes, double *chi2,
+                 double *grad, double *rec_grad, int mem) {
   int st = ensure_npar(ctx, npar > 0 ? npar : 1);
   if (st) return st;
   const size_t nrec = (size_t)ctx->nd * ctx->nfield, nl4 = (size_t)ctx->nl * 4;
+  // tangent floats per pixel as stored by the caller
+  const size_t ntan = ntcol ? (size_t)ntcol * ctx->nd : (size_t)npar * nrec;
   const SmemLayout Lsw = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false);
   const SmemLayout Lfin = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, true);
   ctx->last_ms = 0.0;
@@ -710,17 +720,20 @@ int snapi_adjoint(snapi_ctx *ctx, int npix, const float *records, const float *o
       KParams P = base_params(ctx);
       P.npix = nb;
       P.npar = npar;
+      P.ntcol = ntcol;
+      P.tcol_off = ntcol ? ctx->d_tcol : nullptr;
+      P.tcol_field = ntcol ? ctx->d_tcol + npar + 1 : nullptr;
       for (int s = 0; s < 4; ++s) P.ws[s] = w_stokes ? w_stokes[s] : 1.0;
       const int h = ctx->max_batch >= 2 ? (k & 1) : 0;  // one pixel of staging: no second half
       if (dev) {
         P.rec = records + p0 * nrec;
         P.obs = obs + (size_t)p0 * nl4;
         P.mask = mask ? mask + (size_t)p0 * ctx->nl : nullptr;
-        P.tangent = npar ? tangents + (size_t)p0 * npar * nrec : nullptr;
+        P.tangent = npar ? tangents + (size_t)p0 * ntan : nullptr;
       } else {
         const size_t off = (size_t)h * half;
         float *drec = ctx->d_rec + off * nrec, *dobs = ctx->d_obs + off * nl4, *dmask = ctx->d_mask + off * ctx->nl;
-        float *dtan = ctx->d_tan + off * (size_t)(npar ? npar : 1) * nrec;
+        float *dtan = ctx->d_tan + off * (ntan ? ntan : nrec);
         cudaStream_t cs = ctx->copy_stream;
         SNAPI_CK(cudaStreamWaitEvent(cs, ctx->ev_free[h], 0));  // chunk k-2 is done with this half
         SNAPI_CK(cudaMemcpyAsync(drec, records + p0 * nrec, sizeof(float) * nb * nrec, cudaMemcpyHostToDevice, cs));
@@ -729,7 +742,7 @@ int snapi_adjoint(snapi_ctx *ctx, int npix, const float *records, const float *o
           SNAPI_CK(cudaMemcpyAsync(dmask, mask + (size_t)p0 * ctx->nl, sizeof(float) * nb * ctx->nl,
                                    cudaMemcpyHostToDevice, cs));
         if (npar)
-          SNAPI_CK(cudaMemcpyAsync(dtan, tangents + (size_t)p0 * npar * nrec, sizeof(float) * nb * npar * nrec,
+          SNAPI_CK(cudaMemcpyAsync(dtan, tangents + (size_t)p0 * ntan, sizeof(float) * nb * ntan,
                                    cudaMemcpyHostToDevice, cs));
         SNAPI_CK(cudaEventRecord(ctx->ev_copy[h], cs));
         SNAPI_CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_copy[h], 0));
@@ -766,6 +779,54 @@ int snapi_adjoint(snapi_ctx *ctx, int npix, const float *records, const float *o
     ctx->last_ms = ms;  // first kernel start to the end of the last chunk (host copies included)
   }
   return check_status(ctx);
+}
+}  // namespace
+
+extern "C" {
+
+int snapi_adjoint(snapi_ctx *ctx, int npix, const float *records, const float *obs, const double *w_stokes,
+                  const float *mask, int npar, const float *tangents, float *stokes, double *chi2, double *grad,
+                  double *rec_grad, int mem) {
+  if (!ctx) return SNAPI_EINVAL;
+  if (npix < 0 || npar < 0 || (npix > 0 && (!records || !obs || !chi2)) || (npar > 0 && (!tangents || !grad)) ||
+      (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
+    return set_err(ctx, SNAPI_EINVAL, "snapi_adjoint: invalid arguments");
+  SNAPI_CK(cudaSetDevice(ctx->device));
+  return adjoint_impl(ctx, npix, records, obs, w_stokes, mask, npar, 0, tangents, stokes, chi2, grad, rec_grad, mem);
+}
+
+int snapi_adjoint_packed(snapi_ctx *ctx, int npix, const float *records, const float *obs, const double *w_stokes,
+                         const float *mask, int npar, const unsigned long long *field_mask,
+                         const float *packed_tangents, float *stokes, double *chi2, double *grad, int mem) {
+  if (!ctx) return SNAPI_EINVAL;
+  if (npix < 0 || npar < 1 || !field_mask || (npix > 0 && (!records || !obs || !chi2 || !grad || !packed_tangents)) ||
+      (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE) || ctx->nfield > 64)
+    return set_err(ctx, SNAPI_EINVAL, "snapi_adjoint_packed: invalid arguments");
+  std::vector<int> tab(npar + 1, 0);
+  for (int p = 0; p < npar; ++p) {
+    if (ctx->nfield < 64 && (field_mask[p] >> ctx->nfield) != 0ull)
+      return set_err(ctx, SNAPI_EINVAL, "snapi_adjoint_packed: field_mask[%d] names fields beyond nfield", p);
+    tab[p + 1] = tab[p] + __builtin_popcountll(field_mask[p]);
+  }
+  const int ntcol = tab[npar];
+  if (ntcol < 1) return set_err(ctx, SNAPI_EINVAL, "snapi_adjoint_packed: empty field masks");
+  for (int p = 0; p < npar; ++p)
+    for (int f = 0; f < ctx->nfield; ++f)
+      if ((field_mask[p] >> f) & 1ull) tab.push_back(f);
+  SNAPI_CK(cudaSetDevice(ctx->device));
+  if ((int)tab.size() > ctx->cap_tcol) {
+    SNAPI_CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->d_tcol);
+    ctx->d_tcol = nullptr;
+    ctx->cap_tcol = 0;
+    SNAPI_CK(cudaMalloc(&ctx->d_tcol, sizeof(int) * tab.size()));
+    ctx->cap_tcol = (int)tab.size();
+  }
+  // stream-ordered after every earlier kernel of this context, before this call's kernels; the
+  // source is pageable, so the copy has completed when the call returns
+  SNAPI_CK(cudaMemcpyAsync(ctx->d_tcol, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice, ctx->stream));
+  return adjoint_impl(ctx, npix, records, obs, w_stokes, mask, npar, ntcol, packed_tangents, stokes, chi2, grad,
+                      nullptr, mem);
 }
 
 int snapi_fd_grad(snapi_ctx *ctx, int npix, const float *records, const float *obs, const double *w_stokes,

@@ -55,7 +55,10 @@ struct KParams {
   const float *obs;             // [npix][nl][4]
   double ws[4];
   const float *mask;            // [npix][nl] or null
-  const float *tangent;         // [npix][npar][nd][nfield] or null
+  const float *tangent;         // [npix][npar][nd][nfield], or packed [npix][ntcol][nd]; or null
+  const int *tcol_off;          // packed tangents: node p's columns are [tcol_off[p], tcol_off[p+1])
+  const int *tcol_field;        // packed tangents: record field of each column
+  int ntcol;                    // packed tangents: columns per pixel (0: dense)
   float4 *scratch;              // [npix][nd][4][lpad]     forward state of the adjoint
   float4 *seed;                 // [npix][lpad]            adjoint of the emergent Stokes vector
   float4 *bars;                 // [npix][nl][3][nd]       (eta-bar, j-bar) per wavelength, depth
@@ -285,6 +288,8 @@ struct snapi_ctx {
   snapi::LineConst *d_lines = nullptr;
   float *d_compS = nullptr, *d_compD = nullptr;
   int *d_status = nullptr;
+  int *d_tcol = nullptr;  // packed-tangent column tables: offsets [npar+1] then fields [ntcol]
+  int cap_tcol = 0;
   // work buffers (max_batch pixels)
   float *d_rec = nullptr, *d_stokes = nullptr, *d_obs = nullptr, *d_mask = nullptr, *d_tan = nullptr;
   float *d_dstokes = nullptr, *d_opart = nullptr;

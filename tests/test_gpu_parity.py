@@ -256,3 +256,20 @@ def test_responses_match_oracle_and_reference(sb, oracle_lib, config3):
             # (inclination nodes; 0.1-1 % elsewhere)
             rr = fx["responses"][p, q]
             assert np.abs(ds[p, q] - rr).max() < 8e-2 * np.abs(rr).max(), (p, q)
+
+
+def test_packed_tangents_match_dense(sb, config3):
+    """snapi_adjoint_packed (only the record fields each node touches) gives the dense result."""
+    fx = config3
+    obs = fx["target"]
+    tan = fx["tangent"]
+    fm = sb.tangent_field_mask(tan)
+    assert sum(bin(int(m)).count("1") for m in fm) < tan.shape[1] * tan.shape[3]
+    ptan = sb.pack_tangents(tan, fm)
+    ctx = _ctx(sb, fx, max_batch=5)  # several rounds and chunks of the pipelined host path
+    dense = ctx.adjoint(fx["record"], obs, tan)
+    packed = ctx.adjoint_packed(fx["record"], obs, fm, ptan)
+    ctx.close()
+    np.testing.assert_allclose(packed["chi2"], dense["chi2"], rtol=1e-12)
+    np.testing.assert_allclose(packed["grad"], dense["grad"], rtol=1e-6, atol=1e-9 * np.abs(dense["grad"]).max())
+    assert np.array_equal(packed["stokes"], dense["stokes"])
