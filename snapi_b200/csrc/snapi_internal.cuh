@@ -162,9 +162,24 @@ struct RtScratch {
   float4 *bars;
   int lpad, l, nd;
   bool write;  // false for the padding lanes of the last wavelength chunk
-  __device__ void load(int z, float *I, float *kp, float *S, float &e, float &tau) const {
+  // the sweep asks for depth z+2 while it works on depth z, so the (DRAM-latency) loads of a
+  // depth overlap the 4x4 algebra of the one before
+  float4 pf[4];
+  int pz = -1;
+  __device__ void prefetch(int z) {
+    if (z >= nd) return;
     const float4 *p = state + (size_t)z * 4 * lpad + l;
-    float4 a = p[0], b = p[lpad], c = p[2 * lpad], d = p[3 * lpad];
+    pf[0] = p[0]; pf[1] = p[lpad]; pf[2] = p[2 * lpad]; pf[3] = p[3 * lpad];
+    pz = z;
+  }
+  __device__ void load(int z, float *I, float *kp, float *S, float &e, float &tau) {
+    float4 a, b, c, d;
+    if (z == pz) {
+      a = pf[0]; b = pf[1]; c = pf[2]; d = pf[3];
+    } else {
+      const float4 *p = state + (size_t)z * 4 * lpad + l;
+      a = p[0]; b = p[lpad]; c = p[2 * lpad]; d = p[3 * lpad];
+    }
     I[0] = a.x; I[1] = a.y; I[2] = a.z; I[3] = a.w;
     kp[0] = b.x; kp[1] = b.y; kp[2] = b.z; kp[3] = b.w;
     kp[4] = c.x; kp[5] = c.y; e = c.z; tau = c.w;

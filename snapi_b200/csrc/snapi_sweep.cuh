@@ -101,6 +101,7 @@ SNAPI_HD void reverse_sweep_rt(const PixelView &pv, const float *Ib_in, SC &sc) 
     sc.load(0, Id, kpm, Sm, em_, td);
   }
   sc.load(1, Ic, kpc, Sc, ec, tauc);
+  sc.prefetch(2);
 #pragma unroll
   for (int s = 0; s < 4; ++s) { Ib[s] = Ib_in[s]; Sbm[s] = 0.f; Sbc[s] = 0.f; }
 #pragma unroll
@@ -108,6 +109,7 @@ SNAPI_HD void reverse_sweep_rt(const PixelView &pv, const float *Ib_in, SC &sc) 
   ebm = 0.f; ebc = 0.f; opdb_c = 0.0;
   for (int z = 1; z <= nd - 2; ++z) {
     sc.load(z + 1, In, kpn, Sn, en, taun);
+    sc.prefetch(z + 2);
 #pragma unroll
     for (int s = 0; s < 4; ++s) Sbn[s] = 0.f;
 #pragma unroll

@@ -99,6 +99,7 @@ struct HostScratch {
     for (int q = 0; q < 6; ++q) p[4 + q] = kp[q];
     p[10] = e; p[11] = tau;
   }
+  void prefetch(int) {}
   void load(int z, float *I, float *kp, float *S, float &e, float &tau) const {
     const float *p = &buf[z * 16];
     for (int s = 0; s < 4; ++s) { I[s] = p[s]; S[s] = p[12 + s]; }
