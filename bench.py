@@ -125,7 +125,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def dist_setup(args):
+def dist_setup(args=None, backend="nccl"):
+    """One process per GPU (torchrun's RANK / WORLD_SIZE / LOCAL_RANK).  Pixels are independent, so
+    the ranks only meet for barriers around the timed region and the max-over-ranks time."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -133,8 +135,14 @@ def dist_setup(args):
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
+
+
+def job_throughput(pixels_per_rank, ms_per_step, world, device):
+    """Whole-job pixels/s: every rank's pixels over the slowest rank's step time."""
+    ms = reduce_max(ms_per_step, world, device)
+    return pixels_per_rank * world / (ms / 1e3), ms
 
 
 def reduce_max(x, world, device):
@@ -213,9 +221,7 @@ def run_snapi(args):
     total_ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     barrier(world)
-    total_ms = reduce_max(total_ms, world, dev)
-    ms_step = total_ms / args.steps
-    value = NPIX * world / (ms_step / 1e3)
+    value, ms_step = job_throughput(NPIX, total_ms / args.steps, world, dev)
 
     # plain FD gradient (2 npar + 1 forward solves) on the same inputs, for the adjoint-vs-FD ratio
     def fd_step():
