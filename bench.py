@@ -38,6 +38,11 @@ REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "snapi_ref_bench")
 METRIC = "pixels/s Stokes synth+grad on 1 B200, adjoint vs plain FD, at 1e-5 Ic"
 NPIX = 64 * 64
 FD_STEPS = np.array([5.0, 5.0, 5.0, 5.0, 2e3, 2e3, 2e3, 5.0, 5e-3, 5e-3])
+# ncu (--set full) of the four adjoint kernels on 2048 pixels of this workload, per pixel:
+# dram__bytes_read.sum + dram__bytes_write.sum, and executed FP32 flop (2 FFMA + FMUL + FADD)
+NCU_DRAM_BYTES_PER_PIXEL = 4.96e6
+NCU_FP32_FLOP_PER_PIXEL = 7.49e7
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FMA rate at the 1965 MHz max clock
 
 
 def make_workload(pool, npix=NPIX, seed=3, return_nodes=False):
@@ -301,9 +306,18 @@ def run_snapi(args):
             "fd_baseline": {"value": NPIX * world / (fd_ms / 1e3), "unit": "pixels/s", "ms_per_step": fd_ms,
                             "solves_per_gradient": 2 * npar + 1, "adjoint_speedup": fd_ms / ms_step},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "traffic": None,
-                         "peak_source": peaks["source"], "kernel": "k_adjoint",
-                         "note": "compute (FP32/SFU issue) bound, not HBM bound; see DESIGN.md"},
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": NCU_DRAM_BYTES_PER_PIXEL * NPIX,
+                         "traffic_achieved_gbs": NCU_DRAM_BYTES_PER_PIXEL * NPIX / (kern_per_launch_ms / 1e3) / 1e9,
+                         "peak_source": peaks["source"],
+                         "kernel": "adjoint call (k_adj_forward + k_adj_rt + k_adj_opacity + k_adjoint_finish)",
+                         "note": "achieved = algorithmic bytes (inputs + outputs); traffic (ncu, scaled from "
+                                 "2048 pixels) includes the reverse-mode state written and read back on purpose; "
+                                 "the kernels are FP32-issue bound (see fp32)"},
+            "fp32": {"achieved": NCU_FP32_FLOP_PER_PIXEL * NPIX / (kern_per_launch_ms / 1e3) / 1e12,
+                     "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
+                     "frac": NCU_FP32_FLOP_PER_PIXEL * NPIX / (kern_per_launch_ms / 1e3) / 1e12 / FP32_PEAK_TFLOPS,
+                     "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1965 MHz)",
+                     "flop": "executed FP32 flop per pixel from ncu, not an algorithmic count"},
         }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = reference_cpu_rate(samples_per_core=1, mode=1)
