@@ -232,6 +232,13 @@ int snapi_ali_iter(snapi_ali_ctx *ctx, int ncol, const snapi_ali_columns *cols, 
                    double tol, double *rel_change, int *iters, int *status, int mem);
 double snapi_ali_last_kernel_ms(const snapi_ali_ctx *ctx);
 
+/* Batched small Gram matrices on the tensor cores: G[m] = M[m] M[m]^T for nmat matrices M[m]
+ * [16][K] (row-major, float32, device memory), G [nmat][16][16] float32 (device).  tcgen05 MMA with a
+ * three-product TF32 split (hi hi^T + hi lo^T + lo hi^T), FP32 accumulation: ~1e-6 relative.  This
+ * is how snapi_lm_step forms J^T J and J^T r (atmos_fit.cc:135-137) for up to 15 nodes; exported for
+ * callers with their own small normal equations.  stream: a cudaStream_t or NULL. */
+int snapi_batched_gram(int nmat, int K, const float *M, float *G, void *stream);
+
 int snapi_zeeman_pattern(int ju2, int jl2, double g_upper, double g_lower, snapi_line *line);
 
 /* Pinned host memory for SNAPI_MEM_HOST arguments. */

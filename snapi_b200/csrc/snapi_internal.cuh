@@ -328,6 +328,8 @@ int check_status(snapi_ctx *ctx);
 cudaError_t launch_synth(const snapi_ctx *ctx, const KParams &P);
 cudaError_t launch_responses(const snapi_ctx *ctx, const KParams &P);
 void lm_free(snapi_ctx *ctx);  // LM work buffers (snapi_lm.cu)
+// G[m] = M[m] M[m]^T for nmat matrices [16][K] (row-major) on the tensor cores (snapi_tc.cu)
+cudaError_t launch_gram_tf32(const float *M, int nmat, int K, float *G, int *status, cudaStream_t st);
 }  // namespace snapi
 
 #define SNAPI_CK(call)                                                                                  \

@@ -6,7 +6,10 @@
 //   k_synth          Stokes at the requested nodes (pixels that are done are skipped)
 //   k_lm_eval        one CTA per pixel: chi2, accept / reject, damping, tracked chi2, stop rules
 //   k_resp_sweep     Jacobian at the newly accepted nodes (central differences along tangents)
-//   k_lm_solve       one CTA per pixel: J^T J and J^T r in FP64, damped, symmetric
+//   k_lm_rows        scaled Jacobian rows and residual of every pixel, 16 rows per pixel
+//   k_gram_tf32      J^T J and J^T r of 8 pixels per CTA on the tcgen05 tensor cores, FP32
+//                    accuracy by a three-product TF32 split (snapi_tc.cu); npar <= 15
+//   k_lm_solve       one CTA per pixel: (J^T J and J^T r in FP64 when npar > 15), damped, symmetric
 //                    eigen-decomposition (cyclic Jacobi) with the reference's 1e6 condition cut,
 //                    bracketed trial nodes for the next call
 #include <cmath>
@@ -47,6 +50,7 @@ struct LmDev {
   double *nodes, *req;       // [npix][npar]
   LmPix *pix;
   int *skip_syn, *skip_resp, *active;
+  const float *G;            // [npix][16][16] tensor-core J^T J | J^T r, or null (FP64 sums here)
 };
 
 struct LmWork {
@@ -56,7 +60,7 @@ struct LmWork {
   double *d_nodes = nullptr, *d_req = nullptr, *d_step = nullptr;
   LmPix *d_pix = nullptr;
   float *d_obs = nullptr, *d_mask = nullptr, *d_scur = nullptr, *d_snew = nullptr, *d_J = nullptr;
-  float *d_rec = nullptr, *d_tan = nullptr;
+  float *d_rec = nullptr, *d_tan = nullptr, *d_M = nullptr, *d_G = nullptr;
   int *d_skip_syn = nullptr, *d_skip_resp = nullptr, *d_active = nullptr;
   std::vector<int> h_active, kind;
 };
@@ -172,6 +176,23 @@ __device__ void jacobi_eigen(double *A, double *V, int n) {
   }
 }
 
+// Rows of the tensor-core Gram product: row i < npar = J_i * scale_i * w_s * mask / I_c, row npar =
+// (obs - S) * w_s * mask / I_c, the rest zero (atmos_fit.cc:229-260); one CTA per (pixel, row).
+__global__ void k_lm_rows(LmDev D, float *Mrows) {
+  const int p = blockIdx.x / 16, i = blockIdx.x % 16, K = D.nl * 4;
+  if (D.pix[p].phase == PH_DONE) return;  // CTA-uniform; the solve skips the pixel too
+  float *out = Mrows + ((size_t)p * 16 + i) * K;
+  const double ic = sqrt(D.scale2);
+  const float *mk = D.mask ? D.mask + (size_t)p * D.nl : nullptr;
+  for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    const double w = D.ws[k & 3] * (mk ? (double)mk[k >> 2] : 1.0) / ic;
+    double v = 0.0;
+    if (i < D.npar) v = (double)D.J[((size_t)p * D.npar + i) * K + k] * w * D.scale[i];
+    else if (i == D.npar) v = ((double)D.obs[(size_t)p * K + k] - (double)D.scur[(size_t)p * K + k]) * w;
+    out[k] = (float)v;
+  }
+}
+
 // damped normal equations and the trial nodes (atmos_fit.cc:127-160, mathtools.cc:344-390)
 __global__ void __launch_bounds__(kLmThreads) k_lm_solve(LmDev D) {
   __shared__ double A[kMaxPar * kMaxPar], V[kMaxPar * kMaxPar], rhs[kMaxPar];
@@ -190,7 +211,15 @@ __global__ void __launch_bounds__(kLmThreads) k_lm_solve(LmDev D) {
   // one thread per entry of the upper triangle of J^T J, then one per entry of J^T r; J is
   // scaled by node scale x w_s x mask, r = (obs - S) w_s mask (atmos_fit.cc:229-260)
   const int npair = n * (n + 1) / 2;
-  for (int e = threadIdx.x; e < npair + n; e += blockDim.x) {
+  if (D.G) {  // tensor-core Gram matrix: [0, n) x [0, n) is J^T J, column n is J^T r
+    const float *g = D.G + (size_t)p * 256;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int i = e / n, j = e % n;
+      A[e] = 0.5 * ((double)g[i * 16 + j] + (double)g[j * 16 + i]);
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) rhs[i] = (double)g[i * 16 + n];
+  }
+  for (int e = threadIdx.x; e < (D.G ? 0 : npair + n); e += blockDim.x) {
     int i, j;
     if (e < npair) {
       i = 0;
@@ -257,13 +286,13 @@ void node_constants(int kind, double &scale, double &lo, double &hi) {
 LmWork *work(snapi_ctx *ctx) { return static_cast<LmWork *>(ctx->lm); }
 
 void free_bufs(LmWork *w) {
-  void *b[] = {w->d_nodes, w->d_req, w->d_step, w->d_pix, w->d_obs, w->d_mask, w->d_scur, w->d_snew,
+  void *b[] = {w->d_M, w->d_G, w->d_nodes, w->d_req, w->d_step, w->d_pix, w->d_obs, w->d_mask, w->d_scur, w->d_snew,
                w->d_J, w->d_rec, w->d_tan, w->d_skip_syn, w->d_skip_resp, w->d_active};
   for (void *x : b)
     if (x) cudaFree(x);
   w->d_nodes = w->d_req = w->d_step = nullptr;
   w->d_pix = nullptr;
-  w->d_obs = w->d_mask = w->d_scur = w->d_snew = w->d_J = w->d_rec = w->d_tan = nullptr;
+  w->d_obs = w->d_mask = w->d_scur = w->d_snew = w->d_J = w->d_rec = w->d_tan = w->d_M = w->d_G = nullptr;
   w->d_skip_syn = w->d_skip_resp = w->d_active = nullptr;
   w->cap = w->cap_par = 0;
 }
@@ -307,6 +336,10 @@ int snapi_lm_begin(snapi_ctx *ctx, int npix, const snapi_lm_opts *opts, const do
     SNAPI_CK(cudaMalloc(&w->d_scur, sizeof(float) * npix * nl * 4));
     SNAPI_CK(cudaMalloc(&w->d_snew, sizeof(float) * npix * nl * 4));
     SNAPI_CK(cudaMalloc(&w->d_J, sizeof(float) * npix * npar * nl * 4));
+    if (npar + 1 <= 16) {  // tensor-core normal equations
+      SNAPI_CK(cudaMalloc(&w->d_M, sizeof(float) * npix * 16 * nl * 4));
+      SNAPI_CK(cudaMalloc(&w->d_G, sizeof(float) * npix * 256));
+    }
     SNAPI_CK(cudaMalloc(&w->d_rec, sizeof(float) * npix * nrec));
     SNAPI_CK(cudaMalloc(&w->d_tan, sizeof(float) * npix * npar * nrec));
     SNAPI_CK(cudaMalloc(&w->d_skip_syn, sizeof(int) * npix));
@@ -421,10 +454,17 @@ int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, d
   R.dstokes = w->d_J;
   R.skip = w->d_skip_resp;
   SNAPI_CK(launch_responses(ctx, R));
-  k_lm_solve<<<npix, kLmThreads, 0, ctx->stream>>>(w->D);
+  LmDev Ds = w->D;
+  if (w->d_G && npar + 1 <= 16) {
+    k_lm_rows<<<npix * 16, 256, 0, ctx->stream>>>(Ds, w->d_M);
+    SNAPI_CK(cudaGetLastError());
+    SNAPI_CK(launch_gram_tf32(w->d_M, npix, ctx->nl * 4, w->d_G, ctx->d_status, ctx->stream));
+    Ds.G = w->d_G;
+  }
+  k_lm_solve<<<npix, kLmThreads, 0, ctx->stream>>>(Ds);
   SNAPI_CK(cudaGetLastError());
   SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-  ctx->last_launches = 4;
+  ctx->last_launches = Ds.G ? 6 : 4;
   SNAPI_CK(cudaMemcpyAsync(w->h_active.data(), w->d_active, sizeof(int) * npix, cudaMemcpyDeviceToHost, ctx->stream));
   if (dev) {
     SNAPI_CK(cudaMemcpyAsync(request, w->d_req, sizeof(double) * npix * npar, cudaMemcpyDeviceToDevice, ctx->stream));
