@@ -163,6 +163,9 @@ typedef struct {
   double delta;             /* relative chi2 change that ends the fit (atmos_fit.cc:16, 1e-3) */
   double stopping_chisq;    /* chi2 below which the fit ends after one more step */
   const double *resp_step;  /* [npar] central-difference steps of the Jacobian, node units */
+  double spectral_broadening; /* Gaussian instrumental width [cm] (cfg SPECTRAL_BROADENING mA x 1e-11
+                                 / 2.35), applied to the Stokes vectors and the Jacobian as
+                                 stokes_lm_fit does (atmos_fit.cc:104-109); 0: none */
 } snapi_lm_opts;
 
 /* nodes0, request: double [npix][npar]; obs float [npix][nlambda][4]; mask float [npix][nlambda]
@@ -238,6 +241,14 @@ double snapi_ali_last_kernel_ms(const snapi_ali_ctx *ctx);
  * is how snapi_lm_step forms J^T J and J^T r (atmos_fit.cc:135-137) for up to 15 nodes; exported for
  * callers with their own small normal equations.  stream: a cudaStream_t or NULL. */
 int snapi_batched_gram(int nmat, int K, const float *M, float *G, void *stream);
+
+/* Gaussian instrumental broadening in place: spectra [nvec][nlambda][4] on the context's wavelength
+ * grid (convolve_spectra_with_gauss, cmlib/mathtools.cc:1350-1414; observable::spectral_convolve).
+ * width [cm] as the reference holds it (cfg SPECTRAL_BROADENING in mA x 1e-11 / 2.35).  Where the
+ * reference reads an unset interval width (the first interval of its interpolation grid,
+ * mathtools.cc:1073-1093) this uses that interval's width; the reference's output there is undefined
+ * (values up to 1e44, which its kernel tails spread over ~12 widths from the blue end). */
+int snapi_spectral_broaden(snapi_ctx *ctx, int nvec, float *spectra, double width, int mem);
 
 int snapi_zeeman_pattern(int ju2, int jl2, double g_upper, double g_lower, snapi_line *line);
 

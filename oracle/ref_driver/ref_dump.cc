@@ -10,8 +10,11 @@
 //       responses (obs_stokes_responses_to_nodes), the record tangents d(record)/d(node)
 //       (central differences of build_from_nodes / interpolate_from_nodes with the
 //       reference's own steps) and the reference's normalised opacity at a few wavelengths.
-//   snapi_ref_dump lmfit  <task.tsk> <nodes0.f64> <target.f64> <mask.f64> <npix> <iters> <out.sbin>
-//       Run stokes_lm_fit per pixel from the initial nodes against target Stokes.
+//   snapi_ref_dump lmfit  <task.tsk> <nodes0.f64> <target.f64> <mask.f64> <npix> <iters> <out.sbin> [width]
+//       Run stokes_lm_fit per pixel from the initial nodes against target Stokes (optionally with
+//       Gaussian spectral broadening of width [cm]).
+//   snapi_ref_dump conv   <in.f64> <nlambda> <nvec> <width_cm> <out.f64>
+//       Gaussian instrumental broadening of nvec Stokes spectra (convolve_spectra_with_gauss).
 //   snapi_ref_dump ali    <task.tsk> <nodes.f64> <ncol> <niter> <out.sbin>
 //       NLTE level-population iteration inputs, niter iterations of the reference's loop, and the
 //       populations nltepops converges to (see do_ali).
@@ -389,7 +392,7 @@ static int do_dump(const char *tskname, const char *nodesname, int npix, int fla
 // ----------------------------------------------------------------------------------------------
 // lmfit: reference LM inversion per pixel (atmos_fit.cc:18-227)
 static int do_lmfit(const char *tskname, const char *n0name, const char *tgtname, const char *maskname,
-                    int npix, int iters, const char *outname) {
+                    int npix, int iters, const char *outname, double broadening) {
   const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
   const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
   int ac = 4; cmdln cmd(ac, (char **)argv, options, maps);
@@ -423,7 +426,7 @@ static int do_lmfit(const char *tskname, const char *n0name, const char *tgtname
     o->set_stopping_chisq(1E-30);
     fp_t ws[4] = {1.0, 1.0, 1.0, 1.0};
     o->set_w_stokes(ws);
-    o->set_inv_parameters(0.0, 0.0, 1.0, 1.0);
+    o->set_inv_parameters(0.0, broadening, 1.0, 1.0);  // spectral broadening [cm], 0: none
     double t0 = wall_s();
     observable *fit = a->stokes_lm_fit(o, t.el, t.az, mm);
     t_fit += wall_s() - t0;
@@ -684,14 +687,43 @@ static int do_ali(const char *tskname, const char *nodesname, int ncol, int nite
   return 0;
 }
 
+// ----------------------------------------------------------------------------------------------
+// conv: the reference's Gaussian instrumental broadening (convolve_spectra_with_gauss,
+// cmlib/mathtools.cc:1350-1414) of nvec Stokes spectra.  in.f64: lambda [n], then S [nvec][n][4];
+// out.f64: the convolved S [nvec][n][4].
+static int do_conv(const char *inname, int n, int nvec, double width, const char *outname) {
+  std::vector<uint8_t> b = read_file_bytes(inname);
+  const double *lam = (const double *)b.data(), *S = lam + n;
+  fp_t *l1 = new fp_t[n] - 1;
+  for (int l = 0; l < n; ++l) l1[l + 1] = lam[l];
+  fp_t **T = ft2dim(1, 4, 1, n);
+  std::vector<double> out((size_t)nvec * n * 4);
+  for (int v = 0; v < nvec; ++v) {
+    for (int l = 0; l < n; ++l)
+      for (int s = 0; s < 4; ++s) T[s + 1][l + 1] = S[((size_t)v * n + l) * 4 + s];
+    convolve_spectra_with_gauss(T, l1, n, width);
+    for (int l = 0; l < n; ++l)
+      for (int s = 0; s < 4; ++s) out[((size_t)v * n + l) * 4 + s] = T[s + 1][l + 1];
+  }
+  FILE *f = fopen(outname, "wb");
+  fwrite(out.data(), 8, out.size(), f);
+  fclose(f);
+  del_ft2dim(T, 1, 4, 1, n);
+  delete[] (l1 + 1);
+  return 0;
+}
+
 int main(int argc, char **argv) {
   if (argc >= 4 && !strcmp(argv[1], "pack")) return do_pack(argv[2], argv[3]);
   if (argc >= 7 && !strcmp(argv[1], "dump"))
     return do_dump(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]), argv[6]);
+  if (argc >= 7 && !strcmp(argv[1], "conv"))
+    return do_conv(argv[2], atoi(argv[3]), atoi(argv[4]), atof(argv[5]), argv[6]);
   if (argc >= 7 && !strcmp(argv[1], "ali"))
     return do_ali(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]), argv[6]);
   if (argc >= 9 && !strcmp(argv[1], "lmfit"))
-    return do_lmfit(argv[2], argv[3], argv[4], argv[5], atoi(argv[6]), atoi(argv[7]), argv[8]);
+    return do_lmfit(argv[2], argv[3], argv[4], argv[5], atoi(argv[6]), atoi(argv[7]), argv[8],
+                    argc >= 10 ? atof(argv[9]) : 0.0);
   fprintf(stderr, "usage: snapi_ref_dump pack|dump|lmfit ...\n");
   return 1;
 }

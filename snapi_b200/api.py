@@ -71,6 +71,7 @@ class SnapiLmOpts(ctypes.Structure):
         ("delta", ctypes.c_double),
         ("stopping_chisq", ctypes.c_double),
         ("resp_step", ctypes.POINTER(ctypes.c_double)),
+        ("spectral_broadening", ctypes.c_double),
     ]
 
 
@@ -95,6 +96,7 @@ def lib():
         L.snapi_responses.argtypes = [vp, ip, fp, ip, fp, fp, fp, fp, ip]
         L.snapi_fd_grad.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, ip]
         L.snapi_adjoint_packed.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, fp, ip]
+        L.snapi_spectral_broaden.argtypes = [vp, ip, fp, ctypes.c_double, ip]
         L.snapi_zeeman_pattern.argtypes = [ip, ip, ctypes.c_double, ctypes.c_double, ctypes.POINTER(SnapiLine)]
         L.snapi_host_alloc.restype = vp
         L.snapi_host_alloc.argtypes = [ctypes.c_size_t]
@@ -286,7 +288,7 @@ class Context:
 
     # ---- batched Levenberg-Marquardt (stokes_lm_fit) ----------------------------------------
     def lm_begin(self, nodes0, obs, node_kind, resp_step, mask=None, w_stokes=(1.0, 1.0, 1.0, 1.0), lm_start=1e3,
-                 max_iter=30, delta=1e-3, stopping_chisq=1e-30):
+                 max_iter=30, delta=1e-3, stopping_chisq=1e-30, spectral_broadening=0.0):
         """Start a fit of every pixel; returns the (bracketed) node vectors to build first."""
         n0 = np.ascontiguousarray(nodes0, dtype=np.float64)
         npix, npar = n0.shape
@@ -296,7 +298,7 @@ class Context:
         self._lm_step = np.ascontiguousarray(np.broadcast_to(resp_step, (npar,)), dtype=np.float64)
         opts = SnapiLmOpts(npar, self._lm_kind.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), float(lm_start),
                            int(max_iter), float(delta), float(stopping_chisq),
-                           self._lm_step.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+                           self._lm_step.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), float(spectral_broadening))
         ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
         req = np.zeros_like(n0)
         self._check(lib().snapi_lm_begin(self._ctx, npix, ctypes.byref(opts), _ptr(n0), _ptr(ob), _ptr(ws), _ptr(mk),
@@ -340,6 +342,13 @@ class Context:
         out = self.lm_result()
         out["steps"] = steps
         return out
+
+    def broaden(self, spectra, width):
+        """Gaussian instrumental broadening of [nvec, nlambda, 4] spectra (returns a new array)."""
+        a = np.array(spectra, dtype=np.float32, order="C", copy=True)
+        nvec = a.size // (self.nl * 4)
+        self._check(lib().snapi_spectral_broaden(self._ctx, nvec, _ptr(a), float(width), MEM_HOST))
+        return a
 
     def responses(self, records, tangents, step, want_stokes=True):
         """d Stokes / d node [npix, npar, nlambda, 4] (obs_stokes_responses_to_nodes, batched) by

@@ -508,7 +508,7 @@ void snapi_destroy(snapi_ctx *ctx) {
   void *bufs[] = {ctx->d_lamvac, ctx->d_D, ctx->d_lines, ctx->d_compS, ctx->d_compD, ctx->d_status,
                   ctx->d_rec, ctx->d_stokes, ctx->d_obs, ctx->d_mask, ctx->d_tan, ctx->d_recgrad,
                   ctx->d_dstokes, ctx->d_opart, ctx->d_seed, ctx->d_bars, ctx->d_grad, ctx->d_chi2, ctx->d_c2part, ctx->d_step,
-                  ctx->d_scratch, ctx->d_tcol};
+                  ctx->d_scratch, ctx->d_tcol, ctx->d_lamair, ctx->d_psf_kt};
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -562,6 +562,7 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
   ctx->scale2 = prob->stokes_scale * prob->stokes_scale;
   std::vector<double> lv(ctx->nl);
   for (int l = 0; l < ctx->nl; ++l) lv[l] = airtovac_d(prob->lambda_air[l]);
+  ctx->h_lamair.assign(prob->lambda_air, prob->lambda_air + ctx->nl);
   ctx->lam_mid = (float)(0.5 * (lv[ctx->nl - 1] + lv[0]));
   std::vector<double> D(ctx->nd - 1);
   for (int i = 0; i + 1 < ctx->nd; ++i) D[i] = (prob->tau500[i + 1] - prob->tau500[i]) / prob->mu;
@@ -625,6 +626,8 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
   CKC(cudaMalloc(&ctx->d_status, sizeof(int)));
   CKC(cudaMemset(ctx->d_status, 0, sizeof(int)));
   CKC(cudaMemcpy(ctx->d_lamvac, lv.data(), sizeof(double) * ctx->nl, cudaMemcpyHostToDevice));
+  CKC(cudaMalloc(&ctx->d_lamair, sizeof(double) * ctx->nl));
+  CKC(cudaMemcpy(ctx->d_lamair, prob->lambda_air, sizeof(double) * ctx->nl, cudaMemcpyHostToDevice));
   CKC(cudaMemcpy(ctx->d_D, D.data(), sizeof(double) * (ctx->nd - 1), cudaMemcpyHostToDevice));
   if (ctx->nlines) CKC(cudaMemcpy(ctx->d_lines, lc.data(), sizeof(LineConst) * ctx->nlines, cudaMemcpyHostToDevice));
   if (ctx->ncomp) {

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/snapi_cuda.h"
 #include "snapi_sweep.cuh"
@@ -304,6 +305,12 @@ struct snapi_ctx {
   float *d_compS = nullptr, *d_compD = nullptr;
   int *d_status = nullptr;
   int *d_tcol = nullptr;  // packed-tangent column tables: offsets [npar+1] then fields [ntcol]
+  // Gaussian instrumental broadening (snapi_psf.cu): the observation's (air) grid and one width
+  std::vector<double> h_lamair;
+  double *d_lamair = nullptr;
+  float *d_psf_kt = nullptr;
+  double psf_width = 0.0, psf_lmin = 0.0, psf_step = 0.0;
+  int psf_nf = 0, psf_band = 0;
   int cap_tcol = 0;
   // work buffers (max_batch pixels)
   float *d_rec = nullptr, *d_stokes = nullptr, *d_obs = nullptr, *d_mask = nullptr, *d_tan = nullptr;
@@ -330,6 +337,9 @@ cudaError_t launch_responses(const snapi_ctx *ctx, const KParams &P);
 void lm_free(snapi_ctx *ctx);  // LM work buffers (snapi_lm.cu)
 // G[m] = M[m] M[m]^T for nmat matrices [16][K] (row-major) on the tensor cores (snapi_tc.cu)
 cudaError_t launch_gram_tf32(const float *M, int nmat, int K, float *G, int *status, cudaStream_t st);
+// Gaussian instrumental broadening (snapi_psf.cu): set-up for one width, in-place launch
+int psf_prepare(snapi_ctx *ctx, double width);
+cudaError_t psf_launch(const snapi_ctx *ctx, float *data, int nvec, int vec_per_pix, const int *skip);
 }  // namespace snapi
 
 #define SNAPI_CK(call)                                                                                  \

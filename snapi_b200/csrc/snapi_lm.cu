@@ -63,6 +63,7 @@ struct LmWork {
   float *d_rec = nullptr, *d_tan = nullptr, *d_M = nullptr, *d_G = nullptr;
   int *d_skip_syn = nullptr, *d_skip_resp = nullptr, *d_active = nullptr;
   std::vector<int> h_active, kind;
+  double broaden = 0.0;  // Gaussian instrumental width [cm], 0: none
 };
 
 __device__ double block_sum_d(double v, double *sh) {
@@ -352,6 +353,12 @@ int snapi_lm_begin(snapi_ctx *ctx, int npix, const snapi_lm_opts *opts, const do
   w->npar = npar;
   w->h_active.assign(npix, 1);
   w->kind.assign(opts->node_kind, opts->node_kind + npar);
+  w->broaden = opts->spectral_broadening;
+  if (w->broaden < 0.0) return set_err(ctx, SNAPI_EINVAL, "snapi_lm_begin: negative spectral broadening");
+  if (w->broaden > 0.0) {
+    const int st = psf_prepare(ctx, w->broaden);
+    if (st) return st;
+  }
   LmDev &D = w->D;
   memset(&D, 0, sizeof D);
   D.npix = npix; D.npar = npar; D.nl = nl;
@@ -442,6 +449,7 @@ int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, d
   P.stokes = w->d_snew;
   P.skip = w->d_skip_syn;
   SNAPI_CK(launch_synth(ctx, P));
+  if (w->broaden > 0.0) SNAPI_CK(psf_launch(ctx, w->d_snew, npix, 1, w->d_skip_syn));
   k_lm_eval<<<npix, kLmThreads, 0, ctx->stream>>>(w->D);
   SNAPI_CK(cudaGetLastError());
   KParams R = base_params(ctx);
@@ -454,6 +462,7 @@ int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, d
   R.dstokes = w->d_J;
   R.skip = w->d_skip_resp;
   SNAPI_CK(launch_responses(ctx, R));
+  if (w->broaden > 0.0) SNAPI_CK(psf_launch(ctx, w->d_J, npix * npar, npar, w->d_skip_resp));
   LmDev Ds = w->D;
   if (w->d_G && npar + 1 <= 16) {
     k_lm_rows<<<npix * 16, 256, 0, ctx->stream>>>(Ds, w->d_M);

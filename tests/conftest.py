@@ -41,6 +41,11 @@ def config4():
 
 
 @pytest.fixture(scope="session")
+def config4_psf():
+    return load_fixture("config4_psf")
+
+
+@pytest.fixture(scope="session")
 def config5():
     return load_fixture("config5")
 

@@ -199,27 +199,36 @@ def config4_inputs(npix, seed=4):
     return truth, truth + C4_OFFSET, mask
 
 
-def make_config4(tmp, npix, iters=30):
+def make_config4(tmp, npix, iters=30, broadening=0.0, name="config4"):
     """Reference LM (stokes_lm_fit, DELTA 1e-3 as compiled, start lambda 1e3) on config-4 pixels,
-    one process per pixel."""
+    one process per pixel; with broadening > 0 [cm] the targets are broadened by the reference's
+    own convolution and the fit broadens its synthesis and responses the same way."""
     task = os.path.join(tmp, "c3.tsk")
     truth, nodes0, mask = config4_inputs(npix)
     d = dump(tmp, task, truth, 0, "c4truth")
     rng = np.random.default_rng(44)
     ic = d["stokes"][:, :, 0].max(axis=1)
-    target = d["stokes"] + rng.normal(0.0, 1e-3, d["stokes"].shape) * ic[:, None, None]
+    stokes = d["stokes"]
+    if broadening > 0.0:
+        fin = os.path.join(tmp, "c4b_in.f64")
+        np.concatenate([d["lambda_air"], stokes.ravel()]).astype("<f8").tofile(fin)
+        fout = os.path.join(tmp, "c4b_out.f64")
+        run([DUMP, "conv", fin, str(d["lambda_air"].shape[0]), str(npix), repr(broadening), fout], tmp)
+        stokes = np.fromfile(fout, dtype="<f8").reshape(stokes.shape)
+    target = stokes + rng.normal(0.0, 1e-3, stokes.shape) * ic[:, None, None]
     procs = []
     for i in range(npix):
         for nm, arr in (("n0", nodes0[i:i + 1]), ("tg", target[i:i + 1]), ("mk", mask[i:i + 1])):
             np.ascontiguousarray(arr, dtype="<f8").tofile(os.path.join(tmp, "c4_%s_%d.f64" % (nm, i)))
         args = [DUMP, "lmfit", task] + [os.path.join(tmp, "c4_%s_%d.f64" % (nm, i)) for nm in ("n0", "tg", "mk")] + \
-               ["1", str(iters), os.path.join(tmp, "c4_fit_%d.sbin" % i)]
+               ["1", str(iters), os.path.join(tmp, "c4_fit_%d.sbin" % i), repr(broadening)]
         procs.append(subprocess.Popen(args, cwd=tmp, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
     for p in procs:
         if p.wait() != 0:
             raise RuntimeError("lmfit failed")
     fits = [read_sbin(os.path.join(tmp, "c4_fit_%d.sbin" % i)) for i in range(npix)]
-    np.savez_compressed(os.path.join(HERE, "config4.npz"), lambda_air=d["lambda_air"], tau500=d["tau500"],
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), lambda_air=d["lambda_air"], tau500=d["tau500"],
+                        broadening=np.array([broadening]),
                         node_kind=d["node_kind"], truth=truth, nodes0=nodes0, mask=mask, target=target,
                         fit_nodes=np.concatenate([f["fit_nodes"] for f in fits]),
                         fit_stokes=np.concatenate([f["fit_stokes"] for f in fits]),
@@ -252,6 +261,25 @@ def make_config5(tmp, ncol, niter=3):
                         ref_synth_seconds=s["ref_seconds_per_pixel"], **line_arrays(s))
 
 
+def make_psf(tmp):
+    """The reference's Gaussian instrumental broadening (convolve_spectra_with_gauss) of the
+    config-3 Stokes spectra and node responses at 45 and 150 mA FWHM (cfg SPECTRAL_BROADENING,
+    converted to cm and divided by 2.35 as jsub/cfg.cc:107-110 does)."""
+    c3 = np.load(os.path.join(HERE, "config3.npz"))
+    lam = c3["lambda_air"]
+    vec = np.concatenate([c3["stokes"], c3["responses"].reshape(-1, lam.shape[0], 4)])
+    out = {"lambda_air": lam, "spectra": vec}
+    for fwhm in (45.0, 150.0):
+        width = fwhm * 1e-11 / 2.35
+        fin = os.path.join(tmp, "psf_in.f64")
+        np.concatenate([lam, vec.ravel()]).astype("<f8").tofile(fin)
+        fout = os.path.join(tmp, "psf_out.f64")
+        run([DUMP, "conv", fin, str(lam.shape[0]), str(vec.shape[0]), repr(width), fout], tmp)
+        out["width_%d" % int(fwhm)] = np.array([width])
+        out["conv_%d" % int(fwhm)] = np.fromfile(fout, dtype="<f8").reshape(vec.shape)
+    np.savez_compressed(os.path.join(HERE, "psf.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -262,6 +290,7 @@ def main():
     ap.add_argument("--only-c4", action="store_true")
     ap.add_argument("--c4pix", type=int, default=8)
     ap.add_argument("--only-c5", action="store_true")
+    ap.add_argument("--only-psf", action="store_true")
     ap.add_argument("--c5col", type=int, default=3)
     a = ap.parse_args()
     if not os.path.exists(DUMP):
@@ -270,6 +299,12 @@ def main():
     try:
         for f in CFG_FILES:
             shutil.copy(os.path.join(a.ref, "cfg", f), tmp)
+        if a.only_psf:
+            make_psf(tmp)
+            shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
+            # config 4 with the 45 mA instrumental profile of cfg/invert.cfg
+            make_config4(tmp, 4, broadening=45.0 * 1e-11 / 2.35, name="config4_psf")
+            return
         if a.only_pool or a.only_c4 or a.only_c5:
             shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
         else:

@@ -273,3 +273,21 @@ def test_packed_tangents_match_dense(sb, config3):
     np.testing.assert_allclose(packed["chi2"], dense["chi2"], rtol=1e-12)
     np.testing.assert_allclose(packed["grad"], dense["grad"], rtol=1e-6, atol=1e-9 * np.abs(dense["grad"]).max())
     assert np.array_equal(packed["stokes"], dense["stokes"])
+
+
+@pytest.mark.parametrize("fwhm", [45, 150])
+def test_spectral_broadening_matches_reference(sb, config3, fwhm):
+    """snapi_spectral_broaden against the reference's convolve_spectra_with_gauss (Stokes spectra and
+    node responses), away from the blue end where the reference's output is undefined."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "psf.npz"))
+    lam = z["lambda_air"]
+    w = float(z["width_%d" % fwhm][0])
+    ctx = _ctx(sb, config3)
+    out = ctx.broaden(z["spectra"], w)
+    ctx.close()
+    ref = z["conv_%d" % fwhm]
+    inner = lam > lam[1] + 12 * w  # the reference's blue-end values (up to 1e44) leak ~11 w
+    scale = np.abs(ref[:, inner]).max(axis=(1, 2))
+    err = np.abs(out[:, inner] - ref[:, inner]).max(axis=(1, 2)) / scale
+    assert np.all(np.isfinite(out)) and err.max() < 1e-6, err.max()

@@ -74,3 +74,29 @@ def test_lm_matches_reference_fit(sb, config4):
     assert np.all(np.abs(d[:, 4:7]) < 5e3)           # velocities [cm/s]
     assert np.all(np.abs(d[:, 7]) < 10.0)            # B [G]
     assert np.all(np.abs(d[:, 8:10]) < 0.02)         # angles [rad]
+
+
+@pytest.mark.skipif(not ref_builder_available(), reason="reference builder (oracle/_ref) not built")
+def test_lm_with_spectral_broadening_matches_reference(sb, config4_psf):
+    """LM with the 45 mA Gaussian instrumental profile (synthesis and responses broadened as
+    stokes_lm_fit does) against the reference's fit of the same pixels.  Only pixels 0 and 1: the
+    reference's broadening is undefined near the blue end (its interpolation reads an unset
+    interval width), which wrecks its fits of pixels 2 and 3 whose masks reach that region."""
+    fx = config4_psf
+    sel = np.array([0, 1])
+    w = float(fx["broadening"][0])
+    mask = fx["mask"][sel]
+    target = np.where(mask[:, :, None] > 0, fx["target"][sel], 0.0)  # masked samples do not count
+    ic = float(np.abs(target[:, :, 0]).max())
+    kinds = fx["node_kind"]
+    ctx = sb.Context.from_fixture(fx, stokes_scale=ic)
+    out = ctx.lm_fit(fx["nodes0"][sel], target, RefBuilder(), kinds, 1e-2 * node_scales(kinds), mask=mask,
+                     lm_start=1e3, max_iter=int(fx["iters"][0]), delta=1e-3, spectral_broadening=w)
+    ctx.close()
+    ours = out["chi2"] * ic * ic
+    ref = fx["fit_chi2"][sel]
+    print("broadened fit: chi2 ours / reference", ours / ref, "iterations", out["iters"])
+    assert np.all(ours / ref < 1.01) and np.all(ours / ref > 0.8)
+    d = out["nodes"] - fx["fit_nodes"][sel]
+    d[:, 9] = (d[:, 9] + np.pi / 2) % np.pi - np.pi / 2
+    assert np.all(np.abs(d[:, :4]) < 80.0) and np.all(np.abs(d[:, 7]) < 10.0) and np.all(np.abs(d[:, 8:10]) < 0.02)

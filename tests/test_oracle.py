@@ -119,3 +119,21 @@ def test_ali_restatement_matches_reference_iterations(config5):
         assert not neg
         assert np.abs(p / fx["ali_pops_iter"][0, it] - 1.0).max() < 1e-9
         assert abs(r / fx["ali_relchange"][0, it] - 1.0) < 1e-9
+
+
+def test_psf_restatement_matches_reference():
+    """The numpy restatement of the Gaussian instrumental broadening (oracle/psf_oracle.py) against
+    the reference's convolve_spectra_with_gauss on Stokes spectra and node responses, away from the
+    blue end where the reference reads an unset interval width."""
+    import os
+
+    import psf_oracle as po
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "psf.npz"))
+    lam = z["lambda_air"]
+    for fw in (45, 150):
+        w = float(z["width_%d" % fw][0])
+        inner = lam > lam[1] + 12 * w  # the reference's blue-end values (up to 1e44) leak ~11 w
+        for v in (0, 3, 9, 40, 85):
+            out = po.convolve_gauss(z["spectra"][v], lam, w)
+            ref = z["conv_%d" % fw][v]
+            assert np.abs(out - ref)[inner].max() <= 1e-12 * np.abs(ref[inner]).max()
