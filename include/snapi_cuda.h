@@ -252,6 +252,144 @@ int snapi_spectral_broaden(snapi_ctx *ctx, int nvec, float *spectra, double widt
 
 int snapi_zeeman_pattern(int ju2, int jl2, double g_upper, double g_lower, snapi_line *line);
 
+/* ---------------------------------------------------------------------------------------------
+ * Node model -> column records on the device: atmos_pp::build_from_nodes (atmos/plpar/atmos_pp.cc:
+ * 58-248) followed by the set-up obs_stokes performs before its wavelength loop, i.e. what the
+ * caller otherwise marshals into records:
+ *   - log tau_500 grid tau_min + (tau_max - tau_min) / (nd - 1) * x, and every quantity from its
+ *     nodes by atmospheric_interpolation (cmlib/mathtools.cc:1208-1315: monotone cubic Bezier, flat
+ *     ends except the temperature's bottom slope from the FAL-C table, T bracketed to 3400..20000 K);
+ *     B, inclination, azimuth -> B_x, B_y, B_z (atmos_pp.cc:169-173) -> the ray frame (transform,
+ *     atmos_rad.cc:24-48); v_z projected on the ray (project, atmos_rad.cc:14-22);
+ *   - hydrostatic equilibrium: the top particle density by fixed point from 0.3 / k T (at most 20
+ *     steps, stop at 1e-2 relative change), then downward p_i = p_{i-1} + g dtau / kappa_mean with
+ *     kappa_mean the geometric mean of kappa / rho (at most 20 steps per depth, stop when the change
+ *     is below 1e-2 of the TOP density, as the reference writes it: atmos_pp.cc:209-236), each
+ *     step with the chemistry, the LTE populations, kappa at lambda_referent
+ *     (opacity_continuum) and rho = 1.4 * 1.67e-24 * (free hydrogen nuclei);
+ *   - chemistry per depth (atmosphere::chemeq, atmos/atmos_chm.cc:28-371): the starting electron
+ *     density from the ionisation balance (quadratic guess + halving), then Newton on charge and
+ *     particle conservation and the abundance ratios, molecules through their equilibrium
+ *     constants (moleqc.cc: polynomial in 5040 / T, the H- form), at most 51 iterations, converged
+ *     when every defect is below 1e-4 of its density; ionisation fractions (atom::ionfrc,
+ *     atom.cc:892-925) from the partition functions (Traving with Fischel-Sparks asymptotic terms,
+ *     Irwin, constant; partf.cc:217-283, 345-358); Saha-Boltzmann level populations (atom::lte,
+ *     atom.cc:779-787);
+ *   - the record of each depth: T, v_turb, n_e, projected v_los, |B|, inclination, azimuth,
+ *     kappa_500 at airtovac(lambda_referent) (compute_op_referent, atmos_ppbez_rts.cc:268-281:
+ *     Thomson + bound-free of the LTE atoms with stimulated emission + H- bound-free and free-free,
+ *     atmos_rad.cc:286-294, atom_rad.cc:151-187, mol.cc:669-694), the H- factors, the bound-free
+ *     totals of the wavelength window (atom_rad_synthesis.cc:226-262), per line the opacity and
+ *     emissivity factors and atom::damp_col (atom.cc:938-959);
+ *   - with tangents: d(record)/d(node) by central differences with the reference's steps (or the
+ *     caller's): a temperature node by two full builds (HE + chemistry), the other nodes by
+ *     re-interpolation only (atmos_fit.cc:1225-1307).
+ * Deliberate deviations: the 10 x 10 (atoms + 1) Newton system of chemeq is solved by Gaussian
+ * elimination with partial pivoting instead of an SVD (same solution for the non-singular
+ * system; the reference exits on a singular one); where the FAL-C slope table's interpolation
+ * reads an unset interval width (bottom temperature node in -0.0123..0.088, mathtools.cc:1073,
+ * 1093) this uses that interval's width.
+ *
+ * The caller fills the tables from its atom / molecule objects (the reference: atom::abund, ip,
+ * partf, nl, g, ee, bf; mol components and K; the model's nodes): */
+#define SNAPI_EOS_MAX_ATOMS 16
+#define SNAPI_EOS_MAX_STAGES 12      /* ionisation stages per atom (Z + 1) */
+#define SNAPI_EOS_MAX_LEVELS 16      /* levels per stage (atom::nl[z]) */
+#define SNAPI_EOS_MAX_MOLS 32
+#define SNAPI_MOL_MAX_COMP 4
+#define SNAPI_EOS_MAX_PAR 128         /* nodes of the model (one per depth is common for T) */
+#define SNAPI_PF_MAX_TERMS 8
+#define SNAPI_PF_MAX_COEF 8
+#define SNAPI_PF_NONE 0               /* U = 1 */
+#define SNAPI_PF_CONST 1
+#define SNAPI_PF_TRAV 2
+#define SNAPI_PF_IRWIN 3
+#define SNAPI_EQC_CONST 1
+#define SNAPI_EQC_POLY 2
+#define SNAPI_EQC_HMIN 3              /* marks the H- molecule (h_minus_mol): its continuum opacity */
+
+typedef struct {                      /* one stage's partition function (class pf and derived) */
+  int type;                           /* SNAPI_PF_* */
+  int nterm;                          /* TRAV: terms */
+  int ncoef;                          /* IRWIN: coefficients of ln U in powers of ln T */
+  int m[SNAPI_PF_MAX_TERMS];          /* TRAV: coefficients per term */
+  double value;                       /* CONST */
+  double zeff;                        /* TRAV: stage charge + 1 (trav::z) */
+  double g0;                          /* TRAV: ground statistical weight */
+  double g2[SNAPI_PF_MAX_TERMS], ee[SNAPI_PF_MAX_TERMS], ll[SNAPI_PF_MAX_TERMS];
+  double gam[SNAPI_PF_MAX_TERMS][SNAPI_PF_MAX_COEF];  /* trav::g: excitation energies [eV] */
+  double a[SNAPI_PF_MAX_TERMS][SNAPI_PF_MAX_COEF];    /* trav::a: weights */
+  double coef[SNAPI_PF_MAX_COEF];     /* IRWIN */
+} snapi_partition;
+
+typedef struct {                      /* one level of one stage */
+  double g;                           /* statistical weight (atom::g; 0: population = stage total) */
+  double ee;                          /* energy [erg] (atom::ee) */
+  /* bound-free cross-section bf[z][l]->U(lambda) [cm^2] evaluated by the caller at: */
+  double sigma_he;                    /* lambda_he */
+  double sigma_kappa;                 /* lambda_kappa */
+  double sigma_win;                   /* lambda_win */
+  double lambda_win;                  /* vacuum window wavelength of atom::boundfree_op_em_vector: the
+                                         last of the problem's wavelengths at or blueward of the
+                                         edge [cm]; 0 when the edge lies blueward of all of them */
+} snapi_eos_level;
+
+typedef struct {
+  double abundance;                   /* atom::abund, relative to the first atom */
+  int nstage;                         /* Z + 1 */
+  int nlte;                           /* 1: left out of the continuum opacity (check_if_nlte) */
+  double ip[SNAPI_EOS_MAX_STAGES];    /* ionisation energy of stage z [erg], z < nstage - 1 */
+  int nlevel[SNAPI_EOS_MAX_STAGES];
+  snapi_partition pf[SNAPI_EOS_MAX_STAGES];
+  snapi_eos_level level[SNAPI_EOS_MAX_STAGES][SNAPI_EOS_MAX_LEVELS];
+} snapi_eos_atom;
+
+typedef struct {
+  int ncomp;
+  int comp_atom[SNAPI_MOL_MAX_COMP];  /* atom index, -1 for the electron */
+  int comp_charge[SNAPI_MOL_MAX_COMP];/* component charge (struct ion z; -1 for the electron) */
+  int eqc;                            /* SNAPI_EQC_* */
+  int ncoef;
+  double coef[SNAPI_PF_MAX_COEF];     /* POLY: log10 K = sum coef[i] (5040 / T)^i; CONST: coef[0] = K */
+} snapi_eos_molecule;
+
+typedef struct {                      /* the level pair of each of the problem's lines */
+  int atom, stage, lower, upper;
+  double Blu, Bul, A;                 /* Einstein coefficients (atom::B[z][lo][up], B[z][up][lo], A) */
+  double alpha_col, sigma_col;        /* atom::alpha_col_dam[z][up][lo], col_dam_cross_section[z][up][lo] */
+} snapi_eos_line;
+
+typedef struct {
+  int natom;                          /* atoms in the reference's order; atoms[0] is hydrogen: its
+                                         neutral stage feeds H- and the collisional damping, its
+                                         free total the mass density */
+  const snapi_eos_atom *atoms;
+  int nmol;
+  const snapi_eos_molecule *mols;
+  const snapi_eos_line *lines;        /* [problem nlines] */
+  double lambda_he;                   /* lambda_referent [cm] (opacity of the HE iteration) */
+  double lambda_kappa;                /* airtovac(lambda_referent) [cm] (the record's kappa_500) */
+  double grav;                        /* surface gravity [cm s^-2] (grav_acc) */
+  double tau_min, tau_max;            /* log tau_500 at the first and last depth */
+  double theta, phi;                  /* ray direction [rad] (observable EL, AZ) */
+  int npar;                           /* nodes (<= SNAPI_EOS_MAX_PAR), kinds non-decreasing */
+  const int *node_kind;               /* [npar] 1 T, 2 v_turb, 3 v_los, 4 B, 5 inclination, 6 azimuth */
+  const double *node_tau;             /* [npar] log tau_500 of each node */
+} snapi_eos_model;
+
+/* Attach a node model to the context (tables copied to the device).  The problem's tau500 grid
+ * must be 10^(log tau grid) of the model. */
+int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *model);
+/* Records [npix][nd][nfield] (float) of the node vectors nodes [npix][npar] (double), the particle
+ * density Nt [npix][nd] (double, may be NULL) and, if tangents != NULL, the node tangents
+ * [npix][npar][nd][nfield] with central-difference steps step [npar] (NULL: the reference's 5 K,
+ * 20 cm/s, 20 cm/s, 0.01 G, 1e-3 rad, 1e-3 rad; const.h:27-32).  active [npix] (may be NULL):
+ * rows of pixels with active[p] == 0 are left untouched.  pix_status [npix] (may be NULL): 0, or
+ * a sum of 1 (a chemistry solve hit its iteration cap, as the reference then continues with the
+ * last iterate), 2 (a hydrostatic step hit its cap), 4 (non-finite values). */
+int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int *active, float *records,
+                        double *Nt, float *tangents, const double *step, int *pix_status, int mem);
+
 /* Pinned host memory for SNAPI_MEM_HOST arguments. */
 void *snapi_host_alloc(size_t bytes);
 void snapi_host_free(void *p);

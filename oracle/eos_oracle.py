@@ -1,0 +1,83 @@
+"""ctypes binding of the FP64 CPU restatement of the node -> record build (oracle/eos_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: the checker of snapi_build_records.  Only tests/, __graft_entry__.smoke()
+and bench.py's cpu_baseline leg import this module; the product never does.
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(_HERE))
+from snapi_b200.eos_tables import MAX_LEVELS, MAX_STAGES, EosTables  # noqa: E402
+from snapi_oracle import lib as _lib  # noqa: E402
+
+_D = ctypes.POINTER(ctypes.c_double)
+_ready = False
+
+
+def lib():
+    global _ready
+    L = _lib()
+    if not _ready:
+        L.sne_chem.restype = ctypes.c_int
+        L.sne_chem.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _D, _D, _D, _D, _D]
+        L.sne_build.restype = ctypes.c_int
+        L.sne_build.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D]
+        L.sne_tangents.restype = ctypes.c_int
+        L.sne_tangents.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D]
+        _ready = True
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_D)
+
+
+def chem(tables, T, Nt):
+    """Ne, stage totals [natom][S], level populations [natom][S][L], kappa_he, kappa, passes."""
+    na = tables.model.natom
+    ne = np.zeros(1)
+    nst = np.zeros((na, MAX_STAGES))
+    npop = np.zeros((na, MAX_STAGES, MAX_LEVELS))
+    khe = np.zeros(1)
+    kap = np.zeros(1)
+    passes = lib().sne_chem(ctypes.addressof(tables.model), float(T), float(Nt), _p(ne), _p(nst), _p(npop),
+                            _p(khe), _p(kap))
+    return ne[0], nst, npop, khe[0], kap[0], passes
+
+
+def build(tables, lam0, mass, nodes, nd=None):
+    """T [nd], Nt [nd], record [nd][nfield] (FP64) and status of one node vector."""
+    nd = nd or tables.nd
+    nl = tables.nlines
+    lam0 = np.ascontiguousarray(lam0, np.float64)
+    mass = np.ascontiguousarray(mass, np.float64)
+    nodes = np.ascontiguousarray(nodes, np.float64)
+    T = np.zeros(nd)
+    Nt = np.zeros(nd)
+    rec = np.zeros((nd, 12 + 3 * nl))
+    st = lib().sne_build(ctypes.addressof(tables.model), nd, nl, _p(lam0), _p(mass), _p(nodes), _p(T), _p(Nt),
+                         _p(rec))
+    if st < 0:
+        raise ValueError("sne_build: bad sizes")
+    return T, Nt, rec, st
+
+
+def tangents(tables, lam0, mass, nodes, step=None, nd=None):
+    nd = nd or tables.nd
+    nl = tables.nlines
+    lam0 = np.ascontiguousarray(lam0, np.float64)
+    mass = np.ascontiguousarray(mass, np.float64)
+    nodes = np.ascontiguousarray(nodes, np.float64)
+    tan = np.zeros((tables.npar, nd, 12 + 3 * nl))
+    st = None if step is None else np.ascontiguousarray(step, np.float64)
+    status = lib().sne_tangents(ctypes.addressof(tables.model), nd, nl, _p(lam0), _p(mass), _p(nodes), _p(st),
+                                _p(tan))
+    return tan, status
+
+
+def load_tables(path):
+    return EosTables(np.load(path))

@@ -15,6 +15,10 @@
 //       Gaussian spectral broadening of width [cm]).
 //   snapi_ref_dump conv   <in.f64> <nlambda> <nvec> <width_cm> <out.f64>
 //       Gaussian instrumental broadening of nvec Stokes spectra (convolve_spectra_with_gauss).
+//   snapi_ref_dump eos    <task.tsk> <nodes.f64> <npix> <out.sbin>
+//       The tables of the node -> record build (atoms, partition functions, levels, molecules,
+//       line ties, node model), the reference's chemistry on a (T, Nt) grid and the columns
+//       build_from_nodes leaves for npix node vectors (see do_eos).
 //   snapi_ref_dump ali    <task.tsk> <nodes.f64> <ncol> <niter> <out.sbin>
 //       NLTE level-population iteration inputs, niter iterations of the reference's loop, and the
 //       populations nltepops converges to (see do_ali).
@@ -713,7 +717,257 @@ static int do_conv(const char *inname, int n, int nvec, double width, const char
   return 0;
 }
 
+// ----------------------------------------------------------------------------------------------
+// eos: the data atmos_pp::build_from_nodes needs (atoms with their partition functions, levels
+// and bound-free cross-sections at the wavelengths the build uses; molecules; the line <-> level
+// ties; the node model), read from the reference's own objects after it parsed its configs; the
+// reference's chemistry on a (T, Nt) grid (chemeq + lte + opacity_continuum, atmos_chm.cc:28-371,
+// atom.cc:779-787, atmos_rad.cc:286-294); and, per node vector, the column build_from_nodes leaves
+// (T, Nt, n_e, kappa at lambda_referent, rho).  Array layout: see tests/golden/make_golden.py.
+static const int EMS = 12, EMT = 8, EMC = 8, EML = 16;
+
+struct Rd {  // little-endian reader over a packed object
+  const uint8_t *p;
+  int i8() { int8_t v; memcpy(&v, p, 1); p += 1; return v; }
+  int u8() { uint8_t v; memcpy(&v, p, 1); p += 1; return v; }
+  int i32() { int32_t v; memcpy(&v, p, 4); p += 4; return v; }
+  double f64() { double v; memcpy(&v, p, 8); p += 8; return v; }
+};
+
+static int do_eos(const char *tskname, const char *nodesname, int npix, const char *outname) {
+  const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
+  const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
+  int ac = 4; cmdln cmd(ac, (char **)argv, options, maps);
+  io_class io(cmd);
+  Task t = load_task(tskname);
+  model *m = task_model(t, io);
+  atmosphere *a = task_atmos(t, io);
+  const int nl = t.nlambda;
+  fp_t *lv = airtovac((fp_t *)t.lambda.data(), nl) - 1;   // 1-based vacuum grid
+  const double lam_he = lambda_referent, lam_kap = airtovac(lambda_referent);
+
+  std::vector<atom *> atoms;
+  std::vector<mol *> mols;
+  for (int i = 0; i < a->natm; ++i) {
+    if (atom *at = dynamic_cast<atom *>(a->atml[i])) atoms.push_back(at);
+    else if (mol *mo = dynamic_cast<mol *>(a->atml[i])) mols.push_back(mo);
+  }
+  const int na = atoms.size(), nm = mols.size();
+  std::vector<double> atom_f(na * 4), atom_ip(na * EMS, 0.0);
+  std::vector<double> pf_type(na * EMS, 0.0), pf_value(na * EMS, 0.0), pf_zeff(na * EMS, 0.0),
+      pf_g0(na * EMS, 0.0), pf_nterm(na * EMS, 0.0), pf_ncoef(na * EMS, 0.0), pf_m(na * EMS * EMT, 0.0),
+      pf_g2(na * EMS * EMT, 0.0), pf_ee(na * EMS * EMT, 0.0), pf_ll(na * EMS * EMT, 0.0),
+      pf_a(na * EMS * EMT * EMC, 0.0), pf_gam(na * EMS * EMT * EMC, 0.0), pf_coef(na * EMS * EMC, 0.0);
+  std::vector<double> lev_n(na * EMS, 0.0), lev(na * EMS * EML * 6, 0.0);
+  for (int ia = 0; ia < na; ++ia) {
+    atom *at = atoms[ia];
+    if (at->Z + 1 > EMS) { fprintf(stderr, "too many stages\n"); return 2; }
+    atom_f[ia * 4 + 0] = at->abund; atom_f[ia * 4 + 1] = at->Z + 1;
+    atom_f[ia * 4 + 2] = at->check_if_nlte(); atom_f[ia * 4 + 3] = at->mass;
+    for (int z = 0; z <= at->Z; ++z) {
+      int s = ia * EMS + z;
+      if (z < at->Z) atom_ip[s] = at->ip[z];
+      // partition function data, read back from the object's own wire format (pf::pack and the
+      // trav / irwin / cpf packers, partf.cc:56-63, 88-94, 170-187, 323-332)
+      pf *P = at->partf[z];
+      std::vector<uint8_t> pb(P->size(io) + 64);
+      P->pack(pb.data(), 0, io);
+      Rd r{pb.data()};
+      int type = r.i8();
+      pf_type[s] = type;
+      if (type == PF_TYPE_CONST) pf_value[s] = r.f64();
+      if (type == PF_TYPE_TRAV) {
+        pf_zeff[s] = r.f64(); pf_g0[s] = r.f64();
+        int n = r.i32();
+        if (n > EMT) { fprintf(stderr, "too many partition terms: atom %d stage %d n %d\n", ia, z, n); return 2; }
+        pf_nterm[s] = n;
+        for (int i = 0; i < n; ++i) {
+          pf_g2[s * EMT + i] = r.f64(); pf_ee[s * EMT + i] = r.f64(); pf_ll[s * EMT + i] = r.f64();
+          int mm = r.i32();
+          if (mm > EMC) { fprintf(stderr, "too many partition coefficients\n"); return 2; }
+          pf_m[s * EMT + i] = mm;
+          for (int l = 0; l < mm; ++l) pf_gam[(s * EMT + i) * EMC + l] = r.f64();
+          for (int l = 0; l < mm; ++l) pf_a[(s * EMT + i) * EMC + l] = r.f64();
+          r.i8();
+        }
+      }
+      if (type == PF_TYPE_IRWIN) {
+        pf_zeff[s] = r.f64();
+        int n = r.i32();
+        if (n > EMC) { fprintf(stderr, "too many Irwin coefficients\n"); return 2; }
+        pf_ncoef[s] = n;
+        for (int i = 0; i < n; ++i) pf_coef[s * EMC + i] = r.f64();
+      }
+      if (at->nl[z] > EML) { fprintf(stderr, "too many levels\n"); return 2; }
+      lev_n[s] = at->nl[z];
+      for (int l = 0; l < at->nl[z]; ++l) {
+        double *L = &lev[(s * EML + l) * 6];
+        L[0] = at->g[z][l]; L[1] = at->ee[z][l];
+        bfcs *B = at->bf[z][l];
+        if (B && z < at->Z) {
+          L[2] = B->U(lam_he); L[3] = B->U(lam_kap);
+          // atom::boundfree_op_em_vector (atom_rad_synthesis.cc:229-243): the window wavelength
+          fp_t lc = B->getlambda_crit();
+          int ncrit = 0;
+          for (int q = 1; q <= nl; ++q) { if (lv[q] > lc) break; ++ncrit; }
+          if (ncrit) { L[5] = lv[ncrit]; L[4] = B->U(lv[ncrit]); }
+        }
+      }
+    }
+  }
+  std::vector<double> mol_i(nm * 11, 0.0), mol_coef(nm * EMC, 0.0);
+  for (int im = 0; im < nm; ++im) {
+    mol *mo = mols[im];
+    int nc = 0;
+    struct ion *cmp = mo->components(nc);
+    if (nc > 4) { fprintf(stderr, "too many molecule components\n"); return 2; }
+    mol_i[im * 11 + 0] = nc;
+    for (int i = 0; i < nc; ++i) {
+      int idx = -1;
+      for (int ia = 0; ia < na; ++ia) if ((atmol *)atoms[ia] == cmp[i].atom) idx = ia;
+      mol_i[im * 11 + 1 + i] = idx;
+      mol_i[im * 11 + 5 + i] = cmp[i].z;
+    }
+    // equilibrium constant, read back from its wire format (moleqc.cc: eqc::pack, eqc_cnst::pack,
+    // eqc_poly::pack)
+    eqc *E = mo->K[0];
+    std::vector<uint8_t> eb(E->size(io) + 64);
+    E->pack(eb.data(), 0, io);
+    Rd r{eb.data()};
+    int type = r.u8();
+    mol_i[im * 11 + 9] = type;
+    if (type == EQC_TYPE_POLY) {
+      int n = r.u8();
+      if (n > EMC) { fprintf(stderr, "too many eqc coefficients\n"); return 2; }
+      mol_i[im * 11 + 10] = n;
+      for (int i = 0; i < n; ++i) mol_coef[im * EMC + i] = r.f64();
+    }
+    if (type == EQC_TYPE_CNST) { mol_i[im * 11 + 10] = 1; mol_coef[im * EMC] = r.f64(); }
+  }
+  // line <-> level ties, in the order atmosphere::op_em_vector meets the lines (A > 1)
+  std::vector<double> line_eos;
+  for (int ia = 0; ia < na; ++ia) {
+    atom *at = atoms[ia];
+    for (int z = 0; z <= at->Z; ++z)
+      for (int up = 1; up < at->nl[z]; ++up)
+        for (int lo = 0; lo < up; ++lo) {
+          if (!(at->A[z][up][lo] > 1E0)) continue;
+          double v[9] = {(double)ia, (double)z, (double)lo, (double)up, at->B[z][lo][up], at->B[z][up][lo],
+                         at->A[z][up][lo], at->alpha_col_dam[z][up][lo], at->col_dam_cross_section[z][up][lo]};
+          line_eos.insert(line_eos.end(), v, v + 9);
+        }
+  }
+  const int nlines = line_eos.size() / 9;
+  // node model
+  const int np = m->get_N_nodes_total();
+  std::vector<double> node_kind(np), node_tau(np);
+  {
+    int cnt[6] = {m->get_N_nodes_temp(), m->get_N_nodes_vt(), m->get_N_nodes_vs(), m->get_N_nodes_B(),
+                  m->get_N_nodes_theta(), m->get_N_nodes_phi()};
+    fp_t *tt[6] = {m->get_temp_nodes_tau(), m->get_vt_nodes_tau(), m->get_vs_nodes_tau(), m->get_B_nodes_tau(),
+                   m->get_theta_nodes_tau(), m->get_phi_nodes_tau()};
+    int p = 0;
+    for (int kd = 0; kd < 6; ++kd)
+      for (int i = 1; i <= cnt[kd]; ++i) {
+        node_kind[p] = kd + 1; node_tau[p] = tt[kd][i]; ++p;
+        if (m->which_parameter(p) != kd + 1) { fprintf(stderr, "node order\n"); return 2; }
+      }
+    for (int kd = 0; kd < 6; ++kd) if (cnt[kd]) delete[] (tt[kd] + 1);
+  }
+  const int nd = a->x3h - a->x3l + 1;
+  double meta[13] = {(double)na, (double)nm, (double)nlines, (double)np, (double)nd, m->get_tau_min(),
+                     m->get_tau_max(), t.el, t.az, lam_he, lam_kap, grav_acc, (double)nl};
+
+  // the reference's chemistry on a (T, Nt) grid, stored in depth slot x3l
+  const int nT = 14, nN = 12;
+  std::vector<double> cT(nT), cN(nN), cne(nT * nN), cstage(nT * nN * na * EMS, 0.0),
+      clev(nT * nN * na * EMS * EML, 0.0), ckhe(nT * nN), ckap(nT * nN);
+  for (int i = 0; i < nT; ++i) cT[i] = 3400.0 * pow(20000.0 / 3400.0, i / (double)(nT - 1));
+  for (int j = 0; j < nN; ++j) cN[j] = pow(10.0, 11.0 + 7.0 * j / (double)(nN - 1));
+  a->popsetup();
+  const int x = a->x3l;
+  for (int i = 0; i < nT; ++i)
+    for (int j = 0; j < nN; ++j) {
+      fp_t ne = 1.0;
+      a->chemeq(a->atml, a->natm, cT[i], cN[j], ne, 1, 1, x);
+      for (int q = 0; q < a->natm; ++q) a->atml[q]->lte(cT[i], ne, 1, 1, x);
+      int g = i * nN + j;
+      cne[g] = ne;
+      for (int ia = 0; ia < na; ++ia)
+        for (int z = 0; z <= atoms[ia]->Z; ++z) {
+          cstage[(g * na + ia) * EMS + z] = atoms[ia]->pop[1][1][x].N[z];
+          for (int l = 0; l < atoms[ia]->nl[z]; ++l)
+            clev[((g * na + ia) * EMS + z) * EML + l] = atoms[ia]->pop[1][1][x].n[z][l];
+        }
+      ckhe[g] = a->opacity_continuum(cT[i], ne, lam_he, 1, 1, x);
+      ckap[g] = a->opacity_continuum(cT[i], ne, lam_kap, 1, 1, x);
+    }
+  a->popclean();
+  delete a;
+
+  // columns left by build_from_nodes
+  std::vector<double> hT, hN, hne, hk, hr;
+  if (npix > 0) {
+    std::vector<uint8_t> nb = read_file_bytes(nodesname);
+    if ((int)(nb.size() / 8) < npix * np) { fprintf(stderr, "nodes file too short\n"); return 2; }
+    const double *nodes = (const double *)nb.data();
+    for (int ip = 0; ip < npix; ++ip) {
+      atmosphere *b = task_atmos(t, io);
+      set_nodes(m, nodes + ip * np);
+      b->build_from_nodes(m);
+      for (int xx = b->x3l; xx <= b->x3h; ++xx) {
+        hT.push_back(b->T[1][1][xx]); hN.push_back(b->Nt[1][1][xx]); hne.push_back(b->Ne[1][1][xx]);
+        hk.push_back(b->op_referent[1][1][xx]); hr.push_back(b->rho[1][1][xx]);
+      }
+      delete b;
+    }
+  }
+
+  SbinWriter w(outname);
+  w.put("meta", {13}, meta);
+  w.put("atom_f", {na, 4}, atom_f.data());
+  w.put("atom_ip", {na, EMS}, atom_ip.data());
+  w.put("pf_type", {na, EMS}, pf_type.data());
+  w.put("pf_value", {na, EMS}, pf_value.data());
+  w.put("pf_zeff", {na, EMS}, pf_zeff.data());
+  w.put("pf_g0", {na, EMS}, pf_g0.data());
+  w.put("pf_nterm", {na, EMS}, pf_nterm.data());
+  w.put("pf_m", {na, EMS, EMT}, pf_m.data());
+  w.put("pf_g2", {na, EMS, EMT}, pf_g2.data());
+  w.put("pf_ee", {na, EMS, EMT}, pf_ee.data());
+  w.put("pf_ll", {na, EMS, EMT}, pf_ll.data());
+  w.put("pf_a", {na, EMS, EMT, EMC}, pf_a.data());
+  w.put("pf_gam", {na, EMS, EMT, EMC}, pf_gam.data());
+  w.put("pf_ncoef", {na, EMS}, pf_ncoef.data());
+  w.put("pf_coef", {na, EMS, EMC}, pf_coef.data());
+  w.put("lev_n", {na, EMS}, lev_n.data());
+  w.put("lev", {na, EMS, EML, 6}, lev.data());
+  w.put("mol_i", {nm, 11}, mol_i.data());
+  w.put("mol_coef", {nm, EMC}, mol_coef.data());
+  w.put("line_eos", {nlines, 9}, line_eos.data());
+  w.put("node_kind", {np}, node_kind.data());
+  w.put("node_tau", {np}, node_tau.data());
+  w.put("chem_T", {nT}, cT.data());
+  w.put("chem_Nt", {nN}, cN.data());
+  w.put("chem_ne", {nT, nN}, cne.data());
+  w.put("chem_stage", {nT, nN, na, EMS}, cstage.data());
+  w.put("chem_lev", {nT, nN, na, EMS, EML}, clev.data());
+  w.put("chem_kap_he", {nT, nN}, ckhe.data());
+  w.put("chem_kap", {nT, nN}, ckap.data());
+  if (npix > 0) {
+    w.put("he_T", {npix, nd}, hT.data());
+    w.put("he_Nt", {npix, nd}, hN.data());
+    w.put("he_ne", {npix, nd}, hne.data());
+    w.put("he_kap", {npix, nd}, hk.data());
+    w.put("he_rho", {npix, nd}, hr.data());
+  }
+  delete[] (lv + 1);
+  delete m;
+  return 0;
+}
+
 int main(int argc, char **argv) {
+  if (argc >= 6 && !strcmp(argv[1], "eos")) return do_eos(argv[2], argv[3], atoi(argv[4]), argv[5]);
   if (argc >= 4 && !strcmp(argv[1], "pack")) return do_pack(argv[2], argv[3]);
   if (argc >= 7 && !strcmp(argv[1], "dump"))
     return do_dump(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]), argv[6]);

@@ -97,6 +97,8 @@ def lib():
         L.snapi_fd_grad.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, ip]
         L.snapi_adjoint_packed.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, fp, ip]
         L.snapi_spectral_broaden.argtypes = [vp, ip, fp, ctypes.c_double, ip]
+        L.snapi_eos_set.argtypes = [vp, vp]
+        L.snapi_build_records.argtypes = [vp, ip, fp, fp, fp, fp, fp, fp, fp, ip]
         L.snapi_zeeman_pattern.argtypes = [ip, ip, ctypes.c_double, ctypes.c_double, ctypes.POINTER(SnapiLine)]
         L.snapi_host_alloc.restype = vp
         L.snapi_host_alloc.argtypes = [ctypes.c_size_t]
@@ -349,6 +351,36 @@ class Context:
         nvec = a.size // (self.nl * 4)
         self._check(lib().snapi_spectral_broaden(self._ctx, nvec, _ptr(a), float(width), MEM_HOST))
         return a
+
+    def eos_set(self, tables):
+        """Attach a node model (snapi_b200.eos_tables.EosTables) for build_records."""
+        self._eos = tables  # keep the ctypes tables alive for the call
+        self._check(lib().snapi_eos_set(self._ctx, ctypes.addressof(tables.model)))
+        self._eos_npar = tables.npar
+
+    def build_records(self, nodes, active=None, tangents=True, step=None, want_nt=False):
+        """Column records [npix, nd, nfield] of node vectors [npix, npar] on the GPU (build_from_nodes +
+        chemistry + the record set-up), with node tangents [npix, npar, nd, nfield] if `tangents`.
+        Returns (records, tangents or None, Nt or None, pixel status)."""
+        nodes = np.ascontiguousarray(np.atleast_2d(nodes), dtype=np.float64)
+        npix, npar = nodes.shape
+        if npar != self._eos_npar:
+            raise ValueError("node vectors have %d entries, the model %d" % (npar, self._eos_npar))
+        rec = np.zeros((npix, self.nd, self.nfield), np.float32)
+        tan = np.zeros((npix, npar, self.nd, self.nfield), np.float32) if tangents else None
+        nt = np.zeros((npix, self.nd), np.float64) if want_nt else None
+        act = None if active is None else np.ascontiguousarray(active, dtype=np.int32)
+        stp = None if step is None else np.ascontiguousarray(np.broadcast_to(step, (npar,)), dtype=np.float64)
+        status = np.zeros(npix, np.int32)
+        self._check(lib().snapi_build_records(self._ctx, npix, _ptr(nodes), _ptr(act), _ptr(rec), _ptr(nt), _ptr(tan),
+                                              _ptr(stp), _ptr(status), MEM_HOST))
+        return rec, tan, nt, status
+
+    def build_records_device(self, npix, nodes_ptr, rec_ptr, tan_ptr=0, active_ptr=0, status_ptr=0):
+        """build_records on device pointers (int addresses, e.g. torch .data_ptr())."""
+        p = lambda a: ctypes.c_void_p(a) if a else None  # noqa: E731
+        self._check(lib().snapi_build_records(self._ctx, npix, p(nodes_ptr), p(active_ptr), p(rec_ptr), None,
+                                              p(tan_ptr), None, p(status_ptr), MEM_DEVICE))
 
     def responses(self, records, tangents, step, want_stokes=True):
         """d Stokes / d node [npix, npar, nlambda, 4] (obs_stokes_responses_to_nodes, batched) by

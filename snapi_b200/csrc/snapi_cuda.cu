@@ -505,6 +505,7 @@ void snapi_destroy(snapi_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   lm_free(ctx);
+  eos_free(ctx);
   void *bufs[] = {ctx->d_lamvac, ctx->d_D, ctx->d_lines, ctx->d_compS, ctx->d_compD, ctx->d_status,
                   ctx->d_rec, ctx->d_stokes, ctx->d_obs, ctx->d_mask, ctx->d_tan, ctx->d_recgrad,
                   ctx->d_dstokes, ctx->d_opart, ctx->d_seed, ctx->d_bars, ctx->d_grad, ctx->d_chi2, ctx->d_c2part, ctx->d_step,
@@ -563,6 +564,11 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
   std::vector<double> lv(ctx->nl);
   for (int l = 0; l < ctx->nl; ++l) lv[l] = airtovac_d(prob->lambda_air[l]);
   ctx->h_lamair.assign(prob->lambda_air, prob->lambda_air + ctx->nl);
+  ctx->h_tau500.assign(prob->tau500, prob->tau500 + ctx->nd);
+  for (int j = 0; j < ctx->nlines; ++j) {
+    ctx->h_line_lam0.push_back(prob->lines[j].lam0);
+    ctx->h_line_mass.push_back(prob->lines[j].mass);
+  }
   ctx->lam_mid = (float)(0.5 * (lv[ctx->nl - 1] + lv[0]));
   std::vector<double> D(ctx->nd - 1);
   for (int i = 0; i + 1 < ctx->nd; ++i) D[i] = (prob->tau500[i + 1] - prob->tau500[i]) / prob->mu;

@@ -1,0 +1,1065 @@
+// snapi_eos.cu -- node model -> column records on the device (snapi_eos_set, snapi_build_records).
+//
+// The reference builds each pixel's atmosphere from its nodes on the host before every synthesis
+// (atmos_pp::build_from_nodes, atmos/plpar/atmos_pp.cc:58-248): node interpolation, hydrostatic
+// equilibrium with the chemistry, LTE populations and the continuum opacity at every step, and,
+// for the fit, two more builds per temperature node for the record tangents (atmos_fit.cc:
+// 1225-1307).  Here that whole map runs on the GPU in FP64 (the chemistry spans 40 decades and
+// its Newton system is badly scaled, so FP32 is not an option; the B200's FP64 rate is half its
+// FP32 rate):
+//
+//   k_eos_he   one thread per (pixel, variant): the column's temperature from its nodes and the
+//              hydrostatic particle densities, depth by depth (inherently serial in depth).
+//              Variant 0 is the node vector itself, variants 2i+1 / 2i+2 move temperature node i
+//              by +- step / 2.  Threads are ordered pixel-fastest, so a warp holds 32 pixels of the
+//              same variant at the same depth: similar (T, Nt), similar iteration counts.
+//   k_eos_rec  one thread per (depth, pixel): the chemistry at the final (T, Nt) of every variant,
+//              the record fields, and the tangent rows (thermal nodes from the variants,
+//              kinematic / field nodes by re-interpolation).
+//
+// The chemistry (atmosphere::chemeq, atmos/atmos_chm.cc:28-330) is evaluated per call in the
+// reference's steps, with what depends on T alone hoisted out of the ~20 ionisation sweeps of a
+// call: the Traving partition sums over tabulated levels (partf.cc:224-228), the asymptotic-term
+// weights g2 exp(-2.302585 ee x), the Boltzmann factors of the ionisation energies and the
+// molecular equilibrium constants.  A sweep then costs per stage one Fischel-Sparks polynomial
+// per asymptotic term and one division.  The 10 x 10 Newton system is solved by Gaussian
+// elimination with partial pivoting (the reference: SVD, same solution).  Loops the reference
+// leaves unbounded (the halving of its starting electron density) are capped at 400 passes and
+// flag the pixel.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "snapi_internal.cuh"
+
+namespace snapi {
+namespace {
+
+constexpr int kEA = SNAPI_EOS_MAX_ATOMS;  // atoms
+constexpr int kES = 64;                   // ionisation stages over all atoms
+constexpr int kET = 96;                   // Traving asymptotic terms over all stages
+constexpr int kEC = 512;                  // Traving / Irwin coefficients over all terms
+constexpr int kEM = SNAPI_EOS_MAX_MOLS;   // molecules
+constexpr int kER = 32;                   // stages whose ionisation fraction is kept per sweep
+constexpr int kEL = 64;                   // levels whose population enters a record
+constexpr int kEB = 32;                   // bound-free levels
+constexpr int kEP = SNAPI_EOS_MAX_PAR;    // nodes
+constexpr int kHeThreads = 64;
+constexpr int kRecThreads = 64;
+constexpr int kPolishCap = 400;
+
+// the reference's constants (cmlib/const.h, CGS)
+constexpr double cPI = 3.141592653589793238462643383279502884197169399375105;
+constexpr double cC = 2.99792458E10, cH = 6.6260687652E-27, cK = 1.3806503E-16, cME = 9.1093818872E-28;
+constexpr double cE = 4.8032042510E-10, cRYD = 1.097373156853955E5, cE0 = 7.957747154594775607E-02;
+constexpr double cSAHA = 2.0706615382E-16;
+
+struct EosDev {
+  int natom, nmol, nst, nlev, nbf, nlines, npar, nd, nref, hm, href;
+  double lambda_he, lambda_kappa, grav, tau_min, tau_max, theta, phi, ftrav;
+  double abund[kEA];
+  int s0[kEA], ns[kEA];
+  // stages
+  int pft[kES];
+  double pfv[kES];   // CONST: value; TRAV: g0; NONE: 1
+  double zeff[kES];
+  double eion[kES];  // ionisation energy to the next stage [erg]
+  int t0[kES], t1[kES];  // TRAV: asymptotic terms [t0, t1); IRWIN: coefficients [t0, t1) of cA
+  int ref[kES];      // kept-fraction slot, -1 none
+  int satom[kES];    // atom of each stage
+  // Traving asymptotic terms and level sums
+  double g2[kET], tee[kET], tll[kET];
+  int c0[kET], c1[kET];
+  double cA[kEC], cG[kEC];
+  // molecules (components: 1-based atom, 0 the electron)
+  int mnc[kEM];
+  int matom[kEM][SNAPI_MOL_MAX_COMP], mref[kEM][SNAPI_MOL_MAX_COMP];
+  int mmul[kEM][kEA + 1];
+  double mq[kEM];
+  int meqc[kEM], mncoef[kEM];
+  double mcoef[kEM][SNAPI_PF_MAX_COEF];
+  // levels entering a record: stage, statistical weight, energy
+  int lst[kEL];
+  double lg[kEL], lee[kEL];
+  // bound-free levels: level, next stage's ground level, LTE flag, cross-sections, window
+  int bfl[kEB], bfn[kEB], bflte[kEB];
+  double bfg[kEB], bfgn[kEB], bfip[kEB], sig_he[kEB], sig_k[kEB], sig_w[kEB], lam_w[kEB];
+  // lines: lower / upper level slots
+  int llo[SNAPI_MAX_LINES], lup[SNAPI_MAX_LINES];
+  double lBlu[SNAPI_MAX_LINES], lBul[SNAPI_MAX_LINES], lA[SNAPI_MAX_LINES], lalpha[SNAPI_MAX_LINES],
+      lsig[SNAPI_MAX_LINES], llam0[SNAPI_MAX_LINES], lmass[SNAPI_MAX_LINES];
+  // nodes (kinds contiguous and non-decreasing)
+  double ntau[kEP];
+  int kfirst[7], kcount[7];
+};
+
+// ---- partition functions (partf.cc:217-283) ---------------------------------------------------------
+__device__ __forceinline__ double qas_f(double l, double p, double Dz) {
+  if (p > l) {
+    const double llm = l - 1.0;
+    return ((1.3333333 * p + 0.5) * p + 0.16666667 + 1.33333333 * Dz) * p - 0.4 * Dz * Dz / p -
+           ((0.33333333 * llm - 0.5) * llm - 0.16666667 - Dz) * llm + 0.5 * Dz * Dz / l;
+  }
+  const double axl2 = Dz / (l * l);
+  return (1.0 + axl2 * (0.33333333 + 0.1 * axl2)) * p * p * p * p / l;
+}
+
+__device__ __forceinline__ double dqas_f(double l, double p, double Dz) {
+  if (p > l) return ((3.0 * 1.3333333 * p + 1.0) * p + 0.16666667 + 1.33333333 * Dz) + 0.4 * Dz * Dz / (p * p);
+  const double axl2 = Dz / (l * l);
+  return 4.0 * (1.0 + axl2 * (0.33333333 + 0.1 * axl2)) * p * p * p / l;
+}
+
+// ---- the chemistry of one (T, Nt) point, one thread -----------------------------------------------------
+struct Chem {
+  const EosDev &E;
+  double T, kT, fct;
+  double Ut[kES];   // T-only part of U (whole U for CONST / IRWIN / NONE)
+  double eip[kES];  // exp(-eion / kT)
+  double alp[kES];  // 31.321 z^2 x
+  double w2[kET];   // g2 exp(-2.302585 ee x)
+  double K[kEM];
+  double Ea[kEA + 1], Da[kEA + 1];  // sum_i i f_i, sum_i i df_i / dNe per atom (1-based)
+  double fr[kER], dr[kER];          // kept ionisation fractions and their Ne derivatives
+  double N[kEA + 1];
+  double A[(kEA + 1) * (kEA + 1)], d[kEA + 1];
+  int capped;
+
+  __device__ explicit Chem(const EosDev &e) : E(e), T(-1.0) {}
+
+  __device__ void set_T(double Tin) {
+    T = Tin;
+    kT = cK * T;
+    const double x = 5040.0 / T;
+    fct = 2.0 * pow((2.0 * cPI * cME * cK * T) / (cH * cH), 1.5);
+    for (int s = 0; s < E.nst; ++s) {
+      const int ty = E.pft[s];
+      double u = E.pfv[s];
+      if (ty == SNAPI_PF_TRAV) {
+        for (int t = E.t0[s]; t < E.t1[s]; ++t) {
+          for (int c = E.c0[t]; c < E.c1[t]; ++c) u += E.cA[c] * exp(-2.302585 * E.cG[c] * x);
+          w2[t] = E.g2[t] * exp(-2.302585 * E.tee[t] * x);
+        }
+        alp[s] = 31.321 * E.zeff[s] * E.zeff[s] * x;
+      } else if (ty == SNAPI_PF_IRWIN) {
+        const double lnT = log(T);
+        double sum = 0.0;
+        for (int c = E.t0[s]; c < E.t1[s]; ++c) sum += E.cA[c] * pow(lnT, (double)(c - E.t0[s]));
+        u = exp(sum);
+      }
+      Ut[s] = u;
+      eip[s] = exp(-E.eion[s] / kT);
+    }
+    for (int m = 0; m < E.nmol; ++m) {
+      double k = 0.0;
+      if (E.meqc[m] == SNAPI_EQC_POLY) {
+        const int n = E.mncoef[m];
+        double sum = E.mcoef[m][n - 1];
+        for (int i = n - 2; i >= 0; --i) sum = E.mcoef[m][i] + x * sum;
+        k = exp(2.302585093 * sum);
+      } else if (E.meqc[m] == SNAPI_EQC_HMIN) {
+        k = exp(2.302585093 * (0.1249 + (2.5 * log(T) / 2.302585) - 0.747 * x));
+      } else if (E.meqc[m] == SNAPI_EQC_CONST) {
+        k = E.mcoef[m][0];
+      }
+      K[m] = k;
+    }
+  }
+
+  // U and dU/U of stage s at electron density ne (pne = ne^(1/6))
+  template <bool kDeriv>
+  __device__ __forceinline__ void pfu(int s, double ne, double pne, double &U, double &dUoU) const {
+    double u = Ut[s], du = 0.0;
+    if (E.pft[s] == SNAPI_PF_TRAV) {
+      const double z = E.zeff[s], p = z * E.ftrav / pne, al = alp[s];
+      const int t0 = E.t0[s], t1 = E.t1[s];
+      for (int t = t0; t < t1; ++t) u += w2[t] * qas_f(E.tll[t], p, al);
+      // trav::dU keeps only the last term (partf.cc:247-248)
+      if (kDeriv && t1 > t0) du = -w2[t1 - 1] * dqas_f(E.tll[t1 - 1], p, al) * z * E.ftrav / (6.0 * ne * pne);
+    }
+    U = u;
+    dUoU = kDeriv ? du / u : 0.0;
+  }
+
+  // atom::ionfrc for atom a (0-based) at ne: Ea, Da and the kept fractions (atom.cc:892-925)
+  template <bool kDeriv>
+  __device__ void sweep_atom(int a, double ne, double pne) {
+    const int s0 = E.s0[a], ns = E.ns[a];
+    double Up, dUp;
+    pfu<kDeriv>(s0, ne, pne, Up, dUp);
+    double fk = 1.0, df = 0.0, fsum = 1.0, dfsum = 0.0, S1 = 0.0, S2 = 0.0;
+    if (kDeriv && E.ref[s0] >= 0) { fr[E.ref[s0]] = 1.0; dr[E.ref[s0]] = 0.0; }
+    for (int z = 0; z + 1 < ns; ++z) {
+      double Un, dUn;
+      pfu<kDeriv>(s0 + z + 1, ne, pne, Un, dUn);
+      const double f = fct * (Un / Up) * eip[s0 + z] / ne;
+      if (kDeriv) {
+        const double fd = f * ((dUn) - (dUp * ne + 1.0) / ne);
+        df = df * f + fk * fd;
+        dfsum += df;
+        S2 += (double)(z + 1) * df;
+      }
+      fk = fk * f;
+      fsum += fk;
+      S1 += (double)(z + 1) * fk;
+      if (kDeriv && E.ref[s0 + z + 1] >= 0) { fr[E.ref[s0 + z + 1]] = fk; dr[E.ref[s0 + z + 1]] = df; }
+      Up = Un;
+      dUp = dUn;
+    }
+    Ea[a + 1] = S1 / fsum;
+    if (kDeriv) {
+      Da[a + 1] = (S2 - dfsum * S1 / fsum) / fsum;
+      for (int z = 0; z < ns; ++z) {
+        const int r = E.ref[s0 + z];
+        if (r >= 0) { dr[r] = (dr[r] - dfsum * fr[r] / fsum) / fsum; fr[r] = fr[r] / fsum; }
+      }
+    }
+  }
+
+  template <bool kDeriv>
+  __device__ void sweep(double ne) {
+    const double pne = pow(ne, 1.0 / 6.0);
+    for (int a = 0; a < E.natom; ++a) sweep_atom<kDeriv>(a, ne, pne);
+  }
+
+  // atmosphere::chemeq (atmos_chm.cc:28-330): N[0] = Ne, N[1..na] free atoms; the kept fractions
+  // fr are those of the last Newton sweep (before the last update), as pupdate uses them.
+  __device__ void solve(double Nt) {
+    const int na = E.natom, nm = E.nmol, n = na + 1;
+    capped = 0;
+    double F1 = 0.0, S1 = 0.0;
+    sweep<false>(1.0);
+    for (int a = 0; a < na; ++a) { F1 += E.abund[a] * Ea[a + 1]; S1 += E.abund[a]; }
+    double F3 = 0.0, S3 = 0.0;
+    sweep<false>(Nt);
+    for (int a = 0; a < na; ++a) { F3 += E.abund[a] * Ea[a + 1]; S3 += E.abund[a]; }
+    const double aa = F3 / (S3 * Nt);
+    double bb = F1 / S1 - aa;
+    const double cc = -bb * Nt;
+    bb += 1.0 - aa * Nt;
+    N[0] = fmax((-bb + sqrt(bb * bb - 4.0 * aa * cc)) / (2.0 * aa), 1.0);
+    double esum;
+    int pass = 0;
+    do {
+      esum = 0.0;
+      sweep<false>(N[0]);
+      for (int a = 1; a <= na; ++a) {
+        N[a] = (Nt - N[0]) * E.abund[a - 1] / S3;
+        esum += Ea[a] * N[a];
+      }
+      N[0] = 0.5 * (N[0] + esum);
+      if (++pass >= kPolishCap) { capped = 1; break; }
+    } while ((1E-2 * (N[0] + esum)) < fabs(N[0] - esum));
+    int iter = 0;
+    bool conv;
+    do {
+      sweep<true>(N[0]);
+      // defects (atmos_chm.cc:200-216) and Jacobian (:220-259); molecules enter as rank-one
+      // updates: dm[m][b] = nm count_b / N[b], dm[m][0] = nm (count_e / N0 + sum df / f)
+      d[0] = -N[0];
+      d[1] = N[0] - Nt;
+      A[0] = -1.0;
+      A[n] = 1.0;
+      for (int a = 1; a <= na; ++a) {
+        d[0] += N[a] * Ea[a];
+        d[1] += N[a];
+        A[0] += N[a] * Da[a];
+        A[a] = Ea[a];       // A[0][a]
+        A[n + a] = 1.0;     // A[1][a]
+      }
+      for (int r = 2; r <= na; ++r) {
+        A[r * n] = 0.0;
+        for (int b = 1; b <= na; ++b)
+          A[r * n + b] = (b == 1 ? E.abund[r - 1] : 0.0) - (b == r ? E.abund[0] : 0.0);
+      }
+      double Nr = N[1];
+      double Nc[kEA + 1];
+      for (int a = 2; a <= na; ++a) Nc[a] = N[a];
+      for (int m = 0; m < nm; ++m) {
+        double nmv = 1.0 / (K[m] * kT), dm0 = 0.0;
+        const int nc = E.mnc[m];
+        for (int i = 0; i < nc; ++i) {
+          const int a = E.matom[m][i];
+          if (a == 0) {
+            nmv *= N[0] * kT;
+            dm0 += 1.0 / N[0];
+          } else {
+            const int r = E.mref[m][i];
+            nmv *= fr[r] * N[a] * kT;
+            dm0 += dr[r] / fr[r];
+          }
+        }
+        dm0 *= nmv;
+        const double q = E.mq[m];
+        d[0] += q * nmv;
+        d[1] += nmv;
+        Nr += nmv * (double)E.mmul[m][1];
+        for (int a = 2; a <= na; ++a) Nc[a] += nmv * (double)E.mmul[m][a];
+        A[0] += q * dm0;
+        A[n] += dm0;
+        for (int a = 2; a <= na; ++a)
+          A[a * n] += dm0 * (E.abund[a - 1] * (double)E.mmul[m][1] - E.abund[0] * (double)E.mmul[m][a]);
+        for (int i = 0; i < nc; ++i) {
+          const int b = E.matom[m][i];
+          if (b == 0) continue;
+          bool first = true;  // each distinct component atom once
+          for (int j = 0; j < i; ++j) if (E.matom[m][j] == b) first = false;
+          if (!first) continue;
+          const double dmb = nmv * (double)E.mmul[m][b] / N[b];
+          A[b] += q * dmb;
+          A[n + b] += dmb;
+          for (int a = 2; a <= na; ++a)
+            A[a * n + b] += dmb * (E.abund[a - 1] * (double)E.mmul[m][1] - E.abund[0] * (double)E.mmul[m][a]);
+        }
+      }
+      for (int a = 2; a <= na; ++a) d[a] = E.abund[a - 1] * Nr - E.abund[0] * Nc[a];
+      // Gaussian elimination with partial pivoting; v in place of a copy of d
+      double v[kEA + 1];
+      for (int i = 0; i < n; ++i) v[i] = d[i];
+      for (int c = 0; c < n; ++c) {
+        int p = c;
+        double best = fabs(A[c * n + c]);
+        for (int r = c + 1; r < n; ++r) {
+          const double t = fabs(A[r * n + c]);
+          if (t > best) { best = t; p = r; }
+        }
+        if (p != c) {
+          for (int j = c; j < n; ++j) { const double t = A[c * n + j]; A[c * n + j] = A[p * n + j]; A[p * n + j] = t; }
+          const double t = v[c]; v[c] = v[p]; v[p] = t;
+        }
+        const double piv = A[c * n + c];
+        for (int r = c + 1; r < n; ++r) {
+          const double f = A[r * n + c] / piv;
+          if (f == 0.0) continue;
+          for (int j = c + 1; j < n; ++j) A[r * n + j] -= f * A[c * n + j];
+          v[r] -= f * v[c];
+        }
+      }
+      for (int r = n - 1; r >= 0; --r) {
+        double s = v[r];
+        for (int j = r + 1; j < n; ++j) s -= A[r * n + j] * v[j];
+        v[r] = s / A[r * n + r];
+      }
+      for (int a = 0; a <= na; ++a) {
+        N[a] -= v[a];
+        if (N[a] < 1E-2) N[a] = 1E-2;
+      }
+      iter += 2;  // the reference counts two per pass (atmos_chm.cc:294, 300)
+      if (iter > 100) { capped = 1; break; }
+      conv = true;
+      for (int i = 0; i <= na; ++i) if (fabs(d[i] / N[i]) > 1E-4) conv = false;
+    } while (!conv);
+  }
+
+  // stage total of stage s (with a kept fraction) after solve
+  __device__ __forceinline__ double stage_total(int s, int a) const { return N[a + 1] * fr[E.ref[s]]; }
+
+  // LTE population of level slot l (atom::lte, atom.cc:779-787) at the final Ne (pne = Ne^(1/6))
+  __device__ double level_pop(int l, double pne) const {
+    const int s = E.lst[l];
+    double U, dum;
+    pfu<false>(s, N[0], pne, U, dum);
+    const double g = E.lg[l];
+    return stage_total(s, E.satom[s]) * ((g != 0.0) ? g * exp(-E.lee[l] / (cK * T)) / U : 1.0);
+  }
+};
+
+// ---- node interpolation (atmospheric_interpolation, mathtools.cc:1208-1315) -------------------------------
+__device__ double interpol_1d_falc(double xq) {
+  const double f[11] = {1694.91525424, 2164.5021645, 2342.50815695, 2289.18827635, 2155.92183045,
+                        2094.90240415, 2080.69183003, 2066.44925898, 1960.27182436, 1826.11342193, 1729.74468968};
+  const double x[11] = {-0.01232, 0.08798, 0.2002, 0.32704, 0.46667, 0.61462, 0.7674,
+                        0.92221, 1.07711, 1.22829, 1.37282};
+  const int N = 11;
+  if (xq < x[0]) return f[0];
+  if (xq > x[10]) return f[10];
+  if (!(xq < x[N - 1] && xq > x[0])) return xq >= x[N - 1] ? f[N - 1] : f[0];
+  int i;
+  for (i = 0; i <= N - 2; ++i)
+    if (xq < x[i + 1]) break;
+  double h1, h2, d1, d2, fd1, fd2;
+  if (i > 0) {
+    h1 = x[i] - x[i - 1];
+    h2 = x[i + 1] - x[i];
+    d1 = (f[i] - f[i - 1]) / h1;
+    d2 = (f[i + 1] - f[i]) / h2;
+    const double alpha = 1.0 / 3.0 * (1.0 + h2 / (h1 + h2));
+    fd1 = (d1 * d2 > 0) ? d1 * d2 / (alpha * d2 + (1.0 - alpha) * d1) : 0.0;
+  } else {
+    fd1 = (f[1] - f[0]) / (x[1] - x[0]);
+    h1 = h2 = x[1] - x[0];  // the reference reads an unset h2 here
+  }
+  const double C0 = f[i] + h2 * 0.5 * fd1;
+  if (i + 1 < N - 1) {
+    h1 = x[i + 1] - x[i];
+    h2 = x[i + 2] - x[i + 1];
+    d1 = (f[i + 1] - f[i]) / h1;
+    d2 = (f[i + 2] - f[i + 1]) / h2;
+    const double alpha = 1.0 / 3.0 * (1.0 + h2 / (h1 + h2));
+    fd2 = (d1 * d2 > 0) ? d1 * d2 / (alpha * d2 + (1.0 - alpha) * d1) : 0.0;
+  } else {
+    fd2 = (f[N - 1] - f[N - 2]) / (x[N - 1] - x[N - 2]);
+  }
+  const double C1 = f[i + 1] - h1 * 0.5 * fd2;
+  const double C = (C0 + C1) * 0.5;
+  const double u = (xq - x[i]) / (x[i + 1] - x[i]);
+  return (1.0 - u) * (1.0 - u) * f[i] + u * u * f[i + 1] + u * 2.0 * (1.0 - u) * C;
+}
+
+// Node values of one kind with an optional perturbation of node `pidx` (global index) by `pert`.
+struct NodeView {
+  const double *v;  // the pixel's node vector
+  int pidx;
+  double pert;
+  __device__ double operator()(int g) const { return g == pidx ? v[g] + pert : v[g]; }
+};
+
+// value of kind `kind` at depth x; build: build_from_nodes' defaults, else interpolate_from_nodes'
+__device__ double interp_kind(const EosDev &E, const NodeView &nv, int kind, int x, bool build) {
+  const int N = E.kcount[kind], f0 = E.kfirst[kind];
+  const bool is_temp = (kind == 1);
+  const double lt = E.tau_min + (E.tau_max - E.tau_min) / (E.nd - 1) * x;
+  double q;
+  if (N > 1) {
+    auto der = [&](int i) -> double {
+      if (i == 0) return 0.0;
+      if (i == N - 1) return is_temp ? interpol_1d_falc(E.ntau[f0 + N - 1]) : 0.0;
+      const double h1 = E.ntau[f0 + i] - E.ntau[f0 + i - 1], h2 = E.ntau[f0 + i + 1] - E.ntau[f0 + i];
+      const double d1 = (nv(f0 + i) - nv(f0 + i - 1)) / h1, d2 = (nv(f0 + i + 1) - nv(f0 + i)) / h2;
+      if (d1 * d2 > 0) {
+        const double alpha = 0.3333333 * (1.0 + h2 / (h1 + h2));
+        return d1 * d2 / (alpha * d2 + (1.0 - alpha) * d1);
+      }
+      return 0.0;
+    };
+    if (lt < E.ntau[f0]) q = nv(f0) + der(0) * (lt - E.ntau[f0]);
+    else if (lt > E.ntau[f0 + N - 1]) q = nv(f0 + N - 1) + der(N - 1) * (lt - E.ntau[f0 + N - 1]);
+    else {
+      int ii;
+      for (ii = 0; ii < N - 1; ++ii)
+        if (lt <= E.ntau[f0 + ii + 1]) break;
+      const double ta = E.ntau[f0 + ii], tb = E.ntau[f0 + ii + 1];
+      const double va = nv(f0 + ii), vb = nv(f0 + ii + 1);
+      const double Ec = va + (tb - ta) / 3.0 * der(ii);
+      const double Fc = vb - (tb - ta) / 3.0 * der(ii + 1);
+      const double u = (lt - ta) / (tb - ta);
+      q = (1.0 - u) * (1.0 - u) * (1.0 - u) * va + u * u * u * vb + 3.0 * u * (1.0 - u) * (1.0 - u) * Ec +
+          3.0 * u * u * (1.0 - u) * Fc;
+    }
+    if (is_temp) q = fmin(fmax(q, 3400.0), 20000.0);
+  } else if (N == 1) {
+    q = nv(f0);
+  } else {
+    q = (kind == 4) ? (build ? 1E-3 : 0.0) : (kind >= 5 ? 1E-3 : 0.0);
+  }
+  if (build && kind == 5 && fabs(q) < 1E-3) q = 1E-3;
+  return q;
+}
+
+__device__ __forceinline__ double logtau(const EosDev &E, int x) {
+  return E.tau_min + (E.tau_max - E.tau_min) / (E.nd - 1) * x;
+}
+
+// atmosphere::opacity_continuum (atmos_rad.cc:286-294) from a solved Chem; which: 0 = lambda_he
+// with sigma_he, 1 = lambda_kappa with sigma_kappa.  lev[]: populations of the level slots.
+__device__ double continuum(const EosDev &E, const Chem &c, const double *lev, double nH0, int which) {
+  const double T = c.T, Ne = c.N[0], lambda = which ? E.lambda_kappa : E.lambda_he;
+  double op = 6.65E-25 * Ne;
+  const double stim = exp(-cH * cC / lambda / cK / T);
+  for (int b = 0; b < E.nbf; ++b) {
+    if (!E.bflte[b]) continue;
+    const double sigma = which ? E.sig_k[b] : E.sig_he[b];
+    if (sigma == 0.0) continue;
+    const double pop_mod = lev[E.bfn[b]] * Ne * cSAHA * pow(T, -1.5) * E.bfg[b] / E.bfgn[b] * exp(E.bfip[b] / cK / T);
+    op += sigma * (lev[E.bfl[b]] - pop_mod * stim);
+  }
+  if (E.hm) {
+    const double ca[7] = {1.99654, -1.18267E-5, 2.64243E-6, -4.40524E-10, 3.23992E-14, -1.39568E-18, 2.78701E-23};
+    double alpha = 0.0;
+    for (int i = 0; i < 7; ++i) alpha += ca[i] * pow(lambda * 1E8, (double)i);
+    const double T_P = 5040. / T;
+    const double op_bf =
+        4.158E-28 * alpha * Ne * cK * T * pow(T_P, 2.5) * pow(10.0, 0.754 * T_P) * nH0 * (1.0 - stim);
+    const double l = log10(lambda * 1E8);
+    const double f_0 = -2.2763 - 1.6850 * l + 0.76661 * l * l - 0.053346 * l * l * l;
+    const double f_1 = 15.2827 - 9.2846 * l + 1.99381 * l * l - 0.142631 * l * l * l;
+    const double f_2 = -197.789 + 190.266 * l - 67.9775 * l * l + 10.6913 * l * l * l - 0.625151 * l * l * l * l;
+    const double lt = log10(T_P);
+    op += op_bf + 1E-26 * Ne * cK * T * pow(10.0, f_0 + f_1 * lt + f_2 * lt * lt) * nH0;
+  }
+  return op;
+}
+
+// chemistry + populations + kappa (which as in continuum); returns kappa, fills lev and nH0.  The
+// T-only tables are rebuilt only when T changes (the hydrostatic iterations of one depth share T).
+__device__ double chem_point(const EosDev &E, Chem &c, double T, double Nt, double *lev, double &nH0, int which) {
+  if (T != c.T) c.set_T(T);
+  c.solve(Nt);
+  const double pne = pow(c.N[0], 1.0 / 6.0);
+  for (int l = 0; l < E.nlev; ++l) lev[l] = c.level_pop(l, pne);
+  nH0 = c.stage_total(E.s0[0], 0);
+  return continuum(E, c, lev, nH0, which);
+}
+
+// ---- k_eos_he: hydrostatic equilibrium per (pixel, variant) ---------------------------------------------
+struct EosArgs {
+  const EosDev *tab;
+  int npix, nvar, nd, npar, nf;
+  const double *nodes;    // [npix][npar]
+  const int *active;      // [npix] or null
+  const double *step;     // [npar]
+  double *T, *Nt;         // [npix][nvar][nd]
+  float *rec;             // [npix][nd][nf]
+  float *tan;             // [npix][npar][nd][nf] or null
+  double *Nt_out;         // [npix][nd] or null
+  int *status;            // [npix]
+};
+
+__device__ __forceinline__ void variant_pert(const EosDev &E, const EosArgs &A, int v, int &pidx, double &pert) {
+  pidx = -1;
+  pert = 0.0;
+  if (v > 0) {
+    pidx = E.kfirst[1] + (v - 1) / 2;
+    pert = ((v - 1) % 2 == 0 ? 0.5 : -0.5) * A.step[pidx];
+  }
+}
+
+__global__ void __launch_bounds__(kHeThreads) k_eos_he(EosArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.npix * A.nvar) return;
+  const int p = i % A.npix, v = i / A.npix;
+  if (A.active && !A.active[p]) return;
+  const EosDev &E = *A.tab;
+  NodeView nv{A.nodes + (size_t)p * A.npar, -1, 0.0};
+  variant_pert(E, A, v, nv.pidx, nv.pert);
+  double *Tc = A.T + ((size_t)p * A.nvar + v) * A.nd;
+  double *Nc = A.Nt + ((size_t)p * A.nvar + v) * A.nd;
+  Chem c(E);
+  double lev[kEL];
+  double nH0;
+  int st = 0;
+  // top: fixed point from 0.3 / k T (atmos_pp.cc:184-202)
+  double T0 = interp_kind(E, nv, 1, 0, true);
+  Tc[0] = T0;
+  double Nt = 0.3 / cK / T0, op_prev = 0.0, rho_prev = 0.0;
+  for (int iter = 0; iter < 20; ++iter) {
+    const double op = chem_point(E, c, T0, Nt, lev, nH0, 0);
+    st |= c.capped;
+    const double rho = c.N[1] * 1.4 * 1.67E-24;
+    const double dN = (pow(10.0, logtau(E, 0)) * rho * E.grav / op) / cK / T0 - Nt;
+    Nt += dN;
+    op_prev = op;
+    rho_prev = rho;
+    if (fabs(dN / Nt) < 1E-2) break;
+    if (iter == 19) st |= 2;
+  }
+  Nc[0] = Nt;
+  const double Ntop = Nt;
+  double Tprev = T0, Nprev = Nt;
+  for (int x = 1; x < A.nd; ++x) {
+    const double Tx = interp_kind(E, nv, 1, x, true);
+    Tc[x] = Tx;
+    const double delta_tau = pow(10.0, logtau(E, x)) - pow(10.0, logtau(E, x - 1));
+    double delta_p = rho_prev * E.grav / op_prev * delta_tau;
+    double N = (Nprev * cK * Tprev + delta_p) / cK / Tx;
+    double op = 0.0, rho = 0.0;
+    for (int iter = 0; iter < 20; ++iter) {
+      op = chem_point(E, c, Tx, N, lev, nH0, 0);
+      st |= c.capped;
+      rho = c.N[1] * 1.4 * 1.67E-24;
+      const double kappa_mean = sqrt(op * op_prev / rho / rho_prev);
+      delta_p = E.grav / kappa_mean * delta_tau;
+      const double dN = (Nprev * cK * Tprev + delta_p) / cK / Tx - N;
+      N += dN;
+      if (fabs(dN / Ntop) < 1E-2) break;  // relative to the TOP density, as atmos_pp.cc:235
+      if (iter == 19) st |= 2;
+    }
+    Nc[x] = N;
+    op_prev = op;
+    rho_prev = rho;
+    Tprev = Tx;
+    Nprev = N;
+  }
+  if (st) atomicOr(A.status + p, st);
+}
+
+// ---- k_eos_rec: records and tangents per (depth, pixel) ------------------------------------------------
+// thermal fields of a record (those that move with (T, Nt)); the others are kinematic / field
+__device__ void thermal_fields(const EosDev &E, Chem &c, double T, double Nt, double *f, int &st) {
+  double lev[kEL], nH0;
+  const double kap = chem_point(E, c, T, Nt, lev, nH0, 1);
+  st |= c.capped;
+  const double Ne = c.N[0], tp = 5040.0 / T;
+  f[0] = T;
+  f[2] = Ne;
+  f[7] = kap;
+  f[8] = E.hm ? 4.158E-28 * Ne * cK * T * pow(tp, 2.5) * pow(10.0, 0.754 * tp) * nH0 : 0.0;
+  f[9] = E.hm ? 1E-26 * Ne * cK * T * nH0 : 0.0;
+  double bop = 0.0, bem = 0.0;
+  for (int b = 0; b < E.nbf; ++b) {
+    const double lw = E.lam_w[b];
+    if (!(lw > 0.0)) continue;
+    const double pop_mod = lev[E.bfn[b]] * Ne * cSAHA * pow(T, -1.5) * E.bfg[b] / E.bfgn[b] * exp(E.bfip[b] / cK / T);
+    const double stim = exp(-cH * cC / lw / cK / T);
+    bop += E.sig_w[b] * (lev[E.bfl[b]] - pop_mod * stim);
+    const double planck = 2.0 * 6.62606957 * 8.9875517E-7 / lw / lw / lw / lw / lw / (exp(1.4387769 / lw / T) - 1.0);
+    bem += E.sig_w[b] * pop_mod * (1.0 - stim) * planck;
+  }
+  f[10] = bop;
+  f[11] = bem;
+  for (int j = 0; j < E.nlines; ++j) {
+    const double nl = lev[E.llo[j]], nu = lev[E.lup[j]];
+    f[SNAPI_NFIELD0 + 3 * j + 0] = (nl * E.lBlu[j] - nu * E.lBul[j]) * cH * cC / E.llam0[j] / 4.0 / cPI;
+    f[SNAPI_NFIELD0 + 3 * j + 1] = nu * E.lA[j] * cH * cC / E.llam0[j] / 4.0 / cPI;
+    const double red_mass = 1.66E-24 / (1.0 / 1.008 + 1.66E-24 / E.lmass[j]);
+    const double vmean = sqrt(8.0 * cK * T / cPI / red_mass);
+    f[SNAPI_NFIELD0 + 3 * j + 2] = nH0 * vmean * pow(vmean / 1E6, -E.lalpha[j]) * E.lsig[j];
+  }
+}
+
+// kinematic / field fields 1, 3, 4, 5, 6 (project and transform, atmos_rad.cc:14-48; V_x = V_y = 0)
+__device__ void field_fields(const EosDev &E, const NodeView &nv, int x, bool build, double *f) {
+  const double vt = interp_kind(E, nv, 2, x, build);
+  const double vz = interp_kind(E, nv, 3, x, build);
+  const double B = interp_kind(E, nv, 4, x, build);
+  const double th = interp_kind(E, nv, 5, x, build);
+  const double ph = interp_kind(E, nv, 6, x, build);
+  const double sp = sin(E.phi), cp = cos(E.phi), ct = cos(cPI - E.theta), st = sin(cPI - E.theta);
+  f[1] = vt;
+  f[3] = sp * st * 0.0 + cp * st * 0.0 + ct * vz;
+  const double Bx = B * sin(th) * cos(ph), By = B * sin(th) * sin(ph), Bz = B * cos(th);
+  const double mg = sqrt(Bx * Bx + By * By + Bz * Bz);
+  const double nBx = ct * cp * Bx + sp * By - st * cp * Bz;
+  const double nBy = -ct * sp * Bx + cp * By + st * sp * Bz;
+  const double nBz = st * Bx + ct * Bz;
+  f[4] = mg;
+  f[5] = acos(nBz / mg) * 180.0 / cPI;
+  f[6] = atan(nBy / nBx) * 180.0 / cPI;
+}
+
+__global__ void __launch_bounds__(kRecThreads) k_eos_rec(EosArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.npix * A.nd) return;
+  const int p = i % A.npix, x = i / A.npix;
+  if (A.active && !A.active[p]) return;
+  const EosDev &E = *A.tab;
+  const int nf = A.nf;
+  const double *nodes = A.nodes + (size_t)p * A.npar;
+  Chem c(E);
+  int st = 0;
+  double r0[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES];
+  const double *Tv = A.T + (size_t)p * A.nvar * A.nd;
+  const double *Nv = A.Nt + (size_t)p * A.nvar * A.nd;
+  thermal_fields(E, c, Tv[x], Nv[x], r0, st);
+  NodeView nv0{nodes, -1, 0.0};
+  field_fields(E, nv0, x, true, r0);
+  float *rp = A.rec + ((size_t)p * A.nd + x) * nf;
+  bool finite = true;
+  for (int f = 0; f < nf; ++f) {
+    rp[f] = (float)r0[f];
+    finite &= isfinite(r0[f]);
+  }
+  if (A.Nt_out) A.Nt_out[(size_t)p * A.nd + x] = Nv[x];
+  if (A.tan) {
+    double fp[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES], fm[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES];
+    for (int q = 0; q < A.npar; ++q) {
+      float *tq = A.tan + (((size_t)p * A.npar + q) * A.nd + x) * nf;
+      const double stp = A.step[q];
+      if (q >= E.kfirst[1] && q < E.kfirst[1] + E.kcount[1]) {
+        const int v = 1 + 2 * (q - E.kfirst[1]);
+        thermal_fields(E, c, Tv[(size_t)v * A.nd + x], Nv[(size_t)v * A.nd + x], fp, st);
+        thermal_fields(E, c, Tv[(size_t)(v + 1) * A.nd + x], Nv[(size_t)(v + 1) * A.nd + x], fm, st);
+        for (int f = 0; f < nf; ++f) {
+          const bool th = !(f == 1 || (f >= 3 && f <= 6));
+          tq[f] = th ? (float)((fp[f] - fm[f]) / stp) : 0.f;
+        }
+      } else {
+        NodeView np{nodes, q, 0.5 * stp}, nm{nodes, q, -0.5 * stp};
+        field_fields(E, np, x, false, fp);
+        field_fields(E, nm, x, false, fm);
+        for (int f = 0; f < nf; ++f) {
+          const bool fl = (f == 1 || (f >= 3 && f <= 6));
+          tq[f] = fl ? (float)((fp[f] - fm[f]) / stp) : 0.f;
+        }
+      }
+    }
+  }
+  if (!finite) st |= 4;
+  if (st) atomicOr(A.status + p, st);
+}
+
+// ---- host side ---------------------------------------------------------------------------------------------
+struct EosCtx {
+  EosDev *d_tab = nullptr;
+  int npar = 0, ntherm = 0;
+  std::vector<double> ref_step;
+  // work buffers for cap pixels
+  int cap = 0, cap_var = 0;
+  double *d_T = nullptr, *d_Nt = nullptr, *d_nodes = nullptr, *d_step = nullptr, *d_Ntout = nullptr;
+  int *d_active = nullptr, *d_status = nullptr;
+  float *d_rec = nullptr, *d_tan = nullptr;
+};
+
+void eos_free_bufs(EosCtx *e) {
+  void *b[] = {e->d_T, e->d_Nt, e->d_nodes, e->d_step, e->d_Ntout, e->d_active, e->d_status, e->d_rec, e->d_tan};
+  for (void *p : b) cudaFree(p);
+  e->d_T = e->d_Nt = e->d_nodes = e->d_step = e->d_Ntout = nullptr;
+  e->d_active = e->d_status = nullptr;
+  e->d_rec = e->d_tan = nullptr;
+  e->cap = e->cap_var = 0;
+}
+
+}  // namespace
+
+void eos_free(snapi_ctx *ctx) {
+  EosCtx *e = static_cast<EosCtx *>(ctx->eos);
+  if (!e) return;
+  eos_free_bufs(e);
+  cudaFree(e->d_tab);
+  delete e;
+  ctx->eos = nullptr;
+}
+
+}  // namespace snapi
+
+using snapi::set_err;
+
+extern "C" {
+
+int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
+  using namespace snapi;
+  if (!ctx) return SNAPI_EINVAL;
+  if (!m || m->natom < 1 || m->natom > SNAPI_EOS_MAX_ATOMS || !m->atoms || m->nmol < 0 ||
+      m->nmol > SNAPI_EOS_MAX_MOLS || (m->nmol && !m->mols) || (ctx->nlines && !m->lines) || m->npar < 1 ||
+      m->npar > SNAPI_EOS_MAX_PAR || !m->node_kind || !m->node_tau)
+    return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: invalid model");
+  if (!(m->lambda_he > 0.0) || !(m->lambda_kappa > 0.0) || !(m->grav > 0.0) || !(m->tau_max > m->tau_min))
+    return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: invalid constants");
+  // the context's depth grid must be the model's
+  for (int x = 0; x < ctx->nd; ++x) {
+    const double t = pow(10.0, m->tau_min + (m->tau_max - m->tau_min) / (ctx->nd - 1) * x);
+    if (fabs(t - ctx->h_tau500[x]) > 1e-12 * t)
+      return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: the problem's tau500 is not the model's log tau grid");
+  }
+  std::vector<EosDev> hv(1);
+  EosDev &H = hv[0];
+  memset(&H, 0, sizeof(EosDev));
+  H.natom = m->natom;
+  H.nmol = m->nmol;
+  H.nlines = ctx->nlines;
+  H.npar = m->npar;
+  H.nd = ctx->nd;
+  H.lambda_he = m->lambda_he;
+  H.lambda_kappa = m->lambda_kappa;
+  H.grav = m->grav;
+  H.tau_min = m->tau_min;
+  H.tau_max = m->tau_max;
+  H.theta = m->theta;
+  H.phi = m->phi;
+  {
+    const double er = cE * cRYD * cRYD;
+    H.ftrav = 1.405169521381833474E+05 * ((4.0 * cPI * cE0) / (er * er));
+  }
+  int ns = 0, nt = 0, nc = 0;
+  for (int a = 0; a < m->natom; ++a) {
+    const snapi_eos_atom &At = m->atoms[a];
+    if (At.nstage < 1 || At.nstage > SNAPI_EOS_MAX_STAGES || ns + At.nstage > kES)
+      return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: atom %d: too many ionisation stages", a);
+    H.abund[a] = At.abundance;
+    H.s0[a] = ns;
+    for (int z = 0; z < At.nstage; ++z) H.satom[ns + z] = a;
+    H.ns[a] = At.nstage;
+    for (int z = 0; z < At.nstage; ++z, ++ns) {
+      const snapi_partition &P = At.pf[z];
+      H.pft[ns] = P.type;
+      H.pfv[ns] = P.type == SNAPI_PF_CONST ? P.value : (P.type == SNAPI_PF_TRAV ? P.g0 : 1.0);
+      H.zeff[ns] = P.zeff;
+      H.eion[ns] = z + 1 < At.nstage ? At.ip[z] : 0.0;
+      if (z + 1 < At.nstage && !std::isfinite(At.ip[z]))
+        return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: atom %d stage %d: no ionisation energy", a, z);
+      H.ref[ns] = -1;
+      if (P.type == SNAPI_PF_TRAV) {
+        if (P.nterm < 0 || P.nterm > SNAPI_PF_MAX_TERMS || nt + P.nterm > kET)
+          return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: too many partition-function terms");
+        H.t0[ns] = nt;
+        for (int t = 0; t < P.nterm; ++t, ++nt) {
+          H.g2[nt] = P.g2[t];
+          H.tee[nt] = P.ee[t];
+          H.tll[nt] = P.ll[t];
+          if (P.m[t] < 0 || P.m[t] > SNAPI_PF_MAX_COEF || nc + P.m[t] > kEC)
+            return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: too many partition-function coefficients");
+          H.c0[nt] = nc;
+          for (int k = 0; k < P.m[t]; ++k, ++nc) { H.cA[nc] = P.a[t][k]; H.cG[nc] = P.gam[t][k]; }
+          H.c1[nt] = nc;
+        }
+        H.t1[ns] = nt;
+      } else if (P.type == SNAPI_PF_IRWIN) {
+        if (P.ncoef < 0 || P.ncoef > SNAPI_PF_MAX_COEF || nc + P.ncoef > kEC)
+          return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: too many Irwin coefficients");
+        H.t0[ns] = nc;
+        for (int k = 0; k < P.ncoef; ++k, ++nc) H.cA[nc] = P.coef[k];
+        H.t1[ns] = nc;
+      } else if (P.type != SNAPI_PF_CONST && P.type != SNAPI_PF_NONE) {
+        return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: unknown partition function type %d", P.type);
+      }
+    }
+  }
+  H.nst = ns;
+  // kept fractions: molecule components, then the stages of record levels
+  int nref = 0;
+  auto keep = [&](int s) -> int {
+    if (H.ref[s] < 0) {
+      if (nref >= kER) return -1;
+      H.ref[s] = nref++;
+    }
+    return H.ref[s];
+  };
+  for (int mm = 0; mm < m->nmol; ++mm) {
+    const snapi_eos_molecule &M = m->mols[mm];
+    if (M.ncomp < 1 || M.ncomp > SNAPI_MOL_MAX_COMP)
+      return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: molecule %d: bad component count", mm);
+    if (M.eqc != SNAPI_EQC_POLY && M.eqc != SNAPI_EQC_HMIN && M.eqc != SNAPI_EQC_CONST)
+      return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: molecule %d: unknown equilibrium constant", mm);
+    if (M.eqc == SNAPI_EQC_POLY && (M.ncoef < 1 || M.ncoef > SNAPI_PF_MAX_COEF))
+      return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: molecule %d: bad coefficients", mm);
+    H.mnc[mm] = M.ncomp;
+    H.meqc[mm] = M.eqc;
+    H.mncoef[mm] = M.ncoef;
+    for (int k = 0; k < SNAPI_PF_MAX_COEF; ++k) H.mcoef[mm][k] = M.coef[k];
+    if (M.eqc == SNAPI_EQC_HMIN) H.hm = 1;
+    double q = 0.0;
+    for (int i = 0; i < M.ncomp; ++i) {
+      const int a = M.comp_atom[i];
+      if (a < -1 || a >= m->natom) return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: molecule %d: bad atom", mm);
+      const int idx = a + 1;
+      H.matom[mm][i] = idx;
+      H.mmul[mm][idx] += 1;
+      q += (double)M.comp_charge[i];
+      if (a >= 0) {
+        const int z = M.comp_charge[i] > 0 ? M.comp_charge[i] : 0;
+        if (z >= m->atoms[a].nstage)
+          return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: molecule %d: bad component charge", mm);
+        const int r = keep(H.s0[a] + z);
+        if (r < 0) return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: too many kept ionisation fractions");
+        H.mref[mm][i] = r;
+      } else {
+        H.mref[mm][i] = -1;
+      }
+    }
+    H.mq[mm] = q;
+  }
+  // level slots: hydrogen's neutral stage is always kept (H-, damping, rho uses the free total)
+  if (keep(H.s0[0]) < 0) return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: too many kept ionisation fractions");
+  int nlev = 0;
+  std::vector<int> slot(m->natom * SNAPI_EOS_MAX_STAGES * SNAPI_EOS_MAX_LEVELS, -1);
+  auto level_slot = [&](int a, int z, int l) -> int {
+    int &sl = slot[(a * SNAPI_EOS_MAX_STAGES + z) * SNAPI_EOS_MAX_LEVELS + l];
+    if (sl < 0) {
+      if (nlev >= kEL) return -1;
+      const int s = H.s0[a] + z;
+      if (keep(s) < 0) return -1;
+      H.lst[nlev] = s;
+      H.lg[nlev] = m->atoms[a].level[z][l].g;
+      H.lee[nlev] = m->atoms[a].level[z][l].ee;
+      sl = nlev++;
+    }
+    return sl;
+  };
+  int nbf = 0;
+  for (int a = 0; a < m->natom; ++a) {
+    const snapi_eos_atom &At = m->atoms[a];
+    for (int z = 0; z + 1 < At.nstage; ++z) {
+      if (At.nlevel[z] < 0 || At.nlevel[z] > SNAPI_EOS_MAX_LEVELS)
+        return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: atom %d stage %d: bad level count", a, z);
+      for (int l = 0; l < At.nlevel[z]; ++l) {
+        const snapi_eos_level &L = At.level[z][l];
+        if (L.sigma_he == 0.0 && L.sigma_kappa == 0.0 && !(L.lambda_win > 0.0)) continue;
+        if (At.nlevel[z + 1] < 1)
+          return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: atom %d: bound-free level without a next stage", a);
+        if (nbf >= kEB) return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: too many bound-free levels");
+        const int sl = level_slot(a, z, l), sn = level_slot(a, z + 1, 0);
+        if (sl < 0 || sn < 0) return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: too many levels");
+        H.bfl[nbf] = sl;
+        H.bfn[nbf] = sn;
+        H.bflte[nbf] = At.nlte ? 0 : 1;
+        H.bfg[nbf] = L.g;
+        H.bfgn[nbf] = At.level[z + 1][0].g;
+        H.bfip[nbf] = At.ip[z] - L.ee;
+        H.sig_he[nbf] = L.sigma_he;
+        H.sig_k[nbf] = L.sigma_kappa;
+        H.sig_w[nbf] = L.sigma_win;
+        H.lam_w[nbf] = L.lambda_win;
+        ++nbf;
+      }
+    }
+  }
+  H.nbf = nbf;
+  for (int j = 0; j < ctx->nlines; ++j) {
+    const snapi_eos_line &L = m->lines[j];
+    if (L.atom < 0 || L.atom >= m->natom || L.stage < 0 || L.stage >= m->atoms[L.atom].nstage || L.lower < 0 ||
+        L.upper < 0 || L.lower >= m->atoms[L.atom].nlevel[L.stage] || L.upper >= m->atoms[L.atom].nlevel[L.stage])
+      return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: line %d: bad level reference", j);
+    const int lo = level_slot(L.atom, L.stage, L.lower), up = level_slot(L.atom, L.stage, L.upper);
+    if (lo < 0 || up < 0) return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: too many levels");
+    H.llo[j] = lo;
+    H.lup[j] = up;
+    H.lBlu[j] = L.Blu;
+    H.lBul[j] = L.Bul;
+    H.lA[j] = L.A;
+    H.lalpha[j] = L.alpha_col;
+    H.lsig[j] = L.sigma_col;
+    H.llam0[j] = ctx->h_line_lam0[j];
+    H.lmass[j] = ctx->h_line_mass[j];
+  }
+  H.nlev = nlev;
+  H.nref = nref;
+  H.href = H.ref[H.s0[0]];
+  // nodes: kinds 1..6, contiguous, non-decreasing
+  for (int k = 0; k < 7; ++k) { H.kfirst[k] = 0; H.kcount[k] = 0; }
+  int prev = 0;
+  for (int q = 0; q < m->npar; ++q) {
+    const int k = m->node_kind[q];
+    if (k < 1 || k > 6 || k < prev) return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: node kinds must be 1..6, non-decreasing");
+    if (k != prev) H.kfirst[k] = q;
+    H.kcount[k] += 1;
+    prev = k;
+    H.ntau[q] = m->node_tau[q];
+  }
+  for (int k = 1; k <= 6; ++k)
+    for (int i = 1; i < H.kcount[k]; ++i)
+      if (!(H.ntau[H.kfirst[k] + i] > H.ntau[H.kfirst[k] + i - 1]))
+        return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: node log tau must increase within a kind");
+  if (H.kcount[1] < 1) return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: at least one temperature node");
+
+  SNAPI_CK(cudaSetDevice(ctx->device));
+  SNAPI_CK(cudaStreamSynchronize(ctx->stream));
+  EosCtx *e = static_cast<EosCtx *>(ctx->eos);
+  if (!e) {
+    e = new EosCtx();
+    ctx->eos = e;
+  }
+  if (!e->d_tab) SNAPI_CK(cudaMalloc(&e->d_tab, sizeof(EosDev)));
+  SNAPI_CK(cudaMemcpy(e->d_tab, &H, sizeof(EosDev), cudaMemcpyHostToDevice));
+  e->npar = m->npar;
+  e->ntherm = H.kcount[1];
+  e->ref_step.assign(m->npar, 0.0);
+  static const double ref_step[7] = {0.0, 5.0, 20.0, 20.0, 0.01, 0.001, 0.001};  // const.h:27-32
+  for (int q = 0; q < m->npar; ++q) e->ref_step[q] = ref_step[m->node_kind[q]];
+  return SNAPI_OK;
+}
+
+int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int *active, float *records, double *Nt,
+                        float *tangents, const double *step, int *pix_status, int mem) {
+  using namespace snapi;
+  if (!ctx) return SNAPI_EINVAL;
+  EosCtx *e = static_cast<EosCtx *>(ctx->eos);
+  if (!e) return set_err(ctx, SNAPI_EINVAL, "snapi_build_records: no node model (snapi_eos_set)");
+  if (npix < 0 || (npix > 0 && (!nodes || !records)) || (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
+    return set_err(ctx, SNAPI_EINVAL, "snapi_build_records: invalid arguments");
+  if (npix == 0) return SNAPI_OK;
+  const int npar = e->npar, nd = ctx->nd, nf = ctx->nfield;
+  const int nvar = tangents ? 1 + 2 * e->ntherm : 1;
+  std::vector<double> hstep = e->ref_step;
+  if (step)
+    for (int q = 0; q < npar; ++q) {
+      if (!(step[q] > 0.0)) return set_err(ctx, SNAPI_EINVAL, "snapi_build_records: steps must be positive");
+      hstep[q] = step[q];
+    }
+  SNAPI_CK(cudaSetDevice(ctx->device));
+  const int B = std::min(npix, ctx->max_batch);
+  if (B > e->cap || nvar > e->cap_var) {
+    SNAPI_CK(cudaStreamSynchronize(ctx->stream));
+    eos_free_bufs(e);
+    const size_t Bz = (size_t)B;
+    SNAPI_CK(cudaMalloc(&e->d_T, sizeof(double) * Bz * nvar * nd));
+    SNAPI_CK(cudaMalloc(&e->d_Nt, sizeof(double) * Bz * nvar * nd));
+    SNAPI_CK(cudaMalloc(&e->d_nodes, sizeof(double) * Bz * npar));
+    SNAPI_CK(cudaMalloc(&e->d_step, sizeof(double) * SNAPI_EOS_MAX_PAR));
+    SNAPI_CK(cudaMalloc(&e->d_Ntout, sizeof(double) * Bz * nd));
+    SNAPI_CK(cudaMalloc(&e->d_active, sizeof(int) * Bz));
+    SNAPI_CK(cudaMalloc(&e->d_status, sizeof(int) * Bz));
+    SNAPI_CK(cudaMalloc(&e->d_rec, sizeof(float) * Bz * nd * nf));
+    if (nvar > 1) SNAPI_CK(cudaMalloc(&e->d_tan, sizeof(float) * Bz * npar * nd * nf));
+    e->cap = B;
+    e->cap_var = nvar;
+  }
+  SNAPI_CK(cudaMemcpyAsync(e->d_step, hstep.data(), sizeof(double) * npar, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->last_ms = 0.0;
+  ctx->last_launches = 0;
+  const bool host = (mem == SNAPI_MEM_HOST);
+  for (int p0 = 0; p0 < npix; p0 += B) {
+    const int nb = std::min(B, npix - p0);
+    EosArgs A;
+    A.tab = e->d_tab;
+    A.npix = nb;
+    A.nvar = nvar;
+    A.nd = nd;
+    A.npar = npar;
+    A.nf = nf;
+    A.step = e->d_step;
+    A.T = e->d_T;
+    A.Nt = e->d_Nt;
+    A.status = e->d_status;
+    if (host) {
+      SNAPI_CK(cudaMemcpyAsync(e->d_nodes, nodes + (size_t)p0 * npar, sizeof(double) * nb * npar,
+                               cudaMemcpyHostToDevice, ctx->stream));
+      if (active)
+        SNAPI_CK(cudaMemcpyAsync(e->d_active, active + p0, sizeof(int) * nb, cudaMemcpyHostToDevice, ctx->stream));
+      A.nodes = e->d_nodes;
+      A.active = active ? e->d_active : nullptr;
+      A.rec = e->d_rec;
+      A.tan = tangents ? e->d_tan : nullptr;
+      A.Nt_out = Nt ? e->d_Ntout : nullptr;
+      if (active) {  // rows of inactive pixels are left untouched: start from the caller's
+        SNAPI_CK(cudaMemcpyAsync(e->d_rec, records + (size_t)p0 * nd * nf, sizeof(float) * nb * nd * nf,
+                                 cudaMemcpyHostToDevice, ctx->stream));
+        if (tangents)
+          SNAPI_CK(cudaMemcpyAsync(e->d_tan, tangents + (size_t)p0 * npar * nd * nf,
+                                   sizeof(float) * nb * npar * nd * nf, cudaMemcpyHostToDevice, ctx->stream));
+        if (Nt)
+          SNAPI_CK(cudaMemcpyAsync(e->d_Ntout, Nt + (size_t)p0 * nd, sizeof(double) * nb * nd,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+      }
+    } else {
+      A.nodes = nodes + (size_t)p0 * npar;
+      A.active = active ? active + p0 : nullptr;
+      A.rec = records + (size_t)p0 * nd * nf;
+      A.tan = tangents ? tangents + (size_t)p0 * npar * nd * nf : nullptr;
+      A.Nt_out = Nt ? Nt + (size_t)p0 * nd : nullptr;
+    }
+    SNAPI_CK(cudaMemsetAsync(e->d_status, 0, sizeof(int) * nb, ctx->stream));
+    SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    const int nhe = nb * nvar;
+    k_eos_he<<<(nhe + kHeThreads - 1) / kHeThreads, kHeThreads, 0, ctx->stream>>>(A);
+    SNAPI_CK(cudaGetLastError());
+    const int nrec = nb * nd;
+    k_eos_rec<<<(nrec + kRecThreads - 1) / kRecThreads, kRecThreads, 0, ctx->stream>>>(A);
+    SNAPI_CK(cudaGetLastError());
+    SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    ctx->last_launches += 2;
+    if (host) {
+      SNAPI_CK(cudaMemcpyAsync(records + (size_t)p0 * nd * nf, e->d_rec, sizeof(float) * nb * nd * nf,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+      if (tangents)
+        SNAPI_CK(cudaMemcpyAsync(tangents + (size_t)p0 * npar * nd * nf, e->d_tan, sizeof(float) * nb * npar * nd * nf,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+      if (Nt)
+        SNAPI_CK(cudaMemcpyAsync(Nt + (size_t)p0 * nd, e->d_Ntout, sizeof(double) * nb * nd, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    }
+    if (pix_status)
+      SNAPI_CK(cudaMemcpyAsync(pix_status + p0, e->d_status, sizeof(int) * nb,
+                               host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
+    SNAPI_CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    SNAPI_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->last_ms += ms;
+  }
+  return SNAPI_OK;
+}
+
+}  // extern "C"

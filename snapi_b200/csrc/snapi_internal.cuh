@@ -324,6 +324,9 @@ struct snapi_ctx {
   std::string err;
   // LM work buffers (allocated on first use)
   void *lm = nullptr;
+  // node model -> records (snapi_eos.cu): tables and work buffers, host copies it checks against
+  void *eos = nullptr;
+  std::vector<double> h_tau500, h_line_lam0, h_line_mass;
 };
 
 namespace snapi {
@@ -335,6 +338,7 @@ int check_status(snapi_ctx *ctx);
 cudaError_t launch_synth(const snapi_ctx *ctx, const KParams &P);
 cudaError_t launch_responses(const snapi_ctx *ctx, const KParams &P);
 void lm_free(snapi_ctx *ctx);  // LM work buffers (snapi_lm.cu)
+void eos_free(snapi_ctx *ctx); // node-model tables and work buffers (snapi_eos.cu)
 // G[m] = M[m] M[m]^T for nmat matrices [16][K] (row-major) on the tensor cores (snapi_tc.cu)
 cudaError_t launch_gram_tf32(const float *M, int nmat, int K, float *G, int *status, cudaStream_t st);
 // Gaussian instrumental broadening (snapi_psf.cu): set-up for one width, in-place launch

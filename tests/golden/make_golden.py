@@ -14,6 +14,9 @@ its 80-depth atmosphere file from REF and runs oracle/_ref/snapi_ref_dump).  Wri
   tests/golden/bench_pool.npz     32 more seeded config-3 columns (seed 303) with records, node
                                   tangents and reference Stokes: the thermal structures the
                                   benchmark tiles over its 64x64 pixels
+  tests/golden/eos_c1.npz, eos_c3.npz  (--only-eos) node-model tables of the c1 / c3 tasks, the
+                                  reference's chemistry on a (T, Nt) grid and the columns its
+                                  build_from_nodes leaves for the config-1/2 and config-3 nodes
 
 Synthetic inputs stand in for observations: seeded numpy generators with the shapes and value
 distributions of the benchmark configurations (no dataset is read).
@@ -291,6 +294,7 @@ def main():
     ap.add_argument("--c4pix", type=int, default=8)
     ap.add_argument("--only-c5", action="store_true")
     ap.add_argument("--only-psf", action="store_true")
+    ap.add_argument("--only-eos", action="store_true")
     ap.add_argument("--c5col", type=int, default=3)
     a = ap.parse_args()
     if not os.path.exists(DUMP):
@@ -299,6 +303,9 @@ def main():
     try:
         for f in CFG_FILES:
             shutil.copy(os.path.join(a.ref, "cfg", f), tmp)
+        if a.only_eos:
+            make_eos(tmp)
+            return
         if a.only_psf:
             make_psf(tmp)
             shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
@@ -325,6 +332,26 @@ def main():
         print("fixtures written to", HERE)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+
+
+def make_eos(tmp):
+    """Node-model tables of the c1 / c3 tasks (atoms, partition functions, levels with their
+    bound-free cross-sections, molecules, line ties, nodes), the reference's chemistry on a (T, Nt)
+    grid and the columns (T, Nt, n_e, kappa, rho) its build_from_nodes leaves for the config-1/2
+    and config-3 node vectors -> tests/golden/eos_c1.npz, eos_c3.npz."""
+    c2 = np.load(os.path.join(HERE, "config2.npz"))
+    c1 = np.load(os.path.join(HERE, "config1.npz"))
+    c3 = np.load(os.path.join(HERE, "config3.npz"))
+    for name, task, nodes in (("eos_c1", "c1.tsk", np.concatenate([c1["nodes"], c2["nodes"]])),
+                              ("eos_c3", "c3.tsk", c3["nodes"])):
+        shutil.copy(os.path.join(HERE, task), os.path.join(tmp, task))
+        nf = os.path.join(tmp, name + "_nodes.f64")
+        np.ascontiguousarray(nodes, dtype="<f8").tofile(nf)
+        out = os.path.join(tmp, name + ".sbin")
+        run([DUMP, "eos", task, nf, str(nodes.shape[0]), out], tmp)
+        d = read_sbin(out)
+        d["nodes"] = nodes
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **d)
 
 
 def make_configs_1_to_3(a, tmp):

@@ -1,0 +1,176 @@
+"""Node model -> column records (build_from_nodes, chemistry, hydrostatic equilibrium, record set-up).
+
+CPU: the FP64 restatement (oracle/eos_oracle.c) against the compiled reference's own outputs
+(tests/golden/eos_c1.npz, eos_c3.npz, config3.npz): the chemistry on a (T, Nt) grid, the columns
+build_from_nodes leaves, the records and the node tangents.
+GPU: snapi_build_records against the oracle and against the reference's records.
+"""
+import numpy as np
+import pytest
+
+from conftest import gpu_available, load_fixture
+
+pytestmark_gpu = pytest.mark.skipif(not gpu_available(), reason="needs a CUDA GPU")
+THERMAL = [0, 2, 7, 8, 9, 10, 11]  # + the line fields
+
+
+@pytest.fixture(scope="module")
+def eos3():
+    return load_fixture("eos_c3")
+
+
+@pytest.fixture(scope="module")
+def eos1():
+    return load_fixture("eos_c1")
+
+
+def _tables(d):
+    import eos_oracle as eo
+    return eo.EosTables(d)
+
+
+def _line_const(fx):
+    return fx["line_const"][:, 0].copy(), fx["line_const"][:, 3].copy()
+
+
+# ---- oracle pins (no GPU) ---------------------------------------------------------------------------
+
+def test_oracle_chemistry_grid(oracle_lib, eos3):
+    """chemeq + lte + opacity_continuum on 14 x 12 (T, Nt) points, 3400..20000 K, 1e11..1e18 cm^-3."""
+    import eos_oracle as eo
+    t = _tables(eos3)
+    for i, T in enumerate(eos3["chem_T"]):
+        for j, Nt in enumerate(eos3["chem_Nt"]):
+            ne, nst, npop, khe, kap, passes = eo.chem(t, T, Nt)
+            assert passes > 0
+            assert abs(ne / eos3["chem_ne"][i, j] - 1) < 1e-12
+            assert abs(khe / eos3["chem_kap_he"][i, j] - 1) < 1e-12
+            assert abs(kap / eos3["chem_kap"][i, j] - 1) < 1e-12
+            ref = eos3["chem_stage"][i, j]
+            m = ref > 1e-200
+            np.testing.assert_allclose(nst[m], ref[m], rtol=1e-11)
+            ref = eos3["chem_lev"][i, j]
+            m = ref > 1e-200
+            np.testing.assert_allclose(npop[m], ref[m], rtol=1e-11)
+
+
+@pytest.mark.parametrize("name", ["eos_c3", "eos_c1"])
+def test_oracle_hydrostatic_columns(oracle_lib, name):
+    """T and Nt of build_from_nodes for the config-3 node vectors (4 T nodes) and the config-1/2
+    vectors (one T node per depth)."""
+    import eos_oracle as eo
+    d = load_fixture(name)
+    t = _tables(d)
+    fx = load_fixture("config3" if name == "eos_c3" else "config1")
+    lam0, mass = _line_const(fx)
+    for p in range(min(6, d["nodes"].shape[0])):
+        T, Nt, rec, st = eo.build(t, lam0, mass, d["nodes"][p])
+        assert st == 0
+        np.testing.assert_allclose(T, d["he_T"][p], rtol=1e-13)
+        np.testing.assert_allclose(Nt, d["he_Nt"][p], rtol=1e-11)
+        np.testing.assert_allclose(rec[:, 2], d["he_ne"][p], rtol=1e-11)
+
+
+def test_oracle_records_and_tangents(oracle_lib, eos3, config3):
+    """The full record (27 fields) and the node tangents of config-3 pixels against the reference's
+    (the fixture stores them in float32, hence the 1e-7 tolerances)."""
+    import eos_oracle as eo
+    t = _tables(eos3)
+    lam0, mass = _line_const(config3)
+    for p in (0, 5):
+        T, Nt, rec, st = eo.build(t, lam0, mass, config3["nodes"][p])
+        ref = config3["record"][p].astype(np.float64)
+        np.testing.assert_allclose(rec, ref, rtol=2e-7, atol=0)
+        tan, st = eo.tangents(t, lam0, mass, config3["nodes"][p])
+        assert st == 0
+        rt = config3["tangent"][p].astype(np.float64)
+        for q in range(rt.shape[0]):
+            scale = np.abs(rt[q]).max(axis=0)
+            # a field whose tangent is pure rounding noise in the reference (inclination w.r.t. |B|)
+            # is compared against the field's own scale
+            floor = np.maximum(scale, 1e-6 * np.abs(ref).max(axis=0))
+            err = np.abs(tan[q] - rt[q]).max(axis=0) / floor
+            assert err.max() < 1e-5, (q, err)
+
+
+# ---- GPU ---------------------------------------------------------------------------------------------
+
+def _gpu_ctx(fx, eos, **kw):
+    import snapi_b200 as sb
+    from snapi_b200.eos_tables import EosTables
+    ctx = sb.Context.from_fixture(fx, **kw)
+    ctx.eos_set(EosTables(eos))
+    return ctx
+
+
+@pytest.mark.gpu
+@pytestmark_gpu
+def test_gpu_records_vs_oracle_and_reference(oracle_lib, eos3, config3):
+    """Records of the 8 config-3 node vectors: FP32 rounding of the FP64 device result against
+    the oracle, and against the reference's own records."""
+    import eos_oracle as eo
+    ctx = _gpu_ctx(config3, eos3)
+    nodes = config3["nodes"]
+    rec, tan, nt, status = ctx.build_records(nodes, tangents=False, want_nt=True)
+    assert np.all(status == 0)
+    assert ctx.last_launches() == 2
+    t = _tables(eos3)
+    lam0, mass = _line_const(config3)
+    for p in range(nodes.shape[0]):
+        T, Nt, ro, st = eo.build(t, lam0, mass, nodes[p])
+        np.testing.assert_allclose(nt[p], Nt, rtol=1e-10)
+        np.testing.assert_allclose(rec[p], ro, rtol=3e-7, atol=0)
+        np.testing.assert_allclose(rec[p], config3["record"][p], rtol=3e-7, atol=0)
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytestmark_gpu
+def test_gpu_tangents_vs_reference(oracle_lib, eos3, config3):
+    """Node tangents (central differences with the reference's steps: two full builds per
+    temperature node, re-interpolation for the others) against the reference's."""
+    ctx = _gpu_ctx(config3, eos3)
+    nodes = config3["nodes"]
+    rec, tan, _, status = ctx.build_records(nodes, tangents=True)
+    assert np.all(status == 0)
+    for p in range(nodes.shape[0]):
+        ref = config3["record"][p].astype(np.float64)
+        rt = config3["tangent"][p].astype(np.float64)
+        for q in range(rt.shape[0]):
+            scale = np.abs(rt[q]).max(axis=0)
+            floor = np.maximum(scale, 1e-6 * np.abs(ref).max(axis=0))
+            err = np.abs(tan[p, q] - rt[q]).max(axis=0) / floor
+            assert err.max() < 2e-5, (p, q, err)
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytestmark_gpu
+def test_gpu_dense_temperature_nodes(oracle_lib, eos1, config1, config2):
+    """The config-1/2 model (80 temperature nodes, one per depth, + 5): records of 17 columns
+    against the reference's, and the hydrostatic Nt against its build_from_nodes."""
+    ctx = _gpu_ctx(config1, eos1)
+    nodes = eos1["nodes"]
+    rec, _, nt, status = ctx.build_records(nodes, tangents=False, want_nt=True)
+    assert np.all(status == 0)
+    np.testing.assert_allclose(nt, eos1["he_Nt"], rtol=1e-10)
+    ref = np.concatenate([config1["record"], config2["record"]]).astype(np.float64)
+    np.testing.assert_allclose(rec, ref, rtol=3e-7, atol=0)
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytestmark_gpu
+def test_gpu_active_rows_untouched_and_batches(oracle_lib, eos3, config3):
+    """Inactive pixels keep the caller's rows; several device batches give the same records."""
+    nodes = np.concatenate([config3["nodes"]] * 3)
+    ctx = _gpu_ctx(config3, eos3, max_batch=5)
+    active = np.ones(nodes.shape[0], np.int32)
+    active[[1, 4, 17]] = 0
+    rec, tan, _, status = ctx.build_records(nodes, active=active, tangents=True)
+    assert np.all(status == 0)
+    assert not rec[[1, 4, 17]].any() and not tan[[1, 4, 17]].any()
+    for p in np.flatnonzero(active):
+        np.testing.assert_array_equal(rec[p], rec[p % 8] if active[p % 8] else rec[p])
+    np.testing.assert_allclose(rec[8], config3["record"][0], rtol=3e-7)
+    ctx.close()
