@@ -390,6 +390,15 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *model);
 int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int *active, float *records,
                         double *Nt, float *tangents, const double *step, int *pix_status, int mem);
 
+/* The whole atmosphere::stokes_lm_fit (atmos_fit.cc:18-227) of npix pixels with the node -> record
+ * map on the device: the loop snapi_lm_begin; { snapi_build_records of the requested node vectors of
+ * the active pixels (with the reference's tangent steps); snapi_lm_step } ...; snapi_lm_result, all
+ * buffers resident on the GPU.  The context needs a node model (snapi_eos_set) whose node kinds are
+ * opts->node_kind.  Outputs as snapi_lm_result; n_steps (may be NULL): LM steps taken. */
+int snapi_lm_fit(snapi_ctx *ctx, int npix, const snapi_lm_opts *opts, const double *nodes0, const float *obs,
+                 const double *w_stokes, const float *mask, double *nodes, double *chi2, int *iters, float *stokes,
+                 int *n_steps, int mem);
+
 /* Pinned host memory for SNAPI_MEM_HOST arguments. */
 void *snapi_host_alloc(size_t bytes);
 void snapi_host_free(void *p);

@@ -99,6 +99,8 @@ def lib():
         L.snapi_spectral_broaden.argtypes = [vp, ip, fp, ctypes.c_double, ip]
         L.snapi_eos_set.argtypes = [vp, vp]
         L.snapi_build_records.argtypes = [vp, ip, fp, fp, fp, fp, fp, fp, fp, ip]
+        L.snapi_lm_fit.argtypes = [vp, ip, ctypes.POINTER(SnapiLmOpts), fp, fp, fp, fp, fp, fp, fp, fp,
+                                   ctypes.POINTER(ctypes.c_int), ip]
         L.snapi_zeeman_pattern.argtypes = [ip, ip, ctypes.c_double, ctypes.c_double, ctypes.POINTER(SnapiLine)]
         L.snapi_host_alloc.restype = vp
         L.snapi_host_alloc.argtypes = [ctypes.c_size_t]
@@ -328,6 +330,28 @@ class Context:
         st = np.zeros((npix, self.nl, 4), np.float32)
         self._check(lib().snapi_lm_result(self._ctx, _ptr(nodes), _ptr(chi2), _ptr(iters), _ptr(st), MEM_HOST))
         return {"nodes": nodes, "chi2": chi2, "iters": iters, "stokes": st}
+
+    def lm_fit_device(self, nodes0, obs, node_kind, resp_step, mask=None, w_stokes=(1.0, 1.0, 1.0, 1.0), lm_start=1e3,
+                      max_iter=30, delta=1e-3, stopping_chisq=1e-30, spectral_broadening=0.0):
+        """The whole fit with the node -> record map on the GPU (snapi_lm_fit; needs eos_set)."""
+        n0 = np.ascontiguousarray(nodes0, dtype=np.float64)
+        npix, npar = n0.shape
+        ob = _f32(obs)
+        mk = None if mask is None else _f32(mask)
+        kind = np.ascontiguousarray(node_kind, dtype=np.int32)
+        stp = np.ascontiguousarray(np.broadcast_to(resp_step, (npar,)), dtype=np.float64)
+        opts = SnapiLmOpts(npar, kind.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), float(lm_start), int(max_iter),
+                           float(delta), float(stopping_chisq), stp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                           float(spectral_broadening))
+        ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
+        nodes = np.zeros((npix, npar))
+        chi2 = np.zeros(npix)
+        iters = np.zeros(npix, np.int32)
+        st = np.zeros((npix, self.nl, 4), np.float32)
+        steps = ctypes.c_int(0)
+        self._check(lib().snapi_lm_fit(self._ctx, npix, ctypes.byref(opts), _ptr(n0), _ptr(ob), _ptr(ws), _ptr(mk),
+                                       _ptr(nodes), _ptr(chi2), _ptr(iters), _ptr(st), ctypes.byref(steps), MEM_HOST))
+        return {"nodes": nodes, "chi2": chi2, "iters": iters, "stokes": st, "steps": steps.value}
 
     def lm_fit(self, nodes0, obs, builder, node_kind, resp_step, **kw):
         """Run the fit to the end.  builder(nodes [n, npar], active [n] bool) returns (records,

@@ -696,6 +696,7 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_rec(EosArgs A) {
 struct EosCtx {
   EosDev *d_tab = nullptr;
   int npar = 0, ntherm = 0;
+  std::vector<int> kind;
   std::vector<double> ref_step;
   // work buffers for cap pixels
   int cap = 0, cap_var = 0;
@@ -714,6 +715,14 @@ void eos_free_bufs(EosCtx *e) {
 }
 
 }  // namespace
+
+bool eos_matches(const snapi_ctx *ctx, int npar, const int *node_kind) {
+  const EosCtx *e = static_cast<const EosCtx *>(ctx->eos);
+  if (!e || !node_kind || npar != e->npar) return false;
+  for (int q = 0; q < npar; ++q)
+    if (node_kind[q] != e->kind[q]) return false;
+  return true;
+}
 
 void eos_free(snapi_ctx *ctx) {
   EosCtx *e = static_cast<EosCtx *>(ctx->eos);
@@ -946,6 +955,7 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
   SNAPI_CK(cudaMemcpy(e->d_tab, &H, sizeof(EosDev), cudaMemcpyHostToDevice));
   e->npar = m->npar;
   e->ntherm = H.kcount[1];
+  e->kind.assign(m->node_kind, m->node_kind + m->npar);
   e->ref_step.assign(m->npar, 0.0);
   static const double ref_step[7] = {0.0, 5.0, 20.0, 20.0, 0.01, 0.001, 0.001};  // const.h:27-32
   for (int q = 0; q < m->npar; ++q) e->ref_step[q] = ref_step[m->node_kind[q]];
@@ -970,7 +980,9 @@ int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int
       hstep[q] = step[q];
     }
   SNAPI_CK(cudaSetDevice(ctx->device));
-  const int B = std::min(npix, ctx->max_batch);
+  // the build is latency-bound per column: launch as many columns as the scratch allows (the FP64
+  // (T, Nt) scratch of 16384 columns with 9 variants is 190 MB)
+  const int B = std::min(npix, std::max(ctx->max_batch, 16384));
   if (B > e->cap || nvar > e->cap_var) {
     SNAPI_CK(cudaStreamSynchronize(ctx->stream));
     eos_free_bufs(e);

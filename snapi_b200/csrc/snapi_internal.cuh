@@ -339,6 +339,8 @@ cudaError_t launch_synth(const snapi_ctx *ctx, const KParams &P);
 cudaError_t launch_responses(const snapi_ctx *ctx, const KParams &P);
 void lm_free(snapi_ctx *ctx);  // LM work buffers (snapi_lm.cu)
 void eos_free(snapi_ctx *ctx); // node-model tables and work buffers (snapi_eos.cu)
+// the context has a node model with these npar node kinds (snapi_eos.cu)
+bool eos_matches(const snapi_ctx *ctx, int npar, const int *node_kind);
 // G[m] = M[m] M[m]^T for nmat matrices [16][K] (row-major) on the tensor cores (snapi_tc.cu)
 cudaError_t launch_gram_tf32(const float *M, int nmat, int K, float *G, int *status, cudaStream_t st);
 // Gaussian instrumental broadening (snapi_psf.cu): set-up for one width, in-place launch

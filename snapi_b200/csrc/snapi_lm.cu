@@ -62,6 +62,8 @@ struct LmWork {
   float *d_obs = nullptr, *d_mask = nullptr, *d_scur = nullptr, *d_snew = nullptr, *d_J = nullptr;
   float *d_rec = nullptr, *d_tan = nullptr, *d_M = nullptr, *d_G = nullptr;
   int *d_skip_syn = nullptr, *d_skip_resp = nullptr, *d_active = nullptr;
+  double *d_req_out = nullptr;  // snapi_lm_fit: the step's copies of request / active
+  int *d_act_out = nullptr;
   std::vector<int> h_active, kind;
   double broaden = 0.0;  // Gaussian instrumental width [cm], 0: none
 };
@@ -288,9 +290,11 @@ LmWork *work(snapi_ctx *ctx) { return static_cast<LmWork *>(ctx->lm); }
 
 void free_bufs(LmWork *w) {
   void *b[] = {w->d_M, w->d_G, w->d_nodes, w->d_req, w->d_step, w->d_pix, w->d_obs, w->d_mask, w->d_scur, w->d_snew,
-               w->d_J, w->d_rec, w->d_tan, w->d_skip_syn, w->d_skip_resp, w->d_active};
+               w->d_J, w->d_rec, w->d_tan, w->d_skip_syn, w->d_skip_resp, w->d_active, w->d_req_out, w->d_act_out};
   for (void *x : b)
     if (x) cudaFree(x);
+  w->d_req_out = nullptr;
+  w->d_act_out = nullptr;
   w->d_nodes = w->d_req = w->d_step = nullptr;
   w->d_pix = nullptr;
   w->d_obs = w->d_mask = w->d_scur = w->d_snew = w->d_J = w->d_rec = w->d_tan = w->d_M = w->d_G = nullptr;
@@ -522,6 +526,58 @@ int snapi_lm_result(snapi_ctx *ctx, double *nodes, double *chi2, int *iters, flo
     SNAPI_CK(cudaMemcpy(stokes, w->d_scur, sizeof(float) * npix * ctx->nl * 4,
                         mem == SNAPI_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
   return SNAPI_OK;
+}
+
+// The whole stokes_lm_fit (atmos_fit.cc:18-227) of a batch of pixels with the node -> record map
+// on the device: every step builds the records and node tangents of the requested node vectors
+// (snapi_build_records on the LM's own device buffers, active pixels only) and takes one LM
+// iteration on them.  Nothing returns to the host between steps except the active count.
+int snapi_lm_fit(snapi_ctx *ctx, int npix, const snapi_lm_opts *opts, const double *nodes0, const float *obs,
+                 const double *w_stokes, const float *mask, double *nodes, double *chi2, int *iters, float *stokes,
+                 int *n_steps, int mem) {
+  if (!ctx) return SNAPI_EINVAL;
+  if (!opts || npix < 1 || (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
+    return set_err(ctx, SNAPI_EINVAL, "snapi_lm_fit: invalid arguments");
+  if (!eos_matches(ctx, opts->npar, opts->node_kind))
+    return set_err(ctx, SNAPI_EINVAL, "snapi_lm_fit: no node model (snapi_eos_set) with these node kinds");
+  std::vector<double> hreq;
+  if (mem == SNAPI_MEM_HOST) hreq.resize((size_t)npix * opts->npar);
+  SNAPI_CK(cudaSetDevice(ctx->device));
+  double *req_dev = nullptr;
+  if (mem == SNAPI_MEM_DEVICE) SNAPI_CK(cudaMalloc(&req_dev, sizeof(double) * (size_t)npix * opts->npar));
+  int st = snapi_lm_begin(ctx, npix, opts, nodes0, obs, w_stokes, mask,
+                          mem == SNAPI_MEM_HOST ? hreq.data() : req_dev, mem);
+  if (req_dev) cudaFree(req_dev);
+  if (st) return st;
+  LmWork *w = work(ctx);
+  if (!w->d_req_out) {
+    SNAPI_CK(cudaMalloc(&w->d_req_out, sizeof(double) * (size_t)w->cap * w->cap_par));
+    SNAPI_CK(cudaMalloc(&w->d_act_out, sizeof(int) * (size_t)w->cap));
+  }
+  SNAPI_CK(cudaMemcpyAsync(w->d_active, w->h_active.data(), sizeof(int) * npix, cudaMemcpyHostToDevice, ctx->stream));
+  double ms = 0.0;
+  int launches = 0, steps = 0;
+  const int cap = 10 * opts->max_iter + 10;  // accepted + rejected steps of any pixel stay below this
+  for (;;) {
+    st = snapi_build_records(ctx, npix, w->d_req, w->d_active, w->d_rec, nullptr, w->d_tan, nullptr, nullptr,
+                             SNAPI_MEM_DEVICE);
+    if (st) return st;
+    ms += ctx->last_ms;
+    launches += ctx->last_launches;
+    int na = 0;
+    st = snapi_lm_step(ctx, w->d_rec, w->d_tan, w->d_req_out, w->d_act_out, &na, SNAPI_MEM_DEVICE);
+    if (st) return st;
+    ms += ctx->last_ms;
+    launches += ctx->last_launches;
+    ++steps;
+    if (na == 0) break;
+    if (steps >= cap) return set_err(ctx, SNAPI_ENONCONV, "snapi_lm_fit: %d pixels still active after %d steps", na, steps);
+  }
+  st = snapi_lm_result(ctx, nodes, chi2, iters, stokes, mem);
+  ctx->last_ms = ms;
+  ctx->last_launches = launches;
+  if (n_steps) *n_steps = steps;
+  return st;
 }
 
 }  // extern "C"

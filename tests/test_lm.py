@@ -100,3 +100,57 @@ def test_lm_with_spectral_broadening_matches_reference(sb, config4_psf):
     d = out["nodes"] - fx["fit_nodes"][sel]
     d[:, 9] = (d[:, 9] + np.pi / 2) % np.pi - np.pi / 2
     assert np.all(np.abs(d[:, :4]) < 80.0) and np.all(np.abs(d[:, 7]) < 10.0) and np.all(np.abs(d[:, 8:10]) < 0.02)
+
+
+def _eos_tables():
+    from conftest import load_fixture
+    from snapi_b200.eos_tables import EosTables
+    return EosTables(load_fixture("eos_c3"))
+
+
+def test_lm_device_build_matches_reference_fit(sb, config4):
+    """The whole stokes_lm_fit on the GPU (snapi_lm_fit: node -> record build + LM steps, nothing
+    back on the host between steps) against the reference's fit of the same config-4 pixels, with
+    the tolerances of the host-builder test above."""
+    fx = config4
+    ic = _ic(fx)
+    kinds = fx["node_kind"]
+    ctx = sb.Context.from_fixture(fx, stokes_scale=ic)
+    ctx.eos_set(_eos_tables())
+    out = ctx.lm_fit_device(fx["nodes0"], fx["target"], kinds, 1e-2 * node_scales(kinds), mask=fx["mask"],
+                            lm_start=1e3, max_iter=int(fx["iters"][0]), delta=1e-3)
+    ctx.close()
+    ours = out["chi2"] * ic * ic
+    ref = fx["fit_chi2"]
+    print("device-built fit: chi2 ours / reference:", ours / ref, "iterations", out["iters"], "steps", out["steps"])
+    assert np.all(ours / ref < 1.01) and np.all(ours / ref > 0.8)
+    d = out["nodes"] - fx["fit_nodes"]
+    d[:, 9] = (d[:, 9] + np.pi / 2) % np.pi - np.pi / 2
+    assert np.all(np.abs(d[:, :4]) < 80.0)
+    assert np.all(np.abs(d[:, 4:7]) < 5e3)
+    assert np.all(np.abs(d[:, 7]) < 10.0)
+    assert np.all(np.abs(d[:, 8:10]) < 0.02)
+
+
+def test_lm_device_build_with_spectral_broadening(sb, config4_psf):
+    """snapi_lm_fit with the 45 mA instrumental profile against the reference's broadened fit
+    (pixels 0 and 1, as the host-builder test)."""
+    fx = config4_psf
+    sel = np.array([0, 1])
+    w = float(fx["broadening"][0])
+    mask = fx["mask"][sel]
+    target = np.where(mask[:, :, None] > 0, fx["target"][sel], 0.0)
+    ic = float(np.abs(target[:, :, 0]).max())
+    kinds = fx["node_kind"]
+    ctx = sb.Context.from_fixture(fx, stokes_scale=ic)
+    ctx.eos_set(_eos_tables())
+    out = ctx.lm_fit_device(fx["nodes0"][sel], target, kinds, 1e-2 * node_scales(kinds), mask=mask, lm_start=1e3,
+                            max_iter=int(fx["iters"][0]), delta=1e-3, spectral_broadening=w)
+    ctx.close()
+    ours = out["chi2"] * ic * ic
+    ref = fx["fit_chi2"][sel]
+    print("device-built broadened fit: chi2 ours / reference", ours / ref, "iterations", out["iters"])
+    assert np.all(ours / ref < 1.01) and np.all(ours / ref > 0.8)
+    d = out["nodes"] - fx["fit_nodes"][sel]
+    d[:, 9] = (d[:, 9] + np.pi / 2) % np.pi - np.pi / 2
+    assert np.all(np.abs(d[:, :4]) < 80.0) and np.all(np.abs(d[:, 7]) < 10.0) and np.all(np.abs(d[:, 8:10]) < 0.02)
