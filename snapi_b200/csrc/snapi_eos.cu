@@ -72,7 +72,8 @@ struct EosDev {
   int ref[kES];      // kept-fraction slot, -1 none
   int satom[kES];    // atom of each stage
   // Traving asymptotic terms and level sums
-  double g2[kET], tee[kET], tll[kET];
+  double g2[kET], tee[kET], tll[kET], til[kET], tA[kET];  // til = 1/l, tA = ((1/3 (l-1) - 1/2)(l-1) - 1/6)(l-1)
+  double zf[kES], izf[kES];  // Traving: z * f (Fischel-Sparks cut constant) and its inverse
   int c0[kET], c1[kET];
   double cA[kEC], cG[kEC];
   // molecules (components: 1-based atom, 0 the electron)
@@ -97,30 +98,29 @@ struct EosDev {
   int kfirst[7], kcount[7];
 };
 
-// ---- partition functions (partf.cc:217-283) ---------------------------------------------------------
-__device__ __forceinline__ double qas_f(double l, double p, double Dz) {
-  if (p > l) {
-    const double llm = l - 1.0;
-    return ((1.3333333 * p + 0.5) * p + 0.16666667 + 1.33333333 * Dz) * p - 0.4 * Dz * Dz / p -
-           ((0.33333333 * llm - 0.5) * llm - 0.16666667 - Dz) * llm + 0.5 * Dz * Dz / l;
-  }
-  const double axl2 = Dz / (l * l);
-  return (1.0 + axl2 * (0.33333333 + 0.1 * axl2)) * p * p * p * p / l;
-}
-
-__device__ __forceinline__ double dqas_f(double l, double p, double Dz) {
-  if (p > l) return ((3.0 * 1.3333333 * p + 1.0) * p + 0.16666667 + 1.33333333 * Dz) + 0.4 * Dz * Dz / (p * p);
-  const double axl2 = Dz / (l * l);
-  return 4.0 * (1.0 + axl2 * (0.33333333 + 0.1 * axl2)) * p * p * p / l;
-}
-
 // ---- the chemistry of one (T, Nt) point, one thread -----------------------------------------------------
+// Ionisation sweep (atom::ionfrc, atom.cc:892-925) in division-free form.  The reference chains
+// f_z = fct (U_{z+1} / U_z) exp(-chi_z / kT) / ne and fk_{z+1} = fk_z f_z, then normalises; the chain
+// telescopes to fk_z = (U_z / U_0) prod_{z'<z} c_{z'} / ne with c = fct exp(-chi / kT) (T only), and
+// U_0 cancels in the normalisation, so a stage costs U_z (its Fischel-Sparks terms, whose T-only parts
+// are hoisted) and two products.  Likewise the Ne derivative recursion of the reference,
+// df_{z+1} = df_z f_z + fk_z f_z (dlnU_{z+1} - dlnU_z - 1/ne), sums to df_z = fk_z (dlnU_z - dlnU_0 - z/ne).
+// Traving U (partf.cc:217-238): U = Ut + sum_t w2_t qas_f(l_t, p, Dz) with p = zf / ne^(1/6) and
+// qas_f (Fischel-Sparks eq. 26 / 27, partf.cc:256-270) written as
+//   p > l:  ((4/3 p + 1/2) p + 1/6 + 4/3 Dz) p - 0.4 Dz^2 / p - (A_l - Dz (l - 1)) + 0.5 Dz^2 / l
+//   p <= l: (1 + a (1/3 + a / 10)) p^4 / l,  a = Dz / l^2
+// with A_l = ((1/3 (l-1) - 1/2)(l-1) - 1/6)(l-1) and the reference's decimal constants; dU keeps only
+// the last term, as trav::dU does (partf.cc:247-248).
+//
+// One thread per column: a warp holding one column per lane (and sharing its stage loops) issues 32
+// columns per instruction.  A warp per column (stages in lanes, butterfly sums) shortens a column's
+// chain but measured 14x slower at 4096 columns x 9 variants, where the GPU is full either way.
 struct Chem {
   const EosDev &E;
-  double T, kT, fct;
+  double T, kT;
   double Ut[kES];   // T-only part of U (whole U for CONST / IRWIN / NONE)
-  double eip[kES];  // exp(-eion / kT)
-  double alp[kES];  // 31.321 z^2 x
+  double cz[kES];   // fct exp(-chi / kT): the T-only factor of the stage ratio
+  double Dz[kES];   // 31.321 z^2 x
   double w2[kET];   // g2 exp(-2.302585 ee x)
   double K[kEM];
   double Ea[kEA + 1], Da[kEA + 1];  // sum_i i f_i, sum_i i df_i / dNe per atom (1-based)
@@ -135,7 +135,7 @@ struct Chem {
     T = Tin;
     kT = cK * T;
     const double x = 5040.0 / T;
-    fct = 2.0 * pow((2.0 * cPI * cME * cK * T) / (cH * cH), 1.5);
+    const double fct = 2.0 * pow((2.0 * cPI * cME * cK * T) / (cH * cH), 1.5);
     for (int s = 0; s < E.nst; ++s) {
       const int ty = E.pft[s];
       double u = E.pfv[s];
@@ -144,7 +144,7 @@ struct Chem {
           for (int c = E.c0[t]; c < E.c1[t]; ++c) u += E.cA[c] * exp(-2.302585 * E.cG[c] * x);
           w2[t] = E.g2[t] * exp(-2.302585 * E.tee[t] * x);
         }
-        alp[s] = 31.321 * E.zeff[s] * E.zeff[s] * x;
+        Dz[s] = 31.321 * E.zeff[s] * E.zeff[s] * x;
       } else if (ty == SNAPI_PF_IRWIN) {
         const double lnT = log(T);
         double sum = 0.0;
@@ -152,7 +152,7 @@ struct Chem {
         u = exp(sum);
       }
       Ut[s] = u;
-      eip[s] = exp(-E.eion[s] / kT);
+      cz[s] = fct * exp(-E.eion[s] / kT);
     }
     for (int m = 0; m < E.nmol; ++m) {
       double k = 0.0;
@@ -170,60 +170,78 @@ struct Chem {
     }
   }
 
-  // U and dU/U of stage s at electron density ne (pne = ne^(1/6))
+  // U of stage s and (kDeriv) dU / dNe; ine = 1/ne, pne = ne^(1/6), ipne = 1/pne
   template <bool kDeriv>
-  __device__ __forceinline__ void pfu(int s, double ne, double pne, double &U, double &dUoU) const {
-    double u = Ut[s], du = 0.0;
-    if (E.pft[s] == SNAPI_PF_TRAV) {
-      const double z = E.zeff[s], p = z * E.ftrav / pne, al = alp[s];
-      const int t0 = E.t0[s], t1 = E.t1[s];
-      for (int t = t0; t < t1; ++t) u += w2[t] * qas_f(E.tll[t], p, al);
-      // trav::dU keeps only the last term (partf.cc:247-248)
-      if (kDeriv && t1 > t0) du = -w2[t1 - 1] * dqas_f(E.tll[t1 - 1], p, al) * z * E.ftrav / (6.0 * ne * pne);
+  __device__ __forceinline__ void stage_u(int s, double ine, double pne, double ipne, double &U, double &dU) const {
+    U = Ut[s];
+    dU = 0.0;
+    if (E.pft[s] != SNAPI_PF_TRAV) return;
+    const int t0 = E.t0[s], t1 = E.t1[s];
+    const double zf = E.zf[s], p = zf * ipne, ip = pne * E.izf[s], dz = Dz[s];
+    double dq = 0.0;
+    for (int t = t0; t < t1; ++t) {
+      const double l = E.tll[t], il = E.til[t];
+      double q;
+      if (p > l) {
+        q = ((1.3333333 * p + 0.5) * p + 0.16666667 + 1.33333333 * dz) * p - 0.4 * dz * dz * ip -
+            (E.tA[t] - dz * (l - 1.0)) + 0.5 * dz * dz * il;
+        if (kDeriv) dq = ((3.0 * 1.3333333 * p + 1.0) * p + 0.16666667 + 1.33333333 * dz) + 0.4 * dz * dz * ip * ip;
+      } else {
+        const double axl2 = dz * il * il, k4 = (1.0 + axl2 * (0.33333333 + 0.1 * axl2)) * il;
+        q = k4 * p * p * p * p;
+        if (kDeriv) dq = 4.0 * k4 * p * p * p;
+      }
+      U += w2[t] * q;
     }
-    U = u;
-    dUoU = kDeriv ? du / u : 0.0;
+    if (kDeriv && t1 > t0) dU = -w2[t1 - 1] * dq * zf * ine * ipne * (1.0 / 6.0);
   }
 
-  // atom::ionfrc for atom a (0-based) at ne: Ea, Da and the kept fractions (atom.cc:892-925)
+  // atom a (0-based): Ea, and with kDeriv Da and the kept fractions
   template <bool kDeriv>
-  __device__ void sweep_atom(int a, double ne, double pne) {
+  __device__ __forceinline__ void sweep_atom(int a, double ine, double pne, double ipne) {
     const int s0 = E.s0[a], ns = E.ns[a];
-    double Up, dUp;
-    pfu<kDeriv>(s0, ne, pne, Up, dUp);
-    double fk = 1.0, df = 0.0, fsum = 1.0, dfsum = 0.0, S1 = 0.0, S2 = 0.0;
-    if (kDeriv && E.ref[s0] >= 0) { fr[E.ref[s0]] = 1.0; dr[E.ref[s0]] = 0.0; }
-    for (int z = 0; z + 1 < ns; ++z) {
-      double Un, dUn;
-      pfu<kDeriv>(s0 + z + 1, ne, pne, Un, dUn);
-      const double f = fct * (Un / Up) * eip[s0 + z] / ne;
+    double h = 1.0, fsum = 0.0, S1 = 0.0, dfsum = 0.0, S2 = 0.0, dl0 = 0.0;
+    for (int z = 0; z < ns; ++z) {
+      const int s = s0 + z;
+      double U, dU;
+      stage_u<kDeriv>(s, ine, pne, ipne, U, dU);
+      const double f = U * h;
+      fsum += f;
+      S1 += (double)z * f;
+      double df = 0.0;
       if (kDeriv) {
-        const double fd = f * ((dUn) - (dUp * ne + 1.0) / ne);
-        df = df * f + fk * fd;
+        if (z == 0) dl0 = dU / U;
+        else df = h * dU - f * (dl0 + (double)z * ine);
         dfsum += df;
-        S2 += (double)(z + 1) * df;
+        S2 += (double)z * df;
+        const int r = E.ref[s];
+        if (r >= 0) { fr[r] = f; dr[r] = df; }
       }
-      fk = fk * f;
-      fsum += fk;
-      S1 += (double)(z + 1) * fk;
-      if (kDeriv && E.ref[s0 + z + 1] >= 0) { fr[E.ref[s0 + z + 1]] = fk; dr[E.ref[s0 + z + 1]] = df; }
-      Up = Un;
-      dUp = dUn;
+      h *= cz[s] * ine;
     }
-    Ea[a + 1] = S1 / fsum;
+    const double inv = 1.0 / fsum;
+    Ea[a + 1] = S1 * inv;
     if (kDeriv) {
-      Da[a + 1] = (S2 - dfsum * S1 / fsum) / fsum;
+      Da[a + 1] = (S2 - dfsum * S1 * inv) * inv;
       for (int z = 0; z < ns; ++z) {
         const int r = E.ref[s0 + z];
-        if (r >= 0) { dr[r] = (dr[r] - dfsum * fr[r] / fsum) / fsum; fr[r] = fr[r] / fsum; }
+        if (r >= 0) { dr[r] = (dr[r] - dfsum * fr[r] * inv) * inv; fr[r] *= inv; }
       }
     }
   }
 
   template <bool kDeriv>
   __device__ void sweep(double ne) {
-    const double pne = pow(ne, 1.0 / 6.0);
-    for (int a = 0; a < E.natom; ++a) sweep_atom<kDeriv>(a, ne, pne);
+    const double ine = 1.0 / ne, pne = cbrt(sqrt(ne)), ipne = 1.0 / pne;
+    for (int a = 0; a < E.natom; ++a) sweep_atom<kDeriv>(a, ine, pne, ipne);
+  }
+
+  // U of stage s at the final Ne (atom::lte uses the partition function at T, Ne)
+  __device__ double stage_U(int s, double ne) const {
+    const double pne = cbrt(sqrt(ne));
+    double U, dU;
+    stage_u<false>(s, 1.0 / ne, pne, 1.0 / pne, U, dU);
+    return U;
   }
 
   // atmosphere::chemeq (atmos_chm.cc:28-330): N[0] = Ne, N[1..na] free atoms; the kept fractions
@@ -358,11 +376,9 @@ struct Chem {
   // stage total of stage s (with a kept fraction) after solve
   __device__ __forceinline__ double stage_total(int s, int a) const { return N[a + 1] * fr[E.ref[s]]; }
 
-  // LTE population of level slot l (atom::lte, atom.cc:779-787) at the final Ne (pne = Ne^(1/6))
-  __device__ double level_pop(int l, double pne) const {
+  // LTE population of level slot l (atom::lte, atom.cc:779-787), U = partition function at the final Ne
+  __device__ double level_pop(int l, double U) const {
     const int s = E.lst[l];
-    double U, dum;
-    pfu<false>(s, N[0], pne, U, dum);
     const double g = E.lg[l];
     return stage_total(s, E.satom[s]) * ((g != 0.0) ? g * exp(-E.lee[l] / (cK * T)) / U : 1.0);
   }
@@ -499,8 +515,7 @@ __device__ double continuum(const EosDev &E, const Chem &c, const double *lev, d
 __device__ double chem_point(const EosDev &E, Chem &c, double T, double Nt, double *lev, double &nH0, int which) {
   if (T != c.T) c.set_T(T);
   c.solve(Nt);
-  const double pne = pow(c.N[0], 1.0 / 6.0);
-  for (int l = 0; l < E.nlev; ++l) lev[l] = c.level_pop(l, pne);
+  for (int l = 0; l < E.nlev; ++l) lev[l] = c.level_pop(l, c.stage_U(E.lst[l], c.N[0]));
   nH0 = c.stage_total(E.s0[0], 0);
   return continuum(E, c, lev, nH0, which);
 }
@@ -787,6 +802,8 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
       H.pft[ns] = P.type;
       H.pfv[ns] = P.type == SNAPI_PF_CONST ? P.value : (P.type == SNAPI_PF_TRAV ? P.g0 : 1.0);
       H.zeff[ns] = P.zeff;
+      H.zf[ns] = P.zeff * H.ftrav;
+      H.izf[ns] = P.zeff != 0.0 ? 1.0 / H.zf[ns] : 0.0;
       H.eion[ns] = z + 1 < At.nstage ? At.ip[z] : 0.0;
       if (z + 1 < At.nstage && !std::isfinite(At.ip[z]))
         return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: atom %d stage %d: no ionisation energy", a, z);
@@ -796,9 +813,16 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
           return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: too many partition-function terms");
         H.t0[ns] = nt;
         for (int t = 0; t < P.nterm; ++t, ++nt) {
+          if (!(P.ll[t] > 0.0))
+            return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: atom %d stage %d: Traving term with l <= 0", a, z);
           H.g2[nt] = P.g2[t];
           H.tee[nt] = P.ee[t];
           H.tll[nt] = P.ll[t];
+          H.til[nt] = 1.0 / P.ll[t];
+          {
+            const double llm = P.ll[t] - 1.0;
+            H.tA[nt] = ((0.33333333 * llm - 0.5) * llm - 0.16666667) * llm;
+          }
           if (P.m[t] < 0 || P.m[t] > SNAPI_PF_MAX_COEF || nc + P.m[t] > kEC)
             return set_err(ctx, SNAPI_EINVAL, "snapi_eos_set: too many partition-function coefficients");
           H.c0[nt] = nc;
