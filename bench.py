@@ -323,6 +323,8 @@ def run_snapi(args):
         line["cpu_baseline"] = reference_cpu_rate(samples_per_core=1, mode=1)
     if rank == 0 and not args.no_extras:
         line["lm"] = bench_lm(sb, pool, ic, local)
+        line["node_build"] = bench_build(sb, pool, local)
+        line["lm_device_build"] = bench_lm_device(sb, pool, ic, local)
         line["ali"] = bench_ali(sb, local, cpu=not args.no_cpu_baseline)
     ctx.close()
     if world > 1:
@@ -364,6 +366,62 @@ def bench_lm(sb, pool, ic, device, npix=4096, iters=10):
             "median_iterations": float(np.median(res["iters"])),
             "note": "device work per step: synthesis at the trial nodes, Jacobian (2 npar solves) at accepted "
                     "nodes, FP64 J^T J and damped eigen-solve; node -> record map on the host"}
+
+
+def _eos_tables():
+    from snapi_b200.eos_tables import EosTables
+    return EosTables(dict(np.load(os.path.join(ROOT, "tests", "golden", "eos_c3.npz"))))
+
+
+def bench_build(sb, pool, device, ncol=4096):
+    """Node model -> column records on the GPU (snapi_build_records): hydrostatic equilibrium with
+    the chemistry per depth, the record set-up, and the node tangents (two builds per temperature
+    node, 9 builds per column for 4 temperature nodes), for the 32 seeded config-3 node vectors
+    tiled to ncol columns.  The reference's build_from_nodes time per column (compiled reference,
+    strict FP64, one core) is the fixture's."""
+    nodes = np.tile(pool["nodes"], (ncol // pool["nodes"].shape[0] + 1, 1))[:ncol]
+    ctx = sb.Context.from_fixture(pool, max_batch=4096, device=device)
+    ctx.eos_set(_eos_tables())
+    ctx.build_records(nodes[:64], tangents=True)  # warm-up
+    out = {}
+    for tang in (False, True):
+        t0 = time.perf_counter()
+        _, _, _, status = ctx.build_records(nodes, tangents=tang)
+        wall = time.perf_counter() - t0
+        key = "with_tangents" if tang else "records_only"
+        out[key] = {"device_ms": ctx.last_kernel_ms, "wall_ms": wall * 1e3,
+                    "columns_per_s": ncol / (ctx.last_kernel_ms / 1e3), "flagged": int((status != 0).sum())}
+    ctx.close()
+    ref_build = float(pool["ref_seconds_per_pixel"][0])
+    out["columns"] = ncol
+    out["reference_build_s_per_column_one_core"] = ref_build
+    out["reference_columns_per_s_one_core_with_tangents"] = 1.0 / (ref_build * 9)
+    out["note"] = ("flagged: columns where a hydrostatic step reached the reference's own 20-pass cap "
+                   "(status 2, the reference continues the same way)")
+    return out
+
+
+def bench_lm_device(sb, pool, ic, device, npix=1024, iters=10):
+    """The whole stokes_lm_fit on the GPU (snapi_lm_fit): every step builds records and tangents of
+    the requested nodes on the device and takes one LM iteration; npix pixels, 10 nodes, iters
+    iterations from offset starting nodes against noisy targets synthesised from the pool's nodes."""
+    nodes = np.tile(pool["nodes"], (npix // pool["nodes"].shape[0] + 1, 1))[:npix]
+    ctx = sb.Context.from_fixture(pool, stokes_scale=ic, max_batch=4096, device=device)
+    ctx.eos_set(_eos_tables())
+    rec, _, _, _ = ctx.build_records(nodes, tangents=False)
+    obs = ctx.synth(rec)
+    obs += np.random.default_rng(13).normal(0.0, 1e-3 * ic, obs.shape).astype(np.float32)
+    kinds = pool["node_kind"].astype(int)
+    scale = np.array([{1: 5000.0, 2: 1e5, 3: 1e5, 4: 1000.0}.get(k, 1.0) for k in kinds])
+    n0 = nodes + np.array([200.0, 200.0, 200.0, 200.0, 3e4, 3e4, 3e4, 200.0, 0.1, 0.1])
+    t0 = time.perf_counter()
+    res = ctx.lm_fit_device(n0, obs, kinds, 1e-2 * scale, lm_start=1e3, max_iter=iters, delta=1e-4)
+    wall = time.perf_counter() - t0
+    dev = ctx.last_kernel_ms
+    ctx.close()
+    return {"pixels": npix, "iterations": iters, "steps": res["steps"], "device_s": dev / 1e3, "wall_s": wall,
+            "device_ms_per_step": dev / res["steps"], "pixel_steps_per_s": npix * res["steps"] / (dev / 1e3),
+            "median_iterations": float(np.median(res["iters"]))}
 
 
 def bench_ali(sb, device, ncol=1024, cpu=True):
