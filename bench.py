@@ -572,9 +572,18 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--pixels", type=int, default=NPIX, help="pixels per GPU (smaller cases for profiling)")
     ap.add_argument("--no-extras", action="store_true", help="skip the LM and NLTE measurements")
+    ap.add_argument("--node-build-only", type=int, default=0, metavar="N",
+                    help="only measure the node -> record build of N columns (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.node_build_only:
+        sys.path.insert(0, ROOT)
+        import snapi_b200 as sb
+        from snapi_b200 import build as b
+        b.build_cuda()
+        print(json.dumps({"node_build": bench_build(sb, dict(np.load(POOL)), 0, ncol=args.node_build_only)}), flush=True)
+        return
     line = run_reference(args) if args.impl == "reference" else run_snapi(args)
     if line is not None:
         print(json.dumps(line), flush=True)
