@@ -574,6 +574,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the LM and NLTE measurements")
     ap.add_argument("--node-build-only", type=int, default=0, metavar="N",
                     help="only measure the node -> record build of N columns (profiling)")
+    ap.add_argument("--lm-fit-only", type=int, default=0, metavar="N",
+                    help="only measure the whole LM on the device (snapi_lm_fit) for N pixels, 30 iterations")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -583,6 +585,16 @@ def main():
         from snapi_b200 import build as b
         b.build_cuda()
         print(json.dumps({"node_build": bench_build(sb, dict(np.load(POOL)), 0, ncol=args.node_build_only)}), flush=True)
+        return
+    if args.lm_fit_only:
+        sys.path.insert(0, ROOT)
+        import snapi_b200 as sb
+        from snapi_b200 import build as b
+        b.build_cuda()
+        pool = dict(np.load(POOL))
+        ic = float(pool["stokes"][:, :, 0].max())
+        print(json.dumps({"lm_device_build": bench_lm_device(sb, pool, ic, 0, npix=args.lm_fit_only, iters=30)}),
+              flush=True)
         return
     line = run_reference(args) if args.impl == "reference" else run_snapi(args)
     if line is not None:

@@ -698,7 +698,14 @@ int sne_tangents(const snapi_eos_model *m, int nd, int nlines, const double *lam
       for (int x = 0; x < nd; ++x) record_depth(m, nlines, lam0, mass, c, x, r + (size_t)x * nf, &c->status);
       status |= c->status;
     }
-    for (int i = 0; i < nd * nf; ++i) tan[(size_t)p * nd * nf + i] = (rp[i] - rm[i]) / st;
+    for (int i = 0; i < nd * nf; ++i) {
+      /* a kinematic / field node moves only its own fields (v_turb 1, v_los 3, the field 4-6); the
+         others are unchanged (their difference is 0, or NaN - NaN where B = 0 without B nodes) */
+      const int f = i % nf;
+      const int kin = (f == 1 || (f >= 3 && f <= 6));
+      const int own = kind == 2 ? f == 1 : (kind == 3 ? f == 3 : (f >= 4 && f <= 6));
+      tan[(size_t)p * nd * nf + i] = (kind != 1 && kin && !own) ? 0.0 : (rp[i] - rm[i]) / st;
+    }
   }
   return status;
 }

@@ -95,6 +95,7 @@ struct EosDev {
       lsig[SNAPI_MAX_LINES], llam0[SNAPI_MAX_LINES], lmass[SNAPI_MAX_LINES];
   // nodes (kinds contiguous and non-decreasing)
   double ntau[kEP];
+  int nkind[kEP];
   int kfirst[7], kcount[7];
 };
 
@@ -696,9 +697,12 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_rec(EosArgs A) {
         NodeView np{nodes, q, 0.5 * stp}, nm{nodes, q, -0.5 * stp};
         field_fields(E, np, x, false, fp);
         field_fields(E, nm, x, false, fm);
+        // a kinematic / field node moves only its own fields (v_turb 1, v_los 3, the field 4-6);
+        // the reference's differences of the others are 0, or NaN - NaN where B = 0 without B nodes
+        const int kind = E.nkind[q];
         for (int f = 0; f < nf; ++f) {
-          const bool fl = (f == 1 || (f >= 3 && f <= 6));
-          tq[f] = fl ? (float)((fp[f] - fm[f]) / stp) : 0.f;
+          const bool own = kind == 2 ? f == 1 : (kind == 3 ? f == 3 : (f >= 4 && f <= 6));
+          tq[f] = own ? (float)((fp[f] - fm[f]) / stp) : 0.f;
         }
       }
     }
@@ -961,6 +965,7 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
     H.kcount[k] += 1;
     prev = k;
     H.ntau[q] = m->node_tau[q];
+    H.nkind[q] = k;
   }
   for (int k = 1; k <= 6; ++k)
     for (int i = 1; i < H.kcount[k]; ++i)

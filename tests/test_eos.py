@@ -174,3 +174,83 @@ def test_gpu_active_rows_untouched_and_batches(oracle_lib, eos3, config3):
         np.testing.assert_array_equal(rec[p], rec[p % 8] if active[p % 8] else rec[p])
     np.testing.assert_allclose(rec[8], config3["record"][0], rtol=3e-7)
     ctx.close()
+
+
+def _variant_tables(eos3):
+    """The config-3 tables with paths the Fe I 6300 set does not use: aluminium's neutral stage
+    with an Irwin partition function (ln U = sum a_i (ln T)^i, U ~ 2.7 at 5000 K), the CO molecule
+    with a constant equilibrium constant."""
+    d = {k: np.array(v) for k, v in eos3.items()}
+    al = 7  # atoms_6300.cfg order: H He C N O Ca Si Al Fe
+    d["pf_type"][al, 0] = 3
+    d["pf_ncoef"][al, 0] = 3
+    d["pf_coef"][al, 0, :3] = [-2.0, 0.35, 0.0]
+    d["pf_nterm"][al, 0] = 0
+    co = 6  # mol.cfg order: H- H2+ H2 H2O OH CH CO ...
+    d["mol_i"][co, 9] = 1
+    d["mol_i"][co, 10] = 1
+    d["mol_coef"][co, 0] = 121.1  # its polynomial's value at 5000 K
+    return d
+
+
+def _fieldless_tables(eos3):
+    """The config-3 tables with a node model of temperature and velocities only (no B, inclination,
+    azimuth nodes: the reference's build then puts B = 1e-3 G at angles 1e-3 rad)."""
+    d = {k: np.array(v) for k, v in eos3.items()}
+    keep = d["node_kind"] <= 3
+    d["node_kind"] = d["node_kind"][keep]
+    d["node_tau"] = d["node_tau"][keep]
+    d["meta"] = d["meta"].copy()
+    d["meta"][3] = keep.sum()
+    return d, keep
+
+
+@pytest.mark.gpu
+@pytestmark_gpu
+def test_gpu_irwin_and_constant_equilibrium_vs_oracle(oracle_lib, eos3, config3):
+    import eos_oracle as eo
+    import snapi_b200 as sb
+    from snapi_b200.eos_tables import EosTables
+    d = _variant_tables(eos3)
+    t = EosTables(d)
+    ctx = sb.Context.from_fixture(config3)
+    ctx.eos_set(EosTables(d))
+    nodes = config3["nodes"][:4]
+    rec, tan, _, status = ctx.build_records(nodes, tangents=True)
+    assert np.all(status == 0)
+    lam0, mass = _line_const(config3)
+    base = EosTables(eos3)
+    for p in range(nodes.shape[0]):
+        _, _, ro, st = eo.build(t, lam0, mass, nodes[p])
+        assert st == 0
+        np.testing.assert_allclose(rec[p], ro, rtol=3e-7, atol=0)
+        _, _, r0, _ = eo.build(base, lam0, mass, nodes[p])
+        assert np.abs(ro[:, 2] / r0[:, 2] - 1).max() > 1e-6  # the variant tables do change n_e
+        to, _ = eo.tangents(t, lam0, mass, nodes[p])
+        scale = np.maximum(np.abs(to).max(axis=1, keepdims=True), 1e-6 * np.abs(ro).max(axis=0))
+        assert (np.abs(tan[p] - to) / scale).max() < 2e-5
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytestmark_gpu
+def test_gpu_model_without_field_nodes_vs_oracle(oracle_lib, eos3, config3):
+    import eos_oracle as eo
+    import snapi_b200 as sb
+    from snapi_b200.eos_tables import EosTables
+    d, keep = _fieldless_tables(eos3)
+    t = EosTables(d)
+    ctx = sb.Context.from_fixture(config3)
+    ctx.eos_set(EosTables(d))
+    nodes = np.ascontiguousarray(config3["nodes"][:3][:, keep])
+    rec, tan, _, status = ctx.build_records(nodes, tangents=True)
+    assert np.all(status == 0)
+    lam0, mass = _line_const(config3)
+    for p in range(nodes.shape[0]):
+        _, _, ro, st = eo.build(t, lam0, mass, nodes[p])
+        np.testing.assert_allclose(rec[p], ro, rtol=3e-7, atol=1e-30)
+        assert abs(ro[0, 4] - 1e-3) < 1e-12  # |B| = TINY
+        to, _ = eo.tangents(t, lam0, mass, nodes[p])
+        scale = np.maximum(np.abs(to).max(axis=1, keepdims=True), 1e-6 * np.abs(ro).max(axis=0))
+        assert (np.abs(tan[p] - to) / np.maximum(scale, 1e-30)).max() < 2e-5
+    ctx.close()
