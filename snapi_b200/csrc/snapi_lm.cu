@@ -304,6 +304,61 @@ void free_bufs(LmWork *w) {
 
 }  // namespace
 
+namespace {
+
+// one LM iteration in two phases (snapi_lm_step runs both; snapi_lm_fit builds the tangents between
+// them for the pixels the first phase accepted):
+// 1) synthesis at the requested nodes and the accept / reject decision; skip_resp[p] == 0 marks
+//    the pixels whose Jacobian (and hence node tangents) the second phase needs
+cudaError_t lm_eval_phase(snapi_ctx *ctx, LmWork *w, const float *rec) {
+  KParams P = base_params(ctx);
+  P.npix = w->npix;
+  P.rec = rec;
+  P.stokes = w->d_snew;
+  P.skip = w->d_skip_syn;
+  cudaError_t e = launch_synth(ctx, P);
+  if (e != cudaSuccess) return e;
+  if (w->broaden > 0.0 && (e = psf_launch(ctx, w->d_snew, w->npix, 1, w->d_skip_syn)) != cudaSuccess) return e;
+  k_lm_eval<<<w->npix, kLmThreads, 0, ctx->stream>>>(w->D);
+  return cudaGetLastError();
+}
+
+// 2) Jacobian at the accepted nodes along the tangents, normal equations, damped solve, next request
+cudaError_t lm_solve_phase(snapi_ctx *ctx, LmWork *w, const float *rec, const float *tan, int &launches) {
+  const int npix = w->npix, npar = w->npar;
+  KParams R = base_params(ctx);
+  R.npix = npix;
+  R.npar = npar;
+  R.nvar = npar;
+  R.rec = rec;
+  R.tangent = tan;
+  R.fd_step = w->d_step;
+  R.dstokes = w->d_J;
+  R.skip = w->d_skip_resp;
+  cudaError_t e = launch_responses(ctx, R);
+  if (e != cudaSuccess) return e;
+  if (w->broaden > 0.0 && (e = psf_launch(ctx, w->d_J, npix * npar, npar, w->d_skip_resp)) != cudaSuccess) return e;
+  LmDev Ds = w->D;
+  launches = 2;
+  if (w->d_G && npar + 1 <= 16) {
+    k_lm_rows<<<npix * 16, 256, 0, ctx->stream>>>(Ds, w->d_M);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_gram_tf32(w->d_M, npix, ctx->nl * 4, w->d_G, ctx->d_status, ctx->stream)) != cudaSuccess) return e;
+    Ds.G = w->d_G;
+    launches += 2;
+  }
+  k_lm_solve<<<npix, kLmThreads, 0, ctx->stream>>>(Ds);
+  return cudaGetLastError();
+}
+
+// need[p] = 1 where the Jacobian is needed (skip_resp[p] == 0)
+__global__ void k_lm_need(const int *skip_resp, int *need, int npix) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < npix) need[p] = skip_resp[p] ? 0 : 1;
+}
+
+}  // namespace
+
 void snapi::lm_free(snapi_ctx *ctx) {
   if (!ctx || !ctx->lm) return;
   free_bufs(work(ctx));
@@ -447,37 +502,11 @@ int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, d
     tan = w->d_tan;
   }
   SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  KParams P = base_params(ctx);
-  P.npix = npix;
-  P.rec = rec;
-  P.stokes = w->d_snew;
-  P.skip = w->d_skip_syn;
-  SNAPI_CK(launch_synth(ctx, P));
-  if (w->broaden > 0.0) SNAPI_CK(psf_launch(ctx, w->d_snew, npix, 1, w->d_skip_syn));
-  k_lm_eval<<<npix, kLmThreads, 0, ctx->stream>>>(w->D);
-  SNAPI_CK(cudaGetLastError());
-  KParams R = base_params(ctx);
-  R.npix = npix;
-  R.npar = npar;
-  R.nvar = npar;
-  R.rec = rec;
-  R.tangent = tan;
-  R.fd_step = w->d_step;
-  R.dstokes = w->d_J;
-  R.skip = w->d_skip_resp;
-  SNAPI_CK(launch_responses(ctx, R));
-  if (w->broaden > 0.0) SNAPI_CK(psf_launch(ctx, w->d_J, npix * npar, npar, w->d_skip_resp));
-  LmDev Ds = w->D;
-  if (w->d_G && npar + 1 <= 16) {
-    k_lm_rows<<<npix * 16, 256, 0, ctx->stream>>>(Ds, w->d_M);
-    SNAPI_CK(cudaGetLastError());
-    SNAPI_CK(launch_gram_tf32(w->d_M, npix, ctx->nl * 4, w->d_G, ctx->d_status, ctx->stream));
-    Ds.G = w->d_G;
-  }
-  k_lm_solve<<<npix, kLmThreads, 0, ctx->stream>>>(Ds);
-  SNAPI_CK(cudaGetLastError());
+  SNAPI_CK(lm_eval_phase(ctx, w, rec));
+  int nl_solve = 0;
+  SNAPI_CK(lm_solve_phase(ctx, w, rec, tan, nl_solve));
   SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-  ctx->last_launches = Ds.G ? 6 : 4;
+  ctx->last_launches = 2 + nl_solve;
   SNAPI_CK(cudaMemcpyAsync(w->h_active.data(), w->d_active, sizeof(int) * npix, cudaMemcpyDeviceToHost, ctx->stream));
   if (dev) {
     SNAPI_CK(cudaMemcpyAsync(request, w->d_req, sizeof(double) * npix * npar, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -558,17 +587,47 @@ int snapi_lm_fit(snapi_ctx *ctx, int npix, const snapi_lm_opts *opts, const doub
   double ms = 0.0;
   int launches = 0, steps = 0;
   const int cap = 10 * opts->max_iter + 10;  // accepted + rejected steps of any pixel stay below this
+  auto timed = [&](auto &&fn) -> int {  // device time of a stretch of launches on the context stream
+    SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    SNAPI_CK(fn());
+    SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    SNAPI_CK(cudaEventSynchronize(ctx->ev1));
+    float t = 0.f;
+    SNAPI_CK(cudaEventElapsedTime(&t, ctx->ev0, ctx->ev1));
+    ms += t;
+    return SNAPI_OK;
+  };
   for (;;) {
-    st = snapi_build_records(ctx, npix, w->d_req, w->d_active, w->d_rec, nullptr, w->d_tan, nullptr, nullptr,
+    // records of the requested nodes of the active pixels; synthesis and accept / reject
+    st = snapi_build_records(ctx, npix, w->d_req, w->d_active, w->d_rec, nullptr, nullptr, nullptr, nullptr,
                              SNAPI_MEM_DEVICE);
     if (st) return st;
     ms += ctx->last_ms;
     launches += ctx->last_launches;
-    int na = 0;
-    st = snapi_lm_step(ctx, w->d_rec, w->d_tan, w->d_req_out, w->d_act_out, &na, SNAPI_MEM_DEVICE);
+    st = timed([&] {
+      cudaError_t e = lm_eval_phase(ctx, w, w->d_rec);
+      if (e != cudaSuccess) return e;
+      k_lm_need<<<(npix + 255) / 256, 256, 0, ctx->stream>>>(w->d_skip_resp, w->d_act_out, npix);
+      return cudaGetLastError();
+    });
+    if (st) return st;
+    launches += 3 + (w->broaden > 0.0 ? 1 : 0);
+    // node tangents only where the step was accepted (the Jacobian is taken there), as the
+    // reference computes responses only at accepted models
+    st = snapi_build_records(ctx, npix, w->d_req, w->d_act_out, w->d_rec, nullptr, w->d_tan, nullptr, nullptr,
+                             SNAPI_MEM_DEVICE);
     if (st) return st;
     ms += ctx->last_ms;
     launches += ctx->last_launches;
+    int nls = 0;
+    st = timed([&] { return lm_solve_phase(ctx, w, w->d_rec, w->d_tan, nls); });
+    if (st) return st;
+    launches += nls + (w->broaden > 0.0 ? 1 : 0);
+    SNAPI_CK(cudaMemcpy(w->h_active.data(), w->d_active, sizeof(int) * npix, cudaMemcpyDeviceToHost));
+    st = check_status(ctx);
+    if (st) return st;
+    int na = 0;
+    for (int p = 0; p < npix; ++p) na += w->h_active[p] ? 1 : 0;
     ++steps;
     if (na == 0) break;
     if (steps >= cap) return set_err(ctx, SNAPI_ENONCONV, "snapi_lm_fit: %d pixels still active after %d steps", na, steps);
