@@ -516,10 +516,9 @@ void snapi_destroy(snapi_ctx *ctx) {
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
-  for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < snapi_ctx::kStageChunks; ++h)
     if (ctx->ev_copy[h]) cudaEventDestroy(ctx->ev_copy[h]);
-    if (ctx->ev_free[h]) cudaEventDestroy(ctx->ev_free[h]);
-  }
+  if (ctx->ev_free) cudaEventDestroy(ctx->ev_free);
   delete ctx;
 }
 
@@ -618,10 +617,9 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
   } while (0)
   CKC(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   CKC(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
-  for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < snapi_ctx::kStageChunks; ++h)
     CKC(cudaEventCreateWithFlags(&ctx->ev_copy[h], cudaEventDisableTiming));
-    CKC(cudaEventCreateWithFlags(&ctx->ev_free[h], cudaEventDisableTiming));
-  }
+  CKC(cudaEventCreateWithFlags(&ctx->ev_free, cudaEventDisableTiming));
   CKC(cudaEventCreate(&ctx->ev0));
   CKC(cudaEventCreate(&ctx->ev1));
   CKC(cudaMalloc(&ctx->d_lamvac, sizeof(double) * ctx->nl));
@@ -714,18 +712,32 @@ int adjoint_impl(snapi_ctx *ctx, int npix, const float *records, const float *ob
   ctx->last_ms = 0.0;
   ctx->last_launches = 0;
   const bool dev = mem == SNAPI_MEM_DEVICE;
-  // Host inputs: each round of up to max_batch pixels goes in chunks that alternate between the
-  // two halves of the staging buffers; chunk k+1 is copied on the copy stream while chunk k
-  // computes, so the host->device traffic (the tangents dominate it) hides under the kernels.
-  // Outputs of a round come back after its last chunk.  (Overlap needs page-locked host inputs,
-  // e.g. from snapi_host_alloc; pageable copies serialise with the host thread.)
-  const int half = std::max(1, ctx->max_batch / 2);
-  const int chunk = dev ? ctx->max_batch : std::min(half, std::max(1, (std::min(npix, ctx->max_batch) + 3) / 4));
+  // Host inputs: each round of up to max_batch pixels goes in chunks whose sizes grow sixfold from
+  // ~1/16 of the round, each in its own region of the staging buffers; chunk k+1 is uploaded on the
+  // copy stream while chunk k computes.  An upload costs ~0.9 us per pixel (44 KB with packed
+  // tangents) against ~5.6 us of compute, so only the first, small chunk's upload is exposed, and the
+  // round still runs as a few large launches (rounds of 1024 pixels cost 14 % more device time than
+  // one of 4096).  Outputs of a round come back after its last chunk.  (Overlap needs page-locked
+  // host inputs, e.g. from snapi_host_alloc; pageable copies serialise with the host thread.)
   int k = 0;
   for (int r0 = 0; r0 < npix; r0 += ctx->max_batch) {
     const int nr = std::min(ctx->max_batch, npix - r0);
-    for (int p0 = r0; p0 < r0 + nr; p0 += chunk, ++k) {
-      const int nb = std::min(chunk, r0 + nr - p0), lo = p0 - r0;  // lo: offset within the round
+    int csz[snapi_ctx::kStageChunks], nch = 0;
+    if (dev) {
+      csz[nch++] = nr;
+    } else {
+      int c = std::max(1, (nr + 15) / 16), left = nr;
+      while (left > 0) {
+        const int take = (nch == snapi_ctx::kStageChunks - 1) ? left : std::min(c, left);
+        csz[nch++] = take;
+        left -= take;
+        c *= 6;
+      }
+      if (r0 > 0) SNAPI_CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free, 0));  // previous round done
+    }
+    int lo = 0;  // offset of the chunk within the round
+    for (int ci = 0; ci < nch; ++ci, ++k) {
+      const int nb = csz[ci], p0 = r0 + lo;
       KParams P = base_params(ctx);
       P.npix = nb;
       P.npar = npar;
@@ -733,18 +745,16 @@ int adjoint_impl(snapi_ctx *ctx, int npix, const float *records, const float *ob
       P.tcol_off = ntcol ? ctx->d_tcol : nullptr;
       P.tcol_field = ntcol ? ctx->d_tcol + npar + 1 : nullptr;
       for (int s = 0; s < 4; ++s) P.ws[s] = w_stokes ? w_stokes[s] : 1.0;
-      const int h = ctx->max_batch >= 2 ? (k & 1) : 0;  // one pixel of staging: no second half
       if (dev) {
         P.rec = records + p0 * nrec;
         P.obs = obs + (size_t)p0 * nl4;
         P.mask = mask ? mask + (size_t)p0 * ctx->nl : nullptr;
         P.tangent = npar ? tangents + (size_t)p0 * ntan : nullptr;
       } else {
-        const size_t off = (size_t)h * half;
+        const size_t off = (size_t)lo;
         float *drec = ctx->d_rec + off * nrec, *dobs = ctx->d_obs + off * nl4, *dmask = ctx->d_mask + off * ctx->nl;
         float *dtan = ctx->d_tan + off * (ntan ? ntan : nrec);
         cudaStream_t cs = ctx->copy_stream;
-        SNAPI_CK(cudaStreamWaitEvent(cs, ctx->ev_free[h], 0));  // chunk k-2 is done with this half
         SNAPI_CK(cudaMemcpyAsync(drec, records + p0 * nrec, sizeof(float) * nb * nrec, cudaMemcpyHostToDevice, cs));
         SNAPI_CK(cudaMemcpyAsync(dobs, obs + (size_t)p0 * nl4, sizeof(float) * nb * nl4, cudaMemcpyHostToDevice, cs));
         if (mask)
@@ -753,8 +763,8 @@ int adjoint_impl(snapi_ctx *ctx, int npix, const float *records, const float *ob
         if (npar)
           SNAPI_CK(cudaMemcpyAsync(dtan, tangents + (size_t)p0 * ntan, sizeof(float) * nb * ntan,
                                    cudaMemcpyHostToDevice, cs));
-        SNAPI_CK(cudaEventRecord(ctx->ev_copy[h], cs));
-        SNAPI_CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_copy[h], 0));
+        SNAPI_CK(cudaEventRecord(ctx->ev_copy[ci], cs));
+        SNAPI_CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_copy[ci], 0));
         P.rec = drec; P.obs = dobs; P.mask = mask ? dmask : nullptr; P.tangent = npar ? dtan : nullptr;
       }
       P.stokes = stokes ? (dev ? stokes + (size_t)p0 * nl4 : ctx->d_stokes + (size_t)lo * nl4) : nullptr;
@@ -765,9 +775,10 @@ int adjoint_impl(snapi_ctx *ctx, int npix, const float *records, const float *ob
       launch_adjoint(P, nb, ctx->nchunk, Lsw.total, Lfin.total, ctx->stream);
       SNAPI_CK(cudaGetLastError());
       ctx->last_launches += kAdjointLaunches;
-      if (!dev) SNAPI_CK(cudaEventRecord(ctx->ev_free[h], ctx->stream));
+      lo += nb;
     }
     if (!dev) {
+      SNAPI_CK(cudaEventRecord(ctx->ev_free, ctx->stream));
       if (stokes)
         SNAPI_CK(cudaMemcpyAsync(stokes + (size_t)r0 * nl4, ctx->d_stokes, sizeof(float) * nr * nl4,
                                  cudaMemcpyDeviceToHost, ctx->stream));

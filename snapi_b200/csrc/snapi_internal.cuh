@@ -296,7 +296,8 @@ struct snapi_ctx {
   int device = 0;
   cudaStream_t stream = nullptr, copy_stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  cudaEvent_t ev_copy[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};  // staging halves
+  static constexpr int kStageChunks = 8;  // host-input chunks per round (adjoint_impl)
+  cudaEvent_t ev_copy[kStageChunks] = {}, ev_free = nullptr;  // chunk uploaded / round's kernels done
   int nd = 0, nl = 0, nlines = 0, nfield = 0, ncomp = 0, nred = 0, lpad = 0, nchunk = 0, nwslot = 0, max_batch = 0;
   float lam_mid = 0.f;
   double scale2 = 1.0;
