@@ -382,7 +382,7 @@ def bench_build(sb, pool, device, ncol=4096):
     nodes = np.tile(pool["nodes"], (ncol // pool["nodes"].shape[0] + 1, 1))[:ncol]
     ctx = sb.Context.from_fixture(pool, max_batch=4096, device=device)
     ctx.eos_set(_eos_tables())
-    ctx.build_records(nodes[:64], tangents=True)  # warm-up
+    ctx.build_records(nodes, tangents=True)  # warm-up (allocates the work buffers)
     out = {}
     for tang in (False, True):
         t0 = time.perf_counter()

@@ -13,9 +13,10 @@
 //              Variant 0 is the node vector itself, variants 2i+1 / 2i+2 move temperature node i
 //              by +- step / 2.  Threads are ordered pixel-fastest, so a warp holds 32 pixels of the
 //              same variant at the same depth: similar (T, Nt), similar iteration counts.
-//   k_eos_rec  one thread per (depth, pixel): the chemistry at the final (T, Nt) of every variant,
-//              the record fields, and the tangent rows (thermal nodes from the variants,
-//              kinematic / field nodes by re-interpolation).
+//   k_eos_var  one thread per (pixel, variant, depth): the chemistry at the final (T, Nt) and the
+//              thermal record fields, FP64 (a tangent is a 5 K difference of them).
+//   k_eos_rec  one thread per (depth, pixel): the records, and the tangent rows (thermal nodes from
+//              the variants, kinematic / field nodes by re-interpolation).
 //
 // The chemistry (atmosphere::chemeq, atmos/atmos_chm.cc:28-330) is evaluated per call in the
 // reference's steps, with what depends on T alone hoisted out of the ~20 ionisation sweeps of a
@@ -532,6 +533,7 @@ struct EosArgs {
   float *rec;             // [npix][nd][nf]
   float *tan;             // [npix][npar][nd][nf] or null
   double *Nt_out;         // [npix][nd] or null
+  double *F;              // [npix][nvar][nd][nf]: thermal fields of every variant (FP64)
   int *status;            // [npix]
 };
 
@@ -657,6 +659,28 @@ __device__ void field_fields(const EosDev &E, const NodeView &nv, int x, bool bu
   f[6] = atan(nBy / nBx) * 180.0 / cPI;
 }
 
+// thermal fields of every (pixel, variant, depth), one thread each (pixel fastest: a warp holds 32
+// pixels of one variant at one depth), FP64 into F [npix][nvar][nd][nf]
+__global__ void __launch_bounds__(kRecThreads) k_eos_var(EosArgs A) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)A.npix * A.nvar * A.nd) return;
+  const int p = (int)(i % A.npix);
+  const long long r = i / A.npix;
+  const int v = (int)(r % A.nvar), x = (int)(r / A.nvar);
+  if (A.active && !A.active[p]) return;
+  const EosDev &E = *A.tab;
+  Chem c(E);
+  int st = 0;
+  double f[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES];
+  const size_t cv = ((size_t)p * A.nvar + v) * A.nd + x;
+  thermal_fields(E, c, A.T[cv], A.Nt[cv], f, st);
+  double *o = A.F + cv * A.nf;
+  for (int k = 0; k < A.nf; ++k) o[k] = (k == 1 || (k >= 3 && k <= 6)) ? 0.0 : f[k];
+  if (st) atomicOr(A.status + p, st);
+}
+
+// records and tangent rows per (depth, pixel): thermal fields from F, kinematic / field fields by
+// (re-)interpolation
 __global__ void __launch_bounds__(kRecThreads) k_eos_rec(EosArgs A) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.npix * A.nd) return;
@@ -665,12 +689,10 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_rec(EosArgs A) {
   const EosDev &E = *A.tab;
   const int nf = A.nf;
   const double *nodes = A.nodes + (size_t)p * A.npar;
-  Chem c(E);
   int st = 0;
   double r0[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES];
-  const double *Tv = A.T + (size_t)p * A.nvar * A.nd;
-  const double *Nv = A.Nt + (size_t)p * A.nvar * A.nd;
-  thermal_fields(E, c, Tv[x], Nv[x], r0, st);
+  const double *F0 = A.F + ((size_t)p * A.nvar * A.nd + x) * nf;  // variant 0
+  for (int f = 0; f < nf; ++f) r0[f] = F0[f];
   NodeView nv0{nodes, -1, 0.0};
   field_fields(E, nv0, x, true, r0);
   float *rp = A.rec + ((size_t)p * A.nd + x) * nf;
@@ -679,7 +701,7 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_rec(EosArgs A) {
     rp[f] = (float)r0[f];
     finite &= isfinite(r0[f]);
   }
-  if (A.Nt_out) A.Nt_out[(size_t)p * A.nd + x] = Nv[x];
+  if (A.Nt_out) A.Nt_out[(size_t)p * A.nd + x] = A.Nt[(size_t)p * A.nvar * A.nd + x];
   if (A.tan) {
     double fp[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES], fm[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES];
     for (int q = 0; q < A.npar; ++q) {
@@ -687,11 +709,11 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_rec(EosArgs A) {
       const double stp = A.step[q];
       if (q >= E.kfirst[1] && q < E.kfirst[1] + E.kcount[1]) {
         const int v = 1 + 2 * (q - E.kfirst[1]);
-        thermal_fields(E, c, Tv[(size_t)v * A.nd + x], Nv[(size_t)v * A.nd + x], fp, st);
-        thermal_fields(E, c, Tv[(size_t)(v + 1) * A.nd + x], Nv[(size_t)(v + 1) * A.nd + x], fm, st);
+        const double *Fp = A.F + (((size_t)p * A.nvar + v) * A.nd + x) * nf;
+        const double *Fm = A.F + (((size_t)p * A.nvar + v + 1) * A.nd + x) * nf;
         for (int f = 0; f < nf; ++f) {
           const bool th = !(f == 1 || (f >= 3 && f <= 6));
-          tq[f] = th ? (float)((fp[f] - fm[f]) / stp) : 0.f;
+          tq[f] = th ? (float)((Fp[f] - Fm[f]) / stp) : 0.f;
         }
       } else {
         NodeView np{nodes, q, 0.5 * stp}, nm{nodes, q, -0.5 * stp};
@@ -720,14 +742,16 @@ struct EosCtx {
   // work buffers for cap pixels
   int cap = 0, cap_var = 0;
   double *d_T = nullptr, *d_Nt = nullptr, *d_nodes = nullptr, *d_step = nullptr, *d_Ntout = nullptr;
+  double *d_F = nullptr;
   int *d_active = nullptr, *d_status = nullptr;
   float *d_rec = nullptr, *d_tan = nullptr;
 };
 
 void eos_free_bufs(EosCtx *e) {
-  void *b[] = {e->d_T, e->d_Nt, e->d_nodes, e->d_step, e->d_Ntout, e->d_active, e->d_status, e->d_rec, e->d_tan};
+  void *b[] = {e->d_T, e->d_Nt, e->d_nodes, e->d_step, e->d_Ntout, e->d_active, e->d_status, e->d_rec, e->d_tan,
+               e->d_F};
   for (void *p : b) cudaFree(p);
-  e->d_T = e->d_Nt = e->d_nodes = e->d_step = e->d_Ntout = nullptr;
+  e->d_T = e->d_Nt = e->d_nodes = e->d_step = e->d_Ntout = e->d_F = nullptr;
   e->d_active = e->d_status = nullptr;
   e->d_rec = e->d_tan = nullptr;
   e->cap = e->cap_var = 0;
@@ -1017,6 +1041,7 @@ int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int
     eos_free_bufs(e);
     const size_t Bz = (size_t)B;
     SNAPI_CK(cudaMalloc(&e->d_T, sizeof(double) * Bz * nvar * nd));
+    SNAPI_CK(cudaMalloc(&e->d_F, sizeof(double) * Bz * nvar * nd * nf));
     SNAPI_CK(cudaMalloc(&e->d_Nt, sizeof(double) * Bz * nvar * nd));
     SNAPI_CK(cudaMalloc(&e->d_nodes, sizeof(double) * Bz * npar));
     SNAPI_CK(cudaMalloc(&e->d_step, sizeof(double) * SNAPI_EOS_MAX_PAR));
@@ -1044,6 +1069,7 @@ int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int
     A.step = e->d_step;
     A.T = e->d_T;
     A.Nt = e->d_Nt;
+    A.F = e->d_F;
     A.status = e->d_status;
     if (host) {
       SNAPI_CK(cudaMemcpyAsync(e->d_nodes, nodes + (size_t)p0 * npar, sizeof(double) * nb * npar,
@@ -1077,11 +1103,14 @@ int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int
     const int nhe = nb * nvar;
     k_eos_he<<<(nhe + kHeThreads - 1) / kHeThreads, kHeThreads, 0, ctx->stream>>>(A);
     SNAPI_CK(cudaGetLastError());
+    const long long nvx = (long long)nb * nvar * nd;
+    k_eos_var<<<(unsigned)((nvx + kRecThreads - 1) / kRecThreads), kRecThreads, 0, ctx->stream>>>(A);
+    SNAPI_CK(cudaGetLastError());
     const int nrec = nb * nd;
     k_eos_rec<<<(nrec + kRecThreads - 1) / kRecThreads, kRecThreads, 0, ctx->stream>>>(A);
     SNAPI_CK(cudaGetLastError());
     SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    ctx->last_launches += 2;
+    ctx->last_launches += 3;
     if (host) {
       SNAPI_CK(cudaMemcpyAsync(records + (size_t)p0 * nd * nf, e->d_rec, sizeof(float) * nb * nd * nf,
                                cudaMemcpyDeviceToHost, ctx->stream));

@@ -113,7 +113,7 @@ def test_gpu_records_vs_oracle_and_reference(oracle_lib, eos3, config3):
     nodes = config3["nodes"]
     rec, tan, nt, status = ctx.build_records(nodes, tangents=False, want_nt=True)
     assert np.all(status == 0)
-    assert ctx.last_launches == 2
+    assert ctx.last_launches == 3
     t = _tables(eos3)
     lam0, mass = _line_const(config3)
     for p in range(nodes.shape[0]):
