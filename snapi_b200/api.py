@@ -20,7 +20,7 @@ LIB_PATH = os.environ.get("SNAPI_LIB", os.path.join(_PKG, "libsnapi_cuda.so"))
 OK, EINVAL, ECUDA, ETIMEOUT, ENONCONV, ENOMEM = 0, -1, -2, -3, -4, -5
 MEM_HOST, MEM_DEVICE = 0, 1
 NFIELD0 = 12
-MAX_LINES = 8
+MAX_LINES = 16  # SNAPI_MAX_LINES
 MAX_COMP = 16
 
 # record field indices (include/snapi_cuda.h)
