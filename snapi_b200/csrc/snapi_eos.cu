@@ -59,6 +59,16 @@ constexpr double cC = 2.99792458E10, cH = 6.6260687652E-27, cK = 1.3806503E-16, 
 constexpr double cE = 4.8032042510E-10, cRYD = 1.097373156853955E5, cE0 = 7.957747154594775607E-02;
 constexpr double cSAHA = 2.0706615382E-16;
 
+// per-stage and per-term constants packed for two 16-byte loads each in the ionisation sweep
+struct __align__(16) StageTab {
+  double zf, izf;  // Traving: z f and its inverse
+  int t0, t1;      // Traving asymptotic terms [t0, t1) (empty for the other types)
+  int ref, pad;    // kept-fraction slot (-1 none)
+};
+struct __align__(16) TermTab {
+  double l, il, A, g2;  // l, 1/l, ((1/3 (l-1) - 1/2)(l-1) - 1/6)(l-1), g2
+};
+
 struct EosDev {
   int natom, nmol, nst, nlev, nbf, nlines, npar, nd, nref, hm, href;
   double lambda_he, lambda_kappa, grav, tau_min, tau_max, theta, phi, ftrav;
@@ -75,6 +85,8 @@ struct EosDev {
   // Traving asymptotic terms and level sums
   double g2[kET], tee[kET], tll[kET], til[kET], tA[kET];  // til = 1/l, tA = ((1/3 (l-1) - 1/2)(l-1) - 1/6)(l-1)
   double zf[kES], izf[kES];  // Traving: z * f (Fischel-Sparks cut constant) and its inverse
+  StageTab stab[kES];
+  TermTab ttab[kET];
   int c0[kET], c1[kET];
   double cA[kEC], cG[kEC];
   // molecules (components: 1-based atom, 0 the electron)
@@ -120,9 +132,12 @@ struct EosDev {
 struct Chem {
   const EosDev &E;
   double T, kT;
-  double Ut[kES];   // T-only part of U (whole U for CONST / IRWIN / NONE)
-  double cz[kES];   // fct exp(-chi / kT): the T-only factor of the stage ratio
-  double Dz[kES];   // 31.321 z^2 x
+  struct __align__(16) SLoc {
+    double Ut;  // T-only part of U (whole U for CONST / IRWIN / NONE)
+    double cz;  // fct exp(-chi / kT): the T-only factor of the stage ratio
+    double Dz;  // 31.321 z^2 x
+    double pad;
+  } sl[kES];
   double w2[kET];   // g2 exp(-2.302585 ee x)
   double K[kEM];
   double Ea[kEA + 1], Da[kEA + 1];  // sum_i i f_i, sum_i i df_i / dNe per atom (1-based)
@@ -146,15 +161,15 @@ struct Chem {
           for (int c = E.c0[t]; c < E.c1[t]; ++c) u += E.cA[c] * exp(-2.302585 * E.cG[c] * x);
           w2[t] = E.g2[t] * exp(-2.302585 * E.tee[t] * x);
         }
-        Dz[s] = 31.321 * E.zeff[s] * E.zeff[s] * x;
+        sl[s].Dz = 31.321 * E.zeff[s] * E.zeff[s] * x;
       } else if (ty == SNAPI_PF_IRWIN) {
         const double lnT = log(T);
         double sum = 0.0;
         for (int c = E.t0[s]; c < E.t1[s]; ++c) sum += E.cA[c] * pow(lnT, (double)(c - E.t0[s]));
         u = exp(sum);
       }
-      Ut[s] = u;
-      cz[s] = fct * exp(-E.eion[s] / kT);
+      sl[s].Ut = u;
+      sl[s].cz = fct * exp(-E.eion[s] / kT);
     }
     for (int m = 0; m < E.nmol; ++m) {
       double k = 0.0;
@@ -172,30 +187,39 @@ struct Chem {
     }
   }
 
-  // U of stage s and (kDeriv) dU / dNe; ine = 1/ne, pne = ne^(1/6), ipne = 1/pne
+  // U of a stage and (kDeriv) dU / dNe from its packed constants; ine = 1/ne, pne = ne^(1/6), ipne = 1/pne
   template <bool kDeriv>
-  __device__ __forceinline__ void stage_u(int s, double ine, double pne, double ipne, double &U, double &dU) const {
-    U = Ut[s];
+  __device__ __forceinline__ void stage_u(const StageTab &S, const SLoc &L, double ine, double pne, double ipne,
+                                          double &U, double &dU) const {
+    U = L.Ut;
     dU = 0.0;
-    if (E.pft[s] != SNAPI_PF_TRAV) return;
-    const int t0 = E.t0[s], t1 = E.t1[s];
-    const double zf = E.zf[s], p = zf * ipne, ip = pne * E.izf[s], dz = Dz[s];
-    double dq = 0.0;
-    for (int t = t0; t < t1; ++t) {
-      const double l = E.tll[t], il = E.til[t];
+    if (S.t1 <= S.t0) return;
+    const double zf = S.zf, p = zf * ipne, ip = pne * S.izf, dz = L.Dz;
+    double dq = 0.0, wl = 0.0;
+    for (int t = S.t0; t < S.t1; ++t) {
+      const TermTab Tt = E.ttab[t];
+      const double l = Tt.l, il = Tt.il;
       double q;
       if (p > l) {
         q = ((1.3333333 * p + 0.5) * p + 0.16666667 + 1.33333333 * dz) * p - 0.4 * dz * dz * ip -
-            (E.tA[t] - dz * (l - 1.0)) + 0.5 * dz * dz * il;
+            (Tt.A - dz * (l - 1.0)) + 0.5 * dz * dz * il;
         if (kDeriv) dq = ((3.0 * 1.3333333 * p + 1.0) * p + 0.16666667 + 1.33333333 * dz) + 0.4 * dz * dz * ip * ip;
       } else {
         const double axl2 = dz * il * il, k4 = (1.0 + axl2 * (0.33333333 + 0.1 * axl2)) * il;
         q = k4 * p * p * p * p;
         if (kDeriv) dq = 4.0 * k4 * p * p * p;
       }
-      U += w2[t] * q;
+      wl = w2[t];
+      U += wl * q;
     }
-    if (kDeriv && t1 > t0) dU = -w2[t1 - 1] * dq * zf * ine * ipne * (1.0 / 6.0);
+    if (kDeriv) dU = -wl * dq * zf * ine * ipne * (1.0 / 6.0);
+  }
+
+  template <bool kDeriv>
+  __device__ __forceinline__ void stage_u(int s, double ine, double pne, double ipne, double &U, double &dU) const {
+    const StageTab S = E.stab[s];
+    const SLoc L = sl[s];
+    stage_u<kDeriv>(S, L, ine, pne, ipne, U, dU);
   }
 
   // atom a (0-based): Ea, and with kDeriv Da and the kept fractions
@@ -204,9 +228,10 @@ struct Chem {
     const int s0 = E.s0[a], ns = E.ns[a];
     double h = 1.0, fsum = 0.0, S1 = 0.0, dfsum = 0.0, S2 = 0.0, dl0 = 0.0;
     for (int z = 0; z < ns; ++z) {
-      const int s = s0 + z;
+      const StageTab S = E.stab[s0 + z];
+      const SLoc L = sl[s0 + z];
       double U, dU;
-      stage_u<kDeriv>(s, ine, pne, ipne, U, dU);
+      stage_u<kDeriv>(S, L, ine, pne, ipne, U, dU);
       const double f = U * h;
       fsum += f;
       S1 += (double)z * f;
@@ -216,17 +241,16 @@ struct Chem {
         else df = h * dU - f * (dl0 + (double)z * ine);
         dfsum += df;
         S2 += (double)z * df;
-        const int r = E.ref[s];
-        if (r >= 0) { fr[r] = f; dr[r] = df; }
+        if (S.ref >= 0) { fr[S.ref] = f; dr[S.ref] = df; }
       }
-      h *= cz[s] * ine;
+      h *= L.cz * ine;
     }
     const double inv = 1.0 / fsum;
     Ea[a + 1] = S1 * inv;
     if (kDeriv) {
       Da[a + 1] = (S2 - dfsum * S1 * inv) * inv;
       for (int z = 0; z < ns; ++z) {
-        const int r = E.ref[s0 + z];
+        const int r = E.stab[s0 + z].ref;
         if (r >= 0) { dr[r] = (dr[r] - dfsum * fr[r] * inv) * inv; fr[r] *= inv; }
       }
     }
@@ -979,6 +1003,22 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
   H.nlev = nlev;
   H.nref = nref;
   H.href = H.ref[H.s0[0]];
+  for (int q = 0; q < H.nst; ++q) {
+    StageTab &S = H.stab[q];
+    S.zf = H.zf[q];
+    S.izf = H.izf[q];
+    S.t0 = H.pft[q] == SNAPI_PF_TRAV ? H.t0[q] : 0;
+    S.t1 = H.pft[q] == SNAPI_PF_TRAV ? H.t1[q] : 0;
+    S.ref = H.ref[q];
+    S.pad = 0;
+  }
+  for (int q = 0; q < nt; ++q) {
+    TermTab &Tt = H.ttab[q];
+    Tt.l = H.tll[q];
+    Tt.il = H.til[q];
+    Tt.A = H.tA[q];
+    Tt.g2 = H.g2[q];
+  }
   // nodes: kinds 1..6, contiguous, non-decreasing
   for (int k = 0; k < 7; ++k) { H.kfirst[k] = 0; H.kcount[k] = 0; }
   int prev = 0;
