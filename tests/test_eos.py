@@ -254,3 +254,59 @@ def test_gpu_model_without_field_nodes_vs_oracle(oracle_lib, eos3, config3):
         scale = np.maximum(np.abs(to).max(axis=1, keepdims=True), 1e-6 * np.abs(ro).max(axis=0))
         assert (np.abs(tan[p] - to) / np.maximum(scale, 1e-30)).max() < 2e-5
     ctx.close()
+
+
+@pytest.mark.gpu
+@pytestmark_gpu
+def test_gpu_device_pointers_match_host(oracle_lib, eos3, config3, config4):
+    """snapi_build_records and snapi_lm_fit on device memory (SNAPI_MEM_DEVICE) give the host-memory
+    results."""
+    import ctypes
+    import torch
+    import snapi_b200 as sb
+    from snapi_b200.api import SnapiLmOpts, lib, MEM_DEVICE
+    from snapi_b200.eos_tables import EosTables
+    from helpers import node_scales
+    dev = torch.device("cuda", 0)
+    ctx = sb.Context.from_fixture(config3)
+    ctx.eos_set(EosTables(eos3))
+    nodes = config3["nodes"]
+    rec_h, tan_h, _, _ = ctx.build_records(nodes, tangents=True)
+    n = nodes.shape[0]
+    d_nodes = torch.from_numpy(np.ascontiguousarray(nodes)).to(dev)
+    d_rec = torch.zeros((n, ctx.nd, ctx.nfield), dtype=torch.float32, device=dev)
+    d_tan = torch.zeros((n, nodes.shape[1], ctx.nd, ctx.nfield), dtype=torch.float32, device=dev)
+    ctx.build_records_device(n, d_nodes.data_ptr(), d_rec.data_ptr(), d_tan.data_ptr())
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d_rec.cpu().numpy(), rec_h)
+    np.testing.assert_array_equal(d_tan.cpu().numpy(), tan_h)
+    ctx.close()
+
+    fx = config4
+    ic = float(np.abs(fx["target"][:, :, 0]).max())
+    kinds = np.ascontiguousarray(fx["node_kind"], dtype=np.int32)
+    steps = np.ascontiguousarray(1e-2 * node_scales(kinds), dtype=np.float64)
+    ctx = sb.Context.from_fixture(fx, stokes_scale=ic)
+    ctx.eos_set(EosTables(eos3))
+    host = ctx.lm_fit_device(fx["nodes0"], fx["target"], kinds, steps, mask=fx["mask"], lm_start=1e3, max_iter=5,
+                             delta=1e-3)
+    npix, npar = fx["nodes0"].shape
+    t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)  # noqa: E731
+    d_n0, d_obs, d_mask = t(fx["nodes0"], np.float64), t(fx["target"], np.float32), t(fx["mask"], np.float32)
+    d_out = torch.zeros((npix, npar), dtype=torch.float64, device=dev)
+    d_chi = torch.zeros(npix, dtype=torch.float64, device=dev)
+    d_it = torch.zeros(npix, dtype=torch.int32, device=dev)
+    d_st = torch.zeros((npix, ctx.nl, 4), dtype=torch.float32, device=dev)
+    opts = SnapiLmOpts(npar, kinds.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), 1e3, 5, 1e-3, 1e-30,
+                       steps.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0.0)
+    ws = np.ones(4)
+    nsteps = ctypes.c_int(0)
+    p = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    rc = lib().snapi_lm_fit(ctx._ctx, npix, ctypes.byref(opts), p(d_n0), p(d_obs), ws.ctypes.data_as(ctypes.c_void_p),
+                            p(d_mask), p(d_out), p(d_chi), p(d_it), p(d_st), ctypes.byref(nsteps), MEM_DEVICE)
+    ctx._check(rc)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d_out.cpu().numpy(), host["nodes"])
+    np.testing.assert_array_equal(d_chi.cpu().numpy(), host["chi2"])
+    np.testing.assert_array_equal(d_it.cpu().numpy(), host["iters"])
+    ctx.close()
