@@ -40,8 +40,8 @@ NPIX = 64 * 64
 FD_STEPS = np.array([5.0, 5.0, 5.0, 5.0, 2e3, 2e3, 2e3, 5.0, 5e-3, 5e-3])
 # ncu (--set full) of the four adjoint kernels on 2048 pixels of this workload, per pixel:
 # dram__bytes_read.sum + dram__bytes_write.sum, and executed FP32 flop (2 FFMA + FMUL + FADD)
-NCU_DRAM_BYTES_PER_PIXEL = 4.96e6
-NCU_FP32_FLOP_PER_PIXEL = 7.49e7
+NCU_DRAM_BYTES_PER_PIXEL = 4.90e6
+NCU_FP32_FLOP_PER_PIXEL = 6.49e7
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FMA rate at the 1965 MHz max clock
 
 
