@@ -310,3 +310,36 @@ def test_gpu_device_pointers_match_host(oracle_lib, eos3, config3, config4):
     np.testing.assert_array_equal(d_chi.cpu().numpy(), host["chi2"])
     np.testing.assert_array_equal(d_it.cpu().numpy(), host["iters"])
     ctx.close()
+
+
+@pytest.mark.gpu
+@pytestmark_gpu
+def test_gpu_build_errors(oracle_lib, eos3, config3):
+    """Error codes, not faults: building without a model, a model whose depth grid is not the
+    problem's, node vectors of the wrong length, an LM whose node kinds are not the model's."""
+    import snapi_b200 as sb
+    from snapi_b200.api import SnapiError
+    from snapi_b200.eos_tables import EosTables
+    from helpers import node_scales
+    ctx = sb.Context.from_fixture(config3)
+    ctx._eos_npar = 10
+    with pytest.raises(SnapiError) as e:
+        ctx.build_records(config3["nodes"][:1], tangents=False)
+    assert e.value.code == -1 and "snapi_eos_set" in str(e.value)
+    d = dict(eos3)
+    d["meta"] = np.array(d["meta"])
+    d["meta"][6] = 1.5  # tau_max: another grid
+    with pytest.raises(SnapiError) as e:
+        ctx.eos_set(EosTables(d))
+    assert e.value.code == -1 and "tau500" in str(e.value)
+    ctx.eos_set(EosTables(eos3))
+    with pytest.raises(ValueError):
+        ctx.build_records(config3["nodes"][:1, :9], tangents=False)
+    kinds = config3["node_kind"].copy()
+    kinds[4], kinds[5] = 3, 2  # not the model's order
+    with pytest.raises(SnapiError) as e:
+        ctx.lm_fit_device(config3["nodes"][:2], config3["target"][:2], kinds, 1e-2 * node_scales(kinds), max_iter=2)
+    assert e.value.code == -1
+    rec, _, _, st = ctx.build_records(config3["nodes"][:1], tangents=False)  # the context still works
+    assert st[0] == 0 and np.isfinite(rec).all()
+    ctx.close()
