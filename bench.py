@@ -22,6 +22,7 @@ on the host cores for the same metric.
 """
 import argparse
 import json
+import shutil
 import os
 import subprocess
 import sys
@@ -424,6 +425,44 @@ def bench_lm_device(sb, pool, ic, device, npix=1024, iters=10):
             "median_iterations": float(np.median(res["iters"]))}
 
 
+def bench_cube(sb, pool, ic, device, n=64, iters=30, chunk=0):
+    """The master's invert job (snapi_cube_invert) over an n x n float32 .f0 cube: noisy Stokes
+    synthesised on the GPU from the pool's node vectors tiled over the cube, every pixel started from
+    the same node vector (the job's model) and fitted for up to iters iterations, the cube streamed
+    from the file in chunks while the GPU fits, the node cube and float64 spectra written back."""
+    npix = n * n
+    nodes = np.tile(pool["nodes"], (npix // pool["nodes"].shape[0] + 1, 1))[:npix]
+    ctx = sb.Context.from_fixture(pool, stokes_scale=ic, max_batch=4096, device=device)
+    ctx.eos_set(_eos_tables())
+    rec, _, _, _ = ctx.build_records(nodes, tangents=False)
+    obs = ctx.synth(rec)
+    del rec
+    obs += np.random.default_rng(14).normal(0.0, 1e-3 * ic, obs.shape).astype(np.float32)
+    nl = obs.shape[1]
+    kinds = pool["node_kind"].astype(int)
+    scale = np.array([{1: 5000.0, 2: 1e5, 3: 1e5, 4: 1000.0}.get(k, 1.0) for k in kinds])
+    start = pool["nodes"].mean(axis=0) + np.array([200.0, 200.0, 200.0, 200.0, 3e4, 3e4, 3e4, 200.0, 0.1, 0.1])
+    tmp = tempfile.mkdtemp(prefix="snapi_cube_")
+    try:
+        path = os.path.join(tmp, "obs.f0")
+        sb.api.f0_write(path, np.ascontiguousarray(obs.reshape(n, n, nl, 4).transpose(0, 1, 3, 2)))
+        del obs
+        out = ctx.cube_invert(path, kinds, 1e-2 * scale, nodes0=start, out_nodes=os.path.join(tmp, "nodes.f0"),
+                              out_spectra=os.path.join(tmp, "spectra.f0"), chunk=chunk, lm_start=1e3,
+                              max_iter=iters, delta=1e-4)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    ctx.close()
+    st = out["stats"]
+    return {"cube": [n, n], "pixels": npix, "chunks": st["chunks"], "iterations": iters, "lm_steps": st["lm_steps"],
+            "wall_s": st["wall_s"], "fit_s": st["fit_s"], "read_wait_s": st["read_wait_s"],
+            "write_wait_s": st["write_wait_s"], "device_s": st["kernel_ms"] / 1e3,
+            "pixels_per_s": npix / st["wall_s"], "bytes_read": st["bytes_read"], "bytes_written": st["bytes_written"],
+            "median_iterations": float(np.median(out["iters"])),
+            "note": "wall_s covers the whole job: reads, fits and writes; read / write waits are the I/O "
+                    "not hidden behind the fits"}
+
+
 def bench_ali(sb, device, ncol=1024, cpu=True):
     """NLTE Ca II populations (snapi_ali_iter) for ncol columns to the reference's convergence
     criterion (max relative change < 1e-2): the three reference-built columns of
@@ -576,6 +615,9 @@ def main():
                     help="only measure the node -> record build of N columns (profiling)")
     ap.add_argument("--lm-fit-only", type=int, default=0, metavar="N",
                     help="only measure the whole LM on the device (snapi_lm_fit) for N pixels, 30 iterations")
+    ap.add_argument("--cube-only", type=int, default=0, metavar="N",
+                    help="only measure the invert job (snapi_cube_invert) over an N x N .f0 cube")
+    ap.add_argument("--cube-chunk", type=int, default=0, help="pixels per GPU batch of the invert job")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -594,6 +636,16 @@ def main():
         pool = dict(np.load(POOL))
         ic = float(pool["stokes"][:, :, 0].max())
         print(json.dumps({"lm_device_build": bench_lm_device(sb, pool, ic, 0, npix=args.lm_fit_only, iters=30)}),
+              flush=True)
+        return
+    if args.cube_only:
+        sys.path.insert(0, ROOT)
+        import snapi_b200 as sb
+        from snapi_b200 import build as b
+        b.build_cuda()
+        pool = dict(np.load(POOL))
+        ic = float(pool["stokes"][:, :, 0].max())
+        print(json.dumps({"cube_invert": bench_cube(sb, pool, ic, 0, n=args.cube_only, chunk=args.cube_chunk)}),
               flush=True)
         return
     line = run_reference(args) if args.impl == "reference" else run_snapi(args)

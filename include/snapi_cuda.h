@@ -430,6 +430,90 @@ int snapi_adjoint_noalloc(const snapi_problem *prob, int device, void *stream, i
                           const float *tangents, float *stokes, double *chi2, double *grad);
 const char *snapi_noalloc_last_error(void);
 
+/* ---- ANA ".f0" files: the observed Stokes cubes, model cubes and results ------------------------
+ * Replaces ana_fzread (cmlib/ana_read.cc:74-178), ana_fzwrite (cmlib/ana_write.cc:129-175) and the
+ * streaming ana_file (cmlib/ana_write.cc:177-239).  Elements are stored with dim[0] varying
+ * fastest: a cube the reference writes from an array a[x1][x2][x3][x4] has dim = {n4, n3, n2, n1}.
+ * Uncompressed files only (compressed ones hold integer images, never a cube of this path).
+ * Errors return SNAPI_EINVAL; snapi_f0_error() (per host thread) says why. */
+#define SNAPI_F0_INT8 0
+#define SNAPI_F0_INT16 1
+#define SNAPI_F0_INT32 2
+#define SNAPI_F0_FLOAT32 3
+#define SNAPI_F0_FLOAT64 4
+#define SNAPI_F0_INT64 5
+#define SNAPI_F0_MAX_DIM 16
+
+typedef struct {
+  int type;                      /* SNAPI_F0_* of the stored elements */
+  int ndim;
+  long long dim[SNAPI_F0_MAX_DIM];  /* dim[0] varies fastest */
+  long long nelem;
+  long long data_offset;         /* bytes before the first element (512 per header block) */
+  int nhb;                       /* header blocks */
+  int swap;                      /* 1: elements stored in the other byte order (swapped on read) */
+  int compressed;                /* 1: anacrunch-compressed (not readable here) */
+  int reversed_synch;            /* 1: byte-reversed synch pattern (the reference warns, flips swap) */
+  char header[15 * 256 + 1];     /* text of all header blocks, concatenated */
+} snapi_f0_info;
+
+int snapi_f0_stat(const char *path, snapi_f0_info *info);
+/* Elements [first, first + count) into out, converted to out_type (the file's own type,
+ * SNAPI_F0_FLOAT32 or SNAPI_F0_FLOAT64), native byte order. */
+int snapi_f0_read(const char *path, long long first, long long count, void *out, int out_type);
+/* The file ana_fzwrite writes: header (NULL: none; up to 15 blocks of 255 characters) and data. */
+int snapi_f0_write(const char *path, const void *data, int type, int ndim, const long long *dim, const char *header);
+/* Streaming writer: the same header, then element ranges in any order from any thread;
+ * snapi_f0_close reports a file whose elements were not all written (as ana_file does). */
+typedef struct snapi_f0_file snapi_f0_file;
+snapi_f0_file *snapi_f0_create(const char *path, int type, int ndim, const long long *dim, const char *header,
+                               int *status);
+int snapi_f0_write_at(snapi_f0_file *f, long long first, long long count, const void *data);
+int snapi_f0_close(snapi_f0_file *f);
+const char *snapi_f0_error(void);
+
+/* ---- Cube inversion: the master's invert job with every pixel fitted on the GPU ----------------
+ * Replaces the inversion branch of job_class (master/job.cc:304-379: read the cube, scale it by
+ * synth_qs / obs_qs, cut the subfield and wavelength window, one islave stokes_lm_fit per pixel)
+ * and its result collection (master/job.cc:570-597).  The cube is streamed: a reader thread fetches
+ * the next batch of pixels from the file while the GPU fits the current one (snapi_lm_fit) and a
+ * writer thread stores the previous one.
+ *   observed cube  dims (nl, 4, ny, nx), float32 or float64 (read_file 4-D + transpose, job.cc:308)
+ *   model cube     dims (>= nx_sub, >= ny_sub, npar): node values of each pixel (job.cc:347-369),
+ *                  read as float32 / float64
+ *   out_nodes      inverted_nodes.f0: float32, dims (nx_sub, ny_sub, npar)        (job.cc:579)
+ *   out_spectra    inverted_spectra.f0: float64, dims (nl_win, 4, ny_sub, nx_sub), the fitted
+ *                  Stokes vectors (job.cc:597)
+ *   out_cube       cube_to_invert.f0: float64, the scaled window of the observation (job.cc:334)
+ * The context's wavelength grid is the window ll..lh of the cube's grid. */
+typedef struct {
+  const char *obs_path;
+  int xl, xh, yl, yh, ll, lh;    /* 1-based inclusive subfield and window; xh = 0 etc.: to the end */
+  double obs_qs, synth_qs;       /* the observation is multiplied by synth_qs / obs_qs (0, 0: 1) */
+  const double *nodes0;          /* [npar] starting nodes of every pixel (the job's model), or NULL */
+  const char *model_path;        /* or a model cube of starting nodes (NULL: nodes0) */
+  const float *mask;             /* [nl of the cube] wavelength weights (observable mask), or NULL */
+  const double *w_stokes;        /* [4] Stokes weights, or NULL */
+  const char *out_nodes, *out_spectra, *out_cube;  /* NULL: not written */
+  double *chi2;                  /* [nx_sub * ny_sub] final chi2 per pixel (x major), or NULL */
+  int *iters;                    /* [nx_sub * ny_sub] iterations per pixel, or NULL */
+  int chunk;                     /* pixels per GPU batch (0: 16384) */
+} snapi_cube_job;
+
+typedef struct {
+  long long pixels, chunks, lm_steps;
+  double wall_s;                 /* the whole call */
+  double fit_s;                  /* inside snapi_lm_fit */
+  double read_wait_s;            /* waiting for the reader (reads not hidden behind the fits) */
+  double write_wait_s;           /* waiting for the writer */
+  long long bytes_read, bytes_written;
+  double kernel_ms;              /* device time of all kernels */
+  int launches;
+} snapi_cube_stats;
+
+int snapi_cube_invert(snapi_ctx *ctx, const snapi_lm_opts *opts, const snapi_cube_job *job,
+                      snapi_cube_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -966,6 +966,118 @@ static int do_eos(const char *tskname, const char *nodesname, int npix, const ch
   return 0;
 }
 
+// ----------------------------------------------------------------------------------------------
+// ANA .f0 files and the cube steps of the master's job (cmlib/ana_read.cc, cmlib/ana_write.cc,
+// cmlib/fileio.cc, master/job.cc:306-334, 575-597).  Dump format of f0read (little endian):
+//   int32 mfbd_type; int32 nd; int32 dims[nd]; int32 hlen; char header[hlen]; int64 nbytes; data
+#include "fileio.h"
+#include "ana_io.h"
+#include "obs.h"
+
+static void put_i32(FILE *f, int32_t v) { fwrite(&v, 4, 1, f); }
+
+// ana_fzread of one file; the data as the reader returns it (native byte order)
+static int do_f0read(const char *inname, const char *outname) {
+  const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
+  const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
+  int ac = 4; cmdln cmd(ac, (char **)argv, options, maps);
+  io_class io(cmd);
+  int *ds = 0, nd = 0, type = -1;
+  char *header = 0;
+  byte *data = ana_fzread((char *)inname, ds, nd, header, type, io);
+  if (!data) return 3;
+  int sz[] = MFBD_TYPE_SIZES;
+  int64_t n = 1;
+  for (int d = 1; d <= nd; ++d) n *= ds[d];
+  FILE *f = fopen(outname, "wb");
+  put_i32(f, type); put_i32(f, nd);
+  for (int d = 1; d <= nd; ++d) put_i32(f, ds[d]);
+  int32_t hl = (int32_t)strlen(header);
+  put_i32(f, hl); fwrite(header, 1, hl, f);
+  int64_t nb = n * sz[type];
+  fwrite(&nb, 8, 1, f); fwrite(data, 1, nb, f);
+  fclose(f);
+  delete[] data; delete[] header; delete[] (ds + 1);
+  return 0;
+}
+
+// ana_fzwrite of raw data: type (ANA code), dims (comma separated, fastest first), header file
+// ("-" for none), data file
+static int do_f0write(const char *outname, int type, const char *dims, const char *hdrname,
+                      const char *dataname) {
+  const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
+  const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
+  int ac = 4; cmdln cmd(ac, (char **)argv, options, maps);
+  io_class io(cmd);
+  std::vector<int> dv;
+  for (const char *p = dims; *p;) { dv.push_back(atoi(p)); while (*p && *p != ',') ++p; if (*p) ++p; }
+  int nd = (int)dv.size();
+  int *ds = new int[nd] - 1;
+  for (int d = 1; d <= nd; ++d) ds[d] = dv[d - 1];
+  std::vector<uint8_t> hb, db = read_file_bytes(dataname);
+  char *header = 0;
+  if (strcmp(hdrname, "-")) {
+    hb = read_file_bytes(hdrname); hb.push_back(0);
+    header = (char *)hb.data();
+  }
+  ana_fzwrite(db.data(), (char *)outname, ds, nd, header, type, io);
+  delete[] (ds + 1);
+  return 0;
+}
+
+// The observed-cube steps of job.cc:306-334: read_file (4-D) + transpose + observable::set +
+// normalize (synth_qs / obs_qs) + extract(xl..xh, yl..yh, ll..lh); dumps the extracted S as
+// float64 [x][y][s][l] after a header int32 nx, ny, ns, nl, and writes it as cube_to_invert.f0
+// is written (write_file 4-D, job.cc:333-334) to cubename
+static int do_cubeobs(const char *inname, int xl, int xh, int yl, int yh, int ll, int lh, double obs_qs,
+                      double synth_qs, const char *outname, const char *cubename) {
+  const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
+  const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
+  int ac = 4; cmdln cmd(ac, (char **)argv, options, maps);
+  io_class io(cmd);
+  int n1, n2, n3, n4;
+  fp_t ****test = read_file((char *)inname, n1, n2, n3, n4, io);
+  if (!test) return 3;
+  test = transpose(test, n1, n2, n3, n4);
+  observable *obs = new observable(n4, n3, n2, n1);
+  obs->set(test);
+  del_ft4dim(test, 1, n4, 1, n3, 1, n2, 1, n1);
+  obs->set_inv_parameters(0.0, 0.0, obs_qs, synth_qs);
+  obs->normalize();
+  observable *o2 = obs->extract(xl, xh, yl, yh, ll, lh);
+  delete obs;
+  int nx = xh - xl + 1, ny = yh - yl + 1, nl = lh - ll + 1;
+  fp_t ****S = o2->get_S();
+  FILE *f = fopen(outname, "wb");
+  put_i32(f, nx); put_i32(f, ny); put_i32(f, n2); put_i32(f, nl);
+  fwrite(S[1][1][1] + 1, sizeof(fp_t), (size_t)nx * ny * n2 * nl, f);
+  fclose(f);
+  write_file((char *)cubename, S, nx, ny, 4, nl, io);
+  del_ft4dim(S, 1, nx, 1, ny, 1, n2, 1, nl);
+  delete o2;
+  return 0;
+}
+
+// The output steps of job.cc:575-597: write_file of the node cube (fp_t [x][y][p], 3-D overload)
+// and of the fitted spectra (fp_t [x][y][s][l], 4-D overload), from raw float64 inputs
+static int do_cubewrite(const char *nodesname, const char *specname, int nx, int ny, int np, int nl,
+                        const char *out_nodes, const char *out_spec) {
+  const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
+  const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
+  int ac = 4; cmdln cmd(ac, (char **)argv, options, maps);
+  io_class io(cmd);
+  std::vector<uint8_t> nb = read_file_bytes(nodesname), sb = read_file_bytes(specname);
+  fp_t ***nc = ft3dim(1, nx, 1, ny, 1, np);
+  memcpy(nc[1][1] + 1, nb.data(), (size_t)nx * ny * np * sizeof(fp_t));
+  write_file((char *)out_nodes, nc, nx, ny, np, io);
+  del_ft3dim(nc, 1, nx, 1, ny, 1, np);
+  fp_t ****sc = ft4dim(1, nx, 1, ny, 1, 4, 1, nl);
+  memcpy(sc[1][1][1] + 1, sb.data(), (size_t)nx * ny * 4 * nl * sizeof(fp_t));
+  write_file((char *)out_spec, sc, nx, ny, 4, nl, io);
+  del_ft4dim(sc, 1, nx, 1, ny, 1, 4, 1, nl);
+  return 0;
+}
+
 int main(int argc, char **argv) {
   if (argc >= 6 && !strcmp(argv[1], "eos")) return do_eos(argv[2], argv[3], atoi(argv[4]), argv[5]);
   if (argc >= 4 && !strcmp(argv[1], "pack")) return do_pack(argv[2], argv[3]);
@@ -978,6 +1090,15 @@ int main(int argc, char **argv) {
   if (argc >= 9 && !strcmp(argv[1], "lmfit"))
     return do_lmfit(argv[2], argv[3], argv[4], argv[5], atoi(argv[6]), atoi(argv[7]), argv[8],
                     argc >= 10 ? atof(argv[9]) : 0.0);
+  if (argc >= 4 && !strcmp(argv[1], "f0read")) return do_f0read(argv[2], argv[3]);
+  if (argc >= 7 && !strcmp(argv[1], "f0write"))
+    return do_f0write(argv[2], atoi(argv[3]), argv[4], argv[5], argv[6]);
+  if (argc >= 13 && !strcmp(argv[1], "cubeobs"))
+    return do_cubeobs(argv[2], atoi(argv[3]), atoi(argv[4]), atoi(argv[5]), atoi(argv[6]), atoi(argv[7]),
+                      atoi(argv[8]), atof(argv[9]), atof(argv[10]), argv[11], argv[12]);
+  if (argc >= 10 && !strcmp(argv[1], "cubewrite"))
+    return do_cubewrite(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]), atoi(argv[6]), atoi(argv[7]), argv[8],
+                        argv[9]);
   fprintf(stderr, "usage: snapi_ref_dump pack|dump|lmfit ...\n");
   return 1;
 }

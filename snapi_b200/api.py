@@ -75,6 +75,51 @@ class SnapiLmOpts(ctypes.Structure):
     ]
 
 
+F0_INT8, F0_INT16, F0_INT32, F0_FLOAT32, F0_FLOAT64, F0_INT64 = range(6)
+F0_DTYPES = [np.int8, np.int16, np.int32, np.float32, np.float64, np.int64]
+
+
+class F0Info(ctypes.Structure):
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("ndim", ctypes.c_int),
+        ("dim", ctypes.c_longlong * 16),
+        ("nelem", ctypes.c_longlong),
+        ("data_offset", ctypes.c_longlong),
+        ("nhb", ctypes.c_int),
+        ("swap", ctypes.c_int),
+        ("compressed", ctypes.c_int),
+        ("reversed_synch", ctypes.c_int),
+        ("header", ctypes.c_char * (15 * 256 + 1)),
+    ]
+
+
+class CubeJob(ctypes.Structure):
+    _fields_ = [
+        ("obs_path", ctypes.c_char_p),
+        ("xl", ctypes.c_int), ("xh", ctypes.c_int), ("yl", ctypes.c_int), ("yh", ctypes.c_int),
+        ("ll", ctypes.c_int), ("lh", ctypes.c_int),
+        ("obs_qs", ctypes.c_double), ("synth_qs", ctypes.c_double),
+        ("nodes0", ctypes.c_void_p),
+        ("model_path", ctypes.c_char_p),
+        ("mask", ctypes.c_void_p),
+        ("w_stokes", ctypes.c_void_p),
+        ("out_nodes", ctypes.c_char_p), ("out_spectra", ctypes.c_char_p), ("out_cube", ctypes.c_char_p),
+        ("chi2", ctypes.c_void_p),
+        ("iters", ctypes.c_void_p),
+        ("chunk", ctypes.c_int),
+    ]
+
+
+class CubeStats(ctypes.Structure):
+    _fields_ = [
+        ("pixels", ctypes.c_longlong), ("chunks", ctypes.c_longlong), ("lm_steps", ctypes.c_longlong),
+        ("wall_s", ctypes.c_double), ("fit_s", ctypes.c_double), ("read_wait_s", ctypes.c_double),
+        ("write_wait_s", ctypes.c_double), ("bytes_read", ctypes.c_longlong), ("bytes_written", ctypes.c_longlong),
+        ("kernel_ms", ctypes.c_double), ("launches", ctypes.c_int),
+    ]
+
+
 _LIB = None
 
 
@@ -114,6 +159,19 @@ def lib():
         L.snapi_lm_begin.argtypes = [vp, ip, ctypes.POINTER(SnapiLmOpts), fp, fp, fp, fp, fp, ip]
         L.snapi_lm_step.argtypes = [vp, fp, fp, fp, fp, ctypes.POINTER(ctypes.c_int), ip]
         L.snapi_lm_result.argtypes = [vp, fp, fp, fp, fp, ip]
+        ll = ctypes.c_longlong
+        L.snapi_f0_stat.argtypes = [ctypes.c_char_p, ctypes.POINTER(F0Info)]
+        L.snapi_f0_read.argtypes = [ctypes.c_char_p, ll, ll, vp, ip]
+        L.snapi_f0_write.argtypes = [ctypes.c_char_p, vp, ip, ip, ctypes.POINTER(ll), ctypes.c_char_p]
+        L.snapi_f0_create.restype = vp
+        L.snapi_f0_create.argtypes = [ctypes.c_char_p, ip, ip, ctypes.POINTER(ll), ctypes.c_char_p,
+                                      ctypes.POINTER(ctypes.c_int)]
+        L.snapi_f0_write_at.argtypes = [vp, ll, ll, vp]
+        L.snapi_f0_close.argtypes = [vp]
+        L.snapi_f0_error.restype = ctypes.c_char_p
+        L.snapi_f0_error.argtypes = []
+        L.snapi_cube_invert.argtypes = [vp, ctypes.POINTER(SnapiLmOpts), ctypes.POINTER(CubeJob),
+                                        ctypes.POINTER(CubeStats)]
         _LIB = L
     return _LIB
 
@@ -172,6 +230,44 @@ def pack_tangents(tangents, field_mask):
             if (int(m) >> f) & 1:
                 cols.append(t[:, p, :, f])
     return np.ascontiguousarray(np.stack(cols, axis=1), dtype=np.float32)
+
+
+def _f0_check(rc):
+    if rc != 0:
+        raise SnapiError(rc, lib().snapi_f0_error().decode())
+
+
+def f0_stat(path):
+    """Header of an ANA .f0 file (snapi_f0_stat): dict of type, dims (fastest first), header, ..."""
+    info = F0Info()
+    _f0_check(lib().snapi_f0_stat(os.fsencode(path), ctypes.byref(info)))
+    return {"type": info.type, "dims": tuple(info.dim[d] for d in range(info.ndim)), "nelem": info.nelem,
+            "data_offset": info.data_offset, "nhb": info.nhb, "swap": info.swap, "compressed": info.compressed,
+            "reversed_synch": info.reversed_synch, "header": info.header.decode("latin-1")}
+
+
+def f0_read(path, out_type=None, first=0, count=None):
+    """Elements of an .f0 file as a numpy array shaped like the reference's C array (slowest dimension
+    first), or a flat range [first, first + count) when count is given."""
+    h = f0_stat(path)
+    t = h["type"] if out_type is None else out_type
+    n = h["nelem"] - first if count is None else count
+    out = np.empty(n, F0_DTYPES[t])
+    _f0_check(lib().snapi_f0_read(os.fsencode(path), first, n, out.ctypes.data, t))
+    if count is None and first == 0:
+        out = out.reshape(tuple(reversed(h["dims"])))
+    return out
+
+
+def f0_write(path, data, header=None, type=None):
+    """Write an array as the reference's ana_fzwrite does (dims reversed: the last axis varies fastest)."""
+    a = np.ascontiguousarray(data)
+    t = F0_DTYPES.index(a.dtype.type) if type is None else type
+    if 0 <= t < len(F0_DTYPES):
+        a = np.ascontiguousarray(a, dtype=F0_DTYPES[t])
+    dims = (ctypes.c_longlong * a.ndim)(*reversed(a.shape))
+    hb = None if header is None else header.encode("latin-1")
+    _f0_check(lib().snapi_f0_write(os.fsencode(path), a.ctypes.data, t, a.ndim, dims, hb))
 
 
 class Context:
@@ -352,6 +448,38 @@ class Context:
         self._check(lib().snapi_lm_fit(self._ctx, npix, ctypes.byref(opts), _ptr(n0), _ptr(ob), _ptr(ws), _ptr(mk),
                                        _ptr(nodes), _ptr(chi2), _ptr(iters), _ptr(st), ctypes.byref(steps), MEM_HOST))
         return {"nodes": nodes, "chi2": chi2, "iters": iters, "stokes": st, "steps": steps.value}
+
+    def cube_invert(self, obs_path, node_kind, resp_step, nodes0=None, model_path=None, subfield=(0, 0, 0, 0),
+                    window=(0, 0), obs_qs=0.0, synth_qs=0.0, mask=None, w_stokes=(1.0, 1.0, 1.0, 1.0),
+                    out_nodes=None, out_spectra=None, out_cube=None, chunk=0, lm_start=1e3, max_iter=30, delta=1e-3,
+                    stopping_chisq=1e-30, spectral_broadening=0.0):
+        """The master's invert job over an .f0 cube (snapi_cube_invert; needs eos_set).  subfield
+        (xl, xh, yl, yh) and window (ll, lh) are 1-based inclusive, 0 = the cube's extent.  Returns the
+        per-pixel chi2 and iterations (x major) and the job's statistics."""
+        kind = np.ascontiguousarray(node_kind, dtype=np.int32)
+        npar = kind.size
+        stp = np.ascontiguousarray(np.broadcast_to(resp_step, (npar,)), dtype=np.float64)
+        opts = SnapiLmOpts(npar, kind.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), float(lm_start), int(max_iter),
+                           float(delta), float(stopping_chisq), stp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                           float(spectral_broadening))
+        dims = f0_stat(obs_path)["dims"]
+        nx_full, ny_full = (dims[3], dims[2]) if len(dims) == 4 else (1, 1)  # the library reports the shape
+        xl, xh, yl, yh = subfield
+        nx = (xh or nx_full) - (xl or 1) + 1
+        ny = (yh or ny_full) - (yl or 1) + 1
+        n0 = None if nodes0 is None else np.ascontiguousarray(nodes0, dtype=np.float64)
+        mk = None if mask is None else _f32(mask)
+        ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
+        chi2 = np.zeros(max(nx * ny, 1))
+        iters = np.zeros(max(nx * ny, 1), np.int32)
+        enc = lambda p: None if p is None else os.fsencode(p)
+        job = CubeJob(os.fsencode(obs_path), xl, xh, yl, yh, window[0], window[1], float(obs_qs), float(synth_qs),
+                      _ptr(n0), enc(model_path), _ptr(mk), _ptr(ws), enc(out_nodes), enc(out_spectra), enc(out_cube),
+                      _ptr(chi2), _ptr(iters), int(chunk))
+        stats = CubeStats()
+        self._check(lib().snapi_cube_invert(self._ctx, ctypes.byref(opts), ctypes.byref(job), ctypes.byref(stats)))
+        return {"chi2": chi2.reshape(nx, ny), "iters": iters.reshape(nx, ny),
+                "stats": {k: getattr(stats, k) for k, _ in CubeStats._fields_}}
 
     def lm_fit(self, nodes0, obs, builder, node_kind, resp_step, **kw):
         """Run the fit to the end.  builder(nodes [n, npar], active [n] bool) returns (records,

@@ -12,8 +12,9 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libsnapi_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["snapi_cuda.cu", "snapi_lm.cu", "snapi_ali.cu", "snapi_tc.cu", "snapi_psf.cu", "snapi_eos.cu"]
-HEADERS = ["snapi_core.cuh", "snapi_sweep.cuh", "snapi_internal.cuh"]
+SOURCES = ["snapi_cuda.cu", "snapi_lm.cu", "snapi_ali.cu", "snapi_tc.cu", "snapi_psf.cu", "snapi_eos.cu",
+           "snapi_f0.cu", "snapi_cube.cu"]
+HEADERS = ["snapi_core.cuh", "snapi_sweep.cuh", "snapi_internal.cuh", "snapi_f0_internal.h"]
 
 
 def _stale(target, deps):

@@ -17,6 +17,16 @@ its 80-depth atmosphere file from REF and runs oracle/_ref/snapi_ref_dump).  Wri
   tests/golden/eos_c1.npz, eos_c3.npz  (--only-eos) node-model tables of the c1 / c3 tasks, the
                                   reference's chemistry on a (T, Nt) grid and the columns its
                                   build_from_nodes leaves for the config-1/2 and config-3 nodes
+  tests/golden/config4_256.npz    (--only-c4-subset 256) the config-4 fit of 256 seeded pixels
+                                  (seed 404) by the reference's stokes_lm_fit
+  tests/golden/f0_ref.npz         (--only-f0) ANA .f0 files written by the reference's ana_fzwrite
+                                  and what its ana_fzread returns for them, for hand-made headers
+                                  (reversed synch pattern, big-endian data) and for the two .f0
+                                  files of its test directory; a 4 x 4 pixel observed cube (config-4
+                                  targets) with the subfield / window / scaling the master's invert
+                                  job applies to it (read_file + transpose + normalize + extract)
+                                  and the cube_to_invert.f0 it writes; the node and spectra cubes
+                                  its write_file calls produce from given arrays
 
 Synthetic inputs stand in for observations: seeded numpy generators with the shapes and value
 distributions of the benchmark configurations (no dataset is read).
@@ -202,12 +212,12 @@ def config4_inputs(npix, seed=4):
     return truth, truth + C4_OFFSET, mask
 
 
-def make_config4(tmp, npix, iters=30, broadening=0.0, name="config4"):
+def make_config4(tmp, npix, iters=30, broadening=0.0, name="config4", seed=4, workers=0):
     """Reference LM (stokes_lm_fit, DELTA 1e-3 as compiled, start lambda 1e3) on config-4 pixels,
     one process per pixel; with broadening > 0 [cm] the targets are broadened by the reference's
     own convolution and the fit broadens its synthesis and responses the same way."""
     task = os.path.join(tmp, "c3.tsk")
-    truth, nodes0, mask = config4_inputs(npix)
+    truth, nodes0, mask = config4_inputs(npix, seed=seed)
     d = dump(tmp, task, truth, 0, "c4truth")
     rng = np.random.default_rng(44)
     ic = d["stokes"][:, :, 0].max(axis=1)
@@ -225,6 +235,9 @@ def make_config4(tmp, npix, iters=30, broadening=0.0, name="config4"):
             np.ascontiguousarray(arr, dtype="<f8").tofile(os.path.join(tmp, "c4_%s_%d.f64" % (nm, i)))
         args = [DUMP, "lmfit", task] + [os.path.join(tmp, "c4_%s_%d.f64" % (nm, i)) for nm in ("n0", "tg", "mk")] + \
                ["1", str(iters), os.path.join(tmp, "c4_fit_%d.sbin" % i), repr(broadening)]
+        if workers and len(procs) >= workers:  # at most `workers` reference processes at a time
+            if procs.pop(0).wait() != 0:
+                raise RuntimeError("lmfit failed")
         procs.append(subprocess.Popen(args, cwd=tmp, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
     for p in procs:
         if p.wait() != 0:
@@ -295,6 +308,9 @@ def main():
     ap.add_argument("--only-c5", action="store_true")
     ap.add_argument("--only-psf", action="store_true")
     ap.add_argument("--only-eos", action="store_true")
+    ap.add_argument("--only-f0", action="store_true")
+    ap.add_argument("--only-c4-subset", type=int, default=0, metavar="N",
+                    help="config-4 fit of N pixels by the reference (8 processes at a time)")
     ap.add_argument("--c5col", type=int, default=3)
     a = ap.parse_args()
     if not os.path.exists(DUMP):
@@ -305,6 +321,13 @@ def main():
             shutil.copy(os.path.join(a.ref, "cfg", f), tmp)
         if a.only_eos:
             make_eos(tmp)
+            return
+        if a.only_f0:
+            make_f0(tmp, a.ref)
+            return
+        if a.only_c4_subset:
+            shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
+            make_config4(tmp, a.only_c4_subset, name="config4_%d" % a.only_c4_subset, seed=404, workers=8)
             return
         if a.only_psf:
             make_psf(tmp)
@@ -332,6 +355,134 @@ def main():
         print("fixtures written to", HERE)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+
+
+F0_NP = [np.int8, np.int16, np.int32, np.float32, np.float64, np.int64]
+MFBD_TO_ANA = {0: 0, 1: 1, 2: 2, 3: 5, 4: 3, 5: 4}  # fileio.h MFBD_* -> ana_io.h type codes
+
+
+def f0_header_block(synch_bytes, subf, nhb, datyp, dims, text=b""):
+    b = bytearray(512)
+    b[0:4] = synch_bytes
+    b[4], b[6], b[7], b[8] = subf, nhb, datyp, len(dims)
+    for i, d in enumerate(dims):
+        b[192 + 4 * i:196 + 4 * i] = int(d).to_bytes(4, "little")
+    b[256:256 + len(text)] = text
+    return bytes(b)
+
+
+def ref_f0read(tmp, path):
+    out = os.path.join(tmp, "f0read.dump")
+    run([DUMP, "f0read", path, out], tmp)
+    b = open(out, "rb").read()
+    t, nd = np.frombuffer(b[:8], "<i4")
+    dims = np.frombuffer(b[8:8 + 4 * nd], "<i4").astype(np.int64)
+    o = 8 + 4 * nd
+    hl = int(np.frombuffer(b[o:o + 4], "<i4")[0])
+    hdr = b[o + 4:o + 4 + hl]
+    o += 4 + hl
+    nb = int(np.frombuffer(b[o:o + 8], "<i8")[0])
+    return MFBD_TO_ANA[int(t)], dims, hdr, np.frombuffer(b[o + 8:o + 8 + nb], np.uint8)
+
+
+def make_f0(tmp, ref):
+    out = {}
+    rng = np.random.default_rng(50)
+    # ana_fzwrite: name, ANA type, C shape (slowest first), header text (None: no header)
+    wcases = [("f32_3d", 3, (2, 3, 4), None), ("f64_1d_hdr", 4, (5,), "hello f0"),
+              ("i16_2d_3blk", 1, (3, 7), "h" * 600), ("i32_4d_255", 2, (2, 2, 2, 2), "a" * 255),
+              ("i32_256", 2, (3,), "b" * 256), ("i8_1d", 0, (10,), None), ("i64_clip", 5, (3,), "c" * 4000)]
+    names = []
+    for name, t, shape, hdr in wcases:
+        dt = F0_NP[t]
+        if t in (3, 4):
+            data = rng.standard_normal(shape).astype(dt)
+        else:
+            data = rng.integers(-100, 100, shape).astype(dt)
+        dfile = os.path.join(tmp, name + ".bin")
+        data.tofile(dfile)
+        hfile = "-"
+        if hdr is not None:
+            hfile = os.path.join(tmp, name + ".hdr")
+            open(hfile, "w").write(hdr)
+        f0 = os.path.join(tmp, name + ".f0")
+        run([DUMP, "f0write", f0, str(t), ",".join(str(v) for v in reversed(shape)), hfile, dfile], tmp)
+        out["w_%s_data" % name] = data
+        out["w_%s_type" % name] = np.int64(t)
+        out["w_%s_header" % name] = np.frombuffer((hdr or "").encode(), np.uint8)
+        out["w_%s_has_header" % name] = np.int64(hdr is not None)
+        out["w_%s_bytes" % name] = np.frombuffer(open(f0, "rb").read(), np.uint8)
+        names.append(name)
+    out["w_names"] = np.array(names)
+    # ana_fzread on hand-made headers: (name, file bytes)
+    v = rng.standard_normal((2, 3)).astype(np.float32)
+    v8 = rng.standard_normal((4,)).astype(np.float64)
+    norm, rev = bytes([0xaa, 0xaa, 0x55, 0x55]), bytes([0x55, 0x55, 0xaa, 0xaa])
+    rcases = [
+        ("be_data", f0_header_block(norm, 128, 1, 3, (3, 2)) + v.astype(">f4").tobytes()),
+        ("rev_synch", f0_header_block(rev, 0, 1, 3, (3, 2), b"reversed") + v.astype(">f4").tobytes()),
+        ("rev_synch_be", f0_header_block(rev, 128, 1, 3, (3, 2)) + v.astype("<f4").tobytes()),
+        ("f64_2blk", f0_header_block(norm, 0, 2, 4, (4,), b"x" * 255) +
+         f0_header_block(b"\0\0\0\0", 0, 0, 0, (), b"tail") + v8.tobytes()),
+    ]
+    for fn in ("inverted_atmos.f0", "acoustic_mean.f0"):
+        rcases.append(("test_" + fn[:-3], open(os.path.join(ref, "test", fn), "rb").read()))
+    rnames = []
+    for name, blob in rcases:
+        path = os.path.join(tmp, "r_" + name + ".f0")
+        open(path, "wb").write(blob)
+        t, dims, hdr, data = ref_f0read(tmp, path)
+        out["r_%s_file" % name] = np.frombuffer(blob, np.uint8)
+        out["r_%s_type" % name] = np.int64(t)
+        out["r_%s_dims" % name] = dims
+        out["r_%s_header" % name] = np.frombuffer(hdr, np.uint8)
+        out["r_%s_data" % name] = data
+        rnames.append(name)
+    out["r_names"] = np.array(rnames)
+    # the invert job's cube steps on a 4 x 4 pixel cube of config-4 targets, 3 + 2 padding wavelengths
+    d4 = np.load(os.path.join(HERE, "config4.npz"))
+    tgt = d4["target"]
+    nx, ny, pad0, pad1 = 4, 4, 3, 2
+    nlf = NLAMBDA + pad0 + pad1
+    cube = np.zeros((nx, ny, 4, nlf))
+    for x in range(nx):
+        for y in range(ny):
+            s4 = tgt[(x * ny + y) % tgt.shape[0]].T
+            cube[x, y, :, pad0:pad0 + NLAMBDA] = s4
+            cube[x, y, :, :pad0] = s4[:, :1]
+            cube[x, y, :, pad0 + NLAMBDA:] = s4[:, -1:]
+    sub = (2, 4, 2, 4, pad0 + 1, pad0 + NLAMBDA)
+    for tag, t, qs in (("f32", 3, (2.0, 1.0)), ("f64", 4, (3.0, 1.1))):
+        data = (cube * qs[0] / qs[1]).astype(F0_NP[t])
+        dfile = os.path.join(tmp, "cube_%s.bin" % tag)
+        data.tofile(dfile)
+        f0 = os.path.join(tmp, "cube_%s.f0" % tag)
+        run([DUMP, "f0write", f0, str(t), "%d,4,%d,%d" % (nlf, ny, nx), "-", dfile], tmp)
+        sdump = os.path.join(tmp, "cubeobs_%s.bin" % tag)
+        c2i = os.path.join(tmp, "c2i_%s.f0" % tag)
+        run([DUMP, "cubeobs", f0] + [str(v) for v in sub] + [repr(qs[0]), repr(qs[1]), sdump, c2i], tmp)
+        b = open(sdump, "rb").read()
+        hdr = np.frombuffer(b[:16], "<i4")
+        out["cube_%s_file" % tag] = np.frombuffer(open(f0, "rb").read(), np.uint8)
+        out["cube_%s_qs" % tag] = np.array(qs)
+        out["cube_%s_S" % tag] = np.frombuffer(b[16:], "<f8").reshape(tuple(hdr))
+        out["cube_%s_c2i" % tag] = np.frombuffer(open(c2i, "rb").read(), np.uint8)
+    out["cube_sub"] = np.array(sub)
+    out["cube_pix"] = np.array([(x * ny + y) % tgt.shape[0] for x in range(nx) for y in range(ny)])
+    # write_file of the node cube (3-D) and the fitted spectra (4-D), job.cc:579, 597
+    nxs, nys, npar = 3, 3, 10
+    nodes = rng.standard_normal((nxs, nys, npar)) * 1e3
+    spec = rng.standard_normal((nxs, nys, 4, 7))
+    nf, sf = os.path.join(tmp, "wn.bin"), os.path.join(tmp, "ws.bin")
+    nodes.tofile(nf)
+    spec.tofile(sf)
+    on, osp = os.path.join(tmp, "inverted_nodes.f0"), os.path.join(tmp, "inverted_spectra.f0")
+    run([DUMP, "cubewrite", nf, sf, str(nxs), str(nys), str(npar), "7", on, osp], tmp)
+    out["cw_nodes"] = nodes
+    out["cw_spec"] = spec
+    out["cw_nodes_file"] = np.frombuffer(open(on, "rb").read(), np.uint8)
+    out["cw_spec_file"] = np.frombuffer(open(osp, "rb").read(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "f0_ref.npz"), **out)
 
 
 def make_eos(tmp):

@@ -1,0 +1,136 @@
+"""The master's invert job on the GPU (snapi_cube_invert): an .f0 cube streamed through the
+device fit, against the reference's cube steps (the cube_to_invert.f0 its job writes, byte for
+byte) and against snapi_lm_fit of the same pixels (the fitted nodes, spectra, chi2)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import load_fixture
+from helpers import node_scales
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sb():
+    import snapi_b200
+    from snapi_b200 import build as b
+    b.build_cuda()
+    return snapi_b200
+
+
+@pytest.fixture(scope="module")
+def f0():
+    return load_fixture("f0_ref")
+
+
+def _setup(sb, config4):
+    from snapi_b200.eos_tables import EosTables
+    fx = config4
+    ic = float(np.abs(fx["target"][:, :, 0]).max())
+    ctx = sb.Context.from_fixture(fx, stokes_scale=ic)
+    ctx.eos_set(EosTables(load_fixture("eos_c3")))
+    return ctx
+
+
+def _subfield_pixels(f0):
+    """config-4 pixel of each subfield pixel (x major), and the subfield's size"""
+    xl, xh, yl, yh = [int(v) for v in f0["cube_sub"][:4]]
+    pix = f0["cube_pix"].reshape(4, 4)
+    sel = np.array([pix[x - 1, y - 1] for x in range(xl, xh + 1) for y in range(yl, yh + 1)])
+    return sel, xh - xl + 1, yh - yl + 1
+
+
+def test_cube_invert_matches_lm_fit(sb, config4, f0, tmp_path):
+    """float32 cube scaled by 1 / 2, 3 x 3 subfield of a 4 x 4 cube, the 201-wavelength window of
+    206, starting nodes from a model cube, chunks of 4 pixels (chunks and file rows cross)."""
+    fx = config4
+    api = sb.api
+    sub = [int(v) for v in f0["cube_sub"]]
+    cube = tmp_path / "obs.f0"
+    cube.write_bytes(bytes(f0["cube_f32_file"]))
+    sel, nx, ny = _subfield_pixels(f0)
+    kinds = fx["node_kind"]
+    npar = kinds.size
+    # model cube as the reference reads it: float32, element (x, y, p) at (p * ny + y) * nx + x
+    n0 = fx["nodes0"][sel].astype(np.float32)
+    model = np.ascontiguousarray(n0.reshape(nx, ny, npar).transpose(2, 1, 0))
+    mpath = tmp_path / "model.f0"
+    api.f0_write(str(mpath), model)
+    nlf = int(api.f0_stat(str(cube))["dims"][0])
+    mask = np.zeros(nlf, np.float32)
+    mask[sub[4] - 1:sub[5]] = fx["mask"][0]
+    qs = f0["cube_f32_qs"]
+    opts = dict(lm_start=1e3, max_iter=10, delta=1e-3)
+    ctx = _setup(sb, config4)
+    out = ctx.cube_invert(str(cube), kinds, 1e-2 * node_scales(kinds), model_path=str(mpath), subfield=sub[:4],
+                          window=sub[4:], obs_qs=qs[0], synth_qs=qs[1], mask=mask,
+                          out_nodes=str(tmp_path / "inverted_nodes.f0"),
+                          out_spectra=str(tmp_path / "inverted_spectra.f0"),
+                          out_cube=str(tmp_path / "cube_to_invert.f0"), chunk=4, **opts)
+    st = out["stats"]
+    assert (st["pixels"], st["chunks"]) == (nx * ny, 3)
+    assert st["bytes_read"] == nx * ny * 4 * nlf * 4
+    assert ctx.last_launches > 0
+    # the scaled window the job fitted is the reference's cube_to_invert.f0, byte for byte
+    assert (tmp_path / "cube_to_invert.f0").read_bytes() == bytes(f0["cube_f32_c2i"])
+    # the same pixels through snapi_lm_fit: scaling by 1 / 2 is exact, so the obs are identical
+    obs = f0["cube_f32_S"].reshape(nx * ny, 4, -1).transpose(0, 2, 1).astype(np.float32)
+    ref = ctx.lm_fit_device(n0.astype(np.float64), obs, kinds, 1e-2 * node_scales(kinds),
+                            mask=np.tile(mask[sub[4] - 1:sub[5]], (nx * ny, 1)), **opts)
+    ctx.close()
+    assert np.array_equal(out["chi2"].ravel(), ref["chi2"])
+    assert np.array_equal(out["iters"].ravel(), ref["iters"])
+    nodes = api.f0_read(str(tmp_path / "inverted_nodes.f0"))
+    assert api.f0_stat(str(tmp_path / "inverted_nodes.f0"))["dims"] == (nx, ny, npar)
+    assert np.array_equal(nodes, ref["nodes"].astype(np.float32).reshape(nx, ny, npar).transpose(2, 1, 0))
+    spec = api.f0_read(str(tmp_path / "inverted_spectra.f0"))
+    assert spec.dtype == np.float64 and spec.shape == (nx, ny, 4, obs.shape[1])
+    assert np.array_equal(spec, ref["stokes"].astype(np.float64).reshape(nx, ny, -1, 4).transpose(0, 1, 3, 2))
+
+
+def test_cube_invert_float64_cube(sb, config4, f0, tmp_path):
+    """float64 cube, scale 1.1 / 3 (not a power of two): the window the job fits is the
+    reference's to the last bit; one chunk, starting nodes of the job's model for every pixel."""
+    fx = config4
+    sub = [int(v) for v in f0["cube_sub"]]
+    cube = tmp_path / "obs64.f0"
+    cube.write_bytes(bytes(f0["cube_f64_file"]))
+    kinds = fx["node_kind"]
+    qs = f0["cube_f64_qs"]
+    ctx = _setup(sb, config4)
+    out = ctx.cube_invert(str(cube), kinds, 1e-2 * node_scales(kinds), nodes0=fx["nodes0"][0], subfield=sub[:4],
+                          window=sub[4:], obs_qs=qs[0], synth_qs=qs[1], out_cube=str(tmp_path / "c2i.f0"),
+                          max_iter=2)
+    ctx.close()
+    assert (tmp_path / "c2i.f0").read_bytes() == bytes(f0["cube_f64_c2i"])
+    assert out["stats"]["chunks"] == 1 and np.all(np.isfinite(out["chi2"]))
+
+
+def test_cube_invert_errors(sb, config4, f0, tmp_path):
+    fx = config4
+    api = sb.api
+    kinds = fx["node_kind"]
+    sub = [int(v) for v in f0["cube_sub"]]
+    cube = tmp_path / "obs.f0"
+    cube.write_bytes(bytes(f0["cube_f32_file"]))
+    ctx = _setup(sb, config4)
+    step = 1e-2 * node_scales(kinds)
+    with pytest.raises(sb.SnapiError, match="wavelengths"):   # window of 206 against a 201-point grid
+        ctx.cube_invert(str(cube), kinds, step, nodes0=fx["nodes0"][0])
+    with pytest.raises(sb.SnapiError, match="outside"):
+        ctx.cube_invert(str(cube), kinds, step, nodes0=fx["nodes0"][0], subfield=(1, 5, 1, 4), window=sub[4:])
+    bad_model = tmp_path / "m.f0"
+    api.f0_write(str(bad_model), np.zeros((9, 4, 4), np.float32))
+    with pytest.raises(sb.SnapiError, match="model cube"):
+        ctx.cube_invert(str(cube), kinds, step, model_path=str(bad_model), window=sub[4:])
+    flat = tmp_path / "flat.f0"
+    api.f0_write(str(flat), np.zeros((4, 4, 206), np.float32))
+    with pytest.raises(sb.SnapiError, match="dimensions"):
+        ctx.cube_invert(str(flat), kinds, step, nodes0=fx["nodes0"][0])
+    with pytest.raises(sb.SnapiError):
+        ctx.cube_invert(str(tmp_path / "missing.f0"), kinds, step, nodes0=fx["nodes0"][0])
+    with pytest.raises(sb.SnapiError, match="neither"):
+        ctx.cube_invert(str(cube), kinds, step, window=sub[4:])
+    ctx.close()
