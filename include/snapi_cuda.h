@@ -497,7 +497,7 @@ typedef struct {
   const char *out_nodes, *out_spectra, *out_cube;  /* NULL: not written */
   double *chi2;                  /* [nx_sub * ny_sub] final chi2 per pixel (x major), or NULL */
   int *iters;                    /* [nx_sub * ny_sub] iterations per pixel, or NULL */
-  int chunk;                     /* pixels per GPU batch (0: 16384) */
+  int chunk;                     /* pixels per GPU batch (0: 65536) */
 } snapi_cube_job;
 
 typedef struct {
