@@ -390,6 +390,15 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *model);
 int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int *active, float *records,
                         double *Nt, float *tangents, const double *step, int *pix_status, int mem);
 
+/* The columns of the node vectors as the master collects them after a fit: the 12 rows of
+ * atmosphere::return_as_array (atmos.cc:547-569) after build_from_nodes and compute_op_referent,
+ * atmos [npix][12][nd] float64: log10 tau_500, height (x3 [nd], a host array, the caller's depth
+ * grid; NULL: 0), T, gas pressure Nt k T, electron pressure n_e k T, 0, kappa at
+ * airtovac(lambda_referent), |B|, v_turb, v_z, acos(B_z / |B|), atan(B_y / B_x of the TOP depth)
+ * (the reference divides by the top depth's B_x).  active / pix_status as snapi_build_records. */
+int snapi_build_atmos(snapi_ctx *ctx, int npix, const double *nodes, const int *active, const double *x3,
+                      double *atmos, int *pix_status, int mem);
+
 /* The whole atmosphere::stokes_lm_fit (atmos_fit.cc:18-227) of npix pixels with the node -> record
  * map on the device: the loop snapi_lm_begin; { snapi_build_records of the requested node vectors of
  * the active pixels (with the reference's tangent steps); snapi_lm_step } ...; snapi_lm_result, all
@@ -485,6 +494,10 @@ const char *snapi_f0_error(void);
  *   out_spectra    inverted_spectra.f0: float64, dims (nl_win, 4, ny_sub, nx_sub), the fitted
  *                  Stokes vectors (job.cc:597)
  *   out_cube       cube_to_invert.f0: float64, the scaled window of the observation (job.cc:334)
+ *   out_atmos      inverted_atmos.f0: float64, dims (nd, ny_sub, nx_sub, 12), the columns of the
+ *                  fitted nodes as snapi_build_atmos gives them (job.cc:555-585), built from the
+ *                  returned nodes (angles polished as the reference's model is: the same columns
+ *                  for one inclination and one azimuth node)
  * The context's wavelength grid is the window ll..lh of the cube's grid. */
 typedef struct {
   const char *obs_path;
@@ -498,6 +511,8 @@ typedef struct {
   double *chi2;                  /* [nx_sub * ny_sub] final chi2 per pixel (x major), or NULL */
   int *iters;                    /* [nx_sub * ny_sub] iterations per pixel, or NULL */
   int chunk;                     /* pixels per GPU batch (0: 65536) */
+  const char *out_atmos;         /* NULL: not written */
+  const double *x3;              /* [nd] heights of the job's atmosphere for out_atmos, or NULL */
 } snapi_cube_job;
 
 typedef struct {

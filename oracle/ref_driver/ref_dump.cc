@@ -906,7 +906,7 @@ static int do_eos(const char *tskname, const char *nodesname, int npix, const ch
   delete a;
 
   // columns left by build_from_nodes
-  std::vector<double> hT, hN, hne, hk, hr;
+  std::vector<double> hT, hN, hne, hk, hr, harr;
   if (npix > 0) {
     std::vector<uint8_t> nb = read_file_bytes(nodesname);
     if ((int)(nb.size() / 8) < npix * np) { fprintf(stderr, "nodes file too short\n"); return 2; }
@@ -919,6 +919,17 @@ static int do_eos(const char *tskname, const char *nodesname, int npix, const ch
         hT.push_back(b->T[1][1][xx]); hN.push_back(b->Nt[1][1][xx]); hne.push_back(b->Ne[1][1][xx]);
         hk.push_back(b->op_referent[1][1][xx]); hr.push_back(b->rho[1][1][xx]);
       }
+      // the column as the master collects it after stokes_lm_fit's final build_from_nodes and
+      // forward evaluation (obs_stokes' set-up up to compute_op_referent; atmos_fit.cc:212-214,
+      // atmos_obs.cc:22-28, job.cc:555-557)
+      b->set_grid(b->tau_grid);
+      b->popsetup();
+      b->compute_op_referent();
+      fp_t **arr = b->return_as_array();
+      const int ndd = b->x3h - b->x3l + 1;
+      for (int q = 1; q <= 12; ++q)
+        for (int i = 1; i <= ndd; ++i) harr.push_back(arr[q][i]);
+      del_ft2dim(arr, 1, 12, 1, ndd);
       delete b;
     }
   }
@@ -960,6 +971,7 @@ static int do_eos(const char *tskname, const char *nodesname, int npix, const ch
     w.put("he_ne", {npix, nd}, hne.data());
     w.put("he_kap", {npix, nd}, hk.data());
     w.put("he_rho", {npix, nd}, hr.data());
+    w.put("atm_arr", {npix, 12, nd}, harr.data());
   }
   delete[] (lv + 1);
   delete m;

@@ -108,6 +108,8 @@ class CubeJob(ctypes.Structure):
         ("chi2", ctypes.c_void_p),
         ("iters", ctypes.c_void_p),
         ("chunk", ctypes.c_int),
+        ("out_atmos", ctypes.c_char_p),
+        ("x3", ctypes.c_void_p),
     ]
 
 
@@ -144,6 +146,7 @@ def lib():
         L.snapi_spectral_broaden.argtypes = [vp, ip, fp, ctypes.c_double, ip]
         L.snapi_eos_set.argtypes = [vp, vp]
         L.snapi_build_records.argtypes = [vp, ip, fp, fp, fp, fp, fp, fp, fp, ip]
+        L.snapi_build_atmos.argtypes = [vp, ip, fp, fp, fp, fp, fp, ip]
         L.snapi_lm_fit.argtypes = [vp, ip, ctypes.POINTER(SnapiLmOpts), fp, fp, fp, fp, fp, fp, fp, fp,
                                    ctypes.POINTER(ctypes.c_int), ip]
         L.snapi_zeeman_pattern.argtypes = [ip, ip, ctypes.c_double, ctypes.c_double, ctypes.POINTER(SnapiLine)]
@@ -451,8 +454,8 @@ class Context:
 
     def cube_invert(self, obs_path, node_kind, resp_step, nodes0=None, model_path=None, subfield=(0, 0, 0, 0),
                     window=(0, 0), obs_qs=0.0, synth_qs=0.0, mask=None, w_stokes=(1.0, 1.0, 1.0, 1.0),
-                    out_nodes=None, out_spectra=None, out_cube=None, chunk=0, lm_start=1e3, max_iter=30, delta=1e-3,
-                    stopping_chisq=1e-30, spectral_broadening=0.0):
+                    out_nodes=None, out_spectra=None, out_cube=None, out_atmos=None, x3=None, chunk=0, lm_start=1e3,
+                    max_iter=30, delta=1e-3, stopping_chisq=1e-30, spectral_broadening=0.0):
         """The master's invert job over an .f0 cube (snapi_cube_invert; needs eos_set).  subfield
         (xl, xh, yl, yh) and window (ll, lh) are 1-based inclusive, 0 = the cube's extent.  Returns the
         per-pixel chi2 and iterations (x major) and the job's statistics."""
@@ -473,9 +476,10 @@ class Context:
         chi2 = np.zeros(max(nx * ny, 1))
         iters = np.zeros(max(nx * ny, 1), np.int32)
         enc = lambda p: None if p is None else os.fsencode(p)
+        h3 = None if x3 is None else np.ascontiguousarray(x3, dtype=np.float64)
         job = CubeJob(os.fsencode(obs_path), xl, xh, yl, yh, window[0], window[1], float(obs_qs), float(synth_qs),
                       _ptr(n0), enc(model_path), _ptr(mk), _ptr(ws), enc(out_nodes), enc(out_spectra), enc(out_cube),
-                      _ptr(chi2), _ptr(iters), int(chunk))
+                      _ptr(chi2), _ptr(iters), int(chunk), enc(out_atmos), _ptr(h3))
         stats = CubeStats()
         self._check(lib().snapi_cube_invert(self._ctx, ctypes.byref(opts), ctypes.byref(job), ctypes.byref(stats)))
         return {"chi2": chi2.reshape(nx, ny), "iters": iters.reshape(nx, ny),
@@ -527,6 +531,19 @@ class Context:
         self._check(lib().snapi_build_records(self._ctx, npix, _ptr(nodes), _ptr(act), _ptr(rec), _ptr(nt), _ptr(tan),
                                               _ptr(stp), _ptr(status), MEM_HOST))
         return rec, tan, nt, status
+
+    def build_atmos(self, nodes, x3=None, active=None):
+        """The 12 return_as_array rows of each node vector's column (snapi_build_atmos):
+        atmos [npix][12][nd] float64 and the per-pixel status."""
+        n = np.ascontiguousarray(nodes, dtype=np.float64)
+        npix = n.shape[0]
+        atm = np.zeros((npix, 12, self.nd))
+        st = np.zeros(npix, np.int32)
+        act = None if active is None else np.ascontiguousarray(active, dtype=np.int32)
+        h3 = None if x3 is None else np.ascontiguousarray(x3, dtype=np.float64)
+        self._check(lib().snapi_build_atmos(self._ctx, npix, _ptr(n), _ptr(act), _ptr(h3), _ptr(atm), _ptr(st),
+                                            MEM_HOST))
+        return atm, st
 
     def build_records_device(self, npix, nodes_ptr, rec_ptr, tan_ptr=0, active_ptr=0, status_ptr=0):
         """build_records on device pointers (int addresses, e.g. torch .data_ptr())."""

@@ -7,7 +7,8 @@
 // writing it to cube_to_invert.f0; pack one task per pixel with its starting model (the job's
 // model, or model_cube[x][y] of a model cube, job.cc:347-369) for the islaves, which run
 // stokes_lm_fit; collect the fitted nodes and spectra and write inverted_nodes.f0 (write_file 3-D,
-// fileio.cc:279-292) and inverted_spectra.f0 (write_file 4-D, fileio.cc:318-329).
+// fileio.cc:279-292), inverted_atmos.f0 (the 12 return_as_array rows of each fitted column) and
+// inverted_spectra.f0 (write_file 4-D, fileio.cc:318-329).
 //
 // Here one batch ("chunk") of subfield pixels at a time travels as a contiguous run of file rows:
 // the file stores each pixel's [4][nl] block contiguously (dims (nl, 4, ny, nx)), so a chunk of
@@ -71,6 +72,17 @@ __global__ void k_cube_spectra(const float *__restrict__ stokes, int npix, int n
   }
 }
 
+// atm [npix][12][nd] -> out [12][npix][nd] (the chunk's part of inverted_atmos.f0's rows)
+__global__ void k_cube_atm(const double *__restrict__ atm, int npix, int nd, double *__restrict__ out) {
+  const long long n = (long long)npix * 12 * nd;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(o % nd);
+    const long long t = o / nd;
+    const int p = (int)(t % npix), k = (int)(t / npix);
+    out[o] = atm[((size_t)p * 12 + k) * nd + z];
+  }
+}
+
 // the window of the wavelength weights, repeated for every pixel of a chunk
 __global__ void k_cube_mask(const float *__restrict__ m, int npix, int nl, float *__restrict__ out) {
   const long long n = (long long)npix * nl;
@@ -126,14 +138,16 @@ struct Job {
   void *d_raw = nullptr;
   float *d_obs = nullptr, *d_stokes = nullptr, *d_mask = nullptr, *d_maskwin = nullptr;
   double *d_win = nullptr, *d_spec = nullptr, *d_nodes0 = nullptr, *d_nodes = nullptr, *d_chi2 = nullptr;
+  double *d_atm = nullptr, *d_atmT = nullptr;
   int *d_iters = nullptr;
   // pinned host buffers
   double *h_nodes0 = nullptr, *h_nodes = nullptr, *h_chi2 = nullptr;
   int *h_iters = nullptr;
   Handoff rd, wr;
-  size_t raw_bytes = 0, spec_bytes = 0;
+  size_t raw_bytes = 0, spec_bytes = 0, atm_bytes = 0;
+  int nd = 0;
   bool want_win = false;
-  snapi_f0_file *f_spec = nullptr, *f_cube = nullptr;
+  snapi_f0_file *f_spec = nullptr, *f_cube = nullptr, *f_atm = nullptr;
   std::vector<double> model;      // model cube, float64, file order
   long long mdim0 = 0, mdim1 = 0;
   std::vector<float> node_cube;   // [npar][ny][nx]
@@ -142,13 +156,15 @@ struct Job {
   ~Job() {
     if (fd >= 0) close(fd);
     for (void *p : {(void *)d_raw, (void *)d_obs, (void *)d_stokes, (void *)d_mask, (void *)d_maskwin, (void *)d_win,
-                    (void *)d_spec, (void *)d_nodes0, (void *)d_nodes, (void *)d_chi2, (void *)d_iters})
+                    (void *)d_spec, (void *)d_nodes0, (void *)d_nodes, (void *)d_chi2, (void *)d_iters,
+                    (void *)d_atm, (void *)d_atmT})
       if (p) cudaFree(p);
     for (void *p : {(void *)h_nodes0, (void *)h_nodes, (void *)h_chi2, (void *)h_iters, (void *)rd.slot[0].h,
                     (void *)rd.slot[1].h, (void *)wr.slot[0].h, (void *)wr.slot[1].h})
       if (p) cudaFreeHost(p);
     if (f_spec) snapi_f0_close(f_spec);
     if (f_cube) snapi_f0_close(f_cube);
+    if (f_atm) snapi_f0_close(f_atm);
   }
 
   int chunk_len(int k) const {
@@ -184,7 +200,8 @@ struct Job {
     }
   }
 
-  // writer thread: the chunk's float64 spectra (and window) at its pixels' place in the files
+  // writer thread: the chunk's float64 spectra (and window, and atmosphere rows) at its pixels'
+  // place in the files
   void writer() {
     const long long pix_elems = 4LL * nl;
     for (int k = 0; k < nchunk; ++k) {
@@ -192,6 +209,14 @@ struct Job {
       Handoff::Slot &s = wr.slot[k & 1];
       const double *spec = (const double *)s.h;
       const double *win = spec + (size_t)chunk * pix_elems;
+      const double *atm = (const double *)(s.h + spec_bytes * (want_win ? 2 : 1));
+      if (f_atm)  // row q of inverted_atmos.f0 holds [x][y][z]: this chunk's pixels are one run
+        for (int q = 0; q < 12; ++q)
+          if (snapi_f0_write_at(f_atm, ((long long)q * npix + s.p0) * nd, (long long)s.n * nd,
+                                atm + (size_t)q * s.n * nd)) {
+            wr.fail(std::string("snapi_cube_invert: ") + snapi_f0_error());
+            return;
+          }
       if (f_spec && snapi_f0_write_at(f_spec, s.p0 * pix_elems, s.n * pix_elems, spec)) {
         wr.fail(std::string("snapi_cube_invert: ") + snapi_f0_error());
         return;
@@ -200,7 +225,8 @@ struct Job {
         wr.fail(std::string("snapi_cube_invert: ") + snapi_f0_error());
         return;
       }
-      bytes_written += (long long)s.n * pix_elems * 8 * ((f_spec ? 1 : 0) + (f_cube ? 1 : 0));
+      bytes_written += (long long)s.n * pix_elems * 8 * ((f_spec ? 1 : 0) + (f_cube ? 1 : 0)) +
+                       (f_atm ? (long long)s.n * 12 * nd * 8 : 0);
       wr.set(k, false);
     }
   }
@@ -270,8 +296,10 @@ extern "C" int snapi_cube_invert(snapi_ctx *ctx, const snapi_lm_opts *opts, cons
   }
   const int C = J.chunk, nl = J.nl, npar = J.npar;
   J.want_win = job->out_cube != nullptr;
+  J.nd = ctx->nd;
   J.raw_bytes = (size_t)C * 4 * J.nl_full * J.esz;
   J.spec_bytes = (size_t)C * 4 * nl * sizeof(double);
+  J.atm_bytes = job->out_atmos ? (size_t)C * 12 * J.nd * sizeof(double) : 0;
   SNAPI_CK(cudaSetDevice(ctx->device));
   SNAPI_CK(cudaMalloc(&J.d_raw, J.raw_bytes));
   SNAPI_CK(cudaMalloc(&J.d_obs, sizeof(float) * (size_t)C * nl * 4));
@@ -282,13 +310,18 @@ extern "C" int snapi_cube_invert(snapi_ctx *ctx, const snapi_lm_opts *opts, cons
   SNAPI_CK(cudaMalloc(&J.d_nodes, sizeof(double) * (size_t)C * npar));
   SNAPI_CK(cudaMalloc(&J.d_chi2, sizeof(double) * (size_t)C));
   SNAPI_CK(cudaMalloc(&J.d_iters, sizeof(int) * (size_t)C));
+  if (J.atm_bytes) {
+    SNAPI_CK(cudaMalloc(&J.d_atm, J.atm_bytes));
+    SNAPI_CK(cudaMalloc(&J.d_atmT, J.atm_bytes));
+  }
   SNAPI_CK(cudaHostAlloc((void **)&J.h_nodes0, sizeof(double) * (size_t)C * npar, cudaHostAllocDefault));
   SNAPI_CK(cudaHostAlloc((void **)&J.h_nodes, sizeof(double) * (size_t)C * npar, cudaHostAllocDefault));
   SNAPI_CK(cudaHostAlloc((void **)&J.h_chi2, sizeof(double) * (size_t)C, cudaHostAllocDefault));
   SNAPI_CK(cudaHostAlloc((void **)&J.h_iters, sizeof(int) * (size_t)C, cudaHostAllocDefault));
   for (int i = 0; i < 2; ++i) {
     SNAPI_CK(cudaHostAlloc((void **)&J.rd.slot[i].h, J.raw_bytes, cudaHostAllocDefault));
-    SNAPI_CK(cudaHostAlloc((void **)&J.wr.slot[i].h, J.spec_bytes * (J.want_win ? 2 : 1), cudaHostAllocDefault));
+    SNAPI_CK(cudaHostAlloc((void **)&J.wr.slot[i].h, J.spec_bytes * (J.want_win ? 2 : 1) + J.atm_bytes,
+                           cudaHostAllocDefault));
   }
   double ker_ms = 0.0;
   int launches = 0;
@@ -311,6 +344,11 @@ extern "C" int snapi_cube_invert(snapi_ctx *ctx, const snapi_lm_opts *opts, cons
     const long long dims[4] = {nl, 4, J.ny, J.nx};
     J.f_cube = snapi_f0_create(job->out_cube, SNAPI_F0_FLOAT64, 4, dims, nullptr, &st);
     if (!J.f_cube) return set_err(ctx, SNAPI_EINVAL, "snapi_cube_invert: %s", snapi_f0_error());
+  }
+  if (job->out_atmos) {
+    const long long dims[4] = {J.nd, J.ny, J.nx, 12};
+    J.f_atm = snapi_f0_create(job->out_atmos, SNAPI_F0_FLOAT64, 4, dims, nullptr, &st);
+    if (!J.f_atm) return set_err(ctx, SNAPI_EINVAL, "snapi_cube_invert: %s", snapi_f0_error());
   }
   if (job->out_nodes) J.node_cube.assign((size_t)npar * J.npix, 0.0f);
 
@@ -368,6 +406,12 @@ extern "C" int snapi_cube_invert(snapi_ctx *ctx, const snapi_lm_opts *opts, cons
     ker_ms += ctx->last_ms;
     launches += ctx->last_launches;
     lm_steps += steps;
+    if (J.atm_bytes) {  // the fitted columns (job.cc:555-557)
+      st = snapi_build_atmos(ctx, n, J.d_nodes, nullptr, job->x3, J.d_atm, nullptr, SNAPI_MEM_DEVICE);
+      if (st) return stop(st);
+      ker_ms += ctx->last_ms;
+      launches += ctx->last_launches;
+    }
     if (!J.wr.wait(k, false, &write_wait)) {
       std::string e = J.wr.err;
       return stop(set_err(ctx, SNAPI_EINVAL, "%s", e.c_str()));
@@ -376,12 +420,20 @@ extern "C" int snapi_cube_invert(snapi_ctx *ctx, const snapi_lm_opts *opts, cons
     CUBE_CK(cudaEventRecord(ctx->ev0, ctx->stream));
     k_cube_spectra<<<grid_for((long long)n * nl * 4), kThreads, 0, ctx->stream>>>(J.d_stokes, n, nl, J.d_spec);
     CUBE_CK(cudaGetLastError());
-    CUBE_CK(cudaEventRecord(ctx->ev1, ctx->stream));
     ++launches;
+    if (J.atm_bytes) {
+      k_cube_atm<<<grid_for((long long)n * 12 * J.nd), kThreads, 0, ctx->stream>>>(J.d_atm, n, J.nd, J.d_atmT);
+      CUBE_CK(cudaGetLastError());
+      ++launches;
+    }
+    CUBE_CK(cudaEventRecord(ctx->ev1, ctx->stream));
     CUBE_CK(cudaMemcpyAsync(ws.h, J.d_spec, sizeof(double) * (size_t)n * 4 * nl, cudaMemcpyDeviceToHost, ctx->stream));
     if (J.want_win)
       CUBE_CK(cudaMemcpyAsync(ws.h + J.spec_bytes, J.d_win, sizeof(double) * (size_t)n * 4 * nl,
                               cudaMemcpyDeviceToHost, ctx->stream));
+    if (J.atm_bytes)
+      CUBE_CK(cudaMemcpyAsync(ws.h + J.spec_bytes * (J.want_win ? 2 : 1), J.d_atmT,
+                              sizeof(double) * (size_t)n * 12 * J.nd, cudaMemcpyDeviceToHost, ctx->stream));
     CUBE_CK(cudaMemcpyAsync(J.h_nodes, J.d_nodes, sizeof(double) * (size_t)n * npar, cudaMemcpyDeviceToHost,
                             ctx->stream));
     CUBE_CK(cudaMemcpyAsync(J.h_chi2, J.d_chi2, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
@@ -415,6 +467,7 @@ extern "C" int snapi_cube_invert(snapi_ctx *ctx, const snapi_lm_opts *opts, cons
   if (!J.rd.err.empty()) return set_err(ctx, SNAPI_EINVAL, "%s", J.rd.err.c_str());
   if (J.f_spec) { snapi_f0_file *f = J.f_spec; J.f_spec = nullptr; if (snapi_f0_close(f)) st = SNAPI_EINVAL; }
   if (J.f_cube) { snapi_f0_file *f = J.f_cube; J.f_cube = nullptr; if (snapi_f0_close(f)) st = SNAPI_EINVAL; }
+  if (J.f_atm) { snapi_f0_file *f = J.f_atm; J.f_atm = nullptr; if (snapi_f0_close(f)) st = SNAPI_EINVAL; }
   if (st) return set_err(ctx, st, "snapi_cube_invert: %s", snapi_f0_error());
   if (job->out_nodes) {
     const long long dims[3] = {J.nx, J.ny, npar};

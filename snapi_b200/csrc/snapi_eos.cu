@@ -757,6 +757,49 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_rec(EosArgs A) {
   if (st) atomicOr(A.status + p, st);
 }
 
+// atmosphere::return_as_array (atmos.cc:547-569) of the variant-0 columns, as the master collects
+// them after stokes_lm_fit's final build_from_nodes and compute_op_referent: one thread per
+// (depth, pixel); atm [npix][12][nd]
+__global__ void __launch_bounds__(kRecThreads) k_eos_atm(EosArgs A, const double *x3, double *atm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.npix * A.nd) return;
+  const int p = i % A.npix, x = i / A.npix;
+  if (A.active && !A.active[p]) return;
+  const EosDev &E = *A.tab;
+  const double *F0 = A.F + ((size_t)p * A.nvar * A.nd + x) * A.nf;  // variant 0
+  const double T = F0[0], Ne = F0[2], kap = F0[7], Nt = A.Nt[(size_t)p * A.nvar * A.nd + x];
+  NodeView nv{A.nodes + (size_t)p * A.npar, -1, 0.0};
+  // build_from_nodes' magnetic vector (atmos_pp.cc:169-173); the azimuth row divides by the top
+  // depth's Bx (atmos.cc:566)
+  auto bvec = [&](int xx, double &bx, double &by, double &bz) {
+    const double B = interp_kind(E, nv, 4, xx, true), th = interp_kind(E, nv, 5, xx, true);
+    const double ph = interp_kind(E, nv, 6, xx, true);
+    bx = B * sin(th) * cos(ph);
+    by = B * sin(th) * sin(ph);
+    bz = B * cos(th);
+  };
+  double bx, by, bz, bx0, by0, bz0;
+  bvec(x, bx, by, bz);
+  bvec(0, bx0, by0, bz0);
+  const double mg = sqrt(bx * bx + by * by + bz * bz);
+  const double tau = -pow(10.0, logtau(E, x));  // tau_referent as build_from_nodes stores it
+  double r[12];
+  r[0] = log10(-tau);
+  r[1] = x3 ? x3[x] : 0.0;
+  r[2] = T;
+  r[3] = Nt * cK * T;
+  r[4] = Ne * cK * T;
+  r[5] = 0.0;
+  r[6] = kap;
+  r[7] = mg;
+  r[8] = interp_kind(E, nv, 2, x, true);
+  r[9] = interp_kind(E, nv, 3, x, true);
+  r[10] = acos(bz / mg);
+  r[11] = atan(by / bx0);
+  double *o = atm + (size_t)p * 12 * A.nd + x;
+  for (int k = 0; k < 12; ++k) o[(size_t)k * A.nd] = r[k];
+}
+
 // ---- host side ---------------------------------------------------------------------------------------------
 struct EosCtx {
   EosDev *d_tab = nullptr;
@@ -769,6 +812,9 @@ struct EosCtx {
   double *d_F = nullptr;
   int *d_active = nullptr, *d_status = nullptr;
   float *d_rec = nullptr, *d_tan = nullptr;
+  // return_as_array rows of snapi_build_atmos (cap_atm pixels) and the caller's heights
+  double *d_atm = nullptr, *d_x3 = nullptr;
+  int cap_atm = 0;
 };
 
 void eos_free_bufs(EosCtx *e) {
@@ -779,6 +825,10 @@ void eos_free_bufs(EosCtx *e) {
   e->d_active = e->d_status = nullptr;
   e->d_rec = e->d_tan = nullptr;
   e->cap = e->cap_var = 0;
+  cudaFree(e->d_atm);
+  cudaFree(e->d_x3);
+  e->d_atm = e->d_x3 = nullptr;
+  e->cap_atm = 0;
 }
 
 }  // namespace
@@ -1055,14 +1105,12 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
   return SNAPI_OK;
 }
 
-int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int *active, float *records, double *Nt,
-                        float *tangents, const double *step, int *pix_status, int mem) {
+// snapi_build_records (records != NULL) and snapi_build_atmos (atmos != NULL; x3 a host array)
+static int build_impl(snapi_ctx *ctx, int npix, const double *nodes, const int *active, float *records, double *Nt,
+                      float *tangents, const double *step, int *pix_status, int mem, const double *x3,
+                      double *atmos) {
   using namespace snapi;
-  if (!ctx) return SNAPI_EINVAL;
   EosCtx *e = static_cast<EosCtx *>(ctx->eos);
-  if (!e) return set_err(ctx, SNAPI_EINVAL, "snapi_build_records: no node model (snapi_eos_set)");
-  if (npix < 0 || (npix > 0 && (!nodes || !records)) || (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
-    return set_err(ctx, SNAPI_EINVAL, "snapi_build_records: invalid arguments");
   if (npix == 0) return SNAPI_OK;
   const int npar = e->npar, nd = ctx->nd, nf = ctx->nfield;
   const int nvar = tangents ? 1 + 2 * e->ntherm : 1;
@@ -1093,6 +1141,17 @@ int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int
     e->cap = B;
     e->cap_var = nvar;
   }
+  if (atmos && B > e->cap_atm) {
+    cudaFree(e->d_atm);
+    e->d_atm = nullptr;
+    e->cap_atm = 0;
+    SNAPI_CK(cudaMalloc(&e->d_atm, sizeof(double) * (size_t)B * 12 * nd));
+    e->cap_atm = B;
+  }
+  if (atmos && x3) {
+    if (!e->d_x3) SNAPI_CK(cudaMalloc(&e->d_x3, sizeof(double) * nd));
+    SNAPI_CK(cudaMemcpyAsync(e->d_x3, x3, sizeof(double) * nd, cudaMemcpyHostToDevice, ctx->stream));
+  }
   SNAPI_CK(cudaMemcpyAsync(e->d_step, hstep.data(), sizeof(double) * npar, cudaMemcpyHostToDevice, ctx->stream));
   ctx->last_ms = 0.0;
   ctx->last_launches = 0;
@@ -1118,12 +1177,16 @@ int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int
         SNAPI_CK(cudaMemcpyAsync(e->d_active, active + p0, sizeof(int) * nb, cudaMemcpyHostToDevice, ctx->stream));
       A.nodes = e->d_nodes;
       A.active = active ? e->d_active : nullptr;
-      A.rec = e->d_rec;
+      A.rec = records ? e->d_rec : nullptr;
       A.tan = tangents ? e->d_tan : nullptr;
       A.Nt_out = Nt ? e->d_Ntout : nullptr;
       if (active) {  // rows of inactive pixels are left untouched: start from the caller's
-        SNAPI_CK(cudaMemcpyAsync(e->d_rec, records + (size_t)p0 * nd * nf, sizeof(float) * nb * nd * nf,
-                                 cudaMemcpyHostToDevice, ctx->stream));
+        if (records)
+          SNAPI_CK(cudaMemcpyAsync(e->d_rec, records + (size_t)p0 * nd * nf, sizeof(float) * nb * nd * nf,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+        if (atmos)
+          SNAPI_CK(cudaMemcpyAsync(e->d_atm, atmos + (size_t)p0 * 12 * nd, sizeof(double) * nb * 12 * nd,
+                                   cudaMemcpyHostToDevice, ctx->stream));
         if (tangents)
           SNAPI_CK(cudaMemcpyAsync(e->d_tan, tangents + (size_t)p0 * npar * nd * nf,
                                    sizeof(float) * nb * npar * nd * nf, cudaMemcpyHostToDevice, ctx->stream));
@@ -1134,7 +1197,7 @@ int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int
     } else {
       A.nodes = nodes + (size_t)p0 * npar;
       A.active = active ? active + p0 : nullptr;
-      A.rec = records + (size_t)p0 * nd * nf;
+      A.rec = records ? records + (size_t)p0 * nd * nf : nullptr;
       A.tan = tangents ? tangents + (size_t)p0 * npar * nd * nf : nullptr;
       A.Nt_out = Nt ? Nt + (size_t)p0 * nd : nullptr;
     }
@@ -1147,13 +1210,27 @@ int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int
     k_eos_var<<<(unsigned)((nvx + kRecThreads - 1) / kRecThreads), kRecThreads, 0, ctx->stream>>>(A);
     SNAPI_CK(cudaGetLastError());
     const int nrec = nb * nd;
-    k_eos_rec<<<(nrec + kRecThreads - 1) / kRecThreads, kRecThreads, 0, ctx->stream>>>(A);
-    SNAPI_CK(cudaGetLastError());
+    ctx->last_launches += 2;
+    if (records) {
+      k_eos_rec<<<(nrec + kRecThreads - 1) / kRecThreads, kRecThreads, 0, ctx->stream>>>(A);
+      SNAPI_CK(cudaGetLastError());
+      ++ctx->last_launches;
+    }
+    if (atmos) {
+      double *atm_out = host ? e->d_atm : atmos + (size_t)p0 * 12 * nd;
+      k_eos_atm<<<(nrec + kRecThreads - 1) / kRecThreads, kRecThreads, 0, ctx->stream>>>(A, x3 ? e->d_x3 : nullptr,
+                                                                                        atm_out);
+      SNAPI_CK(cudaGetLastError());
+      ++ctx->last_launches;
+    }
     SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    ctx->last_launches += 3;
-    if (host) {
-      SNAPI_CK(cudaMemcpyAsync(records + (size_t)p0 * nd * nf, e->d_rec, sizeof(float) * nb * nd * nf,
+    if (host && atmos)
+      SNAPI_CK(cudaMemcpyAsync(atmos + (size_t)p0 * 12 * nd, e->d_atm, sizeof(double) * nb * 12 * nd,
                                cudaMemcpyDeviceToHost, ctx->stream));
+    if (host) {
+      if (records)
+        SNAPI_CK(cudaMemcpyAsync(records + (size_t)p0 * nd * nf, e->d_rec, sizeof(float) * nb * nd * nf,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
       if (tangents)
         SNAPI_CK(cudaMemcpyAsync(tangents + (size_t)p0 * npar * nd * nf, e->d_tan, sizeof(float) * nb * npar * nd * nf,
                                  cudaMemcpyDeviceToHost, ctx->stream));
@@ -1170,6 +1247,24 @@ int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int
     ctx->last_ms += ms;
   }
   return SNAPI_OK;
+}
+
+int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int *active, float *records, double *Nt,
+                        float *tangents, const double *step, int *pix_status, int mem) {
+  if (!ctx) return SNAPI_EINVAL;
+  if (!ctx->eos) return snapi::set_err(ctx, SNAPI_EINVAL, "snapi_build_records: no node model (snapi_eos_set)");
+  if (npix < 0 || (npix > 0 && (!nodes || !records)) || (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
+    return snapi::set_err(ctx, SNAPI_EINVAL, "snapi_build_records: invalid arguments");
+  return build_impl(ctx, npix, nodes, active, records, Nt, tangents, step, pix_status, mem, nullptr, nullptr);
+}
+
+int snapi_build_atmos(snapi_ctx *ctx, int npix, const double *nodes, const int *active, const double *x3,
+                      double *atmos, int *pix_status, int mem) {
+  if (!ctx) return SNAPI_EINVAL;
+  if (!ctx->eos) return snapi::set_err(ctx, SNAPI_EINVAL, "snapi_build_atmos: no node model (snapi_eos_set)");
+  if (npix < 0 || (npix > 0 && (!nodes || !atmos)) || (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
+    return snapi::set_err(ctx, SNAPI_EINVAL, "snapi_build_atmos: invalid arguments");
+  return build_impl(ctx, npix, nodes, active, nullptr, nullptr, nullptr, nullptr, pix_status, mem, x3, atmos);
 }
 
 }  // extern "C"

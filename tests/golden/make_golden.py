@@ -16,7 +16,8 @@ its 80-depth atmosphere file from REF and runs oracle/_ref/snapi_ref_dump).  Wri
                                   benchmark tiles over its 64x64 pixels
   tests/golden/eos_c1.npz, eos_c3.npz  (--only-eos) node-model tables of the c1 / c3 tasks, the
                                   reference's chemistry on a (T, Nt) grid and the columns its
-                                  build_from_nodes leaves for the config-1/2 and config-3 nodes
+                                  build_from_nodes leaves for the config-1/2 and config-3 nodes,
+                                  with the 12 return_as_array rows of each (atm_arr)
   tests/golden/config4_256.npz    (--only-c4-subset 256) the config-4 fit of 256 seeded pixels
                                   (seed 404) by the reference's stokes_lm_fit
   tests/golden/f0_ref.npz         (--only-f0) ANA .f0 files written by the reference's ana_fzwrite

@@ -90,6 +90,36 @@ def test_cube_invert_matches_lm_fit(sb, config4, f0, tmp_path):
     assert np.array_equal(spec, ref["stokes"].astype(np.float64).reshape(nx, ny, -1, 4).transpose(0, 1, 3, 2))
 
 
+def test_cube_invert_atmosphere_cube(sb, config4, f0, tmp_path):
+    """inverted_atmos.f0: the 12 return_as_array rows of every fitted column, dims (nd, ny, nx, 12),
+    equal to snapi_build_atmos of the nodes snapi_lm_fit returns for the same pixels; heights passed
+    through."""
+    fx = config4
+    api = sb.api
+    sub = [int(v) for v in f0["cube_sub"]]
+    cube = tmp_path / "obs.f0"
+    cube.write_bytes(bytes(f0["cube_f32_file"]))
+    sel, nx, ny = _subfield_pixels(f0)
+    kinds = fx["node_kind"]
+    x3 = np.linspace(1.5e8, -8e6, fx["tau500"].size)
+    opts = dict(lm_start=1e3, max_iter=3, delta=1e-3)
+    ctx = _setup(sb, config4)
+    out = ctx.cube_invert(str(cube), kinds, 1e-2 * node_scales(kinds), nodes0=fx["nodes0"][0], subfield=sub[:4],
+                          window=sub[4:], obs_qs=2.0, synth_qs=1.0, out_atmos=str(tmp_path / "inverted_atmos.f0"),
+                          x3=x3, chunk=4, **opts)
+    assert out["stats"]["chunks"] == 3
+    h = api.f0_stat(str(tmp_path / "inverted_atmos.f0"))
+    assert h["type"] == api.F0_FLOAT64 and h["dims"] == (x3.size, ny, nx, 12)
+    atm = api.f0_read(str(tmp_path / "inverted_atmos.f0"))  # [12][nx][ny][nd]
+    obs = f0["cube_f32_S"].reshape(nx * ny, 4, -1).transpose(0, 2, 1).astype(np.float32)
+    fit = ctx.lm_fit_device(np.tile(fx["nodes0"][0], (nx * ny, 1)), obs, kinds, 1e-2 * node_scales(kinds), **opts)
+    ref, st = ctx.build_atmos(fit["nodes"], x3=x3)
+    ctx.close()
+    assert np.all(st == 0)
+    assert np.array_equal(atm.transpose(1, 2, 0, 3).reshape(nx * ny, 12, -1), ref)
+    assert np.array_equal(atm[1], np.broadcast_to(x3, (nx, ny, x3.size)))
+
+
 def test_cube_invert_float64_cube(sb, config4, f0, tmp_path):
     """float64 cube, scale 1.1 / 3 (not a power of two): the window the job fits is the
     reference's to the last bit; one chunk, starting nodes of the job's model for every pixel."""

@@ -161,6 +161,31 @@ def test_gpu_dense_temperature_nodes(oracle_lib, eos1, config1, config2):
 
 @pytest.mark.gpu
 @pytestmark_gpu
+@pytest.mark.parametrize("name", ["eos_c3", "eos_c1"])
+def test_gpu_atmosphere_rows_vs_reference(oracle_lib, name, config3, config1):
+    """snapi_build_atmos against the reference's return_as_array after build_from_nodes and
+    compute_op_referent (the columns the master writes to inverted_atmos.f0), for the config-3
+    node vectors and the 80-temperature-node config-1/2 ones, heights taken from the reference."""
+    d = load_fixture(name)
+    fx = config3 if name == "eos_c3" else config1
+    ctx = _gpu_ctx(fx, d)
+    ref = d["atm_arr"]
+    atm, status = ctx.build_atmos(d["nodes"], x3=ref[0, 1])
+    ctx.close()
+    assert np.all(status == 0)
+    assert atm.shape == ref.shape
+    np.testing.assert_array_equal(atm[:, 5], 0.0)
+    np.testing.assert_allclose(atm[:, 0], ref[:, 0], rtol=0, atol=1e-14)          # log10 tau
+    np.testing.assert_array_equal(atm[:, 1], ref[:, 1])                           # heights
+    np.testing.assert_allclose(atm[:, 2], ref[:, 2], rtol=1e-13)                   # T
+    np.testing.assert_allclose(atm[:, 3], ref[:, 3], rtol=1e-10)                   # Nt k T
+    np.testing.assert_allclose(atm[:, [4, 6]], ref[:, [4, 6]], rtol=1e-9)          # n_e k T, kappa
+    np.testing.assert_allclose(atm[:, 7:10], ref[:, 7:10], rtol=1e-13, atol=1e-9)  # |B|, v_turb, v_z
+    np.testing.assert_allclose(atm[:, 10:], ref[:, 10:], rtol=0, atol=1e-12)       # angles
+
+
+@pytest.mark.gpu
+@pytestmark_gpu
 def test_gpu_active_rows_untouched_and_batches(oracle_lib, eos3, config3):
     """Inactive pixels keep the caller's rows; several device batches give the same records."""
     nodes = np.concatenate([config3["nodes"]] * 3)
