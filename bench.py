@@ -327,6 +327,7 @@ def run_snapi(args):
         line["node_build"] = bench_build(sb, pool, local)
         line["lm_device_build"] = bench_lm_device(sb, pool, ic, local)
         line["ali"] = bench_ali(sb, local, cpu=not args.no_cpu_baseline)
+        line["cube_invert"] = bench_cube(sb, pool, ic, local, n=64)
     ctx.close()
     if world > 1:
         import torch.distributed as dist

@@ -664,6 +664,34 @@ int sne_build(const snapi_eos_model *m, int nd, int nlines, const double *lam0, 
   return c.status;
 }
 
+/* The 12 rows of atmosphere::return_as_array (atmos.cc:547-569) of the node vector's column after
+ * build_from_nodes and compute_op_referent (atmos_ppbez_rts.cc:268-281): out [12][nd]; x3 [nd]
+ * the heights (NULL: 0).  Returns the status bits as sne_build. */
+int sne_atmos(const snapi_eos_model *m, int nd, const double *nodes, const double *x3, double *out) {
+  static column c;
+  if (nd > MAXD || nd < 2) return -1;
+  c.status = 0;
+  interp_all(m, nd, nodes, &c, 1);
+  hydrostatic(m, nd, &c);
+  const double bx0 = c.B[0] * sin(c.th[0]) * cos(c.ph[0]);
+  for (int x = 0; x < nd; ++x) {
+    chem_state cs;
+    pops P;
+    cs.Ne = 1.0;
+    const double kap = chem_point(m, c.T[x], c.Nt[x], &cs, &P, 1);
+    if (cs.passes < 0) c.status |= 1;
+    const double Bx = c.B[x] * sin(c.th[x]) * cos(c.ph[x]);
+    const double By = c.B[x] * sin(c.th[x]) * sin(c.ph[x]);
+    const double Bz = c.B[x] * cos(c.th[x]);
+    const double mg = sqrt(Bx * Bx + By * By + Bz * Bz);
+    const double tau = -pow(10.0, c.lt[x]);
+    double r[12] = {log10(-tau), x3 ? x3[x] : 0.0, c.T[x], c.Nt[x] * C_K * c.T[x], cs.Ne * C_K * c.T[x], 0.0, kap,
+                    mg, c.vt[x], c.vz[x], acos(Bz / mg), atan(By / bx0)};
+    for (int k = 0; k < 12; ++k) out[(size_t)k * nd + x] = r[k];
+  }
+  return c.status;
+}
+
 /* Node tangents [npar][nd][nfield] by central differences (steps [npar]; NULL: the reference's). */
 int sne_tangents(const snapi_eos_model *m, int nd, int nlines, const double *lam0, const double *mass,
                  const double *nodes, const double *step, double *tan) {

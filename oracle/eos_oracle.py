@@ -26,6 +26,8 @@ def lib():
         L.sne_chem.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _D, _D, _D, _D, _D]
         L.sne_build.restype = ctypes.c_int
         L.sne_build.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D]
+        L.sne_atmos.restype = ctypes.c_int
+        L.sne_atmos.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
         L.sne_tangents.restype = ctypes.c_int
         L.sne_tangents.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D]
         _ready = True
@@ -64,6 +66,18 @@ def build(tables, lam0, mass, nodes, nd=None):
     if st < 0:
         raise ValueError("sne_build: bad sizes")
     return T, Nt, rec, st
+
+
+def atmos(tables, nodes, x3=None, nd=None):
+    """The 12 return_as_array rows [12][nd] of one node vector's column, and the status."""
+    nd = nd or tables.nd
+    nodes = np.ascontiguousarray(nodes, np.float64)
+    h3 = None if x3 is None else np.ascontiguousarray(x3, np.float64)
+    out = np.zeros((12, nd))
+    st = lib().sne_atmos(ctypes.addressof(tables.model), nd, _p(nodes), _p(h3), _p(out))
+    if st < 0:
+        raise ValueError("sne_atmos: bad sizes")
+    return out, st
 
 
 def tangents(tables, lam0, mass, nodes, step=None, nd=None):

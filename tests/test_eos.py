@@ -71,6 +71,24 @@ def test_oracle_hydrostatic_columns(oracle_lib, name):
         np.testing.assert_allclose(rec[:, 2], d["he_ne"][p], rtol=1e-11)
 
 
+@pytest.mark.parametrize("name", ["eos_c3", "eos_c1"])
+def test_oracle_atmosphere_rows(oracle_lib, name):
+    """The restatement's return_as_array rows against the reference's (build_from_nodes +
+    compute_op_referent), for every node vector of the fixture."""
+    import eos_oracle as eo
+    d = load_fixture(name)
+    t = _tables(d)
+    ref = d["atm_arr"]
+    for p in range(ref.shape[0]):
+        out, st = eo.atmos(t, d["nodes"][p], x3=ref[p, 1])
+        assert st == 0
+        np.testing.assert_array_equal(out[[1, 5]], ref[p, [1, 5]])
+        np.testing.assert_allclose(out[0], ref[p, 0], rtol=0, atol=1e-14)
+        np.testing.assert_allclose(out[[2, 7, 8, 9]], ref[p, [2, 7, 8, 9]], rtol=1e-13, atol=1e-9)
+        np.testing.assert_allclose(out[[3, 4, 6]], ref[p, [3, 4, 6]], rtol=1e-10)
+        np.testing.assert_allclose(out[10:], ref[p, 10:], rtol=0, atol=1e-12)
+
+
 def test_oracle_records_and_tangents(oracle_lib, eos3, config3):
     """The full record (27 fields) and the node tangents of config-3 pixels against the reference's
     (the fixture stores them in float32, hence the 1e-7 tolerances)."""
