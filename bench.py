@@ -464,6 +464,34 @@ def bench_cube(sb, pool, ic, device, n=64, iters=30, chunk=0):
                     "not hidden behind the fits"}
 
 
+def bench_cube_synth(sb, pool, device, n=256, chunk=0):
+    """The synthesis branch of the master's job (snapi_cube_synth) over an n x n float64 atmosphere
+    cube in the 12-row layout (the columns of the pool's node vectors tiled over the cube, built on
+    the GPU by snapi_build_atmos), streamed from the file through records and synthesis to the
+    float64 spectra file."""
+    npix = n * n
+    ctx = sb.Context.from_fixture(pool, max_batch=4096, device=device)
+    ctx.eos_set(_eos_tables())
+    cols, _ = ctx.build_atmos(pool["nodes"])
+    cols = cols[np.arange(npix) % cols.shape[0]]
+    tmp = tempfile.mkdtemp(prefix="snapi_synth_")
+    try:
+        path = os.path.join(tmp, "atmos.f0")
+        sb.api.f0_write(path, np.ascontiguousarray(cols.reshape(n, n, 12, -1).transpose(2, 0, 1, 3)))
+        del cols
+        out = ctx.cube_synth(path, out_spectra=os.path.join(tmp, "spectra.f0"), chunk=chunk, want_stokes=False)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    ctx.close()
+    st = out["stats"]
+    return {"cube": [n, n], "pixels": npix, "chunks": st["chunks"], "wall_s": st["wall_s"], "gpu_s": st["fit_s"],
+            "device_s": st["kernel_ms"] / 1e3, "read_wait_s": st["read_wait_s"], "write_wait_s": st["write_wait_s"],
+            "pixels_per_s": npix / st["wall_s"], "bytes_read": st["bytes_read"], "bytes_written": st["bytes_written"],
+            "flagged": st["flagged"],
+            "note": "wall_s covers reading the atmosphere cube, records, synthesis and writing the spectra; "
+                    "read / write waits are the I/O not hidden behind the GPU work"}
+
+
 def bench_ali(sb, device, ncol=1024, cpu=True):
     """NLTE Ca II populations (snapi_ali_iter) for ncol columns to the reference's convergence
     criterion (max relative change < 1e-2): the three reference-built columns of
@@ -619,6 +647,8 @@ def main():
     ap.add_argument("--cube-only", type=int, default=0, metavar="N",
                     help="only measure the invert job (snapi_cube_invert) over an N x N .f0 cube")
     ap.add_argument("--cube-chunk", type=int, default=0, help="pixels per GPU batch of the invert job")
+    ap.add_argument("--cube-synth-only", type=int, default=0, metavar="N",
+                    help="only measure the synthesis job (snapi_cube_synth) over an N x N atmosphere cube")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -638,6 +668,15 @@ def main():
         ic = float(pool["stokes"][:, :, 0].max())
         print(json.dumps({"lm_device_build": bench_lm_device(sb, pool, ic, 0, npix=args.lm_fit_only, iters=30)}),
               flush=True)
+        return
+    if args.cube_synth_only:
+        sys.path.insert(0, ROOT)
+        import snapi_b200 as sb
+        from snapi_b200 import build as b
+        b.build_cuda()
+        pool = dict(np.load(POOL))
+        print(json.dumps({"cube_synth": bench_cube_synth(sb, pool, 0, n=args.cube_synth_only,
+                                                         chunk=args.cube_chunk)}), flush=True)
         return
     if args.cube_only:
         sys.path.insert(0, ROOT)

@@ -399,6 +399,18 @@ int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int
 int snapi_build_atmos(snapi_ctx *ctx, int npix, const double *nodes, const int *active, const double *x3,
                       double *atmos, int *pix_status, int mem);
 
+/* Records of given atmosphere columns -- the synthesis branch of the master's job, which reads an
+ * atmosphere cube with atmosphere::read_spinor3d (atmos_fio.cc:79-124) and synthesises each column
+ * (master/job.cc:384-409).  columns [npix][12][nd] float64 in the row layout of snapi_build_atmos:
+ * T is floored at 3200 K and Nt = gas pressure / (k T) as read_spinor3d does; |B|, inclination,
+ * azimuth, v_turb and v_z are taken as given; n_e, the populations and kappa are recomputed by the
+ * chemistry as obs_stokes' set-up does (the pressure, n_e and kappa rows of the file are not used).
+ * Needs the context's atom tables (snapi_eos_set).  pix_status [npix] (may be NULL): 0, or a sum of
+ * 1 (chemistry iteration cap), 4 (non-finite values), 8 (the column's log tau row is not the
+ * context's depth grid). */
+int snapi_records_from_columns(snapi_ctx *ctx, int npix, const double *columns, float *records, int *pix_status,
+                               int mem);
+
 /* The whole atmosphere::stokes_lm_fit (atmos_fit.cc:18-227) of npix pixels with the node -> record
  * map on the device: the loop snapi_lm_begin; { snapi_build_records of the requested node vectors of
  * the active pixels (with the reference's tangent steps); snapi_lm_step } ...; snapi_lm_result, all
@@ -518,16 +530,38 @@ typedef struct {
 typedef struct {
   long long pixels, chunks, lm_steps;
   double wall_s;                 /* the whole call */
-  double fit_s;                  /* inside snapi_lm_fit */
+  double fit_s;                  /* inside snapi_lm_fit (snapi_cube_synth: the GPU work of the chunks) */
   double read_wait_s;            /* waiting for the reader (reads not hidden behind the fits) */
   double write_wait_s;           /* waiting for the writer */
   long long bytes_read, bytes_written;
   double kernel_ms;              /* device time of all kernels */
   int launches;
+  long long flagged;             /* snapi_cube_synth: pixels with a non-zero record status */
 } snapi_cube_stats;
 
 int snapi_cube_invert(snapi_ctx *ctx, const snapi_lm_opts *opts, const snapi_cube_job *job,
                       snapi_cube_stats *stats);
+
+/* ---- Cube synthesis: the synthesis branch of the master's job -----------------------------------
+ * Replaces master/job.cc:384-409 with an atmosphere cube read by atmosphere::read_spinor3d
+ * (atmos_fio.cc:79-124): every column of the subfield synthesised (obs_stokes) and the spectra
+ * written as write_file 4-D does (job.cc:595).  The cube is streamed in chunks: a reader thread
+ * fetches the next chunk's rows while the GPU builds records (snapi_records_from_columns) and
+ * synthesises (snapi_synth), and a writer thread stores the previous chunk's spectra.
+ *   atmos cube   dims (nd, ny, nx, 12), float32 or float64: the 12 rows of snapi_build_atmos (what
+ *                snapi_cube_invert writes to inverted_atmos.f0); the log tau row must be the
+ *                context's depth grid and nd the context's
+ *   out_spectra  float64, dims (nlambda, 4, ny_sub, nx_sub) on the context's wavelength grid
+ * A subfield reaching beyond the cube is cut to it, as the job cuts nx / ny to the model's. */
+typedef struct {
+  const char *atmos_path;
+  int xl, xh, yl, yh;            /* 1-based inclusive subfield; 0 = the cube's extent */
+  const char *out_spectra;       /* NULL: not written */
+  float *stokes;                 /* [nx_sub * ny_sub][nlambda][4] host copy (x major), or NULL */
+  int chunk;                     /* pixels per GPU batch (0: 16384) */
+} snapi_cube_synth_job;
+
+int snapi_cube_synth(snapi_ctx *ctx, const snapi_cube_synth_job *job, snapi_cube_stats *stats);
 
 #ifdef __cplusplus
 }

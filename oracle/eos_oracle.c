@@ -692,6 +692,30 @@ int sne_atmos(const snapi_eos_model *m, int nd, const double *nodes, const doubl
   return c.status;
 }
 
+/* The record [nd][nfield] of a given column in the 12-row layout of sne_atmos, as
+ * atmosphere::read_spinor3d reads it (atmos_fio.cc:100-121: T floored at 3200 K, Nt = Pg / (k T))
+ * and obs_stokes' set-up completes it.  Returns the status bits as sne_build. */
+int sne_columns(const snapi_eos_model *m, int nd, int nlines, const double *lam0, const double *mass,
+                const double *cols, double *rec) {
+  static column c;
+  if (nd > MAXD || nd < 2) return -1;
+  c.status = 0;
+  for (int x = 0; x < nd; ++x) {
+    const double T = cols[2 * nd + x] > 3200.0 ? cols[2 * nd + x] : 3200.0;
+    c.lt[x] = cols[x];
+    c.T[x] = T;
+    c.Nt[x] = cols[3 * nd + x] / (C_K * T);
+    c.B[x] = cols[7 * nd + x];
+    c.vt[x] = cols[8 * nd + x];
+    c.vz[x] = cols[9 * nd + x];
+    c.th[x] = cols[10 * nd + x];
+    c.ph[x] = cols[11 * nd + x];
+  }
+  const int nf = SNAPI_NFIELD0 + 3 * nlines;
+  for (int x = 0; x < nd; ++x) record_depth(m, nlines, lam0, mass, &c, x, rec + (size_t)x * nf, &c.status);
+  return c.status;
+}
+
 /* Node tangents [npar][nd][nfield] by central differences (steps [npar]; NULL: the reference's). */
 int sne_tangents(const snapi_eos_model *m, int nd, int nlines, const double *lam0, const double *mass,
                  const double *nodes, const double *step, double *tan) {

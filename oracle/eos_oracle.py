@@ -26,6 +26,8 @@ def lib():
         L.sne_chem.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _D, _D, _D, _D, _D]
         L.sne_build.restype = ctypes.c_int
         L.sne_build.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D]
+        L.sne_columns.restype = ctypes.c_int
+        L.sne_columns.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D]
         L.sne_atmos.restype = ctypes.c_int
         L.sne_atmos.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
         L.sne_tangents.restype = ctypes.c_int
@@ -78,6 +80,19 @@ def atmos(tables, nodes, x3=None, nd=None):
     if st < 0:
         raise ValueError("sne_atmos: bad sizes")
     return out, st
+
+
+def columns(tables, lam0, mass, cols):
+    """Record [nd][nfield] (FP64) of one column [12][nd] in the sne_atmos row layout, and the status."""
+    cols = np.ascontiguousarray(cols, np.float64)
+    nd = cols.shape[1]
+    nl = tables.nlines
+    rec = np.zeros((nd, 12 + 3 * nl))
+    st = lib().sne_columns(ctypes.addressof(tables.model), nd, nl, _p(np.ascontiguousarray(lam0, np.float64)),
+                           _p(np.ascontiguousarray(mass, np.float64)), _p(cols), _p(rec))
+    if st < 0:
+        raise ValueError("sne_columns: bad sizes")
+    return rec, st
 
 
 def tangents(tables, lam0, mass, nodes, step=None, nd=None):

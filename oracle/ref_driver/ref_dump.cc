@@ -979,6 +979,50 @@ static int do_eos(const char *tskname, const char *nodesname, int npix, const ch
 }
 
 // ----------------------------------------------------------------------------------------------
+// spinor: the synthesis branch of the master's job on an atmosphere cube (job.cc:384-409): the
+// cube (12 return_as_array rows, dims (nd, ny, nx, 12)) read by atmosphere::read_spinor3d
+// (atmos_fio.cc:79-124), each column extracted and synthesised (obs_stokes); dumps the column
+// records (as extract_record reads them) and the Stokes vectors, x major.
+static int do_spinor(const char *tskname, const char *cubename, const char *outname) {
+  const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
+  const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
+  int ac = 4; cmdln cmd(ac, (char **)argv, options, maps);
+  io_class io(cmd);
+  Task t = load_task(tskname);
+  atmosphere *a = task_atmos(t, io);
+  char wd[4096];
+  if (!getcwd(wd, sizeof wd)) return 2;
+  if (a->read_spinor3d(wd, cubename, &io) < 0) return 3;
+  const int nx = a->x1h - a->x1l + 1, ny = a->x2h - a->x2l + 1, nl = t.nlambda;
+  fp_t *lam1 = lambda_1based(t);
+  std::vector<int> probe_l;
+  std::vector<double> allrec, allstokes;
+  int nd = 0, nf = 0;
+  for (int x = 1; x <= nx; ++x)
+    for (int y = 1; y <= ny; ++y) {
+      atmosphere *col = a->extract(x, y, io);
+      Record r;
+      extract_record(col, t, r, 0, probe_l);
+      nd = r.nd;
+      nf = NFIELD + 3 * r.nlines;
+      std::vector<double> fl = record_flat(r);
+      allrec.insert(allrec.end(), fl.begin(), fl.end());
+      observable *o = col->obs_stokes(t.el, t.az, lam1, nl);
+      fp_t **S = o->get_S(1, 1);
+      for (int l = 1; l <= nl; ++l) for (int s = 1; s <= 4; ++s) allstokes.push_back(S[s][l]);
+      del_ft2dim(S, 1, 4, 1, nl);
+      delete o;
+      delete col;
+    }
+  SbinWriter w(outname);
+  w.put("record", {nx * ny, nd, nf}, allrec.data());
+  w.put("stokes", {nx * ny, nl, 4}, allstokes.data());
+  delete[] (lam1 + 1);
+  delete a;
+  return 0;
+}
+
+// ----------------------------------------------------------------------------------------------
 // ANA .f0 files and the cube steps of the master's job (cmlib/ana_read.cc, cmlib/ana_write.cc,
 // cmlib/fileio.cc, master/job.cc:306-334, 575-597).  Dump format of f0read (little endian):
 //   int32 mfbd_type; int32 nd; int32 dims[nd]; int32 hlen; char header[hlen]; int64 nbytes; data
@@ -1103,6 +1147,7 @@ int main(int argc, char **argv) {
     return do_lmfit(argv[2], argv[3], argv[4], argv[5], atoi(argv[6]), atoi(argv[7]), argv[8],
                     argc >= 10 ? atof(argv[9]) : 0.0);
   if (argc >= 4 && !strcmp(argv[1], "f0read")) return do_f0read(argv[2], argv[3]);
+  if (argc >= 5 && !strcmp(argv[1], "spinor")) return do_spinor(argv[2], argv[3], argv[4]);
   if (argc >= 7 && !strcmp(argv[1], "f0write"))
     return do_f0write(argv[2], atoi(argv[3]), argv[4], argv[5], argv[6]);
   if (argc >= 13 && !strcmp(argv[1], "cubeobs"))

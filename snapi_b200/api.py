@@ -118,7 +118,17 @@ class CubeStats(ctypes.Structure):
         ("pixels", ctypes.c_longlong), ("chunks", ctypes.c_longlong), ("lm_steps", ctypes.c_longlong),
         ("wall_s", ctypes.c_double), ("fit_s", ctypes.c_double), ("read_wait_s", ctypes.c_double),
         ("write_wait_s", ctypes.c_double), ("bytes_read", ctypes.c_longlong), ("bytes_written", ctypes.c_longlong),
-        ("kernel_ms", ctypes.c_double), ("launches", ctypes.c_int),
+        ("kernel_ms", ctypes.c_double), ("launches", ctypes.c_int), ("flagged", ctypes.c_longlong),
+    ]
+
+
+class CubeSynthJob(ctypes.Structure):
+    _fields_ = [
+        ("atmos_path", ctypes.c_char_p),
+        ("xl", ctypes.c_int), ("xh", ctypes.c_int), ("yl", ctypes.c_int), ("yh", ctypes.c_int),
+        ("out_spectra", ctypes.c_char_p),
+        ("stokes", ctypes.c_void_p),
+        ("chunk", ctypes.c_int),
     ]
 
 
@@ -147,6 +157,7 @@ def lib():
         L.snapi_eos_set.argtypes = [vp, vp]
         L.snapi_build_records.argtypes = [vp, ip, fp, fp, fp, fp, fp, fp, fp, ip]
         L.snapi_build_atmos.argtypes = [vp, ip, fp, fp, fp, fp, fp, ip]
+        L.snapi_records_from_columns.argtypes = [vp, ip, fp, fp, fp, ip]
         L.snapi_lm_fit.argtypes = [vp, ip, ctypes.POINTER(SnapiLmOpts), fp, fp, fp, fp, fp, fp, fp, fp,
                                    ctypes.POINTER(ctypes.c_int), ip]
         L.snapi_zeeman_pattern.argtypes = [ip, ip, ctypes.c_double, ctypes.c_double, ctypes.POINTER(SnapiLine)]
@@ -175,6 +186,7 @@ def lib():
         L.snapi_f0_error.argtypes = []
         L.snapi_cube_invert.argtypes = [vp, ctypes.POINTER(SnapiLmOpts), ctypes.POINTER(CubeJob),
                                         ctypes.POINTER(CubeStats)]
+        L.snapi_cube_synth.argtypes = [vp, ctypes.POINTER(CubeSynthJob), ctypes.POINTER(CubeStats)]
         _LIB = L
     return _LIB
 
@@ -544,6 +556,31 @@ class Context:
         self._check(lib().snapi_build_atmos(self._ctx, npix, _ptr(n), _ptr(act), _ptr(h3), _ptr(atm), _ptr(st),
                                             MEM_HOST))
         return atm, st
+
+    def records_from_columns(self, columns):
+        """Records of atmosphere columns [npix][12][nd] in the snapi_build_atmos row layout
+        (snapi_records_from_columns; needs eos_set): records [npix][nd][nfield] and the status."""
+        c = np.ascontiguousarray(columns, dtype=np.float64)
+        npix = c.shape[0]
+        rec = np.zeros((npix, self.nd, self.nfield), np.float32)
+        st = np.zeros(npix, np.int32)
+        self._check(lib().snapi_records_from_columns(self._ctx, npix, _ptr(c), _ptr(rec), _ptr(st), MEM_HOST))
+        return rec, st
+
+    def cube_synth(self, atmos_path, subfield=(0, 0, 0, 0), out_spectra=None, chunk=0, want_stokes=True):
+        """The synthesis branch of the master's job over an atmosphere .f0 cube (snapi_cube_synth):
+        returns the Stokes vectors [nx][ny][nlambda][4] (if want_stokes) and the job's statistics."""
+        dims = f0_stat(atmos_path)["dims"]
+        nx_full, ny_full = (dims[2], dims[1]) if len(dims) == 4 else (1, 1)
+        xl, xh, yl, yh = subfield
+        nx = min(xh or nx_full, nx_full) - (xl or 1) + 1
+        ny = min(yh or ny_full, ny_full) - (yl or 1) + 1
+        st = np.zeros((max(nx, 1), max(ny, 1), self.nl, 4), np.float32) if want_stokes else None
+        enc = lambda p: None if p is None else os.fsencode(p)
+        job = CubeSynthJob(os.fsencode(atmos_path), xl, xh, yl, yh, enc(out_spectra), _ptr(st), int(chunk))
+        stats = CubeStats()
+        self._check(lib().snapi_cube_synth(self._ctx, ctypes.byref(job), ctypes.byref(stats)))
+        return {"stokes": st, "stats": {k: getattr(stats, k) for k, _ in CubeStats._fields_}}
 
     def build_records_device(self, npix, nodes_ptr, rec_ptr, tan_ptr=0, active_ptr=0, status_ptr=0):
         """build_records on device pointers (int addresses, e.g. torch .data_ptr())."""

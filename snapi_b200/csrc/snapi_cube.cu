@@ -489,6 +489,256 @@ extern "C" int snapi_cube_invert(snapi_ctx *ctx, const snapi_lm_opts *opts, cons
     stats->bytes_written = J.bytes_written;
     stats->kernel_ms = ker_ms;
     stats->launches = launches;
+    stats->flagged = 0;
+  }
+  return SNAPI_OK;
+}
+
+// ---- the synthesis branch of the master's job (master/job.cc:384-409) ----------------------------------
+// An atmosphere cube (the 12 return_as_array rows, dims (nd, ny, nx, 12), as atmosphere::read_spinor3d
+// reads it, atmos_fio.cc:79-124) is streamed column chunk by column chunk: a reader thread fetches the
+// next chunk's rows (12 reads per x row of the chunk), the GPU turns the columns into records
+// (snapi_records_from_columns) and synthesises them (snapi_synth), and a writer thread stores the
+// previous chunk's float64 spectra where write_file 4-D puts them (S[x][y][s][l], job.cc:595).
+namespace {
+
+// rows [12][cap][nd] (the chunk's file rows) -> cols [n][12][nd]
+__global__ void k_cube_cols(const double *__restrict__ rows, int n, int cap, int nd, double *__restrict__ cols) {
+  const long long m = (long long)n * 12 * nd;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < m; o += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(o % nd);
+    const long long t = o / nd;
+    const int k = (int)(t % 12), p = (int)(t / 12);
+    cols[o] = rows[((size_t)k * cap + p) * nd + z];
+  }
+}
+
+struct SynthJob {
+  int fd = -1;
+  snapi_f0_info info{};
+  int nx_full = 0, ny_full = 0, nd = 0, x0 = 0, y0 = 0, nx = 0, ny = 0, nl = 0, chunk = 0, nchunk = 0;
+  long long npix = 0;
+  double *d_rows = nullptr, *d_cols = nullptr, *d_spec = nullptr;
+  float *d_rec = nullptr, *d_stokes = nullptr;
+  int *d_st = nullptr;
+  Handoff rd, wr;
+  size_t rows_bytes = 0, spec_bytes = 0;
+  snapi_f0_file *f_spec = nullptr;
+  long long bytes_read = 0, bytes_written = 0;
+
+  ~SynthJob() {
+    if (fd >= 0) close(fd);
+    for (void *p : {(void *)d_rows, (void *)d_cols, (void *)d_spec, (void *)d_rec, (void *)d_stokes, (void *)d_st})
+      if (p) cudaFree(p);
+    for (void *p : {(void *)rd.slot[0].h, (void *)rd.slot[1].h, (void *)wr.slot[0].h, (void *)wr.slot[1].h})
+      if (p) cudaFreeHost(p);
+    if (f_spec) snapi_f0_close(f_spec);
+  }
+  int chunk_len(int k) const {
+    long long a = (long long)k * chunk, b = a + chunk;
+    return (int)((b > npix ? npix : b) - a);
+  }
+  void reader() {
+    std::vector<uint8_t> scratch;
+    for (int k = 0; k < nchunk; ++k) {
+      if (!rd.wait(k, false, nullptr)) return;
+      Handoff::Slot &s = rd.slot[k & 1];
+      s.p0 = (long long)k * chunk;
+      s.n = chunk_len(k);
+      double *dst = (double *)s.h;
+      long long p = s.p0, end = s.p0 + s.n;
+      while (p < end) {
+        const long long x = p / ny, y = p % ny, i = p - s.p0;
+        long long run = ny - y;
+        if (run > end - p) run = end - p;
+        for (int q = 0; q < 12; ++q) {  // element (q, x, y, z) at ((q * nx + x) * ny + y) * nd + z
+          const long long first = ((q * (long long)nx_full + x0 + x) * ny_full + y0 + y) * nd;
+          if (snapi_f0::read_range(fd, info, first, run * nd, dst + ((size_t)q * chunk + i) * nd, SNAPI_F0_FLOAT64,
+                                   scratch)) {
+            rd.fail(std::string("snapi_cube_synth: ") + snapi_f0_error());
+            return;
+          }
+        }
+        p += run;
+      }
+      bytes_read += (long long)s.n * 12 * nd * snapi_f0::type_size(info.type);
+      rd.set(k, true);
+    }
+  }
+  void writer() {
+    const long long pix_elems = 4LL * nl;
+    for (int k = 0; k < nchunk; ++k) {
+      if (!wr.wait(k, true, nullptr)) return;
+      Handoff::Slot &s = wr.slot[k & 1];
+      if (f_spec && snapi_f0_write_at(f_spec, s.p0 * pix_elems, s.n * pix_elems, s.h)) {
+        wr.fail(std::string("snapi_cube_synth: ") + snapi_f0_error());
+        return;
+      }
+      if (f_spec) bytes_written += (long long)s.n * pix_elems * 8;
+      wr.set(k, false);
+    }
+  }
+};
+
+}  // namespace
+
+extern "C" int snapi_cube_synth(snapi_ctx *ctx, const snapi_cube_synth_job *job, snapi_cube_stats *stats) {
+  using namespace snapi;
+  if (!ctx) return SNAPI_EINVAL;
+  if (!job || !job->atmos_path) return set_err(ctx, SNAPI_EINVAL, "snapi_cube_synth: null argument");
+  const auto t_start = Clock::now();
+  SynthJob J;
+  J.fd = open(job->atmos_path, O_RDONLY);
+  if (J.fd < 0) return set_err(ctx, SNAPI_EINVAL, "snapi_cube_synth: cannot open %s", job->atmos_path);
+  if (snapi_f0::parse(J.fd, &J.info)) return set_err(ctx, SNAPI_EINVAL, "snapi_cube_synth: %s", snapi_f0_error());
+  const snapi_f0_info &I = J.info;
+  if (I.ndim != 4 || I.dim[3] != 12)  // read_spinor3d: "does not have exactly 12 parameters"
+    return set_err(ctx, SNAPI_EINVAL, "snapi_cube_synth: the atmosphere cube must have dims (nd, ny, nx, 12)");
+  if (I.type != SNAPI_F0_FLOAT32 && I.type != SNAPI_F0_FLOAT64)
+    return set_err(ctx, SNAPI_EINVAL, "snapi_cube_synth: data type of the cube is not floating point");
+  if (I.compressed) return set_err(ctx, SNAPI_EINVAL, "snapi_cube_synth: compressed cube");
+  J.nd = (int)I.dim[0];
+  J.ny_full = (int)I.dim[1];
+  J.nx_full = (int)I.dim[2];
+  if (J.nd != ctx->nd)
+    return set_err(ctx, SNAPI_EINVAL, "snapi_cube_synth: the cube has %d depths, the context %d", J.nd, ctx->nd);
+  const int xl = job->xl > 0 ? job->xl : 1, yl = job->yl > 0 ? job->yl : 1;
+  // a range beyond the cube is cut to the cube, as the job reduces nx / ny to the model's (job.cc:391-398)
+  const int xh = (job->xh > 0 && job->xh < J.nx_full) ? job->xh : J.nx_full;
+  const int yh = (job->yh > 0 && job->yh < J.ny_full) ? job->yh : J.ny_full;
+  if (xl > xh || yl > yh) return set_err(ctx, SNAPI_EINVAL, "snapi_cube_synth: empty subfield");
+  J.x0 = xl - 1; J.y0 = yl - 1;
+  J.nx = xh - xl + 1; J.ny = yh - yl + 1;
+  J.nl = ctx->nl;
+  J.npix = (long long)J.nx * J.ny;
+  J.chunk = job->chunk > 0 ? job->chunk : 16384;
+  if (J.chunk > J.npix) J.chunk = (int)J.npix;
+  J.nchunk = (int)((J.npix + J.chunk - 1) / J.chunk);
+  const int C = J.chunk, nd = J.nd, nl = J.nl, nf = ctx->nfield;
+  J.rows_bytes = (size_t)C * 12 * nd * sizeof(double);
+  J.spec_bytes = (size_t)C * 4 * nl * sizeof(double);
+  SNAPI_CK(cudaSetDevice(ctx->device));
+  SNAPI_CK(cudaMalloc(&J.d_rows, J.rows_bytes));
+  SNAPI_CK(cudaMalloc(&J.d_cols, J.rows_bytes));
+  SNAPI_CK(cudaMalloc(&J.d_rec, sizeof(float) * (size_t)C * nd * nf));
+  SNAPI_CK(cudaMalloc(&J.d_stokes, sizeof(float) * (size_t)C * nl * 4));
+  SNAPI_CK(cudaMalloc(&J.d_spec, J.spec_bytes));
+  SNAPI_CK(cudaMalloc(&J.d_st, sizeof(int) * (size_t)C));
+  for (int i = 0; i < 2; ++i) {
+    SNAPI_CK(cudaHostAlloc((void **)&J.rd.slot[i].h, J.rows_bytes, cudaHostAllocDefault));
+    SNAPI_CK(cudaHostAlloc((void **)&J.wr.slot[i].h, J.spec_bytes, cudaHostAllocDefault));
+  }
+  int st = SNAPI_OK;
+  if (job->out_spectra) {
+    const long long dims[4] = {nl, 4, J.ny, J.nx};
+    J.f_spec = snapi_f0_create(job->out_spectra, SNAPI_F0_FLOAT64, 4, dims, nullptr, &st);
+    if (!J.f_spec) return set_err(ctx, SNAPI_EINVAL, "snapi_cube_synth: %s", snapi_f0_error());
+  }
+  std::vector<int> hst(C);
+  double read_wait = 0.0, write_wait = 0.0, ker_ms = 0.0, gpu_s = 0.0;
+  long long flagged = 0;
+  int launches = 0;
+  std::thread t_rd([&] { J.reader(); }), t_wr([&] { J.writer(); });
+  auto stop = [&](int code) {
+    J.rd.fail(J.rd.err.empty() ? "stopped" : J.rd.err);
+    J.wr.fail(J.wr.err.empty() ? "stopped" : J.wr.err);
+    t_rd.join();
+    t_wr.join();
+    return code;
+  };
+#define SYN_CK(call)                                                                                   \
+  do {                                                                                                 \
+    cudaError_t e_ = (call);                                                                           \
+    if (e_ != cudaSuccess)                                                                             \
+      return stop(set_err(ctx, SNAPI_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)));                  \
+  } while (0)
+  for (int k = 0; k < J.nchunk; ++k) {
+    if (!J.rd.wait(k, true, &read_wait)) {
+      std::string e = J.rd.err;
+      return stop(set_err(ctx, SNAPI_EINVAL, "%s", e.c_str()));
+    }
+    const long long p0 = (long long)k * C;
+    const int n = J.chunk_len(k);
+    const auto tg = Clock::now();
+    SYN_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    SYN_CK(cudaMemcpyAsync(J.d_rows, J.rd.slot[k & 1].h, J.rows_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    k_cube_cols<<<grid_for((long long)n * 12 * nd), kThreads, 0, ctx->stream>>>(J.d_rows, n, C, nd, J.d_cols);
+    SYN_CK(cudaGetLastError());
+    SYN_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    SYN_CK(cudaEventSynchronize(ctx->ev1));
+    float t = 0.f;
+    SYN_CK(cudaEventElapsedTime(&t, ctx->ev0, ctx->ev1));
+    ker_ms += t;
+    ++launches;
+    J.rd.set(k, false);
+    st = snapi_records_from_columns(ctx, n, J.d_cols, J.d_rec, J.d_st, SNAPI_MEM_DEVICE);
+    if (st) return stop(st);
+    ker_ms += ctx->last_ms;
+    launches += ctx->last_launches;
+    SYN_CK(cudaMemcpy(hst.data(), J.d_st, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) {
+      if (hst[i] & 8)
+        return stop(set_err(ctx, SNAPI_EINVAL,
+                            "snapi_cube_synth: the log tau row of pixel %lld is not the context's depth grid", p0 + i));
+      if (hst[i]) ++flagged;
+    }
+    st = snapi_synth(ctx, n, J.d_rec, J.d_stokes, SNAPI_MEM_DEVICE);
+    if (st) return stop(st);
+    ker_ms += ctx->last_ms;
+    launches += ctx->last_launches;
+    if (job->stokes)
+      SYN_CK(cudaMemcpy(job->stokes + (size_t)p0 * nl * 4, J.d_stokes, sizeof(float) * (size_t)n * nl * 4,
+                        cudaMemcpyDeviceToHost));
+    if (!J.wr.wait(k, false, &write_wait)) {
+      std::string e = J.wr.err;
+      return stop(set_err(ctx, SNAPI_EINVAL, "%s", e.c_str()));
+    }
+    Handoff::Slot &ws = J.wr.slot[k & 1];
+    SYN_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    k_cube_spectra<<<grid_for((long long)n * nl * 4), kThreads, 0, ctx->stream>>>(J.d_stokes, n, nl, J.d_spec);
+    SYN_CK(cudaGetLastError());
+    SYN_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    ++launches;
+    SYN_CK(cudaMemcpyAsync(ws.h, J.d_spec, sizeof(double) * (size_t)n * 4 * nl, cudaMemcpyDeviceToHost, ctx->stream));
+    SYN_CK(cudaStreamSynchronize(ctx->stream));
+    SYN_CK(cudaEventElapsedTime(&t, ctx->ev0, ctx->ev1));
+    ker_ms += t;
+    gpu_s += secs(tg, Clock::now());
+    ws.p0 = p0;
+    ws.n = n;
+    J.wr.set(k, true);
+  }
+#undef SYN_CK
+  {
+    const auto tw = Clock::now();
+    std::unique_lock<std::mutex> lk(J.wr.mu);
+    J.wr.cv.wait(lk, [&] { return J.wr.abort || (!J.wr.slot[0].full && !J.wr.slot[1].full); });
+    write_wait += secs(tw, Clock::now());
+  }
+  t_rd.join();
+  t_wr.join();
+  if (!J.wr.err.empty()) return set_err(ctx, SNAPI_EINVAL, "%s", J.wr.err.c_str());
+  if (!J.rd.err.empty()) return set_err(ctx, SNAPI_EINVAL, "%s", J.rd.err.c_str());
+  if (J.f_spec) {
+    snapi_f0_file *f = J.f_spec;
+    J.f_spec = nullptr;
+    if (snapi_f0_close(f)) return set_err(ctx, SNAPI_EINVAL, "snapi_cube_synth: %s", snapi_f0_error());
+  }
+  ctx->last_ms = ker_ms;
+  ctx->last_launches = launches;
+  if (stats) {
+    stats->pixels = J.npix;
+    stats->chunks = J.nchunk;
+    stats->lm_steps = 0;
+    stats->wall_s = secs(t_start, Clock::now());
+    stats->fit_s = gpu_s;
+    stats->read_wait_s = read_wait;
+    stats->write_wait_s = write_wait;
+    stats->bytes_read = J.bytes_read;
+    stats->bytes_written = J.bytes_written;
+    stats->kernel_ms = ker_ms;
+    stats->launches = launches;
+    stats->flagged = flagged;
   }
   return SNAPI_OK;
 }

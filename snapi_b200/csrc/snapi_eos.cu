@@ -663,13 +663,9 @@ __device__ void thermal_fields(const EosDev &E, Chem &c, double T, double Nt, do
   }
 }
 
-// kinematic / field fields 1, 3, 4, 5, 6 (project and transform, atmos_rad.cc:14-48; V_x = V_y = 0)
-__device__ void field_fields(const EosDev &E, const NodeView &nv, int x, bool build, double *f) {
-  const double vt = interp_kind(E, nv, 2, x, build);
-  const double vz = interp_kind(E, nv, 3, x, build);
-  const double B = interp_kind(E, nv, 4, x, build);
-  const double th = interp_kind(E, nv, 5, x, build);
-  const double ph = interp_kind(E, nv, 6, x, build);
+// kinematic / field fields 1, 3, 4, 5, 6 of given v_turb, v_z, |B|, inclination, azimuth (project and
+// transform, atmos_rad.cc:14-48; V_x = V_y = 0)
+__device__ void project_fields(const EosDev &E, double vt, double vz, double B, double th, double ph, double *f) {
   const double sp = sin(E.phi), cp = cos(E.phi), ct = cos(cPI - E.theta), st = sin(cPI - E.theta);
   f[1] = vt;
   f[3] = sp * st * 0.0 + cp * st * 0.0 + ct * vz;
@@ -681,6 +677,12 @@ __device__ void field_fields(const EosDev &E, const NodeView &nv, int x, bool bu
   f[4] = mg;
   f[5] = acos(nBz / mg) * 180.0 / cPI;
   f[6] = atan(nBy / nBx) * 180.0 / cPI;
+}
+
+// the same fields of the node model at depth x
+__device__ void field_fields(const EosDev &E, const NodeView &nv, int x, bool build, double *f) {
+  project_fields(E, interp_kind(E, nv, 2, x, build), interp_kind(E, nv, 3, x, build), interp_kind(E, nv, 4, x, build),
+                 interp_kind(E, nv, 5, x, build), interp_kind(E, nv, 6, x, build), f);
 }
 
 // thermal fields of every (pixel, variant, depth), one thread each (pixel fastest: a warp holds 32
@@ -800,6 +802,37 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_atm(EosArgs A, const double
   for (int k = 0; k < 12; ++k) o[(size_t)k * A.nd] = r[k];
 }
 
+// Records of given columns in the 12-row layout of k_eos_atm, as atmosphere::read_spinor3d reads a
+// cube (atmos_fio.cc:100-121: T floored at 3200 K, Nt from the gas pressure, the field from |B|,
+// inclination and azimuth, V_z, V_t) and obs_stokes' set-up completes it (the chemistry, n_e and the
+// opacity at airtovac(lambda_referent)).  One thread per (depth, pixel); status bit 8: the column's
+// log tau row is not the context's grid.
+__global__ void __launch_bounds__(kRecThreads) k_eos_col(const EosDev *tab, int npix, int nd, int nf,
+                                                        const double *cols, float *rec, int *status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npix * nd) return;
+  const int p = i % npix, x = i / npix;
+  const EosDev &E = *tab;
+  const double *c = cols + (size_t)p * 12 * nd + x;
+  auto row = [&](int k) { return c[(size_t)k * nd]; };
+  const double T = row(2) > 3200.0 ? row(2) : 3200.0;
+  const double Nt = row(3) / (cK * T);
+  Chem ch(E);
+  int st = 0;
+  double f[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES];
+  thermal_fields(E, ch, T, Nt, f, st);
+  project_fields(E, row(8), row(9), row(7), row(10), row(11), f);
+  if (!(fabs(row(0) - logtau(E, x)) <= 1e-9)) st |= 8;
+  float *r = rec + ((size_t)p * nd + x) * nf;
+  bool finite = true;
+  for (int k = 0; k < nf; ++k) {
+    r[k] = (float)f[k];
+    finite &= isfinite(f[k]);
+  }
+  if (!finite) st |= 4;
+  if (st) atomicOr(status + p, st);
+}
+
 // ---- host side ---------------------------------------------------------------------------------------------
 struct EosCtx {
   EosDev *d_tab = nullptr;
@@ -815,6 +848,11 @@ struct EosCtx {
   // return_as_array rows of snapi_build_atmos (cap_atm pixels) and the caller's heights
   double *d_atm = nullptr, *d_x3 = nullptr;
   int cap_atm = 0;
+  // snapi_records_from_columns: staged columns, records and status (cap_col pixels)
+  double *d_cols = nullptr;
+  float *d_crec = nullptr;
+  int *d_cst = nullptr;
+  int cap_col = 0;
 };
 
 void eos_free_bufs(EosCtx *e) {
@@ -829,6 +867,13 @@ void eos_free_bufs(EosCtx *e) {
   cudaFree(e->d_x3);
   e->d_atm = e->d_x3 = nullptr;
   e->cap_atm = 0;
+  cudaFree(e->d_cols);
+  cudaFree(e->d_crec);
+  cudaFree(e->d_cst);
+  e->d_cols = nullptr;
+  e->d_crec = nullptr;
+  e->d_cst = nullptr;
+  e->cap_col = 0;
 }
 
 }  // namespace
@@ -1256,6 +1301,69 @@ int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int
   if (npix < 0 || (npix > 0 && (!nodes || !records)) || (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
     return snapi::set_err(ctx, SNAPI_EINVAL, "snapi_build_records: invalid arguments");
   return build_impl(ctx, npix, nodes, active, records, Nt, tangents, step, pix_status, mem, nullptr, nullptr);
+}
+
+int snapi_records_from_columns(snapi_ctx *ctx, int npix, const double *columns, float *records, int *pix_status,
+                               int mem) {
+  using namespace snapi;
+  if (!ctx) return SNAPI_EINVAL;
+  EosCtx *e = static_cast<EosCtx *>(ctx->eos);
+  if (!e) return set_err(ctx, SNAPI_EINVAL, "snapi_records_from_columns: no atom tables (snapi_eos_set)");
+  if (npix < 0 || (npix > 0 && (!columns || !records)) || (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
+    return set_err(ctx, SNAPI_EINVAL, "snapi_records_from_columns: invalid arguments");
+  if (npix == 0) return SNAPI_OK;
+  const int nd = ctx->nd, nf = ctx->nfield;
+  const bool host = mem == SNAPI_MEM_HOST;
+  SNAPI_CK(cudaSetDevice(ctx->device));
+  const int B = std::min(npix, std::max(ctx->max_batch, 16384));
+  if (B > e->cap_col) {
+    SNAPI_CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(e->d_cols);
+    cudaFree(e->d_crec);
+    cudaFree(e->d_cst);
+    e->d_cols = nullptr;
+    e->d_crec = nullptr;
+    e->d_cst = nullptr;
+    e->cap_col = 0;
+    if (host) {
+      SNAPI_CK(cudaMalloc(&e->d_cols, sizeof(double) * (size_t)B * 12 * nd));
+      SNAPI_CK(cudaMalloc(&e->d_crec, sizeof(float) * (size_t)B * nd * nf));
+    }
+    SNAPI_CK(cudaMalloc(&e->d_cst, sizeof(int) * (size_t)B));
+    e->cap_col = B;
+  } else if (host && !e->d_cols) {
+    SNAPI_CK(cudaMalloc(&e->d_cols, sizeof(double) * (size_t)e->cap_col * 12 * nd));
+    SNAPI_CK(cudaMalloc(&e->d_crec, sizeof(float) * (size_t)e->cap_col * nd * nf));
+  }
+  ctx->last_ms = 0.0;
+  ctx->last_launches = 0;
+  for (int p0 = 0; p0 < npix; p0 += B) {
+    const int nb = std::min(B, npix - p0);
+    const double *cols = columns + (size_t)p0 * 12 * nd;
+    float *rec = records + (size_t)p0 * nd * nf;
+    if (host) {
+      SNAPI_CK(cudaMemcpyAsync(e->d_cols, cols, sizeof(double) * nb * 12 * nd, cudaMemcpyHostToDevice, ctx->stream));
+      cols = e->d_cols;
+    }
+    SNAPI_CK(cudaMemsetAsync(e->d_cst, 0, sizeof(int) * nb, ctx->stream));
+    SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    const int n = nb * nd;
+    k_eos_col<<<(n + kRecThreads - 1) / kRecThreads, kRecThreads, 0, ctx->stream>>>(e->d_tab, nb, nd, nf, cols,
+                                                                                    host ? e->d_crec : rec, e->d_cst);
+    SNAPI_CK(cudaGetLastError());
+    SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    ++ctx->last_launches;
+    if (host)
+      SNAPI_CK(cudaMemcpyAsync(rec, e->d_crec, sizeof(float) * nb * nd * nf, cudaMemcpyDeviceToHost, ctx->stream));
+    if (pix_status)
+      SNAPI_CK(cudaMemcpyAsync(pix_status + p0, e->d_cst, sizeof(int) * nb,
+                               host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
+    SNAPI_CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    SNAPI_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->last_ms += ms;
+  }
+  return SNAPI_OK;
 }
 
 int snapi_build_atmos(snapi_ctx *ctx, int npix, const double *nodes, const int *active, const double *x3,

@@ -20,6 +20,10 @@ its 80-depth atmosphere file from REF and runs oracle/_ref/snapi_ref_dump).  Wri
                                   with the 12 return_as_array rows of each (atm_arr)
   tests/golden/config4_256.npz    (--only-c4-subset 256) the config-4 fit of 256 seeded pixels
                                   (seed 404) by the reference's stokes_lm_fit
+  tests/golden/spinor_c3.npz      (--only-spinor) a 4 x 2 atmosphere cube of the eos_c3 columns in
+                                  the 12-row layout (one column below the 3200 K floor at the top)
+                                  and the records and Stokes the reference's synthesis branch gives
+                                  (read_spinor3d, extract, obs_stokes)
   tests/golden/f0_ref.npz         (--only-f0) ANA .f0 files written by the reference's ana_fzwrite
                                   and what its ana_fzread returns for them, for hand-made headers
                                   (reversed synch pattern, big-endian data) and for the two .f0
@@ -311,6 +315,7 @@ def main():
     ap.add_argument("--only-psf", action="store_true")
     ap.add_argument("--only-eos", action="store_true")
     ap.add_argument("--only-f0", action="store_true")
+    ap.add_argument("--only-spinor", action="store_true")
     ap.add_argument("--only-c4-subset", type=int, default=0, metavar="N",
                     help="config-4 fit of N pixels by the reference (8 processes at a time)")
     ap.add_argument("--c5col", type=int, default=3)
@@ -326,6 +331,9 @@ def main():
             return
         if a.only_f0:
             make_f0(tmp, a.ref)
+            return
+        if a.only_spinor:
+            make_spinor(tmp)
             return
         if a.only_c4_subset:
             shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
@@ -485,6 +493,26 @@ def make_f0(tmp, ref):
     out["cw_nodes_file"] = np.frombuffer(open(on, "rb").read(), np.uint8)
     out["cw_spec_file"] = np.frombuffer(open(osp, "rb").read(), np.uint8)
     np.savez_compressed(os.path.join(HERE, "f0_ref.npz"), **out)
+
+
+def make_spinor(tmp):
+    """The synthesis branch of the master's job on a small atmosphere cube: the 8 eos_c3 columns
+    (return_as_array rows) as a 4 x 2 cube, column 3 set to 3000 K in its top 6 depths (below
+    read_spinor3d's 3200 K floor); the reference reads it with read_spinor3d and synthesises every
+    column -> tests/golden/spinor_c3.npz."""
+    sys.path.insert(0, ROOT)
+    from snapi_b200 import api
+    d = np.load(os.path.join(HERE, "eos_c3.npz"))
+    cols = d["atm_arr"].copy()
+    cols[3, 2, :6] = 3000.0
+    nx, ny = 4, 2
+    cube = np.ascontiguousarray(cols.reshape(nx, ny, 12, -1).transpose(2, 0, 1, 3))  # [12][nx][ny][nd]
+    api.f0_write(os.path.join(tmp, "atm.f0"), cube)
+    shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
+    run([DUMP, "spinor", "c3.tsk", "atm.f0", "spinor.sbin"], tmp)
+    o = read_sbin(os.path.join(tmp, "spinor.sbin"))
+    np.savez_compressed(os.path.join(HERE, "spinor_c3.npz"), columns=cols, nx=np.array([nx]), ny=np.array([ny]),
+                        record=o["record"], stokes=o["stokes"])
 
 
 def make_eos(tmp):

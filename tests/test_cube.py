@@ -164,3 +164,76 @@ def test_cube_invert_errors(sb, config4, f0, tmp_path):
     with pytest.raises(sb.SnapiError, match="neither"):
         ctx.cube_invert(str(cube), kinds, step, window=sub[4:])
     ctx.close()
+
+
+# ---- the synthesis branch of the job: atmosphere cubes ------------------------------------------------
+
+def _spinor_setup(sb, config3):
+    from snapi_b200.eos_tables import EosTables
+    ic = float(np.abs(config3["stokes"][:, :, 0]).max())
+    ctx = sb.Context.from_fixture(config3, stokes_scale=ic)
+    ctx.eos_set(EosTables(load_fixture("eos_c3")))
+    return ctx
+
+
+def test_records_from_columns_vs_reference(sb, config3):
+    """snapi_records_from_columns on the 8 eos_c3 columns in the 12-row layout (one below the
+    3200 K floor) against the records and Stokes of the reference's synthesis branch (read_spinor3d,
+    extract, obs_stokes)."""
+    d = load_fixture("spinor_c3")
+    ctx = _spinor_setup(sb, config3)
+    rec, st = ctx.records_from_columns(d["columns"])
+    S = ctx.synth(rec)
+    ctx.close()
+    assert np.all(st == 0)
+    np.testing.assert_allclose(rec, d["record"], rtol=3e-7, atol=0)
+    ic = d["stokes"][:, :, 0].max(axis=1)[:, None, None]
+    assert (np.abs(S - d["stokes"]) / ic).max() < 1e-5
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_cube_synth_streams_the_cube(sb, config3, dtype, tmp_path):
+    """snapi_cube_synth over a 4 x 2 atmosphere cube (float64 and float32 files), subfield x 2..4,
+    chunks of 4 pixels that cross x rows: the spectra equal snapi_synth of snapi_records_from_columns
+    of the same columns, and the file holds them as write_file 4-D does (float64 S[x][y][s][l])."""
+    api = sb.api
+    d = load_fixture("spinor_c3")
+    cols = d["columns"].astype(dtype).astype(np.float64)
+    nx, ny = 4, 2
+    cube = np.ascontiguousarray(cols.reshape(nx, ny, 12, -1).transpose(2, 0, 1, 3)).astype(dtype)
+    path = tmp_path / "atm.f0"
+    api.f0_write(str(path), cube)
+    ctx = _spinor_setup(sb, config3)
+    out = ctx.cube_synth(str(path), subfield=(2, 4, 0, 0), out_spectra=str(tmp_path / "spec.f0"), chunk=4)
+    rec, st = ctx.records_from_columns(cols[ny:])
+    ref = ctx.synth(rec)
+    ctx.close()
+    s = out["stats"]
+    assert (s["pixels"], s["chunks"], s["flagged"]) == (6, 2, 0)
+    assert s["bytes_read"] == 6 * 12 * cols.shape[2] * np.dtype(dtype).itemsize
+    assert np.array_equal(out["stokes"].reshape(6, -1, 4), ref)
+    spec = api.f0_read(str(tmp_path / "spec.f0"))
+    assert spec.dtype == np.float64 and spec.shape == (3, ny, 4, ref.shape[1])
+    assert np.array_equal(spec, ref.astype(np.float64).reshape(3, ny, -1, 4).transpose(0, 1, 3, 2))
+
+
+def test_cube_synth_errors(sb, config3, tmp_path):
+    api = sb.api
+    d = load_fixture("spinor_c3")
+    cols = d["columns"]
+    ctx = _spinor_setup(sb, config3)
+    p11 = tmp_path / "p11.f0"
+    api.f0_write(str(p11), np.zeros((11, 4, 2, cols.shape[2])))
+    with pytest.raises(sb.SnapiError, match="12"):
+        ctx.cube_synth(str(p11))
+    short = tmp_path / "short.f0"
+    api.f0_write(str(short), np.zeros((12, 4, 2, 40)))
+    with pytest.raises(sb.SnapiError, match="depths"):
+        ctx.cube_synth(str(short))
+    bad = cols.copy()
+    bad[5, 0] += 0.01  # a column on another depth grid
+    grid = tmp_path / "grid.f0"
+    api.f0_write(str(grid), np.ascontiguousarray(bad.reshape(4, 2, 12, -1).transpose(2, 0, 1, 3)))
+    with pytest.raises(sb.SnapiError, match="depth grid"):
+        ctx.cube_synth(str(grid))
+    ctx.close()

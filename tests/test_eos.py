@@ -89,6 +89,20 @@ def test_oracle_atmosphere_rows(oracle_lib, name):
         np.testing.assert_allclose(out[10:], ref[p, 10:], rtol=0, atol=1e-12)
 
 
+def test_oracle_column_records(oracle_lib, config3):
+    """Records of given atmosphere columns (the reference's synthesis branch: read_spinor3d, then
+    obs_stokes' set-up) from the restatement against the reference's, including a column below the
+    3200 K floor."""
+    import eos_oracle as eo
+    d = load_fixture("spinor_c3")
+    t = _tables(load_fixture("eos_c3"))
+    lam0, mass = _line_const(config3)
+    for p in range(d["columns"].shape[0]):
+        rec, st = eo.columns(t, lam0, mass, d["columns"][p])
+        assert st == 0
+        np.testing.assert_allclose(rec, d["record"][p], rtol=1e-10, atol=1e-300)
+
+
 def test_oracle_records_and_tangents(oracle_lib, eos3, config3):
     """The full record (27 fields) and the node tangents of config-3 pixels against the reference's
     (the fixture stores them in float32, hence the 1e-7 tolerances)."""
