@@ -406,8 +406,9 @@ int snapi_build_atmos(snapi_ctx *ctx, int npix, const double *nodes, const int *
  * azimuth, v_turb and v_z are taken as given; n_e, the populations and kappa are recomputed by the
  * chemistry as obs_stokes' set-up does (the pressure, n_e and kappa rows of the file are not used).
  * Needs the context's atom tables (snapi_eos_set).  pix_status [npix] (may be NULL): 0, or a sum of
- * 1 (chemistry iteration cap), 4 (non-finite values), 8 (the column's log tau row is not the
- * context's depth grid). */
+ * 1 (chemistry iteration cap), 4 (non-finite values), 8 (the column's log tau row differs from the
+ * context's depth grid by more than 1e-6, i.e. beyond the float32 rounding of a float32 cube; the
+ * records are for the context's grid). */
 int snapi_records_from_columns(snapi_ctx *ctx, int npix, const double *columns, float *records, int *pix_status,
                                int mem);
 

@@ -806,7 +806,7 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_atm(EosArgs A, const double
 // cube (atmos_fio.cc:100-121: T floored at 3200 K, Nt from the gas pressure, the field from |B|,
 // inclination and azimuth, V_z, V_t) and obs_stokes' set-up completes it (the chemistry, n_e and the
 // opacity at airtovac(lambda_referent)).  One thread per (depth, pixel); status bit 8: the column's
-// log tau row is not the context's grid.
+// log tau row is not the context's grid (beyond 1e-6).
 __global__ void __launch_bounds__(kRecThreads) k_eos_col(const EosDev *tab, int npix, int nd, int nf,
                                                         const double *cols, float *rec, int *status) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -822,7 +822,9 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_col(const EosDev *tab, int 
   double f[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES];
   thermal_fields(E, ch, T, Nt, f, st);
   project_fields(E, row(8), row(9), row(7), row(10), row(11), f);
-  if (!(fabs(row(0) - logtau(E, x)) <= 1e-9)) st |= 8;
+  // the grid to float32 rounding (a float32 cube holds log tau to ~2.4e-7); the synthesis runs on
+  // the context's grid
+  if (!(fabs(row(0) - logtau(E, x)) <= 1e-6)) st |= 8;
   float *r = rec + ((size_t)p * nd + x) * nf;
   bool finite = true;
   for (int k = 0; k < nf; ++k) {
