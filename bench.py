@@ -328,6 +328,7 @@ def run_snapi(args):
         line["lm_device_build"] = bench_lm_device(sb, pool, ic, local)
         line["ali"] = bench_ali(sb, local, cpu=not args.no_cpu_baseline)
         line["cube_invert"] = bench_cube(sb, pool, ic, local, n=64)
+        line["cube_synth"] = bench_cube_synth(sb, pool, local, n=256)
     ctx.close()
     if world > 1:
         import torch.distributed as dist
