@@ -570,7 +570,9 @@ __device__ __forceinline__ void variant_pert(const EosDev &E, const EosArgs &A, 
   }
 }
 
-__device__ void he_item(const EosArgs &A, int i) {
+__global__ void __launch_bounds__(kHeThreads) k_eos_he(EosArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.npix * A.nvar) return;
   const int p = i % A.npix, v = i / A.npix;
   if (A.active && !A.active[p]) return;
   const EosDev &E = *A.tab;
@@ -625,13 +627,6 @@ __device__ void he_item(const EosArgs &A, int i) {
     Nprev = N;
   }
   if (st) atomicOr(A.status + p, st);
-}
-
-// One item per (pixel, variant); a grid-stride loop, so the launch's grid (picked by the tuner in
-// the host code) bounds how many columns are in flight at once.
-__global__ void __launch_bounds__(kHeThreads) k_eos_he(EosArgs A) {
-  const int n = A.npix * A.nvar;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) he_item(A, i);
 }
 
 // ---- k_eos_rec: records and tangents per (depth, pixel) ------------------------------------------------
@@ -692,7 +687,9 @@ __device__ void field_fields(const EosDev &E, const NodeView &nv, int x, bool bu
 
 // thermal fields of every (pixel, variant, depth), one thread each (pixel fastest: a warp holds 32
 // pixels of one variant at one depth), FP64 into F [npix][nvar][nd][nf]
-__device__ void var_item(const EosArgs &A, long long i) {
+__global__ void __launch_bounds__(kRecThreads) k_eos_var(EosArgs A) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)A.npix * A.nvar * A.nd) return;
   const int p = (int)(i % A.npix);
   const long long r = i / A.npix;
   const int v = (int)(r % A.nvar), x = (int)(r / A.nvar);
@@ -706,12 +703,6 @@ __device__ void var_item(const EosArgs &A, long long i) {
   double *o = A.F + cv * A.nf;
   for (int k = 0; k < A.nf; ++k) o[k] = (k == 1 || (k >= 3 && k <= 6)) ? 0.0 : f[k];
   if (st) atomicOr(A.status + p, st);
-}
-
-__global__ void __launch_bounds__(kRecThreads) k_eos_var(EosArgs A) {
-  const long long n = (long long)A.npix * A.nvar * A.nd;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    var_item(A, i);
 }
 
 // records and tangent rows per (depth, pixel): thermal fields from F, kinematic / field fields by
@@ -816,8 +807,10 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_atm(EosArgs A, const double
 // inclination and azimuth, V_z, V_t) and obs_stokes' set-up completes it (the chemistry, n_e and the
 // opacity at airtovac(lambda_referent)).  One thread per (depth, pixel); status bit 8: the column's
 // log tau row is not the context's grid (beyond 1e-6).
-__device__ void col_item(const EosDev *tab, int npix, int nd, int nf, const double *cols, float *rec, int *status,
-                         int i) {
+__global__ void __launch_bounds__(kRecThreads) k_eos_col(const EosDev *tab, int npix, int nd, int nf,
+                                                        const double *cols, float *rec, int *status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npix * nd) return;
   const int p = i % npix, x = i / npix;
   const EosDev &E = *tab;
   const double *c = cols + (size_t)p * 12 * nd + x;
@@ -842,13 +835,6 @@ __device__ void col_item(const EosDev *tab, int npix, int nd, int nf, const doub
   if (st) atomicOr(status + p, st);
 }
 
-__global__ void __launch_bounds__(kRecThreads) k_eos_col(const EosDev *tab, int npix, int nd, int nf,
-                                                        const double *cols, float *rec, int *status) {
-  const int n = npix * nd;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    col_item(tab, npix, nd, nf, cols, rec, status, i);
-}
-
 // ---- host side ---------------------------------------------------------------------------------------------
 struct EosCtx {
   EosDev *d_tab = nullptr;
@@ -869,51 +855,7 @@ struct EosCtx {
   float *d_crec = nullptr;
   int *d_cst = nullptr;
   int cap_col = 0;
-  // grids (CTAs) the launch tuner picked for the grid-stride chemistry kernels (0: not yet)
-  int grid_he = 0, grid_var = 0, grid_col = 0;
-  cudaEvent_t tev0 = nullptr, tev1 = nullptr;
 };
-
-// Launch-shape tuner for the chemistry kernels.  Each of their items keeps ~7.5 KB of state (stage
-// tables, kept fractions, the Newton matrix) in thread-local memory; with every item of a large
-// launch in flight that state overflows L1 and L2 and streams from HBM (ncu, k_eos_col over 327 k
-// items: 13 GB of DRAM traffic for 59 MB of inputs and outputs, long-scoreboard stalls dominant).
-// The kernels are grid-stride loops, so a smaller grid keeps fewer items in flight.  The best grid
-// depends on the GPU and on the atom tables, so the first launch of a kernel with at least kTuneMin
-// items times a ladder of grids (multiples of the SM count, and the full grid) on the real work --
-// every candidate computes the same outputs, the items being independent -- and the context keeps
-// the fastest for all later launches of that kernel.
-constexpr long long kTuneMin = 65536;
-
-template <class F>
-cudaError_t tuned_launch(snapi_ctx *ctx, EosCtx *e, int &cached, long long items, int threads, F launch) {
-  const long long fl = (items + threads - 1) / threads;
-  const int full = (int)std::min<long long>(fl, 1 << 30);
-  if (cached > 0) return launch(std::min(cached, full));
-  if (items < kTuneMin) return launch(full);
-  int nsm = 148;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
-  cudaError_t err;
-  if (!e->tev0) {
-    if ((err = cudaEventCreate(&e->tev0)) != cudaSuccess) return err;
-    if ((err = cudaEventCreate(&e->tev1)) != cudaSuccess) return err;
-  }
-  float best = 3.0e38f;
-  int best_g = full;
-  for (int m : {1, 2, 4, 8, 16, 32, 0}) {
-    const int g = m ? std::min(nsm * m, full) : full;
-    if ((err = cudaEventRecord(e->tev0, ctx->stream)) != cudaSuccess) return err;
-    if ((err = launch(g)) != cudaSuccess) return err;
-    if ((err = cudaEventRecord(e->tev1, ctx->stream)) != cudaSuccess) return err;
-    if ((err = cudaEventSynchronize(e->tev1)) != cudaSuccess) return err;
-    float ms = 0.f;
-    if ((err = cudaEventElapsedTime(&ms, e->tev0, e->tev1)) != cudaSuccess) return err;
-    if (ms < best) { best = ms; best_g = g; }
-    if (m && g == full) break;  // the larger multiples are the full grid too
-  }
-  cached = best_g;
-  return cudaSuccess;
-}
 
 void eos_free_bufs(EosCtx *e) {
   void *b[] = {e->d_T, e->d_Nt, e->d_nodes, e->d_step, e->d_Ntout, e->d_active, e->d_status, e->d_rec, e->d_tan,
@@ -950,8 +892,6 @@ void eos_free(snapi_ctx *ctx) {
   EosCtx *e = static_cast<EosCtx *>(ctx->eos);
   if (!e) return;
   eos_free_bufs(e);
-  if (e->tev0) cudaEventDestroy(e->tev0);
-  if (e->tev1) cudaEventDestroy(e->tev1);
   cudaFree(e->d_tab);
   delete e;
   ctx->eos = nullptr;
@@ -1205,7 +1145,6 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
   SNAPI_CK(cudaMemcpy(e->d_tab, &H, sizeof(EosDev), cudaMemcpyHostToDevice));
   e->npar = m->npar;
   e->ntherm = H.kcount[1];
-  e->grid_he = e->grid_var = e->grid_col = 0;  // new tables: tune the launches again
   e->kind.assign(m->node_kind, m->node_kind + m->npar);
   e->ref_step.assign(m->npar, 0.0);
   static const double ref_step[7] = {0.0, 5.0, 20.0, 20.0, 0.01, 0.001, 0.001};  // const.h:27-32
@@ -1312,15 +1251,11 @@ static int build_impl(snapi_ctx *ctx, int npix, const double *nodes, const int *
     SNAPI_CK(cudaMemsetAsync(e->d_status, 0, sizeof(int) * nb, ctx->stream));
     SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
     const int nhe = nb * nvar;
-    SNAPI_CK(tuned_launch(ctx, e, e->grid_he, nhe, kHeThreads, [&](int g) {
-      k_eos_he<<<g, kHeThreads, 0, ctx->stream>>>(A);
-      return cudaGetLastError();
-    }));
+    k_eos_he<<<(nhe + kHeThreads - 1) / kHeThreads, kHeThreads, 0, ctx->stream>>>(A);
+    SNAPI_CK(cudaGetLastError());
     const long long nvx = (long long)nb * nvar * nd;
-    SNAPI_CK(tuned_launch(ctx, e, e->grid_var, nvx, kRecThreads, [&](int g) {
-      k_eos_var<<<g, kRecThreads, 0, ctx->stream>>>(A);
-      return cudaGetLastError();
-    }));
+    k_eos_var<<<(unsigned)((nvx + kRecThreads - 1) / kRecThreads), kRecThreads, 0, ctx->stream>>>(A);
+    SNAPI_CK(cudaGetLastError());
     const int nrec = nb * nd;
     ctx->last_launches += 2;
     if (records) {
@@ -1415,11 +1350,9 @@ int snapi_records_from_columns(snapi_ctx *ctx, int npix, const double *columns, 
     SNAPI_CK(cudaMemsetAsync(e->d_cst, 0, sizeof(int) * nb, ctx->stream));
     SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
     const int n = nb * nd;
-    float *rout = host ? e->d_crec : rec;
-    SNAPI_CK(tuned_launch(ctx, e, e->grid_col, n, kRecThreads, [&](int g) {
-      k_eos_col<<<g, kRecThreads, 0, ctx->stream>>>(e->d_tab, nb, nd, nf, cols, rout, e->d_cst);
-      return cudaGetLastError();
-    }));
+    k_eos_col<<<(n + kRecThreads - 1) / kRecThreads, kRecThreads, 0, ctx->stream>>>(e->d_tab, nb, nd, nf, cols,
+                                                                                    host ? e->d_crec : rec, e->d_cst);
+    SNAPI_CK(cudaGetLastError());
     SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
     ++ctx->last_launches;
     if (host)
