@@ -131,13 +131,13 @@ struct EosDev {
 // chain but measured 14x slower at 4096 columns x 9 variants, where the GPU is full either way.
 struct Chem {
   const EosDev &E;
-  double T, kT, xT;  // xT = 5040 / T
-  // T-only stage factors in shared memory, [2][nst][blockDim.x]: su the T-only part of U (whole U
-  // for CONST / IRWIN / NONE), sc = fct exp(-chi / kT), the T-only factor of the stage ratio.  Every
-  // ionisation sweep (~20 per solve) reads them; as thread-local arrays they overflowed L1 and L2
-  // at large launches and streamed from HBM.
-  double *su, *sc;
-  int sstr;
+  double T, kT;
+  struct __align__(16) SLoc {
+    double Ut;  // T-only part of U (whole U for CONST / IRWIN / NONE)
+    double cz;  // fct exp(-chi / kT): the T-only factor of the stage ratio
+    double Dz;  // 31.321 z^2 x
+    double pad;
+  } sl[kES];
   double w2[kET];   // g2 exp(-2.302585 ee x)
   double K[kEM];
   double Ea[kEA + 1], Da[kEA + 1];  // sum_i i f_i, sum_i i df_i / dNe per atom (1-based)
@@ -146,18 +146,12 @@ struct Chem {
   double A[(kEA + 1) * (kEA + 1)], d[kEA + 1];
   int capped;
 
-  // smem: the CTA's dynamic shared memory, 2 * E.nst * blockDim.x doubles
-  __device__ Chem(const EosDev &e, double *smem) : E(e), T(-1.0) {
-    su = smem + threadIdx.x;
-    sc = su + (size_t)e.nst * blockDim.x;
-    sstr = blockDim.x;
-  }
+  __device__ explicit Chem(const EosDev &e) : E(e), T(-1.0) {}
 
   __device__ void set_T(double Tin) {
     T = Tin;
     kT = cK * T;
     const double x = 5040.0 / T;
-    xT = x;
     const double fct = 2.0 * pow((2.0 * cPI * cME * cK * T) / (cH * cH), 1.5);
     for (int s = 0; s < E.nst; ++s) {
       const int ty = E.pft[s];
@@ -167,14 +161,15 @@ struct Chem {
           for (int c = E.c0[t]; c < E.c1[t]; ++c) u += E.cA[c] * exp(-2.302585 * E.cG[c] * x);
           w2[t] = E.g2[t] * exp(-2.302585 * E.tee[t] * x);
         }
+        sl[s].Dz = 31.321 * E.zeff[s] * E.zeff[s] * x;
       } else if (ty == SNAPI_PF_IRWIN) {
         const double lnT = log(T);
         double sum = 0.0;
         for (int c = E.t0[s]; c < E.t1[s]; ++c) sum += E.cA[c] * pow(lnT, (double)(c - E.t0[s]));
         u = exp(sum);
       }
-      su[s * sstr] = u;
-      sc[s * sstr] = fct * exp(-E.eion[s] / kT);
+      sl[s].Ut = u;
+      sl[s].cz = fct * exp(-E.eion[s] / kT);
     }
     for (int m = 0; m < E.nmol; ++m) {
       double k = 0.0;
@@ -194,13 +189,12 @@ struct Chem {
 
   // U of a stage and (kDeriv) dU / dNe from its packed constants; ine = 1/ne, pne = ne^(1/6), ipne = 1/pne
   template <bool kDeriv>
-  __device__ __forceinline__ void stage_u(const StageTab &S, int s, double Ut, double ine, double pne, double ipne,
+  __device__ __forceinline__ void stage_u(const StageTab &S, const SLoc &L, double ine, double pne, double ipne,
                                           double &U, double &dU) const {
-    U = Ut;
+    U = L.Ut;
     dU = 0.0;
     if (S.t1 <= S.t0) return;
-    const double dz = 31.321 * E.zeff[s] * E.zeff[s] * xT;  // Traving stages only
-    const double zf = S.zf, p = zf * ipne, ip = pne * S.izf;
+    const double zf = S.zf, p = zf * ipne, ip = pne * S.izf, dz = L.Dz;
     double dq = 0.0, wl = 0.0;
     for (int t = S.t0; t < S.t1; ++t) {
       const TermTab Tt = E.ttab[t];
@@ -223,7 +217,9 @@ struct Chem {
 
   template <bool kDeriv>
   __device__ __forceinline__ void stage_u(int s, double ine, double pne, double ipne, double &U, double &dU) const {
-    stage_u<kDeriv>(E.stab[s], s, su[s * sstr], ine, pne, ipne, U, dU);
+    const StageTab S = E.stab[s];
+    const SLoc L = sl[s];
+    stage_u<kDeriv>(S, L, ine, pne, ipne, U, dU);
   }
 
   // atom a (0-based): Ea, and with kDeriv Da and the kept fractions
@@ -233,8 +229,9 @@ struct Chem {
     double h = 1.0, fsum = 0.0, S1 = 0.0, dfsum = 0.0, S2 = 0.0, dl0 = 0.0;
     for (int z = 0; z < ns; ++z) {
       const StageTab S = E.stab[s0 + z];
+      const SLoc L = sl[s0 + z];
       double U, dU;
-      stage_u<kDeriv>(S, s0 + z, su[(s0 + z) * sstr], ine, pne, ipne, U, dU);
+      stage_u<kDeriv>(S, L, ine, pne, ipne, U, dU);
       const double f = U * h;
       fsum += f;
       S1 += (double)z * f;
@@ -246,7 +243,7 @@ struct Chem {
         S2 += (double)z * df;
         if (S.ref >= 0) { fr[S.ref] = f; dr[S.ref] = df; }
       }
-      h *= sc[(s0 + z) * sstr] * ine;
+      h *= L.cz * ine;
     }
     const double inv = 1.0 / fsum;
     Ea[a + 1] = S1 * inv;
@@ -583,8 +580,7 @@ __global__ void __launch_bounds__(kHeThreads) k_eos_he(EosArgs A) {
   variant_pert(E, A, v, nv.pidx, nv.pert);
   double *Tc = A.T + ((size_t)p * A.nvar + v) * A.nd;
   double *Nc = A.Nt + ((size_t)p * A.nvar + v) * A.nd;
-  extern __shared__ double eos_smem[];
-  Chem c(E, eos_smem);
+  Chem c(E);
   double lev[kEL];
   double nH0;
   int st = 0;
@@ -699,8 +695,7 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_var(EosArgs A) {
   const int v = (int)(r % A.nvar), x = (int)(r / A.nvar);
   if (A.active && !A.active[p]) return;
   const EosDev &E = *A.tab;
-  extern __shared__ double eos_smem[];
-  Chem c(E, eos_smem);
+  Chem c(E);
   int st = 0;
   double f[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES];
   const size_t cv = ((size_t)p * A.nvar + v) * A.nd + x;
@@ -822,8 +817,7 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_col(const EosDev *tab, int 
   auto row = [&](int k) { return c[(size_t)k * nd]; };
   const double T = row(2) > 3200.0 ? row(2) : 3200.0;
   const double Nt = row(3) / (cK * T);
-  extern __shared__ double eos_smem[];
-  Chem ch(E, eos_smem);
+  Chem ch(E);
   int st = 0;
   double f[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES];
   thermal_fields(E, ch, T, Nt, f, st);
@@ -844,7 +838,7 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_col(const EosDev *tab, int 
 // ---- host side ---------------------------------------------------------------------------------------------
 struct EosCtx {
   EosDev *d_tab = nullptr;
-  int npar = 0, ntherm = 0, nst = 0;
+  int npar = 0, ntherm = 0;
   std::vector<int> kind;
   std::vector<double> ref_step;
   // work buffers for cap pixels
@@ -862,9 +856,6 @@ struct EosCtx {
   int *d_cst = nullptr;
   int cap_col = 0;
 };
-
-// dynamic shared memory of the chemistry kernels: the T-only stage factors of each thread
-size_t eos_smem_bytes(const EosCtx *e, int threads) { return sizeof(double) * 2 * (size_t)e->nst * threads; }
 
 void eos_free_bufs(EosCtx *e) {
   void *b[] = {e->d_T, e->d_Nt, e->d_nodes, e->d_step, e->d_Ntout, e->d_active, e->d_status, e->d_rec, e->d_tan,
@@ -1154,14 +1145,6 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
   SNAPI_CK(cudaMemcpy(e->d_tab, &H, sizeof(EosDev), cudaMemcpyHostToDevice));
   e->npar = m->npar;
   e->ntherm = H.kcount[1];
-  e->nst = H.nst;
-  // up to 2 x 64 stages x 64 threads x 8 B = 64 KB of stage factors per CTA
-  SNAPI_CK(cudaFuncSetAttribute(k_eos_he, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)eos_smem_bytes(e, kHeThreads)));
-  SNAPI_CK(cudaFuncSetAttribute(k_eos_var, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)eos_smem_bytes(e, kRecThreads)));
-  SNAPI_CK(cudaFuncSetAttribute(k_eos_col, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)eos_smem_bytes(e, kRecThreads)));
   e->kind.assign(m->node_kind, m->node_kind + m->npar);
   e->ref_step.assign(m->npar, 0.0);
   static const double ref_step[7] = {0.0, 5.0, 20.0, 20.0, 0.01, 0.001, 0.001};  // const.h:27-32
@@ -1268,11 +1251,10 @@ static int build_impl(snapi_ctx *ctx, int npix, const double *nodes, const int *
     SNAPI_CK(cudaMemsetAsync(e->d_status, 0, sizeof(int) * nb, ctx->stream));
     SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
     const int nhe = nb * nvar;
-    k_eos_he<<<(nhe + kHeThreads - 1) / kHeThreads, kHeThreads, eos_smem_bytes(e, kHeThreads), ctx->stream>>>(A);
+    k_eos_he<<<(nhe + kHeThreads - 1) / kHeThreads, kHeThreads, 0, ctx->stream>>>(A);
     SNAPI_CK(cudaGetLastError());
     const long long nvx = (long long)nb * nvar * nd;
-    k_eos_var<<<(unsigned)((nvx + kRecThreads - 1) / kRecThreads), kRecThreads, eos_smem_bytes(e, kRecThreads),
-                ctx->stream>>>(A);
+    k_eos_var<<<(unsigned)((nvx + kRecThreads - 1) / kRecThreads), kRecThreads, 0, ctx->stream>>>(A);
     SNAPI_CK(cudaGetLastError());
     const int nrec = nb * nd;
     ctx->last_launches += 2;
@@ -1368,8 +1350,7 @@ int snapi_records_from_columns(snapi_ctx *ctx, int npix, const double *columns, 
     SNAPI_CK(cudaMemsetAsync(e->d_cst, 0, sizeof(int) * nb, ctx->stream));
     SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
     const int n = nb * nd;
-    k_eos_col<<<(n + kRecThreads - 1) / kRecThreads, kRecThreads, eos_smem_bytes(e, kRecThreads), ctx->stream>>>(
-        e->d_tab, nb, nd, nf, cols,
+    k_eos_col<<<(n + kRecThreads - 1) / kRecThreads, kRecThreads, 0, ctx->stream>>>(e->d_tab, nb, nd, nf, cols,
                                                                                     host ? e->d_crec : rec, e->d_cst);
     SNAPI_CK(cudaGetLastError());
     SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
