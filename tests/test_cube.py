@@ -237,3 +237,28 @@ def test_cube_synth_errors(sb, config3, tmp_path):
     with pytest.raises(sb.SnapiError, match="depth grid"):
         ctx.cube_synth(str(grid))
     ctx.close()
+
+
+def test_invert_then_synthesise_round_trip(sb, config4, f0, tmp_path):
+    """The two branches of the job close on each other through the reference's file formats: the
+    atmosphere cube the invert job writes (inverted_atmos.f0), synthesised by the synthesis job,
+    gives back the fitted spectra the invert job wrote (inverted_spectra.f0), within 1e-6 I_c (the
+    columns' records are rebuilt from the written pressures and angles)."""
+    fx = config4
+    api = sb.api
+    sub = [int(v) for v in f0["cube_sub"]]
+    cube = tmp_path / "obs.f0"
+    cube.write_bytes(bytes(f0["cube_f32_file"]))
+    kinds = fx["node_kind"]
+    ctx = _setup(sb, config4)
+    ctx.cube_invert(str(cube), kinds, 1e-2 * node_scales(kinds), nodes0=fx["nodes0"][0], subfield=sub[:4],
+                    window=sub[4:], obs_qs=2.0, synth_qs=1.0, out_spectra=str(tmp_path / "inv_spec.f0"),
+                    out_atmos=str(tmp_path / "inv_atmos.f0"), max_iter=4)
+    out = ctx.cube_synth(str(tmp_path / "inv_atmos.f0"), out_spectra=str(tmp_path / "syn_spec.f0"))
+    ctx.close()
+    assert out["stats"]["flagged"] == 0
+    a = api.f0_read(str(tmp_path / "inv_spec.f0"))
+    b = api.f0_read(str(tmp_path / "syn_spec.f0"))
+    assert a.shape == b.shape
+    ic = np.abs(a[:, :, 0]).max()
+    assert np.abs(a - b).max() / ic < 1e-6
