@@ -1,14 +1,14 @@
 // The master's inversion job (master/job.cc:304-379, 570-597) with every pixel fitted on the GPU
 // and the cube streamed between .f0 files and HBM.
 //
-// Reference flow: read the whole observed cube (read_file 4-D, fileio.cc:72-106) and transpose it
+// Reference flow: read the whole observed cube (read_file 4-D, fileio.cc:54-87) and transpose it
 // (mathtools.cc:603-613) into S[x][y][s][l]; scale it by synth_qs / obs_qs (observable::normalize,
 // obs.cc:398-408); cut the subfield and wavelength window (observable::extract, obs.cc:360-390),
 // writing it to cube_to_invert.f0; pack one task per pixel with its starting model (the job's
 // model, or model_cube[x][y] of a model cube, job.cc:347-369) for the islaves, which run
 // stokes_lm_fit; collect the fitted nodes and spectra and write inverted_nodes.f0 (write_file 3-D,
-// fileio.cc:279-292), inverted_atmos.f0 (the 12 return_as_array rows of each fitted column) and
-// inverted_spectra.f0 (write_file 4-D, fileio.cc:318-329).
+// fileio.cc:274-287), inverted_atmos.f0 (the 12 return_as_array rows of each fitted column) and
+// inverted_spectra.f0 (write_file 4-D, fileio.cc:320-329).
 //
 // Here one batch ("chunk") of subfield pixels at a time travels as a contiguous run of file rows:
 // the file stores each pixel's [4][nl] block contiguously (dims (nl, 4, ny, nx)), so a chunk of
