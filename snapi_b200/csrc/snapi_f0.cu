@@ -174,6 +174,7 @@ int parse(int fd, snapi_f0_info *info) {
     info->dim[d] = (int32_t)rd32(b0 + 192 + 4 * d);
     if (info->dim[d] < 0) return fail(SNAPI_EINVAL, "f0: negative dimension");
     n *= info->dim[d];
+    if (n > (int64_t(1) << 50)) return fail(SNAPI_EINVAL, "f0: too many elements");
   }
   info->nelem = n;
   info->data_offset = (long long)nhb * 512;
