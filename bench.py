@@ -1,6 +1,6 @@
 """Benchmark: pixels/s of Stokes synthesis + chi2 gradient w.r.t. 10 nodes on one B200.
 
-Workload (configs[2] of the metric): 64 x 64 pixels, 80 depths (log tau500 -6..1), 201 wavelengths
+Workload (the responses-and-adjoint configuration): 64 x 64 pixels, 80 depths (log tau500 -6..1), 201 wavelengths
 (Fe I 6301.5 / 6302.5, 12 mA), mu = 1, ten-node model (T x4, v_turb, v_los x2, B, inclination,
 azimuth).  One step = one call over all pixels: forward synthesis, chi2 against a noisy target
 and the adjoint (reverse) sweep giving d chi2 / d node for every pixel.
