@@ -1,6 +1,6 @@
 // Shared helpers of the oracle drivers that run the compiled reference (test infrastructure).
 //
-// The drivers follow the reference's own job flow (SURVEY call stack A/B):
+// The drivers follow the reference's own job flow (jsub set-up, then the islave calls):
 //   jsub:   gcfg -> atmos_new(acfg) -> pack -> atmos_new(buf) -> init -> extract(1,1)
 //   islave: atmos_new(buf) -> build_from_nodes / obs_stokes / obs_stokes_responses_to_nodes /
 //           stokes_lm_fit

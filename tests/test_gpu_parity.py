@@ -74,7 +74,7 @@ def test_adjoint_gradient(sb, oracle_lib, config3):
         _, g_same = oracle_grad(oracle_lib, fx, p, fx["target"][p] + (s64[p] - out["stokes"][p]))
         assert scaled_rel_err(out["grad"][p], g_same, fx["node_kind"]) < 1e-3
         # (b) against the FP64 model with the same noisy target: near the minimum the gradient is a
-        # sum of random-sign terms that amplifies the ~1e-6 Ic FP32 forward error (see DESIGN.md)
+        # sum of random-sign terms that amplifies the ~1e-6 Ic FP32 forward error
         c_ref, g_ref = oracle_grad(oracle_lib, fx, p, fx["target"][p])
         assert abs(out["chi2"][p] - c_ref) < 1e-4 * c_ref
         assert scaled_rel_err(out["grad"][p], g_ref, fx["node_kind"]) < 2e-2
