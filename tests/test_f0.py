@@ -174,3 +174,34 @@ def test_job_cube_steps_restated(api, fx, tmp_path):
         c2i = tmp_path / ("c2i_%s.f0" % tag)
         api.f0_write(str(c2i), S)
         assert c2i.read_bytes() == bytes(fx["cube_%s_c2i" % tag]), tag
+
+
+def test_streaming_writer_concurrent_ranges(api, tmp_path):
+    """snapi_f0_write_at from several host threads at once (positioned writes of disjoint ranges, as
+    the invert job's writer thread and a caller's own threads may issue them) gives the same file as
+    one snapi_f0_write."""
+    import threading
+    L = api.lib()
+    a = np.random.default_rng(7).standard_normal((64, 4, 201)).astype(np.float64)
+    ref = tmp_path / "ref.f0"
+    api.f0_write(str(ref), a)
+    dims = (ctypes.c_longlong * 3)(201, 4, 64)
+    st = ctypes.c_int(0)
+    out = tmp_path / "par.f0"
+    f = L.snapi_f0_create(str(out).encode(), api.F0_FLOAT64, 3, dims, None, ctypes.byref(st))
+    flat = a.ravel()
+    per = 4 * 201
+    rc = []
+
+    def work(k):
+        for px in range(k, 64, 8):
+            rc.append(L.snapi_f0_write_at(f, px * per, per, flat[px * per:].ctypes.data))
+
+    threads = [threading.Thread(target=work, args=(k,)) for k in range(8)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert rc and all(r == 0 for r in rc)
+    assert L.snapi_f0_close(f) == 0
+    assert out.read_bytes() == ref.read_bytes()
