@@ -33,3 +33,32 @@ def test_zeeman_pattern_from_library(oracle_lib):
             assert a.ncomp[g] == b.ncomp[g]
             for i in range(a.ncomp[g]):
                 assert abs(a.S[g][i] - b.S[g][i]) < 1e-15 and abs(a.D[g][i] - b.D[g][i]) < 1e-15
+
+
+def test_ctypes_mirror_matches_header_layout(tmp_path):
+    """Every ctypes structure of the Python mirror has the size and field offsets the C compiler
+    gives the header's struct (a mismatch would pass garbage through the ABI without an error)."""
+    import subprocess
+    from snapi_b200 import api, eos_tables as et
+    structs = {api.SnapiLine: "snapi_line", api.SnapiProblem: "snapi_problem", api.SnapiLmOpts: "snapi_lm_opts",
+               api.F0Info: "snapi_f0_info", api.CubeJob: "snapi_cube_job", api.CubeStats: "snapi_cube_stats",
+               api.CubeSynthJob: "snapi_cube_synth_job", api.SnapiAliProblem: "snapi_ali_problem",
+               api.SnapiAliColumns: "snapi_ali_columns", et.SnapiPartition: "snapi_partition",
+               et.SnapiEosLevel: "snapi_eos_level", et.SnapiEosAtom: "snapi_eos_atom",
+               et.SnapiEosMolecule: "snapi_eos_molecule", et.SnapiEosLine: "snapi_eos_line",
+               et.SnapiEosModel: "snapi_eos_model"}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "snapi_cuda.h"', "int main(void) {"]
+    expect = []
+    for cls, cname in structs.items():
+        lines.append('  printf("%%zu\\n", sizeof(%s));' % cname)
+        expect.append(ctypes.sizeof(cls))
+        for fname, _ in cls._fields_:  # a trailing underscore stands for a Python keyword
+            lines.append('  printf("%%zu\\n", offsetof(%s, %s));' % (cname, fname.rstrip("_")))
+            expect.append(getattr(cls, fname).offset)
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got == expect
