@@ -292,10 +292,7 @@ def run_snapi(args):
             "vs_baseline": None,
             "dtype": "f32 (profiles, formal solver); f64 (optical depth, DELO weights, W4 core derivative)",
             "data": "synthetic: reference-built columns (HE + chemistry) x seeded per-pixel field/velocity nodes",
-            "config": {"workload": ("64x64" if NPIX == 64 * 64 else str(NPIX)) +
-                                   " pixels x 80 depths x 201 wavelengths, Fe I 6301.5/6302.5, mu=1, "
-                                   "10 nodes (T x4, vturb, vlos x2, B, incl, azi): synthesis + chi2 + adjoint "
-                                   "d chi2/d nodes", "pixels_per_gpu": NPIX, "nd": int(nd), "nlambda": int(nl),
+            "config": {"workload": workload_name(NPIX), "pixels_per_gpu": NPIX, "nd": int(nd), "nlambda": int(nl),
                        "npar": int(npar), "node_tangents": "packed: %d of %d record-field columns per pixel"
                                                             % (ntcol, npar * nf),
                        "l2_flush": "inputs (0.18 GB) and adjoint state (8 GB) per step exceed the 126 MB L2",
@@ -592,6 +589,11 @@ def reference_cpu_rate(samples_per_core=1, mode=1, cores=None):
             "wall_s": wall}
 
 
+def workload_name(npix):
+    return (("64x64" if npix == 64 * 64 else str(npix)) + " pixels x 80 depths x 201 wavelengths, Fe I 6301.5/6302.5, "
+            "mu=1, 10 nodes (T x4, vturb, vlos x2, B, incl, azi): synthesis + chi2 + adjoint d chi2/d nodes")
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -623,9 +625,12 @@ def run_reference(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic: seeded config-3 node models (seed 3), the reference builds the columns itself",
-        "config": {"workload": "config-3 pixels (80 depths x 201 wavelengths, 10 nodes): build_from_nodes + "
-                               "obs_stokes_responses_to_nodes (synthesis + node responses)",
+        "data": "synthetic: seeded node models of the workload's distribution (seed 3); the reference builds "
+                "the columns itself",
+        "config": {"workload": workload_name(NPIX),
+                   "sample": "each step a bounded sample of that workload: %d of its pixels (one per host core), "
+                             "each through the reference's build_from_nodes + obs_stokes_responses_to_nodes "
+                             "(synthesis + node responses, the quantities the gradient needs)" % ncores,
                    "pixels_per_step": ncores, "parallelism": "one process per host core"},
         "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": "pixels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
