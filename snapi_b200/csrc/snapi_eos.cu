@@ -132,10 +132,11 @@ struct EosDev {
 struct Chem {
   const EosDev &E;
   double T, kT;
-  struct SLoc {  // 24 bytes: the sweeps read every stage's entry ~20 times per solve
+  struct __align__(16) SLoc {
     double Ut;  // T-only part of U (whole U for CONST / IRWIN / NONE)
     double cz;  // fct exp(-chi / kT): the T-only factor of the stage ratio
     double Dz;  // 31.321 z^2 x
+    double pad;
   } sl[kES];
   double w2[kET];   // g2 exp(-2.302585 ee x)
   double K[kEM];
