@@ -365,7 +365,8 @@ def bench_lm(sb, pool, ic, device, npix=4096, iters=10):
             "device_pixel_steps_per_s": npix * steps / (dev_ms / 1e3), "wall_s_with_host_linear_builder": wall,
             "median_iterations": float(np.median(res["iters"])),
             "note": "device work per step: synthesis at the trial nodes, Jacobian (2 npar solves) at accepted "
-                    "nodes, FP64 J^T J and damped eigen-solve; node -> record map on the host"}
+                    "nodes, J^T J / J^T r on the tcgen05 tensor cores (3xTF32 split, FP32 accumulation), FP64 "
+                    "damped eigen-solve; node -> record map on the host"}
 
 
 def _eos_tables():

@@ -440,11 +440,13 @@ int snapi_last_launches(const snapi_ctx *ctx);
  * No context and no allocation: every work buffer lives in one static device array of
  * SNAPI_STATIC_SCRATCH_BYTES (64 MiB) that each GPU loading this library holds until the process
  * exits.  All array arguments are device pointers on `device`; w_stokes is a host array [4];
- * `stream` is a cudaStream_t (NULL = default stream).  The call returns when the results are in
- * place.  Pixels are processed in batches that fit the static array; a problem whose single pixel
- * does not fit (at nd = 80 and 201 wavelengths one pixel needs ~1.4 MB) is rejected with
- * SNAPI_EINVAL.  The first call on a device looks up the array's device address; make that first
- * call before any stream capture.  Calls share the array: calls that overlap on the GPU race.
+ * `stream` is a cudaStream_t created on `device` (NULL = default stream; a stream of another
+ * device is rejected with SNAPI_EINVAL).  Every call waits for its stream (cudaStreamSynchronize)
+ * and returns when the results are in place.  Pixels are processed in batches that fit the static
+ * array; a problem whose single pixel does not fit (at nd = 80 and 201 wavelengths one pixel needs
+ * ~1.4 MB) is rejected with SNAPI_EINVAL.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream capture.  Calls share
+ * the array and the kernels' shared-memory limits: calls that overlap on the GPU race.
  * On error, snapi_noalloc_last_error() (per host thread) describes it. */
 #define SNAPI_STATIC_SCRATCH_BYTES (64u << 20)
 int snapi_adjoint_noalloc(const snapi_problem *prob, int device, void *stream, int npix, const float *records,

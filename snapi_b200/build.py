@@ -49,8 +49,8 @@ def build_oracle():
     present, the compiled-reference drivers."""
     odir = os.path.join(ROOT, "oracle")
     subprocess.run(["make", "-s", "-C", odir, "oracle"], check=True)
-    if os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-s", "-j8", "-C", odir, "ref"], check=True)
+    # the Makefile knows where the reference checkout is (its REF variable) and skips it if absent
+    subprocess.run(["make", "-s", "-j8", "-C", odir, "ref-if-present"], check=True)
 
 
 def build_emulator():

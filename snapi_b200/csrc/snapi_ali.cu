@@ -468,6 +468,7 @@ snapi_ali_ctx *snapi_ali_create(const snapi_ali_problem *p, int device, int *sta
   }
   if (p->nd > 1024) { ali_err(c, SNAPI_EINVAL, "nd > 1024"); return fail(c, SNAPI_EINVAL); }
   if (cudaSetDevice(device) != cudaSuccess) { ali_err(c, SNAPI_ECUDA, "cudaSetDevice failed"); return fail(c, SNAPI_ECUDA); }
+  int maxsm = 0;
   std::vector<double> ct(p->nray);
   for (int r = 0; r < p->nray; ++r) ct[r] = cos(p->ray_theta[r]);
   std::vector<float> fud(p->fudge, p->fudge + p->nlambda), sig((size_t)c->nbf * p->nlambda);
@@ -491,7 +492,10 @@ snapi_ali_ctx *snapi_ali_create(const snapi_ali_problem *p, int device, int *sta
   if (!ok) { ali_err(c, SNAPI_ENOMEM, "device allocation failed"); return fail(c, SNAPI_ENOMEM); }
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaFuncSetAttribute(k_ali_formal, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S.total) != cudaSuccess) {
+      // the limit is per device and shared by every ALI context: the opt-in maximum, not this
+      // problem's size, so a smaller context never lowers it under a larger one
+      cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
+      cudaFuncSetAttribute(k_ali_formal, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm) != cudaSuccess) {
     ali_err(c, SNAPI_ECUDA, "stream / event / attribute set-up failed");
     return fail(c, SNAPI_ECUDA);
   }

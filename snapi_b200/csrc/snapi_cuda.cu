@@ -426,6 +426,20 @@ int check_status(snapi_ctx *ctx) {
 
 }  // namespace snapi
 
+namespace snapi {
+// Dynamic shared-memory limit of every kernel launched with more than 48 KB, set to `bytes` (the
+// device's opt-in maximum) on the current device.
+cudaError_t raise_smem_limits(int bytes) {
+  const void *k[] = {(const void *)k_synth, (const void *)k_fd_sweep, (const void *)k_resp_sweep,
+                     (const void *)k_adj_forward, (const void *)k_adj_opacity, (const void *)k_adjoint_finish};
+  for (const void *f : k) {
+    const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+}  // namespace snapi
+
 extern "C" {
 
 int snapi_zeeman_pattern(int ju2, int jl2, double gu, double gl, snapi_line *L) {
@@ -649,12 +663,10 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
   CKC(cudaMalloc(&ctx->d_seed, sizeof(float4) * B * ctx->lpad));
   CKC(cudaMalloc(&ctx->d_bars, sizeof(float4) * B * ctx->nl * 3 * ctx->nd));
   CKC(cudaMalloc(&ctx->d_opart, sizeof(float) * B * (1 + ctx->nlines) * op_slices(ctx->nd) * ctx->nd * kOpSlots));
-  CKC(cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
-  CKC(cudaFuncSetAttribute(k_fd_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
-  CKC(cudaFuncSetAttribute(k_resp_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
-  CKC(cudaFuncSetAttribute(k_adj_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
-  CKC(cudaFuncSetAttribute(k_adj_opacity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lsw.total));
-  CKC(cudaFuncSetAttribute(k_adjoint_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lfin.total));
+  // the kernels' dynamic shared-memory limit is a per-device attribute that every context (and the
+  // allocation-free adjoint) shares: raise it to the device's opt-in maximum, never to this
+  // problem's size, so that a smaller problem's context cannot lower it under a larger one's
+  CKC(raise_smem_limits(maxsm));
 #undef CKC
   if (ensure_npar(ctx, 1) != SNAPI_OK) return fail(ctx, SNAPI_ENOMEM);
   if (status) *status = SNAPI_OK;
@@ -976,7 +988,8 @@ int snapi_responses(snapi_ctx *ctx, int npix, const float *records, int npar, co
 // seed (lpad float4), the adjoint bars (nl x 3 x nd float4), the opacity-adjoint sums
 // ((1 + nlines) x nd x kOpSlots float) and the per-warp chi2 sums (nwarp double).  Pixels
 // are processed in chunks that fit the work region.
-// host-side stand-in, so its device address is fetched with cudaGetSymbolAddress -- once per
+// g_snapi_static is a __device__ array: in host code its name denotes only a host-side stand-in,
+// not device memory, so its device address is fetched with cudaGetSymbolAddress -- once per
 // device, by the first call on that device, with that device current.
 // Every call shares the array: the kernels overwrite every slot they read in the same call and
 // the status word is cleared at the start of each call; calls that overlap on the GPU (two host
@@ -1001,13 +1014,14 @@ int static_setup(int device, unsigned char **base, std::string &err) {
       err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
       return SNAPI_ECUDA;
     }
-    const int fin = 227 * 1024;
-    e = cudaFuncSetAttribute(k_adj_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, fin);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_adj_opacity, cudaFuncAttributeMaxDynamicSharedMemorySize, fin);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_adjoint_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, fin);
-    if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return SNAPI_ECUDA; }
     g_static_ptr[device] = static_cast<unsigned char *>(p);
   }
+  // The kernels' shared-memory limit is shared with every context on the device and set on every
+  // call (a context created since the last call must not leave it below what this call needs).
+  int maxsm = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  if (e == cudaSuccess) e = raise_smem_limits(maxsm);
+  if (e != cudaSuccess) { err = std::string("shared-memory limit: ") + cudaGetErrorString(e); return SNAPI_ECUDA; }
   *base = g_static_ptr[device];
   return SNAPI_OK;
 }
@@ -1154,6 +1168,15 @@ int snapi_adjoint_noalloc(const snapi_problem *prob, int device, void *stream, i
   int old = 0;
   if (cudaGetDevice(&old) != cudaSuccess) { g_noalloc_err = "cudaGetDevice failed"; return SNAPI_ECUDA; }
   if (cudaSetDevice(device) != cudaSuccess) { g_noalloc_err = "cudaSetDevice failed"; return SNAPI_ECUDA; }
+  if (stream) {  // the stream must belong to `device` (the NULL stream is the current device's)
+    int sdev = -1;
+    if (cudaStreamGetDevice(static_cast<cudaStream_t>(stream), &sdev) != cudaSuccess || sdev != device) {
+      cudaGetLastError();
+      cudaSetDevice(old);
+      g_noalloc_err = "snapi_adjoint_noalloc: the stream was not created on `device`";
+      return SNAPI_EINVAL;
+    }
+  }
   unsigned char *base = nullptr;
   int rc = static_setup(device, &base, g_noalloc_err);
   if (rc == SNAPI_OK && npix > 0)

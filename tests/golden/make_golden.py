@@ -53,6 +53,9 @@ sys.path.insert(0, HERE)
 from sbin import read_sbin  # noqa: E402
 
 DUMP = os.path.join(ROOT, "oracle", "_ref", "snapi_ref_dump")
+# the same driver over the reference with the configurations' stated settings patched in
+# (oracle/patch_spec.py: stokes_lm_fit's DELTA 1e-4, the 5-point angle set, nltepops' 1e-4 stop)
+DUMP_SPEC = os.path.join(ROOT, "oracle", "_ref", "snapi_ref_dump_spec")
 CFG_FILES = ["atoms_6300.cfg", "mol.cfg", "hydrogen_3lvl.cfg", "helium.cfg", "carbon.cfg", "nitrogen.cfg",
              "oxygen.cfg", "calcium.cfg", "silicon.cfg", "aluminium.cfg", "iron_6300.cfg", "falc_80z.dat",
              "calcium_ir_rh.cfg"]
@@ -217,10 +220,12 @@ def config4_inputs(npix, seed=4):
     return truth, truth + C4_OFFSET, mask
 
 
-def make_config4(tmp, npix, iters=30, broadening=0.0, name="config4", seed=4, workers=0):
-    """Reference LM (stokes_lm_fit, DELTA 1e-3 as compiled, start lambda 1e3) on config-4 pixels,
-    one process per pixel; with broadening > 0 [cm] the targets are broadened by the reference's
-    own convolution and the fit broadens its synthesis and responses the same way."""
+def make_config4(tmp, npix, iters=30, broadening=0.0, name="config4", seed=4, workers=0, spec=False):
+    """Reference LM (stokes_lm_fit, start lambda 1e3) on config-4 pixels, one process per pixel;
+    with broadening > 0 [cm] the targets are broadened by the reference's own convolution and the
+    fit broadens its synthesis and responses the same way.  The relative chi2 stop rule is the
+    compiled DELTA 1e-3, or with spec the configuration's 1e-4 (the patched build)."""
+    lmfit_bin, delta = (DUMP_SPEC, 1e-4) if spec else (DUMP, 1e-3)
     task = os.path.join(tmp, "c3.tsk")
     truth, nodes0, mask = config4_inputs(npix, seed=seed)
     d = dump(tmp, task, truth, 0, "c4truth")
@@ -238,7 +243,7 @@ def make_config4(tmp, npix, iters=30, broadening=0.0, name="config4", seed=4, wo
     for i in range(npix):
         for nm, arr in (("n0", nodes0[i:i + 1]), ("tg", target[i:i + 1]), ("mk", mask[i:i + 1])):
             np.ascontiguousarray(arr, dtype="<f8").tofile(os.path.join(tmp, "c4_%s_%d.f64" % (nm, i)))
-        args = [DUMP, "lmfit", task] + [os.path.join(tmp, "c4_%s_%d.f64" % (nm, i)) for nm in ("n0", "tg", "mk")] + \
+        args = [lmfit_bin, "lmfit", task] + [os.path.join(tmp, "c4_%s_%d.f64" % (nm, i)) for nm in ("n0", "tg", "mk")] + \
                ["1", str(iters), os.path.join(tmp, "c4_fit_%d.sbin" % i), repr(broadening)]
         if workers and len(procs) >= workers:  # at most `workers` reference processes at a time
             if procs.pop(0).wait() != 0:
@@ -251,7 +256,7 @@ def make_config4(tmp, npix, iters=30, broadening=0.0, name="config4", seed=4, wo
     # the fitted Stokes only for the small fixtures (the 256-pixel one compares nodes and chi2)
     extra = {} if npix > 64 else {"fit_stokes": np.concatenate([f["fit_stokes"] for f in fits])}
     np.savez_compressed(os.path.join(HERE, name + ".npz"), lambda_air=d["lambda_air"], tau500=d["tau500"],
-                        broadening=np.array([broadening]),
+                        broadening=np.array([broadening]), delta=np.array([delta]),
                         node_kind=d["node_kind"], truth=truth, nodes0=nodes0, mask=mask, target=target,
                         fit_nodes=np.concatenate([f["fit_nodes"] for f in fits]), **extra,
                         fit_chi2=np.concatenate([f["fit_chi2"] for f in fits]),
@@ -304,7 +309,10 @@ def make_psf(tmp):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("SNAPI_REFERENCE", "/root/reference"),
+                    help="the reference checkout (default $SNAPI_REFERENCE, else /root/reference)")
+    ap.add_argument("--spec", action="store_true",
+                    help="config-4 fits with the configuration's DELTA 1e-4 (patched reference build)")
     ap.add_argument("--c2pix", type=int, default=16)
     ap.add_argument("--c3pix", type=int, default=8)
     ap.add_argument("--pool", type=int, default=32)
@@ -319,6 +327,7 @@ def main():
     ap.add_argument("--only-c4-subset", type=int, default=0, metavar="N",
                     help="config-4 fit of N pixels by the reference (8 processes at a time)")
     ap.add_argument("--c5col", type=int, default=3)
+    ap.add_argument("--workers", type=int, default=8, help="reference processes at a time (config-4 subset)")
     a = ap.parse_args()
     if not os.path.exists(DUMP):
         raise SystemExit("build the oracle first: make -C oracle")
@@ -337,20 +346,21 @@ def main():
             return
         if a.only_c4_subset:
             shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
-            make_config4(tmp, a.only_c4_subset, name="config4_%d" % a.only_c4_subset, seed=404, workers=8)
+            make_config4(tmp, a.only_c4_subset, name="config4_%d" % a.only_c4_subset, seed=404, workers=a.workers,
+                         spec=a.spec)
             return
         if a.only_psf:
             make_psf(tmp)
             shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
             # config 4 with the 45 mA instrumental profile of cfg/invert.cfg
-            make_config4(tmp, 4, broadening=45.0 * 1e-11 / 2.35, name="config4_psf")
+            make_config4(tmp, 4, broadening=45.0 * 1e-11 / 2.35, name="config4_psf", spec=a.spec)
             return
         if a.only_pool or a.only_c4 or a.only_c5:
             shutil.copy(os.path.join(HERE, "c3.tsk"), os.path.join(tmp, "c3.tsk"))
         else:
             make_configs_1_to_3(a, tmp)
         if a.c4pix and not a.only_c5:
-            make_config4(tmp, a.c4pix)
+            make_config4(tmp, a.c4pix, spec=a.spec)
         if a.c5col and not a.only_c4:
             make_config5(tmp, a.c5col)
         if a.pool and not (a.only_c4 or a.only_c5):
