@@ -380,6 +380,24 @@ typedef struct {
 /* Attach a node model to the context (tables copied to the device).  The problem's tau500 grid
  * must be 10^(log tau grid) of the model. */
 int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *model);
+
+/* How the chemistry (atmosphere::chemeq, atmos_chm.cc:28-330) of the hydrostatic march of
+ * snapi_build_records / snapi_build_atmos / snapi_adjoint_nodes / snapi_lm_fit starts each solve.
+ * The reference starts every solve cold: an ionisation-only quadratic for n_e and a halving loop to
+ * 1e-2 (atmos_chm.cc:129-171), then Newton to relative defects below 1e-4 -- about 20 ionisation
+ * sweeps per solve, ~18 of them in the start; the march does ~215 solves per column.
+ *   SNAPI_CHEM_START_CONTINUE (default): in the march, Newton from the previous solution of the
+ *     same column (the next hydrostatic iterate or depth, scaled by the particle-density ratio),
+ *     cold if that has not converged after 8 passes.  Same stop rule; ~2 sweeps per solve.  The
+ *     march's particle densities agree with the cold start's to ~3e-8 relative (the size of the
+ *     last Newton update); the record solves at the final (T, Nt) start cold as the reference's do,
+ *     so records agree to ~4e-8 relative and node tangents to ~4e-5 of each field's scale (the noise
+ *     the 1e-4 stop leaves in the reference's own 5 K differences).
+ *   SNAPI_CHEM_START_COLD: the reference's start at every solve (its iterates, to rounding).
+ * Needs a node model (snapi_eos_set); the setting lasts until changed or the next snapi_eos_set. */
+#define SNAPI_CHEM_START_CONTINUE 0
+#define SNAPI_CHEM_START_COLD 1
+int snapi_eos_chem_start(snapi_ctx *ctx, int mode);
 /* Records [npix][nd][nfield] (float) of the node vectors nodes [npix][npar] (double), the particle
  * density Nt [npix][nd] (double, may be NULL) and, if tangents != NULL, the node tangents
  * [npix][npar][nd][nfield] with central-difference steps step [npar] (NULL: the reference's 5 K,
@@ -389,6 +407,18 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *model);
  * last iterate), 2 (a hydrostatic step hit its cap), 4 (non-finite values). */
 int snapi_build_records(snapi_ctx *ctx, int npix, const double *nodes, const int *active, float *records,
                         double *Nt, float *tangents, const double *step, int *pix_status, int mem);
+
+/* Stokes synthesis, chi2 and its gradient with respect to the nodes, from node vectors: the work of
+ * the reference's build_from_nodes + obs_stokes + obs_stokes_responses_to_nodes (atmos_pp.cc:58-248,
+ * atmos_obs.cc:16-87, atmos_fit.cc:1205-1352) contracted with the weighted residual as
+ * stokes_lm_fit forms J^T r (atmos_fit.cc:125-137), i.e. d chi2 / d node without the responses.
+ * Per chunk of max_batch pixels: snapi_build_records of nodes [npix][npar] with tangents (the
+ * reference's steps) into the context's device buffers, then snapi_adjoint on them.  obs, mask,
+ * w_stokes, stokes, chi2 as snapi_adjoint; grad [npix][npar] (double) in the model's node order;
+ * pix_status [npix] (may be NULL) the build's status bits.  Needs a node model (snapi_eos_set).
+ * snapi_last_kernel_ms: the build's and the adjoint's device time together. */
+int snapi_adjoint_nodes(snapi_ctx *ctx, int npix, const double *nodes, const float *obs, const double *w_stokes,
+                        const float *mask, float *stokes, double *chi2, double *grad, int *pix_status, int mem);
 
 /* The columns of the node vectors as the master collects them after a fit: the 12 rows of
  * atmosphere::return_as_array (atmos.cc:547-569) after build_from_nodes and compute_op_referent,
@@ -429,8 +459,17 @@ void snapi_host_free(void *p);
  * call, measured with CUDA events on that stream [ms]. */
 void *snapi_stream(snapi_ctx *ctx);
 double snapi_last_kernel_ms(const snapi_ctx *ctx);
+/* Device time [ms] of one phase of the last snapi_adjoint_nodes call: 0 the node build (records and
+ * tangents), 1 the adjoint (synthesis, chi2, reverse sweep, chain rule); 0 for other calls' phases. */
+double snapi_last_phase_ms(const snapi_ctx *ctx, int phase);
 /* Number of kernel launches of the last call. */
 int snapi_last_launches(const snapi_ctx *ctx);
+
+/* The measured fused multiply-add peak of GPU `device` in TFLOP/s (fp64 = 0: FP32, 1: FP64): a
+ * kernel of independent FMA chains filling every SM, timed by CUDA events (best of three launches
+ * after a warm-up).  The denominator of the benchmark's compute rooflines; no counterpart in the
+ * reference. */
+int snapi_fma_peak(int device, int fp64, double *tflops);
 
 /* snapi_adjoint for callers that cannot allocate device memory: applications whose GPU memory
  * is owned by another allocator (a framework pool with a fixed budget) and loops that must not

@@ -182,7 +182,17 @@ typedef struct {
   double Natom[MA];
   double fk[MA][MS];
   int passes;
+  int have;        /* Ne / Natom hold an earlier solution of this column, at particle density Nt_prev */
+  double Nt_prev;
 } chem_state;
+
+/* How chemeq starts in the hydrostatic march (SNAPI_CHEM_START_*, the device's
+ * snapi_eos_chem_start): COLD, the reference's start at every solve (the default here); CONTINUE,
+ * the CUDA path's default -- Newton from the previous solution of the same column scaled by the
+ * particle-density ratio, at most 8 passes, else the cold start.  The record solves start cold in
+ * either mode.  Restated here so that the device's continued start has an exact-path checker; the
+ * reference itself always starts cold. */
+static int g_chem_start = SNAPI_CHEM_START_COLD;
 
 static void chemeq(const snapi_eos_model *m, double T, double Nt, chem_state *out) {
   const int na = m->natom, nm = m->nmol;
@@ -234,6 +244,20 @@ static void chemeq(const snapi_eos_model *m, double T, double Nt, chem_state *ou
   double bb = F1 / S1 - aa;
   double cc = -bb * Nt;
   bb += 1.0 - aa * Nt;
+  /* the continued start (g_chem_start): Newton from the previous solution, the cold start if
+     that has not converged after 8 passes or left non-finite values */
+  int warm = g_chem_start == SNAPI_CHEM_START_CONTINUE && out->have;
+  int maxpass = 50;
+  if (warm) {
+    const double sc = Nt / out->Nt_prev;
+    N[0] = out->Ne * sc;
+    for (int a = 1; a <= na; ++a) N[a] = out->Natom[a - 1] * sc;
+    maxpass = 8;
+    goto newton;
+  }
+cold:
+  warm = 0;
+  maxpass = 50;
   N[0] = fmax((-bb + sqrt(bb * bb - 4.0 * aa * cc)) / (2.0 * aa), 1.0);
   double esum;
   do {
@@ -246,6 +270,7 @@ static void chemeq(const snapi_eos_model *m, double T, double Nt, chem_state *ou
     N[0] = 0.5 * (N[0] + esum);
   } while ((1E-2 * (N[0] + esum)) < fabs(N[0] - esum));
   /* Newton-Raphson (atmos_chm.cc:176-305) */
+newton:;
   const int n = na + 1;
   double d[MA + 1], A[(MA + 1) * (MA + 1)];
   int iter = 0, conv;
@@ -309,17 +334,25 @@ static void chemeq(const snapi_eos_model *m, double T, double Nt, chem_state *ou
     double v[MA + 1];
     for (int i = 0; i < n; ++i) v[i] = d[i];
     gauss_solve(n, A, v);
+    int finite = 1;
     for (int a = 0; a <= na; ++a) {
       N[a] -= v[a];
       if (N[a] < 1E-2) N[a] = 1E-2;
+      finite &= isfinite(N[a]) != 0;
     }
+    if (!finite && warm) goto cold;
     iter += 2;   /* ++iter in the message and iter++ after it (atmos_chm.cc:294, 300) */
-    if (iter > 100) break;
+    if (iter > 2 * maxpass) {
+      if (warm) goto cold;
+      break;
+    }
     conv = 1;
     for (int i = 0; i <= na; ++i) if (fabs(d[i] / N[i]) > 1E-4) conv = 0;
   } while (!conv);
   out->Ne = N[0];
-  out->passes = iter > 100 ? -iter / 2 : iter / 2;
+  out->have = 1;
+  out->Nt_prev = Nt;
+  out->passes = iter > 2 * maxpass ? -iter / 2 : iter / 2;
   for (int a = 1; a <= na; ++a) {
     out->Natom[a - 1] = N[a];
     for (int z = 0; z < nk[a]; ++z) out->fk[a - 1][z] = fk[a][z];
@@ -530,6 +563,7 @@ static void hydrostatic(const snapi_eos_model *m, int nd, column *c) {
   const double break_me = 1E-2;
   double op[MAXD], rho[MAXD];
   cs.Ne = 1.0;
+  cs.have = 0;
   c->Nt[0] = 0.3 / C_K / c->T[0];
   for (int iter = 0; iter < MAX_ITER; ++iter) {
     op[0] = chem_point(m, c->T[0], c->Nt[0], &cs, &P, 0);
@@ -569,6 +603,7 @@ static void record_depth(const snapi_eos_model *m, int nlines, const double *lam
   pops P;
   const double T = c->T[x];
   cs.Ne = 1.0;
+  cs.have = 0;  /* record solves start cold in either mode (their fields follow the solve's path) */
   double kap = chem_point(m, T, c->Nt[x], &cs, &P, 1);
   if (cs.passes < 0) *status |= 1;
   const double Ne = cs.Ne;
@@ -627,6 +662,13 @@ static void record_depth(const snapi_eos_model *m, int nlines, const double *lam
 
 /* ---- exported ------------------------------------------------------------------------------------ */
 
+/* The chemistry start of the following calls (SNAPI_CHEM_START_COLD or _CONTINUE); returns the old. */
+int sne_set_chem_start(int mode) {
+  const int old = g_chem_start;
+  g_chem_start = mode;
+  return old;
+}
+
 /* Chemistry of one (T, Nt) point: Ne, stage totals [natom][MS], level populations [natom][MS][ML],
  * kappa at lambda_he and lambda_kappa.  Returns the Newton passes (negative: cap reached). */
 int sne_chem(const snapi_eos_model *m, double T, double Nt, double *Ne, double *Nst, double *npop, double *kap_he,
@@ -634,6 +676,7 @@ int sne_chem(const snapi_eos_model *m, double T, double Nt, double *Ne, double *
   chem_state cs;
   pops P;
   cs.Ne = 1.0;
+  cs.have = 0;
   *kap_he = chem_point(m, T, Nt, &cs, &P, 0);
   *kap = opacity_continuum(m, T, cs.Ne, &P, 1);
   *Ne = cs.Ne;
@@ -678,6 +721,7 @@ int sne_atmos(const snapi_eos_model *m, int nd, const double *nodes, const doubl
     chem_state cs;
     pops P;
     cs.Ne = 1.0;
+    cs.have = 0;
     const double kap = chem_point(m, c.T[x], c.Nt[x], &cs, &P, 1);
     if (cs.passes < 0) c.status |= 1;
     const double Bx = c.B[x] * sin(c.th[x]) * cos(c.ph[x]);

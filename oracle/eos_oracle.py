@@ -30,10 +30,21 @@ def lib():
         L.sne_columns.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D]
         L.sne_atmos.restype = ctypes.c_int
         L.sne_atmos.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
+        L.sne_set_chem_start.restype = ctypes.c_int
+        L.sne_set_chem_start.argtypes = [ctypes.c_int]
         L.sne_tangents.restype = ctypes.c_int
         L.sne_tangents.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D]
         _ready = True
     return L
+
+
+CHEM_START_CONTINUE, CHEM_START_COLD = 0, 1  # SNAPI_CHEM_START_*
+
+
+def set_chem_start(mode):
+    """The chemistry start of the following builds (the reference's cold start by default, or the
+    CUDA path's continued start in the hydrostatic march); returns the previous mode."""
+    return lib().sne_set_chem_start(int(mode))
 
 
 def _p(a):

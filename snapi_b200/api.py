@@ -19,6 +19,7 @@ LIB_PATH = os.environ.get("SNAPI_LIB", os.path.join(_PKG, "libsnapi_cuda.so"))
 
 OK, EINVAL, ECUDA, ETIMEOUT, ENONCONV, ENOMEM = 0, -1, -2, -3, -4, -5
 MEM_HOST, MEM_DEVICE = 0, 1
+CHEM_START_CONTINUE, CHEM_START_COLD = 0, 1  # SNAPI_CHEM_START_*
 NFIELD0 = 12
 MAX_LINES = 16  # SNAPI_MAX_LINES
 MAX_COMP = 16
@@ -155,6 +156,11 @@ def lib():
         L.snapi_adjoint_packed.argtypes = [vp, ip, fp, fp, fp, fp, ip, fp, fp, fp, fp, fp, ip]
         L.snapi_spectral_broaden.argtypes = [vp, ip, fp, ctypes.c_double, ip]
         L.snapi_eos_set.argtypes = [vp, vp]
+        L.snapi_eos_chem_start.argtypes = [vp, ip]
+        L.snapi_adjoint_nodes.argtypes = [vp, ip, fp, fp, fp, fp, fp, fp, fp, fp, ip]
+        L.snapi_fma_peak.argtypes = [ip, ip, ctypes.POINTER(ctypes.c_double)]
+        L.snapi_last_phase_ms.restype = ctypes.c_double
+        L.snapi_last_phase_ms.argtypes = [vp, ip]
         L.snapi_build_records.argtypes = [vp, ip, fp, fp, fp, fp, fp, fp, fp, ip]
         L.snapi_build_atmos.argtypes = [vp, ip, fp, fp, fp, fp, fp, ip]
         L.snapi_records_from_columns.argtypes = [vp, ip, fp, fp, fp, ip]
@@ -189,6 +195,15 @@ def lib():
         L.snapi_cube_synth.argtypes = [vp, ctypes.POINTER(CubeSynthJob), ctypes.POINTER(CubeStats)]
         _LIB = L
     return _LIB
+
+
+def fma_peak(device=0, fp64=False):
+    """Measured FMA peak of GPU `device` [TFLOP/s] (snapi_fma_peak): FP32, or FP64 with fp64."""
+    out = ctypes.c_double(0.0)
+    rc = lib().snapi_fma_peak(int(device), 1 if fp64 else 0, ctypes.byref(out))
+    if rc != 0:
+        raise SnapiError(rc, "snapi_fma_peak failed")
+    return out.value
 
 
 def zeeman_pattern(ju2, jl2, g_upper, g_lower):
@@ -337,6 +352,11 @@ class Context:
     @property
     def last_kernel_ms(self):
         return lib().snapi_last_kernel_ms(self._ctx)
+
+    @property
+    def last_phase_ms(self):
+        """(node build, adjoint) device time [ms] of the last adjoint_nodes call."""
+        return lib().snapi_last_phase_ms(self._ctx, 0), lib().snapi_last_phase_ms(self._ctx, 1)
 
     @property
     def last_launches(self):
@@ -526,6 +546,11 @@ class Context:
         self._check(lib().snapi_eos_set(self._ctx, ctypes.addressof(tables.model)))
         self._eos_npar = tables.npar
 
+    def eos_chem_start(self, mode):
+        """How the march's chemistry starts each solve: CHEM_START_CONTINUE (default; Newton from the
+        previous solution of the same column) or CHEM_START_COLD (the reference's start every time)."""
+        self._check(lib().snapi_eos_chem_start(self._ctx, int(mode)))
+
     def build_records(self, nodes, active=None, tangents=True, step=None, want_nt=False):
         """Column records [npix, nd, nfield] of node vectors [npix, npar] on the GPU (build_from_nodes +
         chemistry + the record set-up), with node tangents [npix, npar, nd, nfield] if `tangents`.
@@ -641,6 +666,35 @@ class Context:
         self._check(lib().snapi_adjoint_packed(self._ctx, npix, _ptr(rec), _ptr(ob), _ptr(ws), _ptr(mk), npar, _ptr(fm),
                                                _ptr(pt), _ptr(st), _ptr(chi2), _ptr(grad), MEM_HOST))
         return {"stokes": st, "chi2": chi2, "grad": grad.reshape(npix, npar)}
+
+    def adjoint_nodes(self, nodes, obs, w_stokes=(1.0, 1.0, 1.0, 1.0), mask=None, out=None):
+        """snapi_adjoint_nodes on host arrays: Stokes, chi2 and d chi2 / d node from node vectors
+        [npix, npar] (records and tangents built on the device).  out: optional dict of
+        preallocated (e.g. page-locked) result arrays "stokes", "chi2", "grad", "status"."""
+        nodes = np.ascontiguousarray(np.atleast_2d(nodes), dtype=np.float64)
+        npix, npar = nodes.shape
+        if npar != self._eos_npar:
+            raise ValueError("nodes have %d columns, the node model %d" % (npar, self._eos_npar))
+        ob = _f32(obs)
+        mk = _f32(mask)
+        ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
+        out = out or {}
+        st = out.get("stokes", np.zeros((npix, self.nl, 4), np.float32))
+        chi2 = out.get("chi2", np.zeros(npix))
+        grad = out.get("grad", np.zeros((npix, npar)))
+        status = out.get("status", np.zeros(npix, np.int32))
+        self._check(lib().snapi_adjoint_nodes(self._ctx, npix, _ptr(nodes), _ptr(ob), _ptr(ws), _ptr(mk), _ptr(st),
+                                              _ptr(chi2), _ptr(grad), _ptr(status), MEM_HOST))
+        return {"stokes": st, "chi2": chi2, "grad": grad, "status": status}
+
+    def adjoint_nodes_device(self, npix, nodes_ptr, obs_ptr, chi2_ptr, grad_ptr, stokes_ptr=None, mask_ptr=None,
+                             status_ptr=None, w_stokes=(1.0, 1.0, 1.0, 1.0)):
+        """snapi_adjoint_nodes on device buffers (raw device pointers)."""
+        ws = np.ascontiguousarray(w_stokes, dtype=np.float64)
+        opt = lambda v: _ptr(int(v)) if v else None  # noqa: E731
+        self._check(lib().snapi_adjoint_nodes(self._ctx, int(npix), _ptr(int(nodes_ptr)), _ptr(int(obs_ptr)), _ptr(ws),
+                                              opt(mask_ptr), opt(stokes_ptr), _ptr(int(chi2_ptr)),
+                                              _ptr(int(grad_ptr)), opt(status_ptr), MEM_DEVICE))
 
     def fd_grad_device(self, npix, rec_ptr, obs_ptr, npar, tan_ptr, step, chi2_ptr, grad_ptr,
                        w_stokes=(1.0, 1.0, 1.0, 1.0)):

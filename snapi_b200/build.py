@@ -13,7 +13,7 @@ LIB = os.path.join(PKG, "libsnapi_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["snapi_cuda.cu", "snapi_lm.cu", "snapi_ali.cu", "snapi_tc.cu", "snapi_psf.cu", "snapi_eos.cu",
-           "snapi_f0.cu", "snapi_cube.cu"]
+           "snapi_f0.cu", "snapi_cube.cu", "snapi_peak.cu"]
 HEADERS = ["snapi_core.cuh", "snapi_sweep.cuh", "snapi_internal.cuh", "snapi_f0_internal.h"]
 
 

@@ -511,6 +511,9 @@ void snapi_host_free(void *p) {
 const char *snapi_last_error(const snapi_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 void *snapi_stream(snapi_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 double snapi_last_kernel_ms(const snapi_ctx *ctx) { return ctx ? ctx->last_ms : 0.0; }
+double snapi_last_phase_ms(const snapi_ctx *ctx, int phase) {
+  return (ctx && phase >= 0 && phase < 2) ? ctx->phase_ms[phase] : 0.0;
+}
 int snapi_last_launches(const snapi_ctx *ctx) { return ctx ? ctx->last_launches : 0; }
 
 void snapi_destroy(snapi_ctx *ctx) {

@@ -145,8 +145,10 @@ struct Chem {
   double N[kEA + 1];
   double A[(kEA + 1) * (kEA + 1)], d[kEA + 1];
   int capped;
+  int have;        // N holds the solution of an earlier solve of this column, at particle density Nt_prev
+  double Nt_prev;
 
-  __device__ explicit Chem(const EosDev &e) : E(e), T(-1.0) {}
+  __device__ explicit Chem(const EosDev &e) : E(e), T(-1.0), have(0), Nt_prev(0.0) {}
 
   __device__ void set_T(double Tin) {
     T = Tin;
@@ -272,9 +274,38 @@ struct Chem {
 
   // atmosphere::chemeq (atmos_chm.cc:28-330): N[0] = Ne, N[1..na] free atoms; the kept fractions
   // fr are those of the last Newton sweep (before the last update), as pupdate uses them.
-  __device__ void solve(double Nt) {
-    const int na = E.natom, nm = E.nmol, n = na + 1;
+  //
+  // Two starts.  Cold (warm = false, or no earlier solution): the reference's, at every call --
+  // the ionisation-only quadratic for n_e and the halving loop to 1e-2 (atmos_chm.cc:129-171),
+  // ~18 of the ~20 ionisation sweeps of a solve.  Continued (warm = true, the hydrostatic march
+  // only): Newton from the previous solution of the same column scaled by the particle-density
+  // ratio (the next hydrostatic iterate at the same depth, or the next depth), ~2 sweeps; if that
+  // Newton has not met the stop rule after kWarmPasses passes, or left non-finite values, the
+  // cold start runs.  Both stop on the reference's rule (all relative defects below 1e-4 before
+  // the last update), so the march's opacities differ by up to that last update's size and its
+  // particle densities by ~3e-8 relative; the records' own solves always start cold (their stage
+  // fractions are those of the last sweep before the final update, i.e. they follow the path).
+  static constexpr int kWarmPasses = 8;
+
+  __device__ void solve(double Nt, bool warm) {
     capped = 0;
+    if (warm && have) {
+      const double sc = Nt / Nt_prev;
+      for (int a = 0; a <= E.natom; ++a) N[a] *= sc;
+      if (newton(Nt, kWarmPasses) == 1) {
+        Nt_prev = Nt;
+        return;
+      }
+    }
+    cold_start(Nt);
+    if (newton(Nt, 50) != 1) capped = 1;
+    have = 1;
+    Nt_prev = Nt;
+  }
+
+  // the reference's starting values: ionisation-only quadratic and the halving loop
+  __device__ void cold_start(double Nt) {
+    const int na = E.natom;
     double F1 = 0.0, S1 = 0.0;
     sweep<false>(1.0);
     for (int a = 0; a < na; ++a) { F1 += E.abund[a] * Ea[a + 1]; S1 += E.abund[a]; }
@@ -298,6 +329,12 @@ struct Chem {
       N[0] = 0.5 * (N[0] + esum);
       if (++pass >= kPolishCap) { capped = 1; break; }
     } while ((1E-2 * (N[0] + esum)) < fabs(N[0] - esum));
+  }
+
+  // Newton passes (atmos_chm.cc:176-305) from N, at most maxpass: 1 converged, 0 the pass cap was
+  // reached (the reference stops there: iter > 100 counting two per pass), -1 a non-finite state
+  __device__ int newton(double Nt, int maxpass) {
+    const int na = E.natom, nm = E.nmol, n = na + 1;
     int iter = 0;
     bool conv;
     do {
@@ -388,15 +425,19 @@ struct Chem {
         for (int j = r + 1; j < n; ++j) s -= A[r * n + j] * v[j];
         v[r] = s / A[r * n + r];
       }
+      bool finite = true;
       for (int a = 0; a <= na; ++a) {
         N[a] -= v[a];
         if (N[a] < 1E-2) N[a] = 1E-2;
+        finite &= isfinite(N[a]);
       }
+      if (!finite) return -1;
       iter += 2;  // the reference counts two per pass (atmos_chm.cc:294, 300)
-      if (iter > 100) { capped = 1; break; }
+      if (iter > 2 * maxpass) return 0;
       conv = true;
       for (int i = 0; i <= na; ++i) if (fabs(d[i] / N[i]) > 1E-4) conv = false;
     } while (!conv);
+    return 1;
   }
 
   // stage total of stage s (with a kept fraction) after solve
@@ -538,9 +579,10 @@ __device__ double continuum(const EosDev &E, const Chem &c, const double *lev, d
 
 // chemistry + populations + kappa (which as in continuum); returns kappa, fills lev and nH0.  The
 // T-only tables are rebuilt only when T changes (the hydrostatic iterations of one depth share T).
-__device__ double chem_point(const EosDev &E, Chem &c, double T, double Nt, double *lev, double &nH0, int which) {
+__device__ double chem_point(const EosDev &E, Chem &c, double T, double Nt, double *lev, double &nH0, int which,
+                             bool warm = false) {
   if (T != c.T) c.set_T(T);
-  c.solve(Nt);
+  c.solve(Nt, warm);
   for (int l = 0; l < E.nlev; ++l) lev[l] = c.level_pop(l, c.stage_U(E.lst[l], c.N[0]));
   nH0 = c.stage_total(E.s0[0], 0);
   return continuum(E, c, lev, nH0, which);
@@ -559,6 +601,7 @@ struct EosArgs {
   double *Nt_out;         // [npix][nd] or null
   double *F;              // [npix][nvar][nd][nf]: thermal fields of every variant (FP64)
   int *status;            // [npix]
+  int warm;               // continued chemistry starts in the hydrostatic march (Chem::solve)
 };
 
 __device__ __forceinline__ void variant_pert(const EosDev &E, const EosArgs &A, int v, int &pidx, double &pert) {
@@ -588,8 +631,9 @@ __global__ void __launch_bounds__(kHeThreads) k_eos_he(EosArgs A) {
   double T0 = interp_kind(E, nv, 1, 0, true);
   Tc[0] = T0;
   double Nt = 0.3 / cK / T0, op_prev = 0.0, rho_prev = 0.0;
+  const bool warm = A.warm != 0;
   for (int iter = 0; iter < 20; ++iter) {
-    const double op = chem_point(E, c, T0, Nt, lev, nH0, 0);
+    const double op = chem_point(E, c, T0, Nt, lev, nH0, 0, warm);
     st |= c.capped;
     const double rho = c.N[1] * 1.4 * 1.67E-24;
     const double dN = (pow(10.0, logtau(E, 0)) * rho * E.grav / op) / cK / T0 - Nt;
@@ -610,7 +654,7 @@ __global__ void __launch_bounds__(kHeThreads) k_eos_he(EosArgs A) {
     double N = (Nprev * cK * Tprev + delta_p) / cK / Tx;
     double op = 0.0, rho = 0.0;
     for (int iter = 0; iter < 20; ++iter) {
-      op = chem_point(E, c, Tx, N, lev, nH0, 0);
+      op = chem_point(E, c, Tx, N, lev, nH0, 0, warm);
       st |= c.capped;
       rho = c.N[1] * 1.4 * 1.67E-24;
       const double kappa_mean = sqrt(op * op_prev / rho / rho_prev);
@@ -699,6 +743,8 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_var(EosArgs A) {
   int st = 0;
   double f[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES];
   const size_t cv = ((size_t)p * A.nvar + v) * A.nd + x;
+  // the reference's start, whatever the march used: the record fields take the stage fractions of
+  // the last Newton sweep before its final update, so they follow the solve's path to ~1e-4
   thermal_fields(E, c, A.T[cv], A.Nt[cv], f, st);
   double *o = A.F + cv * A.nf;
   for (int k = 0; k < A.nf; ++k) o[k] = (k == 1 || (k >= 3 && k <= 6)) ? 0.0 : f[k];
@@ -846,6 +892,10 @@ struct EosCtx {
   double *d_T = nullptr, *d_Nt = nullptr, *d_nodes = nullptr, *d_step = nullptr, *d_Ntout = nullptr;
   double *d_F = nullptr;
   int *d_active = nullptr, *d_status = nullptr;
+  int chem_start = SNAPI_CHEM_START_CONTINUE;
+  // snapi_adjoint_nodes with host arrays: a chunk's node vectors and build status (max_batch pixels)
+  double *d_nn = nullptr;
+  int *d_nst = nullptr;
   float *d_rec = nullptr, *d_tan = nullptr;
   // return_as_array rows of snapi_build_atmos (cap_atm pixels) and the caller's heights
   double *d_atm = nullptr, *d_x3 = nullptr;
@@ -892,6 +942,8 @@ void eos_free(snapi_ctx *ctx) {
   EosCtx *e = static_cast<EosCtx *>(ctx->eos);
   if (!e) return;
   eos_free_bufs(e);
+  cudaFree(e->d_nn);
+  cudaFree(e->d_nst);
   cudaFree(e->d_tab);
   delete e;
   ctx->eos = nullptr;
@@ -1144,11 +1196,23 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
   if (!e->d_tab) SNAPI_CK(cudaMalloc(&e->d_tab, sizeof(EosDev)));
   SNAPI_CK(cudaMemcpy(e->d_tab, &H, sizeof(EosDev), cudaMemcpyHostToDevice));
   e->npar = m->npar;
+  e->chem_start = SNAPI_CHEM_START_CONTINUE;
   e->ntherm = H.kcount[1];
   e->kind.assign(m->node_kind, m->node_kind + m->npar);
   e->ref_step.assign(m->npar, 0.0);
   static const double ref_step[7] = {0.0, 5.0, 20.0, 20.0, 0.01, 0.001, 0.001};  // const.h:27-32
   for (int q = 0; q < m->npar; ++q) e->ref_step[q] = ref_step[m->node_kind[q]];
+  return SNAPI_OK;
+}
+
+int snapi_eos_chem_start(snapi_ctx *ctx, int mode) {
+  using namespace snapi;
+  if (!ctx) return SNAPI_EINVAL;
+  EosCtx *e = static_cast<EosCtx *>(ctx->eos);
+  if (!e) return set_err(ctx, SNAPI_EINVAL, "snapi_eos_chem_start: no node model (snapi_eos_set)");
+  if (mode != SNAPI_CHEM_START_CONTINUE && mode != SNAPI_CHEM_START_COLD)
+    return set_err(ctx, SNAPI_EINVAL, "snapi_eos_chem_start: unknown mode %d", mode);
+  e->chem_start = mode;
   return SNAPI_OK;
 }
 
@@ -1217,6 +1281,7 @@ static int build_impl(snapi_ctx *ctx, int npix, const double *nodes, const int *
     A.Nt = e->d_Nt;
     A.F = e->d_F;
     A.status = e->d_status;
+    A.warm = e->chem_start == SNAPI_CHEM_START_CONTINUE;
     if (host) {
       SNAPI_CK(cudaMemcpyAsync(e->d_nodes, nodes + (size_t)p0 * npar, sizeof(double) * nb * npar,
                                cudaMemcpyHostToDevice, ctx->stream));
@@ -1365,6 +1430,80 @@ int snapi_records_from_columns(snapi_ctx *ctx, int npix, const double *columns, 
     SNAPI_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     ctx->last_ms += ms;
   }
+  return SNAPI_OK;
+}
+
+int snapi_adjoint_nodes(snapi_ctx *ctx, int npix, const double *nodes, const float *obs, const double *w_stokes,
+                        const float *mask, float *stokes, double *chi2, double *grad, int *pix_status, int mem) {
+  using namespace snapi;
+  if (!ctx) return SNAPI_EINVAL;
+  EosCtx *e = static_cast<EosCtx *>(ctx->eos);
+  if (!e) return set_err(ctx, SNAPI_EINVAL, "snapi_adjoint_nodes: no node model (snapi_eos_set)");
+  if (npix < 0 || (npix > 0 && (!nodes || !obs || !chi2 || !grad)) ||
+      (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
+    return set_err(ctx, SNAPI_EINVAL, "snapi_adjoint_nodes: invalid arguments");
+  if (npix == 0) return SNAPI_OK;
+  SNAPI_CK(cudaSetDevice(ctx->device));
+  const int npar = e->npar, nl = ctx->nl;
+  int st = ensure_npar(ctx, npar);
+  if (st) return st;
+  const bool host = mem == SNAPI_MEM_HOST;
+  if (host && !e->d_nn) {
+    SNAPI_CK(cudaMalloc(&e->d_nn, sizeof(double) * (size_t)ctx->max_batch * npar));
+    SNAPI_CK(cudaMalloc(&e->d_nst, sizeof(int) * (size_t)ctx->max_batch));
+  }
+  double total_ms = 0.0, phase[2] = {0.0, 0.0};
+  int launches = 0;
+  for (int p0 = 0; p0 < npix; p0 += ctx->max_batch) {
+    const int nb = std::min(ctx->max_batch, npix - p0);
+    const double *dn = nodes + (size_t)p0 * npar;
+    const float *dobs = obs + (size_t)p0 * nl * 4;
+    const float *dmask = mask ? mask + (size_t)p0 * nl : nullptr;
+    float *dst = stokes ? stokes + (size_t)p0 * nl * 4 : nullptr;
+    double *dchi = chi2 + p0, *dgrad = grad + (size_t)p0 * npar;
+    int *dps = pix_status ? pix_status + p0 : nullptr;
+    if (host) {  // stage the chunk's inputs; results land in the context's buffers
+      SNAPI_CK(cudaMemcpyAsync(e->d_nn, dn, sizeof(double) * nb * npar, cudaMemcpyHostToDevice, ctx->stream));
+      SNAPI_CK(cudaMemcpyAsync(ctx->d_obs, dobs, sizeof(float) * nb * nl * 4, cudaMemcpyHostToDevice, ctx->stream));
+      if (mask)
+        SNAPI_CK(cudaMemcpyAsync(ctx->d_mask, dmask, sizeof(float) * nb * nl, cudaMemcpyHostToDevice, ctx->stream));
+      dn = e->d_nn;
+      dobs = ctx->d_obs;
+      dmask = mask ? ctx->d_mask : nullptr;
+      dst = stokes ? ctx->d_stokes : nullptr;
+      dchi = ctx->d_chi2;
+      dgrad = ctx->d_grad;
+      dps = pix_status ? e->d_nst : nullptr;
+    }
+    // records and node tangents (the reference's steps) of the chunk, kept on the device
+    st = build_impl(ctx, nb, dn, nullptr, ctx->d_rec, nullptr, ctx->d_tan, nullptr, dps, SNAPI_MEM_DEVICE, nullptr,
+                    nullptr);
+    if (st) return st;
+    total_ms += ctx->last_ms;
+    phase[0] += ctx->last_ms;
+    launches += ctx->last_launches;
+    st = snapi_adjoint(ctx, nb, ctx->d_rec, dobs, w_stokes, dmask, npar, ctx->d_tan, dst, dchi, dgrad, nullptr,
+                       SNAPI_MEM_DEVICE);
+    total_ms += ctx->last_ms;
+    phase[1] += ctx->last_ms;
+    launches += ctx->last_launches;
+    if (st) return st;
+    if (host) {
+      if (stokes)
+        SNAPI_CK(cudaMemcpyAsync(stokes + (size_t)p0 * nl * 4, ctx->d_stokes, sizeof(float) * nb * nl * 4,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+      SNAPI_CK(cudaMemcpyAsync(chi2 + p0, ctx->d_chi2, sizeof(double) * nb, cudaMemcpyDeviceToHost, ctx->stream));
+      SNAPI_CK(cudaMemcpyAsync(grad + (size_t)p0 * npar, ctx->d_grad, sizeof(double) * nb * npar,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+      if (pix_status)
+        SNAPI_CK(cudaMemcpyAsync(pix_status + p0, e->d_nst, sizeof(int) * nb, cudaMemcpyDeviceToHost, ctx->stream));
+      SNAPI_CK(cudaStreamSynchronize(ctx->stream));
+    }
+  }
+  ctx->last_ms = total_ms;
+  ctx->phase_ms[0] = phase[0];
+  ctx->phase_ms[1] = phase[1];
+  ctx->last_launches = launches;
   return SNAPI_OK;
 }
 

@@ -321,6 +321,7 @@ struct snapi_ctx {
   float4 *d_scratch = nullptr;
   int cap_npar = 0;
   double last_ms = 0.0;
+  double phase_ms[2] = {0.0, 0.0};  // snapi_adjoint_nodes: node build, adjoint (device time)
   int last_launches = 0;
   std::string err;
   // LM work buffers (allocated on first use)

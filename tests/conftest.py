@@ -51,6 +51,16 @@ def config5():
 
 
 @pytest.fixture(scope="session")
+def eos3():
+    return load_fixture("eos_c3")
+
+
+@pytest.fixture(scope="session")
+def eos1():
+    return load_fixture("eos_c1")
+
+
+@pytest.fixture(scope="session")
 def oracle_lib():
     from snapi_b200 import build as b
     b.build_oracle() if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libsnapi_oracle.so")) else None

@@ -14,16 +14,6 @@ pytestmark_gpu = pytest.mark.skipif(not gpu_available(), reason="needs a CUDA GP
 THERMAL = [0, 2, 7, 8, 9, 10, 11]  # + the line fields
 
 
-@pytest.fixture(scope="module")
-def eos3():
-    return load_fixture("eos_c3")
-
-
-@pytest.fixture(scope="module")
-def eos1():
-    return load_fixture("eos_c1")
-
-
 def _tables(d):
     import eos_oracle as eo
     return eo.EosTables(d)
@@ -125,43 +115,86 @@ def test_oracle_records_and_tangents(oracle_lib, eos3, config3):
             assert err.max() < 1e-5, (q, err)
 
 
+def test_oracle_continued_start_vs_reference(oracle_lib, eos3, config3):
+    """The continued chemistry start in the hydrostatic march (the CUDA path's default), restated in
+    the oracle: particle densities, records and node tangents against the reference's (which
+    starts every solve cold) within the size of the reference's own last Newton update."""
+    import eos_oracle as eo
+    t = _tables(eos3)
+    lam0, mass = _line_const(config3)
+    old = eo.set_chem_start(eo.CHEM_START_CONTINUE)
+    try:
+        for p in range(config3["nodes"].shape[0]):
+            T, Nt, rec, st = eo.build(t, lam0, mass, config3["nodes"][p])
+            assert st == 0
+            np.testing.assert_allclose(Nt, eos3["he_Nt"][p], rtol=TOL["continue"]["nt"])
+            np.testing.assert_allclose(rec, config3["record"][p], rtol=TOL["continue"]["rec"], atol=0)
+            tan, _ = eo.tangents(t, lam0, mass, config3["nodes"][p])
+            ref = config3["record"][p].astype(np.float64)
+            rt = config3["tangent"][p].astype(np.float64)
+            for q in range(rt.shape[0]):
+                floor = np.maximum(np.abs(rt[q]).max(axis=0), 1e-6 * np.abs(ref).max(axis=0))
+                assert (np.abs(tan[q] - rt[q]).max(axis=0) / floor).max() < TOL["continue"]["tan"]
+    finally:
+        eo.set_chem_start(old)
+
+
 # ---- GPU ---------------------------------------------------------------------------------------------
 
-def _gpu_ctx(fx, eos, **kw):
+def _gpu_ctx(fx, eos, start="cold", **kw):
     import snapi_b200 as sb
     from snapi_b200.eos_tables import EosTables
     ctx = sb.Context.from_fixture(fx, **kw)
     ctx.eos_set(EosTables(eos))
+    ctx.eos_chem_start(sb.api.CHEM_START_COLD if start == "cold" else sb.api.CHEM_START_CONTINUE)
     return ctx
+
+
+# Tolerances per chemistry start.  The cold start is the reference's (its iterates to rounding).
+# The continued start (hydrostatic march only) stops on the same Newton rule from a nearby point,
+# so the march differs from the reference by up to the size of the reference's last Newton
+# update: Nt and n_e ~3e-8 relative, records ~4e-8 (below their float32 rounding), node tangents
+# ~4e-5 of each field's scale (the reference's 5 K differences carry that much noise from its
+# 1e-4 stop).
+TOL = {"cold": {"nt": 1e-10, "rec": 3e-7, "tan": 2e-5, "ne": 1e-9},
+       "continue": {"nt": 1e-7, "rec": 3e-7, "tan": 1e-4, "ne": 1e-7}}
 
 
 @pytest.mark.gpu
 @pytestmark_gpu
-def test_gpu_records_vs_oracle_and_reference(oracle_lib, eos3, config3):
+@pytest.mark.parametrize("start", ["cold", "continue"])
+def test_gpu_records_vs_oracle_and_reference(oracle_lib, eos3, config3, start):
     """Records of the 8 config-3 node vectors: FP32 rounding of the FP64 device result against
-    the oracle, and against the reference's own records."""
+    the oracle (the same start), and against the reference's own records."""
     import eos_oracle as eo
-    ctx = _gpu_ctx(config3, eos3)
+    tol = TOL[start]
+    ctx = _gpu_ctx(config3, eos3, start)
     nodes = config3["nodes"]
     rec, tan, nt, status = ctx.build_records(nodes, tangents=False, want_nt=True)
     assert np.all(status == 0)
     assert ctx.last_launches == 3
     t = _tables(eos3)
     lam0, mass = _line_const(config3)
-    for p in range(nodes.shape[0]):
-        T, Nt, ro, st = eo.build(t, lam0, mass, nodes[p])
-        np.testing.assert_allclose(nt[p], Nt, rtol=1e-10)
-        np.testing.assert_allclose(rec[p], ro, rtol=3e-7, atol=0)
-        np.testing.assert_allclose(rec[p], config3["record"][p], rtol=3e-7, atol=0)
+    old = eo.set_chem_start(eo.CHEM_START_COLD if start == "cold" else eo.CHEM_START_CONTINUE)
+    try:
+        for p in range(nodes.shape[0]):
+            T, Nt, ro, st = eo.build(t, lam0, mass, nodes[p])
+            np.testing.assert_allclose(nt[p], Nt, rtol=1e-10)           # the oracle on the same path
+            np.testing.assert_allclose(rec[p], ro, rtol=3e-7, atol=0)
+            np.testing.assert_allclose(nt[p], eos3["he_Nt"][p], rtol=tol["nt"])  # the reference
+            np.testing.assert_allclose(rec[p], config3["record"][p], rtol=tol["rec"], atol=0)
+    finally:
+        eo.set_chem_start(old)
     ctx.close()
 
 
 @pytest.mark.gpu
 @pytestmark_gpu
-def test_gpu_tangents_vs_reference(oracle_lib, eos3, config3):
+@pytest.mark.parametrize("start", ["cold", "continue"])
+def test_gpu_tangents_vs_reference(oracle_lib, eos3, config3, start):
     """Node tangents (central differences with the reference's steps: two full builds per
     temperature node, re-interpolation for the others) against the reference's."""
-    ctx = _gpu_ctx(config3, eos3)
+    ctx = _gpu_ctx(config3, eos3, start)
     nodes = config3["nodes"]
     rec, tan, _, status = ctx.build_records(nodes, tangents=True)
     assert np.all(status == 0)
@@ -172,35 +205,37 @@ def test_gpu_tangents_vs_reference(oracle_lib, eos3, config3):
             scale = np.abs(rt[q]).max(axis=0)
             floor = np.maximum(scale, 1e-6 * np.abs(ref).max(axis=0))
             err = np.abs(tan[p, q] - rt[q]).max(axis=0) / floor
-            assert err.max() < 2e-5, (p, q, err)
+            assert err.max() < TOL[start]["tan"], (p, q, err)
     ctx.close()
 
 
 @pytest.mark.gpu
 @pytestmark_gpu
-def test_gpu_dense_temperature_nodes(oracle_lib, eos1, config1, config2):
+@pytest.mark.parametrize("start", ["cold", "continue"])
+def test_gpu_dense_temperature_nodes(oracle_lib, eos1, config1, config2, start):
     """The config-1/2 model (80 temperature nodes, one per depth, + 5): records of 17 columns
     against the reference's, and the hydrostatic Nt against its build_from_nodes."""
-    ctx = _gpu_ctx(config1, eos1)
+    ctx = _gpu_ctx(config1, eos1, start)
     nodes = eos1["nodes"]
     rec, _, nt, status = ctx.build_records(nodes, tangents=False, want_nt=True)
     assert np.all(status == 0)
-    np.testing.assert_allclose(nt, eos1["he_Nt"], rtol=1e-10)
+    np.testing.assert_allclose(nt, eos1["he_Nt"], rtol=TOL[start]["nt"])
     ref = np.concatenate([config1["record"], config2["record"]]).astype(np.float64)
-    np.testing.assert_allclose(rec, ref, rtol=3e-7, atol=0)
+    np.testing.assert_allclose(rec, ref, rtol=TOL[start]["rec"], atol=0)
     ctx.close()
 
 
 @pytest.mark.gpu
 @pytestmark_gpu
 @pytest.mark.parametrize("name", ["eos_c3", "eos_c1"])
-def test_gpu_atmosphere_rows_vs_reference(oracle_lib, name, config3, config1):
+@pytest.mark.parametrize("start", ["cold", "continue"])
+def test_gpu_atmosphere_rows_vs_reference(oracle_lib, name, config3, config1, start):
     """snapi_build_atmos against the reference's return_as_array after build_from_nodes and
     compute_op_referent (the columns the master writes to inverted_atmos.f0), for the config-3
     node vectors and the 80-temperature-node config-1/2 ones, heights taken from the reference."""
     d = load_fixture(name)
     fx = config3 if name == "eos_c3" else config1
-    ctx = _gpu_ctx(fx, d)
+    ctx = _gpu_ctx(fx, d, start)
     ref = d["atm_arr"]
     atm, status = ctx.build_atmos(d["nodes"], x3=ref[0, 1])
     ctx.close()
@@ -210,8 +245,8 @@ def test_gpu_atmosphere_rows_vs_reference(oracle_lib, name, config3, config1):
     np.testing.assert_allclose(atm[:, 0], ref[:, 0], rtol=0, atol=1e-14)          # log10 tau
     np.testing.assert_array_equal(atm[:, 1], ref[:, 1])                           # heights
     np.testing.assert_allclose(atm[:, 2], ref[:, 2], rtol=1e-13)                   # T
-    np.testing.assert_allclose(atm[:, 3], ref[:, 3], rtol=1e-10)                   # Nt k T
-    np.testing.assert_allclose(atm[:, [4, 6]], ref[:, [4, 6]], rtol=1e-9)          # n_e k T, kappa
+    np.testing.assert_allclose(atm[:, 3], ref[:, 3], rtol=TOL[start]["nt"])        # Nt k T
+    np.testing.assert_allclose(atm[:, [4, 6]], ref[:, [4, 6]], rtol=TOL[start]["ne"])  # n_e k T, kappa
     np.testing.assert_allclose(atm[:, 7:10], ref[:, 7:10], rtol=1e-13, atol=1e-9)  # |B|, v_turb, v_z
     np.testing.assert_allclose(atm[:, 10:], ref[:, 10:], rtol=0, atol=1e-12)       # angles
 
@@ -231,6 +266,31 @@ def test_gpu_active_rows_untouched_and_batches(oracle_lib, eos3, config3):
         np.testing.assert_array_equal(rec[p], rec[p % 8] if active[p % 8] else rec[p])
     np.testing.assert_allclose(rec[8], config3["record"][0], rtol=3e-7)
     ctx.close()
+
+
+@pytest.mark.gpu
+@pytestmark_gpu
+def test_gpu_continued_start_tangents_vs_oracle(oracle_lib, eos3, config3):
+    """The device's continued start against the oracle's restatement of it: the same path, so the
+    cold start's tight tangent tolerance holds."""
+    import eos_oracle as eo
+    ctx = _gpu_ctx(config3, eos3, "continue")
+    nodes = config3["nodes"]
+    rec, tan, nt, status = ctx.build_records(nodes, tangents=True, want_nt=True)
+    ctx.close()
+    assert np.all(status == 0)
+    t = _tables(eos3)
+    lam0, mass = _line_const(config3)
+    old = eo.set_chem_start(eo.CHEM_START_CONTINUE)
+    try:
+        for p in range(nodes.shape[0]):
+            _, _, ro, _ = eo.build(t, lam0, mass, nodes[p])
+            to, _ = eo.tangents(t, lam0, mass, nodes[p])
+            for q in range(to.shape[0]):
+                floor = np.maximum(np.abs(to[q]).max(axis=0), 1e-6 * np.abs(ro).max(axis=0))
+                assert (np.abs(tan[p, q] - to[q]).max(axis=0) / floor).max() < TOL["cold"]["tan"]
+    finally:
+        eo.set_chem_start(old)
 
 
 def _variant_tables(eos3):
@@ -272,6 +332,7 @@ def test_gpu_irwin_and_constant_equilibrium_vs_oracle(oracle_lib, eos3, config3)
     t = EosTables(d)
     ctx = sb.Context.from_fixture(config3)
     ctx.eos_set(EosTables(d))
+    ctx.eos_chem_start(sb.api.CHEM_START_COLD)  # the table variants against the oracle's path
     nodes = config3["nodes"][:4]
     rec, tan, _, status = ctx.build_records(nodes, tangents=True)
     assert np.all(status == 0)
@@ -299,6 +360,7 @@ def test_gpu_model_without_field_nodes_vs_oracle(oracle_lib, eos3, config3):
     t = EosTables(d)
     ctx = sb.Context.from_fixture(config3)
     ctx.eos_set(EosTables(d))
+    ctx.eos_chem_start(sb.api.CHEM_START_COLD)
     nodes = np.ascontiguousarray(config3["nodes"][:3][:, keep])
     rec, tan, _, status = ctx.build_records(nodes, tangents=True)
     assert np.all(status == 0)
