@@ -59,7 +59,7 @@ def test_synth_matches_emulator(sb, emu, oracle_lib, config2):
 
 def test_adjoint_gradient(sb, oracle_lib, config3):
     fx = config3
-    n = 4
+    n = fx["record"].shape[0]  # every pixel of the fixture
     ctx = _ctx(sb, fx)
     out = ctx.adjoint(fx["record"][:n], fx["target"][:n], fx["tangent"][:n], want_rec_grad=True)
     ctx.close()
@@ -89,6 +89,24 @@ def test_adjoint_coherent_residual(sb, oracle_lib, config3):
     for p in range(2):
         _, g_ref = oracle_grad(oracle_lib, fx, p, obs[p])
         assert scaled_rel_err(out["grad"][p], g_ref, fx["node_kind"]) < 1e-4
+
+
+def test_adjoint_coherent_residual_pool(sb, oracle_lib):
+    """The 32 reference-built columns of the benchmark pool (records and node tangents from the
+    reference's build_from_nodes): adjoint gradient against FP64 central differences of the
+    oracle, coherent residual (target = 0.97 x the reference's Stokes), every column."""
+    from conftest import load_fixture
+    fx = load_fixture("bench_pool")
+    obs = (fx["stokes"] * 0.97).astype(np.float32)
+    ctx = _ctx(sb, fx)
+    out = ctx.adjoint(fx["record"], obs, fx["tangent"])
+    ctx.close()
+    worst = 0.0
+    for p in range(fx["record"].shape[0]):
+        _, g_ref = oracle_grad(oracle_lib, fx, p, obs[p].astype(np.float64))
+        worst = max(worst, scaled_rel_err(out["grad"][p], g_ref, fx["node_kind"]))
+    print("pool: worst scaled gradient error %.2e" % worst)
+    assert worst < 1e-4
 
 
 def test_fd_gradient_agrees_with_adjoint(sb, config3):
