@@ -385,20 +385,23 @@ def bench_build(sb, pool, device, ncol=4096):
     ctx.eos_set(_eos_tables())
     ctx.build_records(nodes, tangents=True)  # warm-up (allocates the work buffers)
     out = {}
-    for tang in (False, True):
-        t0 = time.perf_counter()
-        _, _, _, status = ctx.build_records(nodes, tangents=tang)
-        wall = time.perf_counter() - t0
-        key = "with_tangents" if tang else "records_only"
-        out[key] = {"device_ms": ctx.last_kernel_ms, "wall_ms": wall * 1e3,
-                    "columns_per_s": ncol / (ctx.last_kernel_ms / 1e3), "flagged": int((status != 0).sum())}
+    for start, tag in ((sb.api.CHEM_START_CONTINUE, ""), (sb.api.CHEM_START_COLD, "_cold_start")):
+        ctx.eos_chem_start(start)
+        for tang in (False, True):
+            t0 = time.perf_counter()
+            _, _, _, status = ctx.build_records(nodes, tangents=tang)
+            wall = time.perf_counter() - t0
+            key = ("with_tangents" if tang else "records_only") + tag
+            out[key] = {"device_ms": ctx.last_kernel_ms, "wall_ms": wall * 1e3,
+                        "columns_per_s": ncol / (ctx.last_kernel_ms / 1e3), "flagged": int((status != 0).sum())}
     ctx.close()
     ref_build = float(pool["ref_seconds_per_pixel"][0])
     out["columns"] = ncol
     out["reference_build_s_per_column_one_core"] = ref_build
     out["reference_columns_per_s_one_core_with_tangents"] = 1.0 / (ref_build * 9)
     out["note"] = ("flagged: columns where a hydrostatic step reached the reference's own 20-pass cap "
-                   "(status 2, the reference continues the same way)")
+                   "(status 2, the reference continues the same way); *_cold_start: every chemistry solve "
+                   "started as the reference starts it (SNAPI_CHEM_START_COLD)")
     return out
 
 
