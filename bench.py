@@ -1,18 +1,21 @@
 """Benchmark: pixels/s of Stokes synthesis + chi2 gradient w.r.t. 10 nodes on one B200.
 
-Workload (the responses-and-adjoint configuration): 64 x 64 pixels, 80 depths (log tau500 -6..1), 201 wavelengths
-(Fe I 6301.5 / 6302.5, 12 mA), mu = 1, ten-node model (T x4, v_turb, v_los x2, B, inclination,
-azimuth).  One step = one call over all pixels: forward synthesis, chi2 against a noisy target
-and the adjoint (reverse) sweep giving d chi2 / d node for every pixel.
+Workload (the responses-and-adjoint configuration): 64 x 64 pixels, 80 depths (log tau500 -6..1),
+201 wavelengths (Fe I 6301.5 / 6302.5, 12 mA), mu = 1, ten-node model (T x4, v_turb, v_los x2, B,
+inclination, azimuth).  One step = one snapi_adjoint_nodes call over all pixels, from node vectors
+to outputs: the node -> record build on the device (node interpolation, hydrostatic equilibrium with
+the chemistry at every step, the record set-up; the node tangents by the reference's central
+differences: 9 builds per pixel), then forward synthesis, chi2 against a noisy target and the
+adjoint (reverse) sweep giving d chi2 / d node -- the work of the reference's build_from_nodes +
+obs_stokes_responses_to_nodes, which its reference arm times.
 
-Inputs: the thermal structure of each pixel is one of 32 columns built by the reference's own
-hydrostatic-equilibrium + chemistry code (tests/golden/bench_pool.npz, seed 303, with the node
-tangents of the reference's build_from_nodes); v_turb, v_los, B, inclination and azimuth are
-drawn per pixel (seed 3) -- they enter the columns linearly through the node interpolation.
-Target = synthesised truth + N(0, 1e-3 Ic); the evaluated model = truth with fixed node offsets.
-The adjoint takes the node tangents packed (per node only the record fields it moves: 100 of 270
-columns).  Inputs (0.18 GB) and the adjoint's state (8 GB) per step exceed the 126 MB L2, so no
-flush is needed between steps.
+Inputs: seeded config-3 node vectors (seed 3: the reference arm's pixels are the first ones of the
+same generator); target = device synthesis of the truth + N(0, 1e-3 Ic); evaluated model = truth
++ fixed node offsets.  A step's working set (the adjoint's state, 8 GB, and the build scratch)
+exceeds the 126 MB L2, so no flush is needed between steps.  Secondary keys: the adjoint alone on
+device-resident records and packed node tangents (the record boundary), the plain FD gradient at
+that boundary (2 npar + 1 solves) and from node vectors (2 npar + 1 builds + syntheses), the
+measured FP32 / FP64 peaks and the rooflines of both phases.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl snapi|reference]
 
@@ -40,10 +43,15 @@ METRIC = "pixels/s Stokes synth+grad on 1 B200, adjoint vs plain FD, at 1e-5 Ic"
 NPIX = 64 * 64
 FD_STEPS = np.array([5.0, 5.0, 5.0, 5.0, 2e3, 2e3, 2e3, 5.0, 5e-3, 5e-3])
 # ncu (--set full) of the four adjoint kernels on 2048 pixels of this workload, per pixel:
-# dram__bytes_read.sum + dram__bytes_write.sum, and executed FP32 flop (2 FFMA + FMUL + FADD)
+# dram__bytes_read.sum + dram__bytes_write.sum
 NCU_DRAM_BYTES_PER_PIXEL = 4.90e6
-NCU_FP32_FLOP_PER_PIXEL = 6.49e7
-FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FMA rate at the 1965 MHz max clock
+# Algorithmic work, frozen from `python oracle/opcount/count_flops.py --pixels 8` (op-count builds of
+# the kernels' CPU emulator and of the FP64 node -> record restatement; profiles/flops_per_cell.md):
+# flop per pixel of the adjoint call (forward + reverse, 3915 per wavelength x depth cell) and FP64
+# flop per column of the node build with tangents (9 builds, continued chemistry start).
+FLOPS = {"adjoint_flops_per_pixel": 6.296e7, "build_flops_per_column_with_tangents": 1.191e8}
+# the evaluated model = truth + these offsets (T x4, v_turb, v_los x2, B, inclination, azimuth)
+MODEL_OFFSET = np.array([0.0, 0.0, 0.0, 0.0, 0.3e5, 0.3e5, -0.3e5, 200.0, 0.1, 0.1])
 
 
 def make_workload(pool, npix=NPIX, seed=3, return_nodes=False):
@@ -167,6 +175,17 @@ def barrier(world):
         dist.barrier()
 
 
+def node_workload(npix, seed):
+    """The headline workload's node vectors: seeded config-3 truth nodes (T x4 around 4600 / 4900 /
+    5500 / 7400 K with N(0, 150 K), v_turb U(0.5, 2) km/s, v_los N(0, 1 km/s) x2, B log-uniform
+    100-2500 G, inclination U(20, 160) deg, azimuth U(10, 170) deg; the reference arm's pixels are
+    the first ones of the same generator) and the evaluated model = truth + fixed offsets."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import config3_nodes
+    truth = config3_nodes(npix, seed=seed)
+    return truth, truth + MODEL_OFFSET
+
+
 def run_snapi(args):
     import torch
 
@@ -180,22 +199,19 @@ def run_snapi(args):
     b.build_cuda()
     pool = dict(np.load(POOL))
     NPIX = args.pixels
-    truth, model, tan = make_workload(pool, NPIX, seed=3 + 1000 * rank)
     ic = float(pool["stokes"][:, :, 0].max())
-    npar = tan.shape[1]
     nl = pool["lambda_air"].shape[0]
     ctx = sb.Context.from_fixture(pool, stokes_scale=ic, max_batch=NPIX, device=local)
-    # target: synthesised truth + noise (set-up, not timed)
-    obs = ctx.synth(truth)
+    ctx.eos_set(_eos_tables())
+    npar = ctx._eos_npar
+    truth, model = node_workload(NPIX, seed=3 + 1000 * rank)
+    # target: the device synthesis of the truth + N(0, 1e-3 Ic) (set-up, not timed)
+    rec_t, _, _, _ = ctx.build_records(truth, tangents=False)
+    obs = ctx.synth(rec_t)
     obs += np.random.default_rng(77 + rank).normal(0.0, 1e-3 * ic, obs.shape).astype(np.float32)
-    # device-resident inputs
-    d_rec = torch.from_numpy(model).to(dev)
+    del rec_t
+    d_nodes = torch.from_numpy(np.ascontiguousarray(model)).to(dev)
     d_obs = torch.from_numpy(obs).to(dev)
-    d_tan = torch.from_numpy(tan).to(dev)  # dense: the FD baseline perturbs records along it
-    # the adjoint takes the node tangents packed: per node only the record fields it moves
-    fmask = sb.tangent_field_mask(tan)
-    ptan = sb.pack_tangents(tan, fmask)
-    d_ptan = torch.from_numpy(ptan).to(dev)
     d_chi2 = torch.zeros(NPIX, dtype=torch.float64, device=dev)
     d_grad = torch.zeros(NPIX, npar, dtype=torch.float64, device=dev)
     d_st = torch.zeros(NPIX, nl, 4, dtype=torch.float32, device=dev)
@@ -203,8 +219,8 @@ def run_snapi(args):
     torch.cuda.synchronize()
 
     def step():
-        ctx.adjoint_packed_device(NPIX, d_rec.data_ptr(), d_obs.data_ptr(), fmask, d_ptan.data_ptr(), d_chi2.data_ptr(),
-                           d_grad.data_ptr(), stokes_ptr=d_st.data_ptr())
+        ctx.adjoint_nodes_device(NPIX, d_nodes.data_ptr(), d_obs.data_ptr(), d_chi2.data_ptr(), d_grad.data_ptr(),
+                                 stokes_ptr=d_st.data_ptr())
 
     for _ in range(args.warmup):
         step()
@@ -214,13 +230,13 @@ def run_snapi(args):
     clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    kern_ms = 0.0
+    phase = np.zeros(2)
     launches = 0
     torch.cuda.synchronize()
     ev0.record(stream)
     for _ in range(args.steps):
         step()
-        kern_ms += ctx.last_kernel_ms
+        phase += np.array(ctx.last_phase_ms)
         launches += ctx.last_launches
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -228,57 +244,106 @@ def run_snapi(args):
     clk = clocks.stop()
     barrier(world)
     value, ms_step = job_throughput(NPIX, total_ms / args.steps, world, dev)
+    build_ms, adj_ms = phase / args.steps
 
-    # plain FD gradient (2 npar + 1 forward solves) on the same inputs, for the adjoint-vs-FD ratio
-    def fd_step():
-        ctx.fd_grad_device(NPIX, d_rec.data_ptr(), d_obs.data_ptr(), npar, d_tan.data_ptr(), FD_STEPS,
-                           d_chi2.data_ptr(), d_grad.data_ptr())
-
-    fd_step()
-    torch.cuda.synchronize()
-    nfd = max(1, args.steps // 5)
-    ev0.record(stream)
-    for _ in range(nfd):
-        fd_step()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    fd_ms = reduce_max(ev0.elapsed_time(ev1) / nfd, world, dev)
-
-    # end to end through the host API: pinned host inputs, H2D + kernel + D2H every step
-    h_rec = np.frombuffer((ctypes_buffer(ctx, model.nbytes)), dtype=np.float32).reshape(model.shape)
-    h_rec[...] = model
-    h_obs = np.frombuffer((ctypes_buffer(ctx, obs.nbytes)), dtype=np.float32).reshape(obs.shape)
+    # end to end through the host API: page-locked node vectors and targets in, Stokes / chi2 /
+    # gradient out, every step (snapi_adjoint_nodes with host arrays)
+    h_nodes = np.frombuffer(ctypes_buffer(ctx, model.nbytes), dtype=np.float64).reshape(model.shape)
+    h_nodes[...] = model
+    h_obs = np.frombuffer(ctypes_buffer(ctx, obs.nbytes), dtype=np.float32).reshape(obs.shape)
     h_obs[...] = obs
-    h_tan = np.frombuffer((ctypes_buffer(ctx, ptan.nbytes)), dtype=np.float32).reshape(ptan.shape)
-    h_tan[...] = ptan
-    # results land in page-locked buffers too (the C ABI writes into caller-owned memory)
     h_out = {"stokes": np.frombuffer(ctypes_buffer(ctx, 4 * NPIX * nl * 4), dtype=np.float32).reshape(NPIX, nl, 4),
              "chi2": np.frombuffer(ctypes_buffer(ctx, 8 * NPIX), dtype=np.float64),
-             "grad": np.frombuffer(ctypes_buffer(ctx, 8 * NPIX * npar), dtype=np.float64).reshape(NPIX, npar)}
-    ctx.adjoint_packed(h_rec, h_obs, fmask, h_tan, out=h_out)
+             "grad": np.frombuffer(ctypes_buffer(ctx, 8 * NPIX * npar), dtype=np.float64).reshape(NPIX, npar),
+             "status": np.frombuffer(ctypes_buffer(ctx, 4 * NPIX), dtype=np.int32)}
+    ctx.adjoint_nodes(h_nodes, h_obs, out=h_out)
     torch.cuda.synchronize()
     barrier(world)
     ne = max(1, args.steps // 2)
     ev0.record(stream)
     for _ in range(ne):
-        out = ctx.adjoint_packed(h_rec, h_obs, fmask, h_tan, out=h_out)
+        out = ctx.adjoint_nodes(h_nodes, h_obs, out=h_out)
     ev1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = reduce_max(ev0.elapsed_time(ev1) / ne, world, dev)
-    h2d = model.nbytes + obs.nbytes + ptan.nbytes
-    d2h = out["stokes"].nbytes + out["chi2"].nbytes + out["grad"].nbytes
+    h2d = model.nbytes + obs.nbytes
+    d2h = out["stokes"].nbytes + out["chi2"].nbytes + out["grad"].nbytes + out["status"].nbytes
+    flagged = int((out["status"] != 0).sum())
+
+    # the record boundary (snapi_adjoint_packed on device-resident records and packed node tangents,
+    # built once from the same nodes): the adjoint alone, and the plain FD gradient it replaces
+    rec_m, tan_m, _, _ = ctx.build_records(model, tangents=True)
+    fmask = sb.tangent_field_mask(tan_m)
+    ptan = sb.pack_tangents(tan_m, fmask)
+    d_rec = torch.from_numpy(rec_m).to(dev)
+    d_tan = torch.from_numpy(tan_m).to(dev)
+    d_ptan = torch.from_numpy(ptan).to(dev)
+    del tan_m
+
+    def rec_step():
+        ctx.adjoint_packed_device(NPIX, d_rec.data_ptr(), d_obs.data_ptr(), fmask, d_ptan.data_ptr(),
+                                  d_chi2.data_ptr(), d_grad.data_ptr(), stokes_ptr=d_st.data_ptr())
+
+    def fd_step():
+        ctx.fd_grad_device(NPIX, d_rec.data_ptr(), d_obs.data_ptr(), npar, d_tan.data_ptr(), FD_STEPS,
+                           d_chi2.data_ptr(), d_grad.data_ptr())
+
+    def timed(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(n):
+            fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return reduce_max(ev0.elapsed_time(ev1) / n, world, dev)
+
+    rec_ms = timed(rec_step, args.steps)
+    fd_ms = timed(fd_step, max(1, args.steps // 5))
+
+    # plain FD from the node vectors: 2 npar + 1 builds (records only) and syntheses, chi2 each
+    d_nfd = torch.empty_like(d_nodes)
+    d_rfd = torch.empty_like(d_rec)
+
+    def fd_nodes_step():
+        g = []
+        for q in range(-1, npar):
+            for sgn in ((0.0,) if q < 0 else (0.5, -0.5)):
+                with torch.cuda.stream(stream):
+                    d_nfd.copy_(d_nodes)
+                    if q >= 0:
+                        d_nfd[:, q] += sgn * FD_STEPS[q]
+                ctx.build_records_device(NPIX, d_nfd.data_ptr(), d_rfd.data_ptr())
+                ctx.synth_device(NPIX, d_rfd.data_ptr(), d_st.data_ptr())
+                with torch.cuda.stream(stream):
+                    g.append(((d_obs - d_st) ** 2).sum(dim=(1, 2)))
+        return g
+
+    fdn_ms = timed(fd_nodes_step, 1)
+    del d_rec, d_tan, d_ptan, d_rfd
 
     line = None
     if rank == 0:
-        # one call = k_adjoint_sweep (>99 % of the device time) + k_adjoint_finish, timed together
-        kern_per_launch_ms = kern_ms / args.steps
-        # algorithmic bytes per pixel: record + tangents + target in, Stokes + grad + chi2 out
-        nd = model.shape[1]
-        nf = model.shape[2]
-        ntcol = ptan.shape[1]
-        bytes_pix = 4 * (nd * nf + ntcol * nd + nl * 4) + 4 * nl * 4 + 8 * (npar + 1)
-        achieved = bytes_pix * NPIX / (kern_per_launch_ms / 1e3) / 1e9
         peaks = load_peaks()
+        fp32 = sb.api.fma_peak(local, fp64=False)
+        fp64 = sb.api.fma_peak(local, fp64=True)
+        adj_tf = FLOPS["adjoint_flops_per_pixel"] * NPIX / (adj_ms / 1e3) / 1e12
+        bld_tf = FLOPS["build_flops_per_column_with_tangents"] * NPIX / (build_ms / 1e3) / 1e12
+        r_adj = {"bound": "fp32", "achieved": adj_tf, "peak": fp32, "unit": "TFLOP/s", "frac": adj_tf / fp32,
+                 "traffic": NCU_DRAM_BYTES_PER_PIXEL * NPIX,
+                 "kernel": "adjoint (k_adj_forward + k_adj_rt + k_adj_opacity + k_adjoint_finish)",
+                 "ms_per_launch": adj_ms, "peak_source": "measured on this GPU (snapi_fma_peak, FP32 FMA chains)",
+                 "flops": "algorithmic: %.4g flop per pixel from the op-count build of the kernels' CPU emulator "
+                          "(oracle/opcount; 3915 per wavelength x depth cell)" % FLOPS["adjoint_flops_per_pixel"],
+                 "traffic_note": "ncu DRAM bytes of the four adjoint kernels per pixel (2048-pixel capture) x pixels"}
+        r_bld = {"bound": "fp64", "achieved": bld_tf, "peak": fp64, "unit": "TFLOP/s", "frac": bld_tf / fp64,
+                 "traffic": None, "kernel": "node build (k_eos_he + k_eos_var + k_eos_rec)", "ms_per_launch": build_ms,
+                 "peak_source": "measured on this GPU (snapi_fma_peak, FP64 FMA chains)",
+                 "flops": "algorithmic upper bound: %.4g FP64 flop per column with tangents (9 builds) from the "
+                          "op-count build of the FP64 restatement, continued chemistry start (oracle/opcount)"
+                          % FLOPS["build_flops_per_column_with_tangents"],
+                 "bound_note": "a serial chemistry chain per column (latency-bound)"}
+        dominant = r_bld if build_ms >= adj_ms else r_adj
         line = {
             "metric": METRIC,
             "value": value,
@@ -290,32 +355,37 @@ def run_snapi(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32 (profiles, formal solver); f64 (optical depth, DELO weights, W4 core derivative)",
-            "data": "synthetic: reference-built columns (HE + chemistry) x seeded per-pixel field/velocity nodes",
-            "config": {"workload": workload_name(NPIX), "pixels_per_gpu": NPIX, "nd": int(nd), "nlambda": int(nl),
-                       "npar": int(npar), "node_tangents": "packed: %d of %d record-field columns per pixel"
-                                                            % (ntcol, npar * nf),
-                       "l2_flush": "inputs (0.18 GB) and adjoint state (8 GB) per step exceed the 126 MB L2",
+            "dtype": "f32 (profiles, formal solver, adjoint); f64 (chemistry, hydrostatic equilibrium, optical depth)",
+            "data": "synthetic: seeded config-3 node vectors (seed 3); target = device synthesis of the truth + "
+                    "N(0, 1e-3 Ic); evaluated at truth + fixed offsets",
+            "config": {"workload": workload_name(NPIX), "pixels_per_gpu": NPIX, "nd": int(ctx.nd),
+                       "nlambda": int(nl), "npar": int(npar),
+                       "step": "snapi_adjoint_nodes: node vectors -> records + node tangents (hydrostatic "
+                               "equilibrium + chemistry, 9 builds per pixel) -> synthesis + chi2 + adjoint "
+                               "d chi2 / d nodes, all on the device",
+                       "chem_start": "continued in the hydrostatic march (SNAPI_CHEM_START_CONTINUE)",
+                       "l2_flush": "a step's working set (adjoint state 8 GB, build scratch) exceeds the 126 MB L2",
                        "parallelism": "replicas (pixels independent)"},
             "gpu_launches": launches,
             "clocks": clk,
             "e2e": {"value": NPIX * world / (e2e_ms / 1e3), "unit": "pixels/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "fd_baseline": {"value": NPIX * world / (fd_ms / 1e3), "unit": "pixels/s", "ms_per_step": fd_ms,
-                            "solves_per_gradient": 2 * npar + 1, "adjoint_speedup": fd_ms / ms_step},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "traffic": NCU_DRAM_BYTES_PER_PIXEL * NPIX,
-                         "traffic_achieved_gbs": NCU_DRAM_BYTES_PER_PIXEL * NPIX / (kern_per_launch_ms / 1e3) / 1e9,
-                         "peak_source": peaks["source"],
-                         "kernel": "adjoint call (k_adj_forward + k_adj_rt + k_adj_opacity + k_adjoint_finish)",
-                         "note": "achieved = algorithmic bytes (inputs + outputs); traffic (ncu, scaled from "
-                                 "2048 pixels) includes the reverse-mode state written and read back on purpose; "
-                                 "the kernels are FP32-issue bound (see fp32)"},
-            "fp32": {"achieved": NCU_FP32_FLOP_PER_PIXEL * NPIX / (kern_per_launch_ms / 1e3) / 1e12,
-                     "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
-                     "frac": NCU_FP32_FLOP_PER_PIXEL * NPIX / (kern_per_launch_ms / 1e3) / 1e12 / FP32_PEAK_TFLOPS,
-                     "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1965 MHz)",
-                     "flop": "executed FP32 flop per pixel from ncu, not an algorithmic count"},
+            "phases_ms": {"node_build": build_ms, "adjoint": adj_ms},
+            "roofline": dominant,
+            "rooflines": {"adjoint": r_adj, "node_build": r_bld},
+            "record_boundary": {"value": NPIX * world / (rec_ms / 1e3), "unit": "pixels/s", "ms_per_step": rec_ms,
+                                "what": "snapi_adjoint_packed on device-resident records + packed node tangents "
+                                        "(the adjoint alone)"},
+            "fd_baseline": {"record_boundary": {"value": NPIX * world / (fd_ms / 1e3), "unit": "pixels/s",
+                                                "ms_per_step": fd_ms, "solves_per_gradient": 2 * npar + 1,
+                                                "adjoint_speedup": fd_ms / rec_ms},
+                            "from_nodes": {"value": NPIX * world / (fdn_ms / 1e3), "unit": "pixels/s",
+                                           "ms_per_step": fdn_ms,
+                                           "what": "2 npar + 1 node-vector builds (records only) + syntheses",
+                                           "adjoint_speedup": fdn_ms / ms_step}},
+            "measured_peaks": {"fp32_fma_tflops": fp32, "fp64_fma_tflops": fp64, "hbm_gbs": peaks["hbm_gbs"],
+                               "hbm_source": peaks["source"]},
+            "flagged_columns": flagged,
         }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = reference_cpu_rate(samples_per_core=1, mode=1)
