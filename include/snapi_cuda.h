@@ -465,6 +465,28 @@ double snapi_last_phase_ms(const snapi_ctx *ctx, int phase);
 /* Number of kernel launches of the last call. */
 int snapi_last_launches(const snapi_ctx *ctx);
 
+/* The autotuner: launch shapes picked per context and batch size by timing them.  No counterpart in
+ * the reference (its loops have no launch shapes).  The shapes it chooses between compute the same
+ * bits (they change which thread or CTA handles a wavelength or a pixel, never the order of a sum):
+ *   the adjoint: 32, 64 or 128 wavelengths per sweep CTA (the padding of the wavelength grid to the
+ *     CTA width, e.g. 201 -> 224 / 256 / 256, against the CTA's staging cost), and 8, 16 or 32
+ *     pixels per opacity-adjoint tile (L2 reuse of a tile's adjoint bars across its transitions);
+ *   the node build: 32, 64 or 128 threads per hydrostatic-march CTA, 64, 128 or 256 per
+ *     record-chemistry CTA.
+ * mode 1: the first snapi_adjoint / snapi_adjoint_nodes call with device buffers (SNAPI_MEM_DEVICE;
+ * calls on host buffers use tuned shapes but do not tune) and the first node build of each
+ * batch-size bucket (the next power of two >= npix) runs every candidate once on its own inputs,
+ * timed by CUDA events, keeps the fastest and then computes the call with it; later calls of the
+ * bucket reuse it.  cache_path (may be NULL): a text file of earlier choices, read now (entries for
+ * this device and problem shape) and appended to after each tuning, so that other processes skip
+ * the trials.  mode 0 (the default): the compiled shapes (64 wavelengths, 16-pixel tiles, 64 and 64
+ * threads).  Switching the mode forgets earlier choices. */
+int snapi_autotune(snapi_ctx *ctx, int mode, const char *cache_path);
+/* The shapes in use for a batch of npix pixels: cfg[4] = {wavelengths per sweep CTA, pixels per
+ * opacity tile, march CTA threads, record-chemistry CTA threads}.  Returns a bit set: 1 the adjoint
+ * shapes were tuned, 2 the build's were (0: the compiled defaults). */
+int snapi_tuned_config(const snapi_ctx *ctx, int npix, int *cfg);
+
 /* The measured fused multiply-add peak of GPU `device` in TFLOP/s (fp64 = 0: FP32, 1: FP64): a
  * kernel of independent FMA chains filling every SM, timed by CUDA events (best of three launches
  * after a warm-up).  The denominator of the benchmark's compute rooflines; no counterpart in the

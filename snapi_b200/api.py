@@ -161,6 +161,8 @@ def lib():
         L.snapi_fma_peak.argtypes = [ip, ip, ctypes.POINTER(ctypes.c_double)]
         L.snapi_last_phase_ms.restype = ctypes.c_double
         L.snapi_last_phase_ms.argtypes = [vp, ip]
+        L.snapi_autotune.argtypes = [vp, ip, ctypes.c_char_p]
+        L.snapi_tuned_config.argtypes = [vp, ip, fp]
         L.snapi_build_records.argtypes = [vp, ip, fp, fp, fp, fp, fp, fp, fp, ip]
         L.snapi_build_atmos.argtypes = [vp, ip, fp, fp, fp, fp, fp, ip]
         L.snapi_records_from_columns.argtypes = [vp, ip, fp, fp, fp, ip]
@@ -545,6 +547,19 @@ class Context:
         self._eos = tables  # keep the ctypes tables alive for the call
         self._check(lib().snapi_eos_set(self._ctx, ctypes.addressof(tables.model)))
         self._eos_npar = tables.npar
+
+    def autotune(self, on=True, cache_path=None):
+        """snapi_autotune: pick launch shapes by timing them on the first calls of each batch size
+        (on), or use the compiled ones (off); cache_path: optional file shared across processes."""
+        self._check(lib().snapi_autotune(self._ctx, 1 if on else 0,
+                                         None if cache_path is None else str(cache_path).encode()))
+
+    def tuned_config(self, npix):
+        """(shapes dict, tuned bits) of snapi_tuned_config for a batch of npix pixels."""
+        cfg = np.zeros(4, np.int32)
+        bits = lib().snapi_tuned_config(self._ctx, int(npix), _ptr(cfg))
+        keys = ("chunk", "optile", "he_threads", "var_threads")
+        return {k: int(v) for k, v in zip(keys, cfg)}, int(bits)
 
     def eos_chem_start(self, mode):
         """How the march's chemistry starts each solve: CHEM_START_CONTINUE (default; Newton from the

@@ -48,6 +48,9 @@ constexpr int kOpTile = SNAPI_OP_TILE;  // k_adj_opacity: pixels whose CTAs are 
 struct CtaPos {
   int pix, var, chunk, l, warp0, wslot;
 };
+// CTA of C wavelengths (C = blockDim.x): pixel, variant, wavelength chunk; the warp slot is the
+// warp's global wavelength index / 32, the same for every C
+template <int C = kChunk>
 __device__ __forceinline__ CtaPos cta_pos(const KParams &P) {
   CtaPos c;
   const int cta = blockIdx.x;
@@ -55,8 +58,8 @@ __device__ __forceinline__ CtaPos cta_pos(const KParams &P) {
   const int t = cta / P.nchunk;
   c.var = t % P.nvar;
   c.pix = t / P.nvar;
-  c.l = c.chunk * kChunk + threadIdx.x;
-  c.warp0 = c.chunk * kChunk + (threadIdx.x & ~31);
+  c.l = c.chunk * C + threadIdx.x;
+  c.warp0 = c.chunk * C + (threadIdx.x & ~31);
   c.wslot = c.warp0 >> 5;
   return c;
 }
@@ -86,10 +89,12 @@ __global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_synth(KParams P) {
 
 // Adjoint, phase F: forward sweep storing the per-depth state, the emergent Stokes vector, the
 // chi2 partials and the adjoint seed of every wavelength.
-__global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_adj_forward(KParams P) {
+// (C wavelengths per CTA: one of kChunkCands; the register budget per thread is the same for all)
+template <int C>
+__global__ void __launch_bounds__(C, SNAPI_SYN_MINB * kChunk / C) k_adj_forward(KParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const SmemLayout L = smem_layout(P.nd, P.nfield, P.nlines, P.ncomp, P.nred, false);
-  const CtaPos c = cta_pos(P);
+  const CtaPos c = cta_pos<C>(P);
   PixelView pv;
   if (!stage_pixel(P, c.pix, smem, L, pv, -1, 0.f)) return;
   if (c.warp0 >= P.nl) return;
@@ -120,8 +125,9 @@ __global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_adj_forward(KParams 
 
 // Adjoint, phase R1: reverse DELO sweep and optical-depth adjoint per wavelength (no opacity
 // work, no shared memory); writes (eta-bar, j-bar) of every depth.
-__global__ void __launch_bounds__(kChunk, SNAPI_RT_MINB) k_adj_rt(KParams P) {
-  const CtaPos c = cta_pos(P);
+template <int C>
+__global__ void __launch_bounds__(C, SNAPI_RT_MINB) k_adj_rt(KParams P) {
+  const CtaPos c = cta_pos<C>(P);
   if (c.warp0 >= P.nl) return;
   PixelView pv;
   pv.nd = P.nd;
@@ -149,8 +155,8 @@ __global__ void __launch_bounds__(kOpThreads, SNAPI_OP_MINB) k_adj_opacity(KPara
   extern __shared__ __align__(16) unsigned char smem[];
   const SmemLayout L = smem_layout(P.nd, P.nfield, P.nlines, P.ncomp, P.nred, false);
   const int ng = 1 + P.nlines, S = P.nslice;
-  const int tile = blockIdx.x / (ng * kOpTile), r = blockIdx.x % (ng * kOpTile);
-  const int g = r / kOpTile, pix = tile * kOpTile + r % kOpTile;
+  const int tile = blockIdx.x / (ng * P.optile), r = blockIdx.x % (ng * P.optile);
+  const int g = r / P.optile, pix = tile * P.optile + r % P.optile;
   if (pix >= P.npix) return;  // CTA-uniform: the last tile is partial
   PixelView pv;
   if (!stage_pixel(P, pix, smem, L, pv, -1, 0.f)) return;
@@ -358,13 +364,58 @@ namespace {
 
 // the adjoint's kernel sequence for nb pixels (P.npix = nb)
 constexpr int kAdjointLaunches = 4;
-void launch_adjoint(const KParams &P, int nb, int nchunk, size_t smem_sweep, size_t smem_fin, cudaStream_t st) {
-  k_adj_forward<<<nb * nchunk, kChunk, smem_sweep, st>>>(P);
-  k_adj_rt<<<nb * nchunk, kChunk, 0, st>>>(P);
+// with the launch shape cfg: cfg.chunk wavelengths per sweep CTA (the forward state and seed are
+// laid out with lpad = that chunk's padding; the buffers hold the widest), cfg.optile pixels per
+// opacity-adjoint tile
+void launch_adjoint(const KParams &P0, int nb, const AdjCfg &cfg, size_t smem_sweep, size_t smem_fin,
+                    cudaStream_t st) {
+  KParams P = P0;
+  P.nchunk = (P.nl + cfg.chunk - 1) / cfg.chunk;
+  P.lpad = P.nchunk * cfg.chunk;
+  P.nwslot = P.lpad / 32;
+  P.optile = cfg.optile;
+  const int nsw = nb * P.nchunk;
+  if (cfg.chunk == 32) {
+    k_adj_forward<32><<<nsw, 32, smem_sweep, st>>>(P);
+    k_adj_rt<32><<<nsw, 32, 0, st>>>(P);
+  } else if (cfg.chunk == 128) {
+    k_adj_forward<128><<<nsw, 128, smem_sweep, st>>>(P);
+    k_adj_rt<128><<<nsw, 128, 0, st>>>(P);
+  } else {
+    k_adj_forward<64><<<nsw, 64, smem_sweep, st>>>(P);
+    k_adj_rt<64><<<nsw, 64, 0, st>>>(P);
+  }
   const int nthr = std::min(kOpThreads, (P.nd * P.nslice + 31) / 32 * 32);
-  const int ntile = (nb + kOpTile - 1) / kOpTile;
-  k_adj_opacity<<<ntile * (1 + P.nlines) * kOpTile, nthr, smem_sweep, st>>>(P);
+  const int ntile = (nb + P.optile - 1) / P.optile;
+  k_adj_opacity<<<ntile * (1 + P.nlines) * P.optile, nthr, smem_sweep, st>>>(P);
   k_adjoint_finish<<<nb, kFinishThreads, smem_fin, st>>>(P);
+}
+
+// The autotuner's choice for an adjoint of nb pixels: each launch shape is run once on the call's
+// own inputs (all shapes compute the same bits), timed by CUDA events; first the chunk width at
+// the default tile, then the tile at the best width.
+AdjCfg tune_adjoint(snapi_ctx *ctx, const KParams &P, int nb, size_t smem_sweep, size_t smem_fin) {
+  AdjCfg best{kChunk, kOpTile};
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return best;
+  if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return best; }
+  float best_ms = -1.f;
+  auto trial = [&](const AdjCfg &c) {
+    cudaEventRecord(e0, ctx->stream);
+    launch_adjoint(P, nb, c, smem_sweep, smem_fin, ctx->stream);
+    cudaEventRecord(e1, ctx->stream);
+    float ms = -1.f;
+    if (cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    if (ms > 0.f && (best_ms < 0.f || ms < best_ms)) { best_ms = ms; best = c; }
+  };
+  for (int ch : kChunkCands)
+    if ((ctx->nl + ch - 1) / ch * ch <= ctx->lpad_max) trial(AdjCfg{ch, kOpTile});
+  const int bc = best.chunk;
+  for (int t : kOpTileCands)
+    if (t != kOpTile) trial(AdjCfg{bc, t});
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
 }
 
 }  // namespace
@@ -381,6 +432,81 @@ int set_err(snapi_ctx *c, int code, const char *fmt, ...) {
   return code;
 }
 
+// ---- autotuner bookkeeping --------------------------------------------------------------------
+int tune_bucket(int npix) {
+  int b = 64;
+  while (b < npix && b < (1 << 30)) b <<= 1;
+  return b;
+}
+
+// the cache file's key of this context's problem shape on its device
+static std::string tune_key(const snapi_ctx *ctx) {
+  cudaDeviceProp prop;
+  std::string name = cudaGetDeviceProperties(&prop, ctx->device) == cudaSuccess ? prop.name : "unknown";
+  for (char &ch : name)
+    if (ch == ' ' || ch == '|') ch = '_';
+  char b[256];
+  snprintf(b, sizeof b, "%s|%d|%d|%d|%d", name.c_str(), ctx->nd, ctx->nl, ctx->nlines, ctx->ncomp);
+  return b;
+}
+
+bool tuned_adj(const snapi_ctx *ctx, int npix, AdjCfg *cfg) {
+  const int b = tune_bucket(npix);
+  for (const auto &e : ctx->adj_tuned)
+    if (e.first == b) { *cfg = e.second; return true; }
+  return false;
+}
+
+bool tuned_build(const snapi_ctx *ctx, int npix, BuildCfg *cfg) {
+  const int b = tune_bucket(npix);
+  for (const auto &e : ctx->build_tuned)
+    if (e.first == b) { *cfg = e.second; return true; }
+  return false;
+}
+
+static void tune_append(const snapi_ctx *ctx, const char *line) {
+  if (ctx->tune_cache.empty()) return;
+  FILE *f = fopen(ctx->tune_cache.c_str(), "a");
+  if (!f) return;
+  fprintf(f, "%s|%s\n", tune_key(ctx).c_str(), line);
+  fclose(f);
+}
+
+void tune_store_adj(snapi_ctx *ctx, int npix, const AdjCfg &cfg) {
+  ctx->adj_tuned.emplace_back(tune_bucket(npix), cfg);
+  char b[96];
+  snprintf(b, sizeof b, "adj|%d|%d|%d", tune_bucket(npix), cfg.chunk, cfg.optile);
+  tune_append(ctx, b);
+}
+
+void tune_store_build(snapi_ctx *ctx, int npix, const BuildCfg &cfg) {
+  ctx->build_tuned.emplace_back(tune_bucket(npix), cfg);
+  char b[96];
+  snprintf(b, sizeof b, "build|%d|%d|%d", tune_bucket(npix), cfg.he, cfg.var);
+  tune_append(ctx, b);
+}
+
+// earlier tunings of this shape on this device from the cache file (later lines win)
+static void tune_load(snapi_ctx *ctx) {
+  if (ctx->tune_cache.empty()) return;
+  FILE *f = fopen(ctx->tune_cache.c_str(), "r");
+  if (!f) return;
+  const std::string key = tune_key(ctx) + "|";
+  char line[512];
+  auto member = [](const int *cands, int v) { return v == cands[0] || v == cands[1] || v == cands[2]; };
+  while (fgets(line, sizeof line, f)) {
+    if (strncmp(line, key.c_str(), key.size()) != 0) continue;
+    int b = 0, x = 0, y = 0;
+    const char *rest = line + key.size();
+    if (sscanf(rest, "adj|%d|%d|%d", &b, &x, &y) == 3 && member(kChunkCands, x) && member(kOpTileCands, y)) {
+      ctx->adj_tuned.insert(ctx->adj_tuned.begin(), {b, AdjCfg{x, y}});
+    } else if (sscanf(rest, "build|%d|%d|%d", &b, &x, &y) == 3 && member(kHeCands, x) && member(kVarCands, y)) {
+      ctx->build_tuned.insert(ctx->build_tuned.begin(), {b, BuildCfg{x, y}});
+    }
+  }
+  fclose(f);
+}
+
 int ensure_npar(snapi_ctx *ctx, int npar) {
   if (npar <= ctx->cap_npar) return SNAPI_OK;
   const size_t nrec = (size_t)ctx->nd * ctx->nfield, B = ctx->max_batch;
@@ -391,7 +517,7 @@ int ensure_npar(snapi_ctx *ctx, int npar) {
   ctx->cap_npar = 0;
   SNAPI_CK(cudaMalloc(&ctx->d_tan, sizeof(float) * B * npar * nrec));
   SNAPI_CK(cudaMalloc(&ctx->d_grad, sizeof(double) * B * npar));
-  SNAPI_CK(cudaMalloc(&ctx->d_c2part, sizeof(double) * B * (2 * npar + 1) * ctx->nwslot));
+  SNAPI_CK(cudaMalloc(&ctx->d_c2part, sizeof(double) * B * (2 * npar + 1) * (ctx->lpad_max / 32)));
   SNAPI_CK(cudaMalloc(&ctx->d_step, sizeof(double) * npar));
   SNAPI_CK(cudaMalloc(&ctx->d_dstokes, sizeof(float) * B * npar * ctx->nl * 4));
   ctx->cap_npar = npar;
@@ -403,6 +529,7 @@ KParams base_params(const snapi_ctx *ctx) {
   memset(&P, 0, sizeof P);
   P.nd = ctx->nd; P.nl = ctx->nl; P.nlines = ctx->nlines; P.nfield = ctx->nfield; P.lpad = ctx->lpad;
   P.ncomp = ctx->ncomp; P.nred = ctx->nred; P.nchunk = ctx->nchunk; P.nwslot = ctx->nwslot; P.nvar = 1;
+  P.optile = kOpTile;
   P.nslice = op_slices(ctx->nd);
   P.lam_mid = ctx->lam_mid; P.scale2 = ctx->scale2;
   P.lamvac = ctx->d_lamvac; P.lines = ctx->d_lines; P.compS = ctx->d_compS; P.compD = ctx->d_compD;
@@ -431,7 +558,9 @@ namespace snapi {
 // device's opt-in maximum) on the current device.
 cudaError_t raise_smem_limits(int bytes) {
   const void *k[] = {(const void *)k_synth, (const void *)k_fd_sweep, (const void *)k_resp_sweep,
-                     (const void *)k_adj_forward, (const void *)k_adj_opacity, (const void *)k_adjoint_finish};
+                     (const void *)k_adj_forward<32>, (const void *)k_adj_forward<64>,
+                     (const void *)k_adj_forward<128>, (const void *)k_adj_opacity,
+                     (const void *)k_adjoint_finish};
   for (const void *f : k) {
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
@@ -511,6 +640,29 @@ void snapi_host_free(void *p) {
 const char *snapi_last_error(const snapi_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 void *snapi_stream(snapi_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 double snapi_last_kernel_ms(const snapi_ctx *ctx) { return ctx ? ctx->last_ms : 0.0; }
+int snapi_autotune(snapi_ctx *ctx, int mode, const char *cache_path) {
+  if (!ctx) return SNAPI_EINVAL;
+  if (mode != 0 && mode != 1) return set_err(ctx, SNAPI_EINVAL, "snapi_autotune: mode must be 0 or 1");
+  ctx->tune = mode;
+  ctx->adj_tuned.clear();
+  ctx->build_tuned.clear();
+  ctx->tune_cache = cache_path ? cache_path : "";
+  if (mode) tune_load(ctx);
+  return SNAPI_OK;
+}
+
+int snapi_tuned_config(const snapi_ctx *ctx, int npix, int *cfg) {
+  if (!ctx || !cfg) return SNAPI_EINVAL;
+  AdjCfg a{kChunk, kOpTile};
+  BuildCfg b{kHeDefault, kVarDefault};
+  const bool ha = ctx->tune && tuned_adj(ctx, npix, &a), hb = ctx->tune && tuned_build(ctx, npix, &b);
+  cfg[0] = a.chunk;
+  cfg[1] = a.optile;
+  cfg[2] = b.he;
+  cfg[3] = b.var;
+  return (ha ? 1 : 0) | (hb ? 2 : 0);
+}
+
 double snapi_last_phase_ms(const snapi_ctx *ctx, int phase) {
   return (ctx && phase >= 0 && phase < 2) ? ctx->phase_ms[phase] : 0.0;
 }
@@ -575,6 +727,7 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
   ctx->nchunk = (prob->nlambda + kChunk - 1) / kChunk;
   ctx->lpad = ctx->nchunk * kChunk;
   ctx->nwslot = ctx->lpad / 32;
+  ctx->lpad_max = std::max(ctx->lpad, (prob->nlambda + 127) / 128 * 128);
   ctx->max_batch = prob->max_batch > 0 ? prob->max_batch : 4096;
   ctx->scale2 = prob->stokes_scale * prob->stokes_scale;
   std::vector<double> lv(ctx->nl);
@@ -662,8 +815,8 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
   CKC(cudaMalloc(&ctx->d_mask, sizeof(float) * B * ctx->nl));
   CKC(cudaMalloc(&ctx->d_recgrad, sizeof(double) * B * nrec));
   CKC(cudaMalloc(&ctx->d_chi2, sizeof(double) * B));
-  CKC(cudaMalloc(&ctx->d_scratch, sizeof(float4) * B * ctx->nd * 4 * ctx->lpad));
-  CKC(cudaMalloc(&ctx->d_seed, sizeof(float4) * B * ctx->lpad));
+  CKC(cudaMalloc(&ctx->d_scratch, sizeof(float4) * B * ctx->nd * 4 * ctx->lpad_max));
+  CKC(cudaMalloc(&ctx->d_seed, sizeof(float4) * B * ctx->lpad_max));
   CKC(cudaMalloc(&ctx->d_bars, sizeof(float4) * B * ctx->nl * 3 * ctx->nd));
   CKC(cudaMalloc(&ctx->d_opart, sizeof(float) * B * (1 + ctx->nlines) * op_slices(ctx->nd) * ctx->nd * kOpSlots));
   // the kernels' dynamic shared-memory limit is a per-device attribute that every context (and the
@@ -786,8 +939,13 @@ int adjoint_impl(snapi_ctx *ctx, int npix, const float *records, const float *ob
       P.chi2 = dev ? chi2 + p0 : ctx->d_chi2 + lo;
       P.grad = npar ? (dev ? grad + (size_t)p0 * npar : ctx->d_grad + (size_t)lo * npar) : ctx->d_grad;
       P.rec_grad = rec_grad ? (dev ? rec_grad + (size_t)p0 * nrec : ctx->d_recgrad + (size_t)lo * nrec) : nullptr;
+      AdjCfg cfg{kChunk, kOpTile};
+      if (ctx->tune && !tuned_adj(ctx, nr, &cfg) && dev && ci == 0) {
+        cfg = tune_adjoint(ctx, P, nb, Lsw.total, Lfin.total);
+        tune_store_adj(ctx, nr, cfg);
+      }
       if (k == 0) SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
-      launch_adjoint(P, nb, ctx->nchunk, Lsw.total, Lfin.total, ctx->stream);
+      launch_adjoint(P, nb, cfg, Lsw.total, Lfin.total, ctx->stream);
       SNAPI_CK(cudaGetLastError());
       ctx->last_launches += kAdjointLaunches;
       lo += nb;
@@ -1111,7 +1269,7 @@ int noalloc_run(const snapi_problem *prob, void *stream_v, int npix, const float
     KParams P;
     memset(&P, 0, sizeof P);
     P.npix = nb; P.nd = nd; P.nl = nl; P.nlines = nlines; P.nfield = nfield; P.npar = npar; P.lpad = lpad;
-    P.ncomp = ncomp; P.nred = nred; P.nchunk = nchunk; P.nwslot = nwslot; P.nvar = 1;
+    P.ncomp = ncomp; P.nred = nred; P.nchunk = nchunk; P.nwslot = nwslot; P.nvar = 1; P.optile = kOpTile;
     P.nslice = op_slices(nd);
     P.lam_mid = (float)(0.5 * (lv[nl - 1] + lv[0]));
     P.scale2 = prob->stokes_scale * prob->stokes_scale;
@@ -1134,7 +1292,7 @@ int noalloc_run(const snapi_problem *prob, void *stream_v, int npix, const float
     P.stokes = stokes ? stokes + (size_t)p0 * nl * 4 : nullptr;
     P.chi2 = chi2 + p0;
     P.grad = npar ? grad + (size_t)p0 * npar : nullptr;
-    launch_adjoint(P, nb, nchunk, Lsw.total, Lfin.total, stream);
+    launch_adjoint(P, nb, AdjCfg{kChunk, kOpTile}, Lsw.total, Lfin.total, stream);
     CKN(cudaGetLastError());
   }
   int st = 0;

@@ -49,7 +49,6 @@ constexpr int kER = 32;                   // stages whose ionisation fraction is
 constexpr int kEL = 64;                   // levels whose population enters a record
 constexpr int kEB = 32;                   // bound-free levels
 constexpr int kEP = SNAPI_EOS_MAX_PAR;    // nodes
-constexpr int kHeThreads = 64;
 constexpr int kRecThreads = 64;
 constexpr int kPolishCap = 400;
 
@@ -613,7 +612,7 @@ __device__ __forceinline__ void variant_pert(const EosDev &E, const EosArgs &A, 
   }
 }
 
-__global__ void __launch_bounds__(kHeThreads) k_eos_he(EosArgs A) {
+__global__ void __launch_bounds__(128) k_eos_he(EosArgs A) {  // launched with kHeCands threads
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.npix * A.nvar) return;
   const int p = i % A.npix, v = i / A.npix;
@@ -731,7 +730,7 @@ __device__ void field_fields(const EosDev &E, const NodeView &nv, int x, bool bu
 
 // thermal fields of every (pixel, variant, depth), one thread each (pixel fastest: a warp holds 32
 // pixels of one variant at one depth), FP64 into F [npix][nvar][nd][nf]
-__global__ void __launch_bounds__(kRecThreads) k_eos_var(EosArgs A) {
+__global__ void __launch_bounds__(256) k_eos_var(EosArgs A) {  // launched with kVarCands threads
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)A.npix * A.nvar * A.nd) return;
   const int p = (int)(i % A.npix);
@@ -882,6 +881,28 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_col(const EosDev *tab, int 
 }
 
 // ---- host side ---------------------------------------------------------------------------------------------
+// The autotuner's pick among three CTA sizes for one launch: each is run once and timed by CUDA
+// events on the context's stream; the default when no timing succeeds.
+template <class F>
+int tune_launch(snapi_ctx *ctx, const int (&cands)[3], F launch, int fallback) {
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return fallback;
+  if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return fallback; }
+  int best = fallback;
+  float best_ms = -1.f;
+  for (int t : cands) {
+    cudaEventRecord(e0, ctx->stream);
+    launch(t);
+    cudaEventRecord(e1, ctx->stream);
+    float ms = -1.f;
+    if (cudaGetLastError() == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess)
+      cudaEventElapsedTime(&ms, e0, e1);
+    if (ms > 0.f && (best_ms < 0.f || ms < best_ms)) { best_ms = ms; best = t; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
+}
 struct EosCtx {
   EosDev *d_tab = nullptr;
   int npar = 0, ntherm = 0;
@@ -1314,12 +1335,24 @@ static int build_impl(snapi_ctx *ctx, int npix, const double *nodes, const int *
       A.Nt_out = Nt ? Nt + (size_t)p0 * nd : nullptr;
     }
     SNAPI_CK(cudaMemsetAsync(e->d_status, 0, sizeof(int) * nb, ctx->stream));
-    SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
     const int nhe = nb * nvar;
-    k_eos_he<<<(nhe + kHeThreads - 1) / kHeThreads, kHeThreads, 0, ctx->stream>>>(A);
-    SNAPI_CK(cudaGetLastError());
     const long long nvx = (long long)nb * nvar * nd;
-    k_eos_var<<<(unsigned)((nvx + kRecThreads - 1) / kRecThreads), kRecThreads, 0, ctx->stream>>>(A);
+    auto launch_he = [&](int t) { k_eos_he<<<(nhe + t - 1) / t, t, 0, ctx->stream>>>(A); };
+    auto launch_var = [&](int t) {
+      k_eos_var<<<(unsigned)((nvx + t - 1) / t), t, 0, ctx->stream>>>(A);
+    };
+    BuildCfg cfg{kHeDefault, kVarDefault};
+    if (ctx->tune && !tuned_build(ctx, npix, &cfg) && p0 == 0) {
+      // the autotuner: each CTA size once on this chunk (same results; timed by CUDA events)
+      cfg.he = tune_launch(ctx, kHeCands, launch_he, kHeDefault);
+      cfg.var = tune_launch(ctx, kVarCands, launch_var, kVarDefault);
+      tune_store_build(ctx, npix, cfg);
+      SNAPI_CK(cudaMemsetAsync(e->d_status, 0, sizeof(int) * nb, ctx->stream));
+    }
+    SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    launch_he(cfg.he);
+    SNAPI_CK(cudaGetLastError());
+    launch_var(cfg.var);
     SNAPI_CK(cudaGetLastError());
     const int nrec = nb * nd;
     ctx->last_launches += 2;

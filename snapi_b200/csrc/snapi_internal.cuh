@@ -42,9 +42,25 @@ __host__ __device__ inline int op_slices(int nd) {
   return s;
 }
 
+// Launch shapes the autotuner (snapi_autotune) chooses between, per context and batch size; the
+// defaults are the compiled constants.  All of them give bit-identical results: they change which
+// thread or CTA handles a wavelength or pixel, never the order of a sum.
+constexpr int kChunkCands[3] = {32, 64, 128};   // wavelengths per sweep CTA of the adjoint
+constexpr int kOpTileCands[3] = {8, 16, 32};    // pixels per opacity-adjoint CTA tile
+constexpr int kHeCands[3] = {32, 64, 128};      // threads per hydrostatic-march CTA
+constexpr int kVarCands[3] = {64, 128, 256};    // threads per record-chemistry CTA
+constexpr int kHeDefault = 64, kVarDefault = 64;  // the chemistry kernels' compiled CTA sizes
+struct AdjCfg {
+  int chunk, optile;
+};
+struct BuildCfg {
+  int he, var;
+};
+
 struct KParams {
   int npix, nd, nl, nlines, nfield, npar, lpad, ncomp, nred, nchunk, nwslot, nvar;
   int nslice;                   // wavelength slices of the opacity adjoint (threads = nd x nslice)
+  int optile;                   // pixels per opacity-adjoint CTA tile
   float lam_mid;
   double scale2;                // stokes_scale^2
   const float *rec;             // [npix][nd][nfield]
@@ -299,6 +315,13 @@ struct snapi_ctx {
   static constexpr int kStageChunks = 8;  // host-input chunks per round (adjoint_impl)
   cudaEvent_t ev_copy[kStageChunks] = {}, ev_free = nullptr;  // chunk uploaded / round's kernels done
   int nd = 0, nl = 0, nlines = 0, nfield = 0, ncomp = 0, nred = 0, lpad = 0, nchunk = 0, nwslot = 0, max_batch = 0;
+  int lpad_max = 0;  // padded wavelengths of the widest sweep CTA the autotuner may pick (buffer sizes)
+  // autotuner (snapi_autotune): off = the compiled launch shapes; per batch-size bucket the shapes
+  // it measured fastest; an optional cache file shared across processes
+  int tune = 0;
+  std::string tune_cache;
+  std::vector<std::pair<int, snapi::AdjCfg>> adj_tuned;
+  std::vector<std::pair<int, snapi::BuildCfg>> build_tuned;
   float lam_mid = 0.f;
   double scale2 = 1.0;
   double *d_lamvac = nullptr, *d_D = nullptr;
@@ -336,6 +359,13 @@ int set_err(snapi_ctx *c, int code, const char *fmt, ...);
 int ensure_npar(snapi_ctx *ctx, int npar);
 KParams base_params(const snapi_ctx *ctx);
 int check_status(snapi_ctx *ctx);
+// autotuner (snapi_cuda.cu): the batch-size bucket of npix, the tuned shapes of a bucket (false if
+// none yet), their record in the context and the cache file
+int tune_bucket(int npix);
+bool tuned_adj(const snapi_ctx *ctx, int npix, AdjCfg *cfg);
+bool tuned_build(const snapi_ctx *ctx, int npix, BuildCfg *cfg);
+void tune_store_adj(snapi_ctx *ctx, int npix, const AdjCfg &cfg);
+void tune_store_build(snapi_ctx *ctx, int npix, const BuildCfg &cfg);
 // sweep launches for other translation units (P.npix pixels; P.nvar nodes for the responses)
 cudaError_t launch_synth(const snapi_ctx *ctx, const KParams &P);
 cudaError_t launch_responses(const snapi_ctx *ctx, const KParams &P);
