@@ -737,11 +737,16 @@ __global__ void __launch_bounds__(256) k_eos_var(EosArgs A) {  // launched with 
   const long long r = i / A.npix;
   const int v = (int)(r % A.nvar), x = (int)(r / A.nvar);
   if (A.active && !A.active[p]) return;
+  const size_t cv = ((size_t)p * A.nvar + v) * A.nd + x;
+  // A temperature-node variant leaves T, and so the march, bit-identical to variant 0 above the
+  // first depth whose interpolation segment uses that node: its fields there are variant 0's
+  // (k_eos_rec reads those), and the tangent's difference is exactly 0, as the reference's is.
+  const size_t c0 = (size_t)p * A.nvar * A.nd + x;
+  if (v > 0 && A.T[cv] == A.T[c0] && A.Nt[cv] == A.Nt[c0]) return;
   const EosDev &E = *A.tab;
   Chem c(E);
   int st = 0;
   double f[SNAPI_NFIELD0 + 3 * SNAPI_MAX_LINES];
-  const size_t cv = ((size_t)p * A.nvar + v) * A.nd + x;
   // the reference's start, whatever the march used: the record fields take the stage fractions of
   // the last Newton sweep before its final update, so they follow the solve's path to ~1e-4
   thermal_fields(E, c, A.T[cv], A.Nt[cv], f, st);
@@ -780,8 +785,13 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_rec(EosArgs A) {
       const double stp = A.step[q];
       if (q >= E.kfirst[1] && q < E.kfirst[1] + E.kcount[1]) {
         const int v = 1 + 2 * (q - E.kfirst[1]);
-        const double *Fp = A.F + (((size_t)p * A.nvar + v) * A.nd + x) * nf;
-        const double *Fm = A.F + (((size_t)p * A.nvar + v + 1) * A.nd + x) * nf;
+        // a variant identical to variant 0 at this depth has variant 0's fields (k_eos_var skips it)
+        auto fields = [&](int w) {
+          const size_t cw = ((size_t)p * A.nvar + w) * A.nd + x, cb = (size_t)p * A.nvar * A.nd + x;
+          return A.F + ((A.T[cw] == A.T[cb] && A.Nt[cw] == A.Nt[cb]) ? cb : cw) * nf;
+        };
+        const double *Fp = fields(v);
+        const double *Fm = fields(v + 1);
         for (int f = 0; f < nf; ++f) {
           const bool th = !(f == 1 || (f >= 3 && f <= 6));
           tq[f] = th ? (float)((Fp[f] - Fm[f]) / stp) : 0.f;
