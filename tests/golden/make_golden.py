@@ -78,12 +78,12 @@ def config1_temperature(x):
 
 
 def write_cfg(path, t_taus, t_vals, vs_taus, vs_vals, vt=1e5, B=1000.0, theta_deg=45.0, phi_deg=30.0,
-              atoms="atoms_6300.cfg", lam="6301.0-6303.4", dlam=0.012):
+              atoms="atoms_6300.cfg", lam="6301.0-6303.4", dlam=0.012, atmos_file="falc_80z.dat"):
     fmt = lambda a: ",".join("%.6f" % v for v in a)  # noqa: E731
     cfg = f"""atmos{{
   ID=col
   TYPE=SPINOR
-  FILE=falc_80z.dat
+  FILE={atmos_file}
   GEOMETRY=PLANEPARALLEL
   RTSOLVER=Bezier
   ATOM={atoms}
@@ -144,11 +144,11 @@ def run(args, cwd):
     return r.stderr
 
 
-def dump(tmp, task, nodes, flags, name):
+def dump(tmp, task, nodes, flags, name, dump_bin=None):
     nf = os.path.join(tmp, name + "_nodes.f64")
     np.ascontiguousarray(nodes, dtype="<f8").tofile(nf)
     out = os.path.join(tmp, name + ".sbin")
-    log = run([DUMP, "dump", task, nf, str(nodes.shape[0]), str(flags), out], tmp)
+    log = run([dump_bin or DUMP, "dump", task, nf, str(nodes.shape[0]), str(flags), out], tmp)
     sys.stderr.write(log)
     return read_sbin(out)
 
@@ -264,26 +264,55 @@ def make_config4(tmp, npix, iters=30, broadening=0.0, name="config4", seed=4, wo
                         iters=np.array([iters]), **line_arrays(d))
 
 
-def make_config5(tmp, ncol, niter=3):
+def write_atmos_resampled(src, dst, nd):
+    """The reference's SPINOR-format atmosphere file src resampled to nd depths (every column
+    interpolated linearly in the row index).  build_from_nodes takes only the depth count (and the
+    heights, for return_as_array) from it; the model's TAUGRID sets the log tau grid."""
+    rows = open(src).read().split("\n")
+    n0 = int(rows[0].split()[0])
+    a = np.array([[float(v) for v in r.split()] for r in rows[1:1 + n0]])
+    x0 = np.linspace(0.0, 1.0, n0)
+    x1 = np.linspace(0.0, 1.0, nd)
+    b = np.stack([np.interp(x1, x0, a[:, k]) for k in range(a.shape[1])], axis=1)
+    with open(dst, "w") as f:
+        f.write("%d\n" % nd)
+        for r in b:
+            f.write(" ".join("%.6e" % v for v in r) + "\n")
+
+
+def make_config5(tmp, ncol, niter=3, spec=False):
     """NLTE Ca II (config 5): the inputs of the level-population iteration per column, the
     populations after each of the reference's first niter iterations, and the populations its
-    nltepops converges to.  Columns: the ten-node model with seeded T / v_los / B (seed 5)."""
+    nltepops converges to.  Columns: the ten-node model with seeded T / v_los / B (seed 5).
+    Default: the reference as compiled (2 rays, the 1e-2 stop) on the 80-depth grid
+    (config5.npz).  spec: the configuration's stated settings (config5_spec.npz) -- the patched
+    reference build (the 5-point angle set, i.e. 10 ray directions, and a 1e-4 population stop)
+    on a 100-depth grid; the background opacity / emissivity stored as float32 to keep the fixture
+    small (the device takes them as float64; ~6e-8 relative)."""
     with open(os.path.join(tmp, "atoms_c5.cfg"), "w") as f:
         f.write("".join("ATOM=%s\n" % a for a in C5_ATOMS))
+    dump_bin, name, afile = DUMP, "config5", "falc_80z.dat"
+    if spec:
+        dump_bin, name, afile = DUMP_SPEC, "config5_spec", "falc_100z.dat"
+        write_atmos_resampled(os.path.join(tmp, "falc_80z.dat"), os.path.join(tmp, afile), 100)
     write_cfg(os.path.join(tmp, "c5.cfg"), C3_TTAU, C3_TRUTH[:4], C3_VSTAU, C3_TRUTH[5:7], atoms="atoms_c5.cfg",
-              lam="8538.5-8545.985", dlam=0.025)
-    run([DUMP, "pack", "c5.cfg", "c5.tsk"], tmp)
-    shutil.copy(os.path.join(tmp, "c5.tsk"), os.path.join(HERE, "c5.tsk"))
+              lam="8538.5-8545.985", dlam=0.025, atmos_file=afile)
+    run([dump_bin, "pack", "c5.cfg", "c5.tsk"], tmp)
+    if not spec:
+        shutil.copy(os.path.join(tmp, "c5.tsk"), os.path.join(HERE, "c5.tsk"))
     nodes = config3_nodes(ncol, seed=5)
     nf = os.path.join(tmp, "c5_nodes.f64")
     np.ascontiguousarray(nodes, dtype="<f8").tofile(nf)
     out = os.path.join(tmp, "c5.sbin")
-    sys.stderr.write(run([DUMP, "ali", "c5.tsk", nf, str(ncol), str(niter), out], tmp))
+    sys.stderr.write(run([dump_bin, "ali", "c5.tsk", nf, str(ncol), str(niter), out], tmp))
     d = read_sbin(out)
+    if spec:
+        for k in ("ali_bgop", "ali_bgem"):
+            d[k] = d[k].astype(np.float32)
     # the reference's synthesis of the 8542 window with those NLTE populations (obs_stokes runs
     # nltepops itself) and the column records the device synthesis takes
-    s = dump(tmp, os.path.join(tmp, "c5.tsk"), nodes, 0, "c5syn")
-    np.savez_compressed(os.path.join(HERE, "config5.npz"), nodes=nodes, **{k: v for k, v in d.items()},
+    s = dump(tmp, os.path.join(tmp, "c5.tsk"), nodes, 0, "c5syn", dump_bin=dump_bin)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), nodes=nodes, **{k: v for k, v in d.items()},
                         lambda_air=s["lambda_air"], tau500=s["tau500"], record=s["record"], stokes=s["stokes"],
                         ref_synth_seconds=s["ref_seconds_per_pixel"], **line_arrays(s))
 
@@ -362,7 +391,7 @@ def main():
         if a.c4pix and not a.only_c5:
             make_config4(tmp, a.c4pix, spec=a.spec)
         if a.c5col and not a.only_c4:
-            make_config5(tmp, a.c5col)
+            make_config5(tmp, a.c5col, spec=a.spec)
         if a.pool and not (a.only_c4 or a.only_c5):
             n4 = config3_nodes(a.pool, seed=303)
             d4 = dump(tmp, os.path.join(tmp, "c3.tsk"), n4, 2, "pool")

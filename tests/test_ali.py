@@ -1,10 +1,28 @@
 """NLTE level populations (snapi_ali_iter) against the reference's own iteration
-(atmosphere::nltepops on Ca II 8542 columns, tests/golden/config5.npz): the populations after each
-of the first iterations, and the populations the reference converges to."""
+(atmosphere::nltepops on Ca II 8542 columns): the populations after each of the first iterations,
+and the populations the reference converges to.  Two fixtures: config5.npz, the reference as
+compiled (2 ray directions, the 1e-2 stop, 80 depths), and config5_spec.npz, the configuration's
+stated settings from the patched reference build (the 5-point Gauss set, i.e. 10 ray directions,
+the 1e-4 stop, 100 depths)."""
+import os
+
 import numpy as np
 import pytest
 
+from conftest import GOLDEN, load_fixture
+
 pytestmark = pytest.mark.gpu
+
+# fixture -> the reference's population stop (nltepops' relative change)
+FIXTURES = {"config5": 1e-2, "config5_spec": 1e-4}
+
+
+def _have(name):
+    return os.path.exists(os.path.join(GOLDEN, name + ".npz"))
+
+
+_params = [pytest.param(n, marks=pytest.mark.skipif(not _have(n), reason="fixture %s.npz not generated" % n))
+           for n in FIXTURES]
 
 
 @pytest.fixture(scope="module")
@@ -19,8 +37,9 @@ def _rel(a, b):
     return np.abs(a / b - 1.0)
 
 
-def test_ali_iterations_follow_reference(sb, config5):
-    fx = config5
+@pytest.mark.parametrize("name", _params)
+def test_ali_iterations_follow_reference(sb, name):
+    fx = load_fixture(name)
     ctx = sb.api.AliContext.from_fixture(fx)
     cols = ctx.columns_from_fixture(fx)
     ref_it = fx["ali_pops_iter"]  # [ncol, niter, nd, nlevel]
@@ -37,14 +56,16 @@ def test_ali_iterations_follow_reference(sb, config5):
     ctx.close()
 
 
-def test_ali_converges_to_reference_populations(sb, config5):
-    fx = config5
+@pytest.mark.parametrize("name", _params)
+def test_ali_converges_to_reference_populations(sb, name):
+    fx = load_fixture(name)
+    tol = FIXTURES[name]
     ctx = sb.api.AliContext.from_fixture(fx)
-    pops, rel, iters, st = ctx.iterate(ctx.columns_from_fixture(fx), fx["ali_pop0"], max_iter=100, tol=1e-2)
-    assert np.all(st == 0) and np.all(rel < 1e-2)
+    pops, rel, iters, st = ctx.iterate(ctx.columns_from_fixture(fx), fx["ali_pop0"], max_iter=100, tol=tol)
+    assert np.all(st == 0) and np.all(rel < tol)
     err = _rel(pops, fx["ali_pop_conv"])
-    print("iterations", iters, "max relative difference to the reference's converged populations", err.max())
-    # both stop once the largest relative change of an iteration is below 1e-2, after the same
-    # number of iterations (10, 16, 14 for these columns)
+    print(name, "iterations", iters, "max relative difference to the reference's converged populations", err.max())
+    # both stop once the largest relative change of an iteration is below the stop, after the same
+    # number of iterations (config5: 10, 16, 14)
     assert err.max() < 1e-3
     ctx.close()

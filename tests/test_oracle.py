@@ -4,6 +4,7 @@ The golden fixtures were produced by the reference itself (oracle/_ref/snapi_ref
 by tests/golden/make_golden.py): the column record after build_from_nodes, the reference's
 normalised opacity at 7 wavelengths and its obs_stokes Stokes vectors."""
 import numpy as np
+import pytest
 
 
 def _lines(so, fx):
@@ -51,6 +52,21 @@ def test_stokes_config5_nlte_ca(oracle_lib, config5):
     """Ca II 8542 window with the reference's NLTE populations in the record (10 transitions:
     Ca II H, K and the infrared triplet, the hydrogen far wings, Fe I 6301/6302)."""
     assert _stokes_err(oracle_lib, config5) < 1e-12
+
+
+def _spec_fixture():
+    import os
+    from conftest import GOLDEN, load_fixture
+    if not os.path.exists(os.path.join(GOLDEN, "config5_spec.npz")):
+        pytest.skip("fixture config5_spec.npz not generated")
+    return load_fixture("config5_spec")
+
+
+def test_stokes_config5_spec(oracle_lib):
+    """The same window at the configuration's stated settings (100 depths; populations converged
+    by the patched reference with the 5-point angle set to 1e-4)."""
+    fx = _spec_fixture()
+    assert _stokes_err(oracle_lib, fx) < 1e-12
 
 
 def test_zeeman_pattern_matches_reference(oracle_lib, config1):
@@ -119,6 +135,20 @@ def test_ali_restatement_matches_reference_iterations(config5):
         assert not neg
         assert np.abs(p / fx["ali_pops_iter"][0, it] - 1.0).max() < 1e-9
         assert abs(r / fx["ali_relchange"][0, it] - 1.0) < 1e-9
+
+
+def test_ali_restatement_matches_reference_iterations_spec():
+    """As above at the stated settings (10 ray directions, 100 depths).  The fixture stores the
+    background opacity / emissivity in float32 (~6e-8 relative), hence the looser bound."""
+    import ali_oracle as ao
+    fx = _spec_fixture()
+    P = ao.Problem(fx)
+    p = fx["ali_pop0"][0].copy()
+    for it in range(2):
+        p, r, neg = ao.iterate(P, fx, 0, p)
+        assert not neg
+        assert np.abs(p / fx["ali_pops_iter"][0, it] - 1.0).max() < 1e-6
+        assert abs(r / fx["ali_relchange"][0, it] - 1.0) < 1e-5
 
 
 def test_psf_restatement_matches_reference():
