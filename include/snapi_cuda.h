@@ -469,8 +469,9 @@ int snapi_last_launches(const snapi_ctx *ctx);
  * the reference (its loops have no launch shapes).  The shapes it chooses between compute the same
  * bits (they change which thread or CTA handles a wavelength or a pixel, never the order of a sum):
  *   the adjoint: 32, 64 or 128 wavelengths per sweep CTA (the padding of the wavelength grid to the
- *     CTA width, e.g. 201 -> 224 / 256 / 256, against the CTA's staging cost), and 8, 16 or 32
- *     pixels per opacity-adjoint tile (L2 reuse of a tile's adjoint bars across its transitions);
+ *     CTA width, e.g. 201 -> 224 / 256 / 256, against the CTA's staging cost), 8, 16 or 32 pixels
+ *     per opacity-adjoint tile (L2 reuse of a tile's adjoint bars across its transitions), and the
+ *     reverse DELO sweep's register budget (unbounded, or 128 for more resident warps);
  *   the node build: 32, 64 or 128 threads per hydrostatic-march CTA, 64, 128 or 256 per
  *     record-chemistry CTA.
  * mode 1: the first snapi_adjoint / snapi_adjoint_nodes call with device buffers (SNAPI_MEM_DEVICE;
@@ -482,8 +483,8 @@ int snapi_last_launches(const snapi_ctx *ctx);
  * the trials.  mode 0 (the default): the compiled shapes (64 wavelengths, 16-pixel tiles, 64 and 64
  * threads).  Switching the mode forgets earlier choices. */
 int snapi_autotune(snapi_ctx *ctx, int mode, const char *cache_path);
-/* The shapes in use for a batch of npix pixels: cfg[4] = {wavelengths per sweep CTA, pixels per
- * opacity tile, march CTA threads, record-chemistry CTA threads}.  Returns a bit set: 1 the adjoint
+/* The shapes in use for a batch of npix pixels: cfg[5] = {wavelengths per sweep CTA, pixels per
+ * opacity tile, march CTA threads, record-chemistry CTA threads, reverse sweep at 128 registers}.  Returns a bit set: 1 the adjoint
  * shapes were tuned, 2 the build's were (0: the compiled defaults). */
 int snapi_tuned_config(const snapi_ctx *ctx, int npix, int *cfg);
 

@@ -556,9 +556,9 @@ class Context:
 
     def tuned_config(self, npix):
         """(shapes dict, tuned bits) of snapi_tuned_config for a batch of npix pixels."""
-        cfg = np.zeros(4, np.int32)
+        cfg = np.zeros(5, np.int32)
         bits = lib().snapi_tuned_config(self._ctx, int(npix), _ptr(cfg))
-        keys = ("chunk", "optile", "he_threads", "var_threads")
+        keys = ("chunk", "optile", "he_threads", "var_threads", "rt128")
         return {k: int(v) for k, v in zip(keys, cfg)}, int(bits)
 
     def eos_chem_start(self, mode):

@@ -125,8 +125,10 @@ __global__ void __launch_bounds__(C, SNAPI_SYN_MINB * kChunk / C) k_adj_forward(
 
 // Adjoint, phase R1: reverse DELO sweep and optical-depth adjoint per wavelength (no opacity
 // work, no shared memory); writes (eta-bar, j-bar) of every depth.
-template <int C>
-__global__ void __launch_bounds__(C, SNAPI_RT_MINB) k_adj_rt(KParams P) {
+// R128: a register budget of 128 per thread (16 warps per SM; ~20 bytes of spills) instead of the
+// unbounded one (158 registers, 12 warps per SM); the autotuner picks
+template <int C, bool R128>
+__global__ void __launch_bounds__(C, R128 ? 512 / C : SNAPI_RT_MINB) k_adj_rt(KParams P) {
   const CtaPos c = cta_pos<C>(P);
   if (c.warp0 >= P.nl) return;
   PixelView pv;
@@ -377,13 +379,16 @@ void launch_adjoint(const KParams &P0, int nb, const AdjCfg &cfg, size_t smem_sw
   const int nsw = nb * P.nchunk;
   if (cfg.chunk == 32) {
     k_adj_forward<32><<<nsw, 32, smem_sweep, st>>>(P);
-    k_adj_rt<32><<<nsw, 32, 0, st>>>(P);
+    if (cfg.rt128) k_adj_rt<32, true><<<nsw, 32, 0, st>>>(P);
+    else k_adj_rt<32, false><<<nsw, 32, 0, st>>>(P);
   } else if (cfg.chunk == 128) {
     k_adj_forward<128><<<nsw, 128, smem_sweep, st>>>(P);
-    k_adj_rt<128><<<nsw, 128, 0, st>>>(P);
+    if (cfg.rt128) k_adj_rt<128, true><<<nsw, 128, 0, st>>>(P);
+    else k_adj_rt<128, false><<<nsw, 128, 0, st>>>(P);
   } else {
     k_adj_forward<64><<<nsw, 64, smem_sweep, st>>>(P);
-    k_adj_rt<64><<<nsw, 64, 0, st>>>(P);
+    if (cfg.rt128) k_adj_rt<64, true><<<nsw, 64, 0, st>>>(P);
+    else k_adj_rt<64, false><<<nsw, 64, 0, st>>>(P);
   }
   const int nthr = std::min(kOpThreads, (P.nd * P.nslice + 31) / 32 * 32);
   const int ntile = (nb + P.optile - 1) / P.optile;
@@ -393,9 +398,9 @@ void launch_adjoint(const KParams &P0, int nb, const AdjCfg &cfg, size_t smem_sw
 
 // The autotuner's choice for an adjoint of nb pixels: each launch shape is run once on the call's
 // own inputs (all shapes compute the same bits), timed by CUDA events; first the chunk width at
-// the default tile, then the tile at the best width.
+// the default tile, then the tile at the best width, then the reverse sweep's register budget.
 AdjCfg tune_adjoint(snapi_ctx *ctx, const KParams &P, int nb, size_t smem_sweep, size_t smem_fin) {
-  AdjCfg best{kChunk, kOpTile};
+  AdjCfg best{kChunk, kOpTile, 0};
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess) return best;
   if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return best; }
@@ -409,10 +414,11 @@ AdjCfg tune_adjoint(snapi_ctx *ctx, const KParams &P, int nb, size_t smem_sweep,
     if (ms > 0.f && (best_ms < 0.f || ms < best_ms)) { best_ms = ms; best = c; }
   };
   for (int ch : kChunkCands)
-    if ((ctx->nl + ch - 1) / ch * ch <= ctx->lpad_max) trial(AdjCfg{ch, kOpTile});
+    if ((ctx->nl + ch - 1) / ch * ch <= ctx->lpad_max) trial(AdjCfg{ch, kOpTile, 0});
   const int bc = best.chunk;
   for (int t : kOpTileCands)
-    if (t != kOpTile) trial(AdjCfg{bc, t});
+    if (t != kOpTile) trial(AdjCfg{bc, t, 0});
+  trial(AdjCfg{best.chunk, best.optile, 1});
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return best;
@@ -475,7 +481,7 @@ static void tune_append(const snapi_ctx *ctx, const char *line) {
 void tune_store_adj(snapi_ctx *ctx, int npix, const AdjCfg &cfg) {
   ctx->adj_tuned.emplace_back(tune_bucket(npix), cfg);
   char b[96];
-  snprintf(b, sizeof b, "adj|%d|%d|%d", tune_bucket(npix), cfg.chunk, cfg.optile);
+  snprintf(b, sizeof b, "adj|%d|%d|%d|%d", tune_bucket(npix), cfg.chunk, cfg.optile, cfg.rt128);
   tune_append(ctx, b);
 }
 
@@ -496,10 +502,11 @@ static void tune_load(snapi_ctx *ctx) {
   auto member = [](const int *cands, int v) { return v == cands[0] || v == cands[1] || v == cands[2]; };
   while (fgets(line, sizeof line, f)) {
     if (strncmp(line, key.c_str(), key.size()) != 0) continue;
-    int b = 0, x = 0, y = 0;
+    int b = 0, x = 0, y = 0, z = 0;
     const char *rest = line + key.size();
-    if (sscanf(rest, "adj|%d|%d|%d", &b, &x, &y) == 3 && member(kChunkCands, x) && member(kOpTileCands, y)) {
-      ctx->adj_tuned.insert(ctx->adj_tuned.begin(), {b, AdjCfg{x, y}});
+    if (sscanf(rest, "adj|%d|%d|%d|%d", &b, &x, &y, &z) == 4 && member(kChunkCands, x) &&
+        member(kOpTileCands, y) && (z == 0 || z == 1)) {
+      ctx->adj_tuned.insert(ctx->adj_tuned.begin(), {b, AdjCfg{x, y, z}});
     } else if (sscanf(rest, "build|%d|%d|%d", &b, &x, &y) == 3 && member(kHeCands, x) && member(kVarCands, y)) {
       ctx->build_tuned.insert(ctx->build_tuned.begin(), {b, BuildCfg{x, y}});
     }
@@ -653,13 +660,14 @@ int snapi_autotune(snapi_ctx *ctx, int mode, const char *cache_path) {
 
 int snapi_tuned_config(const snapi_ctx *ctx, int npix, int *cfg) {
   if (!ctx || !cfg) return SNAPI_EINVAL;
-  AdjCfg a{kChunk, kOpTile};
+  AdjCfg a{kChunk, kOpTile, 0};
   BuildCfg b{kHeDefault, kVarDefault};
   const bool ha = ctx->tune && tuned_adj(ctx, npix, &a), hb = ctx->tune && tuned_build(ctx, npix, &b);
   cfg[0] = a.chunk;
   cfg[1] = a.optile;
   cfg[2] = b.he;
   cfg[3] = b.var;
+  cfg[4] = a.rt128;
   return (ha ? 1 : 0) | (hb ? 2 : 0);
 }
 
@@ -939,7 +947,7 @@ int adjoint_impl(snapi_ctx *ctx, int npix, const float *records, const float *ob
       P.chi2 = dev ? chi2 + p0 : ctx->d_chi2 + lo;
       P.grad = npar ? (dev ? grad + (size_t)p0 * npar : ctx->d_grad + (size_t)lo * npar) : ctx->d_grad;
       P.rec_grad = rec_grad ? (dev ? rec_grad + (size_t)p0 * nrec : ctx->d_recgrad + (size_t)lo * nrec) : nullptr;
-      AdjCfg cfg{kChunk, kOpTile};
+      AdjCfg cfg{kChunk, kOpTile, 0};
       if (ctx->tune && !tuned_adj(ctx, nr, &cfg) && dev && ci == 0) {
         cfg = tune_adjoint(ctx, P, nb, Lsw.total, Lfin.total);
         tune_store_adj(ctx, nr, cfg);
@@ -1292,7 +1300,7 @@ int noalloc_run(const snapi_problem *prob, void *stream_v, int npix, const float
     P.stokes = stokes ? stokes + (size_t)p0 * nl * 4 : nullptr;
     P.chi2 = chi2 + p0;
     P.grad = npar ? grad + (size_t)p0 * npar : nullptr;
-    launch_adjoint(P, nb, AdjCfg{kChunk, kOpTile}, Lsw.total, Lfin.total, stream);
+    launch_adjoint(P, nb, AdjCfg{kChunk, kOpTile, 0}, Lsw.total, Lfin.total, stream);
     CKN(cudaGetLastError());
   }
   int st = 0;

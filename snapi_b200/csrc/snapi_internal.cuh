@@ -52,6 +52,7 @@ constexpr int kVarCands[3] = {64, 128, 256};    // threads per record-chemistry 
 constexpr int kHeDefault = 64, kVarDefault = 64;  // the chemistry kernels' compiled CTA sizes
 struct AdjCfg {
   int chunk, optile;
+  int rt128;  // the reverse DELO sweep at 128 registers per thread
 };
 struct BuildCfg {
   int he, var;

@@ -62,7 +62,7 @@ def test_tuned_adjoint_bitwise_equal_and_cached(sb, config3, tmp_path):
     assert bits & 1 and cfg["chunk"] in (32, 64, 128) and cfg["optile"] in (8, 16, 32)
     ctx.close()
     lines = cache.read_text().splitlines()
-    assert any("|adj|64|%d|%d" % (cfg["chunk"], cfg["optile"]) in ln for ln in lines)
+    assert any("|adj|64|%d|%d|%d" % (cfg["chunk"], cfg["optile"], cfg["rt128"]) in ln for ln in lines)
     # a new context with the same cache knows the choice before any call
     ctx2 = _ctx(sb, fx)
     ctx2.autotune(True, cache)
@@ -74,8 +74,8 @@ def test_tuned_adjoint_bitwise_equal_and_cached(sb, config3, tmp_path):
     ctx2.close()
 
 
-@pytest.mark.parametrize("chunk,optile", [(32, 8), (128, 32)])
-def test_every_adjoint_shape_bitwise_equal(sb, config3, tmp_path, chunk, optile):
+@pytest.mark.parametrize("chunk,optile,rt128", [(32, 8, 1), (128, 32, 0), (64, 16, 1)])
+def test_every_adjoint_shape_bitwise_equal(sb, config3, tmp_path, chunk, optile, rt128):
     """Each candidate shape, forced through the cache file, gives the compiled shape's bits (the
     tuner may pick any of them)."""
     fx = config3
@@ -90,7 +90,7 @@ def test_every_adjoint_shape_bitwise_equal(sb, config3, tmp_path, chunk, optile)
     _device_adjoint(ctx, rec, obs, tan)  # writes this shape's key
     key = key_probe.read_text().splitlines()[0].split("|adj|")[0]
     forced = tmp_path / "forced.txt"
-    forced.write_text("%s|adj|64|%d|%d\n" % (key, chunk, optile))
+    forced.write_text("%s|adj|64|%d|%d|%d\n" % (key, chunk, optile, rt128))
     ctx.autotune(True, forced)
     assert ctx.tuned_config(24)[0]["chunk"] == chunk
     got = _device_adjoint(ctx, rec, obs, tan)
