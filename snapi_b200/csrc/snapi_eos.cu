@@ -291,13 +291,13 @@ struct Chem {
     if (warm && have) {
       const double sc = Nt / Nt_prev;
       for (int a = 0; a <= E.natom; ++a) N[a] *= sc;
-      if (newton(Nt, kWarmPasses) == 1) {
+      if (newton(Nt, kWarmPasses, true) == 1) {
         Nt_prev = Nt;
         return;
       }
     }
     cold_start(Nt);
-    if (newton(Nt, 50) != 1) capped = 1;
+    if (newton(Nt, 50, false) != 1) capped = 1;
     have = 1;
     Nt_prev = Nt;
   }
@@ -332,7 +332,9 @@ struct Chem {
 
   // Newton passes (atmos_chm.cc:176-305) from N, at most maxpass: 1 converged, 0 the pass cap was
   // reached (the reference stops there: iter > 100 counting two per pass), -1 a non-finite state
-  __device__ int newton(double Nt, int maxpass) {
+  // (only with bail: the continued start then falls back to the cold one; the cold path iterates
+  // on as the reference does)
+  __device__ int newton(double Nt, int maxpass, bool bail) {
     const int na = E.natom, nm = E.nmol, n = na + 1;
     int iter = 0;
     bool conv;
@@ -430,7 +432,7 @@ struct Chem {
         if (N[a] < 1E-2) N[a] = 1E-2;
         finite &= isfinite(N[a]);
       }
-      if (!finite) return -1;
+      if (bail && !finite) return -1;
       iter += 2;  // the reference counts two per pass (atmos_chm.cc:294, 300)
       if (iter > 2 * maxpass) return 0;
       conv = true;
