@@ -178,6 +178,29 @@ def config2_nodes(npix, seed=2):
     return nodes
 
 
+def config2_subset(seed=22):
+    """Indices of config 2's parity subset in its 256 x 256 cube (row-major pixel index): the 4 x 4
+    pixels at each corner (64) and a seeded 1 % random sample of the rest (655), sorted."""
+    corners = [y * 256 + x for y in (0, 1, 2, 3, 252, 253, 254, 255) for x in (0, 1, 2, 3, 252, 253, 254, 255)]
+    rest = np.setdiff1d(np.arange(256 * 256), corners)
+    pick = np.random.default_rng(seed).choice(rest, size=655, replace=False)
+    return np.sort(np.concatenate([np.array(corners), pick]))
+
+
+def make_config2_subset(tmp):
+    """The reference's synthesis of config 2's parity subset (config2_subset) of the seeded cube
+    (config2_nodes over all 65 536 pixels): records as float32 (what the device takes) and the
+    reference's Stokes (float64), in config2_720.npz."""
+    write_cfg(os.path.join(tmp, "c1.cfg"), LOGTAU, config1_temperature(LOGTAU), [0.0], [0.0])
+    run([DUMP, "pack", "c1.cfg", "c1.tsk"], tmp)
+    idx = config2_subset()
+    nodes = config2_nodes(256 * 256)[idx]
+    d = dump(tmp, os.path.join(tmp, "c1.tsk"), nodes, 0, "c2s")
+    np.savez_compressed(os.path.join(HERE, "config2_720.npz"), lambda_air=d["lambda_air"], tau500=d["tau500"],
+                        pixel_index=idx, record=d["record"].astype(np.float32), stokes=d["stokes"], nodes=d["nodes"],
+                        meta=d["meta"], **line_arrays(d))
+
+
 C3_TTAU = np.array([-4.0, -2.5, -1.0, 0.5])
 C3_VSTAU = np.array([-2.0, 0.0])
 C3_TRUTH = np.array([4600.0, 4900.0, 5500.0, 7400.0, 1.0e5, 0.0, 0.0, 800.0, np.deg2rad(60.0), np.deg2rad(40.0)])
@@ -357,6 +380,8 @@ def main():
                     help="config-4 fit of N pixels by the reference (8 processes at a time)")
     ap.add_argument("--c5col", type=int, default=3)
     ap.add_argument("--workers", type=int, default=8, help="reference processes at a time (config-4 subset)")
+    ap.add_argument("--only-c2-subset", action="store_true",
+                    help="config 2's parity subset (64 corner pixels + 1 %% of its 256 x 256 cube)")
     a = ap.parse_args()
     if not os.path.exists(DUMP):
         raise SystemExit("build the oracle first: make -C oracle")
@@ -366,6 +391,9 @@ def main():
             shutil.copy(os.path.join(a.ref, "cfg", f), tmp)
         if a.only_eos:
             make_eos(tmp)
+            return
+        if a.only_c2_subset:
+            make_config2_subset(tmp)
             return
         if a.only_f0:
             make_f0(tmp, a.ref)

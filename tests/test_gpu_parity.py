@@ -28,7 +28,7 @@ def _ctx(sb, fx, **kw):
     return sb.Context.from_fixture(fx, **kw)
 
 
-@pytest.mark.parametrize("cfg", ["config1", "config2", "config3", "config5", "config5_spec"])
+@pytest.mark.parametrize("cfg", ["config1", "config2", "config2_720", "config3", "config5", "config5_spec"])
 def test_synth_matches_oracle(sb, oracle_lib, cfg):
     import os
     from conftest import GOLDEN, load_fixture
