@@ -176,6 +176,13 @@ int snapi_lm_begin(snapi_ctx *ctx, int npix, const snapi_lm_opts *opts, const do
  * request, active [npix] and *n_active are updated. */
 int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, double *request, int *active,
                   int *n_active, int mem);
+/* snapi_lm_step with the caller's Jacobian instead of record tangents: jacobian [npix][npar][nlambda]
+ * [4] (float, unscaled dS/dnode at the requested nodes, in the node order and units of
+ * snapi_responses) -- e.g. the reference's own semi-analytic responses (obs_stokes_responses_to_nodes,
+ * atmos_fit.cc:1205-1352), as its stokes_lm_fit uses them (atmos_fit.cc:100-133).  Rows of pixels
+ * whose step is rejected keep the previous Jacobian, as the reference's do. */
+int snapi_lm_step_jacobian(snapi_ctx *ctx, const float *records, const float *jacobian, double *request,
+                           int *active, int *n_active, int mem);
 /* fitted nodes [npix][npar], chi2 [npix], iterations [npix] and Stokes [npix][nlambda][4]
  * (any may be NULL). */
 int snapi_lm_result(snapi_ctx *ctx, double *nodes, double *chi2, int *iters, float *stokes, int mem);

@@ -159,6 +159,7 @@ def lib():
         L.snapi_eos_chem_start.argtypes = [vp, ip]
         L.snapi_adjoint_nodes.argtypes = [vp, ip, fp, fp, fp, fp, fp, fp, fp, fp, ip]
         L.snapi_fma_peak.argtypes = [ip, ip, ctypes.POINTER(ctypes.c_double)]
+        L.snapi_lm_step_jacobian.argtypes = [vp, fp, fp, fp, fp, ctypes.POINTER(ctypes.c_int), ip]
         L.snapi_last_phase_ms.restype = ctypes.c_double
         L.snapi_last_phase_ms.argtypes = [vp, ip]
         L.snapi_autotune.argtypes = [vp, ip, ctypes.c_char_p]
@@ -443,16 +444,17 @@ class Context:
         self._lm_shape = (npix, npar)
         return req
 
-    def lm_step(self, records, tangents):
+    def lm_step(self, records, tangents, jacobian=False):
         """One LM iteration for every active pixel, from the records / tangents of the node vectors
-        the previous call requested.  Returns (request, active, n_active)."""
+        the previous call requested (jacobian: `tangents` is instead the caller's dS/dnode
+        [npix, npar, nlambda, 4], snapi_lm_step_jacobian).  Returns (request, active, n_active)."""
         rec = _f32(records)
         tn = _f32(tangents)
         req = np.zeros(self._lm_shape)
         act = np.zeros(self._lm_shape[0], np.int32)
         na = ctypes.c_int(0)
-        self._check(lib().snapi_lm_step(self._ctx, _ptr(rec), _ptr(tn), _ptr(req), _ptr(act), ctypes.byref(na),
-                                        MEM_HOST))
+        fn = lib().snapi_lm_step_jacobian if jacobian else lib().snapi_lm_step
+        self._check(fn(self._ctx, _ptr(rec), _ptr(tn), _ptr(req), _ptr(act), ctypes.byref(na), MEM_HOST))
         return req, act.astype(bool), na.value
 
     def lm_result(self):
@@ -519,15 +521,19 @@ class Context:
         return {"chi2": chi2.reshape(nx, ny), "iters": iters.reshape(nx, ny),
                 "stats": {k: getattr(stats, k) for k, _ in CubeStats._fields_}}
 
-    def lm_fit(self, nodes0, obs, builder, node_kind, resp_step, **kw):
+    def lm_fit(self, nodes0, obs, builder, node_kind, resp_step, jacobian=False, trace=None, **kw):
         """Run the fit to the end.  builder(nodes [n, npar], active [n] bool) returns (records,
-        tangents) for all n rows (rows of inactive pixels may hold anything)."""
+        tangents) for all n rows (rows of inactive pixels may hold anything); with jacobian, (records,
+        dS/dnode [n, npar, nlambda, 4]).  trace: optional list that receives every requested node
+        array (the first is the bracketed start, then one trial per LM iteration)."""
         req = self.lm_begin(nodes0, obs, node_kind, resp_step, **kw)
         active = np.ones(req.shape[0], bool)
         steps = 0
         while True:
+            if trace is not None:
+                trace.append(req.copy())
             rec, tan = builder(req, active)
-            req, active, n = self.lm_step(rec, tan)
+            req, active, n = self.lm_step(rec, tan, jacobian=jacobian)
             steps += 1
             if n == 0:
                 break

@@ -324,18 +324,37 @@ cudaError_t lm_eval_phase(snapi_ctx *ctx, LmWork *w, const float *rec) {
 }
 
 // 2) Jacobian at the accepted nodes along the tangents, normal equations, damped solve, next request
-cudaError_t lm_solve_phase(snapi_ctx *ctx, LmWork *w, const float *rec, const float *tan, int &launches) {
+// the caller's Jacobian rows into J where the step renews them (skip[p] == 0)
+__global__ void k_lm_copy_jac(const float *src, float *J, const int *skip, size_t row) {
+  const int p = blockIdx.x;
+  if (skip && skip[p]) return;
+  const float *s = src + (size_t)p * row;
+  float *d = J + (size_t)p * row;
+  for (size_t i = threadIdx.x; i < row; i += blockDim.x) d[i] = s[i];
+}
+
+// jac (may be null): the caller's Jacobian dS/dnode [npix][npar][nl][4] (device), used instead of
+// the responses along the record tangents
+cudaError_t lm_solve_phase(snapi_ctx *ctx, LmWork *w, const float *rec, const float *tan, int &launches,
+                           const float *jac = nullptr) {
   const int npix = w->npix, npar = w->npar;
-  KParams R = base_params(ctx);
-  R.npix = npix;
-  R.npar = npar;
-  R.nvar = npar;
-  R.rec = rec;
-  R.tangent = tan;
-  R.fd_step = w->d_step;
-  R.dstokes = w->d_J;
-  R.skip = w->d_skip_resp;
-  cudaError_t e = launch_responses(ctx, R);
+  cudaError_t e = cudaSuccess;
+  if (jac) {  // rows of pixels whose Jacobian is renewed this step (accepted or new); the others keep theirs
+    const size_t row = (size_t)npar * ctx->nl * 4;
+    k_lm_copy_jac<<<npix, 256, 0, ctx->stream>>>(jac, w->d_J, w->d_skip_resp, row);
+    e = cudaGetLastError();
+  } else {
+    KParams R = base_params(ctx);
+    R.npix = npix;
+    R.npar = npar;
+    R.nvar = npar;
+    R.rec = rec;
+    R.tangent = tan;
+    R.fd_step = w->d_step;
+    R.dstokes = w->d_J;
+    R.skip = w->d_skip_resp;
+    e = launch_responses(ctx, R);
+  }
   if (e != cudaSuccess) return e;
   if (w->broaden > 0.0 && (e = psf_launch(ctx, w->d_J, npix * npar, npar, w->d_skip_resp)) != cudaSuccess) return e;
   LmDev Ds = w->D;
@@ -401,7 +420,8 @@ int snapi_lm_begin(snapi_ctx *ctx, int npix, const snapi_lm_opts *opts, const do
       SNAPI_CK(cudaMalloc(&w->d_G, sizeof(float) * npix * 256));
     }
     SNAPI_CK(cudaMalloc(&w->d_rec, sizeof(float) * npix * nrec));
-    SNAPI_CK(cudaMalloc(&w->d_tan, sizeof(float) * npix * npar * nrec));
+    // record tangents, or the staging of a caller's Jacobian (snapi_lm_step_jacobian)
+    SNAPI_CK(cudaMalloc(&w->d_tan, sizeof(float) * npix * npar * std::max<size_t>(nrec, (size_t)nl * 4)));
     SNAPI_CK(cudaMalloc(&w->d_skip_syn, sizeof(int) * npix));
     SNAPI_CK(cudaMalloc(&w->d_skip_resp, sizeof(int) * npix));
     SNAPI_CK(cudaMalloc(&w->d_active, sizeof(int) * npix));
@@ -473,8 +493,10 @@ int snapi_lm_begin(snapi_ctx *ctx, int npix, const snapi_lm_opts *opts, const do
   return SNAPI_OK;
 }
 
-int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, double *request, int *active,
-                  int *n_active, int mem) {
+// snapi_lm_step (jac == false: `tangents` are record tangents) and snapi_lm_step_jacobian (jac:
+// `tangents` is the caller's Jacobian dS/dnode [npix][npar][nl][4])
+static int lm_step_impl(snapi_ctx *ctx, const float *records, const float *tangents, double *request, int *active,
+                        int *n_active, int mem, bool jac) {
   if (!ctx) return SNAPI_EINVAL;
   LmWork *w = work(ctx);
   if (!w || !w->begun) return set_err(ctx, SNAPI_EINVAL, "snapi_lm_step: call snapi_lm_begin first");
@@ -482,11 +504,13 @@ int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, d
     return set_err(ctx, SNAPI_EINVAL, "snapi_lm_step: invalid arguments");
   SNAPI_CK(cudaSetDevice(ctx->device));
   const int npix = w->npix, npar = w->npar;
-  const size_t nrec = (size_t)ctx->nd * ctx->nfield;
+  const size_t nrec = (size_t)ctx->nd * ctx->nfield, nrow = jac ? (size_t)ctx->nl * 4 * npar : nrec * npar;
   const bool dev = mem == SNAPI_MEM_DEVICE;
   const float *rec = records, *tan = tangents;
   if (!dev) {
-    // rows of inactive pixels are not needed: copy runs of active pixels only
+    // rows of inactive pixels are not needed: copy runs of active pixels only (a caller's Jacobian
+    // is staged in the tangent buffer, which is larger, and copied into J after the evaluation)
+    float *dst = w->d_tan;
     int p = 0;
     while (p < npix) {
       if (!w->h_active[p]) { ++p; continue; }
@@ -494,17 +518,17 @@ int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, d
       while (q < npix && w->h_active[q]) ++q;
       SNAPI_CK(cudaMemcpyAsync(w->d_rec + p * nrec, records + p * nrec, sizeof(float) * (q - p) * nrec,
                                cudaMemcpyHostToDevice, ctx->stream));
-      SNAPI_CK(cudaMemcpyAsync(w->d_tan + (size_t)p * npar * nrec, tangents + (size_t)p * npar * nrec,
-                               sizeof(float) * (size_t)(q - p) * npar * nrec, cudaMemcpyHostToDevice, ctx->stream));
+      SNAPI_CK(cudaMemcpyAsync(dst + (size_t)p * nrow, tangents + (size_t)p * nrow, sizeof(float) * (q - p) * nrow,
+                               cudaMemcpyHostToDevice, ctx->stream));
       p = q;
     }
     rec = w->d_rec;
-    tan = w->d_tan;
+    tan = dst;
   }
   SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
   SNAPI_CK(lm_eval_phase(ctx, w, rec));
   int nl_solve = 0;
-  SNAPI_CK(lm_solve_phase(ctx, w, rec, tan, nl_solve));
+  SNAPI_CK(lm_solve_phase(ctx, w, rec, jac ? nullptr : tan, nl_solve, jac ? tan : nullptr));
   SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
   ctx->last_launches = 2 + nl_solve;
   SNAPI_CK(cudaMemcpyAsync(w->h_active.data(), w->d_active, sizeof(int) * npix, cudaMemcpyDeviceToHost, ctx->stream));
@@ -524,6 +548,16 @@ int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, d
   if (!dev && active) memcpy(active, w->h_active.data(), sizeof(int) * npix);
   if (n_active) *n_active = na;
   return check_status(ctx);
+}
+
+int snapi_lm_step(snapi_ctx *ctx, const float *records, const float *tangents, double *request, int *active,
+                  int *n_active, int mem) {
+  return lm_step_impl(ctx, records, tangents, request, active, n_active, mem, false);
+}
+
+int snapi_lm_step_jacobian(snapi_ctx *ctx, const float *records, const float *jacobian, double *request,
+                           int *active, int *n_active, int mem) {
+  return lm_step_impl(ctx, records, jacobian, request, active, n_active, mem, true);
 }
 
 int snapi_lm_result(snapi_ctx *ctx, double *nodes, double *chi2, int *iters, float *stokes, int mem) {

@@ -243,6 +243,23 @@ def config4_inputs(npix, seed=4):
     return truth, truth + C4_OFFSET, mask
 
 
+def parse_trial_models(path, npar):
+    """The trial node vectors of the reference's LM loop, one per iteration, from the model prints
+    it writes to standard output (model::print, atmos_model.cc:712-760: one line 'i tau value' per
+    node, kinds in the node order; inclination and azimuth in degrees -> radians here)."""
+    vals = []
+    for ln in open(path):
+        f = ln.split()
+        if len(f) == 3 and f[0].isdigit():
+            try:
+                vals.append(float(f[2]))
+            except ValueError:
+                pass
+    a = np.array(vals[:len(vals) // npar * npar]).reshape(-1, npar)
+    a[:, -2:] = np.deg2rad(a[:, -2:])
+    return a
+
+
 def make_config4(tmp, npix, iters=30, broadening=0.0, name="config4", seed=4, workers=0, spec=False):
     """Reference LM (stokes_lm_fit, start lambda 1e3) on config-4 pixels, one process per pixel;
     with broadening > 0 [cm] the targets are broadened by the reference's own convolution and the
@@ -271,13 +288,23 @@ def make_config4(tmp, npix, iters=30, broadening=0.0, name="config4", seed=4, wo
         if workers and len(procs) >= workers:  # at most `workers` reference processes at a time
             if procs.pop(0).wait() != 0:
                 raise RuntimeError("lmfit failed")
-        procs.append(subprocess.Popen(args, cwd=tmp, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+        # the reference prints every trial model of its loop (test_model->print(), atmos_fit.cc:152)
+        out_f = open(os.path.join(tmp, "c4_trace_%d.txt" % i), "w")
+        procs.append(subprocess.Popen(args, cwd=tmp, stdout=out_f, stderr=subprocess.DEVNULL))
+        out_f.close()
     for p in procs:
         if p.wait() != 0:
             raise RuntimeError("lmfit failed")
     fits = [read_sbin(os.path.join(tmp, "c4_fit_%d.sbin" % i)) for i in range(npix)]
+    npar = nodes0.shape[1]
+    trials = [parse_trial_models(os.path.join(tmp, "c4_trace_%d.txt" % i), npar) for i in range(npix)]
+    trace = np.full((npix, iters, npar), np.nan)
+    for i, t in enumerate(trials):
+        trace[i, :t.shape[0]] = t[:iters]
     # the fitted Stokes only for the small fixtures (the 256-pixel one compares nodes and chi2)
     extra = {} if npix > 64 else {"fit_stokes": np.concatenate([f["fit_stokes"] for f in fits])}
+    if npix <= 64:
+        extra["trace_trial"] = trace
     np.savez_compressed(os.path.join(HERE, name + ".npz"), lambda_air=d["lambda_air"], tau500=d["tau500"],
                         broadening=np.array([broadening]), delta=np.array([delta]),
                         node_kind=d["node_kind"], truth=truth, nodes0=nodes0, mask=mask, target=target,

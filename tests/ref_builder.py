@@ -29,10 +29,14 @@ def ref_builder_available():
 
 
 class RefBuilder:
-    def __init__(self, task=TASK, nproc=None):
+    """responses: return the reference's own node responses (obs_stokes_responses_to_nodes, the
+    Jacobian its stokes_lm_fit uses) instead of the record tangents, for snapi_lm_step_jacobian."""
+
+    def __init__(self, task=TASK, nproc=None, responses=False):
         self.task = task
         self.nproc = nproc or os.cpu_count() or 1
         self.calls = 0
+        self.responses = responses
 
     def __call__(self, nodes, active):
         idx = np.flatnonzero(active)
@@ -45,18 +49,20 @@ class RefBuilder:
                 nf = os.path.join(tmp, "n%d.f64" % k)
                 out = os.path.join(tmp, "o%d.sbin" % k)
                 np.ascontiguousarray(nodes[chunk], dtype="<f8").tofile(nf)
-                p = subprocess.Popen([DUMP, "dump", self.task, nf, str(chunk.size), "2", out], cwd=tmp,
+                flags = "1" if self.responses else "2"
+                p = subprocess.Popen([DUMP, "dump", self.task, nf, str(chunk.size), flags, out], cwd=tmp,
                                      stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
                 jobs.append((chunk, out, p))
             for chunk, out, p in jobs:
                 if p.wait() != 0:
                     raise RuntimeError("snapi_ref_dump failed")
                 d = read_sbin(out)
+                key = "responses" if self.responses else "tangent"
                 if rec is None:
                     rec = np.zeros((nodes.shape[0],) + d["record"].shape[1:], np.float32)
-                    tan = np.zeros((nodes.shape[0],) + d["tangent"].shape[1:], np.float32)
+                    tan = np.zeros((nodes.shape[0],) + d[key].shape[1:], np.float32)
                 rec[chunk] = d["record"]
-                tan[chunk] = d["tangent"]
+                tan[chunk] = d[key]
         self.calls += 1
         return rec, tan
 

@@ -86,6 +86,37 @@ def test_lm_matches_reference_fit(sb, config4):
 
 
 @pytest.mark.skipif(not ref_builder_available(), reason="reference builder (oracle/_ref) not built")
+def test_lm_trajectory_with_reference_jacobian(sb, config4):
+    """The LM iteration itself against the reference's: with the reference's own responses as the
+    Jacobian (snapi_lm_step_jacobian, responses from obs_stokes_responses_to_nodes at every requested
+    node vector, as stokes_lm_fit takes them) the trial node vectors of the first three iterations
+    follow the reference's (its printed trial models, fixture trace_trial) to 1e-3 of each step,
+    LM-scaled: the same residual, J^T J, damping and 1e6 condition cut (eigen-decomposition here,
+    SVD there), the same bracketing; the remaining difference is the FP32 synthesis in the
+    residual."""
+    fx = config4
+    if "trace_trial" not in fx:
+        pytest.skip("fixture without the reference's trial models")
+    sel = np.arange(4)
+    ic = _ic(fx)
+    kinds = fx["node_kind"]
+    scale = node_scales(kinds)
+    ctx = sb.Context.from_fixture(fx, stokes_scale=ic)
+    trace = []
+    ctx.lm_fit(fx["nodes0"][sel], fx["target"][sel], RefBuilder(responses=True), kinds, 1e-2 * scale,
+               jacobian=True, trace=trace, mask=fx["mask"][sel], lm_start=1e3, max_iter=4, delta=_delta(fx))
+    ctx.close()
+    ref = fx["trace_trial"][sel]
+    for k in range(1, 4):  # trace[0] is the bracketed start, trace[k] the k-th trial
+        cur = trace[k - 1] if k == 1 else ref[:, k - 2]  # every early step is accepted by both
+        step_ref = (ref[:, k - 1] - cur) / scale
+        err = (trace[k] - ref[:, k - 1]) / scale
+        rel = np.linalg.norm(err, axis=1) / np.linalg.norm(step_ref, axis=1)
+        print("iteration", k, "trial-node difference / step:", rel)
+        assert np.all(rel < 1e-3), (k, rel)
+
+
+@pytest.mark.skipif(not ref_builder_available(), reason="reference builder (oracle/_ref) not built")
 def test_lm_with_spectral_broadening_matches_reference(sb, config4_psf):
     """LM with the 45 mA Gaussian instrumental profile (synthesis and responses broadened as
     stokes_lm_fit does) against the reference's fit of the same pixels.  Only pixels 0 and 1: the
