@@ -48,6 +48,23 @@ def test_stokes_config3(oracle_lib, config3):
     assert _stokes_err(oracle_lib, config3) < 1e-12
 
 
+def test_stokes_config2_subset(oracle_lib):
+    """Config 2's parity subset (64 corner pixels + 1 % of the seeded 256 x 256 cube): the oracle on
+    12 of its pixels against the reference's Stokes.  The fixture stores the records in float32
+    (what the device takes), so the bound is that rounding's effect, not the FP64 restatement's."""
+    import os
+    from conftest import GOLDEN, load_fixture
+    if not os.path.exists(os.path.join(GOLDEN, "config2_720.npz")):
+        pytest.skip("fixture config2_720.npz not generated")
+    fx = load_fixture("config2_720")
+    assert fx["record"].shape[0] == 719 and np.all(np.diff(fx["pixel_index"]) > 0)
+    sel = np.linspace(0, 718, 12).astype(int)
+    lines = oracle_lib.lines_from_arrays(fx["line_const"], fx["line_ncomp"], fx["line_pattern"])
+    st = oracle_lib.synth(fx["lambda_air"], fx["tau500"], fx["record"][sel].astype(np.float64), lines)
+    ic = fx["stokes"][sel][:, :, 0].max(axis=1)[:, None, None]
+    assert (np.abs(st - fx["stokes"][sel]) / ic).max() < 1e-6
+
+
 def test_stokes_config5_nlte_ca(oracle_lib, config5):
     """Ca II 8542 window with the reference's NLTE populations in the record (10 transitions:
     Ca II H, K and the infrared triplet, the hydrogen far wings, Fe I 6301/6302)."""
