@@ -126,6 +126,20 @@ int snapi_adjoint_packed(snapi_ctx *ctx, int npix, const float *records, const f
 int snapi_responses(snapi_ctx *ctx, int npix, const float *records, int npar, const float *tangents,
                     const double *step, float *stokes, float *dstokes, int mem);
 
+/* How snapi_responses and the LM (snapi_lm_step, snapi_lm_fit) form dS/dnode.
+ *   SNAPI_JACOBIAN_FD (default): central differences of the record along each node tangent, steps
+ *     in node units (2 npar forward solves).
+ *   SNAPI_JACOBIAN_TANGENT: forward mode -- the exact derivative of the FP32 synthesis along each
+ *     node tangent, carried through the opacity (W4 with its x / a derivatives), the Bezier
+ *     optical depth and the DELO recursion, as the reference carries its semi-analytic
+ *     derivatives through formal_with_responses_full (atmos_ppbez_rts.cc:1223-1704); steps are not
+ *     used.  One forward pass storing the state, then one sweep per node in which the W4
+ *     evaluations are shared among the nodes.
+ * The setting lasts for the context. */
+#define SNAPI_JACOBIAN_FD 0
+#define SNAPI_JACOBIAN_TANGENT 1
+int snapi_jacobian_mode(snapi_ctx *ctx, int mode);
+
 /* Plain finite-difference gradient (the baseline the adjoint replaces): for each node p the
  * records are perturbed by +-step[p] * tangent_p and synthesised again (2 npar + 1 solves).
  * step [npar] in node units. */

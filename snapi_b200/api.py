@@ -20,6 +20,7 @@ LIB_PATH = os.environ.get("SNAPI_LIB", os.path.join(_PKG, "libsnapi_cuda.so"))
 OK, EINVAL, ECUDA, ETIMEOUT, ENONCONV, ENOMEM = 0, -1, -2, -3, -4, -5
 MEM_HOST, MEM_DEVICE = 0, 1
 CHEM_START_CONTINUE, CHEM_START_COLD = 0, 1  # SNAPI_CHEM_START_*
+JACOBIAN_FD, JACOBIAN_TANGENT = 0, 1  # SNAPI_JACOBIAN_*
 NFIELD0 = 12
 MAX_LINES = 16  # SNAPI_MAX_LINES
 MAX_COMP = 16
@@ -163,6 +164,7 @@ def lib():
         L.snapi_last_phase_ms.restype = ctypes.c_double
         L.snapi_last_phase_ms.argtypes = [vp, ip]
         L.snapi_autotune.argtypes = [vp, ip, ctypes.c_char_p]
+        L.snapi_jacobian_mode.argtypes = [vp, ip]
         L.snapi_tuned_config.argtypes = [vp, ip, fp]
         L.snapi_build_records.argtypes = [vp, ip, fp, fp, fp, fp, fp, fp, fp, ip]
         L.snapi_build_atmos.argtypes = [vp, ip, fp, fp, fp, fp, fp, ip]
@@ -553,6 +555,11 @@ class Context:
         self._eos = tables  # keep the ctypes tables alive for the call
         self._check(lib().snapi_eos_set(self._ctx, ctypes.addressof(tables.model)))
         self._eos_npar = tables.npar
+
+    def jacobian_mode(self, mode):
+        """How responses and the LM Jacobian are formed: JACOBIAN_FD (central differences, default) or
+        JACOBIAN_TANGENT (forward-mode sweeps, exact derivative of the FP32 synthesis)."""
+        self._check(lib().snapi_jacobian_mode(self._ctx, int(mode)))
 
     def autotune(self, on=True, cache_path=None):
         """snapi_autotune: pick launch shapes by timing them on the first calls of each batch size

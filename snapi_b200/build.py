@@ -14,7 +14,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["snapi_cuda.cu", "snapi_lm.cu", "snapi_ali.cu", "snapi_tc.cu", "snapi_psf.cu", "snapi_eos.cu",
            "snapi_f0.cu", "snapi_cube.cu", "snapi_peak.cu"]
-HEADERS = ["snapi_core.cuh", "snapi_sweep.cuh", "snapi_internal.cuh", "snapi_f0_internal.h"]
+HEADERS = ["snapi_core.cuh", "snapi_sweep.cuh", "snapi_jvp.cuh", "snapi_internal.cuh", "snapi_f0_internal.h"]
 
 
 def _stale(target, deps):
@@ -57,7 +57,8 @@ def build_emulator():
     """CPU emulator of the kernels (test infrastructure)."""
     src = os.path.join(ROOT, "tests", "emu", "snapi_emu.cc")
     out = os.path.join(ROOT, "tests", "emu", "libsnapi_emu.so")
-    deps = [src, os.path.join(CSRC, "snapi_core.cuh"), os.path.join(CSRC, "snapi_sweep.cuh")]
+    deps = [src, os.path.join(CSRC, "snapi_core.cuh"), os.path.join(CSRC, "snapi_sweep.cuh"),
+            os.path.join(CSRC, "snapi_jvp.cuh")]
     if _stale(out, deps):
         subprocess.run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-o", out, src], check=True)
     return out

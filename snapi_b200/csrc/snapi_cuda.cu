@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "snapi_internal.cuh"
+#include "snapi_jvp.cuh"
 
 using namespace snapi;
 
@@ -330,6 +331,128 @@ __global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_resp_sweep(KParams P
   }
 }
 
+// ---- node responses by forward-mode sweeps (snapi_responses_jvp) ----------------------------------
+// Phase S: the forward sweep of every wavelength storing its per-depth state (I, K', S, eta_I, dtau)
+// in the adjoint's layout (kChunk wavelengths per CTA), and the Stokes vector.
+__global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_resp_state(KParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const SmemLayout L = smem_layout(P.nd, P.nfield, P.nlines, P.ncomp, P.nred, false);
+  const CtaPos c = cta_pos(P);
+  if (P.skip && P.skip[c.pix]) return;  // CTA-uniform
+  PixelView pv;
+  if (!stage_pixel(P, c.pix, smem, L, pv, -1, 0.f)) return;
+  if (c.warp0 >= P.nl) return;
+  const bool active = c.l < P.nl;
+  LamConst lam;
+  float delta[kMaxLines];
+  thread_lambda(P, pv, active ? c.l : P.nl - 1, lam, delta);
+  DevScratch sc;
+  sc.base = P.scratch + (size_t)c.pix * P.nd * 4 * P.lpad;
+  sc.lpad = P.lpad;
+  sc.l = c.l;
+  float out[4];
+  forward_sweep<true>(pv, lam, delta, out, sc);
+  if (active && P.stokes) {
+    float4 *o = reinterpret_cast<float4 *>(P.stokes + ((size_t)c.pix * P.nl + c.l) * 4);
+    *o = make_float4(out[0], out[1], out[2], out[3]);
+  }
+}
+
+// Phase T: CTA = (pixel, 32 wavelengths, up to kJvpDirs node directions); warp w carries direction
+// q0 + w, lane = wavelength.  At each depth the W4 evaluations with their x / a derivatives
+// (voigt_grad) of the CTA's 32 wavelengths are shared: every warp computes a share of them into
+// shared memory; then each warp forms its direction's opacity tangent from all of them and takes
+// the DELO / optical-depth tangent step, the forward values coming from phase S.  The depth
+// tangents of a direction (DepthTan, LineTan) are computed once per depth by the warp's lane 0.
+// Shared buffers are double-buffered by depth: one __syncthreads per depth.
+size_t jvp_smem_extra(int nw, int nwarp, int nlines) {
+  return sizeof(float) * (2 * 32 * (size_t)(nw * 6 + 1) + 2 * (size_t)nwarp * (12 + 5 * nlines));
+}
+
+__global__ void __launch_bounds__(32 * kJvpDirs) k_resp_jvp(KParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const SmemLayout L = smem_layout(P.nd, P.nfield, P.nlines, P.ncomp, P.nred, false);
+  const int nchk = (P.nl + 31) >> 5, ngrp = (P.npar + kJvpDirs - 1) / kJvpDirs;
+  int b = blockIdx.x;
+  const int chunk = b % nchk;
+  b /= nchk;
+  const int grp = b % ngrp, pix = b / ngrp;
+  const int nwarp = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = grp * kJvpDirs + warp;
+  const bool live = q < P.npar;  // warps past the last direction only help with the W4 share
+  if (P.skip && P.skip[pix]) return;  // CTA-uniform
+  PixelView pv;
+  if (!stage_pixel(P, pix, smem, L, pv, -1, 0.f)) return;
+  const int nd = P.nd, nw = w4_count(pv.lc, P.nlines), lstride = nw * 6 + 1, dtn = 12 + 5 * P.nlines;
+  float *W = reinterpret_cast<float *>(smem + L.total);  // [2][32][lstride]
+  float *DT = W + 2 * 32 * lstride;                       // [2][nwarp][dtn]
+  const int l = chunk * 32 + lane;
+  LamConst lam;
+  float delta[kMaxLines];
+  thread_lambda(P, pv, l < P.nl ? l : P.nl - 1, lam, delta);
+  const float *trec = P.tangent + ((size_t)pix * P.npar + (live ? q : 0)) * nd * P.nfield;
+  DevScratch st;
+  st.base = P.scratch + (size_t)pix * nd * 4 * P.lpad;
+  st.lpad = P.lpad;
+  st.l = l;
+  auto prepare = [&](int z, int buf) {
+    float *dt = DT + (buf * nwarp + warp) * dtn;
+    if (live && lane == 0)
+      depth_tangent(pv.rec + z * P.nfield, trec + z * P.nfield, P.nlines, pv.lc, P.lam_mid, pv.ld + z * P.nlines,
+                    *reinterpret_cast<DepthTan *>(dt), reinterpret_cast<LineTan *>(dt + 12));
+    float *wl = W + (buf * 32 + lane) * lstride;
+    for (int c = warp; c < nw; c += nwarp)
+      w4_eval(pv.dc[z], pv.ld + z * P.nlines, pv.lc, P.nlines, pv.compD, lam, delta, c, wl + 6 * c);
+  };
+  auto tangent = [&](int z, int buf, float *kp, float *S, float &e, float *dkp, float *dS, float &de) {
+    const float *dt = DT + (buf * nwarp + warp) * dtn;
+    const float *wl = W + (buf * 32 + lane) * lstride;
+    float deta[7], djj[4], I[4], tau;
+    cell_opacity_jvp(pv.dc[z], pv.ld + z * P.nlines, pv.lc, P.nlines, pv.compS, pv.compD, lam, delta, wl, 6,
+                     *reinterpret_cast<const DepthTan *>(dt), reinterpret_cast<const LineTan *>(dt + 12), deta, djj);
+    st.load(z, I, kp, S, e, tau);
+    depth_opacity_jvp(kp, S, e, deta, djj, dkp, dS, de);
+  };
+  float kA[6], SA[4], eA, dkA[6], dSA[4], deA, kB[6], SB[4], eB, dkB[6], dSB[4], deB;
+  float kC[6], SC[4], eC, dkC[6], dSC[4], deC;
+  prepare(nd - 1, 0);
+  __syncthreads();
+  if (live) tangent(nd - 1, 0, kA, SA, eA, dkA, dSA, deA);
+  prepare(nd - 2, 1);
+  __syncthreads();
+  if (live) tangent(nd - 2, 1, kB, SB, eB, dkB, dSB, deB);
+  float dI[4] = {live ? dSA[0] : 0.f, 0.f, 0.f, 0.f};
+  double dopd_below = live ? ((double)deB - (double)deA) / pv.D[nd - 2] : 0.0;
+  int buf = 0;
+  for (int z = nd - 2; z >= 1; --z) {
+    prepare(z - 1, buf);
+    __syncthreads();
+    if (live) {
+      tangent(z - 1, buf, kC, SC, eC, dkC, dSC, deC);
+      const double dopd_z = opd_interior_jvp(eA, eB, eC, pv.D[z], pv.D[z - 1], deA, deB, deC);
+      const float dtau = (float)bezier_dtau_jvp(deA, deB, dopd_below, dopd_z, pv.D[z]);
+      float Ip[4], Ic[4], k_[6], S_[4], e_, tau;
+      st.load(z + 1, Ip, k_, S_, e_, tau);
+      st.load(z, Ic, k_, S_, e_, tau);
+      float dIn[4];
+      delo_step_jvp(Ip, kA, SA, kB, SB, tau, Ic, dI, dkA, dSA, dkB, dSB, dtau, dIn);
+#pragma unroll
+      for (int s = 0; s < 4; ++s) dI[s] = dIn[s];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) { kA[k] = kB[k]; kB[k] = kC[k]; dkA[k] = dkB[k]; dkB[k] = dkC[k]; }
+#pragma unroll
+      for (int s = 0; s < 4; ++s) { SA[s] = SB[s]; SB[s] = SC[s]; dSA[s] = dSB[s]; dSB[s] = dSC[s]; }
+      eA = eB; eB = eC; deA = deB; deB = deC;
+      dopd_below = dopd_z;
+    }
+    buf ^= 1;
+  }
+  if (live && l < P.nl) {  // the top point copies the one below
+    float4 *o = reinterpret_cast<float4 *>(P.dstokes + (((size_t)pix * P.npar + q) * P.nl + l) * 4);
+    *o = make_float4(dI[0], dI[1], dI[2], dI[3]);
+  }
+}
+
 double airtovac_d(double lambda_air) {  // cmlib/mathtools.cc:1325-1330
   double s = 1E4 / (lambda_air * 1E8);
   double n = 1.0 + 0.00008336624212083 + 0.02408926869968 / (130.1065924522 - s * s) +
@@ -358,6 +481,29 @@ cudaError_t snapi::launch_synth(const snapi_ctx *ctx, const KParams &P) {
 }
 cudaError_t snapi::launch_responses(const snapi_ctx *ctx, const KParams &P) {
   const SmemLayout L = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false);
+  if (ctx->jac_tangent) {  // forward-mode sweeps (the state in the adjoint's scratch)
+    KParams Q = P;
+    Q.scratch = ctx->d_scratch;
+    Q.stokes = nullptr;
+    const int nwarp = std::min(P.npar, kJvpDirs), ngrp = (P.npar + kJvpDirs - 1) / kJvpDirs;
+    const size_t smem = L.total + jvp_smem_extra(ctx->nw4, nwarp, ctx->nlines);
+    const size_t nrec = (size_t)ctx->nd * ctx->nfield;
+    // in batches of max_batch pixels: the forward state lives in the adjoint's scratch
+    for (int p0 = 0; p0 < P.npix; p0 += ctx->max_batch) {
+      KParams R = Q;
+      R.npix = std::min(ctx->max_batch, P.npix - p0);
+      R.rec = P.rec + p0 * nrec;
+      R.tangent = P.tangent + (size_t)p0 * P.npar * nrec;
+      R.dstokes = P.dstokes + (size_t)p0 * P.npar * ctx->nl * 4;
+      R.skip = P.skip ? P.skip + p0 : nullptr;
+      k_resp_state<<<R.npix * ctx->nchunk, kChunk, L.total, ctx->stream>>>(R);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      k_resp_jvp<<<R.npix * ((ctx->nl + 31) / 32) * ngrp, 32 * nwarp, smem, ctx->stream>>>(R);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
   k_resp_sweep<<<P.npix * P.nvar * ctx->nchunk, kChunk, L.total, ctx->stream>>>(P);
   return cudaGetLastError();
 }
@@ -567,7 +713,7 @@ cudaError_t raise_smem_limits(int bytes) {
   const void *k[] = {(const void *)k_synth, (const void *)k_fd_sweep, (const void *)k_resp_sweep,
                      (const void *)k_adj_forward<32>, (const void *)k_adj_forward<64>,
                      (const void *)k_adj_forward<128>, (const void *)k_adj_opacity,
-                     (const void *)k_adjoint_finish};
+                     (const void *)k_adjoint_finish, (const void *)k_resp_state, (const void *)k_resp_jvp};
   for (const void *f : k) {
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
@@ -647,6 +793,22 @@ void snapi_host_free(void *p) {
 const char *snapi_last_error(const snapi_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 void *snapi_stream(snapi_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 double snapi_last_kernel_ms(const snapi_ctx *ctx) { return ctx ? ctx->last_ms : 0.0; }
+int snapi_jacobian_mode(snapi_ctx *ctx, int mode) {
+  if (!ctx) return SNAPI_EINVAL;
+  if (mode != SNAPI_JACOBIAN_FD && mode != SNAPI_JACOBIAN_TANGENT)
+    return set_err(ctx, SNAPI_EINVAL, "snapi_jacobian_mode: unknown mode %d", mode);
+  if (mode == SNAPI_JACOBIAN_TANGENT) {  // the state layout needs the compiled sweep width's padding
+    const size_t smem = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false).total +
+                        jvp_smem_extra(ctx->nw4, kJvpDirs, ctx->nlines);
+    int maxsm = 0;
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+    if ((int)smem > maxsm)
+      return set_err(ctx, SNAPI_EINVAL, "snapi_jacobian_mode: the problem needs %zu B of shared memory", smem);
+  }
+  ctx->jac_tangent = mode == SNAPI_JACOBIAN_TANGENT;
+  return SNAPI_OK;
+}
+
 int snapi_autotune(snapi_ctx *ctx, int mode, const char *cache_path) {
   if (!ctx) return SNAPI_EINVAL;
   if (mode != 0 && mode != 1) return set_err(ctx, SNAPI_EINVAL, "snapi_autotune: mode must be 0 or 1");
@@ -776,6 +938,7 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
     }
   }
   ctx->ncomp = (int)cS.size();
+  ctx->nw4 = w4_count(lc.data(), ctx->nlines);
   const SmemLayout Lsw = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false);
   const SmemLayout Lfin = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, true);
   int maxsm = 0;
@@ -1114,17 +1277,28 @@ int snapi_responses(snapi_ctx *ctx, int npix, const float *records, int npar, co
     P.dstokes = dev ? dstokes + (size_t)p0 * npar * ctx->nl * 4 : ctx->d_dstokes;
     P.stokes = stokes ? (dev ? stokes + (size_t)p0 * ctx->nl * 4 : ctx->d_stokes) : nullptr;
     SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    if (P.stokes) {
-      KParams Q = P;
-      Q.nvar = 1;
-      k_synth<<<sweep_ctas(ctx, nb), kChunk, L.total, ctx->stream>>>(Q);
+    if (ctx->jac_tangent) {  // forward-mode sweeps: the state pass also gives the Stokes vector
+      P.scratch = ctx->d_scratch;
+      k_resp_state<<<sweep_ctas(ctx, nb), kChunk, L.total, ctx->stream>>>(P);
+      SNAPI_CK(cudaGetLastError());
+      const int nwarp = std::min(npar, kJvpDirs), ngrp = (npar + kJvpDirs - 1) / kJvpDirs;
+      k_resp_jvp<<<nb * ((ctx->nl + 31) / 32) * ngrp, 32 * nwarp,
+                   L.total + jvp_smem_extra(ctx->nw4, nwarp, ctx->nlines), ctx->stream>>>(P);
+      SNAPI_CK(cudaGetLastError());
+      ctx->last_launches += 2;
+    } else {
+      if (P.stokes) {
+        KParams Q = P;
+        Q.nvar = 1;
+        k_synth<<<sweep_ctas(ctx, nb), kChunk, L.total, ctx->stream>>>(Q);
+        SNAPI_CK(cudaGetLastError());
+        ctx->last_launches += 1;
+      }
+      k_resp_sweep<<<sweep_ctas(ctx, nb, npar), kChunk, L.total, ctx->stream>>>(P);
       SNAPI_CK(cudaGetLastError());
       ctx->last_launches += 1;
     }
-    k_resp_sweep<<<sweep_ctas(ctx, nb, npar), kChunk, L.total, ctx->stream>>>(P);
-    SNAPI_CK(cudaGetLastError());
     SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    ctx->last_launches += 1;
     if (!dev) {
       if (stokes)
         SNAPI_CK(cudaMemcpyAsync(stokes + (size_t)p0 * ctx->nl * 4, ctx->d_stokes, sizeof(float) * nb * ctx->nl * 4,

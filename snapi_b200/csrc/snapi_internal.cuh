@@ -50,6 +50,7 @@ constexpr int kOpTileCands[3] = {8, 16, 32};    // pixels per opacity-adjoint CT
 constexpr int kHeCands[3] = {32, 64, 128};      // threads per hydrostatic-march CTA
 constexpr int kVarCands[3] = {64, 128, 256};    // threads per record-chemistry CTA
 constexpr int kHeDefault = 64, kVarDefault = 64;  // the chemistry kernels' compiled CTA sizes
+constexpr int kJvpDirs = 16;  // node directions (warps) per forward-mode responses CTA
 struct AdjCfg {
   int chunk, optile;
   int rt128;  // the reverse DELO sweep at 128 registers per thread
@@ -317,6 +318,8 @@ struct snapi_ctx {
   cudaEvent_t ev_copy[kStageChunks] = {}, ev_free = nullptr;  // chunk uploaded / round's kernels done
   int nd = 0, nl = 0, nlines = 0, nfield = 0, ncomp = 0, nred = 0, lpad = 0, nchunk = 0, nwslot = 0, max_batch = 0;
   int lpad_max = 0;  // padded wavelengths of the widest sweep CTA the autotuner may pick (buffer sizes)
+  int nw4 = 0;       // W4 evaluations per (wavelength, depth): Zeeman components + unsplit lines
+  int jac_tangent = 0;  // node responses / LM Jacobian by forward-mode sweeps (snapi_jacobian_mode)
   // autotuner (snapi_autotune): off = the compiled launch shapes; per batch-size bucket the shapes
   // it measured fastest; an optional cache file shared across processes
   int tune = 0;

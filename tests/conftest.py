@@ -78,6 +78,7 @@ def emu():
     E.emu_synth.argtypes = [ip, ip, ip, vp, vp, dbl, vp, ip, vp, vp]
     E.emu_adjoint.argtypes = [ip, ip, ip, vp, vp, dbl, vp, dbl, ip, vp, vp, vp, vp, ip, vp, vp, vp, vp, vp]
     E.emu_voigt.argtypes = [ctypes.c_float, ctypes.c_float, vp]
+    E.emu_jvp.argtypes = [ip, ip, ip, vp, vp, dbl, vp, ip, vp, ip, vp, vp]
     return E
 
 

@@ -10,6 +10,7 @@
 
 #include <vector>
 
+#include "../../snapi_b200/csrc/snapi_jvp.cuh"
 #include "../../snapi_b200/csrc/snapi_sweep.cuh"
 
 using namespace snapi;
@@ -195,6 +196,74 @@ int emu_adjoint(int nd, int nl, int nlines, const double *lam_air, const double 
       double g = 0.0;
       for (int i = 0; i < nrec; ++i) g += (double)rb[i] * (double)tp[i];
       grad[(size_t)p * npar + q] = g * scale2;
+    }
+  }
+  return 0;
+}
+
+// Node responses by the forward-mode (tangent) sweep, one direction at a time, each doing its own
+// W4 evaluations (the kernel shares them among its directions): dstokes [npix][npar][nl][4].
+int emu_jvp(int nd, int nl, int nlines, const double *lam_air, const double *tau500, double mu, const void *lines,
+            int npix, const float *records, int npar, const float *tangents, float *dstokes) {
+  Problem P = make_problem(nd, nl, nlines, lam_air, tau500, mu, (const EmuLine *)lines);
+  const int nrec = nd * P.nfield, nw = w4_count(P.lc.data(), nlines);
+  PixelState ps;
+  HostScratch sc;
+  sc.buf.resize(nd * 16);
+  std::vector<float> w(6 * (nw ? nw : 1));
+  for (int p = 0; p < npix; ++p) {
+    stage(P, records + (size_t)p * nrec, ps);
+    for (int l = 0; l < nl; ++l) {
+      LamConst lam;
+      float delta[kMaxLines];
+      lambda_setup(P, l, lam, delta);
+      float out[4];
+      forward_sweep<true>(ps.pv, lam, delta, out, sc);
+      for (int q = 0; q < npar; ++q) {
+        const float *tq = tangents + ((size_t)p * npar + q) * nrec;
+        // tangents of K', S, eta_I at depth z
+        auto depth_tan = [&](int z, float *dkp, float *dS, float &de) {
+          DepthConst d;
+          LineDepth ld[kMaxLines];
+          DepthTan dd;
+          LineTan dl[kMaxLines];
+          depth_precompute_jvp(&ps.rec[z * P.nfield], tq + z * P.nfield, nlines, P.lc.data(), P.lam_mid, d, ld, dd,
+                               dl);
+          for (int c = 0; c < nw; ++c) w4_eval(d, ld, P.lc.data(), nlines, P.cD.data(), lam, delta, c, &w[6 * c]);
+          float deta[7], djj[4], I[4], kp[6], S[4], e, tau;
+          cell_opacity_jvp(d, ld, P.lc.data(), nlines, P.cS.data(), P.cD.data(), lam, delta, w.data(), 6, dd, dl,
+                           deta, djj);
+          sc.load(z, I, kp, S, e, tau);
+          depth_opacity_jvp(kp, S, e, deta, djj, dkp, dS, de);
+        };
+        float dkA[6], dSA[4], deA, dkB[6], dSB[4], deB, dkC[6], dSC[4], deC;
+        depth_tan(nd - 1, dkA, dSA, deA);
+        depth_tan(nd - 2, dkB, dSB, deB);
+        float I[4], kA[6], SA[4], eA, tA, kB[6], SB[4], eB, tB, kC[6], SC[4], eC, tC;
+        sc.load(nd - 1, I, kA, SA, eA, tA);
+        sc.load(nd - 2, I, kB, SB, eB, tB);
+        float dI[4] = {dSA[0], 0.f, 0.f, 0.f};
+        double dopd_below = ((double)deB - (double)deA) / P.D[nd - 2];
+        for (int z = nd - 2; z >= 1; --z) {
+          depth_tan(z - 1, dkC, dSC, deC);
+          float Id[4];
+          sc.load(z - 1, Id, kC, SC, eC, tC);
+          const double dopd_z = opd_interior_jvp(eA, eB, eC, P.D[z], P.D[z - 1], deA, deB, deC);
+          const float dtau = (float)bezier_dtau_jvp(deA, deB, dopd_below, dopd_z, P.D[z]);
+          float Ip[4], Ic[4], k_[6], S_[4], e_, tau;
+          sc.load(z + 1, Ip, k_, S_, e_, tau);
+          sc.load(z, Ic, k_, S_, e_, tau);
+          float dIn[4];
+          delo_step_jvp(Ip, kA, SA, kB, SB, tau, Ic, dI, dkA, dSA, dkB, dSB, dtau, dIn);
+          for (int s = 0; s < 4; ++s) dI[s] = dIn[s];
+          for (int k = 0; k < 6; ++k) { kA[k] = kB[k]; kB[k] = kC[k]; dkA[k] = dkB[k]; dkB[k] = dkC[k]; }
+          for (int s = 0; s < 4; ++s) { SA[s] = SB[s]; SB[s] = SC[s]; dSA[s] = dSB[s]; dSB[s] = dSC[s]; }
+          eA = eB; eB = eC; deA = deB; deB = deC;
+          dopd_below = dopd_z;
+        }
+        float *o = dstokes + (((size_t)p * npar + q) * nl + l) * 4;
+        for (int s = 0; s < 4; ++s) o[s] = dI[s];  // the top point copies the one below
+      }
     }
   }
   return 0;

@@ -121,3 +121,48 @@ def test_emulated_record_gradient(emu, oracle_lib, config3):
             t[0, k, f] = 1.0
             _, gq = so.chi2_grad_fd(fx["lambda_air"], fx["tau500"], rec, lines, obs[0], np.ones(4), np.ones(nl), t, h)
             assert abs(rg[0, k, f] - gq[0]) <= 1e-3 * abs(gq[0]) + 1e-30, (k, f, rg[0, k, f], gq[0])
+
+
+def emu_jvp(emu, oracle_lib, fx, rec, tan):
+    lines = emu_lines(oracle_lib, fx)
+    rec = np.ascontiguousarray(rec, np.float32)
+    tan = np.ascontiguousarray(tan, np.float32)
+    npix, npar = tan.shape[0], tan.shape[1]
+    nd, nl = fx["tau500"].shape[0], fx["lambda_air"].shape[0]
+    out = np.zeros((npix, npar, nl, 4), np.float32)
+    emu.emu_jvp(nd, nl, len(lines), P(fx["lambda_air"]), P(fx["tau500"]), 1.0, ctypes.addressof(lines), npix, P(rec),
+                npar, P(tan), P(out))
+    return out
+
+
+# central-difference steps of the FP64 check, per node kind (small: the model is smooth there)
+JVP_FD_STEP = {1: 1e-2, 2: 1.0, 3: 1.0, 4: 1e-3, 5: 1e-6, 6: 1e-6}
+
+
+def test_emulated_tangent_responses_vs_fp64_differences(emu, oracle_lib, config3):
+    """Forward-mode responses (the tangent of the FP32 synthesis along each node tangent,
+    snapi_jvp.cuh) against FP64 central differences of the oracle with small steps.  Where the
+    model has a kink (a branch of the monotone optical-depth derivative or of the W4 regions
+    switching inside the step) a central difference is not a derivative: those points, flagged by
+    differences at two steps that disagree, are left out -- fewer than 1 % of them."""
+    fx = config3
+    n = 3
+    out = emu_jvp(emu, oracle_lib, fx, fx["record"][:n], fx["tangent"][:n])
+    lines = oracle_lib.lines_from_arrays(fx["line_const"], fx["line_ncomp"], fx["line_pattern"])
+    kinds = fx["node_kind"].astype(int)
+    kinks = total = 0
+    for p in range(n):
+        rec = fx["record"][p].astype(np.float32).astype(np.float64)
+        for q in range(kinds.size):
+            t = fx["tangent"][p, q:q + 1].astype(np.float32).astype(np.float64)
+            h = JVP_FD_STEP[kinds[q]]
+            d1 = np.asarray(oracle_lib.stokes_jvp_fd(fx["lambda_air"], fx["tau500"], rec, lines, t, h)).reshape(-1, 4)
+            d2 = np.asarray(oracle_lib.stokes_jvp_fd(fx["lambda_air"], fx["tau500"], rec, lines, t, h / 10))
+            d2 = d2.reshape(-1, 4)
+            sc = np.abs(d1).max()
+            smooth = np.abs(d1 - d2) < 1e-5 * sc
+            kinks += int((~smooth).sum())
+            total += smooth.size
+            err = np.abs(out[p, q] - d1)[smooth].max() / sc
+            assert err < 1e-4, (p, q, err)
+    assert kinks < 0.01 * total, (kinks, total)

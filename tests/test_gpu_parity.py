@@ -313,3 +313,34 @@ def test_spectral_broadening_matches_reference(sb, config3, fwhm):
     scale = np.abs(ref[:, inner]).max(axis=(1, 2))
     err = np.abs(out[:, inner] - ref[:, inner]).max(axis=(1, 2)) / scale
     assert np.all(np.isfinite(out)) and err.max() < 1e-6, err.max()
+
+
+def test_tangent_responses(sb, emu, oracle_lib, config3):
+    """Forward-mode responses (snapi_jacobian_mode TANGENT: k_resp_state + k_resp_jvp, the W4
+    evaluations shared among the nodes' warps) against the CPU emulator of the same tangent sweep
+    (checked there against FP64 differences), against the device's central differences, and
+    against the reference's own semi-analytic responses; also across direction groups (12 nodes
+    made of the 10 repeated: the CTAs carry at most 16 directions, so 32 nodes take two groups)."""
+    from test_emulator import emu_jvp
+    fx = config3
+    n = 4
+    kinds = fx["node_kind"]
+    rec, tan = fx["record"][:n], fx["tangent"][:n]
+    ctx = _ctx(sb, fx)
+    st_fd, ds_fd = ctx.responses(rec, tan, 1e-2 * node_scales(kinds))
+    ctx.jacobian_mode(sb.api.JACOBIAN_TANGENT)
+    st, ds = ctx.responses(rec, tan, np.ones(kinds.size))
+    tan32 = np.concatenate([tan, tan, tan, tan[:, :2]], axis=1)  # 32 directions: two groups of 16
+    ds32 = ctx.responses(rec, tan32, np.ones(32), want_stokes=False)
+    ctx.close()
+    np.testing.assert_array_equal(st, st_fd)  # the state pass synthesises as k_synth does
+    em = emu_jvp(emu, oracle_lib, fx, rec, tan)
+    for p in range(n):
+        for q in range(kinds.size):
+            sc = np.abs(em[p, q]).max()
+            assert np.abs(ds[p, q] - em[p, q]).max() < 1e-4 * sc, (p, q)
+            assert np.abs(ds[p, q] - ds_fd[p, q]).max() < 5e-3 * sc, (p, q)
+            rr = fx["responses"][p, q]
+            assert np.abs(ds[p, q] - rr).max() < 8e-2 * np.abs(rr).max(), (p, q)
+            for k in (q, q + 10, q + 20):
+                np.testing.assert_array_equal(ds32[p, k], ds[p, q])
