@@ -148,15 +148,19 @@ def _eos_tables():
     return EosTables(load_fixture("eos_c3"))
 
 
-def test_lm_device_build_matches_reference_fit(sb, config4):
+@pytest.mark.parametrize("jacobian", ["fd", "tangent"])
+def test_lm_device_build_matches_reference_fit(sb, config4, jacobian):
     """The whole stokes_lm_fit on the GPU (snapi_lm_fit: node -> record build + LM steps, nothing
     back on the host between steps) against the reference's fit of the same config-4 pixels, with
-    the tolerances of the host-builder test above."""
+    the tolerances of the host-builder test above; the Jacobian by central differences or by the
+    forward-mode sweeps."""
     fx = config4
     ic = _ic(fx)
     kinds = fx["node_kind"]
     ctx = sb.Context.from_fixture(fx, stokes_scale=ic)
     ctx.eos_set(_eos_tables())
+    if jacobian == "tangent":
+        ctx.jacobian_mode(sb.api.JACOBIAN_TANGENT)
     out = ctx.lm_fit_device(fx["nodes0"], fx["target"], kinds, 1e-2 * node_scales(kinds), mask=fx["mask"],
                             lm_start=1e3, max_iter=int(fx["iters"][0]), delta=_delta(fx))
     ctx.close()
