@@ -406,13 +406,23 @@ def run_snapi(args):
 
 def bench_lm(sb, pool, ic, device, npix=4096, iters=10):
     """Device time of the batched LM (snapi_lm_step): 10-node fits of npix pixels from offset
-    starting nodes.  The node -> record map between steps is the caller's; here it is the
-    records' linearisation along the node tangents (numpy, not timed on the device)."""
+    starting nodes, with the Jacobian by central differences and by the forward-mode sweeps.  The
+    node -> record map between steps is the caller's; here it is the records' linearisation along
+    the node tangents (numpy, not timed on the device)."""
+    out = {}
+    for mode, key in ((sb.api.JACOBIAN_FD, "fd_jacobian"), (sb.api.JACOBIAN_TANGENT, "tangent_jacobian")):
+        out[key] = _bench_lm_mode(sb, pool, ic, device, npix, iters, mode)
+    out["tangent_speedup"] = out["fd_jacobian"]["device_ms_per_step"] / out["tangent_jacobian"]["device_ms_per_step"]
+    return out
+
+
+def _bench_lm_mode(sb, pool, ic, device, npix, iters, mode):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from ref_builder import LinearBuilder
     truth, _, tan, nodes_t = make_workload(pool, npix, seed=11, return_nodes=True)
     build = LinearBuilder(truth, tan, nodes_t)
     ctx = sb.Context.from_fixture(pool, stokes_scale=ic, max_batch=npix, device=device)
+    ctx.jacobian_mode(mode)
     obs = ctx.synth(truth)
     obs += np.random.default_rng(12).normal(0.0, 1e-3 * ic, obs.shape).astype(np.float32)
     kinds = pool["node_kind"].astype(int)
@@ -434,9 +444,10 @@ def bench_lm(sb, pool, ic, device, npix=4096, iters=10):
     return {"pixels": npix, "npar": int(tan.shape[1]), "steps": steps, "device_ms_per_step": dev_ms / steps,
             "device_pixel_steps_per_s": npix * steps / (dev_ms / 1e3), "wall_s_with_host_linear_builder": wall,
             "median_iterations": float(np.median(res["iters"])),
-            "note": "device work per step: synthesis at the trial nodes, Jacobian (2 npar solves) at accepted "
-                    "nodes, J^T J / J^T r on the tcgen05 tensor cores (3xTF32 split, FP32 accumulation), FP64 "
-                    "damped eigen-solve; node -> record map on the host"}
+            "note": "device work per step: synthesis at the trial nodes, Jacobian at accepted nodes (2 npar "
+                    "solves, or one state pass + the forward-mode sweeps), J^T J / J^T r on the tcgen05 tensor "
+                    "cores (3xTF32 split, FP32 accumulation), FP64 damped eigen-solve; node -> record map on the "
+                    "host"}
 
 
 def _eos_tables():
