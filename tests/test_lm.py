@@ -204,10 +204,11 @@ def test_lm_device_build_with_spectral_broadening(sb, config4_psf):
                     reason="256-pixel reference fit fixture not generated")
 def test_lm_device_build_256_pixels_vs_reference(sb):
     """The whole fit on the device for 256 config-4 pixels (seed 404: uneven masks, noisy targets,
-    offset starting nodes) against the reference's stokes_lm_fit of the same pixels (DELTA 1e-3 as
-    compiled, start damping 1e3, 30 iterations).  Compared as distributions: the reference's
-    semi-analytic responses and our finite-difference Jacobian can take a pixel to different local
-    minima."""
+    offset starting nodes) against the reference's stokes_lm_fit of the same pixels (the fixture's
+    stop rule -- the configuration's DELTA 1e-4 from the patched reference build --, start damping
+    1e3, 30 iterations).  Compared as distributions: the reference's semi-analytic responses and our
+    finite-difference Jacobian can take a pixel to different local minima.  The worst pixels are
+    printed with their node differences (the record for explaining them)."""
     from conftest import load_fixture
     fx = load_fixture("config4_256")
     ic = _ic(fx)
@@ -227,6 +228,9 @@ def test_lm_device_build_256_pixels_vs_reference(sb):
         np.median(ratio), np.percentile(ratio, 5), np.percentile(ratio, 95), ratio.max()))
     print("  |dT| median %.1f K, 90 %% %.1f K; |dB| median %.2f G, 90 %% %.2f G; |d angle| 90 %% %.4f rad" % (
         np.median(dT), np.percentile(dT, 90), np.median(dB), np.percentile(dB, 90), np.percentile(dang, 90)))
+    for i in np.argsort(ratio)[::-1][:5]:
+        print("  pixel %3d: chi2 ratio %.3f, iterations %d, node differences %s" % (
+            i, ratio[i], out["iters"][i], np.array2string(d[i], precision=3, max_line_width=200)))
     assert np.median(ratio) <= 1.0
     assert np.mean(ratio < 1.05) >= 0.95
     assert np.mean(dT < 80.0) >= 0.9 and np.mean(dB < 10.0) >= 0.9 and np.mean(dang < 0.02) >= 0.9
