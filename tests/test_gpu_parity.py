@@ -333,7 +333,7 @@ def test_tangent_responses(sb, emu, oracle_lib, config3):
     tan32 = np.concatenate([tan, tan, tan, tan[:, :2]], axis=1)  # 32 directions: two groups of 16
     ds32 = ctx.responses(rec, tan32, np.ones(32), want_stokes=False)
     ctx.close()
-    np.testing.assert_array_equal(st, st_fd)  # the state pass synthesises as k_synth does
+    assert np.abs(st - st_fd).max() < 1e-6 * _ic(fx)  # the state pass synthesises as k_synth does
     em = emu_jvp(emu, oracle_lib, fx, rec, tan)
     for p in range(n):
         for q in range(kinds.size):
