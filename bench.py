@@ -493,10 +493,19 @@ def bench_build(sb, pool, device, ncol=4096):
 def bench_lm_device(sb, pool, ic, device, npix=1024, iters=10):
     """The whole stokes_lm_fit on the GPU (snapi_lm_fit): every step builds records and tangents of
     the requested nodes on the device and takes one LM iteration; npix pixels, 10 nodes, iters
-    iterations from offset starting nodes against noisy targets synthesised from the pool's nodes."""
+    iterations from offset starting nodes against noisy targets synthesised from the pool's nodes;
+    with the Jacobian by central differences and by the forward-mode sweeps."""
+    out = {}
+    for mode, key in ((sb.api.JACOBIAN_FD, "fd_jacobian"), (sb.api.JACOBIAN_TANGENT, "tangent_jacobian")):
+        out[key] = _bench_lm_device_mode(sb, pool, ic, device, npix, iters, mode)
+    return out
+
+
+def _bench_lm_device_mode(sb, pool, ic, device, npix, iters, mode):
     nodes = np.tile(pool["nodes"], (npix // pool["nodes"].shape[0] + 1, 1))[:npix]
     ctx = sb.Context.from_fixture(pool, stokes_scale=ic, max_batch=4096, device=device)
     ctx.eos_set(_eos_tables())
+    ctx.jacobian_mode(mode)
     rec, _, _, _ = ctx.build_records(nodes, tangents=False)
     obs = ctx.synth(rec)
     obs += np.random.default_rng(13).normal(0.0, 1e-3 * ic, obs.shape).astype(np.float32)
