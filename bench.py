@@ -203,8 +203,9 @@ def run_snapi(args):
     nl = pool["lambda_air"].shape[0]
     ctx = sb.Context.from_fixture(pool, stokes_scale=ic, max_batch=NPIX, device=local)
     ctx.eos_set(_eos_tables())
-    # launch shapes timed on the first (warm-up) calls: the timed steps use the tuned ones
-    ctx.autotune(True)
+    # launch shapes timed on the first (warm-up) calls: the timed steps use the tuned ones; with
+    # --tune-cache an earlier run's choices are read (and new ones appended)
+    ctx.autotune(True, args.tune_cache)
     npar = ctx._eos_npar
     truth, model = node_workload(NPIX, seed=3 + 1000 * rank)
     # target: the device synthesis of the truth + N(0, 1e-3 Ic) (set-up, not timed)
@@ -742,6 +743,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="snapi", choices=["snapi", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune-cache", default=None, help="autotuner cache file (snapi_autotune)")
     ap.add_argument("--pixels", type=int, default=NPIX, help="pixels per GPU (smaller cases for profiling)")
     ap.add_argument("--no-extras", action="store_true", help="skip the LM and NLTE measurements")
     ap.add_argument("--node-build-only", type=int, default=0, metavar="N",
