@@ -279,7 +279,7 @@ static int do_dump(const char *tskname, const char *nodesname, int npix, int fla
   if ((int)(nb.size() / 8) < npix * np) { fprintf(stderr, "nodes file too short\n"); return 2; }
   fp_t *lam1 = lambda_1based(t);
 
-  std::vector<double> allrec, allstokes, allresp, alltan, allrf_ok, alldld, alla, tau;
+  std::vector<double> allrec, allstokes, allstokes_resp, allresp, alltan, allrf_ok, alldld, alla, tau;
   std::vector<double> opprobe;
   std::vector<int> probe_l = {0, 40, 80, 100, 120, 160, 200};
   Record r0;
@@ -316,6 +316,10 @@ static int do_dump(const char *tskname, const char *nodesname, int npix, int fla
       t_resp += wall_s() - t0;
       for (int p = 1; p <= np; ++p) for (int l = 1; l <= nl; ++l) for (int s = 1; s <= 4; ++s) allresp.push_back(resp[p][l][s]);
       del_ft3dim(resp, 1, np, 1, nl, 1, 4);
+      // the Stokes vector of the same call: stokes_lm_fit's residual is formed with it
+      fp_t **S2 = o2->get_S(1, 1);
+      for (int l = 1; l <= nl; ++l) for (int s = 1; s <= 4; ++s) allstokes_resp.push_back(S2[s][l]);
+      del_ft2dim(S2, 1, 4, 1, nl);
       delete o2;
     }
     // record tangents by central differences of the node -> atmosphere map
@@ -380,6 +384,7 @@ static int do_dump(const char *tskname, const char *nodesname, int npix, int fla
   w.put("ref_adamp", {npix, r0.nlines, nd}, alla.data());
   w.put("stokes", {npix, nl, 4}, allstokes.data());
   if (flags & 1) w.put("responses", {npix, np, nl, 4}, allresp.data());
+  if (flags & 1) w.put("stokes_resp", {npix, nl, 4}, allstokes_resp.data());
   if (flags & 2) w.put("tangent", {npix, np, nd, nf}, alltan.data());
   if (flags & 4) {
     std::vector<double> pl(probe_l.begin(), probe_l.end());

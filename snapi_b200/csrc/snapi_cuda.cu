@@ -485,6 +485,7 @@ cudaError_t snapi::launch_responses(const snapi_ctx *ctx, const KParams &P) {
     KParams Q = P;
     Q.scratch = ctx->d_scratch;
     Q.stokes = nullptr;
+    Q.nvar = 1;  // k_resp_state: CTA = (pixel, chunk); k_resp_jvp indexes its own CTAs
     const int nwarp = std::min(P.npar, kJvpDirs), ngrp = (P.npar + kJvpDirs - 1) / kJvpDirs;
     const size_t smem = L.total + jvp_smem_extra(ctx->nw4, nwarp, ctx->nlines);
     const size_t nrec = (size_t)ctx->nd * ctx->nfield;
@@ -1279,6 +1280,7 @@ int snapi_responses(snapi_ctx *ctx, int npix, const float *records, int npar, co
     SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (ctx->jac_tangent) {  // forward-mode sweeps: the state pass also gives the Stokes vector
       P.scratch = ctx->d_scratch;
+      P.nvar = 1;  // k_resp_state: CTA = (pixel, chunk); k_resp_jvp indexes its own CTAs
       k_resp_state<<<sweep_ctas(ctx, nb), kChunk, L.total, ctx->stream>>>(P);
       SNAPI_CK(cudaGetLastError());
       const int nwarp = std::min(npar, kJvpDirs), ngrp = (npar + kJvpDirs - 1) / kJvpDirs;

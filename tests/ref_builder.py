@@ -30,17 +30,22 @@ def ref_builder_available():
 
 class RefBuilder:
     """responses: return the reference's own node responses (obs_stokes_responses_to_nodes, the
-    Jacobian its stokes_lm_fit uses) instead of the record tangents, for snapi_lm_step_jacobian."""
+    Jacobian its stokes_lm_fit uses) instead of the record tangents, for snapi_lm_step_jacobian.
+    history: keep, per call, the requested nodes and the reference's spectra there ("stokes" of
+    obs_stokes; with responses also "stokes_resp", the spectrum of the responses call, which
+    stokes_lm_fit forms its residual with) and the responses."""
 
-    def __init__(self, task=TASK, nproc=None, responses=False):
+    def __init__(self, task=TASK, nproc=None, responses=False, history=False):
         self.task = task
         self.nproc = nproc or os.cpu_count() or 1
         self.calls = 0
         self.responses = responses
+        self.history = [] if history else None
 
     def __call__(self, nodes, active):
         idx = np.flatnonzero(active)
         rec = tan = None
+        kept = {}
         with tempfile.TemporaryDirectory(prefix="snapi_build_") as tmp:
             jobs = []
             for k, chunk in enumerate(np.array_split(idx, min(self.nproc, max(1, idx.size)))):
@@ -63,7 +68,17 @@ class RefBuilder:
                     tan = np.zeros((nodes.shape[0],) + d[key].shape[1:], np.float32)
                 rec[chunk] = d["record"]
                 tan[chunk] = d[key]
+                if self.history is not None:
+                    for k in ("stokes", "stokes_resp", "responses"):
+                        if k in d:
+                            if k not in kept:
+                                kept[k] = np.full((nodes.shape[0],) + d[k].shape[1:], np.nan)
+                            kept[k][chunk] = d[k]
         self.calls += 1
+        if self.history is not None:
+            kept["nodes"] = np.array(nodes, np.float64, copy=True)
+            kept["active"] = np.array(active, bool, copy=True)
+            self.history.append(kept)
         return rec, tan
 
 

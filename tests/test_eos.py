@@ -139,6 +139,24 @@ def test_oracle_continued_start_vs_reference(oracle_lib, eos3, config3):
         eo.set_chem_start(old)
 
 
+def test_oracle_continued_start_dense_nodes(oracle_lib, eos1, config1, config2):
+    """As above on the 80-temperature-node model (17 columns): Nt and records against the
+    reference's build_from_nodes; the wiggly temperature profile moves the march furthest."""
+    import eos_oracle as eo
+    t = _tables(eos1)
+    lam0, mass = _line_const(config1)
+    ref = np.concatenate([config1["record"], config2["record"]]).astype(np.float64)
+    old = eo.set_chem_start(eo.CHEM_START_CONTINUE)
+    try:
+        for p in range(eos1["nodes"].shape[0]):
+            T, Nt, rec, st = eo.build(t, lam0, mass, eos1["nodes"][p])
+            assert st == 0
+            np.testing.assert_allclose(Nt, eos1["he_Nt"][p], rtol=TOL["continue"]["nt"])
+            np.testing.assert_allclose(rec, ref[p], rtol=TOL["continue"]["rec"], atol=0)
+    finally:
+        eo.set_chem_start(old)
+
+
 # ---- GPU ---------------------------------------------------------------------------------------------
 
 def _gpu_ctx(fx, eos, start="cold", **kw):
@@ -153,11 +171,13 @@ def _gpu_ctx(fx, eos, start="cold", **kw):
 # Tolerances per chemistry start.  The cold start is the reference's (its iterates to rounding).
 # The continued start (hydrostatic march only) stops on the same Newton rule from a nearby point,
 # so the march differs from the reference by up to the size of the reference's last Newton
-# update: Nt and n_e ~3e-8 relative, records ~4e-8 (below their float32 rounding), node tangents
-# ~4e-5 of each field's scale (the reference's 5 K differences carry that much noise from its
-# 1e-4 stop).
+# update: Nt and n_e ~3e-8 relative on the 4-temperature-node model and up to 7.3e-7 on the
+# 80-node one (the oracle's continued start shows the same 7.27e-7), records ~4e-8 (below their
+# float32 rounding) and up to 1.9e-6 on the 80-node model (the H- opacities, which go as
+# n_e n_H), node tangents ~4e-5 of each field's scale (the reference's 5 K differences carry that
+# much noise from its 1e-4 stop).
 TOL = {"cold": {"nt": 1e-10, "rec": 3e-7, "tan": 2e-5, "ne": 1e-9},
-       "continue": {"nt": 1e-7, "rec": 3e-7, "tan": 1e-4, "ne": 1e-7}}
+       "continue": {"nt": 1e-6, "rec": 3e-6, "tan": 1e-4, "ne": 1e-6}}
 
 
 @pytest.mark.gpu
