@@ -147,21 +147,25 @@ static double mol_K(const snapi_eos_molecule *M, double T) {
 }
 
 /* ---- linear solve (replaces the SVD of atmos_chm.cc:262-292) ----------------------------------- */
-static void gauss_solve(int n, double *A /*[n][n], destroyed*/, double *b /*rhs in, solution out*/) {
-  int piv[MA + 1];
-  for (int i = 0; i < n; ++i) piv[i] = i;
+/* Gaussian elimination with partial pivoting.  On return A holds the factors in elimination order:
+ * U on and above the diagonal, the multiplier of row r at step c in A[r][c] (rows are swapped from
+ * column c on, so a multiplier stays where it was computed), and piv[c] the row swapped with row c
+ * at step c -- lu_apply solves another right-hand side with them. */
+static void gauss_solve(int n, double *A /*[n][n], factored*/, double *b /*rhs in, solution out*/, int *piv) {
   for (int c = 0; c < n; ++c) {
     int p = c;
     double best = fabs(A[c * n + c]);
     for (int r = c + 1; r < n; ++r)
       if (fabs(A[r * n + c]) > best) { best = fabs(A[r * n + c]); p = r; }
+    piv[c] = p;
     if (p != c) {
-      for (int j = 0; j < n; ++j) { double t = A[c * n + j]; A[c * n + j] = A[p * n + j]; A[p * n + j] = t; }
+      for (int j = c; j < n; ++j) { double t = A[c * n + j]; A[c * n + j] = A[p * n + j]; A[p * n + j] = t; }
       double t = b[c]; b[c] = b[p]; b[p] = t;
     }
     double d = A[c * n + c];
     for (int r = c + 1; r < n; ++r) {
       double f = A[r * n + c] / d;
+      A[r * n + c] = f;
       if (f == 0.0) continue;
       for (int j = c + 1; j < n; ++j) A[r * n + j] -= f * A[c * n + j];
       b[r] -= f * b[c];
@@ -171,6 +175,19 @@ static void gauss_solve(int n, double *A /*[n][n], destroyed*/, double *b /*rhs 
     double s = b[r];
     for (int j = r + 1; j < n; ++j) s -= A[r * n + j] * b[j];
     b[r] = s / A[r * n + r];
+  }
+}
+
+/* the solve of gauss_solve for another right-hand side, from its factors */
+static void lu_apply(int n, const double *LU, const int *piv, double *b) {
+  for (int c = 0; c < n; ++c) {
+    if (piv[c] != c) { double t = b[c]; b[c] = b[piv[c]]; b[piv[c]] = t; }
+    for (int r = c + 1; r < n; ++r) b[r] -= LU[r * n + c] * b[c];
+  }
+  for (int r = n - 1; r >= 0; --r) {
+    double s = b[r];
+    for (int j = r + 1; j < n; ++j) s -= LU[r * n + j] * b[j];
+    b[r] = s / LU[r * n + r];
   }
 }
 
@@ -184,7 +201,20 @@ typedef struct {
   int passes;
   int have;        /* Ne / Natom hold an earlier solution of this column, at particle density Nt_prev */
   double Nt_prev;
+  /* the continued start's predictors: the factors of the last Newton pass's Jacobian (at
+     temperature lu_T; lu_n = 0: none), and log(N / Nt) of the last solutions at the two latest
+     temperatures T1 (the most recent) and T2 (nhist of them held) */
+  double LU[(MA + 1) * (MA + 1)];
+  int piv[MA + 1], lu_n, nhist;
+  double lu_T, lx1[MA + 1], lx2[MA + 1], T1, T2;
 } chem_state;
+
+static void chem_reset(chem_state *c) {
+  c->Ne = 1.0;
+  c->have = 0;
+  c->lu_n = 0;
+  c->nhist = 0;
+}
 
 /* How chemeq starts in the hydrostatic march (SNAPI_CHEM_START_*, the device's
  * snapi_eos_chem_start): COLD, the reference's start at every solve (the default here); CONTINUE,
@@ -193,6 +223,34 @@ typedef struct {
  * either mode.  Restated here so that the device's continued start has an exact-path checker; the
  * reference itself always starts cold. */
 static int g_chem_start = SNAPI_CHEM_START_COLD;
+
+/* The continued start's first iterate (1: N set; 0: none applies, scale the last solution by the
+ * particle-density ratio).  At the temperature of the last Jacobian (the next hydrostatic iterate
+ * of the same depth) a first-order step along dN/dNt = J^-1 e_1 (the defect of row 1 is
+ * sum N - Nt); at a new temperature (the next depth) log(N / Nt) extrapolated linearly in T from
+ * the last two temperatures' solutions (the ratio clipped to [0, 2]; 1 when they share T).  An
+ * iterate with a density below the Newton pass's floor (1e-2) or not finite is not used. */
+static int predict_start(const chem_state *c, int na, double T, double Nt, double *N) {
+  const int n = na + 1;
+  if (c->lu_n == n && T == c->lu_T) {
+    double x[MA + 1];
+    for (int i = 0; i < n; ++i) x[i] = 0.0;
+    x[1] = 1.0;
+    lu_apply(n, c->LU, c->piv, x);
+    const double dNt = Nt - c->Nt_prev;
+    N[0] = c->Ne + x[0] * dNt;
+    for (int a = 1; a <= na; ++a) N[a] = c->Natom[a - 1] + x[a] * dNt;
+  } else if (c->nhist == 2 && T != c->T1) {
+    double r = c->T1 != c->T2 ? (T - c->T1) / (c->T1 - c->T2) : 1.0;
+    r = fmin(fmax(r, 0.0), 2.0);
+    for (int a = 0; a <= na; ++a) N[a] = Nt * exp(c->lx1[a] + (c->lx1[a] - c->lx2[a]) * r);
+  } else {
+    return 0;
+  }
+  for (int a = 0; a <= na; ++a)
+    if (!(N[a] >= 1E-2) || !isfinite(N[a])) return 0;
+  return 1;
+}
 
 static void chemeq(const snapi_eos_model *m, double T, double Nt, chem_state *out) {
   const int na = m->natom, nm = m->nmol;
@@ -249,9 +307,11 @@ static void chemeq(const snapi_eos_model *m, double T, double Nt, chem_state *ou
   int warm = g_chem_start == SNAPI_CHEM_START_CONTINUE && out->have;
   int maxpass = 50;
   if (warm) {
-    const double sc = Nt / out->Nt_prev;
-    N[0] = out->Ne * sc;
-    for (int a = 1; a <= na; ++a) N[a] = out->Natom[a - 1] * sc;
+    if (!predict_start(out, na, T, Nt, N)) {
+      const double sc = Nt / out->Nt_prev;
+      N[0] = out->Ne * sc;
+      for (int a = 1; a <= na; ++a) N[a] = out->Natom[a - 1] * sc;
+    }
     maxpass = 8;
     goto newton;
   }
@@ -273,6 +333,7 @@ cold:
 newton:;
   const int n = na + 1;
   double d[MA + 1], A[(MA + 1) * (MA + 1)];
+  int piv[MA + 1];
   int iter = 0, conv;
   do {
     for (int a = 1; a <= na; ++a) ionfrc(&m->atoms[a - 1], T, N[0], fk[a], df[a]);
@@ -333,7 +394,7 @@ newton:;
     }
     double v[MA + 1];
     for (int i = 0; i < n; ++i) v[i] = d[i];
-    gauss_solve(n, A, v);
+    gauss_solve(n, A, v, piv);
     int finite = 1;
     for (int a = 0; a <= na; ++a) {
       N[a] -= v[a];
@@ -349,6 +410,19 @@ newton:;
     conv = 1;
     for (int i = 0; i <= na; ++i) if (fabs(d[i] / N[i]) > 1E-4) conv = 0;
   } while (!conv);
+  if (g_chem_start == SNAPI_CHEM_START_CONTINUE) {  /* keep what the next start predicts from */
+    memcpy(out->LU, A, sizeof(double) * n * n);
+    memcpy(out->piv, piv, sizeof(int) * n);
+    out->lu_n = n;
+    out->lu_T = T;
+    if (out->nhist == 0 || T != out->T1) {
+      memcpy(out->lx2, out->lx1, sizeof(double) * n);
+      out->T2 = out->T1;
+      if (out->nhist < 2) out->nhist++;
+    }
+    for (int a = 0; a <= na; ++a) out->lx1[a] = log(N[a] / Nt);
+    out->T1 = T;
+  }
   out->Ne = N[0];
   out->have = 1;
   out->Nt_prev = Nt;
@@ -562,8 +636,7 @@ static void hydrostatic(const snapi_eos_model *m, int nd, column *c) {
   const int MAX_ITER = 20;
   const double break_me = 1E-2;
   double op[MAXD], rho[MAXD];
-  cs.Ne = 1.0;
-  cs.have = 0;
+  chem_reset(&cs);
   c->Nt[0] = 0.3 / C_K / c->T[0];
   for (int iter = 0; iter < MAX_ITER; ++iter) {
     op[0] = chem_point(m, c->T[0], c->Nt[0], &cs, &P, 0);
@@ -602,8 +675,7 @@ static void record_depth(const snapi_eos_model *m, int nlines, const double *lam
   chem_state cs;
   pops P;
   const double T = c->T[x];
-  cs.Ne = 1.0;
-  cs.have = 0;  /* record solves start cold in either mode (their fields follow the solve's path) */
+  chem_reset(&cs);  /* record solves start cold in either mode (their fields follow the solve's path) */
   double kap = chem_point(m, T, c->Nt[x], &cs, &P, 1);
   if (cs.passes < 0) *status |= 1;
   const double Ne = cs.Ne;
@@ -675,8 +747,7 @@ int sne_chem(const snapi_eos_model *m, double T, double Nt, double *Ne, double *
              double *kap) {
   chem_state cs;
   pops P;
-  cs.Ne = 1.0;
-  cs.have = 0;
+  chem_reset(&cs);
   *kap_he = chem_point(m, T, Nt, &cs, &P, 0);
   *kap = opacity_continuum(m, T, cs.Ne, &P, 1);
   *Ne = cs.Ne;
@@ -720,8 +791,7 @@ int sne_atmos(const snapi_eos_model *m, int nd, const double *nodes, const doubl
   for (int x = 0; x < nd; ++x) {
     chem_state cs;
     pops P;
-    cs.Ne = 1.0;
-    cs.have = 0;
+    chem_reset(&cs);
     const double kap = chem_point(m, c.T[x], c.Nt[x], &cs, &P, 1);
     if (cs.passes < 0) c.status |= 1;
     const double Bx = c.B[x] * sin(c.th[x]) * cos(c.ph[x]);

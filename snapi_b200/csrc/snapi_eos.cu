@@ -146,8 +146,16 @@ struct Chem {
   int capped;
   int have;        // N holds the solution of an earlier solve of this column, at particle density Nt_prev
   double Nt_prev;
+  // the continued start's predictors: after a solve A holds the factors of its last Newton pass's
+  // Jacobian in elimination order (piv: the row swapped with row c at step c), valid at temperature
+  // lu_T when lu_ok; lx1 / lx2: log(N / Nt) of the last solutions at the two latest temperatures
+  // T1 (the most recent) and T2, nhist of them held
+  int piv[kEA + 1];
+  int lu_ok, nhist;
+  double lu_T, T1, T2;
+  double lx1[kEA + 1], lx2[kEA + 1];
 
-  __device__ explicit Chem(const EosDev &e) : E(e), T(-1.0), have(0), Nt_prev(0.0) {}
+  __device__ explicit Chem(const EosDev &e) : E(e), T(-1.0), have(0), Nt_prev(0.0), lu_ok(0), nhist(0) {}
 
   __device__ void set_T(double Tin) {
     T = Tin;
@@ -277,29 +285,86 @@ struct Chem {
   // Two starts.  Cold (warm = false, or no earlier solution): the reference's, at every call --
   // the ionisation-only quadratic for n_e and the halving loop to 1e-2 (atmos_chm.cc:129-171),
   // ~18 of the ~20 ionisation sweeps of a solve.  Continued (warm = true, the hydrostatic march
-  // only): Newton from the previous solution of the same column scaled by the particle-density
-  // ratio (the next hydrostatic iterate at the same depth, or the next depth), ~2 sweeps; if that
-  // Newton has not met the stop rule after kWarmPasses passes, or left non-finite values, the
-  // cold start runs.  Both stop on the reference's rule (all relative defects below 1e-4 before
-  // the last update), so the march's opacities differ by up to that last update's size and its
-  // particle densities by ~3e-8 relative; the records' own solves always start cold (their stage
-  // fractions are those of the last sweep before the final update, i.e. they follow the path).
+  // only): Newton from a predicted iterate (predict: a step along dN/dNt at the same depth,
+  // ~1.2 passes; a temperature extrapolation at a new depth, ~2.2 passes) or else the previous
+  // solution of the same column scaled by the particle-density ratio; if that Newton has not met
+  // the stop rule after kWarmPasses passes, or left non-finite values, the cold start runs.  Both
+  // stop on the reference's rule (all relative defects below 1e-4 before the last update), so the
+  // march's opacities differ by up to that last update's size and its particle densities by
+  // ~4e-8 relative (up to ~1e-6 on a model with a temperature node at every depth); the records'
+  // own solves always start cold (their stage fractions are those of the last sweep before the
+  // final update, i.e. they follow the path).
   static constexpr int kWarmPasses = 8;
 
   __device__ void solve(double Nt, bool warm) {
     capped = 0;
     if (warm && have) {
-      const double sc = Nt / Nt_prev;
-      for (int a = 0; a <= E.natom; ++a) N[a] *= sc;
+      if (!predict(Nt)) {
+        const double sc = Nt / Nt_prev;
+        for (int a = 0; a <= E.natom; ++a) N[a] *= sc;
+      }
       if (newton(Nt, kWarmPasses, true) == 1) {
-        Nt_prev = Nt;
+        finish(Nt, warm);
         return;
       }
     }
     cold_start(Nt);
     if (newton(Nt, 50, false) != 1) capped = 1;
+    finish(Nt, warm);
+  }
+
+  __device__ void finish(double Nt, bool warm) {
     have = 1;
     Nt_prev = Nt;
+    if (!warm) return;
+    lu_ok = 1;
+    lu_T = T;
+    const int na = E.natom;
+    if (nhist == 0 || T != T1) {
+      for (int a = 0; a <= na; ++a) lx2[a] = lx1[a];
+      T2 = T1;
+      if (nhist < 2) ++nhist;
+    }
+    for (int a = 0; a <= na; ++a) lx1[a] = log(N[a] / Nt);
+    T1 = T;
+  }
+
+  // The continued start's first iterate into N (true), or false: none applies, and the caller
+  // scales the last solution by the particle-density ratio.  At the temperature of the last
+  // Jacobian (the next hydrostatic iterate of the same depth) a first-order step along
+  // dN/dNt = J^-1 e_1 (the defect of row 1 is sum N - Nt), solved with the kept factors; at a new
+  // temperature (the next depth) log(N / Nt) extrapolated linearly in T from the last two
+  // temperatures' solutions (the ratio clipped to [0, 2]; 1 when they share T).  An iterate with a
+  // density below the Newton pass's floor (1e-2) or not finite is not used.
+  __device__ bool predict(double Nt) {
+    const int na = E.natom, n = na + 1;
+    double x[kEA + 1];
+    if (lu_ok && T == lu_T) {
+      for (int i = 0; i < n; ++i) x[i] = 0.0;
+      x[1] = 1.0;
+      for (int c = 0; c < n; ++c) {
+        const int p = piv[c];
+        if (p != c) { const double t = x[c]; x[c] = x[p]; x[p] = t; }
+        for (int r = c + 1; r < n; ++r) x[r] -= A[r * n + c] * x[c];
+      }
+      for (int r = n - 1; r >= 0; --r) {
+        double s = x[r];
+        for (int j = r + 1; j < n; ++j) s -= A[r * n + j] * x[j];
+        x[r] = s / A[r * n + r];
+      }
+      const double dNt = Nt - Nt_prev;
+      for (int a = 0; a <= na; ++a) x[a] = N[a] + x[a] * dNt;
+    } else if (nhist == 2 && T != T1) {
+      double r = T1 != T2 ? (T - T1) / (T1 - T2) : 1.0;
+      r = fmin(fmax(r, 0.0), 2.0);
+      for (int a = 0; a <= na; ++a) x[a] = Nt * exp(lx1[a] + (lx1[a] - lx2[a]) * r);
+    } else {
+      return false;
+    }
+    for (int a = 0; a <= na; ++a)
+      if (!(x[a] >= 1E-2) || !isfinite(x[a])) return false;
+    for (int a = 0; a <= na; ++a) N[a] = x[a];
+    return true;
   }
 
   // the reference's starting values: ionisation-only quadratic and the halving loop
@@ -399,7 +464,9 @@ struct Chem {
         }
       }
       for (int a = 2; a <= na; ++a) d[a] = E.abund[a - 1] * Nr - E.abund[0] * Nc[a];
-      // Gaussian elimination with partial pivoting; v in place of a copy of d
+      // Gaussian elimination with partial pivoting; v in place of a copy of d.  The factors stay
+      // in A (multipliers where they were computed: rows are swapped from column c on) for the
+      // continued start's predictor
       double v[kEA + 1];
       for (int i = 0; i < n; ++i) v[i] = d[i];
       for (int c = 0; c < n; ++c) {
@@ -409,13 +476,15 @@ struct Chem {
           const double t = fabs(A[r * n + c]);
           if (t > best) { best = t; p = r; }
         }
+        piv[c] = p;
         if (p != c) {
           for (int j = c; j < n; ++j) { const double t = A[c * n + j]; A[c * n + j] = A[p * n + j]; A[p * n + j] = t; }
           const double t = v[c]; v[c] = v[p]; v[p] = t;
         }
-        const double piv = A[c * n + c];
+        const double pv = A[c * n + c];
         for (int r = c + 1; r < n; ++r) {
-          const double f = A[r * n + c] / piv;
+          const double f = A[r * n + c] / pv;
+          A[r * n + c] = f;
           if (f == 0.0) continue;
           for (int j = c + 1; j < n; ++j) A[r * n + j] -= f * A[c * n + j];
           v[r] -= f * v[c];
