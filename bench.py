@@ -49,7 +49,7 @@ NCU_DRAM_BYTES_PER_PIXEL = 4.90e6
 # the kernels' CPU emulator and of the FP64 node -> record restatement; profiles/flops_per_cell.md):
 # flop per pixel of the adjoint call (forward + reverse, 3915 per wavelength x depth cell) and FP64
 # flop per column of the node build with tangents (9 builds, continued chemistry start).
-FLOPS = {"adjoint_flops_per_pixel": 6.296e7, "build_flops_per_column_with_tangents": 1.191e8}
+FLOPS = {"adjoint_flops_per_pixel": 6.296e7, "build_flops_per_column_with_tangents": 1.081e8}
 # the evaluated model = truth + these offsets (T x4, v_turb, v_los x2, B, inclination, azimuth)
 MODEL_OFFSET = np.array([0.0, 0.0, 0.0, 0.0, 0.3e5, 0.3e5, -0.3e5, 200.0, 0.1, 0.1])
 

@@ -339,7 +339,10 @@ def test_tangent_responses(sb, emu, oracle_lib, config3):
         for q in range(kinds.size):
             sc = np.abs(em[p, q]).max()
             assert np.abs(ds[p, q] - em[p, q]).max() < 1e-4 * sc, (p, q)
-            assert np.abs(ds[p, q] - ds_fd[p, q]).max() < 5e-3 * sc, (p, q)
+            # central differences with steps of 1e-2 of the node scale (50 K on a temperature
+            # node) carry their truncation error: the FP64 oracle's own differences at that step
+            # and at 1e-4 of the scale differ by up to 5.4e-3 (pixel 3, temperature node 1)
+            assert np.abs(ds[p, q] - ds_fd[p, q]).max() < 1e-2 * sc, (p, q)
             rr = fx["responses"][p, q]
             assert np.abs(ds[p, q] - rr).max() < 8e-2 * np.abs(rr).max(), (p, q)
             for k in (q, q + 10, q + 20):
