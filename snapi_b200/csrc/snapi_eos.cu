@@ -91,6 +91,7 @@ struct EosDev {
   // molecules (components: 1-based atom, 0 the electron)
   int mnc[kEM];
   int matom[kEM][SNAPI_MOL_MAX_COMP], mref[kEM][SNAPI_MOL_MAX_COMP];
+  int mdup[kEM][SNAPI_MOL_MAX_COMP];  // 1: the component's atom is also an earlier component's
   int mmul[kEM][kEA + 1];
   double mq[kEM];
   int meqc[kEM], mncoef[kEM];
@@ -418,11 +419,17 @@ struct Chem {
         A[a] = Ea[a];       // A[0][a]
         A[n + a] = 1.0;     // A[1][a]
       }
+      // abundance rows a >= 2: d_a = abund_a Nr - abund_H Nc_a with Nr = N_H + sum_m nmv_m mul_mH,
+      // Nc_a = N_a + sum_m nmv_m mul_ma, so row a of the Jacobian is
+      //   abund_a (e_1 + gr) - abund_H (e_a + sum_{m contains a} mul_ma grad nmv_m),
+      // gr = sum_m mul_mH grad nmv_m: the dense part is one vector, added to every row at the end;
+      // the rest touches only the rows and columns of each molecule's own atoms
       for (int r = 2; r <= na; ++r) {
-        A[r * n] = 0.0;
-        for (int b = 1; b <= na; ++b)
-          A[r * n + b] = (b == 1 ? E.abund[r - 1] : 0.0) - (b == r ? E.abund[0] : 0.0);
+        for (int b = 0; b <= na; ++b) A[r * n + b] = 0.0;
+        A[r * n + r] = -E.abund[0];
       }
+      double gr[kEA + 1];
+      for (int b = 0; b <= na; ++b) gr[b] = 0.0;
       double Nr = N[1];
       double Nc[kEA + 1];
       for (int a = 2; a <= na; ++a) Nc[a] = N[a];
@@ -441,29 +448,38 @@ struct Chem {
           }
         }
         dm0 *= nmv;
-        const double q = E.mq[m];
+        const double q = E.mq[m], hm = (double)E.mmul[m][1];
         d[0] += q * nmv;
         d[1] += nmv;
-        Nr += nmv * (double)E.mmul[m][1];
-        for (int a = 2; a <= na; ++a) Nc[a] += nmv * (double)E.mmul[m][a];
+        Nr += nmv * hm;
         A[0] += q * dm0;
         A[n] += dm0;
-        for (int a = 2; a <= na; ++a)
-          A[a * n] += dm0 * (E.abund[a - 1] * (double)E.mmul[m][1] - E.abund[0] * (double)E.mmul[m][a]);
+        gr[0] += hm * dm0;
         for (int i = 0; i < nc; ++i) {
           const int b = E.matom[m][i];
-          if (b == 0) continue;
-          bool first = true;  // each distinct component atom once
-          for (int j = 0; j < i; ++j) if (E.matom[m][j] == b) first = false;
-          if (!first) continue;
-          const double dmb = nmv * (double)E.mmul[m][b] / N[b];
+          if (b == 0 || E.mdup[m][i]) continue;  // each distinct component atom once
+          const double mb = (double)E.mmul[m][b];
+          const double dmb = nmv * mb / N[b];
           A[b] += q * dmb;
           A[n + b] += dmb;
-          for (int a = 2; a <= na; ++a)
-            A[a * n + b] += dmb * (E.abund[a - 1] * (double)E.mmul[m][1] - E.abund[0] * (double)E.mmul[m][a]);
+          gr[b] += hm * dmb;
+          if (b >= 2) {
+            Nc[b] += nmv * mb;
+            A[b * n] -= E.abund[0] * mb * dm0;
+          }
+          for (int j = 0; j < nc; ++j) {
+            const int a = E.matom[m][j];
+            if (a < 2 || E.mdup[m][j]) continue;
+            A[a * n + b] -= E.abund[0] * (double)E.mmul[m][a] * dmb;
+          }
         }
       }
-      for (int a = 2; a <= na; ++a) d[a] = E.abund[a - 1] * Nr - E.abund[0] * Nc[a];
+      for (int a = 2; a <= na; ++a) {
+        const double ab = E.abund[a - 1];
+        for (int b = 0; b <= na; ++b) A[a * n + b] += ab * gr[b];
+        A[a * n + 1] += ab;
+        d[a] = ab * Nr - E.abund[0] * Nc[a];
+      }
       // Gaussian elimination with partial pivoting; v in place of a copy of d.  The factors stay
       // in A (multipliers where they were computed: rows are swapped from column c on) for the
       // continued start's predictor
@@ -1174,6 +1190,9 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
       const int idx = a + 1;
       H.matom[mm][i] = idx;
       H.mmul[mm][idx] += 1;
+      H.mdup[mm][i] = 0;
+      for (int j = 0; j < i; ++j)
+        if (H.matom[mm][j] == idx) H.mdup[mm][i] = 1;
       q += (double)M.comp_charge[i];
       if (a >= 0) {
         const int z = M.comp_charge[i] > 0 ? M.comp_charge[i] : 0;

@@ -250,3 +250,32 @@ def test_lm_device_build_256_pixels_vs_reference(sb):
     assert np.median(ratio) <= 1.0
     assert np.mean(ratio < 1.05) >= 0.95
     assert np.mean(dT < 80.0) >= 0.9 and np.mean(dB < 10.0) >= 0.9 and np.mean(dang < 0.02) >= 0.9
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(__file__), "golden", "config4_256.npz")),
+                    reason="256-pixel reference fit fixture not generated")
+def test_lm_256_outliers_are_the_iteration_cap(sb):
+    """The 256-pixel comparison's worst pixels (20: chi2 13.7x the reference's after 30 iterations,
+    18: 4.1x) are not a model difference: at the reference's fitted nodes the device's chi2 is the
+    reference's, and with 100 iterations the device's fit ends well below the reference's chi2 --
+    the reference's 30-iteration result is not a minimum either (both fits are still descending
+    slowly when the iteration cap stops them, along different paths)."""
+    from conftest import load_fixture
+    fx = load_fixture("config4_256")
+    ic = _ic(fx)
+    kinds = fx["node_kind"]
+    sel = np.array([20, 18])
+    tgt, mask = fx["target"][sel], fx["mask"][sel]
+    ctx = sb.Context.from_fixture(fx, stokes_scale=ic)
+    ctx.eos_set(_eos_tables())
+    rec, _, _, st = ctx.build_records(fx["fit_nodes"][sel], tangents=False)
+    r = (tgt - ctx.synth(rec)) * mask[:, :, None]
+    at_ref = (r * r).sum(axis=(1, 2)) / fx["fit_chi2"][sel]
+    out = ctx.lm_fit_device(fx["nodes0"][sel], tgt, kinds, 1e-2 * node_scales(kinds), mask=mask, lm_start=1e3,
+                            max_iter=100, delta=_delta(fx))
+    ctx.close()
+    long_fit = out["chi2"] * ic * ic / fx["fit_chi2"][sel]
+    print("chi2 at the reference's nodes / reference's:", at_ref, " 100-iteration fit / reference's:", long_fit,
+          "iterations", out["iters"])
+    assert np.all(np.abs(at_ref - 1.0) < 1e-2)
+    assert np.all(long_fit < 0.5)
