@@ -61,6 +61,7 @@ constexpr double cSAHA = 2.0706615382E-16;
 // per-stage and per-term constants packed for two 16-byte loads each in the ionisation sweep
 struct __align__(16) StageTab {
   double zf, izf;  // Traving: z f and its inverse
+  double zz;       // Traving: 31.321 z^2 (the asymptotic term's D_z is zz x, x = 5040 / T)
   int t0, t1;      // Traving asymptotic terms [t0, t1) (empty for the other types)
   int ref, pad;    // kept-fraction slot (-1 none)
 };
@@ -132,14 +133,15 @@ struct EosDev {
 struct Chem {
   const EosDev &E;
   double T, kT;
+  double x5040;  // 5040 / T
+  // per stage, one 16-byte load in the sweep: the thread-local state of a column is what the
+  // march's L1 has to hold for every resident column
   struct __align__(16) SLoc {
     double Ut;  // T-only part of U (whole U for CONST / IRWIN / NONE)
     double cz;  // fct exp(-chi / kT): the T-only factor of the stage ratio
-    double Dz;  // 31.321 z^2 x
-    double pad;
   } sl[kES];
   double w2[kET];   // g2 exp(-2.302585 ee x)
-  double K[kEM];
+  double iKkT[kEM];  // 1 / (K_m k T) of each molecule at this T
   double Ea[kEA + 1], Da[kEA + 1];  // sum_i i f_i, sum_i i df_i / dNe per atom (1-based)
   double fr[kER], dr[kER];          // kept ionisation fractions and their Ne derivatives
   double N[kEA + 1];
@@ -162,6 +164,7 @@ struct Chem {
     T = Tin;
     kT = cK * T;
     const double x = 5040.0 / T;
+    x5040 = x;
     const double fct = 2.0 * pow((2.0 * cPI * cME * cK * T) / (cH * cH), 1.5);
     for (int s = 0; s < E.nst; ++s) {
       const int ty = E.pft[s];
@@ -171,7 +174,6 @@ struct Chem {
           for (int c = E.c0[t]; c < E.c1[t]; ++c) u += E.cA[c] * exp(-2.302585 * E.cG[c] * x);
           w2[t] = E.g2[t] * exp(-2.302585 * E.tee[t] * x);
         }
-        sl[s].Dz = 31.321 * E.zeff[s] * E.zeff[s] * x;
       } else if (ty == SNAPI_PF_IRWIN) {
         const double lnT = log(T);
         double sum = 0.0;
@@ -193,7 +195,7 @@ struct Chem {
       } else if (E.meqc[m] == SNAPI_EQC_CONST) {
         k = E.mcoef[m][0];
       }
-      K[m] = k;
+      iKkT[m] = 1.0 / (k * kT);
     }
   }
 
@@ -204,7 +206,7 @@ struct Chem {
     U = L.Ut;
     dU = 0.0;
     if (S.t1 <= S.t0) return;
-    const double zf = S.zf, p = zf * ipne, ip = pne * S.izf, dz = L.Dz;
+    const double zf = S.zf, p = zf * ipne, ip = pne * S.izf, dz = S.zz * x5040;
     double dq = 0.0, wl = 0.0;
     for (int t = S.t0; t < S.t1; ++t) {
       const TermTab Tt = E.ttab[t];
@@ -431,16 +433,17 @@ struct Chem {
       double gr[kEA + 1];
       for (int b = 0; b <= na; ++b) gr[b] = 0.0;
       double Nr = N[1];
-      double Nc[kEA + 1];
+      double Nc[kEA + 1], iN[kEA + 1];
       for (int a = 2; a <= na; ++a) Nc[a] = N[a];
+      for (int a = 0; a <= na; ++a) iN[a] = 1.0 / N[a];
       for (int m = 0; m < nm; ++m) {
-        double nmv = 1.0 / (K[m] * kT), dm0 = 0.0;
+        double nmv = iKkT[m], dm0 = 0.0;
         const int nc = E.mnc[m];
         for (int i = 0; i < nc; ++i) {
           const int a = E.matom[m][i];
           if (a == 0) {
             nmv *= N[0] * kT;
-            dm0 += 1.0 / N[0];
+            dm0 += iN[0];
           } else {
             const int r = E.mref[m][i];
             nmv *= fr[r] * N[a] * kT;
@@ -459,7 +462,7 @@ struct Chem {
           const int b = E.matom[m][i];
           if (b == 0 || E.mdup[m][i]) continue;  // each distinct component atom once
           const double mb = (double)E.mmul[m][b];
-          const double dmb = nmv * mb / N[b];
+          const double dmb = nmv * mb * iN[b];
           A[b] += q * dmb;
           A[n + b] += dmb;
           gr[b] += hm * dmb;
@@ -497,9 +500,9 @@ struct Chem {
           for (int j = c; j < n; ++j) { const double t = A[c * n + j]; A[c * n + j] = A[p * n + j]; A[p * n + j] = t; }
           const double t = v[c]; v[c] = v[p]; v[p] = t;
         }
-        const double pv = A[c * n + c];
+        const double ipv = 1.0 / A[c * n + c];
         for (int r = c + 1; r < n; ++r) {
-          const double f = A[r * n + c] / pv;
+          const double f = A[r * n + c] * ipv;
           A[r * n + c] = f;
           if (f == 0.0) continue;
           for (int j = c + 1; j < n; ++j) A[r * n + j] -= f * A[c * n + j];
@@ -1277,6 +1280,7 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
     StageTab &S = H.stab[q];
     S.zf = H.zf[q];
     S.izf = H.izf[q];
+    S.zz = 31.321 * H.zeff[q] * H.zeff[q];
     S.t0 = H.pft[q] == SNAPI_PF_TRAV ? H.t0[q] : 0;
     S.t1 = H.pft[q] == SNAPI_PF_TRAV ? H.t1[q] : 0;
     S.ref = H.ref[q];
