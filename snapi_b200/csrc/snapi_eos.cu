@@ -239,9 +239,17 @@ struct Chem {
   __device__ __forceinline__ void sweep_atom(int a, double ine, double pne, double ipne) {
     const int s0 = E.s0[a], ns = E.ns[a];
     double h = 1.0, fsum = 0.0, S1 = 0.0, dfsum = 0.0, S2 = 0.0, dl0 = 0.0;
+    // the next stage's constants are loaded while this one is evaluated (the chain of a column
+    // waits on these loads otherwise)
+    StageTab Sn = E.stab[s0];
+    SLoc Ln = sl[s0];
     for (int z = 0; z < ns; ++z) {
-      const StageTab S = E.stab[s0 + z];
-      const SLoc L = sl[s0 + z];
+      const StageTab S = Sn;
+      const SLoc L = Ln;
+      if (z + 1 < ns) {
+        Sn = E.stab[s0 + z + 1];
+        Ln = sl[s0 + z + 1];
+      }
       double U, dU;
       stage_u<kDeriv>(S, L, ine, pne, ipne, U, dU);
       const double f = U * h;
@@ -436,6 +444,8 @@ struct Chem {
       double Nc[kEA + 1], iN[kEA + 1];
       for (int a = 2; a <= na; ++a) Nc[a] = N[a];
       for (int a = 0; a <= na; ++a) iN[a] = 1.0 / N[a];
+      // the molecules' sums into rows 0 / 1 and column 0 stay in registers over the loop
+      double d0 = d[0], d1 = d[1], a00 = A[0], a10 = A[n], gr0 = 0.0;
       for (int m = 0; m < nm; ++m) {
         double nmv = iKkT[m], dm0 = 0.0;
         const int nc = E.mnc[m];
@@ -452,12 +462,12 @@ struct Chem {
         }
         dm0 *= nmv;
         const double q = E.mq[m], hm = (double)E.mmul[m][1];
-        d[0] += q * nmv;
-        d[1] += nmv;
+        d0 += q * nmv;
+        d1 += nmv;
         Nr += nmv * hm;
-        A[0] += q * dm0;
-        A[n] += dm0;
-        gr[0] += hm * dm0;
+        a00 += q * dm0;
+        a10 += dm0;
+        gr0 += hm * dm0;
         for (int i = 0; i < nc; ++i) {
           const int b = E.matom[m][i];
           if (b == 0 || E.mdup[m][i]) continue;  // each distinct component atom once
@@ -477,6 +487,11 @@ struct Chem {
           }
         }
       }
+      d[0] = d0;
+      d[1] = d1;
+      A[0] = a00;
+      A[n] = a10;
+      gr[0] = gr0;
       for (int a = 2; a <= na; ++a) {
         const double ab = E.abund[a - 1];
         for (int b = 0; b <= na; ++b) A[a * n + b] += ab * gr[b];
