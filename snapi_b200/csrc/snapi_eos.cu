@@ -239,17 +239,9 @@ struct Chem {
   __device__ __forceinline__ void sweep_atom(int a, double ine, double pne, double ipne) {
     const int s0 = E.s0[a], ns = E.ns[a];
     double h = 1.0, fsum = 0.0, S1 = 0.0, dfsum = 0.0, S2 = 0.0, dl0 = 0.0;
-    // the next stage's constants are loaded while this one is evaluated (the chain of a column
-    // waits on these loads otherwise)
-    StageTab Sn = E.stab[s0];
-    SLoc Ln = sl[s0];
     for (int z = 0; z < ns; ++z) {
-      const StageTab S = Sn;
-      const SLoc L = Ln;
-      if (z + 1 < ns) {
-        Sn = E.stab[s0 + z + 1];
-        Ln = sl[s0 + z + 1];
-      }
+      const StageTab S = E.stab[s0 + z];
+      const SLoc L = sl[s0 + z];
       double U, dU;
       stage_u<kDeriv>(S, L, ine, pne, ipne, U, dU);
       const double f = U * h;
