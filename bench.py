@@ -237,10 +237,12 @@ def run_snapi(args):
     launches = 0
     torch.cuda.synchronize()
     ev0.record(stream)
+    torch.cuda.nvtx.range_push("timed_steps")  # ncu --nvtx --nvtx-include timed_steps/ selects these launches
     for _ in range(args.steps):
         step()
         phase += np.array(ctx.last_phase_ms)
         launches += ctx.last_launches
+    torch.cuda.nvtx.range_pop()
     ev1.record(stream)
     torch.cuda.synchronize()
     total_ms = ev0.elapsed_time(ev1)

@@ -359,17 +359,23 @@ __global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_resp_state(KParams P
 }
 
 // Phase T: CTA = (pixel, 32 wavelengths, up to kJvpDirs node directions); warp w carries direction
-// q0 + w, lane = wavelength.  At each depth the W4 evaluations with their x / a derivatives
-// (voigt_grad) of the CTA's 32 wavelengths are shared: every warp computes a share of them into
-// shared memory; then each warp forms its direction's opacity tangent from all of them and takes
-// the DELO / optical-depth tangent step, the forward values coming from phase S.  The depth
-// tangents of a direction (DepthTan, LineTan) are computed once per depth by the warp's lane 0.
-// Shared buffers are double-buffered by depth: one __syncthreads per depth.
-size_t jvp_smem_extra(int nw, int nwarp, int nlines) {
-  return sizeof(float) * (2 * 32 * (size_t)(nw * 6 + 1) + 2 * (size_t)nwarp * (12 + 5 * nlines));
+// q0 + w, lane = wavelength.  At each depth the direction-independent part of the opacity tangent
+// -- the sums of each line's Zeeman components' W4 values and x / a derivatives (jvp_basis_task)
+// for the CTA's 32 wavelengths -- is computed once, its tasks (line groups) spread over the warps,
+// into shared memory; the depth tangents of each warp's direction (DepthTan, LineTan) are
+// computed with one line per lane.  Then each warp forms its direction's opacity tangent from the
+// sums and takes the DELO / optical-depth tangent step, the forward values coming from phase S;
+// the step's direction-independent part (DELO weights, the bracket multiplying d tau, the LU of
+// A, the optical-depth coefficients: delo_jvp_prep, opd_interior_coef) is one more task of the
+// same round.  Shared buffers are double-buffered by depth: one __syncthreads per depth.  Directions come in
+// groups of kJvpDirs, every group through the same code, so a direction's result does not depend
+// on how many others share its launch.
+size_t jvp_smem_extra(int nbasis, int nwarp, int nlines) {
+  return sizeof(double) * 2 * 3 * 32 + sizeof(float) * (2 * kDeloPrepFloats * 32 + 2 * 32 * (size_t)(nbasis | 1) +
+                                                         2 * (size_t)nwarp * (12 + 5 * nlines));
 }
 
-__global__ void __launch_bounds__(32 * kJvpDirs) k_resp_jvp(KParams P) {
+__global__ void __launch_bounds__(32 * kJvpDirs, 2) k_resp_jvp(KParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const SmemLayout L = smem_layout(P.nd, P.nfield, P.nlines, P.ncomp, P.nred, false);
   const int nchk = (P.nl + 31) >> 5, ngrp = (P.npar + kJvpDirs - 1) / kJvpDirs;
@@ -379,13 +385,17 @@ __global__ void __launch_bounds__(32 * kJvpDirs) k_resp_jvp(KParams P) {
   const int grp = b % ngrp, pix = b / ngrp;
   const int nwarp = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int q = grp * kJvpDirs + warp;
-  const bool live = q < P.npar;  // warps past the last direction only help with the W4 share
+  const bool live = q < P.npar;  // warps past the last direction only help with the shared sums
   if (P.skip && P.skip[pix]) return;  // CTA-uniform
   PixelView pv;
   if (!stage_pixel(P, pix, smem, L, pv, -1, 0.f)) return;
-  const int nd = P.nd, nw = w4_count(pv.lc, P.nlines), lstride = nw * 6 + 1, dtn = 12 + 5 * P.nlines;
-  float *W = reinterpret_cast<float *>(smem + L.total);  // [2][32][lstride]
-  float *DT = W + 2 * 32 * lstride;                       // [2][nwarp][dtn]
+  const int nd = P.nd, nlines = P.nlines, dtn = 12 + 5 * nlines;
+  const int ntask = jvp_basis_tasks(pv.lc, nlines), bstride = jvp_basis_size(pv.lc, nlines) | 1;
+  double *Pd = reinterpret_cast<double *>(smem + L.total);  // [2][3][32]: optical-depth coefficients
+  float *Pf = reinterpret_cast<float *>(Pd + 2 * 3 * 32);    // [2][kDeloPrepFloats][32]: DeloPrep
+  float *Bs = Pf + 2 * kDeloPrepFloats * 32;                 // [2][32][bstride]
+  float *DT = Bs + 2 * 32 * bstride;                         // [2][nwarp][dtn]
+  const int prep_warp = ntask % nwarp;                       // the step's shared part: task ntask
   const int l = chunk * 32 + lane;
   LamConst lam;
   float delta[kMaxLines];
@@ -395,47 +405,72 @@ __global__ void __launch_bounds__(32 * kJvpDirs) k_resp_jvp(KParams P) {
   st.base = P.scratch + (size_t)pix * nd * 4 * P.lpad;
   st.lpad = P.lpad;
   st.l = l;
-  auto prepare = [&](int z, int buf) {
+  // step: the DELO step z + 1 -> z of the loop below whose shared part this round prepares (-1: none)
+  auto prepare = [&](int z, int buf, int step) {
+    if (step >= 0 && warp == prep_warp) {
+      float Ip[4], kp_p[6], S_p[4], e_p, t_p, Ic[4], kp_c[6], S_c[4], e_c, tau, Id[4], kp_d[6], S_d[4], e_d, t_d;
+      st.load(step + 1, Ip, kp_p, S_p, e_p, t_p);
+      st.load(step, Ic, kp_c, S_c, e_c, tau);
+      st.load(step - 1, Id, kp_d, S_d, e_d, t_d);
+      DeloPrep pr;
+      delo_jvp_prep(Ip, kp_p, S_p, kp_c, S_c, tau, Ic, pr);
+      const float *pf = &pr.w0;
+      for (int k = 0; k < kDeloPrepFloats; ++k) Pf[(buf * kDeloPrepFloats + k) * 32 + lane] = pf[k];
+      double g[3];
+      opd_interior_coef(e_p, e_c, e_d, pv.D[step], pv.D[step - 1], g);
+      for (int k = 0; k < 3; ++k) Pd[(buf * 3 + k) * 32 + lane] = g[k];
+    }
     float *dt = DT + (buf * nwarp + warp) * dtn;
-    if (live && lane == 0)
-      depth_tangent(pv.rec + z * P.nfield, trec + z * P.nfield, P.nlines, pv.lc, P.lam_mid, pv.ld + z * P.nlines,
-                    *reinterpret_cast<DepthTan *>(dt), reinterpret_cast<LineTan *>(dt + 12));
-    float *wl = W + (buf * 32 + lane) * lstride;
-    for (int c = warp; c < nw; c += nwarp)
-      w4_eval(pv.dc[z], pv.ld + z * P.nlines, pv.lc, P.nlines, pv.compD, lam, delta, c, wl + 6 * c);
+    if (live) {
+      const float *rz = pv.rec + z * P.nfield, *tz = trec + z * P.nfield;
+      DepthTan dd;
+      DepthTanHead h;
+      depth_tangent_head(rz, tz, P.lam_mid, dd, h);
+      if (lane == 0) *reinterpret_cast<DepthTan *>(dt) = dd;
+      for (int j = lane; j < nlines; j += 32)
+        depth_tangent_line(rz, tz, pv.lc[j], pv.ld[z * nlines + j], j, h, reinterpret_cast<LineTan *>(dt + 12)[j]);
+    }
+    float *bl = Bs + (buf * 32 + lane) * bstride;
+    for (int k = warp; k < ntask; k += nwarp)
+      jvp_basis_task(pv.dc[z], pv.ld + z * nlines, pv.lc, nlines, pv.compS, pv.compD, lam, delta, k, bl);
   };
   auto tangent = [&](int z, int buf, float *kp, float *S, float &e, float *dkp, float *dS, float &de) {
     const float *dt = DT + (buf * nwarp + warp) * dtn;
-    const float *wl = W + (buf * 32 + lane) * lstride;
+    const float *bl = Bs + (buf * 32 + lane) * bstride;
     float deta[7], djj[4], I[4], tau;
-    cell_opacity_jvp(pv.dc[z], pv.ld + z * P.nlines, pv.lc, P.nlines, pv.compS, pv.compD, lam, delta, wl, 6,
+    cell_opacity_jvp(pv.dc[z], pv.ld + z * nlines, pv.lc, nlines, lam, delta, bl,
                      *reinterpret_cast<const DepthTan *>(dt), reinterpret_cast<const LineTan *>(dt + 12), deta, djj);
     st.load(z, I, kp, S, e, tau);
     depth_opacity_jvp(kp, S, e, deta, djj, dkp, dS, de);
   };
   float kA[6], SA[4], eA, dkA[6], dSA[4], deA, kB[6], SB[4], eB, dkB[6], dSB[4], deB;
   float kC[6], SC[4], eC, dkC[6], dSC[4], deC;
-  prepare(nd - 1, 0);
+  prepare(nd - 1, 0, -1);
   __syncthreads();
   if (live) tangent(nd - 1, 0, kA, SA, eA, dkA, dSA, deA);
-  prepare(nd - 2, 1);
+  prepare(nd - 2, 1, -1);
   __syncthreads();
   if (live) tangent(nd - 2, 1, kB, SB, eB, dkB, dSB, deB);
   float dI[4] = {live ? dSA[0] : 0.f, 0.f, 0.f, 0.f};
   double dopd_below = live ? ((double)deB - (double)deA) / pv.D[nd - 2] : 0.0;
   int buf = 0;
   for (int z = nd - 2; z >= 1; --z) {
-    prepare(z - 1, buf);
+    prepare(z - 1, buf, z);
     __syncthreads();
     if (live) {
       tangent(z - 1, buf, kC, SC, eC, dkC, dSC, deC);
-      const double dopd_z = opd_interior_jvp(eA, eB, eC, pv.D[z], pv.D[z - 1], deA, deB, deC);
+      double g[3];
+      for (int k = 0; k < 3; ++k) g[k] = Pd[(buf * 3 + k) * 32 + lane];
+      const double dopd_z = opd_interior_apply(g, deA, deB, deC);
       const float dtau = (float)bezier_dtau_jvp(deA, deB, dopd_below, dopd_z, pv.D[z]);
-      float Ip[4], Ic[4], k_[6], S_[4], e_, tau;
-      st.load(z + 1, Ip, k_, S_, e_, tau);
-      st.load(z, Ic, k_, S_, e_, tau);
+      DeloPrep pr;
+      float *pf = &pr.w0;
+      for (int k = 0; k < kDeloPrepFloats; ++k) pf[k] = Pf[(buf * kDeloPrepFloats + k) * 32 + lane];
+      float Ip[4], Ic[4];
+      st.load_I(z + 1, Ip);
+      st.load_I(z, Ic);
       float dIn[4];
-      delo_step_jvp(Ip, kA, SA, kB, SB, tau, Ic, dI, dkA, dSA, dkB, dSB, dtau, dIn);
+      delo_jvp_apply(pr, Ip, kA, Ic, dI, dkA, dSA, dkB, dSB, dtau, dIn);
 #pragma unroll
       for (int s = 0; s < 4; ++s) dI[s] = dIn[s];
 #pragma unroll
@@ -451,6 +486,10 @@ __global__ void __launch_bounds__(32 * kJvpDirs) k_resp_jvp(KParams P) {
     float4 *o = reinterpret_cast<float4 *>(P.dstokes + (((size_t)pix * P.npar + q) * P.nl + l) * 4);
     *o = make_float4(dI[0], dI[1], dI[2], dI[3]);
   }
+}
+
+void launch_jvp(int nctas, int nwarp, size_t smem, cudaStream_t st, const KParams &P) {
+  k_resp_jvp<<<nctas, 32 * nwarp, smem, st>>>(P);
 }
 
 double airtovac_d(double lambda_air) {  // cmlib/mathtools.cc:1325-1330
@@ -487,7 +526,7 @@ cudaError_t snapi::launch_responses(const snapi_ctx *ctx, const KParams &P) {
     Q.stokes = nullptr;
     Q.nvar = 1;  // k_resp_state: CTA = (pixel, chunk); k_resp_jvp indexes its own CTAs
     const int nwarp = std::min(P.npar, kJvpDirs), ngrp = (P.npar + kJvpDirs - 1) / kJvpDirs;
-    const size_t smem = L.total + jvp_smem_extra(ctx->nw4, nwarp, ctx->nlines);
+    const size_t smem = L.total + jvp_smem_extra(ctx->nbasis, nwarp, ctx->nlines);
     const size_t nrec = (size_t)ctx->nd * ctx->nfield;
     // in batches of max_batch pixels: the forward state lives in the adjoint's scratch
     for (int p0 = 0; p0 < P.npix; p0 += ctx->max_batch) {
@@ -500,7 +539,7 @@ cudaError_t snapi::launch_responses(const snapi_ctx *ctx, const KParams &P) {
       k_resp_state<<<R.npix * ctx->nchunk, kChunk, L.total, ctx->stream>>>(R);
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
-      k_resp_jvp<<<R.npix * ((ctx->nl + 31) / 32) * ngrp, 32 * nwarp, smem, ctx->stream>>>(R);
+      launch_jvp(R.npix * ((ctx->nl + 31) / 32) * ngrp, nwarp, smem, ctx->stream, R);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -800,7 +839,7 @@ int snapi_jacobian_mode(snapi_ctx *ctx, int mode) {
     return set_err(ctx, SNAPI_EINVAL, "snapi_jacobian_mode: unknown mode %d", mode);
   if (mode == SNAPI_JACOBIAN_TANGENT) {  // the state layout needs the compiled sweep width's padding
     const size_t smem = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false).total +
-                        jvp_smem_extra(ctx->nw4, kJvpDirs, ctx->nlines);
+                        jvp_smem_extra(ctx->nbasis, kJvpDirs, ctx->nlines);
     int maxsm = 0;
     cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
     if ((int)smem > maxsm)
@@ -939,7 +978,7 @@ snapi_ctx *snapi_create(const snapi_problem *prob, int device, int *status) {
     }
   }
   ctx->ncomp = (int)cS.size();
-  ctx->nw4 = w4_count(lc.data(), ctx->nlines);
+  ctx->nbasis = jvp_basis_size(lc.data(), ctx->nlines);
   const SmemLayout Lsw = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false);
   const SmemLayout Lfin = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, true);
   int maxsm = 0;
@@ -1284,8 +1323,8 @@ int snapi_responses(snapi_ctx *ctx, int npix, const float *records, int npar, co
       k_resp_state<<<sweep_ctas(ctx, nb), kChunk, L.total, ctx->stream>>>(P);
       SNAPI_CK(cudaGetLastError());
       const int nwarp = std::min(npar, kJvpDirs), ngrp = (npar + kJvpDirs - 1) / kJvpDirs;
-      k_resp_jvp<<<nb * ((ctx->nl + 31) / 32) * ngrp, 32 * nwarp,
-                   L.total + jvp_smem_extra(ctx->nw4, nwarp, ctx->nlines), ctx->stream>>>(P);
+      launch_jvp(nb * ((ctx->nl + 31) / 32) * ngrp, nwarp, L.total + jvp_smem_extra(ctx->nbasis, nwarp, ctx->nlines),
+                 ctx->stream, P);
       SNAPI_CK(cudaGetLastError());
       ctx->last_launches += 2;
     } else {

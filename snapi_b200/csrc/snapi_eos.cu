@@ -74,6 +74,7 @@ struct EosDev {
   double lambda_he, lambda_kappa, grav, tau_min, tau_max, theta, phi, ftrav;
   double abund[kEA];
   int s0[kEA], ns[kEA];
+  int zkeep[kEA];  // 1 + the highest stage of the atom with a kept fraction (0: none)
   // stages
   int pft[kES];
   double pfv[kES];   // CONST: value; TRAV: g0; NONE: 1
@@ -237,7 +238,8 @@ struct Chem {
   // atom a (0-based): Ea, and with kDeriv Da and the kept fractions
   template <bool kDeriv>
   __device__ __forceinline__ void sweep_atom(int a, double ine, double pne, double ipne) {
-    const int s0 = E.s0[a], ns = E.ns[a];
+    const int s0 = E.s0[a], ns = E.ns[a], zk = E.zkeep[a];
+    int zend = ns;
     double h = 1.0, fsum = 0.0, S1 = 0.0, dfsum = 0.0, S2 = 0.0, dl0 = 0.0;
     for (int z = 0; z < ns; ++z) {
       const StageTab S = E.stab[s0 + z];
@@ -256,12 +258,20 @@ struct Chem {
         if (S.ref >= 0) { fr[S.ref] = f; dr[S.ref] = df; }
       }
       h *= L.cz * ine;
+      // Past the stages with kept fractions, stop once the next stage's weight is below 1e-30 of
+      // the sum: the ionisation energies rise with z, so every further ratio c_z / n_e is smaller
+      // than the ones that brought h this low, and the remaining terms (< 1e-26 of each sum with
+      // U <= 1e4) cannot change an FP64 sum.
+      if (z + 1 >= zk && h < 1e-30 * fsum) {
+        zend = z + 1;
+        break;
+      }
     }
     const double inv = 1.0 / fsum;
     Ea[a + 1] = S1 * inv;
     if (kDeriv) {
       Da[a + 1] = (S2 - dfsum * S1 * inv) * inv;
-      for (int z = 0; z < ns; ++z) {
+      for (int z = 0; z < zend; ++z) {
         const int r = E.stab[s0 + z].ref;
         if (r >= 0) { dr[r] = (dr[r] - dfsum * fr[r] * inv) * inv; fr[r] *= inv; }
       }
@@ -1283,6 +1293,11 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
   H.nlev = nlev;
   H.nref = nref;
   H.href = H.ref[H.s0[0]];
+  for (int a = 0; a < m->natom; ++a) {
+    H.zkeep[a] = 0;
+    for (int z = 0; z < H.ns[a]; ++z)
+      if (H.ref[H.s0[a] + z] >= 0) H.zkeep[a] = z + 1;
+  }
   for (int q = 0; q < H.nst; ++q) {
     StageTab &S = H.stab[q];
     S.zf = H.zf[q];

@@ -50,7 +50,7 @@ constexpr int kOpTileCands[3] = {8, 16, 32};    // pixels per opacity-adjoint CT
 constexpr int kHeCands[3] = {32, 64, 128};      // threads per hydrostatic-march CTA
 constexpr int kVarCands[3] = {64, 128, 256};    // threads per record-chemistry CTA
 constexpr int kHeDefault = 64, kVarDefault = 64;  // the chemistry kernels' compiled CTA sizes
-constexpr int kJvpDirs = 16;  // node directions (warps) per forward-mode responses CTA
+constexpr int kJvpDirs = 10;  // node directions (warps) per forward-mode responses CTA (two CTAs per SM)
 struct AdjCfg {
   int chunk, optile;
   int rt128;  // the reverse DELO sweep at 128 registers per thread
@@ -163,6 +163,10 @@ struct DevScratch {
     p[lpad] = make_float4(kp[0], kp[1], kp[2], kp[3]);
     p[2 * lpad] = make_float4(kp[4], kp[5], e, tau);
     p[3 * lpad] = make_float4(S[0], S[1], S[2], S[3]);
+  }
+  __device__ void load_I(int z, float *I) const {
+    const float4 a = base[(size_t)z * 4 * lpad + l];
+    I[0] = a.x; I[1] = a.y; I[2] = a.z; I[3] = a.w;
   }
   __device__ void load(int z, float *I, float *kp, float *S, float &e, float &tau) const {
     const float4 *p = base + (size_t)z * 4 * lpad + l;
@@ -318,7 +322,7 @@ struct snapi_ctx {
   cudaEvent_t ev_copy[kStageChunks] = {}, ev_free = nullptr;  // chunk uploaded / round's kernels done
   int nd = 0, nl = 0, nlines = 0, nfield = 0, ncomp = 0, nred = 0, lpad = 0, nchunk = 0, nwslot = 0, max_batch = 0;
   int lpad_max = 0;  // padded wavelengths of the widest sweep CTA the autotuner may pick (buffer sizes)
-  int nw4 = 0;       // W4 evaluations per (wavelength, depth): Zeeman components + unsplit lines
+  int nbasis = 0;    // direction-independent W4 sums per (wavelength, depth) (jvp_basis_size)
   int jac_tangent = 0;  // node responses / LM Jacobian by forward-mode sweeps (snapi_jacobian_mode)
   // autotuner (snapi_autotune): off = the compiled launch shapes; per batch-size bucket the shapes
   // it measured fastest; an optional cache file shared across processes

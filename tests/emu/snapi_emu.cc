@@ -201,16 +201,17 @@ int emu_adjoint(int nd, int nl, int nlines, const double *lam_air, const double 
   return 0;
 }
 
-// Node responses by the forward-mode (tangent) sweep, one direction at a time, each doing its own
-// W4 evaluations (the kernel shares them among its directions): dstokes [npix][npar][nl][4].
+// Node responses by the forward-mode (tangent) sweep, one direction at a time, each forming the
+// direction-independent W4 sums of its cells itself (the kernel shares them among its directions):
+// dstokes [npix][npar][nl][4].
 int emu_jvp(int nd, int nl, int nlines, const double *lam_air, const double *tau500, double mu, const void *lines,
             int npix, const float *records, int npar, const float *tangents, float *dstokes) {
   Problem P = make_problem(nd, nl, nlines, lam_air, tau500, mu, (const EmuLine *)lines);
-  const int nrec = nd * P.nfield, nw = w4_count(P.lc.data(), nlines);
+  const int nrec = nd * P.nfield, nb = jvp_basis_size(P.lc.data(), nlines), ntask = jvp_basis_tasks(P.lc.data(), nlines);
   PixelState ps;
   HostScratch sc;
   sc.buf.resize(nd * 16);
-  std::vector<float> w(6 * (nw ? nw : 1));
+  std::vector<float> w(nb ? nb : 1);
   for (int p = 0; p < npix; ++p) {
     stage(P, records + (size_t)p * nrec, ps);
     for (int l = 0; l < nl; ++l) {
@@ -229,10 +230,10 @@ int emu_jvp(int nd, int nl, int nlines, const double *lam_air, const double *tau
           LineTan dl[kMaxLines];
           depth_precompute_jvp(&ps.rec[z * P.nfield], tq + z * P.nfield, nlines, P.lc.data(), P.lam_mid, d, ld, dd,
                                dl);
-          for (int c = 0; c < nw; ++c) w4_eval(d, ld, P.lc.data(), nlines, P.cD.data(), lam, delta, c, &w[6 * c]);
+          for (int k = 0; k < ntask; ++k)
+            jvp_basis_task(d, ld, P.lc.data(), nlines, P.cS.data(), P.cD.data(), lam, delta, k, w.data());
           float deta[7], djj[4], I[4], kp[6], S[4], e, tau;
-          cell_opacity_jvp(d, ld, P.lc.data(), nlines, P.cS.data(), P.cD.data(), lam, delta, w.data(), 6, dd, dl,
-                           deta, djj);
+          cell_opacity_jvp(d, ld, P.lc.data(), nlines, lam, delta, w.data(), dd, dl, deta, djj);
           sc.load(z, I, kp, S, e, tau);
           depth_opacity_jvp(kp, S, e, deta, djj, dkp, dS, de);
         };

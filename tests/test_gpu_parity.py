@@ -316,11 +316,12 @@ def test_spectral_broadening_matches_reference(sb, config3, fwhm):
 
 
 def test_tangent_responses(sb, emu, oracle_lib, config3):
-    """Forward-mode responses (snapi_jacobian_mode TANGENT: k_resp_state + k_resp_jvp, the W4
-    evaluations shared among the nodes' warps) against the CPU emulator of the same tangent sweep
-    (checked there against FP64 differences), against the device's central differences, and
-    against the reference's own semi-analytic responses; also across direction groups (12 nodes
-    made of the 10 repeated: the CTAs carry at most 16 directions, so 32 nodes take two groups)."""
+    """Forward-mode responses (snapi_jacobian_mode TANGENT: k_resp_state + k_resp_jvp, the
+    direction-independent W4 sums shared among the nodes' warps) against the CPU emulator of the
+    same tangent sweep (checked there against FP64 differences), against the device's central
+    differences, and against the reference's own semi-analytic responses; also across direction
+    groups (32 nodes made of the 10 repeated: the CTAs carry at most 10 directions, so 32 nodes
+    take four groups, and each node's result is bit-identical to its 10-node run)."""
     from test_emulator import emu_jvp
     fx = config3
     n = 4
