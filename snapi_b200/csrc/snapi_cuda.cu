@@ -360,16 +360,17 @@ __global__ void __launch_bounds__(kChunk, SNAPI_SYN_MINB) k_resp_state(KParams P
 
 // Phase T: CTA = (pixel, 32 wavelengths, up to kJvpDirs node directions); warp w carries direction
 // q0 + w, lane = wavelength.  At each depth the direction-independent part of the opacity tangent
-// -- the sums of each line's Zeeman components' W4 values and x / a derivatives (jvp_basis_task)
-// for the CTA's 32 wavelengths -- is computed once, its tasks (line groups) spread over the warps,
-// into shared memory; the depth tangents of each warp's direction (DepthTan, LineTan) are
-// computed with one line per lane.  Then each warp forms its direction's opacity tangent from the
-// sums and takes the DELO / optical-depth tangent step, the forward values coming from phase S;
-// the step's direction-independent part (DELO weights, the bracket multiplying d tau, the LU of
-// A, the optical-depth coefficients: delo_jvp_prep, opd_interior_coef) is one more task of the
-// same round.  Shared buffers are double-buffered by depth: one __syncthreads per depth.  Directions come in
-// groups of kJvpDirs, every group through the same code, so a direction's result does not depend
-// on how many others share its launch.
+// -- the sums of each line's Zeeman components' W4 values and x / a derivatives and the H-
+// exponentials (jvp_basis_task) for the CTA's 32 wavelengths -- is computed once, its tasks (line
+// groups) spread over the warps, into shared memory; the depth tangents of the directions
+// (DepthTan, LineTan) are items of one (direction, head or line) each, spread over the CTA's
+// threads; the DELO step's direction-independent part (weights, the bracket multiplying d tau,
+// the LU of A, the optical-depth coefficients: delo_jvp_prep, opd_interior_coef) is one more
+// task.  Then each warp forms its direction's opacity tangent from the sums and takes the DELO /
+// optical-depth tangent step, the forward values coming from phase S.  Shared buffers are
+// double-buffered by depth: one __syncthreads per depth.  Directions come in groups of kJvpDirs,
+// every group through the same code, so a direction's result does not depend on how many others
+// share its launch.
 size_t jvp_smem_extra(int nbasis, int nwarp, int nlines) {
   return sizeof(double) * 2 * 3 * 32 + sizeof(float) * (2 * kDeloPrepFloats * 32 + 2 * 32 * (size_t)(nbasis | 1) +
                                                          2 * (size_t)nwarp * (12 + 5 * nlines));
@@ -396,11 +397,11 @@ __global__ void __launch_bounds__(32 * kJvpDirs, 2) k_resp_jvp(KParams P) {
   float *Bs = Pf + 2 * kDeloPrepFloats * 32;                 // [2][32][bstride]
   float *DT = Bs + 2 * 32 * bstride;                         // [2][nwarp][dtn]
   const int prep_warp = ntask % nwarp;                       // the step's shared part: task ntask
+  const int nlive = min(kJvpDirs, P.npar - grp * kJvpDirs), nitem = nlive * (1 + nlines);
   const int l = chunk * 32 + lane;
   LamConst lam;
   float delta[kMaxLines];
   thread_lambda(P, pv, l < P.nl ? l : P.nl - 1, lam, delta);
-  const float *trec = P.tangent + ((size_t)pix * P.npar + (live ? q : 0)) * nd * P.nfield;
   DevScratch st;
   st.base = P.scratch + (size_t)pix * nd * 4 * P.lpad;
   st.lpad = P.lpad;
@@ -420,15 +421,21 @@ __global__ void __launch_bounds__(32 * kJvpDirs, 2) k_resp_jvp(KParams P) {
       opd_interior_coef(e_p, e_c, e_d, pv.D[step], pv.D[step - 1], g);
       for (int k = 0; k < 3; ++k) Pd[(buf * 3 + k) * 32 + lane] = g[k];
     }
-    float *dt = DT + (buf * nwarp + warp) * dtn;
-    if (live) {
-      const float *rz = pv.rec + z * P.nfield, *tz = trec + z * P.nfield;
-      DepthTan dd;
+    // the depth tangents of the group's directions: one item per (direction, head or line), the
+    // items on the threads counted from the CTA's last one (the basis tasks start at warp 0)
+    for (int t = nwarp * 32 - 1 - threadIdx.x; t < nitem; t += nwarp * 32) {
+      const int w = t < nlive ? t : (t - nlive) / nlines;
+      const float *rz = pv.rec + z * P.nfield;
+      const float *tz = P.tangent + (((size_t)pix * P.npar + grp * kJvpDirs + w) * nd + z) * P.nfield;
+      float *dt = DT + (buf * nwarp + w) * dtn;
       DepthTanHead h;
-      depth_tangent_head(rz, tz, P.lam_mid, dd, h);
-      if (lane == 0) *reinterpret_cast<DepthTan *>(dt) = dd;
-      for (int j = lane; j < nlines; j += 32)
+      if (t < nlive) {
+        depth_tangent_head(rz, tz, P.lam_mid, *reinterpret_cast<DepthTan *>(dt), h);
+      } else {
+        const int j = (t - nlive) % nlines;
+        depth_tangent_scalars(rz, tz, h);
         depth_tangent_line(rz, tz, pv.lc[j], pv.ld[z * nlines + j], j, h, reinterpret_cast<LineTan *>(dt + 12)[j]);
+      }
     }
     float *bl = Bs + (buf * 32 + lane) * bstride;
     for (int k = warp; k < ntask; k += nwarp)

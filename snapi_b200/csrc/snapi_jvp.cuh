@@ -35,13 +35,22 @@ struct DepthTanHead {
   float T, vt, B, dT, dvt, dB, invk, dinvk;
 };
 
+// the scalars of a depth row that every line's tangent uses
+SNAPI_HD void depth_tangent_scalars(const float *rec, const float *trec, DepthTanHead &h) {
+  h.T = rec[F_T];
+  h.vt = rec[F_VT];
+  h.B = rec[F_B];
+  h.dT = trec[F_T];
+  h.dvt = trec[F_VT];
+  h.dB = trec[F_B];
+  h.invk = 1.0f / rec[F_KAP];
+  h.dinvk = -trec[F_KAP] * h.invk * h.invk;
+}
+
 // the tangent of depth_precompute's depth constants along trec (the record row's tangent)
 SNAPI_HD void depth_tangent_head(const float *rec, const float *trec, float lam_mid, DepthTan &dd, DepthTanHead &h) {
-  const float T = rec[F_T], vt = rec[F_VT], ne = rec[F_NE], B = rec[F_B];
-  const float dT = trec[F_T], dvt = trec[F_VT], dne = trec[F_NE], dB = trec[F_B];
-  const float invk = 1.0f / rec[F_KAP];
-  const float dinvk = -trec[F_KAP] * invk * invk;
-  h.T = T; h.vt = vt; h.B = B; h.dT = dT; h.dvt = dvt; h.dB = dB; h.invk = invk; h.dinvk = dinvk;
+  depth_tangent_scalars(rec, trec, h);
+  const float T = h.T, ne = rec[F_NE], B = h.B, dT = h.dT, dne = trec[F_NE], invk = h.invk, dinvk = h.dinvk;
   const float xpm = 1.4387769f / lam_mid;
   const float Em = fexp(xpm / T);
   const float plm = (float)(2.0 * 6.62606957 * 8.9875517E-7) / (lam_mid * lam_mid * lam_mid * lam_mid * lam_mid) / (Em - 1.0f);
@@ -108,14 +117,14 @@ SNAPI_HD void depth_precompute_jvp(const float *rec, const float *trec, int nlin
 // H, Hx, Ha.  The cell's basis holds them in line order; the W4 work of a cell is done once for
 // all directions and each direction's tangent costs a few multiply-adds per line.
 SNAPI_HD int jvp_basis_size(const LineConst *lc, int nlines) {
-  int n = 0;
+  int n = 3;  // + the H- factors exp(-xs / T), 10^f(log theta), exp(xp / T), one more task
   for (int j = 0; j < nlines; ++j) n += lc[j].split ? 24 : 3;
   return n;
 }
 
 // the basis is filled by tasks: one per (split line, group) and one per unsplit line
 SNAPI_HD int jvp_basis_tasks(const LineConst *lc, int nlines) {
-  int n = 0;
+  int n = 1;
   for (int j = 0; j < nlines; ++j) n += lc[j].split ? 3 : 1;
   return n;
 }
@@ -130,6 +139,12 @@ SNAPI_HD void jvp_basis_task(const DepthConst &d, const LineDepth *ld, const Lin
     if (k < nt) break;
     k -= nt;
     off += lc[j].split ? 24 : 3;
+  }
+  if (j == nlines) {  // the H- bound-free / free-free factors of the cell
+    B[off] = fexp(-lam.xs * d.invT);
+    B[off + 1] = fexp(kLn10 * (lam.F0 + lam.f1 * d.lt + lam.f2 * d.lt * d.lt));
+    B[off + 2] = fexp(lam.xp * d.invT);
+    return;
   }
   const LineConst &L = lc[j];
   const LineDepth &q = ld[j];
@@ -221,16 +236,16 @@ SNAPI_HD void cell_opacity_jvp(const DepthConst &d, const LineDepth *ld, const L
       djj[3] += deV * q.emn + eV * t.emn;
     }
   }
-  // H- bound-free + free-free and their LTE emissivity
-  const float e1 = fexp(-lam.xs * d.invT);
+  // H- bound-free + free-free and their LTE emissivity (the exponentials from the basis)
+  const float e1 = B[off];
   const float de1 = -lam.xs * e1 * dd.invT;
   const float opbf = lam.afud * d.hb * (1.0f - e1);
   const float dopbf = lam.afud * (dd.hb * (1.0f - e1) - d.hb * de1);
-  const float E10 = fexp(kLn10 * (lam.F0 + lam.f1 * d.lt + lam.f2 * d.lt * d.lt));
+  const float E10 = B[off + 1];
   const float dE10 = E10 * kLn10 * (lam.f1 + 2.0f * lam.f2 * d.lt) * dd.lt;
   const float opff = d.hf * E10, dopff = dd.hf * E10 + d.hf * dE10;
   const float oph = opbf + opff, doph = dopbf + dopff;
-  const float Ep = fexp(lam.xp * d.invT);
+  const float Ep = B[off + 2];
   const float dEp = lam.xp * Ep * dd.invT;
   const float pl = lam.pp / (Ep - 1.0f), dpl = -pl / (Ep - 1.0f) * dEp;
   deta[0] += doph;
