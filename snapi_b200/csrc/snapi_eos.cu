@@ -49,6 +49,8 @@ constexpr int kER = 32;                   // stages whose ionisation fraction is
 constexpr int kEL = 64;                   // levels whose population enters a record
 constexpr int kEB = 32;                   // bound-free levels
 constexpr int kEP = SNAPI_EOS_MAX_PAR;    // nodes
+constexpr int kEBm = 8;                    // bound-free edges of the march's opacity (compact path)
+constexpr int kELm = 16;                   // their levels
 constexpr int kRecThreads = 64;
 constexpr int kPolishCap = 400;
 
@@ -80,6 +82,12 @@ struct EosDev {
   // (-1: an atom in no molecule, eliminated); simple[0..nsimple) those atoms' full indices
   int nr, nsimple;
   int rfull[kEA + 1], rmap[kEA + 1], simple[kEA];
+  int nmref, mrefs[kER];  // the kept-fraction slots that molecule components read
+  // the hydrostatic march's opacity (continuum at lambda_he): its LTE bound-free edges and the
+  // levels they read, compact (mfast = 0: more than the compact lists hold, the general path)
+  int mfast, nbf_m, nlev_m;
+  int bf_m[kEBm], bfl_m[kEBm], bfn_m[kEBm];  // bound-free index, its level and next-stage ground in lev_m
+  int lev_m[kELm];                           // level slots
   // stages
   int pft[kES];
   double pfv[kES];   // CONST: value; TRAV: g0; NONE: 1
@@ -148,6 +156,9 @@ struct Chem {
   } sl[kES];
   double w2[kET];   // g2 exp(-2.302585 ee x)
   double iKkT[kEM];  // 1 / (K_m k T) of each molecule at this T
+  // the march's opacity factors at this T (set_march): stimulated emission, each edge's
+  // saha T^-1.5 g / g_next exp(chi / kT), each level's g exp(-E / kT), the H- bf + ff factor
+  double mstim, mhm, mcb[kEBm], mlf[kELm];
   double Ea[kEA + 1], Da[kEA + 1];  // sum_i i f_i, sum_i i df_i / dNe per atom (1-based)
   double fr[kER], dr[kER];          // kept ionisation fractions and their Ne derivatives
   double N[kEA + 1];
@@ -203,6 +214,35 @@ struct Chem {
         k = E.mcoef[m][0];
       }
       iKkT[m] = 1.0 / (k * kT);
+    }
+  }
+
+  // the T-only factors of the march's opacity (continuum at lambda_he, atmos_rad.cc:286-294 and
+  // mol.cc's H- bound-free / free-free) for the compact path of chem_point
+  __device__ void set_march() {
+    const double lambda = E.lambda_he;
+    mstim = exp(-cH * cC / lambda / cK / T);
+    for (int k = 0; k < E.nbf_m; ++k) {
+      const int b = E.bf_m[k];
+      mcb[k] = cSAHA * pow(T, -1.5) * E.bfg[b] / E.bfgn[b] * exp(E.bfip[b] / cK / T);
+    }
+    for (int k = 0; k < E.nlev_m; ++k) {
+      const int l = E.lev_m[k];
+      mlf[k] = E.lg[l] != 0.0 ? E.lg[l] * exp(-E.lee[l] / (cK * T)) : 0.0;
+    }
+    mhm = 0.0;
+    if (E.hm) {
+      const double ca[7] = {1.99654, -1.18267E-5, 2.64243E-6, -4.40524E-10, 3.23992E-14, -1.39568E-18, 2.78701E-23};
+      double alpha = 0.0;
+      for (int i = 0; i < 7; ++i) alpha += ca[i] * pow(lambda * 1E8, (double)i);
+      const double T_P = 5040. / T;
+      const double l = log10(lambda * 1E8);
+      const double f_0 = -2.2763 - 1.6850 * l + 0.76661 * l * l - 0.053346 * l * l * l;
+      const double f_1 = 15.2827 - 9.2846 * l + 1.99381 * l * l - 0.142631 * l * l * l;
+      const double f_2 = -197.789 + 190.266 * l - 67.9775 * l * l + 10.6913 * l * l * l - 0.625151 * l * l * l * l;
+      const double lt = log10(T_P);
+      mhm = 4.158E-28 * alpha * cK * T * pow(T_P, 2.5) * pow(10.0, 0.754 * T_P) * (1.0 - mstim) +
+            1E-26 * cK * T * pow(10.0, f_0 + f_1 * lt + f_2 * lt * lt);
     }
   }
 
@@ -474,7 +514,9 @@ struct Chem {
       double Nr = N[1];
       double Nc[kEA + 1], iN[kEA + 1];
       for (int a = 2; a <= na; ++a) Nc[a] = N[a];
-      for (int a = 0; a <= na; ++a) iN[a] = 1.0 / N[a];
+      double dlf[kER];  // dr / fr of the kept fractions the molecules use
+      for (int k = 0; k < nr; ++k) iN[E.rfull[k]] = 1.0 / N[E.rfull[k]];
+      for (int k = 0; k < E.nmref; ++k) dlf[E.mrefs[k]] = dr[E.mrefs[k]] / fr[E.mrefs[k]];
       double gr0 = 0.0;
       for (int m = 0; m < nm; ++m) {
         double nmv = iKkT[m], dm0 = 0.0;
@@ -487,7 +529,7 @@ struct Chem {
           } else {
             const int r = E.mref[m][i];
             nmv *= fr[r] * N[a] * kT;
-            dm0 += dr[r] / fr[r];
+            dm0 += dlf[r];
           }
         }
         dm0 *= nmv;
@@ -734,8 +776,28 @@ __device__ double continuum(const EosDev &E, const Chem &c, const double *lev, d
 // T-only tables are rebuilt only when T changes (the hydrostatic iterations of one depth share T).
 __device__ double chem_point(const EosDev &E, Chem &c, double T, double Nt, double *lev, double &nH0, int which,
                              bool warm = false) {
-  if (T != c.T) c.set_T(T);
+  const bool fast = which == 0 && E.mfast;
+  if (T != c.T) {
+    c.set_T(T);
+    if (fast) c.set_march();
+  }
   c.solve(Nt, warm);
+  if (fast) {  // the march: the levels of the LTE bound-free edges at lambda_he only
+    const double ne = c.N[0], pne = cbrt(sqrt(ne)), ine = 1.0 / ne, ipne = 1.0 / pne;
+    double lm[kELm];
+    for (int k = 0; k < E.nlev_m; ++k) {
+      const int l = E.lev_m[k], st = E.lst[l];
+      double U, dU;
+      c.stage_u<false>(st, ine, pne, ipne, U, dU);
+      const double tot = c.stage_total(st, E.satom[st]);
+      lm[k] = E.lg[l] != 0.0 ? tot * (c.mlf[k] / U) : tot;
+    }
+    nH0 = c.stage_total(E.s0[0], 0);
+    double op = 6.65E-25 * ne;
+    for (int k = 0; k < E.nbf_m; ++k)
+      op += E.sig_he[E.bf_m[k]] * (lm[E.bfl_m[k]] - lm[E.bfn_m[k]] * ne * c.mcb[k] * c.mstim);
+    return op + c.mhm * ne * nH0;
+  }
   for (int l = 0; l < E.nlev; ++l) lev[l] = c.level_pop(l, c.stage_U(E.lst[l], c.N[0]));
   nH0 = c.stage_total(E.s0[0], 0);
   return continuum(E, c, lev, nH0, which);
@@ -1320,6 +1382,29 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
     }
   }
   H.nbf = nbf;
+  {  // the march's compact opacity lists
+    H.mfast = 1;
+    H.nbf_m = H.nlev_m = 0;
+    auto mslot = [&](int l) -> int {
+      for (int k = 0; k < H.nlev_m; ++k)
+        if (H.lev_m[k] == l) return k;
+      if (H.nlev_m >= kELm) return -1;
+      H.lev_m[H.nlev_m] = l;
+      return H.nlev_m++;
+    };
+    for (int b = 0; b < nbf && H.mfast; ++b) {
+      if (!H.bflte[b] || H.sig_he[b] == 0.0) continue;
+      const int kl = mslot(H.bfl[b]), kn = mslot(H.bfn[b]);
+      if (kl < 0 || kn < 0 || H.nbf_m >= kEBm) {
+        H.mfast = 0;
+        break;
+      }
+      H.bf_m[H.nbf_m] = b;
+      H.bfl_m[H.nbf_m] = kl;
+      H.bfn_m[H.nbf_m] = kn;
+      ++H.nbf_m;
+    }
+  }
   for (int j = 0; j < ctx->nlines; ++j) {
     const snapi_eos_line &L = m->lines[j];
     if (L.atom < 0 || L.atom >= m->natom || L.stage < 0 || L.stage >= m->atoms[L.atom].nstage || L.lower < 0 ||
@@ -1345,6 +1430,14 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
     inmol[0] = inmol[1] = true;
     for (int mm = 0; mm < m->nmol; ++mm)
       for (int i = 0; i < H.mnc[mm]; ++i) inmol[H.matom[mm][i]] = true;
+    H.nmref = 0;
+    bool seen[kER] = {};
+    for (int mm = 0; mm < m->nmol; ++mm)
+      for (int i = 0; i < H.mnc[mm]; ++i)
+        if (H.matom[mm][i] > 0 && !seen[H.mref[mm][i]]) {
+          seen[H.mref[mm][i]] = true;
+          H.mrefs[H.nmref++] = H.mref[mm][i];
+        }
     H.nr = H.nsimple = 0;
     for (int b = 0; b <= m->natom; ++b) {
       if (inmol[b]) {
