@@ -525,7 +525,15 @@ cudaError_t snapi::launch_synth(const snapi_ctx *ctx, const KParams &P) {
   k_synth<<<P.npix * ctx->nchunk, kChunk, L.total, ctx->stream>>>(P);
   return cudaGetLastError();
 }
-cudaError_t snapi::launch_responses(const snapi_ctx *ctx, const KParams &P) {
+cudaError_t snapi::launch_synth_state(const snapi_ctx *ctx, const KParams &P) {
+  const SmemLayout L = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false);
+  KParams Q = P;
+  Q.scratch = ctx->d_scratch;
+  Q.nvar = 1;
+  k_resp_state<<<P.npix * ctx->nchunk, kChunk, L.total, ctx->stream>>>(Q);
+  return cudaGetLastError();
+}
+cudaError_t snapi::launch_responses(const snapi_ctx *ctx, const KParams &P, bool state_ready) {
   const SmemLayout L = smem_layout(ctx->nd, ctx->nfield, ctx->nlines, ctx->ncomp, ctx->nred, false);
   if (ctx->jac_tangent) {  // forward-mode sweeps (the state in the adjoint's scratch)
     KParams Q = P;
@@ -543,9 +551,11 @@ cudaError_t snapi::launch_responses(const snapi_ctx *ctx, const KParams &P) {
       R.tangent = P.tangent + (size_t)p0 * P.npar * nrec;
       R.dstokes = P.dstokes + (size_t)p0 * P.npar * ctx->nl * 4;
       R.skip = P.skip ? P.skip + p0 : nullptr;
-      k_resp_state<<<R.npix * ctx->nchunk, kChunk, L.total, ctx->stream>>>(R);
-      cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess) return e;
+      cudaError_t e = cudaSuccess;
+      if (!(state_ready && P.npix <= ctx->max_batch)) {
+        k_resp_state<<<R.npix * ctx->nchunk, kChunk, L.total, ctx->stream>>>(R);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      }
       launch_jvp(R.npix * ((ctx->nl + 31) / 32) * ngrp, nwarp, smem, ctx->stream, R);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }

@@ -376,7 +376,10 @@ void tune_store_adj(snapi_ctx *ctx, int npix, const AdjCfg &cfg);
 void tune_store_build(snapi_ctx *ctx, int npix, const BuildCfg &cfg);
 // sweep launches for other translation units (P.npix pixels; P.nvar nodes for the responses)
 cudaError_t launch_synth(const snapi_ctx *ctx, const KParams &P);
-cudaError_t launch_responses(const snapi_ctx *ctx, const KParams &P);
+// the synthesis that also stores the forward state of every pixel in the context's scratch
+// (P.npix <= max_batch), so that launch_responses with state_ready skips its own state pass
+cudaError_t launch_synth_state(const snapi_ctx *ctx, const KParams &P);
+cudaError_t launch_responses(const snapi_ctx *ctx, const KParams &P, bool state_ready = false);
 void lm_free(snapi_ctx *ctx);  // LM work buffers (snapi_lm.cu)
 void eos_free(snapi_ctx *ctx); // node-model tables and work buffers (snapi_eos.cu)
 // the context has a node model with these npar node kinds (snapi_eos.cu)

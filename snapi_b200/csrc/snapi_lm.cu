@@ -66,6 +66,9 @@ struct LmWork {
   int *d_act_out = nullptr;
   std::vector<int> h_active, kind;
   double broaden = 0.0;  // Gaussian instrumental width [cm], 0: none
+  // the last evaluation stored the forward state of its pixels (forward-mode Jacobian): the
+  // Jacobian of the accepted pixels, evaluated at the same nodes, starts from it
+  bool state_ready = false;
 };
 
 __device__ double block_sum_d(double v, double *sh) {
@@ -316,7 +319,10 @@ cudaError_t lm_eval_phase(snapi_ctx *ctx, LmWork *w, const float *rec) {
   P.rec = rec;
   P.stokes = w->d_snew;
   P.skip = w->d_skip_syn;
-  cudaError_t e = launch_synth(ctx, P);
+  // forward-mode Jacobian: the synthesis at the requested nodes stores its sweep state, which the
+  // Jacobian of the pixels it accepts reuses (their nodes are the requested ones)
+  w->state_ready = ctx->jac_tangent && w->npix <= ctx->max_batch;
+  cudaError_t e = w->state_ready ? launch_synth_state(ctx, P) : launch_synth(ctx, P);
   if (e != cudaSuccess) return e;
   if (w->broaden > 0.0 && (e = psf_launch(ctx, w->d_snew, w->npix, 1, w->d_skip_syn)) != cudaSuccess) return e;
   k_lm_eval<<<w->npix, kLmThreads, 0, ctx->stream>>>(w->D);
@@ -353,7 +359,7 @@ cudaError_t lm_solve_phase(snapi_ctx *ctx, LmWork *w, const float *rec, const fl
     R.fd_step = w->d_step;
     R.dstokes = w->d_J;
     R.skip = w->d_skip_resp;
-    e = launch_responses(ctx, R);
+    e = launch_responses(ctx, R, w->state_ready);
   }
   if (e != cudaSuccess) return e;
   if (w->broaden > 0.0 && (e = psf_launch(ctx, w->d_J, npix * npar, npar, w->d_skip_resp)) != cudaSuccess) return e;
