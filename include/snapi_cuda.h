@@ -260,7 +260,9 @@ double snapi_ali_last_kernel_ms(const snapi_ali_ctx *ctx);
  * [16][K] (row-major, float32, device memory), G [nmat][16][16] float32 (device).  tcgen05 MMA with a
  * three-product TF32 split (hi hi^T + hi lo^T + lo hi^T), FP32 accumulation: ~1e-6 relative.  This
  * is how snapi_lm_step forms J^T J and J^T r (atmos_fit.cc:135-137) for up to 15 nodes; exported for
- * callers with their own small normal equations.  stream: a cudaStream_t or NULL. */
+ * callers with their own small normal equations.  stream: a cudaStream_t or NULL.  The call
+ * allocates nothing (its status word is a static device word, shared by calls that overlap on a
+ * GPU) and waits for its stream once. */
 int snapi_batched_gram(int nmat, int K, const float *M, float *G, void *stream);
 
 /* Gaussian instrumental broadening in place: spectra [nvec][nlambda][4] on the context's wavelength
@@ -528,8 +530,9 @@ int snapi_fma_peak(int device, int fp64, double *tflops);
  * and returns when the results are in place.  Pixels are processed in batches that fit the static
  * array; a problem whose single pixel does not fit (at nd = 80 and 201 wavelengths one pixel needs
  * ~1.4 MB) is rejected with SNAPI_EINVAL.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream capture.  Calls share
- * the array and the kernels' shared-memory limits: calls that overlap on the GPU race.
+ * address (cudaGetSymbolAddress).  Every call synchronizes its stream, so none can be captured
+ * into a CUDA graph.  Calls share the array and the kernels' shared-memory limits: calls that
+ * overlap on the GPU race.
  * On error, snapi_noalloc_last_error() (per host thread) describes it. */
 #define SNAPI_STATIC_SCRATCH_BYTES (64u << 20)
 int snapi_adjoint_noalloc(const snapi_problem *prob, int device, void *stream, int npix, const float *records,

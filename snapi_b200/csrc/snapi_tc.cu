@@ -169,22 +169,26 @@ cudaError_t launch_gram_tf32(const float *M, int nmat, int K, float *G, int *sta
 
 }  // namespace snapi
 
+namespace {
+// the bounded-wait status word of snapi_batched_gram (one per device that loads the library;
+// calls that overlap on a GPU share it)
+__device__ int g_gram_status;
+}  // namespace
+
 extern "C" {
 
 int snapi_batched_gram(int nmat, int K, const float *M, float *G, void *stream) {
   if (nmat < 0 || K < 1 || (nmat > 0 && (!M || !G))) return SNAPI_EINVAL;
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
   int *status = nullptr;
-  // a small device word for the bounded-wait status
-  if (cudaMallocAsync(&status, sizeof(int), static_cast<cudaStream_t>(stream)) != cudaSuccess) return SNAPI_ENOMEM;
-  cudaMemsetAsync(status, 0, sizeof(int), static_cast<cudaStream_t>(stream));
-  cudaError_t e = snapi::launch_gram_tf32(M, nmat, K, G, status, static_cast<cudaStream_t>(stream));
-  int st = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream));
-  if (e == cudaSuccess) e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
-  cudaFreeAsync(status, static_cast<cudaStream_t>(stream));
-  cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+  if (cudaGetSymbolAddress(reinterpret_cast<void **>(&status), g_gram_status) != cudaSuccess) return SNAPI_ECUDA;
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = snapi::launch_gram_tf32(M, nmat, K, G, status, st);
+  int word = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&word, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return SNAPI_ECUDA;
-  return st ? st : SNAPI_OK;
+  return word ? word : SNAPI_OK;
 }
 
 }  // extern "C"
