@@ -22,6 +22,9 @@
 //   snapi_ref_dump ali    <task.tsk> <nodes.f64> <ncol> <niter> <out.sbin>
 //       NLTE level-population iteration inputs, niter iterations of the reference's loop, and the
 //       populations nltepops converges to (see do_ali).
+//   snapi_ref_dump alisetup <task.tsk> <nodes.f64> <ncol> <out.sbin>
+//       The tables of nltepops' population-independent set-up (background opacity, collisional
+//       rates, line damping) and the columns of ncol node vectors (see do_alisetup).
 //
 // flags: 1 = responses, 2 = tangents, 4 = opacity probe (pixel 0 only)
 //
@@ -696,6 +699,143 @@ static int do_ali(const char *tskname, const char *nodesname, int ncol, int nite
   return 0;
 }
 
+struct Rd {  // little-endian reader over a packed object
+  const uint8_t *p;
+  int i8() { int8_t v; memcpy(&v, p, 1); p += 1; return v; }
+  int u8() { uint8_t v; memcpy(&v, p, 1); p += 1; return v; }
+  int i32() { int32_t v; memcpy(&v, p, 4); p += 4; return v; }
+  double f64() { double v; memcpy(&v, p, 8); p += 8; return v; }
+};
+
+// ----------------------------------------------------------------------------------------------
+// alisetup: the tables of the population-independent part of atmosphere::nltepops (atmos_pop.cc:
+// 67-240) -- the LTE background of opacity_lte (atmos_rad.cc:225-235: every LTE atom's free-free,
+// Rayleigh, bound-free and bound-bound opacity, atom_rad.cc:203-535, and H- bound-free / free-free,
+// mol.cc:516-632), the NLTE atom's collisional rates (atom_rad.cc:1769-1901) and line damping -- in
+// the atom order of the eos mode, and the columns (return_as_array rows after build_from_nodes and
+// compute_op_referent) of ncol node vectors.
+static int do_alisetup(const char *tskname, const char *nodesname, int ncol, const char *outname) {
+  const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
+  const char *options[] = CMDOPTS, *maps[] = CMDMAPS;
+  int ac = 4; cmdln cmd(ac, (char **)argv, options, maps);
+  io_class io(cmd);
+  Task t = load_task(tskname);
+  std::vector<uint8_t> nb = read_file_bytes(nodesname);
+  const double *nodes = (const double *)nb.data();
+  model *m = task_model(t, io);
+  const int np = m->get_N_nodes_total();
+  atmosphere *a = task_atmos(t, io);
+  set_nodes(m, nodes);
+  a->build_from_nodes(m);
+  a->set_grid(a->tau_grid);
+  a->popsetup();
+  a->compute_op_referent();
+  a->ltepops();
+  fp_t *lambda = 0;
+  int32_t nlambda = 0;
+  for (int i = 0; i < a->natm; ++i) a->atml[i]->rtsetup(a->x1l, a->x1h, a->x2l, a->x2h, a->x3l, a->x3h);
+  for (int i = 0; i < a->natm; ++i)
+    lambda = a->atml[i]->getlambda(lambda, nlambda, a->T[1][1][a->x3h], a->Nt[1][1][a->x3h], a->Ne[1][1][a->x3h]);
+  std::vector<atom *> atoms;
+  for (int i = 0; i < a->natm; ++i)
+    if (atom *at = dynamic_cast<atom *>(a->atml[i])) atoms.push_back(at);
+  int inlte = -1;
+  for (size_t ia = 0; ia < atoms.size(); ++ia)
+    if (atoms[ia]->check_if_nlte()) inlte = ia;
+  if (inlte < 0 || !nlambda) { fprintf(stderr, "no NLTE atom / wavelengths\n"); return 4; }
+  // background: bound-free levels and bound-bound pairs of the LTE atoms, Rayleigh atoms (Z == 1)
+  std::vector<double> bfl, bfs, bb, ray;
+  for (size_t ia = 0; ia < atoms.size(); ++ia) {
+    atom *at = atoms[ia];
+    if (at->check_if_nlte()) continue;
+    if (at->Z == 1) ray.push_back(ia);
+    for (int z = 0; z < at->Z; ++z)
+      for (int l = 0; l < at->nl[z]; ++l) {
+        if (!at->bf[z][l]) continue;
+        double v[3] = {(double)ia, (double)z, (double)l};
+        bfl.insert(bfl.end(), v, v + 3);
+        for (int q = 0; q < nlambda; ++q) bfs.push_back(at->bf[z][l]->U(lambda[q]));
+      }
+    for (int z = 0; z <= at->Z; ++z)
+      for (int up = 1; up < at->nl[z]; ++up)
+        for (int lo = 0; lo < up; ++lo) {
+          double v[11] = {(double)ia, (double)z, (double)lo, (double)up, h * c / (at->ee[z][up] - at->ee[z][lo]),
+                          at->B[z][lo][up], at->B[z][up][lo], at->damp_rad(at->A[z], lo, up),
+                          at->alpha_col_dam[z][up][lo], at->col_dam_cross_section[z][up][lo], at->mass};
+          bb.insert(bb.end(), v, v + 11);
+        }
+  }
+  // the NLTE atom: mapped levels, line damping, edge cross-sections, collisional tables
+  atom *at = atoms[inlte];
+  const int nmap = at->nmap;
+  std::vector<double> lev, line, sedge, cn(nmap * nmap, 0.0), ct(nmap * nmap * 8, 0.0), cv(nmap * nmap * 8, 0.0);
+  for (int i = 0; i < nmap; ++i) {
+    const int z = at->zmap[i], l = at->lmap[i];
+    lev.push_back(z); lev.push_back(l);
+    double se = 0.0;
+    if (z < at->Z) se = at->bf[z][l] ? at->bf[z][l]->U(h * c / (at->ip[z] - at->ee[z][l])) : -1.0;
+    sedge.push_back(se);
+  }
+  for (int tr = 1; tr <= at->ntr; ++tr) {
+    const int z = at->inverse_tmap[tr][2], lo = at->inverse_tmap[tr][3], up = at->inverse_tmap[tr][4];
+    if (up >= at->nl[z]) continue;
+    double v[4] = {at->alpha_col_dam[z][up][lo], at->col_dam_cross_section[z][up][lo], at->mass,
+                   at->damp_rad(at->A[z], lo, up)};
+    line.insert(line.end(), v, v + 4);
+  }
+  for (int i = 0; i < nmap; ++i)
+    for (int j = 0; j < nmap; ++j) {
+      const int zi = at->zmap[i], li = at->lmap[i], zj = at->zmap[j], lj = at->lmap[j];
+      if (zi != zj || li == lj || li >= at->nl[zi] || lj >= at->nl[zj]) continue;
+      colr *C = at->cr[zi][li > lj ? li : lj][li > lj ? lj : li];
+      // the table, read back from the object's own wire format (colr::pack / tbcr::pack, colr.cc:46-99)
+      std::vector<uint8_t> pb(C->size(io) + 64);
+      C->pack(pb.data(), 0, io);
+      Rd r{pb.data()};
+      if (r.i8() != COLR_TYPE_TAB) continue;
+      const int n = r.i32();
+      if (n > 8) { fprintf(stderr, "collision table too long\n"); return 2; }
+      cn[i * nmap + j] = n;
+      for (int q = 0; q < n; ++q) ct[(i * nmap + j) * 8 + q] = r.f64();
+      for (int q = 0; q < n; ++q) cv[(i * nmap + j) * 8 + q] = r.f64();
+    }
+  const double meta[4] = {(double)inlte, (double)at->Z, (double)nlambda, (double)nmap};
+  delete a;
+  // the columns
+  std::vector<double> harr;
+  int nd = 0;
+  for (int ic = 0; ic < ncol; ++ic) {
+    atmosphere *b = task_atmos(t, io);
+    set_nodes(m, nodes + ic * np);
+    b->build_from_nodes(m);
+    b->set_grid(b->tau_grid);
+    b->popsetup();
+    b->compute_op_referent();
+    fp_t **arr = b->return_as_array();
+    nd = b->x3h - b->x3l + 1;
+    for (int q = 1; q <= 12; ++q)
+      for (int i = 1; i <= nd; ++i) harr.push_back(arr[q][i]);
+    del_ft2dim(arr, 1, 12, 1, nd);
+    delete b;
+  }
+  SbinWriter w(outname);
+  w.put("alis_meta", {4}, meta);
+  w.put("alis_bf", {(int64_t)bfl.size() / 3, 3}, bfl.data());
+  w.put("alis_bfsig", {(int64_t)bfl.size() / 3, nlambda}, bfs.data());
+  w.put("alis_bb", {(int64_t)bb.size() / 11, 11}, bb.data());
+  w.put("alis_ray", {(int64_t)ray.size()}, ray.data());
+  w.put("alis_lev", {nmap, 2}, lev.data());
+  w.put("alis_line", {(int64_t)line.size() / 4, 4}, line.data());
+  w.put("alis_sedge", {nmap}, sedge.data());
+  w.put("alis_coll_n", {nmap, nmap}, cn.data());
+  w.put("alis_coll_t", {nmap, nmap, 8}, ct.data());
+  w.put("alis_coll_v", {nmap, nmap, 8}, cv.data());
+  w.put("alis_atm", {ncol, 12, nd}, harr.data());
+  delete[] lambda;
+  delete m;
+  return 0;
+}
+
 // ----------------------------------------------------------------------------------------------
 // conv: the reference's Gaussian instrumental broadening (convolve_spectra_with_gauss,
 // cmlib/mathtools.cc:1350-1414) of nvec Stokes spectra.  in.f64: lambda [n], then S [nvec][n][4];
@@ -730,14 +870,6 @@ static int do_conv(const char *inname, int n, int nvec, double width, const char
 // atom.cc:779-787, atmos_rad.cc:286-294); and, per node vector, the column build_from_nodes leaves
 // (T, Nt, n_e, kappa at lambda_referent, rho).  Array layout: see tests/golden/make_golden.py.
 static const int EMS = 12, EMT = 8, EMC = 8, EML = 16;
-
-struct Rd {  // little-endian reader over a packed object
-  const uint8_t *p;
-  int i8() { int8_t v; memcpy(&v, p, 1); p += 1; return v; }
-  int u8() { uint8_t v; memcpy(&v, p, 1); p += 1; return v; }
-  int i32() { int32_t v; memcpy(&v, p, 4); p += 4; return v; }
-  double f64() { double v; memcpy(&v, p, 8); p += 8; return v; }
-};
 
 static int do_eos(const char *tskname, const char *nodesname, int npix, const char *outname) {
   const char *argv[] = {"snapi_ref_dump", "-q", "-q", "-q", 0};
@@ -1148,6 +1280,7 @@ int main(int argc, char **argv) {
     return do_conv(argv[2], atoi(argv[3]), atoi(argv[4]), atof(argv[5]), argv[6]);
   if (argc >= 7 && !strcmp(argv[1], "ali"))
     return do_ali(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]), argv[6]);
+  if (argc >= 6 && !strcmp(argv[1], "alisetup")) return do_alisetup(argv[2], argv[3], atoi(argv[4]), argv[5]);
   if (argc >= 9 && !strcmp(argv[1], "lmfit"))
     return do_lmfit(argv[2], argv[3], argv[4], argv[5], atoi(argv[6]), atoi(argv[7]), argv[8],
                     argc >= 10 ? atof(argv[9]) : 0.0);

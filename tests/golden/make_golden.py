@@ -32,6 +32,12 @@ its 80-depth atmosphere file from REF and runs oracle/_ref/snapi_ref_dump).  Wri
                                   job applies to it (read_file + transpose + normalize + extract)
                                   and the cube_to_invert.f0 it writes; the node and spectra cubes
                                   its write_file calls produce from given arrays
+  tests/golden/config5.npz, config5_spec.npz  (--only-c5 [--spec]) NLTE Ca II columns: the
+                                  level-population iteration's inputs and the reference's
+                                  iterates; with the set-up tables (alis_*: background
+                                  bound-free / bound-bound lists, collisional tables, line
+                                  damping, the columns' return_as_array rows; eos_*: the task's
+                                  atom tables).  --only-c5-setup adds those to an existing one
 
 Synthetic inputs stand in for observations: seeded numpy generators with the shapes and value
 distributions of the benchmark configurations (no dataset is read).
@@ -330,15 +336,10 @@ def write_atmos_resampled(src, dst, nd):
             f.write(" ".join("%.6e" % v for v in r) + "\n")
 
 
-def make_config5(tmp, ncol, niter=3, spec=False):
-    """NLTE Ca II (config 5): the inputs of the level-population iteration per column, the
-    populations after each of the reference's first niter iterations, and the populations its
-    nltepops converges to.  Columns: the ten-node model with seeded T / v_los / B (seed 5).
-    Default: the reference as compiled (2 rays, the 1e-2 stop) on the 80-depth grid
-    (config5.npz).  spec: the configuration's stated settings (config5_spec.npz) -- the patched
-    reference build (the 5-point angle set, i.e. 10 ray directions, and a 1e-4 population stop)
-    on a 100-depth grid; the background opacity / emissivity stored as float32 to keep the fixture
-    small (the device takes them as float64; ~6e-8 relative)."""
+def config5_task(tmp, spec=False):
+    """Write and pack the config-5 task in tmp (c5.tsk); returns the dump binary and the fixture
+    name.  Default: the reference as compiled on the 80-depth grid; spec: the patched build on the
+    100-depth grid (see make_config5)."""
     with open(os.path.join(tmp, "atoms_c5.cfg"), "w") as f:
         f.write("".join("ATOM=%s\n" % a for a in C5_ATOMS))
     dump_bin, name, afile = DUMP, "config5", "falc_80z.dat"
@@ -348,6 +349,34 @@ def make_config5(tmp, ncol, niter=3, spec=False):
     write_cfg(os.path.join(tmp, "c5.cfg"), C3_TTAU, C3_TRUTH[:4], C3_VSTAU, C3_TRUTH[5:7], atoms="atoms_c5.cfg",
               lam="8538.5-8545.985", dlam=0.025, atmos_file=afile)
     run([dump_bin, "pack", "c5.cfg", "c5.tsk"], tmp)
+    return dump_bin, name
+
+
+def config5_setup_arrays(tmp, dump_bin, nodes):
+    """The tables of nltepops' population-independent set-up and the columns of the node vectors
+    (snapi_ref_dump alisetup: alis_*), and the task's atom / molecule tables with the reference's
+    chemistry (snapi_ref_dump eos: eos_*) -- the inputs of the device set-up (snapi_ali_setup)."""
+    nf = os.path.join(tmp, "c5s_nodes.f64")
+    np.ascontiguousarray(nodes, dtype="<f8").tofile(nf)
+    out = {}
+    run([dump_bin, "alisetup", "c5.tsk", nf, str(nodes.shape[0]), os.path.join(tmp, "c5s.sbin")], tmp)
+    out.update(read_sbin(os.path.join(tmp, "c5s.sbin")))
+    run([dump_bin, "eos", "c5.tsk", nf, "0", os.path.join(tmp, "c5e.sbin")], tmp)
+    out.update({"eos_" + k: v for k, v in read_sbin(os.path.join(tmp, "c5e.sbin")).items()})
+    return out
+
+
+def make_config5(tmp, ncol, niter=3, spec=False):
+    """NLTE Ca II (config 5): the inputs of the level-population iteration per column, the
+    populations after each of the reference's first niter iterations, and the populations its
+    nltepops converges to.  Columns: the ten-node model with seeded T / v_los / B (seed 5).
+    Default: the reference as compiled (2 rays, the 1e-2 stop) on the 80-depth grid
+    (config5.npz).  spec: the configuration's stated settings (config5_spec.npz) -- the patched
+    reference build (the 5-point angle set, i.e. 10 ray directions, and a 1e-4 population stop)
+    on a 100-depth grid; the background opacity / emissivity stored as float32 to keep the fixture
+    small (the device takes them as float64; ~6e-8 relative).  Also the set-up tables
+    (config5_setup_arrays)."""
+    dump_bin, name = config5_task(tmp, spec)
     if not spec:
         shutil.copy(os.path.join(tmp, "c5.tsk"), os.path.join(HERE, "c5.tsk"))
     nodes = config3_nodes(ncol, seed=5)
@@ -359,12 +388,23 @@ def make_config5(tmp, ncol, niter=3, spec=False):
     if spec:
         for k in ("ali_bgop", "ali_bgem"):
             d[k] = d[k].astype(np.float32)
+    d.update(config5_setup_arrays(tmp, dump_bin, nodes))
     # the reference's synthesis of the 8542 window with those NLTE populations (obs_stokes runs
     # nltepops itself) and the column records the device synthesis takes
     s = dump(tmp, os.path.join(tmp, "c5.tsk"), nodes, 0, "c5syn", dump_bin=dump_bin)
     np.savez_compressed(os.path.join(HERE, name + ".npz"), nodes=nodes, **{k: v for k, v in d.items()},
                         lambda_air=s["lambda_air"], tau500=s["tau500"], record=s["record"], stokes=s["stokes"],
                         ref_synth_seconds=s["ref_seconds_per_pixel"], **line_arrays(s))
+
+
+def add_config5_setup(tmp, spec=False):
+    """Add the set-up arrays (config5_setup_arrays) to an existing config-5 fixture, for its node
+    vectors, without running the reference's iterations again (make_config5 writes the same)."""
+    dump_bin, name = config5_task(tmp, spec)
+    path = os.path.join(HERE, name + ".npz")
+    d = dict(np.load(path))
+    d.update(config5_setup_arrays(tmp, dump_bin, d["nodes"]))
+    np.savez_compressed(path, **d)
 
 
 def make_psf(tmp):
@@ -400,6 +440,8 @@ def main():
     ap.add_argument("--c4pix", type=int, default=8)
     ap.add_argument("--only-c5", action="store_true")
     ap.add_argument("--only-psf", action="store_true")
+    ap.add_argument("--only-c5-setup", action="store_true",
+                    help="add the NLTE set-up tables to the existing config-5 fixture (--spec: config5_spec)")
     ap.add_argument("--only-eos", action="store_true")
     ap.add_argument("--only-f0", action="store_true")
     ap.add_argument("--only-spinor", action="store_true")
@@ -418,6 +460,9 @@ def main():
             shutil.copy(os.path.join(a.ref, "cfg", f), tmp)
         if a.only_eos:
             make_eos(tmp)
+            return
+        if a.only_c5_setup:
+            add_config5_setup(tmp, spec=a.spec)
             return
         if a.only_c2_subset:
             make_config2_subset(tmp)
