@@ -256,6 +256,74 @@ int snapi_ali_iter(snapi_ali_ctx *ctx, int ncol, const snapi_ali_columns *cols, 
                    double tol, double *rel_change, int *iters, int *status, int mem);
 double snapi_ali_last_kernel_ms(const snapi_ali_ctx *ctx);
 
+/* ---------------------------------------------------------------------------------------------
+ * The population-independent set-up of nltepops on the device: what the reference computes once
+ * per column before its iterations (atmos/atmos_pop.cc:70-130) and what snapi_ali_iter otherwise
+ * takes from the caller.  From a column (the 12 rows of snapi_build_atmos: T, the gas pressure
+ * Nt k T, v_turb and v_z are read) and the node model's atom tables (snapi_eos_set on ctx):
+ *   - the chemistry and LTE populations at (T, Nt) (ltepops, atmos_pop.cc:31-46; chemeq with the
+ *     reference's cold start, atom::lte), kappa_500 (compute_op_referent), the NLTE atom's total
+ *     over all its levels (compute_active_population, atom.cc:793-810) and its LTE populations
+ *     (pops0 [ncol][nd][nlevel], the iteration's start);
+ *   - per ray the projected velocity (atmosphere::project, atmos_rad.cc:15-30);
+ *   - the LTE background per ray, NLTE wavelength and depth (opacity_lte / emissivity_lte,
+ *     atmos_rad.cc:225-246, whose Thomson term is zeroed): every LTE atom's free-free (atom_rad.cc:
+ *     203-236), Rayleigh (atom_rad.cc:268-298, atoms with atom::Z == 1, the reference's coefficient
+ *     loop as it stands), bound-free (atom_rad.cc:312-340) and bound-bound opacity (atom_rad.cc:
+ *     502-535: every level pair, FP64 W4 profile), H- bound-free and free-free (mol.cc:516-632), plus
+ *     the NLTE atom's own free-free; the emissivity is the opacity times the Planck function;
+ *   - per line of the NLTE atom the Doppler width and damping (atom_rad.cc:879-883, atom.cc:926-959),
+ *     per bound-free transition the LTE ratio factor (atom_rad.cc:327-335), and the collisional
+ *     rates of the rate matrix (atom_rad.cc:1769-1901: tabulated de-excitation rates linear in T
+ *     times n_e, excitation by detailed balance; Seaton's continuum rate and its inverse).
+ * All FP64.  The caller fills the tables from its atom objects (the reference: atom::bf, B, A,
+ * alpha_col_dam, col_dam_cross_section, mass, cr, rmap): */
+typedef struct {
+  int atom, stage, lower, upper;  /* LTE atom (index in the node model's tables) and level pair */
+  double lambda0;                 /* h c / (E_upper - E_lower) [cm] */
+  double Blu, Bul;                /* atom::B[z][lower][upper], B[z][upper][lower] */
+  double a_rad;                   /* atom::damp_rad(A[z], lower, upper) */
+  double alpha_col, sigma_col;    /* alpha_col_dam[z][upper][lower], col_dam_cross_section[z][upper][lower] */
+  double mass;                    /* atom mass [g] */
+} snapi_ali_bb;
+
+typedef struct {
+  int nbf;                  /* bound-free levels of the LTE atoms (atom::bf[z][l] set, z < Z) */
+  const int *bf_level;      /* [nbf][3]: atom, stage, level */
+  const double *bf_sigma;   /* [nbf][nlambda]: bf[z][l]->U at the problem's NLTE wavelengths [cm^2] */
+  int nbb;                  /* bound-bound level pairs of the LTE atoms (every pair of every stage) */
+  const snapi_ali_bb *bb;   /* [nbb] */
+  int nray_atom;            /* atoms with Rayleigh scattering (atom::Z == 1) */
+  const int *ray_atom;      /* [nray_atom] */
+  int atom;                 /* the NLTE atom (index in the node model's tables) */
+  int atom_Z;               /* its atom::Z (Seaton's factor: 0.1 for Z = 1, 0.2 for Z = 2, else 0.3) */
+  const int *level;         /* [nlevel][2]: stage and level of each of the problem's levels; the
+                               levels of a stage consecutive and in order (atom::rmap) */
+  const double *line_damp;  /* [nline][4] per line transition (problem order): alpha_col, sigma_col,
+                               mass [g], a_rad */
+  const double *sigma_edge; /* [nlevel] bf[z][l]->U(h c / (ip_z - E_l)) (-1 where the reference has
+                               no cross-section; 0 for the top stage) */
+  const int *coll_n;        /* [nlevel][nlevel] points of the tabulated rate between two levels of a
+                               stage (atom::cr[z][upper][lower], stored for both orders; <= 8) */
+  const double *coll_t;     /* [nlevel][nlevel][8] temperatures [K] */
+  const double *coll_v;     /* [nlevel][nlevel][8] de-excitation rate coefficients [cm^3 s^-1] */
+} snapi_ali_setup_tables;
+
+typedef struct {            /* output arrays, the layout of snapi_ali_columns */
+  double *T, *ne, *na, *kappa, *vray, *dld, *adamp, *bfratio, *coll, *bg_op, *bg_em;
+} snapi_ali_setup_out;
+
+/* The set-up of ncol columns [ncol][12][nd] (nd = prob->nd; the rows of snapi_build_atmos) for the
+ * NLTE problem prob (the same problem as the snapi_ali_ctx that iterates them) with ctx's atom
+ * tables: out (every array set), pops0 [ncol][nd][nlevel], status [ncol] (may be NULL: 0, or a sum
+ * of 1 -- a chemistry solve hit its iteration cap -- and 4 -- non-finite values).  The arrays of
+ * out, passed on as a snapi_ali_columns, and pops0 are the inputs of snapi_ali_iter.  mem: all
+ * arrays on the host (SNAPI_MEM_HOST) or on ctx's GPU (SNAPI_MEM_DEVICE).  Returns SNAPI_EINVAL
+ * for a pair of the NLTE atom's levels without a tabulated collisional rate (the reference's
+ * van Regemorter fallback is not on the device). */
+int snapi_ali_setup(snapi_ctx *ctx, const snapi_ali_problem *prob, const snapi_ali_setup_tables *tab, int ncol,
+                    const double *columns, const snapi_ali_setup_out *out, double *pops0, int *status, int mem);
+
 /* Batched small Gram matrices on the tensor cores: G[m] = M[m] M[m]^T for nmat matrices M[m]
  * [16][K] (row-major, float32, device memory), G [nmat][16][16] float32 (device).  tcgen05 MMA with a
  * three-product TF32 split (hi hi^T + hi lo^T + lo hi^T), FP32 accumulation: ~1e-6 relative.  This

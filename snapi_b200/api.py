@@ -779,6 +779,9 @@ class AliContext:
         self.nd, self.nl, self.nray, self.nlev = len(k[0]), len(k[1]), len(k[4]), k[9].shape[0]
         self.ntr = k[6].shape[0]
         p = SnapiAliProblem(self.nd, self.nl, self.nray, self.nlev, self.ntr, *[a.ctypes.data for a in k])
+        self._prob = p
+        self.nline = int(sum(1 for t in range(self.ntr) if k[12][k[6][t, 0]] != k[6][t, 1]))
+        self.nbf = self.ntr - self.nline
         st = ctypes.c_int(0)
         self._ctx = _ali_lib().snapi_ali_create(ctypes.byref(p), device, ctypes.byref(st))
         if not self._ctx:
@@ -831,6 +834,110 @@ class AliContext:
             raise RuntimeError("snapi_ali_iter: %s" % _ali_lib().snapi_ali_last_error(self._ctx).decode())
         return p, rel, it, st
 
+    def iterate_device(self, ncol, cols, pops_ptr, max_iter=100, tol=1e-2, rel_ptr=0, iters_ptr=0, status_ptr=0):
+        """iterate on device arrays: cols maps the SnapiAliColumns field names to device addresses
+        (e.g. torch .data_ptr()), pops_ptr [ncol][nd][nlevel] in / out."""
+        c = SnapiAliColumns(*[cols[n] for n, _ in SnapiAliColumns._fields_])
+        rc = _ali_lib().snapi_ali_iter(self._ctx, int(ncol), ctypes.byref(c), pops_ptr, int(max_iter), float(tol),
+                                       rel_ptr or None, iters_ptr or None, status_ptr or None, MEM_DEVICE)
+        if rc != 0:
+            raise RuntimeError("snapi_ali_iter: %s" % _ali_lib().snapi_ali_last_error(self._ctx).decode())
+
+    def column_shapes(self, ncol):
+        """Shapes of the SnapiAliColumns arrays (and 'pops') for ncol columns."""
+        nd, nr, nl, nv = self.nd, self.nray, self.nl, self.nlev
+        return {"T": (ncol, nd), "ne": (ncol, nd), "na": (ncol, nd), "kappa": (ncol, nd), "vray": (ncol, nr, nd),
+                "dld": (ncol, self.nline, nd), "adamp": (ncol, self.nline, nd), "bfratio": (ncol, self.nbf, nd),
+                "coll": (ncol, nd, nv, nv), "bg_op": (ncol, nr, nl, nd), "bg_em": (ncol, nr, nl, nd),
+                "pops": (ncol, nd, nv)}
+
+    def setup(self, ctx, tables, columns):
+        """The population-independent set-up on the device (snapi_ali_setup) of host columns
+        [ncol][12][nd] with ctx's atom tables (Context.eos_set) and the set-up tables
+        (AliSetupTables): returns (cols, pops0, status) as host arrays, cols keyed like
+        columns_from_fixture."""
+        cols = np.ascontiguousarray(columns, dtype=np.float64)
+        ncol = cols.shape[0]
+        sh = self.column_shapes(ncol)
+        out = {n: np.zeros(sh[n]) for n in sh}
+        st = np.zeros(ncol, np.int32)
+        o = SnapiAliSetupOut(*[out[n].ctypes.data for n, _ in SnapiAliSetupOut._fields_])
+        rc = _ali_setup_lib().snapi_ali_setup(ctx._ctx, ctypes.byref(self._prob), ctypes.byref(tables.tab), ncol,
+                                             cols.ctypes.data, ctypes.byref(o), out["pops"].ctypes.data,
+                                             st.ctypes.data, MEM_HOST)
+        ctx._check(rc)
+        cmap = {"T": "T", "ne": "ne", "na": "na", "kap": "kappa", "vray": "vray", "dld": "dld", "adamp": "adamp",
+                "bfratio": "bfratio", "coll": "coll", "bgop": "bg_op", "bgem": "bg_em"}
+        return {k: out[v] for k, v in cmap.items()}, out["pops"], st
+
+    def setup_device(self, ctx, tables, ncol, columns_ptr, out, pops_ptr, status_ptr=0):
+        """snapi_ali_setup on device arrays: out maps the SnapiAliSetupOut field names to device
+        addresses."""
+        o = SnapiAliSetupOut(*[out[n] for n, _ in SnapiAliSetupOut._fields_])
+        ctx._check(_ali_setup_lib().snapi_ali_setup(ctx._ctx, ctypes.byref(self._prob), ctypes.byref(tables.tab),
+                                                    int(ncol), columns_ptr, ctypes.byref(o), pops_ptr,
+                                                    status_ptr or None, MEM_DEVICE))
+
     @property
     def last_kernel_ms(self):
         return _ali_lib().snapi_ali_last_kernel_ms(self._ctx)
+
+
+class SnapiAliBB(ctypes.Structure):
+    _fields_ = [("atom", ctypes.c_int), ("stage", ctypes.c_int), ("lower", ctypes.c_int), ("upper", ctypes.c_int)] + \
+        [(n, ctypes.c_double) for n in ("lambda0", "Blu", "Bul", "a_rad", "alpha_col", "sigma_col", "mass")]
+
+
+class SnapiAliSetupTables(ctypes.Structure):
+    _fields_ = [("nbf", ctypes.c_int), ("bf_level", ctypes.c_void_p), ("bf_sigma", ctypes.c_void_p),
+                ("nbb", ctypes.c_int), ("bb", ctypes.c_void_p), ("nray_atom", ctypes.c_int),
+                ("ray_atom", ctypes.c_void_p), ("atom", ctypes.c_int), ("atom_Z", ctypes.c_int)] + \
+        [(n, ctypes.c_void_p) for n in ("level", "line_damp", "sigma_edge", "coll_n", "coll_t", "coll_v")]
+
+
+class SnapiAliSetupOut(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("T", "ne", "na", "kappa", "vray", "dld", "adamp", "bfratio", "coll",
+                                               "bg_op", "bg_em")]
+
+
+def _ali_setup_lib():
+    L = _ali_lib()
+    if not getattr(L, "_alis_set", False):
+        vp, ip = ctypes.c_void_p, ctypes.c_int
+        L.snapi_ali_setup.argtypes = [vp, ctypes.POINTER(SnapiAliProblem), ctypes.POINTER(SnapiAliSetupTables), ip, vp,
+                                      ctypes.POINTER(SnapiAliSetupOut), vp, vp, ip]
+        L._alis_set = True
+    return L
+
+
+class AliSetupTables:
+    """The set-up tables of snapi_ali_setup (snapi_ali_setup_tables), kept alive by this object.
+
+    bf_level [nbf, 3] (atom, stage, level) and bf_sigma [nbf, nlambda]: bound-free levels of the LTE
+    atoms; bb [nbb, 11]: atom, stage, lower, upper, lambda0, Blu, Bul, a_rad, alpha_col, sigma_col,
+    mass; ray_atom: Rayleigh atoms; atom / atom_Z: the NLTE atom; level [nlevel, 2]: stage and
+    level of the problem's levels; line_damp [nline, 4]; sigma_edge [nlevel]; coll_n [nlevel, nlevel],
+    coll_t / coll_v [nlevel, nlevel, 8]."""
+
+    def __init__(self, bf_level, bf_sigma, bb, ray_atom, atom, atom_Z, level, line_damp, sigma_edge, coll_n, coll_t,
+                 coll_v):
+        d = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)  # noqa: E731
+        bb = np.asarray(bb, np.float64).reshape(-1, 11)
+        self._bb = (SnapiAliBB * max(1, bb.shape[0]))()
+        for q, r in enumerate(bb):
+            self._bb[q] = SnapiAliBB(int(r[0]), int(r[1]), int(r[2]), int(r[3]), *[float(v) for v in r[4:]])
+        self._keep = [i32(np.asarray(bf_level).reshape(-1, 3)), d(bf_sigma), i32(np.asarray(ray_atom).reshape(-1)),
+                      i32(level), d(line_damp), d(sigma_edge), i32(coll_n), d(coll_t), d(coll_v)]
+        k = self._keep
+        self.tab = SnapiAliSetupTables(k[0].shape[0], k[0].ctypes.data, k[1].ctypes.data, bb.shape[0],
+                                       ctypes.addressof(self._bb), k[2].shape[0], k[2].ctypes.data, int(atom),
+                                       int(atom_Z), k[3].ctypes.data, k[4].ctypes.data, k[5].ctypes.data,
+                                       k[6].ctypes.data, k[7].ctypes.data, k[8].ctypes.data)
+
+    @classmethod
+    def from_fixture(cls, fx):
+        m = fx["alis_meta"]
+        return cls(fx["alis_bf"].astype(int), fx["alis_bfsig"], fx["alis_bb"], fx["alis_ray"].astype(int), int(m[0]),
+                   int(m[1]), fx["alis_lev"].astype(int), fx["alis_line"], fx["alis_sedge"],
+                   fx["alis_coll_n"].astype(int), fx["alis_coll_t"], fx["alis_coll_v"])

@@ -144,7 +144,9 @@ struct EosDev {
 // One thread per column: a warp holding one column per lane (and sharing its stage loops) issues 32
 // columns per instruction.  A warp per column (stages in lanes, butterfly sums) shortens a column's
 // chain but measured 14x slower at 4096 columns x 9 variants, where the GPU is full either way.
-struct Chem {
+// R: the kept-fraction capacity (the build kernels: kER; the NLTE set-up keeps every stage)
+template <int R>
+struct ChemT {
   const EosDev &E;
   double T, kT;
   double x5040;  // 5040 / T
@@ -160,7 +162,7 @@ struct Chem {
   // saha T^-1.5 g / g_next exp(chi / kT), each level's g exp(-E / kT), the H- bf + ff factor
   double mstim, mhm, mcb[kEBm], mlf[kELm];
   double Ea[kEA + 1], Da[kEA + 1];  // sum_i i f_i, sum_i i df_i / dNe per atom (1-based)
-  double fr[kER], dr[kER];          // kept ionisation fractions and their Ne derivatives
+  double fr[R], dr[R];              // kept ionisation fractions and their Ne derivatives
   double N[kEA + 1];
   double A[(kEA + 1) * (kEA + 1)], d[kEA + 1];
   int capped;
@@ -176,7 +178,7 @@ struct Chem {
   double lu_T, T1, T2;
   double lx1[kEA + 1], lx2[kEA + 1];
 
-  __device__ explicit Chem(const EosDev &e) : E(e), T(-1.0), have(0), Nt_prev(0.0), lu_ok(0), nhist(0) {}
+  __device__ explicit ChemT(const EosDev &e) : E(e), T(-1.0), have(0), Nt_prev(0.0), lu_ok(0), nhist(0) {}
 
   __device__ void set_T(double Tin) {
     T = Tin;
@@ -514,7 +516,7 @@ struct Chem {
       double Nr = N[1];
       double Nc[kEA + 1], iN[kEA + 1];
       for (int a = 2; a <= na; ++a) Nc[a] = N[a];
-      double dlf[kER];  // dr / fr of the kept fractions the molecules use
+      double dlf[R];  // dr / fr of the kept fractions the molecules use
       for (int k = 0; k < nr; ++k) iN[E.rfull[k]] = 1.0 / N[E.rfull[k]];
       for (int k = 0; k < E.nmref; ++k) dlf[E.mrefs[k]] = dr[E.mrefs[k]] / fr[E.mrefs[k]];
       double gr0 = 0.0;
@@ -645,6 +647,7 @@ struct Chem {
     return stage_total(s, E.satom[s]) * ((g != 0.0) ? g * exp(-E.lee[l] / (cK * T)) / U : 1.0);
   }
 };
+using Chem = ChemT<kER>;
 
 // ---- node interpolation (atmospheric_interpolation, mathtools.cc:1208-1315) -------------------------------
 __device__ double interpol_1d_falc(double xq) {
@@ -744,7 +747,8 @@ __device__ __forceinline__ double logtau(const EosDev &E, int x) {
 
 // atmosphere::opacity_continuum (atmos_rad.cc:286-294) from a solved Chem; which: 0 = lambda_he
 // with sigma_he, 1 = lambda_kappa with sigma_kappa.  lev[]: populations of the level slots.
-__device__ double continuum(const EosDev &E, const Chem &c, const double *lev, double nH0, int which) {
+template <class CH>
+__device__ double continuum(const EosDev &E, const CH &c, const double *lev, double nH0, int which) {
   const double T = c.T, Ne = c.N[0], lambda = which ? E.lambda_kappa : E.lambda_he;
   double op = 6.65E-25 * Ne;
   const double stim = exp(-cH * cC / lambda / cK / T);
@@ -774,7 +778,8 @@ __device__ double continuum(const EosDev &E, const Chem &c, const double *lev, d
 
 // chemistry + populations + kappa (which as in continuum); returns kappa, fills lev and nH0.  The
 // T-only tables are rebuilt only when T changes (the hydrostatic iterations of one depth share T).
-__device__ double chem_point(const EosDev &E, Chem &c, double T, double Nt, double *lev, double &nH0, int which,
+template <class CH>
+__device__ double chem_point(const EosDev &E, CH &c, double T, double Nt, double *lev, double &nH0, int which,
                              bool warm = false) {
   const bool fast = which == 0 && E.mfast;
   if (T != c.T) {
@@ -788,7 +793,7 @@ __device__ double chem_point(const EosDev &E, Chem &c, double T, double Nt, doub
     for (int k = 0; k < E.nlev_m; ++k) {
       const int l = E.lev_m[k], st = E.lst[l];
       double U, dU;
-      c.stage_u<false>(st, ine, pne, ipne, U, dU);
+      c.template stage_u<false>(st, ine, pne, ipne, U, dU);
       const double tot = c.stage_total(st, E.satom[st]);
       lm[k] = E.lg[l] != 0.0 ? tot * (c.mlf[k] / U) : tot;
     }
@@ -1152,6 +1157,13 @@ struct EosCtx {
   float *d_crec = nullptr;
   int *d_cst = nullptr;
   int cap_col = 0;
+  // the NLTE set-up (snapi_ali_setup): the host copy of the tables and the model's atoms it derives
+  // its own tables from, its device tables and work buffers (cap_su columns: bgf, staged inputs /
+  // outputs for host arrays)
+  std::vector<EosDev> h_tab;
+  std::vector<snapi_eos_atom> atoms;
+  void *d_su = nullptr;
+  size_t cap_su = 0;
 };
 
 void eos_free_bufs(EosCtx *e) {
@@ -1173,6 +1185,9 @@ void eos_free_bufs(EosCtx *e) {
   e->d_crec = nullptr;
   e->d_cst = nullptr;
   e->cap_col = 0;
+  cudaFree(e->d_su);
+  e->d_su = nullptr;
+  e->cap_su = 0;
 }
 
 }  // namespace
@@ -1498,6 +1513,8 @@ int snapi_eos_set(snapi_ctx *ctx, const snapi_eos_model *m) {
   }
   if (!e->d_tab) SNAPI_CK(cudaMalloc(&e->d_tab, sizeof(EosDev)));
   SNAPI_CK(cudaMemcpy(e->d_tab, &H, sizeof(EosDev), cudaMemcpyHostToDevice));
+  e->h_tab.assign(1, H);
+  e->atoms.assign(m->atoms, m->atoms + m->natom);
   e->npar = m->npar;
   e->chem_start = SNAPI_CHEM_START_CONTINUE;
   e->ntherm = H.kcount[1];
@@ -1829,6 +1846,589 @@ int snapi_build_atmos(snapi_ctx *ctx, int npix, const double *nodes, const int *
   if (npix < 0 || (npix > 0 && (!nodes || !atmos)) || (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
     return snapi::set_err(ctx, SNAPI_EINVAL, "snapi_build_atmos: invalid arguments");
   return build_impl(ctx, npix, nodes, active, nullptr, nullptr, nullptr, nullptr, pix_status, mem, x3, atmos);
+}
+
+}  // extern "C"
+
+// ==== NLTE set-up on the device (snapi_ali_setup) ==========================================================
+// The population-independent inputs of the level-population iteration (atmosphere::nltepops,
+// atmos/atmos_pop.cc:70-130), per column, in FP64:
+//   k_alis_depth  thread = (column, depth): the chemistry at (T, Nt) with the reference's cold start and
+//                 every ionisation stage's fraction kept (ChemT<kES>), LTE populations, kappa_500, the
+//                 NLTE atom's total and start populations, projected velocities, line widths and damping,
+//                 bound-free LTE ratios, collisional rates, and the depth's background factors: the
+//                 free-free coefficient, the Rayleigh density, the H- factors, each LTE bound-free
+//                 level's population and LTE ratio, each LTE level pair's width, damping and opacity
+//                 factor (bgf [column][field][depth]).
+//   k_alis_bg     thread = (column, ray, wavelength, depth), depth fastest: the LTE background opacity
+//                 and emissivity from those factors and the per-wavelength table (cross-sections, the
+//                 fudge factor, H- polynomials, Rayleigh cross-section); bound-bound profiles by W4 in
+//                 FP64.
+namespace snapi {
+namespace {
+
+constexpr int kSuLev = 16, kSuLine = 32, kSuBft = 16, kSuRay = 32, kSuBf = 32, kSuBb = 64, kSuAtomLev = 96;
+constexpr int kSuRayAtom = 8, kSuLt = 8, kSuThreads = 128;
+
+struct AlisDev {
+  int nd, nray, nlam, nlev, nline, nbft, nbf, nbb, nray_atom, nal, nst, nf;
+  double gcont;                 // Seaton's factor of the NLTE atom
+  double ct[kSuRay];            // cos(pi - theta) of each ray (atmosphere::project with V_x = V_y = 0)
+  // every level of the NLTE atom (its total, compute_active_population): stage, g, E
+  int al_st[kSuAtomLev];
+  double al_g[kSuAtomLev], al_e[kSuAtomLev];
+  // the problem's levels: stage, offset to the continuum level (0: none), g, E, the stage's ionisation
+  // energy, the next stage's ground g, the edge cross-section
+  int lv_st[kSuLev], lv_dl[kSuLev];
+  double lv_g[kSuLev], lv_e[kSuLev], lv_ip[kSuLev], lv_gn[kSuLev], lv_se[kSuLev];
+  int cn[kSuLev * kSuLev];      // collisional table points (0: no rate: the diagonal, other stages)
+  double ctab[kSuLev * kSuLev * 8], cval[kSuLev * kSuLev * 8];
+  // lines of the problem: lambda0, damping constants, mass, radiative damping
+  double ln_l0[kSuLine], ln_al[kSuLine], ln_sg[kSuLine], ln_ms[kSuLine], ln_ar[kSuLine];
+  int bft_lev[kSuBft];          // lower level of each bound-free transition
+  // background bound-free levels: stage, g, E, next stage ground g / E, ionisation energy
+  int bf_st[kSuBf];
+  double bf_g[kSuBf], bf_e[kSuBf], bf_gn[kSuBf], bf_en[kSuBf], bf_ip[kSuBf];
+  // background level pairs
+  int bb_st[kSuBb];
+  double bb_glo[kSuBb], bb_elo[kSuBb], bb_gup[kSuBb], bb_eup[kSuBb], bb_l0[kSuBb], bb_blu[kSuBb], bb_bul[kSuBb],
+      bb_ar[kSuBb], bb_al[kSuBb], bb_sg[kSuBb], bb_ms[kSuBb];
+  double zz[kES];               // z^2 of every stage (free-free)
+  int ray_st[kSuRayAtom];       // neutral stage of each Rayleigh atom
+};
+
+// n of a level (atom::lte, atom.cc:763-789) from the solved chemistry: stage total x Boltzmann / U
+template <class CH>
+__device__ __forceinline__ double su_level(const EosDev &E, const CH &c, int s, double g, double ee) {
+  const double tot = c.stage_total(s, E.satom[s]);
+  return g != 0.0 ? tot * (g * exp(-ee / (cK * c.T)) / c.stage_U(s, c.N[0])) : tot;
+}
+
+// collisional damping of a line (atom::damp_col, atom.cc:939-959)
+__device__ __forceinline__ double su_damp_col(double T, double nH0, double alpha, double sig, double mass) {
+  const double red_mass = 1.66E-24 / (1.0 / 1.008 + 1.66E-24 / mass);
+  const double vmean = sqrt(8.0 * cK * T / cPI / red_mass);
+  return nH0 * vmean * pow(vmean / 1E6, -alpha) * sig;
+}
+
+// tabulated rate (tbcr::interpol, colr.cc:111-115)
+__device__ __forceinline__ double su_tab(const double *t, const double *v, int n, double T) {
+  for (int i = 1; i < n; ++i)
+    if (t[i] > T) return (v[i] * (T - t[i - 1]) + v[i - 1] * (t[i] - T)) / (t[i] - t[i - 1]);
+  return v[n - 1];
+}
+
+__global__ void __launch_bounds__(kSuThreads) k_alis_depth(const EosDev *tab, const AlisDev *ad, int ncol,
+                                                          const double *cols, double *oT, double *one, double *ona,
+                                                          double *okap, double *ovray, double *odld, double *oad,
+                                                          double *obfr, double *ocoll, double *opop, double *bgf,
+                                                          int *status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const AlisDev &A = *ad;
+  const int nd = A.nd;
+  if (i >= ncol * nd) return;
+  const int p = i / nd, x = i % nd;
+  const EosDev &E = *tab;
+  const double *cc = cols + (size_t)p * 12 * nd + x;
+  const double T = cc[2 * nd], Nt = cc[3 * nd] / (cK * cc[2 * nd]), vt = cc[8 * nd], vz = cc[9 * nd];
+  ChemT<kES> c(E);
+  double lev[kEL], nH0;
+  const double kap = chem_point(E, c, T, Nt, lev, nH0, 1);
+  int st = c.capped;
+  const double ne = c.N[0], kT = cK * T;
+  const size_t pd = (size_t)p * nd + x;
+  oT[pd] = T;
+  one[pd] = ne;
+  okap[pd] = kap;
+  double na = 0.0;
+  for (int k = 0; k < A.nal; ++k) na += su_level(E, c, A.al_st[k], A.al_g[k], A.al_e[k]);
+  ona[pd] = na;
+  bool fin = isfinite(ne) && isfinite(kap) && isfinite(na);
+  double *pp = opop + pd * A.nlev;
+  for (int k = 0; k < A.nlev; ++k) pp[k] = su_level(E, c, A.lv_st[k], A.lv_g[k], A.lv_e[k]);
+  for (int r = 0; r < A.nray; ++r) ovray[((size_t)p * A.nray + r) * nd + x] = A.ct[r] * vz;
+  for (int q = 0; q < A.nline; ++q) {
+    const double l0 = A.ln_l0[q];
+    const double dld = sqrt(2.0 * cK * T / A.ln_ms[q] + vt * vt) * l0 / cC;
+    const double gc = su_damp_col(T, nH0, A.ln_al[q], A.ln_sg[q], A.ln_ms[q]);
+    odld[((size_t)p * A.nline + q) * nd + x] = dld;
+    oad[((size_t)p * A.nline + q) * nd + x] = l0 * l0 / (4.0 * cPI * cC) * (A.ln_ar[q] + gc) / dld;
+  }
+  for (int q = 0; q < A.nbft; ++q) {
+    const int k = A.bft_lev[q];
+    obfr[((size_t)p * A.nbft + q) * nd + x] =
+        ne * cSAHA * pow(T, -1.5) * A.lv_g[k] / A.lv_gn[k] * exp((A.lv_ip[k] - A.lv_e[k]) / kT);
+  }
+  // the rate matrix's collisional rates (atom_pop.cc:27-145, atom_rad.cc:1769-1901)
+  {
+    const int nl = A.nlev;
+    double *C = ocoll + pd * nl * nl;
+    for (int k = 0; k < nl * nl; ++k) C[k] = 0.0;
+    for (int a = 0; a + 1 < nl; ++a) {
+      for (int b = 0; b < nl; ++b) {
+        const int n = A.cn[a * nl + b];
+        if (!n) continue;
+        double rate = su_tab(A.ctab + (size_t)(a * nl + b) * 8, A.cval + (size_t)(a * nl + b) * 8, n, T) * ne;
+        if (a < b) {  // excitation: detailed balance of the tabulated de-excitation
+          const double u0 = fabs(A.lv_e[b] - A.lv_e[a]) / kT;
+          rate *= exp(-u0) * A.lv_g[b] / A.lv_g[a];
+        }
+        C[a * nl + b] = rate;
+      }
+      const int dl = A.lv_dl[a];
+      if (dl) {
+        const double dE = A.lv_ip[a] - A.lv_e[a], u0 = dE / kT;
+        const double ci = 1.55E13 / sqrt(T) * A.gcont * A.lv_se[a] * exp(-u0) / u0 * ne;
+        C[a * nl + a + dl] = ci;
+        C[(a + dl) * nl + a] = ci * A.lv_g[a] / A.lv_gn[a] * exp(dE / kT) * pow(T, -1.5) * ne * cSAHA;
+      }
+    }
+  }
+  // background factors of this depth
+  const size_t fs = (size_t)nd, f0 = (size_t)p * A.nf * nd + x;
+  double zs = 0.0;
+  for (int s = 0; s < A.nst; ++s)
+    if (A.zz[s] != 0.0) zs += A.zz[s] * c.stage_total(s, E.satom[s]);
+  const double fct = (cE * cE * cC * cH * cH * cRYD) / (6.0 * cPI * cPI * cPI * cE0 * cME * cC) *
+                     sqrt((2.0 * cPI) / (3.0 * cK * cME * cME * cME));
+  double nray0 = 0.0;
+  for (int k = 0; k < A.nray_atom; ++k) nray0 += c.stage_total(A.ray_st[k], E.satom[A.ray_st[k]]);
+  const double tp = 5040.0 / T;
+  bgf[f0] = T;
+  bgf[f0 + fs] = fct * 1.1 * ne / (sqrt(T) * cC * cC * cC) * zs;
+  bgf[f0 + 2 * fs] = nray0;
+  bgf[f0 + 3 * fs] = E.hm ? 4.158E-28 * ne * kT * pow(tp, 2.5) * pow(10.0, 0.754 * tp) * nH0 : 0.0;
+  bgf[f0 + 4 * fs] = E.hm ? 1E-26 * ne * kT * nH0 : 0.0;
+  bgf[f0 + 5 * fs] = log10(tp);
+  for (int b = 0; b < A.nbf; ++b) {
+    const int s = A.bf_st[b];
+    const double nl_ = su_level(E, c, s, A.bf_g[b], A.bf_e[b]);
+    const double nn = su_level(E, c, s + 1, A.bf_gn[b], A.bf_en[b]);
+    bgf[f0 + (6 + 2 * b) * fs] = nl_;
+    bgf[f0 + (7 + 2 * b) * fs] = nn * ne * cSAHA * pow(T, -1.5) * A.bf_g[b] / A.bf_gn[b] * exp((A.bf_ip[b] - A.bf_e[b]) / kT);
+  }
+  const int fb = 6 + 2 * A.nbf;
+  for (int q = 0; q < A.nbb; ++q) {
+    const int s = A.bb_st[q];
+    const double nlo = su_level(E, c, s, A.bb_glo[q], A.bb_elo[q]);
+    const double nup = su_level(E, c, s, A.bb_gup[q], A.bb_eup[q]);
+    const double l0 = A.bb_l0[q];
+    const double dld = sqrt(2.0 * cK * T / A.bb_ms[q] + vt * vt) * l0 / cC;
+    const double gc = su_damp_col(T, nH0, A.bb_al[q], A.bb_sg[q], A.bb_ms[q]);
+    bgf[f0 + (fb + 3 * q) * fs] = dld;
+    bgf[f0 + (fb + 3 * q + 1) * fs] = l0 * l0 / (4.0 * cPI * cC) * (A.bb_ar[q] + gc) / dld;
+    bgf[f0 + (fb + 3 * q + 2) * fs] = nlo * A.bb_blu[q] * (1.0 - nup / nlo * A.bb_bul[q] / A.bb_blu[q]);
+  }
+  if (!fin) st |= 4;
+  if (st) atomicOr(status + p, st);
+}
+
+// Humlicek W4 real part / sqrt(pi) in FP64 (cmlib/profiles.cc:7-37: the published region split and
+// coefficients, cos taken as sqrt(1 - sin^2) in region 4 as there)
+struct Cd {
+  double re, im;
+};
+__device__ __forceinline__ Cd cd_mul(Cd a, Cd b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__device__ __forceinline__ Cd cd_div(Cd a, Cd b) {
+  const double d = b.re * b.re + b.im * b.im;
+  return {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
+}
+__device__ __forceinline__ Cd cd_add(double s, Cd a) { return {s + a.re, a.im}; }
+__device__ __forceinline__ Cd cd_rsub(double s, Cd a) { return {s - a.re, -a.im}; }
+__device__ __forceinline__ Cd cd_scl(Cd a, double s) { return {a.re * s, a.im * s}; }
+
+__device__ double w4_re(double v, double a) {
+  const double s = fabs(v) + a;
+  const Cd t = {a, -v}, u = {a * a - v * v, -2.0 * a * v};
+  Cd w;
+  if (s >= 15.0) {
+    w = cd_div(cd_scl(t, 0.5641896), cd_add(0.5, u));
+  } else if (s > 5.5) {
+    w = cd_div(cd_mul(t, cd_add(1.410474, cd_scl(u, 0.5641896))), cd_add(0.75, cd_mul(u, cd_add(3.0, u))));
+  } else if (a > (0.195 * fabs(v) - 0.176)) {
+    Cd n = cd_add(3.778987, cd_scl(t, 0.5642236));
+    n = cd_add(11.96482, cd_mul(t, n));
+    n = cd_add(20.20933, cd_mul(t, n));
+    n = cd_add(16.4955, cd_mul(t, n));
+    Cd d = cd_add(6.699398, t);
+    d = cd_add(21.69274, cd_mul(t, d));
+    d = cd_add(39.27121, cd_mul(t, d));
+    d = cd_add(38.82363, cd_mul(t, d));
+    d = cd_add(16.4955, cd_mul(t, d));
+    w = cd_div(n, d);
+  } else {
+    Cd pn = cd_rsub(1.320522, cd_scl(u, 0.56419));
+    pn = cd_rsub(35.76683, cd_mul(u, pn));
+    pn = cd_rsub(219.0313, cd_mul(u, pn));
+    pn = cd_rsub(1540.787, cd_mul(u, pn));
+    pn = cd_rsub(3321.9905, cd_mul(u, pn));
+    pn = cd_rsub(36183.31, cd_mul(u, pn));
+    Cd q = cd_rsub(1.841439, u);
+    q = cd_rsub(61.57037, cd_mul(u, q));
+    q = cd_rsub(364.2191, cd_mul(u, q));
+    q = cd_rsub(2186.181, cd_mul(u, q));
+    q = cd_rsub(9022.228, cd_mul(u, q));
+    q = cd_rsub(24322.84, cd_mul(u, q));
+    q = cd_rsub(32066.6, cd_mul(u, q));
+    const double su = sin(u.im), eu = exp(u.re);
+    const Cd r = cd_div(cd_mul(t, pn), q);
+    w = {eu * sqrt(1.0 - su * su) - r.re, eu * su - r.im};
+  }
+  return w.re / 1.77245386399759;
+}
+
+// per-wavelength table: lambda, fudge, h c / lambda, H- bound-free polynomial, H- free-free f0 f1 f2,
+// Rayleigh cross-section (kSuLt doubles per wavelength)
+__global__ void __launch_bounds__(kSuThreads) k_alis_bg(const AlisDev *ad, int ncol, const double *lt,
+                                                       const double *sig, const double *bgf, const double *vray,
+                                                       double *bgop, double *bgem) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const AlisDev &A = *ad;
+  const int nd = A.nd, nl = A.nlam, nr = A.nray;
+  if (i >= (long long)ncol * nr * nl * nd) return;
+  const int x = (int)(i % nd);
+  const long long q1 = i / nd;
+  const int l = (int)(q1 % nl);
+  const long long q2 = q1 / nl;
+  const int r = (int)(q2 % nr), p = (int)(q2 / nr);
+  const double *L = lt + (size_t)l * kSuLt;
+  const double lam = L[0], fudge = L[1], hcl = L[2];
+  const size_t fs = (size_t)nd;
+  const double *F = bgf + (size_t)p * A.nf * nd + x;
+  const double T = F[0], kT = cK * T;
+  const double v = vray[((size_t)p * nr + r) * nd + x];
+  const double lv = lam * (1.0 + v / cC);
+  double op = F[fs] * lv * lv * lv * (1.0 - exp(-(cH * cC) / kT / lv)) * fudge;
+  op += L[7] * F[2 * fs];
+  const double stim = exp(-hcl / kT);
+  for (int b = 0; b < A.nbf; ++b) {
+    const double s = sig[(size_t)b * nl + l];
+    if (s != 0.0) op += s * (F[(6 + 2 * b) * fs] - F[(7 + 2 * b) * fs] * stim) * fudge;
+  }
+  const int fb = 6 + 2 * A.nbf;
+  for (int q = 0; q < A.nbb; ++q) {
+    const double dld = F[(fb + 3 * q) * fs];
+    const double xv = (A.bb_l0[q] - lv) / dld;
+    op += w4_re(xv, F[(fb + 3 * q + 1) * fs]) / dld * F[(fb + 3 * q + 2) * fs] * cH * cC / lam / 4.0 / cPI;
+  }
+  const double lt_ = F[5 * fs];
+  op += L[3] * F[3 * fs] * (1.0 - stim) * fudge;
+  op += pow(10.0, L[4] + L[5] * lt_ + L[6] * lt_ * lt_) * F[4 * fs] * fudge;
+  const size_t o = (((size_t)p * nr + r) * nl + l) * nd + x;
+  bgop[o] = op;
+  bgem[o] = op * (2.0 * 6.62606957 * 8.9875517E-7 / lam / lam / lam / lam / lam / (exp(1.4387769 / lam / T) - 1.0));
+}
+
+}  // namespace
+}  // namespace snapi
+
+namespace snapi {
+namespace {
+
+// the set-up's device tables from the ALI problem, the caller's set-up tables and the model's atoms;
+// returns an error text, or nullptr
+const char *alis_tables(const EosCtx *e, const snapi_ali_problem *P, const snapi_ali_setup_tables *T, AlisDev &A,
+                        std::vector<double> &lt, std::vector<double> &sig) {
+  const EosDev &H = e->h_tab[0];
+  const auto &At = e->atoms;
+  const int natom = (int)At.size();
+  memset(&A, 0, sizeof(AlisDev));
+  A.nd = P->nd;
+  A.nray = P->nray;
+  A.nlam = P->nlambda;
+  A.nlev = P->nlevel;
+  A.nst = H.nst;
+  if (P->nray > kSuRay) return "too many rays (<= 32)";
+  if (P->nlevel > kSuLev) return "too many levels (<= 16)";
+  if (T->atom < 0 || T->atom >= natom) return "bad NLTE atom";
+  if (T->nbf < 0 || T->nbf > kSuBf || (T->nbf && (!T->bf_level || !T->bf_sigma))) return "bad bound-free list (<= 32)";
+  if (T->nbb < 0 || T->nbb > kSuBb || (T->nbb && !T->bb)) return "bad bound-bound list (<= 64)";
+  if (T->nray_atom < 0 || T->nray_atom > kSuRayAtom - 1 || (T->nray_atom && !T->ray_atom)) return "bad Rayleigh atoms";
+  if (!T->level || !T->sigma_edge || !T->coll_n || !T->coll_t || !T->coll_v || !T->line_damp)
+    return "missing set-up tables";
+  A.gcont = T->atom_Z == 1 ? 0.1 : (T->atom_Z == 2 ? 0.2 : 0.3);
+  for (int r = 0; r < P->nray; ++r) A.ct[r] = cos(cPI - P->ray_theta[r]);
+  const snapi_eos_atom &Na = At[T->atom];
+  const int s0 = H.s0[T->atom];
+  for (int z = 0; z < Na.nstage; ++z)
+    for (int l = 0; l < Na.nlevel[z]; ++l) {
+      if (A.nal >= kSuAtomLev) return "NLTE atom: too many levels";
+      A.al_st[A.nal] = s0 + z;
+      A.al_g[A.nal] = Na.level[z][l].g;
+      A.al_e[A.nal] = Na.level[z][l].ee;
+      ++A.nal;
+    }
+  const int nlev = P->nlevel;
+  for (int k = 0; k < nlev; ++k) {
+    const int z = T->level[2 * k], l = T->level[2 * k + 1];
+    if (z < 0 || z >= Na.nstage || l < 0 || l >= Na.nlevel[z]) return "bad level map";
+    // the rate-matrix loop of the reference walks the levels of a stage as consecutive indices
+    if (k > 0 && T->level[2 * k - 2] == z && T->level[2 * k - 1] != l - 1) return "levels of a stage not consecutive";
+    if (l > 0 && (k == 0 || T->level[2 * k - 2] != z)) return "levels of a stage not consecutive";
+    A.lv_st[k] = s0 + z;
+    A.lv_g[k] = Na.level[z][l].g;
+    A.lv_e[k] = Na.level[z][l].ee;
+    A.lv_se[k] = T->sigma_edge[k];
+    if (z + 1 < Na.nstage) {
+      A.lv_ip[k] = Na.ip[z];
+      A.lv_gn[k] = Na.level[z + 1][0].g;
+    }
+  }
+  for (int k = 0; k + 1 < nlev; ++k) {
+    const int z = T->level[2 * k], l = T->level[2 * k + 1];
+    for (int ll = 0; ll < Na.nlevel[z]; ++ll) {
+      const int j = k + (ll - l);
+      if (j < 0 || j >= nlev) return "rate-matrix level outside the problem's levels";
+      if (ll == l) continue;
+      const int n = T->coll_n[k * nlev + j];
+      if (n < 1 || n > 8) return "a collisional rate without a table (only tabulated rates on the device)";
+      A.cn[k * nlev + j] = n;
+      for (int q = 0; q < n; ++q) {
+        A.ctab[(k * nlev + j) * 8 + q] = T->coll_t[(k * nlev + j) * 8 + q];
+        A.cval[(k * nlev + j) * 8 + q] = T->coll_v[(k * nlev + j) * 8 + q];
+      }
+    }
+    const int dl = Na.nlevel[z] - l;
+    if (k + dl >= nlev) return "continuum level outside the problem's levels";
+    A.lv_dl[k] = dl;
+  }
+  for (int t = 0; t < P->ntrans; ++t) {
+    const int lo = P->trans[2 * t], up = P->trans[2 * t + 1];
+    if (P->cont_of[lo] == up) {
+      if (A.nbft >= kSuBft) return "too many bound-free transitions";
+      A.bft_lev[A.nbft++] = lo;
+    } else {
+      if (A.nline >= kSuLine) return "too many lines";
+      const int q = A.nline++;
+      A.ln_l0[q] = P->line_c[4 * t];
+      A.ln_al[q] = T->line_damp[4 * q];
+      A.ln_sg[q] = T->line_damp[4 * q + 1];
+      A.ln_ms[q] = T->line_damp[4 * q + 2];
+      A.ln_ar[q] = T->line_damp[4 * q + 3];
+    }
+  }
+  A.nbf = T->nbf;
+  for (int b = 0; b < T->nbf; ++b) {
+    const int a = T->bf_level[3 * b], z = T->bf_level[3 * b + 1], l = T->bf_level[3 * b + 2];
+    if (a < 0 || a >= natom || z < 0 || z + 1 >= At[a].nstage || l < 0 || l >= At[a].nlevel[z] ||
+        At[a].nlevel[z + 1] < 1)
+      return "bad bound-free level";
+    A.bf_st[b] = H.s0[a] + z;
+    A.bf_g[b] = At[a].level[z][l].g;
+    A.bf_e[b] = At[a].level[z][l].ee;
+    A.bf_gn[b] = At[a].level[z + 1][0].g;
+    A.bf_en[b] = At[a].level[z + 1][0].ee;
+    A.bf_ip[b] = At[a].ip[z];
+  }
+  A.nbb = T->nbb;
+  for (int q = 0; q < T->nbb; ++q) {
+    const snapi_ali_bb &B = T->bb[q];
+    if (B.atom < 0 || B.atom >= natom || B.stage < 0 || B.stage >= At[B.atom].nstage || B.lower < 0 ||
+        B.upper < 0 || B.lower >= At[B.atom].nlevel[B.stage] || B.upper >= At[B.atom].nlevel[B.stage] ||
+        !(B.mass > 0.0))
+      return "bad bound-bound pair";
+    A.bb_st[q] = H.s0[B.atom] + B.stage;
+    A.bb_glo[q] = At[B.atom].level[B.stage][B.lower].g;
+    A.bb_elo[q] = At[B.atom].level[B.stage][B.lower].ee;
+    A.bb_gup[q] = At[B.atom].level[B.stage][B.upper].g;
+    A.bb_eup[q] = At[B.atom].level[B.stage][B.upper].ee;
+    A.bb_l0[q] = B.lambda0;
+    A.bb_blu[q] = B.Blu;
+    A.bb_bul[q] = B.Bul;
+    A.bb_ar[q] = B.a_rad;
+    A.bb_al[q] = B.alpha_col;
+    A.bb_sg[q] = B.sigma_col;
+    A.bb_ms[q] = B.mass;
+  }
+  // Rayleigh: the listed atoms, and the NLTE atom itself when its Z is 1 (its free-free and Rayleigh
+  // opacity enter the background as the LTE atoms' do)
+  for (int k = 0; k < T->nray_atom; ++k) {
+    if (T->ray_atom[k] < 0 || T->ray_atom[k] >= natom) return "bad Rayleigh atom";
+    A.ray_st[A.nray_atom++] = H.s0[T->ray_atom[k]];
+  }
+  if (T->atom_Z == 1) A.ray_st[A.nray_atom++] = s0;
+  for (int a = 0; a < natom; ++a)
+    for (int z = 0; z < At[a].nstage; ++z) A.zz[H.s0[a] + z] = (double)z * (double)z;
+  A.nf = 6 + 2 * A.nbf + 3 * A.nbb;
+  // per-wavelength table (kSuLt): lambda, fudge, h c / lambda, H- bound-free polynomial (mol.cc:
+  // 609-632), H- free-free f0 f1 f2 (mol.cc:516-545), Rayleigh cross-section (atom_rad.cc:268-298)
+  lt.assign((size_t)P->nlambda * kSuLt, 0.0);
+  for (int l = 0; l < P->nlambda; ++l) {
+    const double lam = P->lambda[l];
+    double *L = &lt[(size_t)l * kSuLt];
+    L[0] = lam;
+    L[1] = P->fudge[l];
+    L[2] = cH * cC / lam;
+    const double ca[7] = {1.99654, -1.18267E-5, 2.64243E-6, -4.40524E-10, 3.23992E-14, -1.39568E-18, 2.78701E-23};
+    double alpha = 0.0;
+    for (int i = 0; i < 7; ++i) alpha += ca[i] * pow(lam * 1E8, (double)i);
+    L[3] = alpha;
+    const double lg = log10(lam * 1E8);
+    L[4] = -2.2763 - 1.6850 * lg + 0.76661 * lg * lg - 0.053346 * lg * lg * lg;
+    L[5] = 15.2827 - 9.2846 * lg + 1.99381 * lg * lg - 0.142631 * lg * lg * lg;
+    L[6] = -197.789 + 190.266 * lg - 67.9775 * lg * lg + 10.6913 * lg * lg * lg - 0.625151 * lg * lg * lg * lg;
+    // the reference's coefficient loop reads its first coefficient for every power and then squares
+    // the cross-section; kept as it stands
+    const double l0 = 1215.67E-8;
+    double cs = 0.0;
+    for (int ii = 0; ii <= 5; ++ii) cs += 1.26563 * pow(l0 / lam, 2 * ii);
+    cs *= pow(l0 / lam, 4);
+    L[7] = cs * cs * 6.65E-25;
+  }
+  sig.assign(T->bf_sigma, T->bf_sigma + (size_t)T->nbf * P->nlambda);
+  return nullptr;
+}
+
+}  // namespace
+}  // namespace snapi
+
+extern "C" {
+
+int snapi_ali_setup(snapi_ctx *ctx, const snapi_ali_problem *prob, const snapi_ali_setup_tables *tab, int ncol,
+                    const double *columns, const snapi_ali_setup_out *out, double *pops0, int *status, int mem) {
+  using namespace snapi;
+  if (!ctx) return SNAPI_EINVAL;
+  EosCtx *e = static_cast<EosCtx *>(ctx->eos);
+  if (!e || e->h_tab.empty()) return set_err(ctx, SNAPI_EINVAL, "snapi_ali_setup: no atom tables (snapi_eos_set)");
+  if (!prob || !tab || !out || ncol < 0 || (ncol > 0 && (!columns || !pops0)) ||
+      (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
+    return set_err(ctx, SNAPI_EINVAL, "snapi_ali_setup: invalid arguments");
+  if (prob->nd < 3 || prob->nlambda < 1 || prob->nray < 1 || prob->nlevel < 2 || prob->ntrans < 1 || !prob->lambda ||
+      !prob->fudge || !prob->ray_theta || !prob->trans || !prob->line_c || !prob->cont_of)
+    return set_err(ctx, SNAPI_EINVAL, "snapi_ali_setup: invalid ALI problem");
+  for (int t = 0; t < prob->ntrans; ++t)
+    if (prob->trans[2 * t] < 0 || prob->trans[2 * t] >= prob->nlevel || prob->trans[2 * t + 1] < 0 ||
+        prob->trans[2 * t + 1] >= prob->nlevel)
+      return set_err(ctx, SNAPI_EINVAL, "snapi_ali_setup: transition levels out of range");
+  std::vector<AlisDev> hv(1);
+  AlisDev &A = hv[0];
+  std::vector<double> lt, sig;
+  if (const char *msg = alis_tables(e, prob, tab, A, lt, sig)) return set_err(ctx, SNAPI_EINVAL, "snapi_ali_setup: %s", msg);
+  if (!out->T || !out->ne || !out->na || !out->kappa || !out->vray || (A.nline && (!out->dld || !out->adamp)) ||
+      (A.nbft && !out->bfratio) || !out->coll || !out->bg_op || !out->bg_em)
+    return set_err(ctx, SNAPI_EINVAL, "snapi_ali_setup: missing output arrays");
+  if (ncol == 0) return SNAPI_OK;
+  // the set-up's chemistry table: the node model's, every ionisation stage's fraction kept
+  std::vector<EosDev> ev(1, e->h_tab[0]);
+  {
+    EosDev &S = ev[0];
+    int nref = S.nref;
+    for (int s = 0; s < S.nst; ++s)
+      if (S.ref[s] < 0) S.ref[s] = nref++;
+    S.nref = nref;
+    for (int a = 0; a < S.natom; ++a) S.zkeep[a] = S.ns[a];
+    for (int q = 0; q < S.nst; ++q) S.stab[q].ref = S.ref[q];
+  }
+  const int nd = A.nd, nr = A.nray, nl = A.nlam, nv = A.nlev, nli = A.nline, nbt = A.nbft;
+  const bool host = mem == SNAPI_MEM_HOST;
+  // work arena: tables, per-wavelength table, cross-sections, status, background factors; host arrays
+  // also stage the columns and every output.  Chunks of up to 4096 columns, host staging within ~2 GB.
+  const size_t per_col_out = (size_t)nd * (4 + nr + 2 * nli + nbt + nv * nv + nv) + 2 * (size_t)nr * nl * nd;
+  int B = std::min(ncol, 4096);
+  if (host) B = (int)std::max<size_t>(1, std::min<size_t>(B, ((size_t)2 << 30) / (sizeof(double) * per_col_out)));
+  size_t off = 0;
+  auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 255) & ~(size_t)255; return o; };
+  const size_t o_tab = take(sizeof(EosDev)), o_ad = take(sizeof(AlisDev)), o_lt = take(sizeof(double) * lt.size()),
+               o_sig = take(sizeof(double) * std::max<size_t>(sig.size(), 1)), o_st = take(sizeof(int) * B),
+               o_bgf = take(sizeof(double) * (size_t)B * A.nf * nd);
+  const size_t o_cols = host ? take(sizeof(double) * (size_t)B * 12 * nd) : 0;
+  const size_t o_out = host ? take(sizeof(double) * (size_t)B * per_col_out) : 0;
+  SNAPI_CK(cudaSetDevice(ctx->device));
+  if (off > e->cap_su) {
+    SNAPI_CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(e->d_su);
+    e->d_su = nullptr;
+    e->cap_su = 0;
+    SNAPI_CK(cudaMalloc(&e->d_su, off));
+    e->cap_su = off;
+  }
+  char *base = static_cast<char *>(e->d_su);
+  EosDev *d_tab = reinterpret_cast<EosDev *>(base + o_tab);
+  AlisDev *d_ad = reinterpret_cast<AlisDev *>(base + o_ad);
+  double *d_lt = reinterpret_cast<double *>(base + o_lt), *d_sig = reinterpret_cast<double *>(base + o_sig);
+  int *d_st = reinterpret_cast<int *>(base + o_st);
+  double *d_bgf = reinterpret_cast<double *>(base + o_bgf);
+  SNAPI_CK(cudaMemcpyAsync(d_tab, ev.data(), sizeof(EosDev), cudaMemcpyHostToDevice, ctx->stream));
+  SNAPI_CK(cudaMemcpyAsync(d_ad, hv.data(), sizeof(AlisDev), cudaMemcpyHostToDevice, ctx->stream));
+  SNAPI_CK(cudaMemcpyAsync(d_lt, lt.data(), sizeof(double) * lt.size(), cudaMemcpyHostToDevice, ctx->stream));
+  if (!sig.empty())
+    SNAPI_CK(cudaMemcpyAsync(d_sig, sig.data(), sizeof(double) * sig.size(), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->last_ms = 0.0;
+  ctx->last_launches = 0;
+  for (int p0 = 0; p0 < ncol; p0 += B) {
+    const int nb = std::min(B, ncol - p0);
+    // this chunk's arrays: the caller's (device) or the staging area (host)
+    const double *cols = columns + (size_t)p0 * 12 * nd;
+    double *aT, *ane, *ana, *akap, *avr, *adld, *aad, *abfr, *acoll, *aop, *aem, *apop;
+    if (host) {
+      SNAPI_CK(cudaMemcpyAsync(base + o_cols, cols, sizeof(double) * nb * 12 * nd, cudaMemcpyHostToDevice, ctx->stream));
+      cols = reinterpret_cast<const double *>(base + o_cols);
+      double *q = reinterpret_cast<double *>(base + o_out);
+      aT = q; q += (size_t)B * nd;
+      ane = q; q += (size_t)B * nd;
+      ana = q; q += (size_t)B * nd;
+      akap = q; q += (size_t)B * nd;
+      avr = q; q += (size_t)B * nr * nd;
+      adld = q; q += (size_t)B * nli * nd;
+      aad = q; q += (size_t)B * nli * nd;
+      abfr = q; q += (size_t)B * nbt * nd;
+      acoll = q; q += (size_t)B * nd * nv * nv;
+      apop = q; q += (size_t)B * nd * nv;
+      aop = q; q += (size_t)B * nr * nl * nd;
+      aem = q;
+    } else {
+      aT = out->T + (size_t)p0 * nd;
+      ane = out->ne + (size_t)p0 * nd;
+      ana = out->na + (size_t)p0 * nd;
+      akap = out->kappa + (size_t)p0 * nd;
+      avr = out->vray + (size_t)p0 * nr * nd;
+      adld = nli ? out->dld + (size_t)p0 * nli * nd : nullptr;
+      aad = nli ? out->adamp + (size_t)p0 * nli * nd : nullptr;
+      abfr = nbt ? out->bfratio + (size_t)p0 * nbt * nd : nullptr;
+      acoll = out->coll + (size_t)p0 * nd * nv * nv;
+      apop = pops0 + (size_t)p0 * nd * nv;
+      aop = out->bg_op + (size_t)p0 * nr * nl * nd;
+      aem = out->bg_em + (size_t)p0 * nr * nl * nd;
+    }
+    SNAPI_CK(cudaMemsetAsync(d_st, 0, sizeof(int) * nb, ctx->stream));
+    SNAPI_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    const int n1 = nb * nd;
+    k_alis_depth<<<(n1 + kSuThreads - 1) / kSuThreads, kSuThreads, 0, ctx->stream>>>(
+        d_tab, d_ad, nb, cols, aT, ane, ana, akap, avr, adld, aad, abfr, acoll, apop, d_bgf, d_st);
+    SNAPI_CK(cudaGetLastError());
+    const long long n2 = (long long)nb * nr * nl * nd;
+    k_alis_bg<<<(unsigned)((n2 + kSuThreads - 1) / kSuThreads), kSuThreads, 0, ctx->stream>>>(d_ad, nb, d_lt, d_sig,
+                                                                                              d_bgf, avr, aop, aem);
+    SNAPI_CK(cudaGetLastError());
+    SNAPI_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    ctx->last_launches += 2;
+    if (host) {
+      auto back = [&](double *dst, const double *src, size_t per_col) -> cudaError_t {
+        return cudaMemcpyAsync(dst + (size_t)p0 * per_col, src, sizeof(double) * nb * per_col, cudaMemcpyDeviceToHost,
+                               ctx->stream);
+      };
+      SNAPI_CK(back(out->T, aT, nd));
+      SNAPI_CK(back(out->ne, ane, nd));
+      SNAPI_CK(back(out->na, ana, nd));
+      SNAPI_CK(back(out->kappa, akap, nd));
+      SNAPI_CK(back(out->vray, avr, (size_t)nr * nd));
+      if (nli) SNAPI_CK(back(out->dld, adld, (size_t)nli * nd));
+      if (nli) SNAPI_CK(back(out->adamp, aad, (size_t)nli * nd));
+      if (nbt) SNAPI_CK(back(out->bfratio, abfr, (size_t)nbt * nd));
+      SNAPI_CK(back(out->coll, acoll, (size_t)nd * nv * nv));
+      SNAPI_CK(back(pops0, apop, (size_t)nd * nv));
+      SNAPI_CK(back(out->bg_op, aop, (size_t)nr * nl * nd));
+      SNAPI_CK(back(out->bg_em, aem, (size_t)nr * nl * nd));
+    }
+    if (status)
+      SNAPI_CK(cudaMemcpyAsync(status + p0, d_st, sizeof(int) * nb, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+    SNAPI_CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    SNAPI_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->last_ms += ms;
+  }
+  return SNAPI_OK;
 }
 
 }  // extern "C"

@@ -57,3 +57,98 @@ def test_oracle_setup_matches_reference(name):
             # background in float32
             tol = 2e-7 if (name == "config5_spec" and fk in ("ali_bgop", "ali_bgem")) else 1e-12
             assert err < tol, (name, c, fk, err)
+
+
+# ---- the device set-up (snapi_ali_setup) ---------------------------------------------------------
+@pytest.fixture(scope="module")
+def sb():
+    import snapi_b200
+    from snapi_b200 import build as b
+    b.build_cuda()
+    return snapi_b200
+
+
+def _contexts(sb, fx):
+    from snapi_b200.eos_tables import EosTables
+    ctx = sb.Context.from_fixture(fx)
+    ctx.eos_set(EosTables({k[4:]: v for k, v in fx.items() if k.startswith("eos_")}))
+    ali = sb.api.AliContext.from_fixture(fx)
+    return ctx, ali, sb.api.AliSetupTables.from_fixture(fx)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", _params)
+def test_device_setup_matches_reference(sb, name):
+    fx = load_fixture(name)
+    ctx, ali, tabs = _contexts(sb, fx)
+    cols, pops0, st = ali.setup(ctx, tabs, fx["alis_atm"])
+    assert np.all(st == 0)
+    worst = {}
+    for fk, ok in KEYS:
+        ck = {"kap": "kap", "bgop": "bgop", "bgem": "bgem"}.get(ok, ok)
+        v = pops0 if ok == "pop0" else cols[ck]
+        worst[fk] = _relerr(v, fx[fk])
+    print(name, worst)
+    for fk, err in worst.items():
+        # FP64 on the device against the reference's FP64: the chemistry's Newton solution (pivoted
+        # elimination on the reduced system against the reference's SVD) agrees to ~1e-12, the rest
+        # follows; the spec fixture stores the background in float32
+        tol = 2e-7 if (name == "config5_spec" and fk in ("ali_bgop", "ali_bgem")) else 1e-9
+        assert err < tol, (name, fk, err)
+    ctx.close()
+    ali.close()
+
+
+@pytest.mark.gpu
+def test_device_setup_device_arrays_equal_host_arrays(sb):
+    import torch
+    fx = load_fixture("config5")
+    ctx, ali, tabs = _contexts(sb, fx)
+    cols, pops0, _ = ali.setup(ctx, tabs, fx["alis_atm"])
+    ncol = fx["alis_atm"].shape[0]
+    dev = torch.device("cuda:0")
+    sh = ali.column_shapes(ncol)
+    out = {n: torch.zeros(sh[n], dtype=torch.float64, device=dev) for n in sh}
+    d_cols = torch.tensor(fx["alis_atm"], dtype=torch.float64, device=dev)
+    d_st = torch.zeros(ncol, dtype=torch.int32, device=dev)
+    ali.setup_device(ctx, tabs, ncol, d_cols.data_ptr(), {n: out[n].data_ptr() for n in sh if n != "pops"},
+                     out["pops"].data_ptr(), d_st.data_ptr())
+    torch.cuda.synchronize()
+    cmap = {"kap": "kappa", "bgop": "bg_op", "bgem": "bg_em"}
+    for k, v in cols.items():
+        assert np.array_equal(out[cmap.get(k, k)].cpu().numpy(), v), k
+    assert np.array_equal(out["pops"].cpu().numpy(), pops0)
+    assert int(d_st.abs().sum()) == 0
+    ctx.close()
+    ali.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", _params)
+def test_populations_from_device_setup(sb, name):
+    """Columns -> device set-up -> device iteration, all on the device: the populations the
+    reference's nltepops converges to."""
+    import torch
+    fx = load_fixture(name)
+    tol = {"config5": 1e-2, "config5_spec": 1e-4}[name]
+    ctx, ali, tabs = _contexts(sb, fx)
+    ncol = fx["alis_atm"].shape[0]
+    dev = torch.device("cuda:0")
+    sh = ali.column_shapes(ncol)
+    out = {n: torch.zeros(sh[n], dtype=torch.float64, device=dev) for n in sh}
+    d_cols = torch.tensor(fx["alis_atm"], dtype=torch.float64, device=dev)
+    ali.setup_device(ctx, tabs, ncol, d_cols.data_ptr(), {n: out[n].data_ptr() for n in sh if n != "pops"},
+                     out["pops"].data_ptr())
+    rel = torch.zeros(ncol, dtype=torch.float64, device=dev)
+    it = torch.zeros(ncol, dtype=torch.int32, device=dev)
+    st = torch.zeros(ncol, dtype=torch.int32, device=dev)
+    ali.iterate_device(ncol, {n: out[n].data_ptr() for n in sh if n != "pops"}, out["pops"].data_ptr(),
+                       max_iter=100, tol=tol, rel_ptr=rel.data_ptr(), iters_ptr=it.data_ptr(), status_ptr=st.data_ptr())
+    torch.cuda.synchronize()
+    pops = out["pops"].cpu().numpy()
+    assert np.all(st.cpu().numpy() == 0) and np.all(rel.cpu().numpy() < tol)
+    err = np.abs(pops / fx["ali_pop_conv"] - 1.0).max()
+    print(name, "iterations", it.cpu().numpy(), "max relative difference to the reference's populations", err)
+    assert err < 1e-3
+    ctx.close()
+    ali.close()
