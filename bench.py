@@ -612,9 +612,56 @@ def bench_ali(sb, device, ncol=1024, cpu=True):
            "iterations_max": int(iters.max()), "device_ms": dev_ms, "columns_per_s_device": ncol / (dev_ms / 1e3),
            "columns_per_s_e2e": ncol / wall, "max_rel_to_reference_converged":
                float(np.abs(pops[:3] / fx["ali_pop_conv"] - 1.0).max()), "negative_columns": int((st < 0).sum())}
+    out["from_columns"] = bench_ali_from_columns(sb, device, fx, ncol)
     if cpu:
         out["reference_cpu"] = reference_ali_rate()
     return out
+
+
+def bench_ali_from_columns(sb, device, fx, ncol):
+    """The same populations from atmosphere columns alone, everything on the device: the columns
+    (12 return_as_array rows, float64) from pinned host memory, the population-independent set-up
+    (snapi_ali_setup: chemistry, LTE background per ray and wavelength, rates), the iteration, the
+    populations back to the host."""
+    import torch
+    from snapi_b200.eos_tables import EosTables
+    dev = torch.device("cuda", device)
+    ctx = sb.Context.from_fixture(fx, device=device)
+    ctx.eos_set(EosTables({k[4:]: v for k, v in fx.items() if k.startswith("eos_")}))
+    ali = sb.api.AliContext.from_fixture(fx, device=device)
+    tabs = sb.api.AliSetupTables.from_fixture(fx)
+    idx = np.arange(ncol) % fx["alis_atm"].shape[0]
+    h_cols = torch.from_numpy(np.ascontiguousarray(fx["alis_atm"][idx])).pin_memory()
+    sh = ali.column_shapes(ncol)
+    out = {n: torch.empty(sh[n], dtype=torch.float64, device=dev) for n in sh}
+    ptrs = {n: out[n].data_ptr() for n in sh if n != "pops"}
+    d_cols = torch.empty(h_cols.shape, dtype=torch.float64, device=dev)
+    h_pops = torch.empty(sh["pops"], dtype=torch.float64).pin_memory()
+    st = torch.zeros(ncol, dtype=torch.int32, device=dev)
+
+    def run(n):
+        d_cols[:n].copy_(h_cols[:n], non_blocking=True)
+        torch.cuda.synchronize(dev)
+        ali.setup_device(ctx, tabs, n, d_cols.data_ptr(), ptrs, out["pops"].data_ptr())
+        setup_ms = ctx.last_kernel_ms
+        ali.iterate_device(n, ptrs, out["pops"].data_ptr(), max_iter=100, tol=1e-2, status_ptr=st.data_ptr())
+        h_pops[:n].copy_(out["pops"][:n])
+        torch.cuda.synchronize(dev)
+        return setup_ms, ali.last_kernel_ms
+
+    run(8)  # warm-up
+    t0 = time.perf_counter()
+    setup_ms, iter_ms = run(ncol)
+    wall = time.perf_counter() - t0
+    pops = h_pops.numpy()
+    res = {"setup_device_ms": setup_ms, "iterate_device_ms": iter_ms,
+           "columns_per_s_device": ncol / ((setup_ms + iter_ms) / 1e3), "columns_per_s_e2e": ncol / wall,
+           "h2d_bytes": int(h_cols.numel() * 8), "d2h_bytes": int(pops.size * 8),
+           "max_rel_to_reference_converged": float(np.abs(pops[:3] / fx["ali_pop_conv"] - 1.0).max()),
+           "negative_columns": int((st < 0).sum())}
+    ctx.close()
+    ali.close()
+    return res
 
 
 def reference_ali_rate(cores=None):
@@ -757,6 +804,9 @@ def main():
     ap.add_argument("--cube-chunk", type=int, default=0, help="pixels per GPU batch of the invert job")
     ap.add_argument("--cube-synth-only", type=int, default=0, metavar="N",
                     help="only measure the synthesis job (snapi_cube_synth) over an N x N atmosphere cube")
+    ap.add_argument("--ali-only", type=int, default=0, metavar="N",
+                    help="only measure the NLTE populations of N columns (snapi_ali_iter; from columns with "
+                         "snapi_ali_setup)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -785,6 +835,13 @@ def main():
         pool = dict(np.load(POOL))
         print(json.dumps({"cube_synth": bench_cube_synth(sb, pool, 0, n=args.cube_synth_only,
                                                          chunk=args.cube_chunk)}), flush=True)
+        return
+    if args.ali_only:
+        sys.path.insert(0, ROOT)
+        import snapi_b200 as sb
+        from snapi_b200 import build as b
+        b.build_cuda()
+        print(json.dumps({"ali": bench_ali(sb, 0, ncol=args.ali_only, cpu=not args.no_cpu_baseline)}), flush=True)
         return
     if args.cube_only:
         sys.path.insert(0, ROOT)

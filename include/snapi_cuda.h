@@ -324,6 +324,18 @@ typedef struct {            /* output arrays, the layout of snapi_ali_columns */
 int snapi_ali_setup(snapi_ctx *ctx, const snapi_ali_problem *prob, const snapi_ali_setup_tables *tab, int ncol,
                     const double *columns, const snapi_ali_setup_out *out, double *pops0, int *status, int mem);
 
+/* The records of an NLTE atom's lines from its level populations -- the synthesis after nltepops
+ * (obs_stokes, atmos_obs.cc:16-87: op_em_vector reads the populations nltepops left,
+ * atom_rad_synthesis.cc:405-435).  For each of the context's lines j with line_level[j] = {lower,
+ * upper} (indices into the levels of pops [npix][nd][nlevel], e.g. snapi_ali_iter's), the opacity
+ * and emissivity fields of records [npix][nd][nfield] become (n_l B_lu - n_u B_ul) h c / (4 pi
+ * lambda0) and n_u A h c / (4 pi lambda0) with the node model's Einstein coefficients (snapi_eos_set);
+ * lines with {-1, -1} keep their fields.  The other fields do not depend on the NLTE atom's
+ * populations (its continuum is not in kappa_500, nltepops leaves n_e as it is).  mem: records and
+ * pops on the host or on the device; line_level [nlines][2] is always a host array. */
+int snapi_records_set_populations(snapi_ctx *ctx, int npix, float *records, const double *pops, int nlevel,
+                                  const int *line_level, int mem);
+
 /* Batched small Gram matrices on the tensor cores: G[m] = M[m] M[m]^T for nmat matrices M[m]
  * [16][K] (row-major, float32, device memory), G [nmat][16][16] float32 (device).  tcgen05 MMA with a
  * three-product TF32 split (hi hi^T + hi lo^T + lo hi^T), FP32 accumulation: ~1e-6 relative.  This

@@ -148,7 +148,9 @@ class Setup:
             for r in range(nray):
                 ll_ = lam * (1.0 + out["vray"][r, x] / C)
                 op = aff * ll_ ** 3 * (1.0 - np.exp(-(H * C) / kT / ll_)) * fudge
-                for b in d["alis_ray"].astype(int):
+                # Rayleigh: the listed LTE atoms, and the NLTE atom when its Z is 1 (its Rayleigh
+                # opacity joins the background with its free-free)
+                for b in list(d["alis_ray"].astype(int)) + ([a] if self.Z == 1 else []):
                     l0 = 1215.67E-8
                     cs = 1.26563 * sum((l0 / lam) ** (2 * ii) for ii in range(6)) * (l0 / lam) ** 4
                     op = op + cs * cs * 6.65E-25 * nst[b, 0]

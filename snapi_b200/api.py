@@ -610,6 +610,17 @@ class Context:
                                             MEM_HOST))
         return atm, st
 
+    def records_set_populations(self, records, pops, line_level):
+        """The opacity / emissivity fields of the lines with line_level[j] = (lower, upper) >= 0 from
+        level populations pops [npix][nd][nlevel] (snapi_records_set_populations; needs eos_set);
+        returns a new records array."""
+        rec = np.array(records, dtype=np.float32, order="C", copy=True)
+        p = np.ascontiguousarray(pops, dtype=np.float64)
+        ll = np.ascontiguousarray(line_level, dtype=np.int32)
+        self._check(_pop_lib().snapi_records_set_populations(self._ctx, rec.shape[0], _ptr(rec), _ptr(p), p.shape[2],
+                                                             _ptr(ll), MEM_HOST))
+        return rec
+
     def records_from_columns(self, columns):
         """Records of atmosphere columns [npix][12][nd] in the snapi_build_atmos row layout
         (snapi_records_from_columns; needs eos_set): records [npix][nd][nfield] and the status."""
@@ -881,6 +892,28 @@ class AliContext:
     @property
     def last_kernel_ms(self):
         return _ali_lib().snapi_ali_last_kernel_ms(self._ctx)
+
+
+def _pop_lib():
+    L = lib()
+    if not getattr(L, "_pop_set", False):
+        vp, ip = ctypes.c_void_p, ctypes.c_int
+        L.snapi_records_set_populations.argtypes = [vp, ip, vp, vp, ip, vp, ip]
+        L._pop_set = True
+    return L
+
+
+def ali_line_levels(line_eos, nlte_atom, level_map):
+    """line_level [nlines][2] of snapi_records_set_populations: for each line (the node model's
+    line ties, rows atom, stage, lower, upper) of the NLTE atom, the indices of its levels among the
+    ALI problem's (level_map [nlevel][2]: stage, level); (-1, -1) for the other lines."""
+    lm = {(int(z), int(l)): k for k, (z, l) in enumerate(np.asarray(level_map).astype(int))}
+    out = -np.ones((len(line_eos), 2), np.int32)
+    for j, r in enumerate(np.asarray(line_eos)):
+        a, z, lo, up = (int(v) for v in r[:4])
+        if a == nlte_atom:
+            out[j] = (lm[(z, lo)], lm[(z, up)])
+    return out
 
 
 class SnapiAliBB(ctypes.Structure):

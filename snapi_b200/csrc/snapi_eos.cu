@@ -2432,3 +2432,91 @@ int snapi_ali_setup(snapi_ctx *ctx, const snapi_ali_problem *prob, const snapi_a
 }
 
 }  // extern "C"
+
+// ==== records of an NLTE atom's lines from level populations (snapi_records_set_populations) =============
+namespace snapi {
+namespace {
+
+struct PopLines {
+  int n;                                    // lines whose fields are set
+  int line[SNAPI_MAX_LINES], lo[SNAPI_MAX_LINES], up[SNAPI_MAX_LINES];
+  double Blu[SNAPI_MAX_LINES], Bul[SNAPI_MAX_LINES], A[SNAPI_MAX_LINES], lam0[SNAPI_MAX_LINES];
+};
+
+// thread = (pixel, depth): the opacity and emissivity fields of each listed line
+__global__ void __launch_bounds__(kRecThreads) k_rec_pops(PopLines L, int npix, int nd, int nf, int nlev,
+                                                         const double *pops, float *rec) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npix * nd) return;
+  const double *n = pops + (size_t)i * nlev;
+  float *r = rec + (size_t)i * nf;
+  for (int k = 0; k < L.n; ++k) {
+    const double nl = n[L.lo[k]], nu = n[L.up[k]];
+    const int j = L.line[k];
+    // the record's line fields as the node build forms them from LTE populations (thermal_fields)
+    r[SNAPI_NFIELD0 + 3 * j] = (float)((nl * L.Blu[k] - nu * L.Bul[k]) * cH * cC / L.lam0[k] / 4.0 / cPI);
+    r[SNAPI_NFIELD0 + 3 * j + 1] = (float)(nu * L.A[k] * cH * cC / L.lam0[k] / 4.0 / cPI);
+  }
+}
+
+}  // namespace
+}  // namespace snapi
+
+extern "C" {
+
+int snapi_records_set_populations(snapi_ctx *ctx, int npix, float *records, const double *pops, int nlevel,
+                                  const int *line_level, int mem) {
+  using namespace snapi;
+  if (!ctx) return SNAPI_EINVAL;
+  EosCtx *e = static_cast<EosCtx *>(ctx->eos);
+  if (!e || e->h_tab.empty())
+    return set_err(ctx, SNAPI_EINVAL, "snapi_records_set_populations: no atom tables (snapi_eos_set)");
+  if (npix < 0 || (npix > 0 && (!records || !pops)) || nlevel < 1 || !line_level ||
+      (mem != SNAPI_MEM_HOST && mem != SNAPI_MEM_DEVICE))
+    return set_err(ctx, SNAPI_EINVAL, "snapi_records_set_populations: invalid arguments");
+  const EosDev &H = e->h_tab[0];
+  PopLines L;
+  memset(&L, 0, sizeof(L));
+  for (int j = 0; j < ctx->nlines; ++j) {
+    const int lo = line_level[2 * j], up = line_level[2 * j + 1];
+    if (lo < 0 && up < 0) continue;
+    if (lo < 0 || up < 0 || lo >= nlevel || up >= nlevel)
+      return set_err(ctx, SNAPI_EINVAL, "snapi_records_set_populations: line %d: bad level indices", j);
+    const int k = L.n++;
+    L.line[k] = j;
+    L.lo[k] = lo;
+    L.up[k] = up;
+    // atom_rad_synthesis.cc:405-435 with the node model's Einstein coefficients
+    L.Blu[k] = H.lBlu[j];
+    L.Bul[k] = H.lBul[j];
+    L.A[k] = H.lA[j];
+    L.lam0[k] = H.llam0[j];
+  }
+  if (npix == 0 || L.n == 0) return SNAPI_OK;
+  const int nd = ctx->nd, nf = ctx->nfield;
+  SNAPI_CK(cudaSetDevice(ctx->device));
+  float *d_rec = records;
+  const double *d_pops = pops;
+  void *stage = nullptr;
+  const size_t brec = sizeof(float) * (size_t)npix * nd * nf, bpop = sizeof(double) * (size_t)npix * nd * nlevel;
+  if (mem == SNAPI_MEM_HOST) {
+    SNAPI_CK(cudaMalloc(&stage, brec + bpop));
+    d_rec = static_cast<float *>(stage);
+    d_pops = reinterpret_cast<const double *>(static_cast<char *>(stage) + brec);
+    SNAPI_CK(cudaMemcpyAsync(d_rec, records, brec, cudaMemcpyHostToDevice, ctx->stream));
+    SNAPI_CK(cudaMemcpyAsync(const_cast<double *>(d_pops), pops, bpop, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  const int n = npix * nd;
+  k_rec_pops<<<(n + kRecThreads - 1) / kRecThreads, kRecThreads, 0, ctx->stream>>>(L, npix, nd, nf, nlevel, d_pops,
+                                                                                  d_rec);
+  cudaError_t err = cudaGetLastError();
+  if (err == cudaSuccess && mem == SNAPI_MEM_HOST)
+    err = cudaMemcpyAsync(records, d_rec, brec, cudaMemcpyDeviceToHost, ctx->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(ctx->stream);
+  if (stage) cudaFree(stage);
+  if (err != cudaSuccess) return set_err(ctx, SNAPI_ECUDA, "snapi_records_set_populations: %s", cudaGetErrorString(err));
+  ctx->last_launches = 1;
+  return SNAPI_OK;
+}
+
+}  // extern "C"
