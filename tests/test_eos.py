@@ -291,6 +291,23 @@ def test_gpu_active_rows_untouched_and_batches(oracle_lib, eos3, config3):
 
 @pytest.mark.gpu
 @pytestmark_gpu
+def test_gpu_segmented_march_records_equal_records_only_build(oracle_lib, eos3, config3):
+    """With tangents the march runs in depth segments (its state carried between launches) with the
+    record chemistry of finished segments on a second stream; without tangents in one launch.  The
+    node vector's records are the same computation either way: equal bit for bit."""
+    nodes = np.concatenate([config3["nodes"]] * 4)
+    ctx = _gpu_ctx(config3, eos3)
+    rec_t, tan, nt_t, st_t = ctx.build_records(nodes, tangents=True, want_nt=True)
+    rec_0, _, nt_0, st_0 = ctx.build_records(nodes, tangents=False, want_nt=True)
+    np.testing.assert_array_equal(rec_t, rec_0)
+    np.testing.assert_array_equal(nt_t, nt_0)
+    np.testing.assert_array_equal(st_t, st_0)
+    assert np.all(np.isfinite(tan))
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytestmark_gpu
 def test_gpu_continued_start_tangents_vs_oracle(oracle_lib, eos3, config3):
     """The device's continued start against the oracle's restatement of it: the same path, so the
     cold start's tight tangent tolerance holds."""
