@@ -43,7 +43,9 @@ def test_ctypes_mirror_matches_header_layout(tmp_path):
     structs = {api.SnapiLine: "snapi_line", api.SnapiProblem: "snapi_problem", api.SnapiLmOpts: "snapi_lm_opts",
                api.F0Info: "snapi_f0_info", api.CubeJob: "snapi_cube_job", api.CubeStats: "snapi_cube_stats",
                api.CubeSynthJob: "snapi_cube_synth_job", api.SnapiAliProblem: "snapi_ali_problem",
-               api.SnapiAliColumns: "snapi_ali_columns", et.SnapiPartition: "snapi_partition",
+               api.SnapiAliColumns: "snapi_ali_columns", api.SnapiAliBB: "snapi_ali_bb",
+               api.SnapiAliSetupTables: "snapi_ali_setup_tables", api.SnapiAliSetupOut: "snapi_ali_setup_out",
+               et.SnapiPartition: "snapi_partition",
                et.SnapiEosLevel: "snapi_eos_level", et.SnapiEosAtom: "snapi_eos_atom",
                et.SnapiEosMolecule: "snapi_eos_molecule", et.SnapiEosLine: "snapi_eos_line",
                et.SnapiEosModel: "snapi_eos_model"}
