@@ -184,3 +184,26 @@ def test_nlte_synthesis_from_node_vectors(sb, name):
     assert perr < 1e-3 and serr < 5e-5
     ctx.close()
     ali.close()
+
+
+@pytest.mark.gpu
+def test_device_setup_rejects_untabulated_collisions(sb):
+    """A pair of the NLTE atom's levels without a tabulated rate (the reference would fall back to
+    van Regemorter's formula, which the device does not have): SNAPI_EINVAL with a message, nothing
+    launched; a level map that is not consecutive within a stage: SNAPI_EINVAL."""
+    fx = dict(load_fixture("config5"))
+    ctx, ali, _ = _contexts(sb, fx)
+    cn = fx["alis_coll_n"].copy()
+    cn[2, 1] = 0
+    bad = dict(fx, alis_coll_n=cn)
+    with pytest.raises(sb.api.SnapiError, match="tabulated"):
+        ali.setup(ctx, sb.api.AliSetupTables.from_fixture(bad), fx["alis_atm"][:1])
+    lev = fx["alis_lev"].copy()
+    lev[[1, 2]] = lev[[2, 1]]
+    with pytest.raises(sb.api.SnapiError, match="consecutive"):
+        ali.setup(ctx, sb.api.AliSetupTables.from_fixture(dict(fx, alis_lev=lev)), fx["alis_atm"][:1])
+    # the context still works
+    cols, pops0, st = ali.setup(ctx, sb.api.AliSetupTables.from_fixture(fx), fx["alis_atm"][:1])
+    assert np.all(st == 0) and np.all(np.isfinite(cols["bgop"]))
+    ctx.close()
+    ali.close()
