@@ -33,6 +33,7 @@ constexpr int kAliChunk = 64;
 constexpr int kAliMaxLev = 16, kAliMaxLine = 32, kAliMaxBf = 16;
 constexpr double kHc = kH * kC;
 constexpr double kPi4 = 4.0 * kPi;
+constexpr double kInvPi4 = 1.0 / kPi4, kInvHc = 1.0 / kHc;
 
 struct AliDev {
   int ncol, nd, nl, nray, nlev, nline, nbf, nchunk;
@@ -133,8 +134,9 @@ __global__ void __launch_bounds__(kAliChunk) k_ali_formal(AliDev D) {
       }
     }
     op = o;
-    oo = o / (double)kap[z];
-    ee = e / (double)kap[z];
+    const double ik = 1.0 / (double)kap[z];
+    oo = o * ik;
+    ee = e * ik;
   };
   double *Io = D.I + row, *Lo = D.L + row, *Oo = D.opp + row;
   const double ct = D.ray_ct[ray];
@@ -167,8 +169,9 @@ __global__ void __launch_bounds__(kAliChunk) k_ali_formal(AliDev D) {
       w1 = 0.5 * tb * (1.0 - tb / 3.0 * (1.0 - tb / 4.0));
     } else {
       etb = exp(-tb);
-      w0 = 1.0 / tb - etb * (1.0 + 1.0 / tb);
-      w1 = 1.0 - 1.0 / tb + etb / tb;
+      const double itb = 1.0 / tb;
+      w0 = itb - etb * (1.0 + itb);
+      w1 = 1.0 - itb + etb * itb;
     }
     I = I * etb + w0 * (eep / oop) + w1 * (eec / ooc);
     Io[z] = I;
@@ -282,29 +285,34 @@ __global__ void k_ali_rates(AliDev D) {
     Jbu[b] = Jbd[b] = 0.0;
     bfr[b] = D.bfratio[((size_t)col * D.nbf + b) * nd + zz];
   }
+  const double hckT = kHc / (kK * Tz);
   for (int r = 0; r < D.nray; ++r) {
     const float vrc = (float)(D.vray[((size_t)col * D.nray + r) * nd + zz] / kC);
     const double wr = D.ray_w[r];
     const size_t base = ((size_t)col * D.nray + r) * D.nl * nd + zz;
+    // FP64 divisions hoisted: one reciprocal of the opacity and of lambda per (ray, wavelength), the
+    // constant ones folded (the sums move by rounding only)
     for (int l = 0; l < D.nl; ++l) {
       const double I = D.I[base + (size_t)l * nd], Ls = D.L[base + (size_t)l * nd], op = D.opp[base + (size_t)l * nd];
-      const double lam = D.lambda[l], w = D.lw[l] * wr;
+      const double lam = D.lambda[l], w = D.lw[l] * wr, iop = 1.0 / op, wq = w * kInvPi4;
       const float lamf = (float)lam;
       for (int k = 0; k < D.nline; ++k) {
         float H, F;
         voigt(((float)(D.lam0[k] - lam) - lamf * vrc) * iv[k], av[k], H, F);
         const double phi = (double)(H * iv[k]);
-        const double wp = w * phi / kPi4;
-        const double lf = lfac[k] * phi / op;
+        const double wp = wq * phi;
+        const double lf = lfac[k] * phi * iop;
         nrm[k] += wp;
         Jl[k] += wp * I * lf;
         Ll[k] += wp * Ls * lf;
       }
       if (D.nbf) {
-        const double e = exp(-kHc / (lam * kK * Tz));
-        const double p5 = 2.0 * kHc * kC / (lam * lam * lam * lam * lam);
+        const double il = 1.0 / lam, il2 = il * il;
+        const double e = exp(-hckT * il);
+        const double p5 = 2.0 * kHc * kC * (il2 * il2 * il);
+        const double wl = w * lam * kInvHc;
         for (int b = 0; b < D.nbf; ++b) {
-          const double s = w * (double)D.sigma[(size_t)b * D.nl + l] * lam / kHc;
+          const double s = wl * (double)D.sigma[(size_t)b * D.nl + l];
           Jbu[b] += s * I;
           Jbd[b] += s * (I + p5) * e;
         }
