@@ -37,6 +37,7 @@ constexpr double kInvPi4 = 1.0 / kPi4, kInvHc = 1.0 / kHc;
 
 struct AliDev {
   int ncol, nd, nl, nray, nlev, nline, nbf, nchunk;
+  int nsl;  // k_ali_rates: wavelength slices per depth (adjacent lanes; a power of two <= 32)
   double tol;
   int max_iter;
   // problem
@@ -262,7 +263,10 @@ __device__ bool solve_rates(const AliDev &D, const double *n, const double *coll
 __global__ void k_ali_rates(AliDev D) {
   __shared__ int s_neg;
   __shared__ double s_max;
-  const int col = blockIdx.x, z = threadIdx.x, nd = D.nd, m = D.nlev;
+  // thread = (depth, wavelength slice): the nsl lanes of a depth take every nsl-th wavelength and
+  // their sums meet by shuffles, so a column's CTA keeps nsl times the warps in flight
+  const int col = blockIdx.x, sl = threadIdx.x % D.nsl, z = threadIdx.x / D.nsl, nd = D.nd, m = D.nlev;
+  const bool lead = sl == 0;
   if (D.state[col] != 0) return;  // CTA-uniform
   if (threadIdx.x == 0) { s_neg = 0; s_max = 0.0; }
   __syncthreads();
@@ -292,7 +296,7 @@ __global__ void k_ali_rates(AliDev D) {
     const size_t base = ((size_t)col * D.nray + r) * D.nl * nd + zz;
     // FP64 divisions hoisted: one reciprocal of the opacity and of lambda per (ray, wavelength), the
     // constant ones folded (the sums move by rounding only)
-    for (int l = 0; l < D.nl; ++l) {
+    for (int l = sl; l < D.nl; l += D.nsl) {
       const double I = D.I[base + (size_t)l * nd], Ls = D.L[base + (size_t)l * nd], op = D.opp[base + (size_t)l * nd];
       const double lam = D.lambda[l], w = D.lw[l] * wr, iop = 1.0 / op, wq = w * kInvPi4;
       const float lamf = (float)lam;
@@ -319,6 +323,17 @@ __global__ void k_ali_rates(AliDev D) {
       }
     }
   }
+  for (int off = 1; off < D.nsl; off <<= 1) {  // every lane of the depth ends with the totals
+    for (int k = 0; k < D.nline; ++k) {
+      Jl[k] += __shfl_xor_sync(0xffffffffu, Jl[k], off);
+      Ll[k] += __shfl_xor_sync(0xffffffffu, Ll[k], off);
+      nrm[k] += __shfl_xor_sync(0xffffffffu, nrm[k], off);
+    }
+    for (int b = 0; b < D.nbf; ++b) {
+      Jbu[b] += __shfl_xor_sync(0xffffffffu, Jbu[b], off);
+      Jbd[b] += __shfl_xor_sync(0xffffffffu, Jbd[b], off);
+    }
+  }
   const double *cz = D.coll + ((size_t)col * nd + zz) * m * m;
   // step with the local operator; negative populations anywhere -> without it (atmos_pop.cc:185-205)
   double rmax = 0.0;
@@ -330,7 +345,7 @@ __global__ void k_ali_rates(AliDev D) {
     rmax = fmax(rmax, fabs(rc));
   }
   if (!ok) neg = 1;
-  if (valid && neg) atomicOr(&s_neg, 1);
+  if (valid && lead && neg) atomicOr(&s_neg, 1);
   __syncthreads();
   int negative = s_neg;
   __syncthreads();
@@ -345,7 +360,7 @@ __global__ void k_ali_rates(AliDev D) {
       if (!(rc >= -1.0)) neg = 1;
       rmax = fmax(rmax, fabs(rc));
     }
-    if (valid && neg) atomicOr(&s_neg, 1);
+    if (valid && lead && neg) atomicOr(&s_neg, 1);
     __syncthreads();
     negative = s_neg;
   }
@@ -353,7 +368,7 @@ __global__ void k_ali_rates(AliDev D) {
     if (threadIdx.x == 0) { D.state[col] = -1; D.iters[col] += 1; }
     return;
   }
-  if (valid) {
+  if (valid && lead) {
     for (int i = 0; i < m; ++i) pz[i] = nn[i];
     // max of non-negative doubles through their bit patterns
     atomicMax(reinterpret_cast<unsigned long long *>(&s_max), __double_as_longlong(rmax));
@@ -486,6 +501,7 @@ snapi_ali_ctx *snapi_ali_create(const snapi_ali_problem *p, int device, int *sta
   AliDev &D = c->D;
   memset(&D, 0, sizeof D);
   D.nd = c->nd; D.nl = c->nl; D.nray = c->nray; D.nlev = m; D.nline = c->nline; D.nbf = c->nbf; D.nchunk = c->nchunk;
+  D.nsl = c->nd <= 256 ? 4 : (c->nd <= 512 ? 2 : 1);  // nd * nsl <= 1024 threads per CTA
   bool ok = (D.grid = upload(c, p->grid, p->nd)) && (D.lambda = upload(c, p->lambda, p->nlambda)) &&
             (D.lw = upload(c, p->lambda_w, p->nlambda)) && (D.ray_ct = upload(c, ct.data(), ct.size())) &&
             (D.ray_w = upload(c, p->ray_w, p->nray)) && (D.fudge = upload(c, fud.data(), fud.size())) &&
@@ -588,7 +604,7 @@ int snapi_ali_iter(snapi_ali_ctx *c, int ncol, const snapi_ali_columns *in, doub
   D.pops = c->d_pops; D.I = c->d_I; D.L = c->d_L; D.opp = c->d_opp; D.state = c->d_state; D.iters = c->d_iters;
   D.rel = c->d_rel;
   const FormalSmem S = formal_smem(c->nd, c->nline, c->nbf);
-  const int nthr = (int)((nd + 31) / 32 * 32);
+  const int nthr = (int)((nd * D.nsl + 31) / 32 * 32);
   std::vector<int> st(ncol);
   c->last_ms = 0.0;
   for (int it = 0; it < max_iter; ++it) {
