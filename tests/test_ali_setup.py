@@ -207,3 +207,29 @@ def test_device_setup_rejects_untabulated_collisions(sb):
     assert np.all(st == 0) and np.all(np.isfinite(cols["bgop"]))
     ctx.close()
     ali.close()
+
+
+@pytest.mark.gpu
+def test_device_setup_chunks(sb):
+    """More columns than one device chunk (4096): the columns of every chunk get the same set-up
+    as the same columns in the first, bit for bit."""
+    import torch
+    fx = load_fixture("config5")
+    ctx, ali, tabs = _contexts(sb, fx)
+    n0 = fx["alis_atm"].shape[0]
+    ncol = 4096 + 2 * n0
+    dev = torch.device("cuda:0")
+    sh = ali.column_shapes(ncol)
+    out = {n: torch.zeros(sh[n], dtype=torch.float64, device=dev) for n in sh}
+    idx = np.arange(ncol) % n0
+    d_cols = torch.tensor(fx["alis_atm"][idx], dtype=torch.float64, device=dev)
+    d_st = torch.zeros(ncol, dtype=torch.int32, device=dev)
+    ali.setup_device(ctx, tabs, ncol, d_cols.data_ptr(), {n: out[n].data_ptr() for n in sh if n != "pops"},
+                     out["pops"].data_ptr(), d_st.data_ptr())
+    torch.cuda.synchronize()
+    assert int(d_st.abs().sum()) == 0
+    for n, t in out.items():
+        first, last = t[:n0].cpu().numpy(), t[ncol - n0:].cpu().numpy()
+        np.testing.assert_array_equal(first[idx[ncol - n0:]], last, err_msg=n)
+    ctx.close()
+    ali.close()
