@@ -615,10 +615,20 @@ def bench_ali(sb, device, ncol=1024, cpu=True):
     out["from_columns"] = bench_ali_from_columns(sb, device, fx, ncol)
     if cpu:
         out["reference_cpu"] = reference_ali_rate()
+    # config 5 at its stated settings: 10 ray directions (5-point Gauss set), 100 depths, the 1e-4
+    # population stop (the patched reference build); the six columns of tests/golden/config5_spec.npz
+    # tiled, from columns with the set-up on the device
+    fs = dict(np.load(os.path.join(ROOT, "tests", "golden", "config5_spec.npz")))
+    spec = bench_ali_from_columns(sb, device, fs, ncol, tol=1e-4)
+    spec.update({"columns": ncol, "nd": int(fs["ali_T"].shape[1]), "rays": int(fs["ali_th"].shape[0]),
+                 "tol": 1e-4})
+    if cpu:
+        spec["reference_cpu"] = reference_ali_rate(spec=True)
+    out["spec"] = spec
     return out
 
 
-def bench_ali_from_columns(sb, device, fx, ncol):
+def bench_ali_from_columns(sb, device, fx, ncol, tol=1e-2):
     """The same populations from atmosphere columns alone, everything on the device: the columns
     (12 return_as_array rows, float64) from pinned host memory, the population-independent set-up
     (snapi_ali_setup: chemistry, LTE background per ray and wavelength, rates), the iteration, the
@@ -639,17 +649,17 @@ def bench_ali_from_columns(sb, device, fx, ncol):
     h_pops = torch.empty(sh["pops"], dtype=torch.float64).pin_memory()
     st = torch.zeros(ncol, dtype=torch.int32, device=dev)
 
-    def run(n):
+    def run(n, max_iter=100):
         d_cols[:n].copy_(h_cols[:n], non_blocking=True)
         torch.cuda.synchronize(dev)
         ali.setup_device(ctx, tabs, n, d_cols.data_ptr(), ptrs, out["pops"].data_ptr())
         setup_ms = ctx.last_kernel_ms
-        ali.iterate_device(n, ptrs, out["pops"].data_ptr(), max_iter=100, tol=1e-2, status_ptr=st.data_ptr())
+        ali.iterate_device(n, ptrs, out["pops"].data_ptr(), max_iter=max_iter, tol=tol, status_ptr=st.data_ptr())
         h_pops[:n].copy_(out["pops"][:n])
         torch.cuda.synchronize(dev)
         return setup_ms, ali.last_kernel_ms
 
-    run(8)  # warm-up
+    run(ncol, max_iter=1)  # warm-up: the contexts' work buffers sized for ncol columns
     t0 = time.perf_counter()
     setup_ms, iter_ms = run(ncol)
     wall = time.perf_counter() - t0
@@ -657,20 +667,22 @@ def bench_ali_from_columns(sb, device, fx, ncol):
     res = {"setup_device_ms": setup_ms, "iterate_device_ms": iter_ms,
            "columns_per_s_device": ncol / ((setup_ms + iter_ms) / 1e3), "columns_per_s_e2e": ncol / wall,
            "h2d_bytes": int(h_cols.numel() * 8), "d2h_bytes": int(pops.size * 8),
-           "max_rel_to_reference_converged": float(np.abs(pops[:3] / fx["ali_pop_conv"] - 1.0).max()),
+           "max_rel_to_reference_converged":
+               float(np.abs(pops[:fx["ali_pop_conv"].shape[0]] / fx["ali_pop_conv"] - 1.0).max()),
            "negative_columns": int((st < 0).sum())}
     ctx.close()
     ali.close()
     return res
 
 
-def reference_ali_rate(cores=None):
-    """The reference's nltepops on config-5 columns, one process per host core (one column each)."""
+def reference_ali_rate(cores=None, spec=False):
+    """The reference's nltepops on config-5 columns, one process per host core (one column each);
+    spec: the patched build at the configuration's stated settings (10 rays, 100 depths, 1e-4)."""
     sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
     from make_golden import config3_nodes
     from sbin import read_sbin
-    dump = os.path.join(ROOT, "oracle", "_ref", "snapi_ref_dump")
-    task = os.path.join(ROOT, "tests", "golden", "c5.tsk")
+    dump = os.path.join(ROOT, "oracle", "_ref", "snapi_ref_dump_spec" if spec else "snapi_ref_dump")
+    task = os.path.join(ROOT, "tests", "golden", "c5_spec.tsk" if spec else "c5.tsk")
     if not os.path.exists(dump):
         return None
     ncores = cores or os.cpu_count() or 1
@@ -691,8 +703,9 @@ def reference_ali_rate(cores=None):
     if not ok:
         return None
     return {"columns_per_s": ncores / max(secs), "cores": ncores, "seconds_per_column_mean": float(np.mean(secs)),
-            "kind": "reference", "sample": "%d seeded config-5 columns, atmosphere::nltepops (strict FP64 build), "
-                                          "one process per core" % ncores}
+            "kind": "reference", "sample": "%d seeded config-5 columns, atmosphere::nltepops (strict FP64 build%s), "
+                                          "one process per core" % (ncores, ", patched to 10 rays and the 1e-4 stop"
+                                                                    if spec else "")}
 
 
 def ctypes_buffer(ctx, nbytes):

@@ -144,22 +144,26 @@ __global__ void __launch_bounds__(kAliChunk) k_ali_formal(AliDev D) {
   const int dz = ct > 0.0 ? 1 : -1, zl = ct > 0.0 ? 0 : nd - 1, zh = ct > 0.0 ? nd - 1 : 0;
   const double mct = -ct;
   // window: p (z - dz), c (z), n (z + dz)
+  // each cell's source function and each interval's length once: the window carries them
   double oop, eep, opp_, ooc, eec, opc, oon = 0.0, een = 0.0, opn = 0.0;
   cell(zl, oop, eep, opp_);
   cell(zl + dz, ooc, eec, opc);
-  double dprev = (ooc - oop) / ((D.grid[zl + dz] - D.grid[zl]) / mct);
-  double I = ct > 0.0 ? 0.0 : eep / oop;
+  double sp = eep / oop, sc = eec / ooc, sn = 0.0;
+  double hz = (D.grid[zl + dz] - D.grid[zl]) / mct, hn = 0.0;
+  double dprev = (ooc - oop) / hz;
+  double I = ct > 0.0 ? 0.0 : sp;
   Io[zl] = I;
   Lo[zl] = ct > 0.0 ? 0.0 : 1.0;
   Oo[zl] = opp_;
   for (int z = zl + dz;; z += dz) {
-    const double hz = (D.grid[z] - D.grid[z - dz]) / mct;
     double dcur;
     if (z == zh) {
       dcur = (ooc - oop) / hz;
     } else {
       cell(z + dz, oon, een, opn);
-      dcur = opd_interior(oop, ooc, oon, hz, (D.grid[z + dz] - D.grid[z]) / mct);
+      sn = een / oon;
+      hn = (D.grid[z + dz] - D.grid[z]) / mct;
+      dcur = opd_interior(oop, ooc, oon, hz, hn);
     }
     const double tb = bezier_dtau(oop, ooc, dprev, dcur, hz);
     // linear weights with the Taylor branch below 1e-2 (atmos_ppbez_rts.cc:1070-1096 scalar form)
@@ -174,13 +178,14 @@ __global__ void __launch_bounds__(kAliChunk) k_ali_formal(AliDev D) {
       w0 = itb - etb * (1.0 + itb);
       w1 = 1.0 - itb + etb * itb;
     }
-    I = I * etb + w0 * (eep / oop) + w1 * (eec / ooc);
+    I = I * etb + w0 * sp + w1 * sc;
     Io[z] = I;
     Lo[z] = w1;
     Oo[z] = opc;
     if (z == zh) break;
-    oop = ooc; eep = eec; opp_ = opc;
-    ooc = oon; eec = een; opc = opn;
+    oop = ooc; opp_ = opc; sp = sc;
+    ooc = oon; opc = opn; sc = sn;
+    hz = hn;
     dprev = dcur;
   }
 }

@@ -4,7 +4,8 @@ Runs in the development container only (it reads the reference's atom / molecule
 its 80-depth atmosphere file from REF and runs oracle/_ref/snapi_ref_dump).  Writes:
 
   tests/golden/c1.tsk, c3.tsk     task blobs (packed atmosphere column + node model + lambda
-                                  grid), the payload the reference's master sends a slave
+                                  grid), the payload the reference's master sends a slave;
+                                  c5.tsk, c5_spec.tsk the config-5 tasks (80 / 100 depths)
   tests/golden/config1.npz        one column, 80 depths, 201 lambda: record, reference Stokes,
                                   reference opacity at 7 wavelengths, line constants
   tests/golden/config2.npz        16 pixels of the seeded 256x256 synthesis cube (seed 2)
@@ -377,8 +378,7 @@ def make_config5(tmp, ncol, niter=3, spec=False):
     small (the device takes them as float64; ~6e-8 relative).  Also the set-up tables
     (config5_setup_arrays)."""
     dump_bin, name = config5_task(tmp, spec)
-    if not spec:
-        shutil.copy(os.path.join(tmp, "c5.tsk"), os.path.join(HERE, "c5.tsk"))
+    shutil.copy(os.path.join(tmp, "c5.tsk"), os.path.join(HERE, "c5_spec.tsk" if spec else "c5.tsk"))
     nodes = config3_nodes(ncol, seed=5)
     nf = os.path.join(tmp, "c5_nodes.f64")
     np.ascontiguousarray(nodes, dtype="<f8").tofile(nf)
@@ -401,6 +401,7 @@ def add_config5_setup(tmp, spec=False):
     """Add the set-up arrays (config5_setup_arrays) to an existing config-5 fixture, for its node
     vectors, without running the reference's iterations again (make_config5 writes the same)."""
     dump_bin, name = config5_task(tmp, spec)
+    shutil.copy(os.path.join(tmp, "c5.tsk"), os.path.join(HERE, "c5_spec.tsk" if spec else "c5.tsk"))
     path = os.path.join(HERE, name + ".npz")
     d = dict(np.load(path))
     d.update(config5_setup_arrays(tmp, dump_bin, d["nodes"]))
