@@ -727,7 +727,20 @@ typedef struct {
   int xl, xh, yl, yh;            /* 1-based inclusive subfield; 0 = the cube's extent */
   const char *out_spectra;       /* NULL: not written */
   float *stokes;                 /* [nx_sub * ny_sub][nlambda][4] host copy (x major), or NULL */
-  int chunk;                     /* pixels per GPU batch (0: 16384) */
+  int chunk;                     /* pixels per GPU batch (0: 16384; 2048 with an NLTE atom) */
+  /* An NLTE atom (all NULL: LTE populations).  As obs_stokes runs nltepops for an NLTE atom
+   * (atmos_obs.cc:16-87, atmos_pop.cc:67-240), each chunk's columns get the population-independent
+   * set-up (snapi_ali_setup with ctx's atom tables, T floored at 3200 K as read_spinor3d floors it),
+   * the level-population iteration (snapi_ali_iter on ali, from the LTE populations, up to
+   * ali_max_iter iterations to ali_tol) and the NLTE atom's line fields from those populations
+   * (snapi_records_set_populations with line_level) before the synthesis.  A column whose
+   * populations stayed negative is counted in stats->flagged and synthesised with the last ones. */
+  snapi_ali_ctx *ali;
+  const snapi_ali_problem *ali_prob;       /* the problem ali was created with */
+  const snapi_ali_setup_tables *ali_tables;
+  const int *line_level;                   /* [nlines][2], host */
+  int ali_max_iter;                        /* 0: 100 */
+  double ali_tol;                          /* 0: 1e-2, the reference's stop */
 } snapi_cube_synth_job;
 
 int snapi_cube_synth(snapi_ctx *ctx, const snapi_cube_synth_job *job, snapi_cube_stats *stats);

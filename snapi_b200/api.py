@@ -131,6 +131,8 @@ class CubeSynthJob(ctypes.Structure):
         ("out_spectra", ctypes.c_char_p),
         ("stokes", ctypes.c_void_p),
         ("chunk", ctypes.c_int),
+        ("ali", ctypes.c_void_p), ("ali_prob", ctypes.c_void_p), ("ali_tables", ctypes.c_void_p),
+        ("line_level", ctypes.c_void_p), ("ali_max_iter", ctypes.c_int), ("ali_tol", ctypes.c_double),
     ]
 
 
@@ -631,9 +633,11 @@ class Context:
         self._check(lib().snapi_records_from_columns(self._ctx, npix, _ptr(c), _ptr(rec), _ptr(st), MEM_HOST))
         return rec, st
 
-    def cube_synth(self, atmos_path, subfield=(0, 0, 0, 0), out_spectra=None, chunk=0, want_stokes=True):
+    def cube_synth(self, atmos_path, subfield=(0, 0, 0, 0), out_spectra=None, chunk=0, want_stokes=True, ali=None,
+                   ali_tables=None, line_level=None, ali_max_iter=0, ali_tol=0.0):
         """The synthesis branch of the master's job over an atmosphere .f0 cube (snapi_cube_synth):
-        returns the Stokes vectors [nx][ny][nlambda][4] (if want_stokes) and the job's statistics."""
+        returns the Stokes vectors [nx][ny][nlambda][4] (if want_stokes) and the job's statistics.
+        With an NLTE atom: ali (AliContext), ali_tables (AliSetupTables), line_level [nlines][2]."""
         dims = f0_stat(atmos_path)["dims"]
         nx_full, ny_full = (dims[2], dims[1]) if len(dims) == 4 else (1, 1)
         xl, xh, yl, yh = subfield
@@ -641,7 +645,12 @@ class Context:
         ny = min(yh or ny_full, ny_full) - (yl or 1) + 1
         st = np.zeros((max(nx, 1), max(ny, 1), self.nl, 4), np.float32) if want_stokes else None
         enc = lambda p: None if p is None else os.fsencode(p)
-        job = CubeSynthJob(os.fsencode(atmos_path), xl, xh, yl, yh, enc(out_spectra), _ptr(st), int(chunk))
+        ll = None if line_level is None else np.ascontiguousarray(line_level, dtype=np.int32)
+        job = CubeSynthJob(os.fsencode(atmos_path), xl, xh, yl, yh, enc(out_spectra), _ptr(st), int(chunk),
+                           ali._ctx if ali is not None else None,
+                           ctypes.addressof(ali._prob) if ali is not None else None,
+                           ctypes.addressof(ali_tables.tab) if ali_tables is not None else None, _ptr(ll),
+                           int(ali_max_iter), float(ali_tol))
         stats = CubeStats()
         self._check(lib().snapi_cube_synth(self._ctx, ctypes.byref(job), ctypes.byref(stats)))
         return {"stokes": st, "stats": {k: getattr(stats, k) for k, _ in CubeStats._fields_}}

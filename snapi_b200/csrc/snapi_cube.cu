@@ -503,6 +503,16 @@ extern "C" int snapi_cube_invert(snapi_ctx *ctx, const snapi_lm_opts *opts, cons
 namespace {
 
 // rows [12][cap][nd] (the chunk's file rows) -> cols [n][12][nd]
+// T of columns [n][12][nd] floored at 3200 K in place (read_spinor3d's floor, which the records apply
+// themselves, for the NLTE set-up that reads the columns as given)
+__global__ void k_cube_floor_T(double *cols, int n, int nd) {
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < (long long)n * nd;
+       o += (long long)gridDim.x * blockDim.x) {
+    double *t = cols + (o / nd) * 12 * nd + 2 * nd + o % nd;
+    if (!(*t > 3200.0)) *t = 3200.0;
+  }
+}
+
 __global__ void k_cube_cols(const double *__restrict__ rows, int n, int cap, int nd, double *__restrict__ cols) {
   const long long m = (long long)n * 12 * nd;
   for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < m; o += (long long)gridDim.x * blockDim.x) {
@@ -525,10 +535,16 @@ struct SynthJob {
   size_t rows_bytes = 0, spec_bytes = 0;
   snapi_f0_file *f_spec = nullptr;
   long long bytes_read = 0, bytes_written = 0;
+  // an NLTE atom: the set-up's outputs (the iteration's columns), populations and statuses of a chunk
+  double *d_ali = nullptr;
+  snapi_ali_setup_out ali_out{};
+  double *d_pops = nullptr;
+  int *d_ast = nullptr;
 
   ~SynthJob() {
     if (fd >= 0) close(fd);
-    for (void *p : {(void *)d_rows, (void *)d_cols, (void *)d_spec, (void *)d_rec, (void *)d_stokes, (void *)d_st})
+    for (void *p : {(void *)d_rows, (void *)d_cols, (void *)d_spec, (void *)d_rec, (void *)d_stokes, (void *)d_st,
+                    (void *)d_ali, (void *)d_pops, (void *)d_ast})
       if (p) cudaFree(p);
     for (void *p : {(void *)rd.slot[0].h, (void *)rd.slot[1].h, (void *)wr.slot[0].h, (void *)wr.slot[1].h})
       if (p) cudaFreeHost(p);
@@ -611,7 +627,11 @@ extern "C" int snapi_cube_synth(snapi_ctx *ctx, const snapi_cube_synth_job *job,
   J.nx = xh - xl + 1; J.ny = yh - yl + 1;
   J.nl = ctx->nl;
   J.npix = (long long)J.nx * J.ny;
-  J.chunk = job->chunk > 0 ? job->chunk : 16384;
+  const bool nlte = job->ali != nullptr;
+  if (nlte && (!job->ali_prob || !job->ali_tables || !job->line_level || job->ali_prob->nd != J.nd))
+    return set_err(ctx, SNAPI_EINVAL, "snapi_cube_synth: an NLTE atom needs its problem (the cube's depths), set-up "
+                                      "tables and line levels");
+  J.chunk = job->chunk > 0 ? job->chunk : (nlte ? 2048 : 16384);
   if (J.chunk > J.npix) J.chunk = (int)J.npix;
   J.nchunk = (int)((J.npix + J.chunk - 1) / J.chunk);
   const int C = J.chunk, nd = J.nd, nl = J.nl, nf = ctx->nfield;
@@ -624,6 +644,28 @@ extern "C" int snapi_cube_synth(snapi_ctx *ctx, const snapi_cube_synth_job *job,
   SNAPI_CK(cudaMalloc(&J.d_stokes, sizeof(float) * (size_t)C * nl * 4));
   SNAPI_CK(cudaMalloc(&J.d_spec, J.spec_bytes));
   SNAPI_CK(cudaMalloc(&J.d_st, sizeof(int) * (size_t)C));
+  if (nlte) {  // the set-up's outputs in the layout of snapi_ali_columns, one block
+    const snapi_ali_problem &P = *job->ali_prob;
+    int nline = 0;
+    for (int t = 0; t < P.ntrans; ++t) nline += P.cont_of[P.trans[2 * t]] != P.trans[2 * t + 1];
+    const int nbf = P.ntrans - nline, nr = P.nray, nv = P.nlevel;
+    const size_t sz[11] = {(size_t)nd, (size_t)nd, (size_t)nd, (size_t)nd, (size_t)nr * nd, (size_t)nline * nd,
+                           (size_t)nline * nd, (size_t)nbf * nd, (size_t)nd * nv * nv, (size_t)nr * P.nlambda * nd,
+                           (size_t)nr * P.nlambda * nd};
+    size_t tot = 0;
+    for (size_t v : sz) tot += v;
+    SNAPI_CK(cudaMalloc(&J.d_ali, sizeof(double) * tot * C));
+    double *q = J.d_ali;
+    double **dst[11] = {&J.ali_out.T, &J.ali_out.ne, &J.ali_out.na, &J.ali_out.kappa, &J.ali_out.vray,
+                        &J.ali_out.dld, &J.ali_out.adamp, &J.ali_out.bfratio, &J.ali_out.coll, &J.ali_out.bg_op,
+                        &J.ali_out.bg_em};
+    for (int i = 0; i < 11; ++i) {
+      *dst[i] = q;
+      q += sz[i] * C;
+    }
+    SNAPI_CK(cudaMalloc(&J.d_pops, sizeof(double) * (size_t)C * nd * nv));
+    SNAPI_CK(cudaMalloc(&J.d_ast, sizeof(int) * (size_t)C));
+  }
   for (int i = 0; i < 2; ++i) {
     SNAPI_CK(cudaHostAlloc((void **)&J.rd.slot[i].h, J.rows_bytes, cudaHostAllocDefault));
     SNAPI_CK(cudaHostAlloc((void **)&J.wr.slot[i].h, J.spec_bytes, cudaHostAllocDefault));
@@ -681,6 +723,30 @@ extern "C" int snapi_cube_synth(snapi_ctx *ctx, const snapi_cube_synth_job *job,
         return stop(set_err(ctx, SNAPI_EINVAL,
                             "snapi_cube_synth: the log tau row of pixel %lld is not the context's depth grid", p0 + i));
       if (hst[i]) ++flagged;
+    }
+    if (nlte) {  // nltepops of the chunk's columns, then the NLTE atom's line fields
+      k_cube_floor_T<<<grid_for((long long)n * nd), kThreads, 0, ctx->stream>>>(J.d_cols, n, nd);
+      SYN_CK(cudaGetLastError());
+      ++launches;
+      st = snapi_ali_setup(ctx, job->ali_prob, job->ali_tables, n, J.d_cols, &J.ali_out, J.d_pops, J.d_ast,
+                           SNAPI_MEM_DEVICE);
+      if (st) return stop(st);
+      ker_ms += ctx->last_ms;
+      launches += ctx->last_launches;
+      const snapi_ali_columns ac = {J.ali_out.T,    J.ali_out.ne,      J.ali_out.na,    J.ali_out.kappa,
+                                    J.ali_out.vray, J.ali_out.dld,     J.ali_out.adamp, J.ali_out.bfratio,
+                                    J.ali_out.coll, J.ali_out.bg_op,   J.ali_out.bg_em};
+      st = snapi_ali_iter(job->ali, n, &ac, J.d_pops, job->ali_max_iter > 0 ? job->ali_max_iter : 100,
+                          job->ali_tol > 0.0 ? job->ali_tol : 1e-2, nullptr, nullptr, J.d_ast, SNAPI_MEM_DEVICE);
+      if (st) return stop(set_err(ctx, st, "snapi_cube_synth: %s", snapi_ali_last_error(job->ali)));
+      ker_ms += snapi_ali_last_kernel_ms(job->ali);
+      SYN_CK(cudaMemcpy(hst.data(), J.d_ast, sizeof(int) * n, cudaMemcpyDeviceToHost));
+      for (int i = 0; i < n; ++i)
+        if (hst[i] < 0) ++flagged;
+      st = snapi_records_set_populations(ctx, n, J.d_rec, J.d_pops, job->ali_prob->nlevel, job->line_level,
+                                         SNAPI_MEM_DEVICE);
+      if (st) return stop(st);
+      launches += ctx->last_launches;
     }
     st = snapi_synth(ctx, n, J.d_rec, J.d_stokes, SNAPI_MEM_DEVICE);
     if (st) return stop(st);

@@ -233,3 +233,31 @@ def test_device_setup_chunks(sb):
         np.testing.assert_array_equal(first[idx[ncol - n0:]], last, err_msg=n)
     ctx.close()
     ali.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", _params)
+def test_nlte_synthesis_job_over_a_cube(sb, name, tmp_path):
+    """The master's synthesis job (snapi_cube_synth) over an atmosphere cube of an NLTE atom's
+    columns: read_spinor3d's columns, nltepops per column (set-up and iteration on the device), the
+    NLTE line fields, the synthesis -- against the reference's obs_stokes of the same columns."""
+    fx = load_fixture(name)
+    tol = {"config5": 1e-2, "config5_spec": 1e-4}[name]
+    ctx, ali, tabs = _contexts(sb, fx)
+    cols = np.asarray(fx["alis_atm"], np.float64)  # [n][12][nd], pixel p = x * ny + y
+    n = cols.shape[0]
+    nx, ny = n, 1
+    cube = np.ascontiguousarray(cols.reshape(nx, ny, 12, -1).transpose(2, 0, 1, 3))
+    path = tmp_path / "atm.f0"
+    sb.api.f0_write(str(path), cube)
+    ll = sb.api.ali_line_levels(fx["eos_line_eos"], int(fx["alis_meta"][0]), fx["alis_lev"])
+    out = ctx.cube_synth(str(path), chunk=2, ali=ali, ali_tables=tabs, line_level=ll, ali_tol=tol)
+    S = out["stokes"].reshape(n, -1, 4)
+    ic = fx["stokes"][:, :, 0].max()
+    err = float(np.abs(S - fx["stokes"]).max() / ic)
+    print(name, "stats", out["stats"], "Stokes vs reference %.2e Ic" % err)
+    assert out["stats"]["flagged"] == 0 and out["stats"]["chunks"] == (n + 1) // 2
+    # the populations converge separately to the same stop (as the node-vector chain above)
+    assert err < 5e-5
+    ctx.close()
+    ali.close()
