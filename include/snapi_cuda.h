@@ -733,8 +733,9 @@ typedef struct {
    * set-up (snapi_ali_setup with ctx's atom tables, T floored at 3200 K as read_spinor3d floors it),
    * the level-population iteration (snapi_ali_iter on ali, from the LTE populations, up to
    * ali_max_iter iterations to ali_tol) and the NLTE atom's line fields from those populations
-   * (snapi_records_set_populations with line_level) before the synthesis.  A column whose
-   * populations stayed negative is counted in stats->flagged and synthesised with the last ones. */
+   * (snapi_records_set_populations with line_level) before the synthesis.  A column whose set-up
+   * chemistry was flagged (snapi_ali_setup's status) or whose populations stayed negative is
+   * counted in stats->flagged and synthesised with the last populations. */
   snapi_ali_ctx *ali;
   const snapi_ali_problem *ali_prob;       /* the problem ali was created with */
   const snapi_ali_setup_tables *ali_tables;

@@ -733,6 +733,8 @@ extern "C" int snapi_cube_synth(snapi_ctx *ctx, const snapi_cube_synth_job *job,
       if (st) return stop(st);
       ker_ms += ctx->last_ms;
       launches += ctx->last_launches;
+      std::vector<int> sst(n);  // the set-up's chemistry flags (cap, non-finite)
+      SYN_CK(cudaMemcpy(sst.data(), J.d_ast, sizeof(int) * n, cudaMemcpyDeviceToHost));
       const snapi_ali_columns ac = {J.ali_out.T,    J.ali_out.ne,      J.ali_out.na,    J.ali_out.kappa,
                                     J.ali_out.vray, J.ali_out.dld,     J.ali_out.adamp, J.ali_out.bfratio,
                                     J.ali_out.coll, J.ali_out.bg_op,   J.ali_out.bg_em};
@@ -740,9 +742,10 @@ extern "C" int snapi_cube_synth(snapi_ctx *ctx, const snapi_cube_synth_job *job,
                           job->ali_tol > 0.0 ? job->ali_tol : 1e-2, nullptr, nullptr, J.d_ast, SNAPI_MEM_DEVICE);
       if (st) return stop(set_err(ctx, st, "snapi_cube_synth: %s", snapi_ali_last_error(job->ali)));
       ker_ms += snapi_ali_last_kernel_ms(job->ali);
-      SYN_CK(cudaMemcpy(hst.data(), J.d_ast, sizeof(int) * n, cudaMemcpyDeviceToHost));
-      for (int i = 0; i < n; ++i)
-        if (hst[i] < 0) ++flagged;
+      std::vector<int> ast(n);  // the iteration's: -1 populations that stayed negative
+      SYN_CK(cudaMemcpy(ast.data(), J.d_ast, sizeof(int) * n, cudaMemcpyDeviceToHost));
+      for (int i = 0; i < n; ++i)  // hst: the records' flags, counted above
+        if (hst[i] == 0 && (sst[i] != 0 || ast[i] < 0)) ++flagged;
       st = snapi_records_set_populations(ctx, n, J.d_rec, J.d_pops, job->ali_prob->nlevel, job->line_level,
                                          SNAPI_MEM_DEVICE);
       if (st) return stop(st);
