@@ -862,10 +862,16 @@ struct EosArgs {
   double *F;              // [npix][nvar][nd][nf]: thermal fields of every variant (FP64)
   int *status;            // [npix]
   int warm;               // continued chemistry starts in the hydrostatic march (Chem::solve)
-  // k_eos_he: the depths [x0, x1) of the march; hs (x1 < nd or x0 > 0): the march's state between
-  // launches, [kHeStateWords][npix * nvar]
+  // k_eos_he: the depths [x0, x1) of the march; hs_in / hs_out (x0 > 0 / x1 < nd): the march's state
+  // at the segment's start / end, [kHeStateWords][npix * nvar] each (two buffers: a variant starting
+  // in this segment reads variant 0's start state while variant 0 writes its end state)
   int x0, x1;
-  double *hs;
+  const double *hs_in;
+  double *hs_out;
+  // [npix][nvar]: each variant's first depth whose temperature differs from variant 0's (above it
+  // the variant's march, records and fields are variant 0's, bit for bit); written by the march's
+  // first launch
+  int *xf;
   // k_eos_var: the depths [vx0, vx1)
   int vx0, vx1;
 };
@@ -874,8 +880,8 @@ constexpr int kHeStateWords = Chem::kStateWords + 6;
 // depth segments of the march with tangents: boundaries at these fractions of the depth count (the
 // record chemistry grows with depth: the temperature-node variants differ from the node vector only
 // below their nodes' first segment)
-constexpr int kHeMaxSeg = 4;
-constexpr double kHeSegFrac[kHeMaxSeg - 1] = {0.45, 0.7, 0.85};
+constexpr int kHeMaxSeg = 5;
+constexpr double kHeSegFrac[kHeMaxSeg - 1] = {0.28, 0.5, 0.7, 0.85};
 
 __device__ __forceinline__ void variant_pert(const EosDev &E, const EosArgs &A, int v, int &pidx, double &pert) {
   pidx = -1;
@@ -886,7 +892,26 @@ __device__ __forceinline__ void variant_pert(const EosDev &E, const EosArgs &A, 
   }
 }
 
-__global__ void __launch_bounds__(128) k_eos_he(EosArgs A) {  // launched with kHeCands threads
+// each temperature-node variant's first depth whose temperature differs from the node vector's
+// (interpolation only, before the march), thread = (pixel, variant > 0)
+__global__ void __launch_bounds__(kRecThreads) k_eos_xf(EosArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.npix * (A.nvar - 1)) return;
+  const int p = i % A.npix, v = 1 + i / A.npix;
+  if (A.active && !A.active[p]) return;
+  const EosDev &E = *A.tab;
+  NodeView nv{A.nodes + (size_t)p * A.npar, -1, 0.0};
+  variant_pert(E, A, v, nv.pidx, nv.pert);
+  const NodeView n0{A.nodes + (size_t)p * A.npar, -1, 0.0};
+  int xf = 0;
+  while (xf < A.nd && interp_kind(E, nv, 1, xf, true) == interp_kind(E, n0, 1, xf, true)) ++xf;
+  A.xf[(size_t)p * A.nvar + v] = xf;
+}
+
+// kSeg: a depth segment of the march with tangents (variants start where they first differ, the state
+// carried between launches); without: the whole march of every (pixel, variant) in one launch
+template <bool kSeg>
+__global__ void __launch_bounds__(128, 4) k_eos_he(EosArgs A) {  // launched with kHeCands threads; <= 128 registers
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nth = A.npix * A.nvar;
   if (i >= nth) return;
@@ -897,13 +922,22 @@ __global__ void __launch_bounds__(128) k_eos_he(EosArgs A) {  // launched with k
   variant_pert(E, A, v, nv.pidx, nv.pert);
   double *Tc = A.T + ((size_t)p * A.nvar + v) * A.nd;
   double *Nc = A.Nt + ((size_t)p * A.nvar + v) * A.nd;
+  // A temperature-node variant is variant 0 above the first depth whose temperature it moves: it
+  // runs no segment that ends above that depth, and starts in its first segment from variant 0's
+  // state at the segment's top (the same bits its own march would have reached there).
+  int xf = 0;  // k_eos_xf
+  if (kSeg && v > 0) {
+    xf = A.xf[(size_t)p * A.nvar + v];
+    if (xf >= A.x1) return;
+  }
+  const bool from_v0 = kSeg && v > 0 && A.x0 > 0 && xf >= A.x0;
   Chem c(E);
   double lev[kEL];
   double nH0;
   int st = 0;
   const bool warm = A.warm != 0;
   double Ntop, op_prev, rho_prev, Tprev, Nprev;
-  if (A.x0 == 0) {
+  if (!kSeg || A.x0 == 0) {
     // top: fixed point from 0.3 / k T (atmos_pp.cc:184-202)
     double T0 = interp_kind(E, nv, 1, 0, true);
     Tc[0] = T0;
@@ -924,8 +958,8 @@ __global__ void __launch_bounds__(128) k_eos_he(EosArgs A) {  // launched with k
     Ntop = Nt;
     Tprev = T0;
     Nprev = Nt;
-  } else {  // the state the previous segment left
-    const double *hs = A.hs + i;
+  } else {  // the state the previous segment left (variant 0's for a variant starting here)
+    const double *hs = A.hs_in + (from_v0 ? p : i);
     c.load_state(hs, (size_t)nth);
     const double *m = hs + (size_t)Chem::kStateWords * nth;
     Ntop = m[0];
@@ -934,7 +968,8 @@ __global__ void __launch_bounds__(128) k_eos_he(EosArgs A) {  // launched with k
     Tprev = m[3 * (size_t)nth];
     Nprev = m[4 * (size_t)nth];
   }
-  for (int x = A.x0 > 1 ? A.x0 : 1; x < A.x1; ++x) {
+  const int xb = kSeg ? A.x0 : 0, xe = kSeg ? A.x1 : A.nd;
+  for (int x = xb > 1 ? xb : 1; x < xe; ++x) {
     const double Tx = interp_kind(E, nv, 1, x, true);
     Tc[x] = Tx;
     const double delta_tau = pow(10.0, logtau(E, x)) - pow(10.0, logtau(E, x - 1));
@@ -958,8 +993,8 @@ __global__ void __launch_bounds__(128) k_eos_he(EosArgs A) {  // launched with k
     Tprev = Tx;
     Nprev = N;
   }
-  if (A.x1 < A.nd) {
-    double *hs = A.hs + i;
+  if (kSeg && A.x1 < A.nd) {
+    double *hs = A.hs_out + i;
     c.save_state(hs, (size_t)nth);
     double *m = hs + (size_t)Chem::kStateWords * nth;
     m[0] = Ntop;
@@ -1040,8 +1075,7 @@ __global__ void __launch_bounds__(256) k_eos_var(EosArgs A) {  // launched with 
   // A temperature-node variant leaves T, and so the march, bit-identical to variant 0 above the
   // first depth whose interpolation segment uses that node: its fields there are variant 0's
   // (k_eos_rec reads those), and the tangent's difference is exactly 0, as the reference's is.
-  const size_t c0 = (size_t)p * A.nvar * A.nd + x;
-  if (v > 0 && A.T[cv] == A.T[c0] && A.Nt[cv] == A.Nt[c0]) return;
+  if (v > 0 && x < A.xf[(size_t)p * A.nvar + v]) return;
   const EosDev &E = *A.tab;
   Chem c(E);
   int st = 0;
@@ -1087,7 +1121,7 @@ __global__ void __launch_bounds__(kRecThreads) k_eos_rec(EosArgs A) {
         // a variant identical to variant 0 at this depth has variant 0's fields (k_eos_var skips it)
         auto fields = [&](int w) {
           const size_t cw = ((size_t)p * A.nvar + w) * A.nd + x, cb = (size_t)p * A.nvar * A.nd + x;
-          return A.F + ((A.T[cw] == A.T[cb] && A.Nt[cw] == A.Nt[cb]) ? cb : cw) * nf;
+          return A.F + (x < A.xf[(size_t)p * A.nvar + w] ? cb : cw) * nf;
         };
         const double *Fp = fields(v);
         const double *Fm = fields(v + 1);
@@ -1243,9 +1277,12 @@ struct EosCtx {
   std::vector<snapi_eos_atom> atoms;
   void *d_su = nullptr;
   size_t cap_su = 0;
-  // the march in depth segments: its state between segments (cap_hs words)
+  // the march in depth segments: its state between segments (two buffers of cap_hs words), each
+  // variant's first moved depth (cap_xf entries)
   double *d_hs = nullptr;
   size_t cap_hs = 0;
+  int *d_xf = nullptr;
+  size_t cap_xf = 0;
 };
 
 void eos_free_bufs(EosCtx *e) {
@@ -1273,6 +1310,9 @@ void eos_free_bufs(EosCtx *e) {
   cudaFree(e->d_hs);
   e->d_hs = nullptr;
   e->cap_hs = 0;
+  cudaFree(e->d_xf);
+  e->d_xf = nullptr;
+  e->cap_xf = 0;
 }
 
 }  // namespace
@@ -1689,9 +1729,19 @@ static int build_impl(snapi_ctx *ctx, int npix, const double *nodes, const int *
     A.warm = e->chem_start == SNAPI_CHEM_START_CONTINUE;
     A.x0 = 0;
     A.x1 = nd;
-    A.hs = nullptr;
+    A.hs_in = nullptr;
+    A.hs_out = nullptr;
     A.vx0 = 0;
     A.vx1 = nd;
+    if ((size_t)nb * nvar > e->cap_xf) {
+      SNAPI_CK(cudaStreamSynchronize(ctx->stream));
+      cudaFree(e->d_xf);
+      e->d_xf = nullptr;
+      e->cap_xf = 0;
+      SNAPI_CK(cudaMalloc(&e->d_xf, sizeof(int) * (size_t)B * nvar));
+      e->cap_xf = (size_t)B * nvar;
+    }
+    A.xf = e->d_xf;
     if (host) {
       SNAPI_CK(cudaMemcpyAsync(e->d_nodes, nodes + (size_t)p0 * npar, sizeof(double) * nb * npar,
                                cudaMemcpyHostToDevice, ctx->stream));
@@ -1724,9 +1774,14 @@ static int build_impl(snapi_ctx *ctx, int npix, const double *nodes, const int *
       A.Nt_out = Nt ? Nt + (size_t)p0 * nd : nullptr;
     }
     SNAPI_CK(cudaMemsetAsync(e->d_status, 0, sizeof(int) * nb, ctx->stream));
+    if (nvar > 1) {  // the variants' first moved depths, read by the march, the record chemistry, the records
+      const int nx = nb * (nvar - 1);
+      k_eos_xf<<<(nx + kRecThreads - 1) / kRecThreads, kRecThreads, 0, ctx->stream>>>(A);
+      SNAPI_CK(cudaGetLastError());
+    }
     const int nhe = nb * nvar;
     const long long nvx = (long long)nb * nvar * nd;
-    auto launch_he = [&](int t) { k_eos_he<<<(nhe + t - 1) / t, t, 0, ctx->stream>>>(A); };
+    auto launch_he = [&](int t) { k_eos_he<false><<<(nhe + t - 1) / t, t, 0, ctx->stream>>>(A); };
     auto launch_var = [&](int t) {
       k_eos_var<<<(unsigned)((nvx + t - 1) / t), t, 0, ctx->stream>>>(A);
     };
@@ -1756,7 +1811,7 @@ static int build_impl(snapi_ctx *ctx, int npix, const double *nodes, const int *
         cudaFree(e->d_hs);
         e->d_hs = nullptr;
         e->cap_hs = 0;
-        SNAPI_CK(cudaMalloc(&e->d_hs, sizeof(double) * need));
+        SNAPI_CK(cudaMalloc(&e->d_hs, 2 * sizeof(double) * need));
         e->cap_hs = need;
       }
     }
@@ -1768,11 +1823,12 @@ static int build_impl(snapi_ctx *ctx, int npix, const double *nodes, const int *
       SNAPI_CK(cudaGetLastError());
       ctx->last_launches += 2;
     } else {
-      A.hs = e->d_hs;
       for (int k = 0; k < nseg; ++k) {
         A.x0 = A.vx0 = bounds[k];
         A.x1 = A.vx1 = bounds[k + 1];
-        k_eos_he<<<(nhe + cfg.he - 1) / cfg.he, cfg.he, 0, ctx->stream>>>(A);
+        A.hs_in = e->d_hs + (size_t)(k & 1) * e->cap_hs;
+        A.hs_out = e->d_hs + (size_t)((k + 1) & 1) * e->cap_hs;
+        k_eos_he<true><<<(nhe + cfg.he - 1) / cfg.he, cfg.he, 0, ctx->stream>>>(A);
         SNAPI_CK(cudaGetLastError());
         const long long nv_k = (long long)nb * nvar * (A.vx1 - A.vx0);
         k_eos_var<<<(unsigned)((nv_k + cfg.var - 1) / cfg.var), cfg.var, 0, ctx->stream>>>(A);
